@@ -1,0 +1,180 @@
+/* SPDX-License-Identifier: MIT
+ * pmb200 core: the rigid AVBD tick on one B200, behind a plain C ABI.
+ *
+ * This is the internal operator seam that the reference's CUDA backend
+ * implements with per-stage launch wrappers (reference
+ * src/simulation/geometry_constraints_dispatch.hpp:12-52 prepare/solve,
+ * src/simulation/geometry_dispatch.hpp and primitives.hpp for the spatial and
+ * contact stages, sequenced by emit_rigid_solve in
+ * src/simulation/production_realtime_backend.cu.inc:7664-7866). One call,
+ * pmb_world_step, runs the whole tick on the device: predict, swept proxies,
+ * broadphase, convex face narrowphase, contact cache, prepare, colouring,
+ * per-colour primal / dual solve, commit, speed clamp, cache save.
+ *
+ * Records are little-endian, 4-byte fields, tightly packed.
+ * Every function returns 0 on success or a negative PMB_ERROR_* code.
+ */
+#ifndef PMB200_CORE_H
+#define PMB200_CORE_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PMB_API __attribute__((visibility("default")))
+
+enum {
+    PMB_SUCCESS = 0,
+    PMB_ERROR_INVALID_ARGUMENT = -1,
+    PMB_ERROR_OUT_OF_DEVICE_MEMORY = -4,
+    PMB_ERROR_FEATURE_NOT_PRESENT = -5,
+    PMB_ERROR_CAPACITY_EXCEEDED = -7,
+    PMB_ERROR_DEVICE_LOST = -8,
+    PMB_ERROR_NO_DEVICE = -10
+};
+
+/* Status bits latched by a tick (pmb_step_stats.status). */
+enum {
+    PMB_STATUS_CANDIDATE_OVERFLOW = 1u << 0,
+    PMB_STATUS_CONTACT_OVERFLOW = 1u << 1,
+    PMB_STATUS_PAIR_OVERFLOW = 1u << 2,
+    PMB_STATUS_INVALID_BOUNDS = 1u << 3,
+    PMB_STATUS_BARRIER_TIMEOUT = 1u << 4,
+    PMB_STATUS_COLOR_OVERFLOW = 1u << 5,
+    PMB_STATUS_GRID_OVERFLOW = 1u << 6
+};
+
+/* BodyParameters order (reference src/slang/types.slang:81-95) without ids
+ * or user data. motion: 0 static, 1 kinematic, 2 dynamic. */
+typedef struct pmb_body {
+    uint32_t motion, mesh;
+    float inv_mass, inv_inertia[3], friction, restitution, linear_damping, angular_damping;
+    float max_linear_speed, max_angular_speed, margin;
+} pmb_body;
+
+/* RigidBodyState / PmRigidState: position, orientation (x,y,z,w), linear and
+ * angular velocity (reference include/parallel_mater/parallel_mater.h:392-397). */
+typedef struct pmb_state {
+    float x[3], q[4], v[3], w[3];
+} pmb_state;
+
+/* RigidConstraintOptions (reference src/slang/geometry.slang:95-113) with
+ * dense body indices. type: 0 fixed, 1 point, 2 hinge, 3 slider, 4 piston,
+ * 5 generic, 6 generic spring, 7 motor. */
+typedef struct pmb_joint {
+    uint32_t type, body_a, body_b;
+    float anchor_a[3], anchor_b[3], frame_a[4], frame_b[4];
+    uint32_t lin_limit_axes;
+    float lin_lower[3], lin_upper[3];
+    uint32_t ang_limit_axes;
+    float ang_lower[3], ang_upper[3];
+    uint32_t lin_spring_axes;
+    float lin_stiffness[3], lin_damping[3];
+    uint32_t ang_spring_axes;
+    float ang_stiffness[3], ang_damping[3];
+    uint32_t motor_linear, motor_angular;
+    float motor_linear_velocity, motor_linear_max_impulse;
+    float motor_angular_velocity, motor_angular_max_impulse;
+    uint32_t enabled, disable_collisions;
+    float breaking_threshold;
+    uint32_t solver_iterations;
+} pmb_joint;
+
+/* Scene description. Meshes are triangle meshes; mesh m owns vertices
+ * [vertex_offsets[m], vertex_offsets[m+1]) and indices [index_offsets[m],
+ * index_offsets[m+1]). Capacities of 0 select defaults sized from body_count. */
+typedef struct pmb_world_desc {
+    uint32_t body_count;
+    const pmb_body* bodies;
+    const pmb_state* states;
+    uint32_t mesh_count;
+    const uint32_t* vertex_offsets; /* mesh_count + 1 */
+    const float* vertices;          /* xyz */
+    const uint32_t* index_offsets;  /* mesh_count + 1 */
+    const uint32_t* indices;
+    uint32_t joint_count;
+    const pmb_joint* joints;
+    uint32_t candidate_capacity; /* broadphase pairs */
+    uint32_t pair_capacity;      /* non-empty manifolds */
+    uint32_t contact_capacity;   /* contact points */
+    int32_t device;              /* CUDA ordinal */
+} pmb_world_desc;
+
+/* profile: 1 = realtime v1 (8 sweeps, 5% damping), otherwise legacy
+ * (requested_iterations, or base_iterations raised by joint iteration hints,
+ * plus the velocity impact phase). residual_tolerance > 0 switches to the
+ * residual-driven schedule: sweep until the residual is at or below the
+ * tolerance, at most max_iterations sweeps. warm_start: 0 plain, 1 learned. */
+typedef struct pmb_step_desc {
+    float dt, gravity[3];
+    uint32_t profile, requested_iterations, base_iterations;
+    float residual_tolerance;
+    uint32_t max_iterations;
+} pmb_step_desc;
+
+typedef struct pmb_step_stats {
+    uint32_t candidate_pairs, active_pairs, contacts, colors, islands, iterations, impact, status;
+    float residual;
+} pmb_step_stats;
+
+typedef struct pmb_world pmb_world;
+
+/* Create a world on a CUDA device; uploads the scene and prepares meshes.
+ * Fails with PMB_ERROR_NO_DEVICE when no CUDA device is present: there is
+ * no CPU fallback. */
+PMB_API int pmb_world_create(const pmb_world_desc* desc, pmb_world** out);
+PMB_API void pmb_world_destroy(pmb_world* world);
+
+/* Bind a CUDA stream (cudaStream_t as void*) used by every later call. */
+PMB_API int pmb_world_set_stream(pmb_world* world, void* stream);
+
+/* One tick. Enqueued on the world's stream; returns without synchronising
+ * unless stats is non-null, in which case it waits and fills stats. */
+PMB_API int pmb_world_step(pmb_world* world, const pmb_step_desc* step, pmb_step_stats* stats);
+
+/* Capture `steps` ticks into a CUDA graph (replayed by pmb_world_replay). */
+PMB_API int pmb_world_capture(pmb_world* world, const pmb_step_desc* step, uint32_t steps);
+PMB_API int pmb_world_replay(pmb_world* world);
+
+/* Host <-> device state transfer (synchronous on the world's stream). */
+PMB_API int pmb_world_get_states(pmb_world* world, pmb_state* out);
+PMB_API int pmb_world_set_states(pmb_world* world, const pmb_state* in);
+/* Stats of the last tick (synchronises). */
+PMB_API int pmb_world_last_stats(pmb_world* world, pmb_step_stats* out);
+/* Linear and angular impulse applied by the next tick's predictor. */
+PMB_API int pmb_world_apply_impulse(pmb_world* world, uint32_t body, const float* linear, const float* angular);
+
+/* Inspection of the last tick (synchronous). Counts are returned even when
+ * the output pointer is null or the capacity is too small. */
+PMB_API int pmb_world_candidate_pairs(pmb_world* world, uint32_t* codes, uint32_t capacity, uint32_t* count);
+/* Per non-empty manifold: pair code, point count; 8 contact slots of 22
+ * floats (normal, point, penetration, error, dual lambda/penalty x3,
+ * anchor a, anchor b). */
+PMB_API int pmb_world_manifolds(pmb_world* world, uint32_t* codes, uint32_t* counts, float* contacts,
+                                uint32_t capacity, uint32_t* count);
+PMB_API int pmb_world_graph(pmb_world* world, uint32_t* colors, uint32_t* parents);
+PMB_API int pmb_world_residual_trace(pmb_world* world, float* out, uint32_t capacity, uint32_t* count);
+
+/* Snapshot / restore of the complete dynamic state (states, contact cache,
+ * warm-start history) into a second device buffer owned by the world. */
+PMB_API int pmb_world_snapshot(pmb_world* world);
+PMB_API int pmb_world_restore(pmb_world* world);
+
+/* Device pointer to the current states (pmb_state[body_count]) on the
+ * world's device, for callers that keep inputs resident. */
+PMB_API int pmb_world_device_states(pmb_world* world, void** device_ptr);
+
+/* Core AVBD math on the device, one thread per record, for parity checks
+ * against the CPU restatement. Host pointers; synchronous.
+ * block: in 27 floats (h[21], g[6]) -> out 7 floats (delta[6], solved).
+ * dual:  in 7 floats -> out 5 (warm lambda/penalty, force, updated lambda/penalty).
+ * contact: in 4 floats (trial n,t0,t1, friction) -> out 6 (projected, scales).
+ * row: in 42 floats -> out 7 (see tests). */
+PMB_API int pmb_math_eval(uint32_t kind, uint32_t count, const float* in, float* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,263 @@
+// SPDX-License-Identifier: MIT
+// Predict, swept proxies and broadphase.
+//
+// k_integrate fuses the reference's predictor (geometry.slang:524-612) with
+// its spatial proxy emitter (geometry.slang:716-827): one thread per body
+// writes the predicted state and the swept AABB min/max(prev, pred) +- (reach
+// + bounded correction).
+//
+// The reference builds a Karras LBVH over those AABBs and queries it per
+// dynamic body (primitives/spatial_build.slang:889-1011); the pair SET is
+// defined by the inclusive AABB overlap predicate (:631-635) and the filter of
+// geometry.slang:897-913, and its ORDER by (query body, candidate identity).
+// Here the same predicate is evaluated over a uniform grid whose cell is the
+// largest AABB extent among "small" bodies, so two overlapping small AABBs
+// always sit in adjacent cells; bodies beyond a size threshold (ground,
+// walls) are tested against every query. Cells are bucketed by the low bits
+// of their Morton code and bodies are placed by a one-pass counting sort; each
+// query's candidates are sorted by body index, which is the identity order of
+// a world built without removals. Pair codes are a*N+b as in the reference.
+#include "pmb_world.cuh"
+
+namespace pmb {
+
+__device__ __forceinline__ uint32_t expand10(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+__device__ __forceinline__ uint32_t cell_bucket(int cx, int cy, int cz, uint32_t size) {
+    uint32_t m = expand10(uint32_t(cx)) | (expand10(uint32_t(cy)) << 1) | (expand10(uint32_t(cz)) << 2);
+    uint32_t hi = (uint32_t(cx) >> 10) * 73856093u ^ (uint32_t(cy) >> 10) * 19349663u ^ (uint32_t(cz) >> 10) * 83492791u;
+    return (m ^ hi) & (size - 1u);
+}
+__device__ __forceinline__ int4 cell_of(float4 lo, float4 hi, float hs) {
+    V3 c = mul(add(v3(lo), v3(hi)), 0.5f);
+    return make_int4(int(floorf(c.x / hs)), int(floorf(c.y / hs)), int(floorf(c.z / hs)), 0);
+}
+
+// Per-body constants computed once on the device, with the reference's
+// operation order: reach = |centre| + radius + margin + 1e-5 and
+// correction = min(0.5, 0.25 * max(0, min extent)) for dynamic bodies.
+__global__ void k_body_constants(Dev d, const float4* mesh_lo, const float4* mesh_hi, const float4* mesh_sphere) {
+    for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
+        uint32_t m = d.mesh[i];
+        V3 lo = v3(mesh_lo[m]), hi = v3(mesh_hi[m]);
+        float4 sph = mesh_sphere[m];
+        float4 p2 = d.p2[i];
+        float corr = 0.0f;
+        if (d.motion[i] == kDynamic) {
+            V3 e = sub(hi, lo);
+            corr = fmn(0.5f, 0.25f * fmx(0.0f, fmn(e.x, fmn(e.y, e.z))));
+        }
+        p2.w = corr;
+        d.p2[i] = p2;
+        float reach = len(v3(sph)) + sph.w + p2.z + 1.0e-5f;
+        d.expand[i] = fmn(1.0f, corr) + reach;
+        V3 ma{fmx(fab(lo.x), fab(hi.x)), fmx(fab(lo.y), fab(hi.y)), fmx(fab(lo.z), fab(hi.z))};
+        d.rotb[i] = len(ma);
+    }
+}
+void launch_body_constants(const Dev& d, const float4* lo, const float4* hi, const float4* sph, cudaStream_t s) {
+    k_body_constants<<<blocks_for(d.n), kBlock, 0, s>>>(d, lo, hi, sph);
+}
+
+__global__ void k_integrate(Dev d, StepParams sp, float4* ox, float4* oq, float4* ov, float4* ow) {
+    const float dt = sp.dt;
+    const V3 g{sp.gx, sp.gy, sp.gz};
+    for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
+        const uint32_t motion = d.motion[i];
+        float4 x = d.x[i], q = d.q[i], v = d.v[i], w = d.w[i];
+        V3 nx = v3(x), nv = v3(v), nw = v3(w);
+        Q4 nq = q4(q);
+        if (motion != kDynamic) {
+            nv = {0, 0, 0};
+            nw = {0, 0, 0};
+        } else {
+            const float4 p0 = d.p0[i], p1 = d.p1[i], p2 = d.p2[i];
+            const V3 force{0, 0, 0};
+            nv = add(nv, mul(add(g, mul(force, p0.x)), dt));
+            nw = add(nw, mul(inv_inertia_world(p0, nq, V3{0, 0, 0}), dt));
+            nv = add(nv, mul(v3(d.lin_imp[i]), p0.x));
+            nw = add(nw, inv_inertia_world(p0, nq, v3(d.ang_imp[i])));
+            nv = mul(nv, 1.0f / (1.0f + p1.z * dt));
+            nw = mul(nw, 1.0f / (1.0f + p1.w * dt));
+            nv = clamp_length(nv, p2.x);
+            nw = clamp_length(nw, p2.y);
+            nx = add(nx, mul(nv, dt));
+            Q4 dq = qmul(Q4{nw.x, nw.y, nw.z, 0.0f}, nq);
+            nq = qnormalize(Q4{nq.x + 0.5f * dq.x * dt, nq.y + 0.5f * dq.y * dt, nq.z + 0.5f * dq.z * dt,
+                               nq.w + 0.5f * dq.w * dt});
+            d.lin_imp[i] = make_float4(0, 0, 0, 0);
+            d.ang_imp[i] = make_float4(0, 0, 0, 0);
+        }
+        // The predicted state is both the AVBD target and the initial solved
+        // state (bodies the solve does not move keep it).
+        d.tx[i] = ox[i] = f4(nx);
+        d.tq[i] = oq[i] = f4(nq);
+        d.tv[i] = ov[i] = f4(nv);
+        d.tw[i] = ow[i] = f4(nw);
+        // Swept proxy.
+        const float e = d.expand[i];
+        const V3 ex{e, e, e};
+        V3 lo = sub(vmin(v3(x), nx), ex), hi = add(vmax(v3(x), nx), ex);
+        d.lo[i] = f4(lo);
+        d.hi[i] = f4(hi);
+        bool finite = isfinite(lo.x) && isfinite(lo.y) && isfinite(lo.z) && isfinite(hi.x) && isfinite(hi.y) &&
+                      isfinite(hi.z);
+        V3 ext = sub(hi, lo);
+        float m = fmx(ext.x, fmx(ext.y, ext.z));
+        if (!finite) {
+            atomicOr(&d.ctr->status, kStInvalidBounds);
+            d.is_large[i] = 2;  // excluded
+            continue;
+        }
+        if (m > d.large_extent) {
+            d.is_large[i] = 1;
+            uint32_t slot = atomicAdd(&d.ctr->n_large, 1u);
+            d.large_list[slot] = i;
+        } else {
+            d.is_large[i] = 0;
+            atomicMax(reinterpret_cast<int*>(&d.ctr->hs), __float_as_int(m));
+        }
+    }
+}
+
+void launch_integrate(const Dev& d, const StepParams& sp, cudaStream_t s, const SolveBuffers& o) {
+    k_integrate<<<blocks_for(d.n), kBlock, 0, s>>>(d, sp, o.ox, o.oq, o.ov, o.ow);
+}
+
+__global__ void k_grid_count(Dev d) {
+    const float hs = d.ctr->hs > 0.0f ? d.ctr->hs : 1.0f;
+    for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
+        if (d.is_large[i] != 0) continue;
+        int4 c = cell_of(d.lo[i], d.hi[i], hs);
+        d.grid_cell[i] = c;
+        atomicAdd(&d.bucket_count[cell_bucket(c.x, c.y, c.z, d.grid_size)], 1u);
+    }
+}
+
+__global__ void k_grid_scatter(Dev d) {
+    for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
+        if (d.is_large[i] != 0) continue;
+        int4 c = d.grid_cell[i];
+        uint32_t b = cell_bucket(c.x, c.y, c.z, d.grid_size);
+        uint32_t slot = d.bucket_off[b] + atomicAdd(&d.bucket_cursor[b], 1u);
+        d.grid_body[slot] = i;
+    }
+}
+
+__device__ __forceinline__ bool aabb_overlap(float4 alo, float4 ahi, float4 blo, float4 bhi) {
+    return ahi.x >= blo.x && ahi.y >= blo.y && ahi.z >= blo.z && bhi.x >= alo.x && bhi.y >= alo.y && bhi.z >= alo.z;
+}
+
+__device__ __forceinline__ bool collision_disabled(const Dev& d, uint32_t a, uint32_t b) {
+    if (d.n_dis == 0) return false;
+    const uint64_t* keys = reinterpret_cast<const uint64_t*>(d.dis_keys);
+    uint64_t key = (uint64_t(a < b ? a : b) << 32) | uint64_t(a < b ? b : a);
+    uint32_t lo = 0, hi = d.n_dis;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (keys[mid] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo < d.n_dis && keys[lo] == key;
+}
+
+// Candidate predicate: overlap (leaf b against query a), a != b, identity
+// order between two dynamic bodies, no collision-disabling joint.
+__device__ __forceinline__ bool candidate(const Dev& d, uint32_t a, uint32_t b, float4 alo, float4 ahi) {
+    if (b == a || d.is_large[b] == 2) return false;
+    if (!aabb_overlap(d.lo[b], d.hi[b], alo, ahi)) return false;
+    if (d.motion[b] == kDynamic && !(a < b)) return false;
+    if (collision_disabled(d, a, b)) return false;
+    return true;
+}
+
+template <bool kWrite> __device__ uint32_t visit_candidates(const Dev& d, uint32_t a, uint32_t* out, uint32_t cap) {
+    const float4 alo = d.lo[a], ahi = d.hi[a];
+    uint32_t count = 0;
+    auto emit = [&](uint32_t b) {
+        if (kWrite && count < cap) out[count] = b;
+        ++count;
+    };
+    const uint32_t nl = d.ctr->n_large;
+    for (uint32_t k = 0; k < nl; ++k) {
+        uint32_t b = d.large_list[k];
+        if (candidate(d, a, b, alo, ahi)) emit(b);
+    }
+    if (d.is_large[a] == 1) {
+        for (uint32_t b = 0; b < d.n; ++b)
+            if (d.is_large[b] == 0 && candidate(d, a, b, alo, ahi)) emit(b);
+        return count;
+    }
+    const int4 c = d.grid_cell[a];
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                int cx = c.x + dx, cy = c.y + dy, cz = c.z + dz;
+                uint32_t bk = cell_bucket(cx, cy, cz, d.grid_size);
+                uint32_t s = d.bucket_off[bk], e = d.bucket_off[bk + 1];
+                for (uint32_t k = s; k < e; ++k) {
+                    uint32_t b = d.grid_body[k];
+                    int4 cb = d.grid_cell[b];
+                    if (cb.x != cx || cb.y != cy || cb.z != cz) continue;
+                    if (candidate(d, a, b, alo, ahi)) emit(b);
+                }
+            }
+    return count;
+}
+
+__global__ void k_query_count(Dev d) {
+    for (uint32_t a = grid_stride_begin(); a < d.n; a += grid_stride()) {
+        uint32_t c = 0;
+        if (d.motion[a] == kDynamic && d.is_large[a] != 2) c = visit_candidates<false>(d, a, nullptr, 0);
+        d.cand_count[a] = c;
+    }
+}
+
+__global__ void k_query_write(Dev d) {
+    const uint32_t total = d.ctr->n_cand;
+    if (grid_stride_begin() == 0 && total > d.cap_cand) atomicOr(&d.ctr->status, kStCandidateOverflow);
+    for (uint32_t a = grid_stride_begin(); a < d.n; a += grid_stride()) {
+        uint32_t c = d.cand_count[a];
+        if (c == 0) continue;
+        uint32_t off = d.cand_off[a];
+        if (off >= d.cap_cand) continue;
+        uint32_t cap = min(c, d.cap_cand - off);
+        uint32_t* seg = d.cand_b + off;
+        visit_candidates<true>(d, a, seg, cap);
+        // Insertion sort by identity (dense index).
+        for (uint32_t i = 1; i < cap; ++i) {
+            uint32_t v = seg[i];
+            uint32_t j = i;
+            while (j > 0 && seg[j - 1] > v) {
+                seg[j] = seg[j - 1];
+                --j;
+            }
+            seg[j] = v;
+        }
+        for (uint32_t i = 0; i < cap; ++i) d.cand_a[off + i] = a;
+    }
+}
+
+__global__ void k_clamp_count(uint32_t* count, uint32_t cap) {
+    if (*count > cap) *count = cap;
+}
+
+void launch_broadphase(const Dev& d, cudaStream_t s) {
+    cudaMemsetAsync(d.bucket_count, 0, sizeof(uint32_t) * (d.grid_size + 1), s);
+    cudaMemsetAsync(d.bucket_cursor, 0, sizeof(uint32_t) * d.grid_size, s);
+    k_grid_count<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    scan_u32(d.bucket_count, d.bucket_off, nullptr, d.grid_size, nullptr, d.scan_tmp32, s);
+    k_grid_scatter<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    k_query_count<<<blocks_for(d.n, 128), 128, 0, s>>>(d);
+    scan_u32(d.cand_count, d.cand_off, nullptr, d.n, &d.ctr->n_cand, d.scan_tmp32, s);
+    k_query_write<<<blocks_for(d.n, 128), 128, 0, s>>>(d);
+    k_clamp_count<<<1, 1, 0, s>>>(&d.ctr->n_cand, d.cap_cand);
+}
+
+}  // namespace pmb

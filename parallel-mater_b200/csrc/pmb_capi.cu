@@ -1,0 +1,690 @@
+// SPDX-License-Identifier: MIT
+// C ABI of the pmb200 core (include/pmb200_core.h): world allocation and
+// upload, the tick sequence, graph capture, inspection and snapshots.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/pmb200_core.h"
+#include "pmb_joint.cuh"
+#include "pmb_mesh.hpp"
+
+namespace pmb {
+__global__ void k_math_eval(uint32_t kind, uint32_t count, const float* in, float* out);
+
+int coop_blocks_for(const void* kernel, int threads, size_t smem) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem);
+    return std::max(1, per) * sms;
+}
+}  // namespace pmb
+
+using namespace pmb;
+
+struct pmb_world {
+    int device{};
+    cudaStream_t stream{};
+    bool own_stream{};
+    Dev d{};
+    SolveBuffers out{};
+    std::vector<void*> allocs;
+    std::vector<std::pair<void*, size_t>> dynamic_state;  // snapshot set
+    std::vector<void*> snapshot;
+    int coop_solve{}, coop_color{};
+    cudaGraphExec_t graph{};
+    uint32_t step_parity{}, snapshot_parity{};
+    Counters host_ctr{};
+};
+
+namespace {
+
+template <class T> int alloc(pmb_world* w, T*& p, size_t count) {
+    p = nullptr;
+    if (count == 0) count = 1;
+    if (cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * count) != cudaSuccess) return PMB_ERROR_OUT_OF_DEVICE_MEMORY;
+    w->allocs.push_back(p);
+    cudaMemsetAsync(p, 0, sizeof(T) * count, w->stream);
+    return PMB_SUCCESS;
+}
+template <class T> int alloc_state(pmb_world* w, T*& p, size_t count) {
+    int r = alloc(w, p, count);
+    if (r == PMB_SUCCESS) w->dynamic_state.push_back({p, sizeof(T) * (count ? count : 1)});
+    return r;
+}
+
+uint32_t next_pow2(uint32_t v) {
+    uint32_t p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+StepParams params_from(const pmb_step_desc& s) {
+    StepParams p{};
+    p.dt = s.dt;
+    p.gx = s.gravity[0];
+    p.gy = s.gravity[1];
+    p.gz = s.gravity[2];
+    p.realtime = s.profile == 1 ? 1u : 0u;
+    p.requested = s.requested_iterations;
+    p.budget_request = p.realtime ? 8u : (s.requested_iterations ? s.requested_iterations : s.base_iterations);
+    p.tolerance = s.residual_tolerance;
+    p.max_iterations = s.max_iterations;
+    return p;
+}
+
+__global__ void k_reset_counters(Counters* c) {
+    // bar_gen is left alone: it only ever increases.
+    uint32_t* w = reinterpret_cast<uint32_t*>(c);
+    const uint32_t words = sizeof(Counters) / 4;
+    const uint32_t skip = offsetof(Counters, bar_gen) / 4;
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x)
+        if (i != skip) w[i] = 0;
+}
+
+void enqueue_step(pmb_world* w, const StepParams& sp) {
+    cudaStream_t s = w->stream;
+    Dev& d = w->d;
+    k_reset_counters<<<1, 256, 0, s>>>(d.ctr);
+    launch_integrate(d, sp, s, w->out);
+    launch_broadphase(d, s);
+    launch_narrowphase(d, sp, s);
+    launch_prepare(d, sp, s);
+    launch_graph(d, sp, s, w->coop_color);
+    launch_solve_all(d, sp, s, w->coop_solve, w->out);
+    // The cache written this tick is read by the next one.
+    std::swap(d.sv_code, d.out_code);
+    std::swap(d.sv_off, d.out_off);
+    std::swap(d.sv_cnt, d.out_cnt);
+    std::swap(d.sv_n_pairs, d.out_n_pairs);
+    std::swap(d.sv_local, d.out_local);
+    std::swap(d.sv_normal, d.out_normal);
+    std::swap(d.sv_fimp, d.out_fimp);
+    std::swap(d.sv_lam, d.out_lam);
+    std::swap(d.sv_pen, d.out_pen);
+    std::swap(d.sv_aa, d.out_aa);
+    std::swap(d.sv_ab, d.out_ab);
+    std::swap(d.sv_dt, d.out_dt);
+    w->step_parity ^= 1u;
+}
+
+void swap_cache(pmb_world* w) {
+    Dev& d = w->d;
+    std::swap(d.sv_code, d.out_code);
+    std::swap(d.sv_off, d.out_off);
+    std::swap(d.sv_cnt, d.out_cnt);
+    std::swap(d.sv_n_pairs, d.out_n_pairs);
+    std::swap(d.sv_local, d.out_local);
+    std::swap(d.sv_normal, d.out_normal);
+    std::swap(d.sv_fimp, d.out_fimp);
+    std::swap(d.sv_lam, d.out_lam);
+    std::swap(d.sv_pen, d.out_pen);
+    std::swap(d.sv_aa, d.out_aa);
+    std::swap(d.sv_ab, d.out_ab);
+    std::swap(d.sv_dt, d.out_dt);
+    w->step_parity ^= 1u;
+}
+
+int check(cudaError_t e) {
+    if (e == cudaSuccess) return PMB_SUCCESS;
+    if (e == cudaErrorMemoryAllocation) return PMB_ERROR_OUT_OF_DEVICE_MEMORY;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return PMB_ERROR_NO_DEVICE;
+    std::fprintf(stderr, "pmb200: CUDA error %s\n", cudaGetErrorString(e));
+    return PMB_ERROR_DEVICE_LOST;
+}
+
+void fill_stats(const Counters& c, pmb_step_stats* s) {
+    s->candidate_pairs = c.n_cand;
+    s->active_pairs = c.n_act;
+    s->contacts = c.n_contacts;
+    s->colors = c.colors;
+    s->islands = c.islands;
+    s->iterations = c.iterations;
+    s->impact = c.impact;
+    s->status = c.status;
+    s->residual = c.residual;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
+    if (!desc || !out || desc->body_count == 0 || !desc->bodies || !desc->states || desc->mesh_count == 0)
+        return PMB_ERROR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return PMB_ERROR_NO_DEVICE;
+    if (desc->device < 0 || desc->device >= ndev) return PMB_ERROR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < desc->body_count; ++i)
+        if (desc->bodies[i].mesh >= desc->mesh_count || desc->bodies[i].motion > 2) return PMB_ERROR_INVALID_ARGUMENT;
+    for (uint32_t j = 0; j < desc->joint_count; ++j)
+        if (desc->joints[j].type > 7) return PMB_ERROR_INVALID_ARGUMENT;
+    pmb_world* w = new (std::nothrow) pmb_world;
+    if (!w) return PMB_ERROR_OUT_OF_DEVICE_MEMORY;
+    w->device = desc->device;
+    cudaSetDevice(w->device);
+    if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete w;
+        return PMB_ERROR_NO_DEVICE;
+    }
+    w->own_stream = true;
+    Dev& d = w->d;
+    const uint32_t n = desc->body_count, nm = desc->mesh_count, nj = desc->joint_count;
+    d.n = n;
+    d.nm = nm;
+    d.nj = nj;
+    d.cap_cand = desc->candidate_capacity ? desc->candidate_capacity : 64u * n + 4096u;
+    d.cap_pair = desc->pair_capacity ? desc->pair_capacity : 24u * n + 1024u;
+    d.cap_contact = desc->contact_capacity ? desc->contact_capacity : 64u * n + 4096u;
+    d.cap_stage = d.cap_contact;
+    d.grid_size = next_pow2(std::max(2u * n, 1024u));
+
+    // ---- meshes (host preparation, then upload)
+    std::vector<uint32_t> m_vo(nm), m_vc(nm), m_to(nm), m_tc(nm), m_convex(nm);
+    std::vector<float4> verts, planes, mlo(nm), mhi(nm), msph(nm);
+    for (uint32_t m = 0; m < nm; ++m) {
+        const uint32_t v0 = desc->vertex_offsets[m], v1 = desc->vertex_offsets[m + 1];
+        const uint32_t i0 = desc->index_offsets[m], i1 = desc->index_offsets[m + 1];
+        if (v1 <= v0 || i1 < i0 || (i1 - i0) % 3) {
+            pmb_world_destroy(w);
+            return PMB_ERROR_INVALID_ARGUMENT;
+        }
+        for (uint32_t k = i0; k < i1; ++k)
+            if (desc->indices[k] >= v1 - v0) {
+                pmb_world_destroy(w);
+                return PMB_ERROR_INVALID_ARGUMENT;
+            }
+        PreparedMesh pm = prepare_mesh(desc->vertices + 3 * size_t(v0), v1 - v0, desc->indices + i0, i1 - i0);
+        const uint32_t nt = (i1 - i0) / 3;
+        m_vo[m] = uint32_t(verts.size());
+        m_vc[m] = v1 - v0;
+        for (uint32_t k = v0; k < v1; ++k)
+            verts.push_back(make_float4(desc->vertices[3 * k], desc->vertices[3 * k + 1], desc->vertices[3 * k + 2], 0));
+        m_to[m] = uint32_t(planes.size());
+        m_tc[m] = nt;
+        m_convex[m] = pm.convex && (i1 - i0) <= 96 ? 1u : 0u;
+        for (uint32_t t = 0; t < nt; ++t)
+            planes.push_back(pm.convex ? make_float4(pm.planes[t][0], pm.planes[t][1], pm.planes[t][2], pm.planes[t][3])
+                                       : make_float4(0, 0, 0, 0));
+        for (uint32_t t = 0; t < nt; ++t) {
+            float4 pk;
+            uint32_t tri[3] = {pm.indices[3 * t], pm.indices[3 * t + 1], pm.indices[3 * t + 2]};
+            std::memcpy(&pk.x, &tri[0], 4);
+            std::memcpy(&pk.y, &tri[1], 4);
+            std::memcpy(&pk.z, &tri[2], 4);
+            pk.w = 0;
+            planes.push_back(pk);
+        }
+        mlo[m] = make_float4(pm.lo[0], pm.lo[1], pm.lo[2], 0);
+        mhi[m] = make_float4(pm.hi[0], pm.hi[1], pm.hi[2], 0);
+        msph[m] = make_float4(pm.center[0], pm.center[1], pm.center[2], pm.radius);
+    }
+
+    int r = PMB_SUCCESS;
+#define ALLOC(p, c) if (r == PMB_SUCCESS) r = alloc(w, p, c)
+#define ALLOCS(p, c) if (r == PMB_SUCCESS) r = alloc_state(w, p, c)
+    ALLOC(d.motion, n); ALLOC(d.mesh, n); ALLOC(d.p0, n); ALLOC(d.p1, n); ALLOC(d.p2, n);
+    ALLOC(d.expand, n); ALLOC(d.rotb, n);
+    ALLOCS(d.x, n); ALLOCS(d.q, n); ALLOCS(d.v, n); ALLOCS(d.w, n);
+    ALLOC(d.tx, n); ALLOC(d.tq, n); ALLOC(d.tv, n); ALLOC(d.tw, n);
+    ALLOC(w->out.ox, n); ALLOC(w->out.oq, n); ALLOC(w->out.ov, n); ALLOC(w->out.ow, n);
+    ALLOCS(d.lin_imp, n); ALLOCS(d.ang_imp, n);
+    ALLOC(d.m_vo, nm); ALLOC(d.m_vc, nm); ALLOC(d.m_to, nm); ALLOC(d.m_tc, nm); ALLOC(d.m_convex, nm);
+    ALLOC(d.m_verts, verts.size()); ALLOC(d.m_planes, planes.size());
+    ALLOC(d.dxl, n); ALLOC(d.dxa, n); ALLOC(d.dq, n); ALLOC(d.inA, n); ALLOC(d.inB, n);
+    ALLOCS(d.prev_vel, n); ALLOCS(d.color, n);
+    ALLOC(d.parent, n); ALLOC(d.impact, n); ALLOC(d.anchored, n); ALLOC(d.mean, n);
+    ALLOC(d.lo, n); ALLOC(d.hi, n); ALLOC(d.is_large, n); ALLOC(d.large_list, n);
+    ALLOC(d.bucket_count, d.grid_size + 1); ALLOC(d.bucket_off, d.grid_size + 1); ALLOC(d.bucket_cursor, d.grid_size);
+    ALLOC(d.grid_body, n); ALLOC(d.grid_cell, n);
+    ALLOC(d.cand_count, n + 1); ALLOC(d.cand_off, n + 1);
+    ALLOC(d.cand_a, d.cap_cand); ALLOC(d.cand_b, d.cap_cand);
+    ALLOC(d.np_count, d.cap_cand); ALLOC(d.np_scan, d.cap_cand + 1); ALLOC(d.np_stage, d.cap_cand);
+    ALLOC(d.st_n, d.cap_stage); ALLOC(d.st_p, d.cap_stage);
+    ALLOC(d.act_a, d.cap_pair); ALLOC(d.act_b, d.cap_pair); ALLOC(d.act_code, d.cap_pair);
+    ALLOC(d.act_off, d.cap_pair + 1); ALLOC(d.act_cnt, d.cap_pair); ALLOC(d.act_impact, d.cap_pair);
+    ALLOC(d.c_pair, d.cap_contact);
+    ALLOC(d.c_n, d.cap_contact); ALLOC(d.c_p, d.cap_contact); ALLOC(d.c_e, d.cap_contact);
+    ALLOC(d.c_aa, d.cap_contact); ALLOC(d.c_ab, d.cap_contact); ALLOC(d.c_lam, d.cap_contact);
+    ALLOC(d.c_pen, d.cap_contact); ALLOC(d.c_accf, d.cap_contact);
+    for (int side = 0; side < 2; ++side) {
+        uint32_t** code = side ? &d.out_code : &d.sv_code;
+        uint32_t** off = side ? &d.out_off : &d.sv_off;
+        uint32_t** cnt = side ? &d.out_cnt : &d.sv_cnt;
+        uint32_t** np = side ? &d.out_n_pairs : &d.sv_n_pairs;
+        float4** f[7] = {side ? &d.out_local : &d.sv_local, side ? &d.out_normal : &d.sv_normal,
+                         side ? &d.out_fimp : &d.sv_fimp, side ? &d.out_lam : &d.sv_lam,
+                         side ? &d.out_pen : &d.sv_pen, side ? &d.out_aa : &d.sv_aa, side ? &d.out_ab : &d.sv_ab};
+        float** dtp = side ? &d.out_dt : &d.sv_dt;
+        ALLOCS(*code, d.cap_pair); ALLOCS(*off, d.cap_pair); ALLOCS(*cnt, d.cap_pair); ALLOCS(*np, 1);
+        for (auto* p : f) ALLOCS(*p, d.cap_contact);
+        ALLOCS(*dtp, 1);
+    }
+    ALLOC(d.deg, n); ALLOC(d.inc_off, n + 1); ALLOC(d.inc_cursor, n); ALLOC(d.inc_list, 2 * size_t(d.cap_pair));
+    ALLOC(d.jdeg, n); ALLOC(d.jinc_off, n + 1); ALLOC(d.jinc_cursor, n); ALLOC(d.jinc_list, 2 * size_t(nj) + 2);
+    ALLOC(d.corder, n);
+    ALLOC(d.joints, nj); ALLOCS(d.jstate, nj); ALLOCS(d.jrows, size_t(nj) * 18);
+    {
+        // Scan scratch: one slot per 2048-element tile of the longest scan plus the total.
+        size_t longest = std::max<size_t>({d.cap_cand, d.grid_size, n, d.cap_pair});
+        size_t tiles = (longest + 2047) / 2048 + 2;
+        ALLOC(d.scan_tmp, tiles); ALLOC(d.scan_tmp32, tiles);
+    }
+    ALLOC(d.ctr, 1);
+    float4 *dlo = nullptr, *dhi = nullptr, *dsph = nullptr;
+    ALLOC(dlo, nm); ALLOC(dhi, nm); ALLOC(dsph, nm);
+    uint64_t* dis = nullptr;
+    std::vector<uint64_t> dis_keys;
+    for (uint32_t j = 0; j < nj; ++j) {
+        const pmb_joint& o = desc->joints[j];
+        if (o.enabled && o.disable_collisions) {
+            uint64_t a = std::min(o.body_a, o.body_b), b = std::max(o.body_a, o.body_b);
+            dis_keys.push_back((a << 32) | b);
+        }
+    }
+    std::sort(dis_keys.begin(), dis_keys.end());
+    dis_keys.erase(std::unique(dis_keys.begin(), dis_keys.end()), dis_keys.end());
+    ALLOC(dis, dis_keys.size());
+    d.dis_keys = reinterpret_cast<uint32_t*>(dis);
+    d.n_dis = uint32_t(dis_keys.size());
+#undef ALLOC
+#undef ALLOCS
+    if (r != PMB_SUCCESS) {
+        pmb_world_destroy(w);
+        return r;
+    }
+    // ---- upload
+    std::vector<uint32_t> motion(n), mesh(n);
+    std::vector<float4> p0(n), p1(n), p2(n), x(n), q(n), v(n), wv(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const pmb_body& b = desc->bodies[i];
+        motion[i] = b.motion;
+        mesh[i] = b.mesh;
+        p0[i] = make_float4(b.inv_mass, b.inv_inertia[0], b.inv_inertia[1], b.inv_inertia[2]);
+        p1[i] = make_float4(b.friction, b.restitution, b.linear_damping, b.angular_damping);
+        p2[i] = make_float4(b.max_linear_speed, b.max_angular_speed, b.margin, 0.0f);
+        const pmb_state& s = desc->states[i];
+        Q4 qq = qnormalize(Q4{s.q[0], s.q[1], s.q[2], s.q[3]});
+        x[i] = make_float4(s.x[0], s.x[1], s.x[2], 0);
+        q[i] = f4(qq);
+        v[i] = make_float4(s.v[0], s.v[1], s.v[2], 0);
+        wv[i] = make_float4(s.w[0], s.w[1], s.w[2], 0);
+    }
+    cudaStream_t s = w->stream;
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        if (bytes) cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+    };
+    up(d.motion, motion.data(), 4 * n);
+    up(d.mesh, mesh.data(), 4 * n);
+    up(d.p0, p0.data(), 16 * n);
+    up(d.p1, p1.data(), 16 * n);
+    up(d.p2, p2.data(), 16 * n);
+    up(d.x, x.data(), 16 * n);
+    up(d.q, q.data(), 16 * n);
+    up(d.v, v.data(), 16 * n);
+    up(d.w, wv.data(), 16 * n);
+    up(d.m_vo, m_vo.data(), 4 * nm);
+    up(d.m_vc, m_vc.data(), 4 * nm);
+    up(d.m_to, m_to.data(), 4 * nm);
+    up(d.m_tc, m_tc.data(), 4 * nm);
+    up(d.m_convex, m_convex.data(), 4 * nm);
+    up(d.m_verts, verts.data(), 16 * verts.size());
+    up(d.m_planes, planes.data(), 16 * planes.size());
+    up(dlo, mlo.data(), 16 * nm);
+    up(dhi, mhi.data(), 16 * nm);
+    up(dsph, msph.data(), 16 * nm);
+    if (nj) up(d.joints, desc->joints, sizeof(Joint) * nj);
+    if (!dis_keys.empty()) up(dis, dis_keys.data(), 8 * dis_keys.size());
+    std::vector<uint32_t> colors(n, kInvalid);
+    up(d.color, colors.data(), 4 * n);
+    launch_body_constants(d, dlo, dhi, dsph, s);
+    // Bodies larger than 4x the median proxy extent are tested by brute force.
+    std::vector<float> expand(n);
+    cudaMemcpyAsync(expand.data(), d.expand, 4 * n, cudaMemcpyDeviceToHost, s);
+    r = check(cudaStreamSynchronize(s));
+    if (r != PMB_SUCCESS) {
+        pmb_world_destroy(w);
+        return r;
+    }
+    std::vector<float> sorted = expand;
+    std::nth_element(sorted.begin(), sorted.begin() + n / 2, sorted.end());
+    d.large_extent = 2.0f * sorted[n / 2] * 4.0f;
+    w->coop_solve = coop_blocks_for(solve_kernel_ptr, kBlock, 0);
+    w->coop_color = coop_blocks_for(color_kernel_ptr, kBlock, 0);
+    for (auto& p : w->dynamic_state) {
+        void* snap = nullptr;
+        if (cudaMalloc(&snap, p.second) != cudaSuccess) {
+            pmb_world_destroy(w);
+            return PMB_ERROR_OUT_OF_DEVICE_MEMORY;
+        }
+        w->snapshot.push_back(snap);
+    }
+    *out = w;
+    return PMB_SUCCESS;
+}
+
+void pmb_world_destroy(pmb_world* w) {
+    if (!w) return;
+    cudaSetDevice(w->device);
+    if (w->stream) cudaStreamSynchronize(w->stream);
+    if (w->graph) cudaGraphExecDestroy(w->graph);
+    for (void* p : w->allocs) cudaFree(p);
+    for (void* p : w->snapshot) cudaFree(p);
+    if (w->own_stream && w->stream) cudaStreamDestroy(w->stream);
+    delete w;
+}
+
+int pmb_world_set_stream(pmb_world* w, void* stream) {
+    if (!w) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    cudaStreamSynchronize(w->stream);
+    if (w->own_stream) cudaStreamDestroy(w->stream);
+    w->own_stream = false;
+    w->stream = static_cast<cudaStream_t>(stream);
+    return PMB_SUCCESS;
+}
+
+int pmb_world_step(pmb_world* w, const pmb_step_desc* step, pmb_step_stats* stats) {
+    if (!w || !step || !(step->dt > 0.0f)) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    enqueue_step(w, params_from(*step));
+    int r = check(cudaGetLastError());
+    if (r != PMB_SUCCESS) return r;
+    if (stats) return pmb_world_last_stats(w, stats);
+    return PMB_SUCCESS;
+}
+
+int pmb_world_capture(pmb_world* w, const pmb_step_desc* step, uint32_t steps) {
+    if (!w || !step || steps == 0 || (steps & 1u)) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    if (w->graph) {
+        cudaGraphExecDestroy(w->graph);
+        w->graph = nullptr;
+    }
+    StepParams sp = params_from(*step);
+    cudaGraph_t g;
+    int r = check(cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal));
+    if (r != PMB_SUCCESS) return r;
+    for (uint32_t k = 0; k < steps; ++k) enqueue_step(w, sp);
+    r = check(cudaStreamEndCapture(w->stream, &g));
+    if (r != PMB_SUCCESS) return r;
+    r = check(cudaGraphInstantiate(&w->graph, g, 0));
+    cudaGraphDestroy(g);
+    return r;
+}
+
+int pmb_world_replay(pmb_world* w) {
+    if (!w || !w->graph) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    return check(cudaGraphLaunch(w->graph, w->stream));
+}
+
+int pmb_world_last_stats(pmb_world* w, pmb_step_stats* out) {
+    if (!w || !out) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    cudaMemcpyAsync(&w->host_ctr, w->d.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, w->stream);
+    int r = check(cudaStreamSynchronize(w->stream));
+    if (r != PMB_SUCCESS) return r;
+    fill_stats(w->host_ctr, out);
+    return PMB_SUCCESS;
+}
+
+int pmb_world_get_states(pmb_world* w, pmb_state* out) {
+    if (!w || !out) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    const uint32_t n = w->d.n;
+    std::vector<float4> x(n), q(n), v(n), wv(n);
+    cudaMemcpyAsync(x.data(), w->d.x, 16 * n, cudaMemcpyDeviceToHost, w->stream);
+    cudaMemcpyAsync(q.data(), w->d.q, 16 * n, cudaMemcpyDeviceToHost, w->stream);
+    cudaMemcpyAsync(v.data(), w->d.v, 16 * n, cudaMemcpyDeviceToHost, w->stream);
+    cudaMemcpyAsync(wv.data(), w->d.w, 16 * n, cudaMemcpyDeviceToHost, w->stream);
+    int r = check(cudaStreamSynchronize(w->stream));
+    if (r != PMB_SUCCESS) return r;
+    for (uint32_t i = 0; i < n; ++i) {
+        out[i] = {{x[i].x, x[i].y, x[i].z}, {q[i].x, q[i].y, q[i].z, q[i].w}, {v[i].x, v[i].y, v[i].z},
+                  {wv[i].x, wv[i].y, wv[i].z}};
+    }
+    return PMB_SUCCESS;
+}
+
+int pmb_world_set_states(pmb_world* w, const pmb_state* in) {
+    if (!w || !in) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    const uint32_t n = w->d.n;
+    std::vector<float4> x(n), q(n), v(n), wv(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        x[i] = make_float4(in[i].x[0], in[i].x[1], in[i].x[2], 0);
+        q[i] = make_float4(in[i].q[0], in[i].q[1], in[i].q[2], in[i].q[3]);
+        v[i] = make_float4(in[i].v[0], in[i].v[1], in[i].v[2], 0);
+        wv[i] = make_float4(in[i].w[0], in[i].w[1], in[i].w[2], 0);
+    }
+    cudaMemcpyAsync(w->d.x, x.data(), 16 * n, cudaMemcpyHostToDevice, w->stream);
+    cudaMemcpyAsync(w->d.q, q.data(), 16 * n, cudaMemcpyHostToDevice, w->stream);
+    cudaMemcpyAsync(w->d.v, v.data(), 16 * n, cudaMemcpyHostToDevice, w->stream);
+    cudaMemcpyAsync(w->d.w, wv.data(), 16 * n, cudaMemcpyHostToDevice, w->stream);
+    return check(cudaStreamSynchronize(w->stream));
+}
+
+int pmb_world_apply_impulse(pmb_world* w, uint32_t body, const float* linear, const float* angular) {
+    if (!w || body >= w->d.n) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    float4 l{0, 0, 0, 0}, a{0, 0, 0, 0};
+    cudaMemcpyAsync(&l, w->d.lin_imp + body, 16, cudaMemcpyDeviceToHost, w->stream);
+    cudaMemcpyAsync(&a, w->d.ang_imp + body, 16, cudaMemcpyDeviceToHost, w->stream);
+    cudaStreamSynchronize(w->stream);
+    if (linear) { l.x += linear[0]; l.y += linear[1]; l.z += linear[2]; }
+    if (angular) { a.x += angular[0]; a.y += angular[1]; a.z += angular[2]; }
+    cudaMemcpyAsync(w->d.lin_imp + body, &l, 16, cudaMemcpyHostToDevice, w->stream);
+    cudaMemcpyAsync(w->d.ang_imp + body, &a, 16, cudaMemcpyHostToDevice, w->stream);
+    return check(cudaStreamSynchronize(w->stream));
+}
+
+int pmb_world_candidate_pairs(pmb_world* w, uint32_t* codes, uint32_t capacity, uint32_t* count) {
+    if (!w) return PMB_ERROR_INVALID_ARGUMENT;
+    pmb_step_stats st;
+    int r = pmb_world_last_stats(w, &st);
+    if (r) return r;
+    const uint32_t n = w->host_ctr.n_cand;
+    if (count) *count = n;
+    if (codes && capacity >= n && n) {
+        std::vector<uint32_t> a(n), b(n);
+        cudaMemcpy(a.data(), w->d.cand_a, 4 * n, cudaMemcpyDeviceToHost);
+        cudaMemcpy(b.data(), w->d.cand_b, 4 * n, cudaMemcpyDeviceToHost);
+        for (uint32_t k = 0; k < n; ++k) codes[k] = a[k] * w->d.n + b[k];
+    }
+    return check(cudaGetLastError());
+}
+
+int pmb_world_manifolds(pmb_world* w, uint32_t* codes, uint32_t* counts, float* contacts, uint32_t capacity,
+                        uint32_t* count) {
+    if (!w) return PMB_ERROR_INVALID_ARGUMENT;
+    pmb_step_stats st;
+    int r = pmb_world_last_stats(w, &st);
+    if (r) return r;
+    const uint32_t n = w->host_ctr.n_act, nc = w->host_ctr.n_contacts;
+    if (count) *count = n;
+    if (!codes || capacity < n || n == 0) return PMB_SUCCESS;
+    std::vector<uint32_t> off(n), cnt(n);
+    cudaMemcpy(codes, w->d.act_code, 4 * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(off.data(), w->d.act_off, 4 * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(cnt.data(), w->d.act_cnt, 4 * n, cudaMemcpyDeviceToHost);
+    if (counts) std::memcpy(counts, cnt.data(), 4 * n);
+    if (contacts) {
+        std::vector<float4> cn(nc), cp(nc), ce(nc), cl(nc), ck(nc), ca(nc), cb(nc);
+        cudaMemcpy(cn.data(), w->d.c_n, 16 * nc, cudaMemcpyDeviceToHost);
+        cudaMemcpy(cp.data(), w->d.c_p, 16 * nc, cudaMemcpyDeviceToHost);
+        cudaMemcpy(ce.data(), w->d.c_e, 16 * nc, cudaMemcpyDeviceToHost);
+        cudaMemcpy(cl.data(), w->d.c_lam, 16 * nc, cudaMemcpyDeviceToHost);
+        cudaMemcpy(ck.data(), w->d.c_pen, 16 * nc, cudaMemcpyDeviceToHost);
+        cudaMemcpy(ca.data(), w->d.c_aa, 16 * nc, cudaMemcpyDeviceToHost);
+        cudaMemcpy(cb.data(), w->d.c_ab, 16 * nc, cudaMemcpyDeviceToHost);
+        std::memset(contacts, 0, sizeof(float) * 22 * 8 * size_t(n));
+        for (uint32_t k = 0; k < n; ++k)
+            for (uint32_t p = 0; p < cnt[k] && p < 8; ++p) {
+                const uint32_t c = off[k] + p;
+                float* o = contacts + (size_t(k) * 8 + p) * 22;
+                float v[22] = {cn[c].x, cn[c].y, cn[c].z, cp[c].x, cp[c].y, cp[c].z, cn[c].w, ce[c].x,
+                               ce[c].y, ce[c].z, cl[c].x, ck[c].x, cl[c].y, ck[c].y, cl[c].z, ck[c].z,
+                               ca[c].x, ca[c].y, ca[c].z, cb[c].x, cb[c].y, cb[c].z};
+                std::memcpy(o, v, sizeof(v));
+            }
+    }
+    return check(cudaGetLastError());
+}
+
+int pmb_world_graph(pmb_world* w, uint32_t* colors, uint32_t* parents) {
+    if (!w) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    cudaStreamSynchronize(w->stream);
+    if (colors) cudaMemcpy(colors, w->d.color, 4 * w->d.n, cudaMemcpyDeviceToHost);
+    if (parents) cudaMemcpy(parents, w->d.parent, 4 * w->d.n, cudaMemcpyDeviceToHost);
+    return check(cudaGetLastError());
+}
+
+int pmb_world_residual_trace(pmb_world* w, float* out, uint32_t capacity, uint32_t* count) {
+    if (!w) return PMB_ERROR_INVALID_ARGUMENT;
+    pmb_step_stats st;
+    int r = pmb_world_last_stats(w, &st);
+    if (r) return r;
+    uint32_t n = std::min<uint32_t>(w->host_ctr.iterations, kMaxIterations);
+    if (count) *count = n;
+    if (out)
+        for (uint32_t k = 0; k < n && k < capacity; ++k) out[k] = w->host_ctr.residual_trace[k];
+    return PMB_SUCCESS;
+}
+
+int pmb_world_snapshot(pmb_world* w) {
+    if (!w) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    w->snapshot_parity = w->step_parity;
+    for (size_t k = 0; k < w->dynamic_state.size(); ++k)
+        cudaMemcpyAsync(w->snapshot[k], w->dynamic_state[k].first, w->dynamic_state[k].second,
+                        cudaMemcpyDeviceToDevice, w->stream);
+    return check(cudaStreamSynchronize(w->stream));
+}
+
+int pmb_world_restore(pmb_world* w) {
+    if (!w) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    if (w->step_parity != w->snapshot_parity) swap_cache(w);
+    for (size_t k = 0; k < w->dynamic_state.size(); ++k)
+        cudaMemcpyAsync(w->dynamic_state[k].first, w->snapshot[k], w->dynamic_state[k].second,
+                        cudaMemcpyDeviceToDevice, w->stream);
+    return check(cudaStreamSynchronize(w->stream));
+}
+
+int pmb_world_device_states(pmb_world* w, void** device_ptr) {
+    if (!w || !device_ptr) return PMB_ERROR_INVALID_ARGUMENT;
+    *device_ptr = w->d.x;
+    return PMB_SUCCESS;
+}
+
+int pmb_math_eval(uint32_t kind, uint32_t count, const float* in, float* out) {
+    static const uint32_t in_w[4] = {27, 7, 4, 42}, out_w[4] = {7, 5, 6, 7};
+    if (kind > 3 || !in || !out) return PMB_ERROR_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return PMB_ERROR_NO_DEVICE;
+    if (count == 0) return PMB_SUCCESS;
+    float *din = nullptr, *dout = nullptr;
+    if (cudaMalloc(&din, 4 * size_t(count) * in_w[kind]) != cudaSuccess) return PMB_ERROR_OUT_OF_DEVICE_MEMORY;
+    if (cudaMalloc(&dout, 4 * size_t(count) * out_w[kind]) != cudaSuccess) {
+        cudaFree(din);
+        return PMB_ERROR_OUT_OF_DEVICE_MEMORY;
+    }
+    cudaMemcpy(din, in, 4 * size_t(count) * in_w[kind], cudaMemcpyHostToDevice);
+    k_math_eval<<<(count + 127) / 128, 128>>>(kind, count, din, dout);
+    cudaMemcpy(out, dout, 4 * size_t(count) * out_w[kind], cudaMemcpyDeviceToHost);
+    int r = check(cudaGetLastError());
+    cudaFree(din);
+    cudaFree(dout);
+    return r;
+}
+
+}  // extern "C"
+
+namespace pmb {
+__global__ void k_math_eval(uint32_t kind, uint32_t count, const float* in, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    if (kind == 0) {
+        const float* v = in + 27 * size_t(i);
+        Blk b;
+        for (int k = 0; k < 21; ++k) b.h[k] = v[k];
+        for (int k = 0; k < 6; ++k) b.g[k] = v[21 + k];
+        V6 dd;
+        bool ok = block_solve(b, dd);
+        float* o = out + 7 * size_t(i);
+        for (int k = 0; k < 6; ++k) o[k] = dd.v[k];
+        o[6] = ok ? 1.0f : 0.0f;
+    } else if (kind == 1) {
+        const float* v = in + 7 * size_t(i);
+        Dual du{v[0], v[1]};
+        Dual ws = warm_start(du, v[6]);
+        Dual up = update_dual(du, v[2], v[3], v[4], v[5], v[6]);
+        float* o = out + 5 * size_t(i);
+        o[0] = ws.lambda;
+        o[1] = ws.penalty;
+        o[2] = dual_force(du, v[2], v[4], v[5]);
+        o[3] = up.lambda;
+        o[4] = up.penalty;
+    } else if (kind == 2) {
+        const float* v = in + 4 * size_t(i);
+        F3 t{v[0], v[1], v[2]};
+        F3 p = project_contact(t, v[3]), s = stiffness_scales(t, v[3]);
+        float* o = out + 6 * size_t(i);
+        o[0] = p.n;
+        o[1] = p.t0;
+        o[2] = p.t1;
+        o[3] = s.n;
+        o[4] = s.t0;
+        o[5] = s.t1;
+    } else {
+        const float* v = in + 42 * size_t(i);
+        Row r;
+        for (int k = 0; k < 6; ++k) {
+            r.a.v[k] = v[k];
+            r.b.v[k] = v[6 + k];
+        }
+        r.dual = {v[12], v[13]};
+        r.error = v[14];
+        r.velocity = v[15];
+        r.lower = v[16];
+        r.upper = v[17];
+        r.stiffness = v[18];
+        r.damping = v[19];
+        r.beta = v[20];
+        r.reference_force = v[21];
+        V6 a, b;
+        for (int k = 0; k < 6; ++k) {
+            a.v[k] = v[22 + k];
+            b.v[k] = v[28 + k];
+        }
+        const float dt = v[34];
+        Blk blk;
+        for (int k = 0; k < 21; ++k) blk.h[k] = 0.0f;
+        for (int k = 0; k < 6; ++k) {
+            blk.g[k] = 0.0f;
+            blk.h[bidx(k, k)] = v[35 + k];
+        }
+        row_accumulate(blk, r, v[41] != 0.0f, a, b, dt);
+        Row adv = row_advance(r, a, b);
+        float* o = out + 7 * size_t(i);
+        o[0] = row_error(r, a, b);
+        o[1] = row_trial(r, a, b, dt);
+        o[2] = row_force(r, a, b, dt);
+        o[3] = adv.dual.lambda;
+        o[4] = adv.dual.penalty;
+        float gs = 0, ds = 0;
+        for (int k = 0; k < 6; ++k) {
+            gs += blk.g[k];
+            ds += blk.h[bidx(k, k)];
+        }
+        o[5] = gs;
+        o[6] = ds;
+    }
+}
+}  // namespace pmb

@@ -1,0 +1,402 @@
+// SPDX-License-Identifier: MIT
+// AVBD prepare and the constraint graph.
+//
+// The reference prepares on one 128-thread block and builds the graph on
+// lane 0 alone (geometry_constraints.slang:1213-1591). Here every part runs
+// across the grid:
+//   bodies    inertia blocks and the history-weighted gravity displacement
+//   contacts  cold anchors, normal/tangent errors, warm-started duals
+//   joints    row initialisation (visit_joint, init)
+//   graph     per-body incident lists (CSR, descending pair index: the order
+//             of the reference's head-inserted linked lists), islands by a
+//             lock-free union-find that always hooks the larger root under
+//             the smaller (so every root is its island's lowest index, as the
+//             reference's serial union-find leaves it), impact marking
+//   colours   the reference's first-fit greedy colouring in body-index order,
+//             which gives body v the smallest colour absent among its
+//             lower-index dynamic neighbours. That colouring is the unique
+//             fixpoint of "colour(v) = mex(colours of lower neighbours)", so
+//             a persistent kernel iterates that map from the previous tick's
+//             colours until a round changes nothing: the result equals the
+//             serial colouring exactly, in few rounds when the graph changed
+//             little.
+#include "pmb_joint.cuh"
+
+namespace pmb {
+
+__global__ void k_prepare_bodies(Dev d, StepParams sp) {
+    const float dt = sp.dt;
+    const V3 g{sp.gx, sp.gy, sp.gz};
+    for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
+        const float4 pv = d.prev_vel[i];
+        const V3 old_v = v3(pv);
+        const bool hist = pv.w != 0.0f;
+        d.parent[i] = i;
+        d.impact[i] = 0;
+        d.anchored[i] = 0;
+        d.mean[i] = make_float4(0, 0, 0, 0);
+        d.dq[i] = make_float4(0, 0, 0, 1);
+        d.dxa[i] = make_float4(0, 0, 0, 0);
+        d.deg[i] = 0;
+        d.jdeg[i] = 0;
+        d.inc_cursor[i] = 0;
+        d.jinc_cursor[i] = 0;
+        if (d.motion[i] != kDynamic) {
+            d.color[i] = kInvalid;
+            d.prev_vel[i] = make_float4(0, 0, 0, 0);
+            d.dxl[i] = make_float4(0, 0, 0, 0);
+            d.inA[i] = make_float4(0, 0, 0, 0);
+            d.inB[i] = make_float4(0, 0, 0, 0);
+            continue;
+        }
+        if (d.color[i] == kInvalid) d.color[i] = 0;
+        const V3 vprev = v3(d.v[i]);
+        float g2 = len2(g);
+        V3 acc = mul(sub(vprev, old_v), 1.0f / dt);
+        float wgt = hist && g2 > 0.0f ? fclamp(dot(acc, g) / g2, 0.0f, 1.0f) : 0.0f;
+        if (!isfinite(wgt)) wgt = 0.0f;
+        V3 corr = mul(g, -(1.0f - wgt) * dt * dt);
+        d.dxl[i] = f4(corr);
+        d.prev_vel[i] = f4(vprev, 1.0f);
+        const float4 p0 = d.p0[i];
+        const float mass = 1.0f / fmx(p0.x, 1.0e-12f);
+        const Q4 q = q4(d.tq[i]);
+        float h[6];  // h33 h43 h53 h44 h54 h55
+        float inv[3] = {p0.y, p0.z, p0.w};
+        for (unsigned ax = 0; ax < 3; ++ax) {
+            V3 la = inv_rotate(q, unit_axis(ax));
+            V3 col = rotate(q, V3{la.x / fmx(inv[0], 1.0e-12f), la.y / fmx(inv[1], 1.0e-12f),
+                                  la.z / fmx(inv[2], 1.0e-12f)});
+            for (unsigned r = ax; r < 3; ++r) {
+                float v = comp(col, r) / (dt * dt);
+                if (ax == 0) h[r] = v;
+                else if (ax == 1) h[2 + r] = v;
+                else h[5] = v;
+            }
+        }
+        d.inA[i] = make_float4(mass / (dt * dt), h[0], h[1], h[3]);
+        d.inB[i] = make_float4(h[2], h[4], h[5], 0.0f);
+    }
+}
+
+__device__ __forceinline__ float pair_stiffness(float ima, float imb, float dt) {
+    return 1.0f / (fmx(ima + imb, 1.0e-6f) * dt * dt);
+}
+
+// geometry_constraints.slang:1297-1389 and the impact test :983-1006.
+__global__ void k_prepare_pairs(Dev d, StepParams sp) {
+    const float dt = sp.dt;
+    const bool realtime = sp.realtime != 0;
+    const uint32_t n_act = d.ctr->n_act;
+    for (uint32_t i = grid_stride_begin(); i < n_act; i += grid_stride()) {
+        const uint32_t a = d.act_a[i], b = d.act_b[i];
+        const float4 pa0 = d.p0[a], pb0 = d.p0[b], pa1 = d.p1[a], pb1 = d.p1[b], pa2 = d.p2[a], pb2 = d.p2[b];
+        const float penalty = pair_stiffness(pa0.x, pb0.x, dt);
+        const V3 xa0 = v3(d.x[a]), xb0 = v3(d.x[b]), xa = v3(d.tx[a]), xb = v3(d.tx[b]);
+        const Q4 qa0 = q4(d.q[a]), qb0 = q4(d.q[b]), qa = q4(d.tq[a]), qb = q4(d.tq[b]);
+        const float skin = fmn(pa2.z + pb2.z, 1.0e-3f) + 2.0f * 1.0e-5f;
+        const V3 mo_a = sub(xa, xa0), mo_b = sub(xb, xb0);
+        const V3 an_a = mul(delta_velocity(qa0, qa, dt), dt);
+        const V3 an_b = mul(delta_velocity(qb0, qb, dt), dt);
+        const uint32_t off = d.act_off[i], cnt = d.act_cnt[i];
+        bool impact = false;
+        for (uint32_t p = 0; p < cnt; ++p) {
+            const uint32_t c = off + p;
+            const float4 n4 = d.c_n[c], p4 = d.c_p[c];
+            float4 aa = d.c_aa[c], ab = d.c_ab[c];
+            const bool cached = aa.w != 0.0f;
+            const V3 n = v3(n4), pt = v3(p4);
+            const float pen = n4.w;
+            V3 anc_a = v3(aa), anc_b = v3(ab);
+            if (!cached) {
+                anc_a = inv_rotate(qa0, sub(pt, xa0));
+                anc_b = inv_rotate(qb0, sub(pt, xb0));
+                d.c_aa[c] = f4(anc_a, 0.0f);
+                d.c_ab[c] = f4(anc_b, 0.0f);
+            }
+            const V3 arm_a = sub(pt, xa), arm_b = sub(pt, xb);
+            const float closing = dot(n, sub(add(mo_b, cross(an_b, arm_b)), add(mo_a, cross(an_a, arm_a))));
+            const float old_pen = pen - closing;
+            V3 t0, t1;
+            basis(n, t0, t1);
+            const V3 anchor_motion = add(sub(mo_b, mo_a), sub(rotation_displacement(qb0, qb, anc_b),
+                                                              rotation_displacement(qa0, qa, anc_a)));
+            const V3 old_delta = !cached ? V3{0, 0, 0}
+                                         : add(sub(xb0, xa0), sub(rotate(qb0, anc_b), rotate(qa0, anc_a)));
+            const V3 terr = add(anchor_motion, mul(old_delta, 1.0f - kAlpha));
+            const float speed = -closing / dt;
+            const float impact_disp = realtime && !cached && speed < -0.1f
+                                          ? -(1.0f + fmn(pa1.y, pb1.y)) * speed * dt
+                                          : 0.0f;
+            const V3 err{pen - fclamp(old_pen, 0.0f, skin) + impact_disp, dot(terr, t0), dot(terr, t1)};
+            d.c_e[c] = f4(err, speed);
+            float4 lam = d.c_lam[c], pk = d.c_pen[c];
+            Dual du[3];
+            if (cached) {
+                du[0] = {lam.x, pk.x};
+                du[1] = {lam.y, pk.y};
+                du[2] = {lam.z, pk.z};
+            } else {
+                du[0] = du[1] = du[2] = {0.0f, penalty};
+            }
+            for (int x = 0; x < 3; ++x) du[x] = warm_start(du[x], kMaxPenalty);
+            d.c_lam[c] = make_float4(du[0].lambda, du[1].lambda, du[2].lambda, lam.w);
+            d.c_pen[c] = make_float4(du[0].penalty, du[1].penalty, du[2].penalty, 0.0f);
+            const float impact_fraction = p4.w;
+            bool fresh = (!cached || du[0].lambda <= 1.0e-6f || (impact_fraction > 0.0f && impact_fraction < 1.0f)) &&
+                         speed < -0.1f && pen >= -1.0e-5f;
+            float prev_pen = pen + speed * dt;
+            impact = impact || fresh || prev_pen > skin + 1.0e-4f;
+        }
+        d.act_impact[i] = impact ? 1u : 0u;
+    }
+}
+
+__global__ void k_prepare_joints(Dev d, StepParams sp) {
+    const float dt = sp.dt;
+    for (uint32_t j = grid_stride_begin(); j < d.nj; j += grid_stride()) {
+        JointState st = d.jstate[j];
+        const Joint& o = d.joints[j];
+        st.count = 0;
+        st.enabled = (o.enabled != 0 && st.broken == 0) ? 1u : 0u;
+        if (st.enabled) {
+            st.applied = 0.0f;
+            st.dense_a = o.body_a < d.n ? o.body_a : kInvalid;
+            st.dense_b = o.body_b < d.n ? o.body_b : kInvalid;
+            if (st.dense_a != kInvalid && st.dense_b != kInvalid) {
+                const uint32_t a = st.dense_a, b = st.dense_b;
+                BodyView A = load_body(d, a), B = load_body(d, b);
+                Blk scratch{};
+                uint32_t count = 0;
+                visit_joint(o, d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]), q4(d.q[b]),
+                            d.p0[a], d.p0[b], dt, &scratch, true, kVisitInit, &count, nullptr);
+                st.count = count;
+            }
+        }
+        d.jstate[j] = st;
+    }
+}
+
+// ---------------------------------------------------------------- graph
+// Lock-free union-find over parent[] with parent[i] <= i: finds shorten paths
+// in place, unions hook the larger root under the smaller by CAS.
+__device__ uint32_t uf_find(uint32_t* parent, uint32_t i) {
+    volatile uint32_t* P = parent;
+    uint32_t cur = P[i];
+    if (cur != i) {
+        uint32_t prev = i, next;
+        while (cur > (next = P[cur])) {
+            P[prev] = next;
+            prev = cur;
+            cur = next;
+        }
+    }
+    return cur;
+}
+__device__ void uf_unite(uint32_t* parent, uint32_t a, uint32_t b) {
+    uint32_t ra = uf_find(parent, a), rb = uf_find(parent, b);
+    for (int guard = 0; guard < (1 << 24) && ra != rb; ++guard) {
+        if (ra < rb) {
+            uint32_t old = atomicCAS(&parent[rb], rb, ra);
+            if (old == rb) return;
+            rb = old;
+        } else {
+            uint32_t old = atomicCAS(&parent[ra], ra, rb);
+            if (old == ra) return;
+            ra = old;
+        }
+    }
+}
+
+__global__ void k_graph_degrees(Dev d, StepParams sp) {
+    const uint32_t n_act = d.ctr->n_act;
+    for (uint32_t i = grid_stride_begin(); i < n_act; i += grid_stride()) {
+        const uint32_t a = d.act_a[i], b = d.act_b[i];
+        const bool da = d.motion[a] == kDynamic, db = d.motion[b] == kDynamic;
+        if (da) atomicAdd(&d.deg[a], 1u);
+        if (db) atomicAdd(&d.deg[b], 1u);
+        if (da && db) uf_unite(d.parent, a, b);
+        if (d.act_impact[i]) d.ctr->impact = 1;
+    }
+    for (uint32_t j = grid_stride_begin(); j < d.nj; j += grid_stride()) {
+        const JointState st = d.jstate[j];
+        if (st.count == 0) continue;
+        const uint32_t a = st.dense_a, b = st.dense_b;
+        const bool da = d.motion[a] == kDynamic, db = d.motion[b] == kDynamic;
+        if (da) atomicAdd(&d.jdeg[a], 1u);
+        if (db) atomicAdd(&d.jdeg[b], 1u);
+        if (da && db) uf_unite(d.parent, a, b);
+        if (!sp.realtime && sp.requested == 0) atomicMax(&d.ctr->joint_iters, d.joints[j].solver_iterations);
+    }
+}
+
+__global__ void k_graph_fill(Dev d) {
+    const uint32_t n_act = d.ctr->n_act;
+    for (uint32_t i = grid_stride_begin(); i < n_act; i += grid_stride()) {
+        const uint32_t a = d.act_a[i], b = d.act_b[i];
+        if (d.motion[a] == kDynamic) d.inc_list[d.inc_off[a] + atomicAdd(&d.inc_cursor[a], 1u)] = i;
+        if (d.motion[b] == kDynamic) d.inc_list[d.inc_off[b] + atomicAdd(&d.inc_cursor[b], 1u)] = i;
+    }
+    for (uint32_t j = grid_stride_begin(); j < d.nj; j += grid_stride()) {
+        const JointState st = d.jstate[j];
+        if (st.count == 0) continue;
+        const uint32_t a = st.dense_a, b = st.dense_b;
+        if (d.motion[a] == kDynamic) d.jinc_list[d.jinc_off[a] + atomicAdd(&d.jinc_cursor[a], 1u)] = j;
+        if (d.motion[b] == kDynamic) d.jinc_list[d.jinc_off[b] + atomicAdd(&d.jinc_cursor[b], 1u)] = j;
+    }
+}
+
+__device__ __forceinline__ void sort_desc(uint32_t* seg, uint32_t n) {
+    for (uint32_t i = 1; i < n; ++i) {
+        uint32_t v = seg[i], j = i;
+        while (j > 0 && seg[j - 1] < v) {
+            seg[j] = seg[j - 1];
+            --j;
+        }
+        seg[j] = v;
+    }
+}
+
+// Sort lists; find every root. Concurrent finds may still shorten paths
+// (writing ancestors), so roots go to a scratch array (corder, refilled by the
+// colour pass later) and are published by a second kernel.
+__global__ void k_graph_lists(Dev d) {
+    for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
+        sort_desc(d.inc_list + d.inc_off[i], d.deg[i]);
+        sort_desc(d.jinc_list + d.jinc_off[i], d.jdeg[i]);
+        d.corder[i] = uf_find(d.parent, i);
+    }
+}
+__global__ void k_graph_roots(Dev d) {
+    for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) d.parent[i] = d.corder[i];
+}
+
+__global__ void k_graph_impact(Dev d) {
+    const uint32_t n_act = d.ctr->n_act;
+    for (uint32_t i = grid_stride_begin(); i < n_act; i += grid_stride()) {
+        if (!d.act_impact[i]) continue;
+        const uint32_t a = d.act_a[i], b = d.act_b[i];
+        if (d.motion[a] == kDynamic) d.impact[d.parent[a]] = 1;
+        if (d.motion[b] == kDynamic) d.impact[d.parent[b]] = 1;
+    }
+}
+
+__global__ void k_graph_islands(Dev d) {
+    for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
+        if (d.motion[i] != kDynamic) continue;
+        const uint32_t r = d.parent[i];
+        if (r != i) d.impact[i] = d.impact[r];
+        if (r == i && (d.deg[i] > 0 || d.jdeg[i] > 0)) atomicAdd(&d.ctr->islands, 1u);
+    }
+}
+
+// Colour fixpoint (persistent cooperative kernel).
+__device__ __forceinline__ uint32_t mex_lower(const Dev& d, uint32_t v, bool& overflow) {
+    uint64_t mask[4] = {0, 0, 0, 0};
+    const uint32_t so = d.inc_off[v], sn = d.deg[v];
+    for (uint32_t k = 0; k < sn; ++k) {
+        const uint32_t p = d.inc_list[so + k];
+        const uint32_t a = d.act_a[p], b = d.act_b[p];
+        const uint32_t u = a == v ? b : a;
+        if (u < v && d.motion[u] == kDynamic) {
+            uint32_t c = ((volatile uint32_t*)d.color)[u];
+            if (c < kMaxColors) mask[c >> 6] |= 1ull << (c & 63);
+        }
+    }
+    const uint32_t jo = d.jinc_off[v], jn = d.jdeg[v];
+    for (uint32_t k = 0; k < jn; ++k) {
+        const JointState st = d.jstate[d.jinc_list[jo + k]];
+        const uint32_t u = st.dense_a == v ? st.dense_b : st.dense_a;
+        if (u < v && d.motion[u] == kDynamic) {
+            uint32_t c = ((volatile uint32_t*)d.color)[u];
+            if (c < kMaxColors) mask[c >> 6] |= 1ull << (c & 63);
+        }
+    }
+    for (int w = 0; w < 4; ++w)
+        if (~mask[w]) return uint32_t(w * 64 + __ffsll((long long)~mask[w]) - 1);
+    overflow = true;
+    return kMaxColors - 1;
+}
+
+__global__ void __launch_bounds__(kBlock) k_color(Dev d) {
+    Counters* c = d.ctr;
+    for (uint32_t round = 0; round < d.n + 2; ++round) {
+        const uint32_t before = ((volatile uint32_t*)&c->changed)[0];
+        if (!grid_sync(c)) return;
+        bool overflow = false;
+        uint32_t changes = 0;
+        for (uint32_t v = grid_stride_begin(); v < d.n; v += grid_stride()) {
+            if (d.motion[v] != kDynamic) continue;
+            uint32_t col = mex_lower(d, v, overflow);
+            if (col != d.color[v]) {
+                ((volatile uint32_t*)d.color)[v] = col;
+                ++changes;
+            }
+        }
+        if (overflow) atomicOr(&c->status, kStColorOverflow);
+        if (changes) atomicAdd(&c->changed, changes);
+        if (!grid_sync(c)) return;
+        const uint32_t after = ((volatile uint32_t*)&c->changed)[0];
+        if (after == before) {
+            if (grid_stride_begin() == 0) c->rounds = round + 1;
+            return;
+        }
+    }
+    if (grid_stride_begin() == 0) atomicOr(&c->status, kStColorOverflow);
+}
+
+__global__ void k_color_count(Dev d) {
+    for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
+        if (d.motion[i] != kDynamic) continue;
+        const uint32_t col = d.color[i];
+        atomicAdd(&d.ctr->color_count[col], 1u);
+        atomicMax(&d.ctr->colors, col + 1);
+    }
+}
+
+__global__ void k_color_offsets(Dev d) {
+    if (threadIdx.x == 0) {
+        uint32_t s = 0;
+        for (uint32_t k = 0; k < kMaxColors; ++k) {
+            d.ctr->color_off[k] = s;
+            s += d.ctr->color_count[k];
+            d.ctr->color_count[k] = 0;
+        }
+        d.ctr->color_off[kMaxColors] = s;
+    }
+}
+
+__global__ void k_color_scatter(Dev d) {
+    for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
+        if (d.motion[i] != kDynamic) continue;
+        const uint32_t col = d.color[i];
+        d.corder[d.ctr->color_off[col] + atomicAdd(&d.ctr->color_count[col], 1u)] = i;
+    }
+}
+
+void launch_prepare(const Dev& d, const StepParams& sp, cudaStream_t s) {
+    k_prepare_bodies<<<blocks_for(d.n), kBlock, 0, s>>>(d, sp);
+    k_prepare_pairs<<<blocks_for(d.cap_pair, 128), 128, 0, s>>>(d, sp);
+    if (d.nj) k_prepare_joints<<<blocks_for(d.nj, 64), 64, 0, s>>>(d, sp);
+}
+
+const void* color_kernel_ptr = reinterpret_cast<const void*>(&k_color);
+
+void launch_graph(const Dev& d, const StepParams& sp, cudaStream_t s, int coop_blocks) {
+    uint32_t gb = blocks_for(d.cap_pair > d.nj ? d.cap_pair : d.nj);
+    k_graph_degrees<<<gb, kBlock, 0, s>>>(d, sp);
+    scan_u32(d.deg, d.inc_off, nullptr, d.n, nullptr, d.scan_tmp32, s);
+    scan_u32(d.jdeg, d.jinc_off, nullptr, d.n, nullptr, d.scan_tmp32, s);
+    k_graph_fill<<<gb, kBlock, 0, s>>>(d);
+    k_graph_lists<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    k_graph_roots<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    k_graph_impact<<<blocks_for(d.cap_pair), kBlock, 0, s>>>(d);
+    k_graph_islands<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    void* args[] = {const_cast<Dev*>(&d)};
+    cudaLaunchCooperativeKernel(color_kernel_ptr, dim3(coop_blocks), dim3(kBlock), args, 0, s);
+    k_color_count<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    k_color_offsets<<<1, 32, 0, s>>>(d);
+    k_color_scatter<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+}
+
+}  // namespace pmb

@@ -1,0 +1,221 @@
+// SPDX-License-Identifier: MIT
+// Device-side layout of one rigid world. Everything the tick touches lives in
+// HBM as structure-of-arrays, float4-packed so a warp's loads coalesce:
+//   bodies    N   x (params 3 x float4, state 4 x float4 current + target)
+//   pairs     P   (a, b, contact offset, count) for non-empty manifolds, code order
+//   contacts  C   8 float4 per point (normal|pen, point|impact, error|speed,
+//                 anchor a|cached, anchor b, lambda|acc_n, penalty, acc_f)
+//   graph     per-body CSR of incident pairs (descending pair index, which is
+//             the reference's head-inserted list order), joints likewise
+// Counters live in one device struct so no stage needs a host round trip and
+// a whole tick can be captured into a CUDA graph.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pmb_math.cuh"
+
+namespace pmb {
+
+enum : uint32_t { kStatic = 0, kKinematic = 1, kDynamic = 2 };
+enum : uint32_t { kFixed, kPoint, kHinge, kSlider, kPiston, kGeneric, kGenericSpring, kMotor };
+constexpr uint32_t kMaxColors = 256;
+constexpr uint32_t kMaxIterations = 256;
+constexpr int kBlock = 256;
+
+// Status bits (pmb200_core.h).
+enum : uint32_t {
+    kStCandidateOverflow = 1u << 0,
+    kStContactOverflow = 1u << 1,
+    kStPairOverflow = 1u << 2,
+    kStInvalidBounds = 1u << 3,
+    kStBarrierTimeout = 1u << 4,
+    kStColorOverflow = 1u << 5,
+    kStGridOverflow = 1u << 6,
+};
+
+struct Counters {
+    uint32_t n_cand, n_stage, n_act, n_contacts;
+    uint32_t n_large, colors, islands, iterations;
+    uint32_t impact, status, changed, rounds;
+    uint32_t bar_count, bar_gen, budget, joint_iters;
+    float hs, residual, pad1, pad2;
+    uint32_t color_count[kMaxColors];
+    uint32_t color_off[kMaxColors + 1];
+    uint32_t color_cursor[kMaxColors];
+    float residual_trace[kMaxIterations];
+};
+
+struct StepParams {
+    float dt;
+    float gx, gy, gz;
+    uint32_t realtime;
+    uint32_t budget_request;  // requested or base iterations
+    uint32_t requested;
+    float tolerance;
+    uint32_t max_iterations;
+};
+
+struct JointRow {  // constraint_math.slang AvbdRow, packed for the device
+    float a[6], b[6];
+    float lambda, penalty, error, velocity, lower, upper, stiffness, damping, beta, reference_force;
+};
+
+struct Joint {
+    uint32_t type, body_a, body_b;
+    float anchor_a[3], anchor_b[3], frame_a[4], frame_b[4];
+    uint32_t lin_limit_axes;
+    float lin_lower[3], lin_upper[3];
+    uint32_t ang_limit_axes;
+    float ang_lower[3], ang_upper[3];
+    uint32_t lin_spring_axes;
+    float lin_stiffness[3], lin_damping[3];
+    uint32_t ang_spring_axes;
+    float ang_stiffness[3], ang_damping[3];
+    uint32_t motor_linear, motor_angular;
+    float motor_linear_velocity, motor_linear_max_impulse;
+    float motor_angular_velocity, motor_angular_max_impulse;
+    uint32_t enabled, disable_collisions;
+    float breaking_threshold;
+    uint32_t solver_iterations;
+};
+static_assert(sizeof(Joint) == 220, "joint record");
+
+struct JointState {
+    uint32_t enabled, broken, count, dense_a, dense_b, pad0, pad1, pad2;
+    float applied;
+};
+
+// Every device pointer of a world. Passed by value to kernels.
+struct Dev {
+    uint32_t n, nm, nj;
+    uint32_t cap_cand, cap_stage, cap_pair, cap_contact;
+    uint32_t grid_size;  // hash table buckets (power of two)
+    float large_extent;  // AABB extent above which a body is tested by brute force
+    // body parameters
+    uint32_t* motion;
+    uint32_t* mesh;
+    float4* p0;  // inv_mass, inv_inertia xyz
+    float4* p1;  // friction, restitution, linear damping, angular damping
+    float4* p2;  // max linear, max angular, margin, correction reach
+    float* expand;  // proxy expansion: min(1, correction) + reach
+    float* rotb;    // |max-abs mesh corner| for the rotational motion bound
+    // state: current (start of tick) and target (predicted, then solved)
+    float4 *x, *q, *v, *w;
+    float4 *tx, *tq, *tv, *tw;
+    float4 *lin_imp, *ang_imp;
+    // meshes
+    uint32_t *m_vo, *m_vc, *m_to, *m_tc, *m_convex;
+    float4* m_verts;
+    float4* m_planes;
+    // AVBD body state
+    float4 *dxl, *dxa, *dq;
+    float4 *inA, *inB;  // inertia block: (m/dt2, h33, h43, h44), (h53, h54, h55, -)
+    float4* prev_vel;   // xyz + history flag in w
+    uint32_t *color, *parent, *impact, *anchored;
+    float4* mean;       // free-island mean displacement (roots)
+    // broadphase
+    float4 *lo, *hi;
+    uint32_t* is_large;
+    uint32_t* large_list;
+    uint32_t *bucket_count, *bucket_off, *bucket_cursor;
+    uint32_t* grid_body;
+    int4* grid_cell;
+    uint32_t *cand_count, *cand_off;
+    uint32_t *cand_a, *cand_b;
+    // narrowphase
+    uint32_t* np_count;
+    uint64_t* np_scan;
+    uint32_t* np_stage;
+    float4 *st_n, *st_p;
+    // active pairs / contacts
+    uint32_t *act_a, *act_b, *act_code, *act_off, *act_cnt, *act_impact;
+    uint32_t* c_pair;
+    float4 *c_n, *c_p, *c_e, *c_aa, *c_ab, *c_lam, *c_pen, *c_accf;
+    // contact cache from the previous tick (double-buffered by the host)
+    uint32_t *sv_code, *sv_off, *sv_cnt;
+    uint32_t* sv_n_pairs;  // device count of saved pairs
+    float4 *sv_local, *sv_normal, *sv_fimp, *sv_lam, *sv_pen, *sv_aa, *sv_ab;
+    float* sv_dt;
+    uint32_t *out_code, *out_off, *out_cnt, *out_n_pairs;
+    float4 *out_local, *out_normal, *out_fimp, *out_lam, *out_pen, *out_aa, *out_ab;
+    float* out_dt;
+    // graph
+    uint32_t *deg, *inc_off, *inc_cursor, *inc_list;
+    uint32_t *jdeg, *jinc_off, *jinc_cursor, *jinc_list;
+    uint32_t* corder;
+    uint32_t *mem_count, *mem_off, *mem_cursor, *mem_list;
+    // joints
+    Joint* joints;
+    JointState* jstate;
+    JointRow* jrows;  // 18 per joint
+    uint32_t* dis_keys;    // sorted (min<<32|max) keys of collision-disabling joints
+    uint32_t n_dis;
+    // scratch for scans
+    uint64_t* scan_tmp;
+    uint32_t* scan_tmp32;
+    Counters* ctr;
+};
+
+// ---------------------------------------------------------------- helpers
+__device__ __forceinline__ uint32_t grid_stride_begin() { return blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ uint32_t grid_stride() { return gridDim.x * blockDim.x; }
+
+// Grid barrier for cooperative launches: arrive on a counter, the last block
+// bumps the generation. Waits are bounded; a timeout latches
+// kStBarrierTimeout and the caller abandons the tick.
+__device__ __forceinline__ bool grid_sync(Counters* c) {
+    __syncthreads();
+    __shared__ int ok;
+    if (threadIdx.x == 0) {
+        ok = 1;
+        volatile uint32_t* gen = &c->bar_gen;
+        uint32_t g = *gen;
+        __threadfence();
+        uint32_t arrived = atomicAdd(&c->bar_count, 1u);
+        if (arrived == gridDim.x - 1) {
+            c->bar_count = 0;
+            __threadfence();
+            atomicAdd(&c->bar_gen, 1u);
+        } else {
+            uint32_t spins = 0;
+            while (*gen == g) {
+                if (++spins > (1u << 26)) {
+                    atomicOr(&c->status, kStBarrierTimeout);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// Host-side stage launchers (defined in the .cu files).
+void launch_broadphase(const Dev& d, cudaStream_t s);
+void launch_narrowphase(const Dev& d, const StepParams& sp, cudaStream_t s);
+void launch_prepare(const Dev& d, const StepParams& sp, cudaStream_t s);
+void launch_graph(const Dev& d, const StepParams& sp, cudaStream_t s, int coop_blocks);
+struct SolveBuffers { float4 *ox, *oq, *ov, *ow; };
+void launch_integrate(const Dev& d, const StepParams& sp, cudaStream_t s, const SolveBuffers& o);
+void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, int coop_blocks, const SolveBuffers& o);
+void launch_body_constants(const Dev& d, const float4* lo, const float4* hi, const float4* sph, cudaStream_t s);
+void launch_finish(const Dev& d, const StepParams& sp, cudaStream_t s);
+void scan_u32(const uint32_t* in, uint32_t* out, const uint32_t* count_ptr, uint32_t capacity, uint32_t* total,
+              uint32_t* tmp, cudaStream_t s);
+void scan_u64(const uint64_t* in, uint64_t* out, const uint32_t* count_ptr, uint32_t capacity, uint64_t* tmp,
+              cudaStream_t s);
+int coop_blocks_for(const void* kernel, int threads, size_t smem);
+extern const void* solve_kernel_ptr;
+extern const void* color_kernel_ptr;
+
+inline uint32_t blocks_for(uint32_t n, int threads = kBlock) {
+    uint32_t b = (n + threads - 1) / threads;
+    return b == 0 ? 1 : b;
+}
+
+}  // namespace pmb

@@ -1,0 +1,205 @@
+# SPDX-License-Identifier: MIT
+"""ctypes binding of libpmb200_core.so (include/pmb200_core.h).
+
+There is no CPU path: constructing a ``World`` without the built library or
+without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from .scenes import STATE_DTYPE, STATS_DTYPE, Scene
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "libpmb200_core.so")
+
+ERRORS = {-1: "invalid argument", -4: "out of device memory", -5: "feature not present",
+          -7: "capacity exceeded", -8: "device lost", -10: "no CUDA device"}
+
+STATUS_BITS = {1: "candidate overflow", 2: "contact overflow", 4: "pair overflow",
+               8: "invalid bounds", 16: "barrier timeout", 32: "colour overflow",
+               64: "grid overflow"}
+
+
+class PmbError(RuntimeError):
+    pass
+
+
+class WorldDesc(ctypes.Structure):
+    _fields_ = [("body_count", ctypes.c_uint32), ("bodies", ctypes.c_void_p),
+                ("states", ctypes.c_void_p), ("mesh_count", ctypes.c_uint32),
+                ("vertex_offsets", ctypes.c_void_p), ("vertices", ctypes.c_void_p),
+                ("index_offsets", ctypes.c_void_p), ("indices", ctypes.c_void_p),
+                ("joint_count", ctypes.c_uint32), ("joints", ctypes.c_void_p),
+                ("candidate_capacity", ctypes.c_uint32), ("pair_capacity", ctypes.c_uint32),
+                ("contact_capacity", ctypes.c_uint32), ("device", ctypes.c_int32)]
+
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-j8", "-C", PKG_DIR], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise PmbError(f"{LIB_PATH} is not built (run `make -C {PKG_DIR}`)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, u32, i32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int
+        sig = {
+            "pmb_world_create": [vp, vp], "pmb_world_destroy": [vp],
+            "pmb_world_set_stream": [vp, vp], "pmb_world_step": [vp, vp, vp],
+            "pmb_world_capture": [vp, vp, u32], "pmb_world_replay": [vp],
+            "pmb_world_get_states": [vp, vp], "pmb_world_set_states": [vp, vp],
+            "pmb_world_last_stats": [vp, vp], "pmb_world_apply_impulse": [vp, u32, vp, vp],
+            "pmb_world_candidate_pairs": [vp, vp, u32, vp],
+            "pmb_world_manifolds": [vp, vp, vp, vp, u32, vp],
+            "pmb_world_graph": [vp, vp, vp], "pmb_world_residual_trace": [vp, vp, u32, vp],
+            "pmb_world_snapshot": [vp], "pmb_world_restore": [vp],
+            "pmb_world_device_states": [vp, vp], "pmb_math_eval": [u32, u32, vp, vp],
+        }
+        for name, args in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = None if name == "pmb_world_destroy" else i32
+        _lib = L
+    return _lib
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise PmbError(f"{what}: {ERRORS.get(rc, rc)}")
+
+
+def _p(a):
+    return a.ctypes.data if a is not None and a.size else None
+
+
+class World:
+    """A rigid world resident on one GPU, stepped by the CUDA kernels."""
+
+    def __init__(self, scene: Scene, device=0, candidate_capacity=0, pair_capacity=0,
+                 contact_capacity=0):
+        self.scene = scene
+        L = lib()
+        s = scene
+        self._keep = [np.ascontiguousarray(x) for x in (s.bodies, s.states, s.mesh_vertex_offsets,
+                                                         s.vertices, s.mesh_index_offsets, s.indices,
+                                                         s.joints)]
+        b, st, vo, v, io, i, j = self._keep
+        d = WorldDesc(len(b), _p(b), _p(st), len(vo) - 1, _p(vo), _p(v), _p(io), _p(i), len(j), _p(j),
+                      candidate_capacity, pair_capacity, contact_capacity, device)
+        h = ctypes.c_void_p()
+        _check(L.pmb_world_create(ctypes.byref(d), ctypes.byref(h)), "pmb_world_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.pmb_world_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def step(self, desc=None, stats=True, **kw):
+        d = np.ascontiguousarray(self.scene.step_desc(**kw) if desc is None else desc)
+        out = np.zeros((), STATS_DTYPE) if stats else None
+        _check(lib().pmb_world_step(self.h, d.ctypes.data, out.ctypes.data if stats else None),
+               "pmb_world_step")
+        return out
+
+    def capture(self, steps=2, desc=None, **kw):
+        d = np.ascontiguousarray(self.scene.step_desc(**kw) if desc is None else desc)
+        _check(lib().pmb_world_capture(self.h, d.ctypes.data, steps), "pmb_world_capture")
+
+    def replay(self):
+        _check(lib().pmb_world_replay(self.h), "pmb_world_replay")
+
+    def set_stream(self, stream_ptr):
+        _check(lib().pmb_world_set_stream(self.h, stream_ptr), "pmb_world_set_stream")
+
+    def stats(self):
+        out = np.zeros((), STATS_DTYPE)
+        _check(lib().pmb_world_last_stats(self.h, out.ctypes.data), "pmb_world_last_stats")
+        return out
+
+    def states(self):
+        out = np.zeros(self.scene.n, STATE_DTYPE)
+        _check(lib().pmb_world_get_states(self.h, out.ctypes.data), "pmb_world_get_states")
+        return out
+
+    def set_states(self, states):
+        s = np.ascontiguousarray(states, STATE_DTYPE)
+        _check(lib().pmb_world_set_states(self.h, s.ctypes.data), "pmb_world_set_states")
+
+    def apply_impulse(self, body, linear, angular=(0, 0, 0)):
+        lin = np.asarray(linear, np.float32)
+        ang = np.asarray(angular, np.float32)
+        _check(lib().pmb_world_apply_impulse(self.h, body, lin.ctypes.data, ang.ctypes.data),
+               "pmb_world_apply_impulse")
+
+    def candidate_pairs(self):
+        n = ctypes.c_uint32()
+        _check(lib().pmb_world_candidate_pairs(self.h, None, 0, ctypes.byref(n)), "candidate_pairs")
+        out = np.zeros(max(n.value, 1), np.uint32)
+        _check(lib().pmb_world_candidate_pairs(self.h, out.ctypes.data, n.value, ctypes.byref(n)),
+               "candidate_pairs")
+        return out[:n.value]
+
+    def manifolds(self):
+        n = ctypes.c_uint32()
+        _check(lib().pmb_world_manifolds(self.h, None, None, None, 0, ctypes.byref(n)), "manifolds")
+        k = max(n.value, 1)
+        codes = np.zeros(k, np.uint32)
+        counts = np.zeros(k, np.uint32)
+        contacts = np.zeros((k, 8, 22), np.float32)
+        _check(lib().pmb_world_manifolds(self.h, codes.ctypes.data, counts.ctypes.data,
+                                         contacts.ctypes.data, k, ctypes.byref(n)), "manifolds")
+        return codes[:n.value], counts[:n.value], contacts[:n.value]
+
+    def graph(self):
+        colors = np.zeros(self.scene.n, np.uint32)
+        parents = np.zeros(self.scene.n, np.uint32)
+        _check(lib().pmb_world_graph(self.h, colors.ctypes.data, parents.ctypes.data), "graph")
+        return colors, parents
+
+    def residual_trace(self):
+        out = np.zeros(256, np.float32)
+        n = ctypes.c_uint32()
+        _check(lib().pmb_world_residual_trace(self.h, out.ctypes.data, 256, ctypes.byref(n)),
+               "residual_trace")
+        return out[:n.value]
+
+    def snapshot(self):
+        _check(lib().pmb_world_snapshot(self.h), "snapshot")
+
+    def restore(self):
+        _check(lib().pmb_world_restore(self.h), "restore")
+
+    def device_states_ptr(self):
+        p = ctypes.c_void_p()
+        _check(lib().pmb_world_device_states(self.h, ctypes.byref(p)), "device_states")
+        return p.value
+
+
+_MATH_WIDTH = {0: (27, 7), 1: (7, 5), 2: (4, 6), 3: (42, 7)}
+
+
+def math_eval(kind: int, inputs: np.ndarray) -> np.ndarray:
+    """Run the device AVBD math (0 block solve, 1 dual, 2 contact, 3 row)."""
+    win, wout = _MATH_WIDTH[kind]
+    x = np.ascontiguousarray(inputs, np.float32).reshape(-1, win)
+    out = np.zeros((len(x), wout), np.float32)
+    _check(lib().pmb_math_eval(kind, len(x), x.ctypes.data, out.ctypes.data), "pmb_math_eval")
+    return out
+
+
+def status_names(status: int):
+    return [v for k, v in STATUS_BITS.items() if status & k]

@@ -1,0 +1,316 @@
+# SPDX-License-Identifier: MIT
+"""Synthetic rigid scenes with the shapes and distributions of the benchmark
+configurations: a cube pyramid, random box piles in a walled container,
+capsule chains hanging from static anchors, and batches of independent
+scenes. Every random draw comes from numpy's counter-based Philox generator,
+so a seed fixes the scene bit for bit on any host.
+
+A scene is a ``Scene`` of record arrays whose layouts are the C records of
+``include/pmb200_core.h``: ``BODY_DTYPE`` (52 B, BodyParameters order),
+``STATE_DTYPE`` (13 floats, PmRigidState order) and ``JOINT_DTYPE`` (220 B,
+RigidConstraintOptions order with dense body indices). Rigid bodies are
+triangle meshes, as in the reference: a box is a 12-triangle mesh
+(tests/api/command_api_tests.cpp:339-350) and a capsule is a closed convex
+tessellation small enough (<= 96 indices) for the convex face-contact path.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+STATIC, KINEMATIC, DYNAMIC = 0, 1, 2
+FIXED, POINT, HINGE, SLIDER, PISTON, GENERIC, GENERIC_SPRING, MOTOR = range(8)
+
+BODY_DTYPE = np.dtype([
+    ("motion", "<u4"), ("mesh", "<u4"), ("inv_mass", "<f4"), ("inv_inertia", "<f4", 3),
+    ("friction", "<f4"), ("restitution", "<f4"), ("linear_damping", "<f4"),
+    ("angular_damping", "<f4"), ("max_linear_speed", "<f4"), ("max_angular_speed", "<f4"),
+    ("margin", "<f4")])
+assert BODY_DTYPE.itemsize == 52
+
+STATE_DTYPE = np.dtype([("x", "<f4", 3), ("q", "<f4", 4), ("v", "<f4", 3), ("w", "<f4", 3)])
+assert STATE_DTYPE.itemsize == 52
+
+JOINT_DTYPE = np.dtype([
+    ("type", "<u4"), ("body_a", "<u4"), ("body_b", "<u4"),
+    ("anchor_a", "<f4", 3), ("anchor_b", "<f4", 3), ("frame_a", "<f4", 4), ("frame_b", "<f4", 4),
+    ("lin_limit_axes", "<u4"), ("lin_lower", "<f4", 3), ("lin_upper", "<f4", 3),
+    ("ang_limit_axes", "<u4"), ("ang_lower", "<f4", 3), ("ang_upper", "<f4", 3),
+    ("lin_spring_axes", "<u4"), ("lin_stiffness", "<f4", 3), ("lin_damping", "<f4", 3),
+    ("ang_spring_axes", "<u4"), ("ang_stiffness", "<f4", 3), ("ang_damping", "<f4", 3),
+    ("motor_linear", "<u4"), ("motor_angular", "<u4"),
+    ("motor_linear_velocity", "<f4"), ("motor_linear_max_impulse", "<f4"),
+    ("motor_angular_velocity", "<f4"), ("motor_angular_max_impulse", "<f4"),
+    ("enabled", "<u4"), ("disable_collisions", "<u4"), ("breaking_threshold", "<f4"),
+    ("solver_iterations", "<u4")])
+assert JOINT_DTYPE.itemsize == 220
+
+STEP_DTYPE = np.dtype([
+    ("dt", "<f4"), ("gravity", "<f4", 3), ("profile", "<u4"), ("requested_iterations", "<u4"),
+    ("base_iterations", "<u4"), ("residual_tolerance", "<f4"), ("max_iterations", "<u4")])
+
+STATS_DTYPE = np.dtype([
+    ("candidate_pairs", "<u4"), ("active_pairs", "<u4"), ("contacts", "<u4"), ("colors", "<u4"),
+    ("islands", "<u4"), ("iterations", "<u4"), ("impact", "<u4"), ("status", "<u4"),
+    ("residual", "<f4")])
+
+LEGACY, REALTIME = 0, 1
+DT = np.float32(1.0 / 60.0)
+
+
+@dataclasses.dataclass
+class Scene:
+    bodies: np.ndarray           # BODY_DTYPE[N]
+    states: np.ndarray           # STATE_DTYPE[N]
+    mesh_vertex_offsets: np.ndarray  # u32[M+1]
+    vertices: np.ndarray         # f32[V, 3]
+    mesh_index_offsets: np.ndarray   # u32[M+1]
+    indices: np.ndarray          # u32[I]
+    joints: np.ndarray           # JOINT_DTYPE[J]
+    name: str = ""
+    iterations: int = 10
+    profile: int = LEGACY
+
+    @property
+    def n(self) -> int:
+        return len(self.bodies)
+
+    def step_desc(self, *, dt=DT, profile=None, iterations=None, residual_tolerance=0.0,
+                  max_iterations=0) -> np.ndarray:
+        s = np.zeros((), STEP_DTYPE)
+        s["dt"] = dt
+        s["gravity"] = (0.0, -9.81, 0.0)
+        s["profile"] = self.profile if profile is None else profile
+        s["requested_iterations"] = self.iterations if iterations is None else iterations
+        s["base_iterations"] = 10
+        s["residual_tolerance"] = residual_tolerance
+        s["max_iterations"] = max_iterations
+        return s
+
+
+class _Builder:
+    def __init__(self):
+        self.bodies, self.states, self.meshes, self.joints = [], [], [], []
+
+    def mesh(self, vertices, indices) -> int:
+        self.meshes.append((np.asarray(vertices, np.float32).reshape(-1, 3),
+                            np.asarray(indices, np.uint32).reshape(-1)))
+        return len(self.meshes) - 1
+
+    def body(self, mesh, motion, x, q=(0, 0, 0, 1), v=(0, 0, 0), w=(0, 0, 0), mass=1.0,
+             inertia=(1, 1, 1), friction=0.5, restitution=0.0, margin=0.005,
+             max_speed=100.0) -> int:
+        b = np.zeros((), BODY_DTYPE)
+        b["motion"], b["mesh"] = motion, mesh
+        if motion == DYNAMIC:
+            b["inv_mass"] = np.float32(1.0) / np.float32(mass)
+            b["inv_inertia"] = np.float32(1.0) / np.asarray(inertia, np.float32)
+        b["friction"], b["restitution"], b["margin"] = friction, restitution, margin
+        b["max_linear_speed"] = b["max_angular_speed"] = max_speed
+        s = np.zeros((), STATE_DTYPE)
+        s["x"], s["q"], s["v"], s["w"] = x, q, v, w
+        self.bodies.append(b)
+        self.states.append(s)
+        return len(self.bodies) - 1
+
+    def joint(self, kind, a, b, anchor_a, anchor_b, disable_collisions=True, iterations=0):
+        j = np.zeros((), JOINT_DTYPE)
+        j["type"], j["body_a"], j["body_b"] = kind, a, b
+        j["anchor_a"], j["anchor_b"] = anchor_a, anchor_b
+        j["frame_a"] = j["frame_b"] = (0, 0, 0, 1)
+        j["enabled"] = 1
+        j["disable_collisions"] = 1 if disable_collisions else 0
+        j["solver_iterations"] = iterations
+        self.joints.append(j)
+        return len(self.joints) - 1
+
+    def build(self, name, iterations, profile=LEGACY) -> Scene:
+        voff = np.zeros(len(self.meshes) + 1, np.uint32)
+        ioff = np.zeros(len(self.meshes) + 1, np.uint32)
+        for k, (v, i) in enumerate(self.meshes):
+            voff[k + 1] = voff[k] + len(v)
+            ioff[k + 1] = ioff[k] + len(i)
+        verts = np.concatenate([v for v, _ in self.meshes]) if self.meshes else np.zeros((0, 3), np.float32)
+        idx = np.concatenate([i for _, i in self.meshes]) if self.meshes else np.zeros(0, np.uint32)
+        return Scene(np.array(self.bodies, BODY_DTYPE), np.array(self.states, STATE_DTYPE), voff,
+                     verts.astype(np.float32), ioff, idx.astype(np.uint32),
+                     np.array(self.joints, JOINT_DTYPE).reshape(-1), name, iterations, profile)
+
+
+# Outward-wound box triangles over the 8 corners (x fastest, then y, then z).
+_BOX_TRIS = np.array([
+    0, 2, 1, 1, 2, 3,  # -z
+    4, 5, 6, 5, 7, 6,  # +z
+    0, 1, 4, 1, 5, 4,  # -y
+    2, 6, 3, 3, 6, 7,  # +y
+    0, 4, 2, 2, 4, 6,  # -x
+    1, 3, 5, 3, 7, 5,  # +x
+], np.uint32)
+
+
+def box_mesh(half):
+    hx, hy, hz = (float(h) for h in half)
+    v = np.array([[sx * hx, sy * hy, sz * hz] for sz in (-1, 1) for sy in (-1, 1) for sx in (-1, 1)],
+                 np.float32)
+    return v, _BOX_TRIS.copy()
+
+
+def capsule_mesh(radius, length, segments=6):
+    """Convex capsule tessellation along +y: a ``segments``-gon ring at each
+    end of the cylinder and one pole per cap. 4*segments triangles (<= 96
+    indices for segments <= 8)."""
+    half = 0.5 * length
+    ring = []
+    for end in (-1, 1):
+        for k in range(segments):
+            a = 2.0 * math.pi * k / segments
+            ring.append([radius * math.cos(a), end * half, radius * math.sin(a)])
+    poles = [[0.0, -half - radius, 0.0], [0.0, half + radius, 0.0]]
+    v = np.array(ring + poles, np.float32)
+    lo, hi, pb, pt = 0, segments, 2 * segments, 2 * segments + 1
+    tris = []
+    for k in range(segments):
+        k1 = (k + 1) % segments
+        tris += [lo + k, hi + k, lo + k1, lo + k1, hi + k, hi + k1]   # side quad
+        tris += [pb, lo + k, lo + k1]                                  # bottom cap
+        tris += [pt, hi + k1, hi + k]                                  # top cap
+    return v, np.array(tris, np.uint32)
+
+
+def _fix_winding(v, t):
+    """Orient every triangle outward from the centroid (convex meshes)."""
+    t = t.reshape(-1, 3).copy()
+    c = v.mean(axis=0)
+    for row in t:
+        a, b, d = v[row[0]], v[row[1]], v[row[2]]
+        if np.dot(np.cross(b - a, d - a), a - c) < 0:
+            row[1], row[2] = row[2], row[1]
+    return t.reshape(-1)
+
+
+def box_inertia(mass, half):
+    h = np.asarray(half, np.float64)
+    return (mass / 3.0 * (h[1] ** 2 + h[2] ** 2), mass / 3.0 * (h[0] ** 2 + h[2] ** 2),
+            mass / 3.0 * (h[0] ** 2 + h[1] ** 2))
+
+
+def _ground(b: _Builder, half_x, half_z, thickness=0.5, friction=0.5):
+    m = b.mesh(*box_mesh((half_x, thickness, half_z)))
+    return b.body(m, STATIC, (0.0, -thickness, 0.0), friction=friction)
+
+
+def pyramid(levels=10, seed=1, jitter=1e-3, friction=0.5, density=1000.0, iterations=10,
+            profile=LEGACY) -> Scene:
+    """Planar pyramid of unit cubes (levels*(levels+1)/2 of them) on a static
+    ground box; every cube centre jittered uniformly by +-jitter."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    b = _Builder()
+    _ground(b, 20.0, 20.0, friction=friction)
+    cube = b.mesh(*box_mesh((0.5, 0.5, 0.5)))
+    mass = density * 1.0
+    inertia = box_inertia(mass, (0.5, 0.5, 0.5))
+    for row in range(levels):
+        count = levels - row
+        for k in range(count):
+            x = (k - 0.5 * (count - 1)) * 1.0
+            y = 0.5 + row * 1.0
+            d = rng.uniform(-jitter, jitter, 3)
+            b.body(cube, DYNAMIC, (x + d[0], y + d[1], d[2]), mass=mass, inertia=inertia,
+                   friction=friction)
+    return b.build(f"pyramid{levels}", iterations, profile)
+
+
+def box_pile(grid=(16, 16, 16), seed=2, spacing=1.8, iterations=10, profile=LEGACY,
+             wall_height=8.0) -> Scene:
+    """Random boxes (edges U[0.5,1.5] per axis, density U[500,2000], friction
+    U[0.3,0.8]) on a jittered grid (gx along x, gy layers along y, gz along z)
+    above a static walled container sized to the grid footprint."""
+    gx, gy, gz = grid
+    rng = np.random.Generator(np.random.Philox(seed))
+    b = _Builder()
+    half_x = 0.5 * gx * spacing + 1.0
+    half_z = 0.5 * gz * spacing + 1.0
+    _ground(b, half_x + 1.0, half_z + 1.0)
+    wall_x = b.mesh(*box_mesh((0.5, 0.5 * wall_height, half_z + 1.0)))
+    wall_z = b.mesh(*box_mesh((half_x + 1.0, 0.5 * wall_height, 0.5)))
+    for s in (-1, 1):
+        b.body(wall_x, STATIC, (s * (half_x + 0.5), 0.5 * wall_height, 0.0))
+        b.body(wall_z, STATIC, (0.0, 0.5 * wall_height, s * (half_z + 0.5)))
+    n = gx * gy * gz
+    edges = rng.uniform(0.5, 1.5, (n, 3)).astype(np.float32)
+    density = rng.uniform(500.0, 2000.0, n)
+    friction = rng.uniform(0.3, 0.8, n).astype(np.float32)
+    jit = rng.uniform(-0.1, 0.1, (n, 3))
+    k = 0
+    for y in range(gy):
+        for z in range(gz):
+            for x in range(gx):
+                half = 0.5 * edges[k]
+                m = b.mesh(*box_mesh(half))
+                mass = float(density[k] * np.prod(edges[k].astype(np.float64)))
+                pos = ((x - 0.5 * (gx - 1)) * spacing + jit[k, 0],
+                       1.0 + y * spacing + jit[k, 1],
+                       (z - 0.5 * (gz - 1)) * spacing + jit[k, 2])
+                b.body(m, DYNAMIC, pos, mass=mass, inertia=box_inertia(mass, half),
+                       friction=float(friction[k]))
+                k += 1
+    return b.build(f"pile{gx}x{gy}x{gz}", iterations, profile)
+
+
+def chains(count=512, links=64, seed=3, radius=0.05, length=0.4, spacing=1.0,
+           iterations=20, profile=LEGACY, link_density=1000.0) -> Scene:
+    """``count`` chains of ``links`` capsule links joined by point joints,
+    the top link jointed to a static anchor, a box of 100x link mass on each
+    free end, initial lateral velocity U(+-2) m/s per chain."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    b = _Builder()
+    cap_v, cap_t = capsule_mesh(radius, length)
+    cap = b.mesh(cap_v, _fix_winding(cap_v, cap_t))
+    anchor = b.mesh(*box_mesh((0.05, 0.05, 0.05)))
+    link_mass = link_density * (math.pi * radius ** 2 * length + 4.0 / 3.0 * math.pi * radius ** 3)
+    link_inertia = (link_mass * (3 * radius ** 2 + length ** 2) / 12.0, link_mass * radius ** 2 / 2.0,
+                    link_mass * (3 * radius ** 2 + length ** 2) / 12.0)
+    box_half = (0.2, 0.2, 0.2)
+    end = b.mesh(*box_mesh(box_half))
+    end_mass = 100.0 * link_mass
+    side = int(math.ceil(math.sqrt(count)))
+    top = 2.0 + links * length + 1.0
+    vel = rng.uniform(-2.0, 2.0, (count, 2))
+    pitch = length + 2 * radius
+    for c in range(count):
+        cx = (c % side - 0.5 * (side - 1)) * spacing
+        cz = (c // side - 0.5 * (side - 1)) * spacing
+        a = b.body(anchor, STATIC, (cx, top, cz))
+        v0 = (float(vel[c, 0]), 0.0, float(vel[c, 1]))
+        prev, prev_anchor = a, (0.0, 0.0, 0.0)
+        for k in range(links):
+            y = top - 0.5 * pitch - k * pitch
+            link = b.body(cap, DYNAMIC, (cx, y, cz), v=v0, mass=link_mass, inertia=link_inertia,
+                          friction=0.5)
+            b.joint(POINT, prev, link, prev_anchor, (0.0, 0.5 * pitch, 0.0))
+            prev, prev_anchor = link, (0.0, -0.5 * pitch, 0.0)
+        y = top - links * pitch - box_half[1]
+        box = b.body(end, DYNAMIC, (cx, y, cz), v=v0, mass=end_mass,
+                     inertia=box_inertia(end_mass, box_half), friction=0.5)
+        b.joint(POINT, prev, box, prev_anchor, (0.0, box_half[1], 0.0))
+    return b.build(f"chains{count}x{links}", iterations, profile)
+
+
+def config(index: int) -> Scene:
+    """The benchmark configurations 1-4 at full size (0-based ``index``)."""
+    if index == 0:
+        return pyramid()
+    if index == 1:
+        return box_pile((16, 16, 16), seed=2)
+    if index == 2:
+        return chains()
+    if index == 3:
+        return box_pile((64, 32, 32), seed=4)
+    raise ValueError(index)
+
+
+def pile_grid_for_config4():
+    """64x32x32 spawn grid: 64 along x, 32 layers, 32 along z."""
+    return (64, 32, 32)
