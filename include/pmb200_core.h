@@ -134,6 +134,16 @@ PMB_API int pmb_world_set_stream(pmb_world* world, void* stream);
  * unless stats is non-null, in which case it waits and fills stats. */
 PMB_API int pmb_world_step(pmb_world* world, const pmb_step_desc* step, pmb_step_stats* stats);
 
+/* Diagnostic: run one tick with CUDA events between its stages and write
+ * "stage  ms" lines into report (synchronous). */
+PMB_API int pmb_world_profile_step(pmb_world* world, const pmb_step_desc* step, char* report, uint32_t capacity);
+
+/* Dominant-kernel timing: with enable != 0, later ticks bracket every solve
+ * launch with CUDA events on the world's stream. Each call synchronises,
+ * returns the summed duration and launch count of the launches recorded since
+ * the previous call, and sets the enable state. */
+PMB_API int pmb_world_solve_timer(pmb_world* world, int enable, float* total_ms, uint32_t* launches);
+
 /* Capture `steps` ticks into a CUDA graph (replayed by pmb_world_replay). */
 PMB_API int pmb_world_capture(pmb_world* world, const pmb_step_desc* step, uint32_t steps);
 PMB_API int pmb_world_replay(pmb_world* world);

@@ -128,6 +128,7 @@ __global__ void k_integrate(Dev d, StepParams sp, float4* ox, float4* oq, float4
 
 void launch_integrate(const Dev& d, const StepParams& sp, cudaStream_t s, const SolveBuffers& o) {
     k_integrate<<<blocks_for(d.n), kBlock, 0, s>>>(d, sp, o.ox, o.oq, o.ov, o.ow);
+    prof_mark(s, "integrate+proxy");
 }
 
 __global__ void k_grid_count(Dev d) {
@@ -254,10 +255,13 @@ void launch_broadphase(const Dev& d, cudaStream_t s) {
     k_grid_count<<<blocks_for(d.n), kBlock, 0, s>>>(d);
     scan_u32(d.bucket_count, d.bucket_off, nullptr, d.grid_size, nullptr, d.scan_tmp32, s);
     k_grid_scatter<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    prof_mark(s, "grid build");
     k_query_count<<<blocks_for(d.n, 128), 128, 0, s>>>(d);
+    prof_mark(s, "query count");
     scan_u32(d.cand_count, d.cand_off, nullptr, d.n, &d.ctr->n_cand, d.scan_tmp32, s);
     k_query_write<<<blocks_for(d.n, 128), 128, 0, s>>>(d);
     k_clamp_count<<<1, 1, 0, s>>>(&d.ctr->n_cand, d.cap_cand);
+    prof_mark(s, "query write");
 }
 
 }  // namespace pmb

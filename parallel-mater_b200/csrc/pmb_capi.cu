@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <string>
 #include <vector>
 
 #include "../../include/pmb200_core.h"
@@ -13,6 +14,41 @@
 
 namespace pmb {
 __global__ void k_math_eval(uint32_t kind, uint32_t count, const float* in, float* out);
+
+struct Prof {
+    bool on{};
+    std::vector<cudaEvent_t> events;
+    std::vector<const char*> names;
+};
+static Prof g_prof;
+
+void prof_mark(cudaStream_t s, const char* stage) {
+    if (!g_prof.on) return;
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, s);
+    g_prof.events.push_back(e);
+    g_prof.names.push_back(stage);
+}
+
+struct SolveTimer {
+    bool on{};
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pairs;
+};
+static SolveTimer g_timer;
+
+void solve_timer_begin(cudaStream_t s) {
+    if (!g_timer.on) return;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, s);
+    g_timer.pairs.push_back({a, b});
+}
+void solve_timer_end(cudaStream_t s) {
+    if (!g_timer.on || g_timer.pairs.empty()) return;
+    cudaEventRecord(g_timer.pairs.back().second, s);
+}
 
 int coop_blocks_for(const void* kernel, int threads, size_t smem) {
     int dev = 0, sms = 0, per = 0;
@@ -247,7 +283,7 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     ALLOC(d.st_n, d.cap_stage); ALLOC(d.st_p, d.cap_stage);
     ALLOC(d.act_a, d.cap_pair); ALLOC(d.act_b, d.cap_pair); ALLOC(d.act_code, d.cap_pair);
     ALLOC(d.act_off, d.cap_pair + 1); ALLOC(d.act_cnt, d.cap_pair); ALLOC(d.act_impact, d.cap_pair);
-    ALLOC(d.c_pair, d.cap_contact);
+    ALLOC(d.c_pair, d.cap_contact); ALLOC(d.c_bodies, d.cap_contact); ALLOC(d.c_jac, 9 * size_t(d.cap_contact));
     ALLOC(d.c_n, d.cap_contact); ALLOC(d.c_p, d.cap_contact); ALLOC(d.c_e, d.cap_contact);
     ALLOC(d.c_aa, d.cap_contact); ALLOC(d.c_ab, d.cap_contact); ALLOC(d.c_lam, d.cap_contact);
     ALLOC(d.c_pen, d.cap_contact); ALLOC(d.c_accf, d.cap_contact);
@@ -267,6 +303,7 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     ALLOC(d.deg, n); ALLOC(d.inc_off, n + 1); ALLOC(d.inc_cursor, n); ALLOC(d.inc_list, 2 * size_t(d.cap_pair));
     ALLOC(d.jdeg, n); ALLOC(d.jinc_off, n + 1); ALLOC(d.jinc_cursor, n); ALLOC(d.jinc_list, 2 * size_t(nj) + 2);
     ALLOC(d.corder, n);
+    ALLOC(d.rcount, n); ALLOC(d.roff, n + 1); ALLOC(d.blist, 2 * size_t(d.cap_contact)); ALLOC(d.bother, 2 * size_t(d.cap_contact));
     ALLOC(d.joints, nj); ALLOCS(d.jstate, nj); ALLOCS(d.jrows, size_t(nj) * 18);
     {
         // Scan scratch: one slot per 2048-element tile of the longest scan plus the total.
@@ -353,7 +390,8 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     std::vector<float> sorted = expand;
     std::nth_element(sorted.begin(), sorted.begin() + n / 2, sorted.end());
     d.large_extent = 2.0f * sorted[n / 2] * 4.0f;
-    w->coop_solve = coop_blocks_for(solve_kernel_ptr, kBlock, 0);
+    cudaFuncSetAttribute(solve_kernel_ptr, cudaFuncAttributeMaxDynamicSharedMemorySize, int(solve_kernel_smem));
+    w->coop_solve = coop_blocks_for(solve_kernel_ptr, solve_kernel_threads, solve_kernel_smem);
     w->coop_color = coop_blocks_for(color_kernel_ptr, kBlock, 0);
     for (auto& p : w->dynamic_state) {
         void* snap = nullptr;
@@ -396,6 +434,67 @@ int pmb_world_step(pmb_world* w, const pmb_step_desc* step, pmb_step_stats* stat
     if (r != PMB_SUCCESS) return r;
     if (stats) return pmb_world_last_stats(w, stats);
     return PMB_SUCCESS;
+}
+
+int pmb_world_profile_step(pmb_world* w, const pmb_step_desc* step, char* report, uint32_t capacity) {
+    if (!w || !step || !report || capacity == 0) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    g_prof = Prof{};
+    g_prof.on = true;
+    prof_mark(w->stream, "start");
+    StepParams sp = params_from(*step);
+    sp.debug_timing = 1;
+    enqueue_step(w, sp);
+    g_prof.on = false;
+    int r = check(cudaStreamSynchronize(w->stream));
+    std::string text;
+    for (size_t k = 1; k < g_prof.events.size(); ++k) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, g_prof.events[k - 1], g_prof.events[k]);
+        char line[160];
+        std::snprintf(line, sizeof(line), "%-24s %9.3f ms\n", g_prof.names[k], ms);
+        text += line;
+    }
+    for (auto e : g_prof.events) cudaEventDestroy(e);
+    Counters hc;
+    cudaMemcpy(&hc, w->d.ctr, sizeof(Counters), cudaMemcpyDeviceToHost);
+    {
+        char line[160];
+        std::snprintf(line, sizeof(line), "solve iteration 0 (us from kernel start): colours %u\n", hc.colors);
+        text += line;
+        for (uint32_t k = 0; k < 20; ++k) {
+            if (!hc.dbg_work[k]) continue;
+            std::snprintf(line, sizeof(line), "  %s %2u work-end %8.1f release %8.1f\n", k == 19 ? "dual  " : "colour", k,
+                          (hc.dbg_work[k] - hc.dbg_start) * 1e-3, (hc.dbg_release[k] - hc.dbg_start) * 1e-3);
+            text += line;
+        }
+        std::snprintf(line, sizeof(line), "  last colour body (max rn %u): stage %.1f gather %.1f solve %.1f crossing %.1f solve2 %.1f us\n",
+                      hc.dbg_rn, hc.dbg_body[0] * 1e-3, hc.dbg_body[1] * 1e-3, hc.dbg_body[2] * 1e-3, hc.dbg_body[3] * 1e-3,
+                      hc.dbg_body[4] * 1e-3);
+        text += line;
+    }
+    g_prof = Prof{};
+    std::snprintf(report, capacity, "%s", text.c_str());
+    return r;
+}
+
+int pmb_world_solve_timer(pmb_world* w, int enable, float* total_ms, uint32_t* launches) {
+    if (!w) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    int r = check(cudaStreamSynchronize(w->stream));
+    float total = 0.0f;
+    for (auto& p : g_timer.pairs) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, p.first, p.second);
+        total += ms;
+        cudaEventDestroy(p.first);
+        cudaEventDestroy(p.second);
+    }
+    if (total_ms) *total_ms = total;
+    if (launches) *launches = uint32_t(g_timer.pairs.size());
+    g_timer.pairs.clear();
+    g_timer.on = enable != 0;
+    return r;
 }
 
 int pmb_world_capture(pmb_world* w, const pmb_step_desc* step, uint32_t steps) {

@@ -345,6 +345,7 @@ __global__ void k_compact(Dev d) {
             V3 cv = add(vb, cross(wb, sub(pp, xb)));
             float speed = dot(sub(bv, cv), nn);
             d.c_pair[c] = i;
+            d.c_bodies[c] = make_uint2(a, b);
             d.c_n[c] = n;
             d.c_p[c] = pt;
             d.c_e[c] = make_float4(0, 0, 0, speed);
@@ -415,9 +416,12 @@ __global__ void k_cache_load(Dev d, StepParams sp) {
 
 void launch_narrowphase(const Dev& d, const StepParams& sp, cudaStream_t s) {
     k_narrow<<<blocks_for(d.cap_cand, 128), 128, 0, s>>>(d);
+    prof_mark(s, "narrowphase");
     scan_u64(d.np_scan, d.np_scan, &d.ctr->n_cand, d.cap_cand, d.scan_tmp, s);
     k_compact<<<blocks_for(d.cap_cand), kBlock, 0, s>>>(d);
+    prof_mark(s, "compact");
     k_cache_load<<<blocks_for(d.cap_pair, 128), 128, 0, s>>>(d, sp);
+    prof_mark(s, "cache load");
 }
 
 }  // namespace pmb

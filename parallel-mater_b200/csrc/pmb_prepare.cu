@@ -268,7 +268,33 @@ __global__ void k_graph_lists(Dev d) {
     }
 }
 __global__ void k_graph_roots(Dev d) {
-    for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) d.parent[i] = d.corder[i];
+    for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
+        d.parent[i] = d.corder[i];
+        uint32_t rc = 0;
+        const uint32_t lo = d.inc_off[i], n = d.deg[i];
+        for (uint32_t k = 0; k < n; ++k) rc += d.act_cnt[d.inc_list[lo + k]];
+        d.rcount[i] = rc;
+    }
+}
+
+// Flattened contact list per body, in the reference's visiting order
+// (incident pairs by descending index, points in manifold order).
+__global__ void k_row_lists(Dev d) {
+    for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
+        uint32_t pos = d.roff[i];
+        const uint32_t lo = d.inc_off[i], n = d.deg[i];
+        for (uint32_t k = 0; k < n; ++k) {
+            const uint32_t p = d.inc_list[lo + k];
+            const uint32_t a = d.act_a[p], b = d.act_b[p];
+            const uint32_t second = a == i ? 0u : 0x80000000u;
+            const uint32_t other = a == i ? b : a;
+            const uint32_t off = d.act_off[p], cnt = d.act_cnt[p];
+            for (uint32_t q = 0; q < cnt; ++q) {
+                d.bother[pos] = other;
+                d.blist[pos++] = (off + q) | second;
+            }
+        }
+    }
 }
 
 __global__ void k_graph_impact(Dev d) {
@@ -378,6 +404,8 @@ void launch_prepare(const Dev& d, const StepParams& sp, cudaStream_t s) {
     k_prepare_bodies<<<blocks_for(d.n), kBlock, 0, s>>>(d, sp);
     k_prepare_pairs<<<blocks_for(d.cap_pair, 128), 128, 0, s>>>(d, sp);
     if (d.nj) k_prepare_joints<<<blocks_for(d.nj, 64), 64, 0, s>>>(d, sp);
+    launch_contact_jacobians(d, 0, s);
+    prof_mark(s, "prepare");
 }
 
 const void* color_kernel_ptr = reinterpret_cast<const void*>(&k_color);
@@ -390,13 +418,18 @@ void launch_graph(const Dev& d, const StepParams& sp, cudaStream_t s, int coop_b
     k_graph_fill<<<gb, kBlock, 0, s>>>(d);
     k_graph_lists<<<blocks_for(d.n), kBlock, 0, s>>>(d);
     k_graph_roots<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    scan_u32(d.rcount, d.roff, nullptr, d.n, nullptr, d.scan_tmp32, s);
+    k_row_lists<<<blocks_for(d.n), kBlock, 0, s>>>(d);
     k_graph_impact<<<blocks_for(d.cap_pair), kBlock, 0, s>>>(d);
     k_graph_islands<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    prof_mark(s, "graph lists+islands");
     void* args[] = {const_cast<Dev*>(&d)};
     cudaLaunchCooperativeKernel(color_kernel_ptr, dim3(coop_blocks), dim3(kBlock), args, 0, s);
+    prof_mark(s, "colour fixpoint");
     k_color_count<<<blocks_for(d.n), kBlock, 0, s>>>(d);
     k_color_offsets<<<1, 32, 0, s>>>(d);
     k_color_scatter<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    prof_mark(s, "colour buckets");
 }
 
 }  // namespace pmb

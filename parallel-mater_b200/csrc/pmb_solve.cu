@@ -14,33 +14,83 @@
 
 namespace pmb {
 
-struct Lite {  // what a contact row needs of a body
-    V3 x;
-    Q4 q;
+struct Lite {  // what a contact row needs of a body during the solve: its displacement
     V6 dx;
 };
 __device__ __forceinline__ Lite load_lite(const Dev& d, uint32_t i) {
-    float4 l = d.dxl[i], a = d.dxa[i];
-    return {v3(d.tx[i]), q4(d.tq[i]), {{l.x, l.y, l.z, a.x, a.y, a.z}}};
+    const float4 l = d.dxl[i], a = d.dxa[i];
+    return {{{l.x, l.y, l.z, a.x, a.y, a.z}}};
 }
 
-// geometry_constraints.slang:508-532
-__device__ __forceinline__ void contact_rows(V3 n, V3 pt, V3 anc_a, V3 anc_b, float4 e, const Lite& A, const Lite& B,
-                                             V6 ja[3], V6 jb[3], float err[3]) {
+// Contact jacobians (geometry_constraints.slang:508-532). They depend only on
+// the contact geometry and the AVBD target poses, both fixed during a solve
+// phase, so they are evaluated once per phase (k_contact_jacobians) and
+// stored: 36 floats per contact, rows n, t0, t1 for body a then body b.
+__device__ __forceinline__ void contact_jacobians(V3 n, V3 pt, V3 anc_a, V3 anc_b, V3 xa, Q4 qa, V3 xb, Q4 qb,
+                                                  V6 ja[3], V6 jb[3]) {
     V3 t0, t1;
     basis(n, t0, t1);
     const V3 axes[3] = {n, t0, t1};
-    const V3 arm_a = sub(pt, A.x), arm_b = sub(pt, B.x);
-    const V3 ra_t = rotate(A.q, anc_a), rb_t = rotate(B.q, anc_b);
-    const float e3[3] = {e.x, e.y, e.z};
+    const V3 arm_a = sub(pt, xa), arm_b = sub(pt, xb);
+    const V3 ra_t = rotate(qa, anc_a), rb_t = rotate(qb, anc_b);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         V3 ra = k == 0 ? arm_a : ra_t;
         V3 rb = k == 0 ? arm_b : rb_t;
         ja[k] = jac(mul(axes[k], -1.0f), mul(cross(ra, axes[k]), -1.0f));
         jb[k] = jac(axes[k], cross(rb, axes[k]));
-        err[k] = e3[k] + dot6(ja[k], A.dx) + dot6(jb[k], B.dx);
     }
+}
+__device__ __forceinline__ void load_jac(const Dev& d, uint32_t c, V6 ja[3], V6 jb[3]) {
+    const float4* p = d.c_jac + size_t(c) * 9;
+    float f[36];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        const float4 v = p[k];
+        f[4 * k] = v.x;
+        f[4 * k + 1] = v.y;
+        f[4 * k + 2] = v.z;
+        f[4 * k + 3] = v.w;
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            ja[r].v[k] = f[6 * r + k];
+            jb[r].v[k] = f[18 + 6 * r + k];
+        }
+}
+__device__ __forceinline__ void contact_rows(const Dev& d, uint32_t c, float4 e, const Lite& A, const Lite& B,
+                                             V6 ja[3], V6 jb[3], float err[3]) {
+    load_jac(d, c, ja, jb);
+    const float e3[3] = {e.x, e.y, e.z};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) err[k] = e3[k] + dot6(ja[k], A.dx) + dot6(jb[k], B.dx);
+}
+
+__global__ void k_contact_jacobians(Dev d, uint32_t phase) {
+    if (phase != 0 && d.ctr->impact == 0) return;
+    const uint32_t n_con = d.ctr->n_contacts;
+    for (uint32_t c = grid_stride_begin(); c < n_con; c += grid_stride()) {
+        const uint2 ab = d.c_bodies[c];
+        V6 ja[3], jb[3];
+        contact_jacobians(v3(d.c_n[c]), v3(d.c_p[c]), v3(d.c_aa[c]), v3(d.c_ab[c]), v3(d.tx[ab.x]), q4(d.tq[ab.x]),
+                          v3(d.tx[ab.y]), q4(d.tq[ab.y]), ja, jb);
+        float f[36];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                f[6 * r + k] = ja[r].v[k];
+                f[18 + 6 * r + k] = jb[r].v[k];
+            }
+        float4* p = d.c_jac + size_t(c) * 9;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) p[k] = make_float4(f[4 * k], f[4 * k + 1], f[4 * k + 2], f[4 * k + 3]);
+    }
+}
+void launch_contact_jacobians(const Dev& d, uint32_t phase, cudaStream_t s) {
+    k_contact_jacobians<<<blocks_for(d.cap_contact), kBlock, 0, s>>>(d, phase);
 }
 
 __device__ __forceinline__ void apply_pose_update(const Dev& d, uint32_t i, const V6& u) {
@@ -59,162 +109,313 @@ __device__ __forceinline__ void apply_pose_update(const Dev& d, uint32_t i, cons
     d.dxa[i] = make_float4(2.0f * rel.x, 2.0f * rel.y, 2.0f * rel.z, 0.0f);
 }
 
-// geometry_constraints_solve.slang:331-491 for one body.
-__device__ void solve_body(const Dev& d, uint32_t i, uint32_t phase, float dt) {
-    const Lite me = load_lite(d, i);
-    const float4 ia = d.inA[i], ib = d.inB[i];
-    Blk blk;
+// Group-per-body primal: 8 lanes solve one body, 4 bodies per warp, so a
+// whole colour of a large pile is in flight at once. Lanes evaluate the
+// body's contact rows 8 at a time (coalesced SoA loads) and stage them in
+// shared memory; each lane owns 3-4 of the 27 entries of the packed 6x6 block
+// (21 Hessian, 6 gradient) and adds the staged rows to them in list order.
+// Every entry thus sees exactly the additions, in exactly the order, of the
+// serial per-body loop of geometry_constraints_solve.slang:339-400, and the
+// block is bit-identical to it; the LDL^T solve then runs in registers. The
+// crossing safeguard reuses the staged normal rows: its error term is the
+// same expression at the same displacements.
+constexpr int kGroup = 8;
+constexpr uint32_t kNormSlots = 32;
+constexpr int kSolveThreads = 512;
+constexpr int kGroupsPerBlock = kSolveThreads / kGroup;
+struct GroupRows {
+    float r[kGroup][3][8];      // chunk being accumulated: 3 rows of (jacobian[6], stiffness, force)
+    float nrow[kNormSlots][8];  // normal row: jacobian[6], raw penalty, trial force
+    uint32_t flag[kGroup];
+};
+
+__device__ __forceinline__ void entry_ik(int e, int& i, int& k) {
+    i = e >= 15 ? 5 : e >= 10 ? 4 : e >= 6 ? 3 : e >= 3 ? 2 : e >= 1 ? 1 : 0;
+    k = e - i * (i + 1) / 2;
+}
+
+// Lane gl owns entries gl, gl+8, gl+16, gl+24 (those below 27).
+__device__ __forceinline__ void gather_block(const float ent[4], Blk& blk, uint32_t gmask, int gbase) {
 #pragma unroll
-    for (int k = 0; k < 21; ++k) blk.h[k] = 0.0f;
-    blk.h[bidx(0, 0)] = ia.x;
-    blk.h[bidx(1, 1)] = ia.x;
-    blk.h[bidx(2, 2)] = ia.x;
-    blk.h[bidx(3, 3)] = ia.y;
-    blk.h[bidx(4, 3)] = ia.z;
-    blk.h[bidx(5, 3)] = ib.x;
-    blk.h[bidx(4, 4)] = ia.w;
-    blk.h[bidx(5, 4)] = ib.y;
-    blk.h[bidx(5, 5)] = ib.z;
+    for (int e = 0; e < 21; ++e) blk.h[e] = __shfl_sync(gmask, ent[e / 8], gbase + (e % 8));
 #pragma unroll
-    for (int r = 0; r < 6; ++r) {
-        blk.g[r] = 0.0f;
+    for (int r = 0; r < 6; ++r) blk.g[r] = __shfl_sync(gmask, ent[(21 + r) / 8], gbase + ((21 + r) % 8));
+}
+__device__ __forceinline__ void own_entries(const Blk& blk, int gl, float ent[4]) {
 #pragma unroll
-        for (int c = 0; c < 6; ++c) blk.g[r] += blk.h[bidx(r, c)] * me.dx.v[c];
-    }
-    const uint32_t lo = d.inc_off[i], cnt = d.deg[i];
-    for (uint32_t k = 0; k < cnt; ++k) {
-        const uint32_t p = d.inc_list[lo + k];
-        const uint32_t a = d.act_a[p], b = d.act_b[p];
-        const bool first = i == a;
-        const Lite other = load_lite(d, first ? b : a);
-        const Lite& A = first ? me : other;
-        const Lite& B = first ? other : me;
-        const float friction = sqrtf(d.p1[a].x * d.p1[b].x);
-        const uint32_t off = d.act_off[p], np = d.act_cnt[p];
-        for (uint32_t q = 0; q < np; ++q) {
-            const uint32_t c = off + q;
-            const float4 n4 = d.c_n[c], lam = d.c_lam[c], pen = d.c_pen[c];
-            V6 ja[3], jb[3];
-            float err[3];
-            contact_rows(v3(n4), v3(d.c_p[c]), v3(d.c_aa[c]), v3(d.c_ab[c]), d.c_e[c], A, B, ja, jb, err);
-            F3 trial{lam.x + pen.x * err[0], lam.y + pen.y * err[1], lam.z + pen.z * err[2]};
-            F3 f = project_contact(trial, friction);
-            F3 s = stiffness_scales(trial, friction);
-            float forces[3] = {f.n, f.t0, f.t1};
-            if (phase != 0) {
-                V3 t0, t1;
-                basis(v3(n4), t0, t1);
-                const V3 af = v3(d.c_accf[c]);
-                forces[0] = f.n - lam.w / dt;
-                forces[1] = f.t0 - dot(af, t0) / dt;
-                forces[2] = f.t1 - dot(af, t1) / dt;
-            }
-            const float st[3] = {s.n, s.t0, s.t1};
-            const float pk[3] = {pen.x, pen.y, pen.z};
+    for (int m = 0; m < 4; ++m) {
+        const int e = gl + 8 * m;
+        float v = 0.0f;
 #pragma unroll
-            for (int x = 0; x < 3; ++x) add_row(blk, first ? ja[x] : jb[x], pk[x] * st[x], forces[x]);
-        }
-    }
-    const uint32_t jlo = d.jinc_off[i], jcnt = d.jdeg[i];
-    for (uint32_t k = 0; k < jcnt; ++k) {
-        const uint32_t j = d.jinc_list[jlo + k];
-        const JointState js = d.jstate[j];
-        if (!js.enabled) continue;
-        const uint32_t a = js.dense_a, b = js.dense_b;
-        const bool first = i == a;
-        if (phase == 0) {
-            BodyView A = load_body(d, a), B = load_body(d, b);
-            visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]), q4(d.q[b]),
-                        d.p0[a], d.p0[b], dt, &blk, first, kVisitAccumulate, nullptr, nullptr);
-        } else {
-            const Lite A = load_lite(d, a), B = load_lite(d, b);
-            for (uint32_t r = 0; r < js.count; ++r) {
-                Row row = load_row(d.jrows[size_t(j) * 18 + r]);
-                if (row.stiffness >= kMaxPenalty) row_accumulate(blk, row, first, A.dx, B.dx, dt);
-            }
-        }
-    }
-    V6 upd;
-    if (!block_solve(blk, upd)) return;
-    bool crossing = false;
-    for (uint32_t k = 0; k < cnt; ++k) {
-        const uint32_t p = d.inc_list[lo + k];
-        const uint32_t a = d.act_a[p], b = d.act_b[p];
-        const bool first = i == a;
-        const Lite other = load_lite(d, first ? b : a);
-        const Lite& A = first ? me : other;
-        const Lite& B = first ? other : me;
-        const uint32_t off = d.act_off[p], np = d.act_cnt[p];
-        for (uint32_t q = 0; q < np; ++q) {
-            const uint32_t c = off + q;
-            const V3 n = v3(d.c_n[c]), pt = v3(d.c_p[c]);
-            const V3 arm_a = sub(pt, A.x), arm_b = sub(pt, B.x);
-            V6 ja = jac(mul(n, -1.0f), mul(cross(arm_a, n), -1.0f));
-            V6 jb = jac(n, cross(arm_b, n));
-            float e = d.c_e[c].x + dot6(ja, A.dx) + dot6(jb, B.dx);
-            const V6& nr = first ? ja : jb;
-            const float lam0 = d.c_lam[c].x, k0 = d.c_pen[c].x;
-            float trial = lam0 + k0 * e;
-            if (trial <= 0.0f && trial + k0 * dot6(nr, upd) > k0 * 1.0e-6f) {
-                add_row(blk, nr, k0, trial);
-                crossing = true;
-            }
-        }
-    }
-    if (crossing) {
-        V6 safe;
-        if (block_solve(blk, safe)) upd = safe;
-    }
-    if (phase == 0) {
-        apply_pose_update(d, i, upd);
-    } else {
-        float4 l = d.dxl[i], a = d.dxa[i];
-        l.x += upd.v[0];
-        l.y += upd.v[1];
-        l.z += upd.v[2];
-        a.x += upd.v[3];
-        a.y += upd.v[4];
-        a.z += upd.v[5];
-        d.dxl[i] = l;
-        d.dxa[i] = a;
+        for (int q = 0; q < 21; ++q) v = e == q ? blk.h[q] : v;
+#pragma unroll
+        for (int r = 0; r < 6; ++r) v = e == 21 + r ? blk.g[r] : v;
+        ent[m] = v;
     }
 }
 
-// advance_duals for one pair (geometry_constraints_solve.slang:494-565 without
-// the last-iteration block); returns max(0, C_n) over its points.
-__device__ float dual_pair(const Dev& d, uint32_t i, float dt) {
-    const uint32_t a = d.act_a[i], b = d.act_b[i];
+__device__ __forceinline__ void accumulate_chunk(float ent[4], int gl, const GroupRows& sm, uint32_t m) {
+    // Products first (independent, pipelined loads), then the ordered adds.
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int e = gl + 8 * q;
+        if (e >= 27) continue;
+        int ei = 0, ek = 0;
+        const bool hess = e < 21;
+        if (hess) entry_ik(e, ei, ek);
+        else ei = e - 21;
+        float prod[kGroup][3];
+#pragma unroll
+        for (int t = 0; t < kGroup; ++t)
+#pragma unroll
+            for (int x = 0; x < 3; ++x) {
+                const float* row = sm.r[t][x];
+                prod[t][x] = hess ? row[6] * row[ei] * row[ek] : row[ei] * row[7];
+            }
+#pragma unroll
+        for (int t = 0; t < kGroup; ++t)
+#pragma unroll
+            for (int x = 0; x < 3; ++x)
+                if (t < int(m)) ent[q] += prod[t][x];
+    }
+}
+
+__device__ __forceinline__ void accumulate_crossing(float ent[4], int gl, const GroupRows& sm, uint32_t s0,
+                                                    uint32_t m) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int e = gl + 8 * q;
+        if (e >= 27) continue;
+        int ei = 0, ek = 0;
+        if (e < 21) entry_ik(e, ei, ek);
+        for (uint32_t t = 0; t < m; ++t) {
+            if (!sm.flag[t]) continue;
+            const float* row = sm.nrow[(s0 + t) % kNormSlots];
+            if (e < 21) ent[q] += row[6] * row[ei] * row[ek];
+            else ent[q] += row[e - 21] * row[7];
+        }
+    }
+}
+
+// Rows of one contact for body i into chunk slot `slot`; its normal row,
+// raw penalty and normal trial also go to nrow[nslot].
+__device__ __forceinline__ void stage_contact(const Dev& d, const Lite& me, float my_friction, uint32_t code,
+                                              uint32_t other_body, uint32_t phase, float dt, GroupRows& sm, int slot,
+                                              int nslot) {
+    const uint32_t c = code & 0x7fffffffu;
+    const bool first = (code >> 31) == 0;
+    const Lite other = load_lite(d, other_body);
+    const Lite& A = first ? me : other;
+    const Lite& B = first ? other : me;
+    const float of = d.p1[other_body].x;
+    const float friction = sqrtf(first ? my_friction * of : of * my_friction);
+    const float4 lam = d.c_lam[c], pen = d.c_pen[c];
+    V6 ja[3], jb[3];
+    float err[3];
+    contact_rows(d, c, d.c_e[c], A, B, ja, jb, err);
+    F3 trial{lam.x + pen.x * err[0], lam.y + pen.y * err[1], lam.z + pen.z * err[2]};
+    if (nslot >= 0) {
+        const V6& nr = first ? ja[0] : jb[0];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) sm.nrow[nslot][k] = nr.v[k];
+        sm.nrow[nslot][6] = pen.x;
+        sm.nrow[nslot][7] = trial.n;
+    }
+    if (slot < 0) return;
+    F3 f = project_contact(trial, friction);
+    F3 sc = stiffness_scales(trial, friction);
+    float forces[3] = {f.n, f.t0, f.t1};
+    if (phase != 0) {
+        V3 t0, t1;
+        basis(v3(d.c_n[c]), t0, t1);
+        const V3 af = v3(d.c_accf[c]);
+        forces[0] = f.n - lam.w / dt;
+        forces[1] = f.t0 - dot(af, t0) / dt;
+        forces[2] = f.t1 - dot(af, t1) / dt;
+    }
+    const float st[3] = {pen.x * sc.n, pen.y * sc.t0, pen.z * sc.t1};
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        const V6& row = first ? ja[x] : jb[x];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) sm.r[slot][x][k] = row.v[k];
+        sm.r[slot][x][6] = st[x];
+        sm.r[slot][x][7] = forces[x];
+    }
+}
+
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float dt, GroupRows& sm, uint32_t gmask,
+                                 int gl, int gbase, bool trace = false) {
+    const unsigned long long t0 = trace ? gtimer() : 0ull;
+    auto mark = [&](int k) {
+        if (trace && gl == 0) atomicMax(&d.ctr->dbg_body[k], gtimer() - t0);
+    };
+    const Lite me = load_lite(d, i);
+    const float my_friction = d.p1[i].x;
+    const uint32_t ro = d.roff[i], rn = d.rcount[i];
+    float ent[4];
+    {
+        const float4 ia = d.inA[i], ib = d.inB[i];
+        float H[21];
+#pragma unroll
+        for (int k = 0; k < 21; ++k) H[k] = 0.0f;
+        H[bidx(0, 0)] = ia.x;
+        H[bidx(1, 1)] = ia.x;
+        H[bidx(2, 2)] = ia.x;
+        H[bidx(3, 3)] = ia.y;
+        H[bidx(4, 3)] = ia.z;
+        H[bidx(5, 3)] = ib.x;
+        H[bidx(4, 4)] = ia.w;
+        H[bidx(5, 4)] = ib.y;
+        H[bidx(5, 5)] = ib.z;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int e = gl + 8 * q;
+            float v = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 21; ++k) v = e == k ? H[k] : v;
+            if (e >= 21 && e < 27) {
+                const int r = e - 21;
+                float gs = 0.0f;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) gs += H[bidx(r, c)] * me.dx.v[c];
+                v = gs;
+            }
+            ent[q] = v;
+        }
+    }
+    for (uint32_t base = 0; base < rn; base += kGroup) {
+        const uint32_t sidx = base + gl;
+        if (sidx < rn)
+            stage_contact(d, me, my_friction, d.blist[ro + sidx], d.bother[ro + sidx], phase, dt, sm, gl,
+                          sidx < kNormSlots ? int(sidx) : -1);
+        __syncwarp(gmask);
+        accumulate_chunk(ent, gl, sm, min(uint32_t(kGroup), rn - base));
+        __syncwarp(gmask);
+    }
+    mark(0);
+    Blk blk;
+    gather_block(ent, blk, gmask, gbase);
+    mark(1);
+    const uint32_t jcnt = d.jdeg[i];
+    if (jcnt) {
+        if (gl == 0) {
+            const uint32_t jlo = d.jinc_off[i];
+            for (uint32_t k = 0; k < jcnt; ++k) {
+                const uint32_t j = d.jinc_list[jlo + k];
+                const JointState js = d.jstate[j];
+                if (!js.enabled) continue;
+                const uint32_t a = js.dense_a, b = js.dense_b;
+                const bool first = i == a;
+                if (phase == 0) {
+                    BodyView A = load_body(d, a), B = load_body(d, b);
+                    visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]),
+                                q4(d.q[b]), d.p0[a], d.p0[b], dt, &blk, first, kVisitAccumulate, nullptr, nullptr);
+                } else {
+                    const Lite A = load_lite(d, a), B = load_lite(d, b);
+                    for (uint32_t r = 0; r < js.count; ++r) {
+                        Row row = load_row(d.jrows[size_t(j) * 18 + r]);
+                        if (row.stiffness >= kMaxPenalty) row_accumulate(blk, row, first, A.dx, B.dx, dt);
+                    }
+                }
+            }
+        }
+        __syncwarp(gmask);
+#pragma unroll
+        for (int e = 0; e < 21; ++e) blk.h[e] = __shfl_sync(gmask, blk.h[e], gbase);
+#pragma unroll
+        for (int r = 0; r < 6; ++r) blk.g[r] = __shfl_sync(gmask, blk.g[r], gbase);
+    }
+    V6 upd;
+    if (!block_solve(blk, upd)) return;
+    mark(2);
+    // Crossing safeguard (geometry_constraints_solve.slang:433-475).
+    own_entries(blk, gl, ent);
+    bool crossing = false;
+    for (uint32_t base = 0; base < rn; base += kGroup) {
+        const uint32_t sidx = base + gl;
+        if (rn > kNormSlots && base >= kNormSlots && sidx < rn)
+            stage_contact(d, me, my_friction, d.blist[ro + sidx], d.bother[ro + sidx], phase, dt, sm, -1,
+                          int(sidx % kNormSlots));
+        __syncwarp(gmask);
+        uint32_t flag = 0;
+        if (sidx < rn) {
+            const float* row = sm.nrow[sidx % kNormSlots];
+            V6 nr;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) nr.v[k] = row[k];
+            const float k0 = row[6], trial = row[7];
+            flag = (trial <= 0.0f && trial + k0 * dot6(nr, upd) > k0 * 1.0e-6f) ? 1u : 0u;
+        }
+        sm.flag[gl] = flag;
+        __syncwarp(gmask);
+        if (__any_sync(gmask, flag)) {
+            crossing = true;
+            accumulate_crossing(ent, gl, sm, base % kNormSlots, min(uint32_t(kGroup), rn - base));
+        }
+        __syncwarp(gmask);
+    }
+    mark(3);
+    if (crossing) {
+        gather_block(ent, blk, gmask, gbase);
+        V6 safe;
+        if (block_solve(blk, safe)) upd = safe;
+    }
+    mark(4);
+    if (trace && gl == 0) atomicMax(&d.ctr->dbg_rn, rn);
+    if (gl == 0) {
+        if (phase == 0) {
+            apply_pose_update(d, i, upd);
+        } else {
+            float4 l = d.dxl[i], a = d.dxa[i];
+            l.x += upd.v[0];
+            l.y += upd.v[1];
+            l.z += upd.v[2];
+            a.x += upd.v[3];
+            a.y += upd.v[4];
+            a.z += upd.v[5];
+            d.dxl[i] = l;
+            d.dxa[i] = a;
+        }
+    }
+}
+
+// advance_duals for one contact point (geometry_constraints_solve.slang:
+// 494-532; the last-iteration block runs in k_contact_finalize). Returns
+// max(0, C_n) at the current displacements.
+__device__ float dual_contact(const Dev& d, uint32_t c, float dt, uint32_t phase) {
+    const uint2 ab = d.c_bodies[c];
+    const uint32_t a = ab.x, b = ab.y;
+    if (phase != 0 && d.impact[a] == 0 && d.impact[b] == 0) return 0.0f;
     const Lite A = load_lite(d, a), B = load_lite(d, b);
     const float friction = sqrtf(d.p1[a].x * d.p1[b].x);
     const float beta = (1.0f / (fmx(d.p0[a].x + d.p0[b].x, 1.0e-6f) * dt * dt)) * 100.0f;
-    const uint32_t off = d.act_off[i], np = d.act_cnt[i];
-    float res = 0.0f;
-    for (uint32_t q = 0; q < np; ++q) {
-        const uint32_t c = off + q;
-        const float4 n4 = d.c_n[c];
-        float4 lam = d.c_lam[c], pen = d.c_pen[c];
-        V6 ja[3], jb[3];
-        float err[3];
-        contact_rows(v3(n4), v3(d.c_p[c]), v3(d.c_aa[c]), v3(d.c_ab[c]), d.c_e[c], A, B, ja, jb, err);
-        res = fmx(res, err[0]);
-        F3 f = project_contact(F3{lam.x + pen.x * err[0], lam.y + pen.y * err[1], lam.z + pen.z * err[2]}, friction);
-        float tx = lam.y + pen.y * err[1];
-        float ty = lam.z + pen.z * err[2];
-        float bound = friction * f.n;
-        bool stick = tx * tx + ty * ty <= bound * bound;
-        lam.x = f.n;
-        lam.y = f.t0;
-        lam.z = f.t1;
-        if (f.n > 0.0f) pen.x = fmn(kMaxPenalty, pen.x + beta * fab(err[0]));
-        if (stick) {
-            pen.y = fmn(kMaxPenalty, pen.y + beta * fab(err[1]));
-            pen.z = fmn(kMaxPenalty, pen.z + beta * fab(err[2]));
-        }
-        pen.w = stick ? 1.0f : 0.0f;
-        d.c_lam[c] = lam;
-        d.c_pen[c] = pen;
+    float4 lam = d.c_lam[c], pen = d.c_pen[c];
+    V6 ja[3], jb[3];
+    float err[3];
+    contact_rows(d, c, d.c_e[c], A, B, ja, jb, err);
+    F3 f = project_contact(F3{lam.x + pen.x * err[0], lam.y + pen.y * err[1], lam.z + pen.z * err[2]}, friction);
+    const float tx = lam.y + pen.y * err[1];
+    const float ty = lam.z + pen.z * err[2];
+    const float bound = friction * f.n;
+    const bool stick = tx * tx + ty * ty <= bound * bound;
+    lam.x = f.n;
+    lam.y = f.t0;
+    lam.z = f.t1;
+    if (f.n > 0.0f) pen.x = fmn(kMaxPenalty, pen.x + beta * fab(err[0]));
+    if (stick) {
+        pen.y = fmn(kMaxPenalty, pen.y + beta * fab(err[1]));
+        pen.z = fmn(kMaxPenalty, pen.z + beta * fab(err[2]));
     }
-    return res;
+    pen.w = stick ? 1.0f : 0.0f;
+    d.c_lam[c] = lam;
+    d.c_pen[c] = pen;
+    return fmx(0.0f, err[0]);
 }
 
 __device__ float dual_joint(const Dev& d, uint32_t j, uint32_t phase, float dt) {
@@ -251,40 +452,59 @@ __device__ __forceinline__ void atomic_max_pos(float* addr, float v) {
     atomicMax(reinterpret_cast<int*>(addr), __float_as_int(fmx(v, 0.0f)));
 }
 
-__global__ void __launch_bounds__(kBlock) k_solve(Dev d, StepParams sp, uint32_t phase) {
+__global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev d, StepParams sp, uint32_t phase) {
     Counters* c = d.ctr;
     if (phase != 0 && c->impact == 0) return;
+    extern __shared__ GroupRows rows[];
+    const int lane = threadIdx.x & 31;
+    const int gl = lane % kGroup, gbase = lane - gl;
+    const uint32_t gmask = 0xffu << gbase;
+    GroupRows& sm = rows[threadIdx.x / kGroup];
     const float dt = sp.dt;
     const uint32_t colors = c->colors;
     uint32_t budget = sp.budget_request;
     if (!sp.realtime && sp.requested == 0) budget = max(budget, c->joint_iters);
+    if (phase != 0 && sp.tolerance > 0.0f) budget = c->budget;
     const bool adaptive = phase == 0 && sp.tolerance > 0.0f;
     const uint32_t iters = adaptive ? min(max(sp.max_iterations, 1u), kMaxIterations) : min(budget, kMaxIterations);
-    const uint32_t n_act = c->n_act;
+    const uint32_t n_con = c->n_contacts;
+    const uint32_t group = (blockIdx.x * kSolveThreads + threadIdx.x) / kGroup;
+    const uint32_t groups = gridDim.x * kGroupsPerBlock;
     __shared__ float block_res;
+    const bool timing = sp.debug_timing && phase == 0;
+    auto now = [] {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        return t;
+    };
+    if (timing && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_start = now();
     for (uint32_t it = 0; it < iters; ++it) {
         for (uint32_t col = 0; col < colors; ++col) {
             const uint32_t b0 = c->color_off[col], b1 = c->color_off[col + 1];
-            for (uint32_t k = b0 + grid_stride_begin(); k < b1; k += grid_stride()) {
+            for (uint32_t k = b0 + group; k < b1; k += groups) {
                 const uint32_t i = d.corder[k];
                 if (phase != 0 && d.impact[i] == 0) continue;
-                solve_body(d, i, phase, dt);
+                solve_body_group(d, i, phase, dt, sm, gmask, gl, gbase, timing && it == 0 && col + 1 == colors);
+            }
+            if (timing && it == 0 && col < 18) {
+                __syncthreads();
+                if (threadIdx.x == 0) atomicMax(&c->dbg_work[col], now());
             }
             if (!grid_sync(c)) return;
+            if (timing && it == 0 && col < 18 && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_release[col] = now();
         }
         if (threadIdx.x == 0) block_res = 0.0f;
         __syncthreads();
         float res = 0.0f;
-        for (uint32_t i = grid_stride_begin(); i < n_act; i += grid_stride()) {
-            if (phase != 0 && d.impact[d.act_a[i]] == 0 && d.impact[d.act_b[i]] == 0) continue;
-            res = fmx(res, dual_pair(d, i, dt));
-        }
+        for (uint32_t k = grid_stride_begin(); k < n_con; k += grid_stride()) res = fmx(res, dual_contact(d, k, dt, phase));
         for (uint32_t j = grid_stride_begin(); j < d.nj; j += grid_stride()) res = fmx(res, dual_joint(d, j, phase, dt));
         for (int o = 16; o > 0; o >>= 1) res = fmx(res, __shfl_xor_sync(0xffffffffu, res, o));
         if ((threadIdx.x & 31) == 0) atomic_max_pos(&block_res, res);
         __syncthreads();
         if (threadIdx.x == 0 && phase == 0) atomic_max_pos(&c->residual_trace[it], block_res);
+        if (timing && it == 0 && threadIdx.x == 0) atomicMax(&c->dbg_work[19], now());
         if (!grid_sync(c)) return;
+        if (timing && it == 0 && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_release[19] = now();
         bool last = it + 1 == iters;
         if (adaptive && ((volatile float*)c->residual_trace)[it] <= sp.tolerance) last = true;
         if (last) {
@@ -301,44 +521,44 @@ __global__ void __launch_bounds__(kBlock) k_solve(Dev d, StepParams sp, uint32_t
 }
 
 const void* solve_kernel_ptr = reinterpret_cast<const void*>(&k_solve);
+const int solve_kernel_threads = kSolveThreads;
+const size_t solve_kernel_smem = sizeof(GroupRows) * kGroupsPerBlock;
 
-// Last-iteration contact work (geometry_constraints_solve.slang:533-561).
+// Last-iteration contact work (geometry_constraints_solve.slang:533-561),
+// one thread per contact point.
 __global__ void k_contact_finalize(Dev d, StepParams sp, uint32_t phase) {
     if (phase != 0 && d.ctr->impact == 0) return;
     const float dt = sp.dt;
-    const uint32_t n_act = d.ctr->n_act;
-    for (uint32_t i = grid_stride_begin(); i < n_act; i += grid_stride()) {
-        const uint32_t a = d.act_a[i], b = d.act_b[i];
+    const uint32_t n_con = d.ctr->n_contacts;
+    for (uint32_t c = grid_stride_begin(); c < n_con; c += grid_stride()) {
+        const uint2 ab = d.c_bodies[c];
+        const uint32_t a = ab.x, b = ab.y;
         if (phase != 0 && d.impact[a] == 0 && d.impact[b] == 0) continue;
-        V3 xa, xb;
-        Q4 qa, qb;
-        if (phase != 0) {
-            xa = v3(d.tx[a]);
-            qa = q4(d.tq[a]);
-            xb = v3(d.tx[b]);
-            qb = q4(d.tq[b]);
-        } else {
-            BodyView A = load_body(d, a), B = load_body(d, b);
-            body_pose(A, xa, qa);
-            body_pose(B, xb, qb);
-        }
-        const uint32_t off = d.act_off[i], np = d.act_cnt[i];
-        for (uint32_t q = 0; q < np; ++q) {
-            const uint32_t c = off + q;
-            const V3 n = v3(d.c_n[c]);
-            float4 lam = d.c_lam[c];
-            const float stick = d.c_pen[c].w;
-            V3 t0, t1;
-            basis(n, t0, t1);
-            lam.w = lam.x * dt;
-            d.c_lam[c] = lam;
-            d.c_accf[c] = f4(mul(add(mul(t0, lam.y), mul(t1, lam.z)), dt));
-            if (stick == 0.0f) {
-                const V3 pt = v3(d.c_p[c]);
-                float4 aa = d.c_aa[c], ab = d.c_ab[c];
-                d.c_aa[c] = f4(inv_rotate(qa, sub(pt, xa)), aa.w);
-                d.c_ab[c] = f4(inv_rotate(qb, sub(pt, xb)), ab.w);
+        const V3 n = v3(d.c_n[c]);
+        float4 lam = d.c_lam[c];
+        const float stick = d.c_pen[c].w;
+        V3 t0, t1;
+        basis(n, t0, t1);
+        lam.w = lam.x * dt;
+        d.c_lam[c] = lam;
+        d.c_accf[c] = f4(mul(add(mul(t0, lam.y), mul(t1, lam.z)), dt));
+        if (stick == 0.0f) {
+            V3 xa, xb;
+            Q4 qa, qb;
+            if (phase != 0) {
+                xa = v3(d.tx[a]);
+                qa = q4(d.tq[a]);
+                xb = v3(d.tx[b]);
+                qb = q4(d.tq[b]);
+            } else {
+                BodyView A = load_body(d, a), B = load_body(d, b);
+                body_pose(A, xa, qa);
+                body_pose(B, xb, qb);
             }
+            const V3 pt = v3(d.c_p[c]);
+            const float4 aa = d.c_aa[c], ab = d.c_ab[c];
+            d.c_aa[c] = f4(inv_rotate(qa, sub(pt, xa)), aa.w);
+            d.c_ab[c] = f4(inv_rotate(qb, sub(pt, xb)), ab.w);
         }
     }
 }
@@ -464,11 +684,10 @@ __global__ void k_impact_setup(Dev d, StepParams sp, const float4* ox, const flo
         const Lite A = load_lite(d, a), B = load_lite(d, b);
         for (uint32_t q = d.act_off[i]; q < d.act_off[i] + d.act_cnt[i]; ++q) {
             const float4 n4 = d.c_n[q];
-            const V3 n = v3(n4), pt = v3(d.c_p[q]);
-            V6 ja = jac(mul(n, -1.0f), mul(cross(sub(pt, A.x), n), -1.0f));
-            V6 jb = jac(n, cross(sub(pt, B.x), n));
+            V6 ja[3], jb[3];
+            load_jac(d, q, ja, jb);  // normal rows: the phase-0 targets' arms
             float4 e = d.c_e[q];
-            e.x = fmx(0.0f, -(n4.w + dot6(ja, A.dx) + dot6(jb, B.dx)));
+            e.x = fmx(0.0f, -(n4.w + dot6(ja[0], A.dx) + dot6(jb[0], B.dx)));
             d.c_e[q] = e;
         }
     }
@@ -504,7 +723,6 @@ __global__ void k_impact_constraints(Dev d, StepParams sp, const float4* ov, con
     for (uint32_t i = grid_stride_begin(); i < n_act; i += grid_stride()) {
         const uint32_t a = d.act_a[i], b = d.act_b[i];
         if (d.impact[a] == 0 && d.impact[b] == 0) continue;
-        const Lite A = load_lite(d, a), B = load_lite(d, b);
         const V6 va = jac(mul(v3(ov[a]), dt), mul(v3(ow[a]), dt));
         const V6 vb = jac(mul(v3(ov[b]), dt), mul(v3(ow[b]), dt));
         const float rest_ab = fmn(d.p1[a].y, d.p1[b].y);
@@ -512,8 +730,7 @@ __global__ void k_impact_constraints(Dev d, StepParams sp, const float4* ov, con
             float4 e = d.c_e[q];
             const float gap = e.x;
             V6 ja[3], jb[3];
-            float err[3];
-            contact_rows(v3(d.c_n[q]), v3(d.c_p[q]), v3(d.c_aa[q]), v3(d.c_ab[q]), e, A, B, ja, jb, err);
+            load_jac(d, q, ja, jb);  // recomputed from the reset targets
             const bool cached = d.c_aa[q].w != 0.0f;
             const float speed = e.w;
             const float rest = !cached && speed < -1.0f ? rest_ab : 0.0f;
@@ -578,22 +795,29 @@ void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, int co
         if (phase != 0) {
             k_impact_setup<<<blocks_for(d.cap_pair), kBlock, 0, s>>>(d, sp, o.ox, o.oq, o.ov, o.ow);
             k_impact_bodies<<<blocks_for(d.n), kBlock, 0, s>>>(d, o.ox, o.oq, o.ov, o.ow);
+            launch_contact_jacobians(d, 1, s);
             k_impact_constraints<<<pb, kBlock, 0, s>>>(d, sp, o.ov, o.ow);
+            prof_mark(s, "impact setup");
         }
         Dev dd = d;
         uint32_t ph = phase;
         StepParams spp = sp;
         void* args[] = {&dd, &spp, &ph};
-        cudaLaunchCooperativeKernel(solve_kernel_ptr, dim3(coop_blocks), dim3(kBlock), args, 0, s);
-        k_contact_finalize<<<blocks_for(d.cap_pair), kBlock, 0, s>>>(d, sp, phase);
+        solve_timer_begin(s);
+        cudaLaunchCooperativeKernel(solve_kernel_ptr, dim3(coop_blocks), dim3(kSolveThreads), args, solve_kernel_smem, s);
+        solve_timer_end(s);
+        prof_mark(s, phase ? "solve phase 1" : "solve phase 0");
+        k_contact_finalize<<<blocks_for(d.cap_contact), kBlock, 0, s>>>(d, sp, phase);
         k_free_anchor<<<blocks_for(d.cap_pair > d.n ? d.cap_pair : d.n), kBlock, 0, s>>>(d, phase);
         k_free_mean<<<blocks_for(d.n), kBlock, 0, s>>>(d, phase);
         k_free_subtract<<<blocks_for(d.n), kBlock, 0, s>>>(d, phase);
         k_apply<<<blocks_for(d.n), kBlock, 0, s>>>(d, sp, phase, o.ox, o.oq, o.ov, o.ow);
         if (phase == 0 && d.nj) k_project_hinges<<<1, 32, 0, s>>>(d, o.ox, o.oq);
+        prof_mark(s, phase ? "finish phase 1" : "finish phase 0");
     }
     k_clamp_commit<<<blocks_for(d.n), kBlock, 0, s>>>(d, o.ox, o.oq, o.ov, o.ow);
     k_cache_save<<<blocks_for(d.cap_pair), kBlock, 0, s>>>(d, sp);
+    prof_mark(s, "commit+cache save");
 }
 
 }  // namespace pmb

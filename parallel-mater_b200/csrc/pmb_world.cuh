@@ -45,6 +45,9 @@ struct Counters {
     uint32_t color_off[kMaxColors + 1];
     uint32_t color_cursor[kMaxColors];
     float residual_trace[kMaxIterations];
+    unsigned long long dbg_work[20], dbg_release[20], dbg_start;
+    unsigned long long dbg_body[8];
+    uint32_t dbg_rn;
 };
 
 struct StepParams {
@@ -55,6 +58,7 @@ struct StepParams {
     uint32_t requested;
     float tolerance;
     uint32_t max_iterations;
+    uint32_t debug_timing;  // record solve-kernel timestamps for iteration 0
 };
 
 struct JointRow {  // constraint_math.slang AvbdRow, packed for the device
@@ -132,6 +136,8 @@ struct Dev {
     // active pairs / contacts
     uint32_t *act_a, *act_b, *act_code, *act_off, *act_cnt, *act_impact;
     uint32_t* c_pair;
+    uint2* c_bodies;  // (a, b) of the contact's pair
+    float4* c_jac;    // 9 per contact: jacobian rows n,t0,t1 of body a then body b
     float4 *c_n, *c_p, *c_e, *c_aa, *c_ab, *c_lam, *c_pen, *c_accf;
     // contact cache from the previous tick (double-buffered by the host)
     uint32_t *sv_code, *sv_off, *sv_cnt;
@@ -145,6 +151,8 @@ struct Dev {
     uint32_t *deg, *inc_off, *inc_cursor, *inc_list;
     uint32_t *jdeg, *jinc_off, *jinc_cursor, *jinc_list;
     uint32_t* corder;
+    uint32_t *rcount, *roff, *blist;  // per-body flattened contact rows (bit 31: second body)
+    uint32_t* bother;                 // the other body of each flattened row
     uint32_t *mem_count, *mem_off, *mem_cursor, *mem_list;
     // joints
     Joint* joints;
@@ -210,7 +218,16 @@ void scan_u32(const uint32_t* in, uint32_t* out, const uint32_t* count_ptr, uint
 void scan_u64(const uint64_t* in, uint64_t* out, const uint32_t* count_ptr, uint32_t capacity, uint64_t* tmp,
               cudaStream_t s);
 int coop_blocks_for(const void* kernel, int threads, size_t smem);
+// Stage timing for diagnosis: records a CUDA event named `stage` when a
+// profiled step is being enqueued (never during graph capture).
+void prof_mark(cudaStream_t s, const char* stage);
+// Dominant-kernel timing: brackets each solve launch with CUDA events when on.
+void solve_timer_begin(cudaStream_t s);
+void solve_timer_end(cudaStream_t s);
 extern const void* solve_kernel_ptr;
+extern const int solve_kernel_threads;
+extern const size_t solve_kernel_smem;
+void launch_contact_jacobians(const Dev& d, uint32_t phase, cudaStream_t s);
 extern const void* color_kernel_ptr;
 
 inline uint32_t blocks_for(uint32_t n, int threads = kBlock) {

@@ -57,6 +57,8 @@ def lib():
             "pmb_world_create": [vp, vp], "pmb_world_destroy": [vp],
             "pmb_world_set_stream": [vp, vp], "pmb_world_step": [vp, vp, vp],
             "pmb_world_capture": [vp, vp, u32], "pmb_world_replay": [vp],
+            "pmb_world_profile_step": [vp, vp, vp, u32],
+            "pmb_world_solve_timer": [vp, i32, vp, vp],
             "pmb_world_get_states": [vp, vp], "pmb_world_set_states": [vp, vp],
             "pmb_world_last_stats": [vp, vp], "pmb_world_apply_impulse": [vp, u32, vp, vp],
             "pmb_world_candidate_pairs": [vp, vp, u32, vp],
@@ -118,6 +120,20 @@ class World:
     def capture(self, steps=2, desc=None, **kw):
         d = np.ascontiguousarray(self.scene.step_desc(**kw) if desc is None else desc)
         _check(lib().pmb_world_capture(self.h, d.ctypes.data, steps), "pmb_world_capture")
+
+    def profile_step(self, desc=None, **kw):
+        d = np.ascontiguousarray(self.scene.step_desc(**kw) if desc is None else desc)
+        buf = ctypes.create_string_buffer(8192)
+        _check(lib().pmb_world_profile_step(self.h, d.ctypes.data, buf, 8192), "pmb_world_profile_step")
+        return buf.value.decode()
+
+    def solve_timer(self, enable=True):
+        """(summed solve-kernel ms, launches) since the last call; sets enable."""
+        ms = ctypes.c_float()
+        n = ctypes.c_uint32()
+        _check(lib().pmb_world_solve_timer(self.h, 1 if enable else 0, ctypes.byref(ms), ctypes.byref(n)),
+               "pmb_world_solve_timer")
+        return ms.value, n.value
 
     def replay(self):
         _check(lib().pmb_world_replay(self.h), "pmb_world_replay")

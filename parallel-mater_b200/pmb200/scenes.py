@@ -223,16 +223,20 @@ def pyramid(levels=10, seed=1, jitter=1e-3, friction=0.5, density=1000.0, iterat
 
 
 def box_pile(grid=(16, 16, 16), seed=2, spacing=1.8, iterations=10, profile=LEGACY,
-             wall_height=8.0) -> Scene:
+             wall_height=None) -> Scene:
     """Random boxes (edges U[0.5,1.5] per axis, density U[500,2000], friction
     U[0.3,0.8]) on a jittered grid (gx along x, gy layers along y, gz along z)
-    above a static walled container sized to the grid footprint."""
+    above a static walled container sized to the grid footprint. Walls are
+    0.75 m per spawn layer high (at least 8 m) and the ground extends 10 m
+    past them, so a settled pile stays on the ground."""
     gx, gy, gz = grid
+    if wall_height is None:
+        wall_height = max(8.0, 0.75 * gy)
     rng = np.random.Generator(np.random.Philox(seed))
     b = _Builder()
     half_x = 0.5 * gx * spacing + 1.0
     half_z = 0.5 * gz * spacing + 1.0
-    _ground(b, half_x + 1.0, half_z + 1.0)
+    _ground(b, half_x + 11.0, half_z + 11.0)
     wall_x = b.mesh(*box_mesh((0.5, 0.5 * wall_height, half_z + 1.0)))
     wall_z = b.mesh(*box_mesh((half_x + 1.0, 0.5 * wall_height, 0.5)))
     for s in (-1, 1):
