@@ -1,0 +1,290 @@
+#!/usr/bin/env python3
+# SPDX-License-Identifier: MIT
+"""Benchmark: steps/sec of the 65,536-box pile at equal residual.
+
+Workload: box_pile((64, 32, 32), seed=4) -- 65,536 random boxes (edges
+U[0.5,1.5] m, density U[500,2000] kg/m^3, friction U[0.3,0.8]) plus a static
+ground and four walls -- starting from the settled state in
+tests/golden/settled_pile_64x32x32.npz (300 ticks of plain AVBD from the spawn
+grid). A step is one rigid AVBD tick (legacy profile: predict, broadphase,
+narrowphase, contact cache, prepare, colouring, solve, impact phase, commit)
+run with the residual-driven schedule: sweep until the contact residual (RMS
+over active normal rows) is at or below --tolerance, at most --max-iterations
+sweeps. Inputs are synthetic (seeded); no dataset is involved.
+
+GPU arm (default): `value` is steps/s with the state resident in HBM, timed
+with CUDA events on the world's stream (max over ranks); `e2e` is the same
+metric through the C ABI with host buffers (state upload from pinned host
+memory, tick, state download each step). Multi-GPU runs independent replicas
+(the coupled pile does not shard). Reference arm (--impl reference): the CPU
+restatement of the reference's serial Slang CPU driver (oracle/, one core),
+on the same state and schedule, over a bounded number of ticks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "parallel-mater_b200"))
+
+METRIC = "steps/sec at 64k boxes to equal residual: learned warm-start vs plain GPU AVBD"
+GRID = (64, 32, 32)
+SEED = 4
+SETTLED = os.path.join(ROOT, "tests", "golden", "settled_pile_64x32x32.npz")
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_solve_pile65k_traffic.json")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="pmb", choices=["pmb", "reference"])
+    ap.add_argument("--tolerance", type=float, default=1e-4)
+    ap.add_argument("--max-iterations", type=int, default=64)
+    ap.add_argument("--cpu-ticks", type=int, default=1, help="ticks timed by the CPU baseline leg")
+    return ap.parse_args()
+
+
+def load_scene():
+    from pmb200 import scenes
+    scene = scenes.box_pile(GRID, seed=SEED)
+    z = np.load(SETTLED)
+    scene.states = z["states"].astype(np.float32).view(scenes.STATE_DTYPE).reshape(-1).copy()
+    return scene
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def solve_bytes(stats, n_dynamic):
+    """Algorithmic bytes of the solve kernel for one tick (per iteration:
+    primal 124 B per body + 2 x 112 B per contact point, dual 160 B per
+    contact point), over both phases when the impact phase ran."""
+    per_iter = 124 * n_dynamic + 384 * int(stats["contacts"])
+    phases = 2 if int(stats["impact"]) else 1
+    return phases * int(stats["iterations"]) * per_iter
+
+
+def cpu_baseline(scene, desc, ticks):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    w = O.OracleWorld(scene)
+    t0 = time.perf_counter()
+    stats = None
+    for _ in range(ticks):
+        stats = w.step(desc)
+    dt = time.perf_counter() - t0
+    return ticks / dt, stats
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    scene = load_scene()
+    desc = scene.step_desc(residual_tolerance=args.tolerance, max_iterations=args.max_iterations)
+    ticks = max(1, min(args.steps, args.cpu_ticks))
+    value, stats = cpu_baseline(scene, desc, ticks)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
+        "steps": ticks, "warmup": 0, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "box pile 64x32x32 (65,536 boxes), settled state, residual-driven AVBD",
+                   "bodies": scene.n, "tolerance": args.tolerance, "max_iterations": args.max_iterations,
+                   "iterations": int(stats["iterations"]), "contacts": int(stats["contacts"])},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "port",
+                         "sample": f"{ticks} tick(s) of the settled 65,541-body pile; CPU restatement of the "
+                                   "reference's serial Slang CPU driver (the generated driver needs slangc, absent)"},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def gpu_arm(args):
+    import torch
+    import torch.distributed as dist
+    from pmb200 import core, scenes
+
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world_size > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    scene = load_scene()
+    n_dyn = int((scene.bodies["motion"] == scenes.DYNAMIC).sum())
+    desc = scene.step_desc(residual_tolerance=args.tolerance, max_iterations=args.max_iterations)
+    world = core.World(scene, device=local)
+    stream = torch.cuda.current_stream()
+    world.set_stream(stream.cuda_stream)
+
+    def barrier():
+        if world_size > 1:
+            dist.barrier()
+
+    # ---- device-resident timing
+    for _ in range(args.warmup):
+        world.step(desc, stats=False)
+    world.snapshot()
+    barrier()
+    torch.cuda.synchronize()
+    world.solve_timer(True)
+    launches0 = core.kernel_launches()
+    sampler = ClockSampler(local)
+    sampler.start()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    iters, contacts, stats_all = [], [], []
+    for _ in range(args.steps):
+        world.step(desc, stats=False)
+    end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    launches = core.kernel_launches() - launches0
+    solve_ms, solve_launches = world.solve_timer(False)
+    elapsed = start.elapsed_time(end)
+    t = torch.tensor([elapsed], device="cuda")
+    if world_size > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    elapsed_max = float(t.item())
+    value = world_size * args.steps / (elapsed_max * 1e-3)
+    # Per-tick statistics of the same ticks, replayed from the snapshot
+    # (outside the timed region) for the roofline's algorithmic bytes.
+    world.restore()
+    for _ in range(args.steps):
+        st = world.step(desc)
+        stats_all.append(st)
+        iters.append(int(st["iterations"]))
+        contacts.append(int(st["contacts"]))
+    alg_bytes = sum(solve_bytes(st, n_dyn) for st in stats_all)
+    achieved = alg_bytes / (solve_ms * 1e-3) / 1e9 if solve_ms > 0 else None
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        peak, peak_src = 6650.0, "fallback"
+    traffic = None
+    try:
+        with open(PROFILE_TRAFFIC) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        pass
+
+    # ---- end to end through the C ABI with host buffers
+    world.restore()
+    host = torch.empty((scene.n, 13), dtype=torch.float32, pin_memory=True)
+    host_np = host.numpy().view(scenes.STATE_DTYPE).reshape(-1)
+    host_np[:] = world.states()
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        world.set_states(host_np)            # h2d: the step's input states
+        world.step(desc, stats=False)
+        host_np[:] = world.states()          # d2h: the step's result
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], device="cuda")
+    if world_size > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world_size * args.steps / float(te.item())
+    state_bytes = scene.n * 52
+
+    cpu = None
+    if rank == 0 and world_size == 1 and args.cpu_ticks > 0:
+        cv, cst = cpu_baseline(scene, desc, args.cpu_ticks)
+        cpu = {"value": cv, "unit": "steps/s", "cores": 1, "kind": "port",
+               "sample": f"{args.cpu_ticks} tick(s) of the same settled pile, same schedule; serial CPU "
+                         f"restatement (oracle/), {int(cst['iterations'])} sweeps"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world_size,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "box pile 64x32x32 (65,536 boxes + ground and walls), settled state, "
+                                   "legacy AVBD profile, residual-driven schedule, plain warm start",
+                       "bodies": scene.n, "tolerance": args.tolerance,
+                       "max_iterations": args.max_iterations,
+                       "iterations_mean": float(np.mean(iters)), "contacts_mean": float(np.mean(contacts)),
+                       "parallelism": f"replicas x{world_size}",
+                       "l2": "inputs larger than L2: per-tick working set ~%d MB (126 MB L2)" % int(
+                           (np.mean(contacts) * (8 + 9) * 16 + scene.n * 400 + 1.2e6 * 24) / 1e6)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "kernel": "k_solve", "launches": solve_launches,
+                         "kernel_ms_per_launch": solve_ms / max(1, solve_launches),
+                         "peak_source": peak_src},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
+                    "d2h_bytes_per_step": state_bytes},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    world.close()
+    if world_size > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

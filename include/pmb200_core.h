@@ -114,9 +114,13 @@ typedef struct pmb_step_desc {
     uint32_t max_iterations;
 } pmb_step_desc;
 
+/* residual: RMS, over contact normal rows that carry force or penetrate and
+ * hard joint rows, of the constraint violation after the last sweep (|C| for
+ * rows with force, C for rows active by penetration only), in metres;
+ * residual_max: the largest single row violation in the tick. */
 typedef struct pmb_step_stats {
     uint32_t candidate_pairs, active_pairs, contacts, colors, islands, iterations, impact, status;
-    float residual;
+    float residual, residual_max;
 } pmb_step_stats;
 
 typedef struct pmb_world pmb_world;
@@ -143,6 +147,18 @@ PMB_API int pmb_world_profile_step(pmb_world* world, const pmb_step_desc* step, 
  * returns the summed duration and launch count of the launches recorded since
  * the previous call, and sets the enable state. */
 PMB_API int pmb_world_solve_timer(pmb_world* world, int enable, float* total_ms, uint32_t* launches);
+
+/* Host mesh preparation used at world creation (no device work): triangles
+ * reordered into median-split BVH leaf order, one outward plane (n, d) per
+ * triangle when the mesh is a closed convex shell, bounds (lo, hi, centre,
+ * radius). Mirrors the reference's upload path
+ * (src/simulation/runtime_deformables.cu.inc:103-270). */
+PMB_API int pmb_prepare_mesh(const float* vertices, uint32_t vertex_count, const uint32_t* indices,
+                             uint32_t index_count, uint32_t* out_indices, float* out_planes, float* out_bounds,
+                             int* convex);
+
+/* Number of CUDA kernels this library has enqueued in this process. */
+PMB_API int pmb_kernel_launches(unsigned long long* count);
 
 /* Capture `steps` ticks into a CUDA graph (replayed by pmb_world_replay). */
 PMB_API int pmb_world_capture(pmb_world* world, const pmb_step_desc* step, uint32_t steps);

@@ -491,14 +491,12 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
                     }
                 }
             }
-            // Residual at the primal iterate; drives the adaptive schedule.
-            bool last = it + 1 == iters;
-            if (phase == 0) {
-                R res = contact_residual(w, bodies);
-                w.residual_trace.push_back(res);
-                if (adaptive && res <= R(o.residual_tolerance)) last = true;
-            }
-            // advance_duals (:492-616)
+            // advance_duals (:492-616). The reference's last-iteration block
+            // (impulses, sliding re-anchoring) runs after the loop from the
+            // final duals and stick flags, which is the same arithmetic.
+            w.res_sq = 0;
+            w.res_n = 0;
+            w.res_max = 0;
             for (uint32_t k = 0; k < P; ++k) {
                 uint32_t a = w.active_pairs[k] / n, b = w.active_pairs[k] % n;
                 if (phase != 0 && bodies[a].impact == 0 && bodies[b].impact == 0) continue;
@@ -518,26 +516,16 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
                     R ty = c.dual[2].lambda + c.dual[2].penalty * err[2];
                     R bound = friction * f.n;
                     bool stick = tx * tx + ty * ty <= bound * bound;
+                    bool active = false;
+                    R rv = contact_row_residual(err[0], f.n, active);
+                    if (active) w.residual_add(rv);
                     c.dual[0].lambda = f.n;
                     c.dual[1].lambda = f.t0;
                     c.dual[2].lambda = f.t1;
                     for (unsigned x = 0; x < 3; ++x)
                         if (x == 0 ? f.n > R(0) : stick)
                             c.dual[x].penalty = mn(K<R>::kmax, c.dual[x].penalty + beta * ab(err[x]));
-                    if (last) {
-                        V3<R> t0, t1;
-                        basis(c.normal, t0, t1);
-                        c.acc_n = f.n * dt;
-                        c.rep_n = c.acc_n;
-                        c.acc_f = mul(add(mul(t0, f.t0), mul(t1, f.t1)), dt);
-                        c.rep_f = c.acc_f;
-                        if (!stick) {
-                            State<R> pa = phase != 0 ? bodies[a].target : pose(bodies[a]);
-                            State<R> pb = phase != 0 ? bodies[b].target : pose(bodies[b]);
-                            c.anchor_a = inv_rotate(pa.q, sub(c.point, pa.x));
-                            c.anchor_b = inv_rotate(pb.q, sub(c.point, pb.x));
-                        }
-                    }
+                    c.stick = stick ? 1u : 0u;
                 }
             }
             for (auto& j : w.joints) {
@@ -547,7 +535,10 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
                 R impulse = 0;
                 if (phase == 0) {
                     scratch = Block<R>{};
+                    j.residual_sink = [](void* ctx, R v) { static_cast<World<R>*>(ctx)->residual_add(v); };
+                    j.residual_ctx = &w;
                     impulse = visit_joint(j, w, prev, bodies, dt, scratch, true, kAdvance);
+                    j.residual_sink = nullptr;
                 } else {
                     for (uint32_t r = 0; r < j.count; ++r) {
                         Row<R> row = j.rows[r];
@@ -563,8 +554,36 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
                     j.enabled = 0;
                 }
             }
-            if (phase == 0) used_iterations = it + 1;
+            bool last = it + 1 == iters;
+            if (phase == 0) {
+                R res = w.res_n ? R(std::sqrt(w.res_sq / double(w.res_n))) : R(0);
+                w.residual_trace.push_back(res);
+                w.residual_max_last = w.res_max;
+                if (adaptive && res <= R(o.residual_tolerance)) last = true;
+                used_iterations = it + 1;
+            }
             if (last) break;
+        }
+        // Last-iteration contact work (:533-561).
+        for (uint32_t k = 0; k < P; ++k) {
+            uint32_t a = w.active_pairs[k] / n, b = w.active_pairs[k] % n;
+            if (phase != 0 && bodies[a].impact == 0 && bodies[b].impact == 0) continue;
+            Manifold<R>& m = w.manifolds[k];
+            for (uint32_t p = 0; p < m.count; ++p) {
+                Contact<R>& c = m.c[p];
+                V3<R> t0, t1;
+                basis(c.normal, t0, t1);
+                c.acc_n = c.dual[0].lambda * dt;
+                c.rep_n = c.acc_n;
+                c.acc_f = mul(add(mul(t0, c.dual[1].lambda), mul(t1, c.dual[2].lambda)), dt);
+                c.rep_f = c.acc_f;
+                if (!c.stick) {
+                    State<R> pa = phase != 0 ? bodies[a].target : pose(bodies[a]);
+                    State<R> pb = phase != 0 ? bodies[b].target : pose(bodies[b]);
+                    c.anchor_a = inv_rotate(pa.q, sub(c.point, pa.x));
+                    c.anchor_b = inv_rotate(pb.q, sub(c.point, pb.x));
+                }
+            }
         }
         if (phase == 0 && adaptive) budget = used_iterations;
         // free_mean / free_subtract / free_clear (:617-698)
@@ -652,6 +671,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
     }
     st.iterations = used_iterations;
     st.residual = w.residual_trace.empty() ? 0.0f : float(w.residual_trace.back());
+    st.residual_max = float(w.residual_max_last);
 
     // ---- speed clamp (geometry.slang:3086-3100)
     for (uint32_t i = 0; i < n; ++i) {

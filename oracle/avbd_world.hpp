@@ -70,7 +70,7 @@ struct StepDesc {
 };
 struct StepStats {
     uint32_t candidate_pairs, active_pairs, contacts, colors, islands, iterations, impact, status;
-    float residual;
+    float residual, residual_max;
 };
 
 // ------------------------------------------------------------ world types
@@ -97,6 +97,7 @@ template <class R> struct Contact {
     Dual<R> dual[3];
     V3<R> error, anchor_a, anchor_b;
     uint32_t cached{};
+    uint32_t stick{};  // stick flag of the latest dual pass
 };
 template <class R> struct Manifold {
     Contact<R> c[8];
@@ -111,6 +112,9 @@ template <class R> struct JointRt {
     Row<R> rows[18];
     uint32_t count{};
     uint32_t next_a{kInvalid}, next_b{kInvalid};
+    // Residual sink for hard rows visited by an advance pass.
+    void (*residual_sink)(void*, R){};
+    void* residual_ctx{};
 };
 template <class R> struct AvbdBody {
     State<R> target;
@@ -242,6 +246,15 @@ template <class R> struct World {
     std::vector<V3<R>> aabb_lo, aabb_hi;
     std::vector<R> residual_trace;
     StepStats stats{};
+    // Residual of the current dual pass: squares, rows, largest violation.
+    double res_sq{};
+    uint64_t res_n{};
+    R res_max{}, residual_max_last{};
+    void residual_add(R v) {
+        res_sq += double(v) * double(v);
+        ++res_n;
+        res_max = v > res_max ? v : res_max;
+    }
 };
 
 template <class R> inline State<R> to_state(const StateDesc& s) {
@@ -616,6 +629,7 @@ inline void joint_row(JointRt<R>& j, std::vector<AvbdBody<R>>& bodies, Block<R>&
         }
     } else if (visit == kAdvance) {
         impulse += ab(row_force(row, A.dx, B.dx, dt)) * dt;
+        if (stiffness >= K<R>::kmax && j.residual_sink) j.residual_sink(j.residual_ctx, ab(row_error(row, A.dx, B.dx)));
         j.rows[ri] = row_advance(row, A.dx, B.dx);
     } else if (visit == kImpact) {
         if (stiffness < K<R>::kmax) {
@@ -769,27 +783,14 @@ template <class R> inline uint32_t find_root(std::vector<AvbdBody<R>>& bodies, u
     return i;
 }
 
-// Residual (added by this build, not in the reference): the largest remaining
-// normal-row violation max(0, C_n) over contact points and |C| over hard joint
-// rows, evaluated at the current displacements.
-template <class R> inline R contact_residual(const World<R>& w, const std::vector<AvbdBody<R>>& bodies) {
-    R r = 0;
-    for (size_t k = 0; k < w.active_pairs.size(); ++k) {
-        uint32_t a = w.active_pairs[k] / w.n, b = w.active_pairs[k] % w.n;
-        const Manifold<R>& m = w.manifolds[k];
-        for (uint32_t p = 0; p < m.count; ++p) {
-            Vec6<R> ja, jb;
-            R e = contact_normal_row(m.c[p], bodies[a], bodies[b], ja, jb);
-            r = mx(r, e);
-        }
-    }
-    for (auto& j : w.joints) {
-        if (j.count == 0 || !j.enabled) continue;
-        for (uint32_t k = 0; k < j.count; ++k)
-            if (j.rows[k].stiffness >= K<R>::kmax)
-                r = mx(r, ab(row_error(j.rows[k], bodies[j.dense_a].dx, bodies[j.dense_b].dx)));
-    }
-    return r;
+// Residual (added by this build, not in the reference): over contact normal
+// rows that carry force or penetrate, |C_n| where the force is positive and
+// C_n where only penetration makes the row active (a complementarity
+// violation in metres), plus |C| of hard joint rows; reported as the RMS
+// over those rows, with the largest single violation kept beside it.
+template <class R> inline R contact_row_residual(R err_n, R force_n, bool& active) {
+    active = force_n > R(0) || err_n > R(0);
+    return force_n > R(0) ? ab(err_n) : err_n;
 }
 
 }  // namespace oracle

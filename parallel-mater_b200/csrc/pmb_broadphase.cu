@@ -63,6 +63,7 @@ __global__ void k_body_constants(Dev d, const float4* mesh_lo, const float4* mes
 }
 void launch_body_constants(const Dev& d, const float4* lo, const float4* hi, const float4* sph, cudaStream_t s) {
     k_body_constants<<<blocks_for(d.n), kBlock, 0, s>>>(d, lo, hi, sph);
+    ++g_kernel_launches;
 }
 
 __global__ void k_integrate(Dev d, StepParams sp, float4* ox, float4* oq, float4* ov, float4* ow) {
@@ -128,6 +129,7 @@ __global__ void k_integrate(Dev d, StepParams sp, float4* ox, float4* oq, float4
 
 void launch_integrate(const Dev& d, const StepParams& sp, cudaStream_t s, const SolveBuffers& o) {
     k_integrate<<<blocks_for(d.n), kBlock, 0, s>>>(d, sp, o.ox, o.oq, o.ov, o.ow);
+    ++g_kernel_launches;
     prof_mark(s, "integrate+proxy");
 }
 
@@ -253,14 +255,19 @@ void launch_broadphase(const Dev& d, cudaStream_t s) {
     cudaMemsetAsync(d.bucket_count, 0, sizeof(uint32_t) * (d.grid_size + 1), s);
     cudaMemsetAsync(d.bucket_cursor, 0, sizeof(uint32_t) * d.grid_size, s);
     k_grid_count<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    ++g_kernel_launches;
     scan_u32(d.bucket_count, d.bucket_off, nullptr, d.grid_size, nullptr, d.scan_tmp32, s);
     k_grid_scatter<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    ++g_kernel_launches;
     prof_mark(s, "grid build");
     k_query_count<<<blocks_for(d.n, 128), 128, 0, s>>>(d);
+    ++g_kernel_launches;
     prof_mark(s, "query count");
     scan_u32(d.cand_count, d.cand_off, nullptr, d.n, &d.ctr->n_cand, d.scan_tmp32, s);
     k_query_write<<<blocks_for(d.n, 128), 128, 0, s>>>(d);
+    ++g_kernel_launches;
     k_clamp_count<<<1, 1, 0, s>>>(&d.ctr->n_cand, d.cap_cand);
+    ++g_kernel_launches;
     prof_mark(s, "query write");
 }
 

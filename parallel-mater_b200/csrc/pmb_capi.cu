@@ -21,6 +21,7 @@ struct Prof {
     std::vector<const char*> names;
 };
 static Prof g_prof;
+unsigned long long g_kernel_launches = 0;
 
 void prof_mark(cudaStream_t s, const char* stage) {
     if (!g_prof.on) return;
@@ -125,6 +126,7 @@ void enqueue_step(pmb_world* w, const StepParams& sp) {
     cudaStream_t s = w->stream;
     Dev& d = w->d;
     k_reset_counters<<<1, 256, 0, s>>>(d.ctr);
+    ++g_kernel_launches;
     launch_integrate(d, sp, s, w->out);
     launch_broadphase(d, s);
     launch_narrowphase(d, sp, s);
@@ -182,6 +184,7 @@ void fill_stats(const Counters& c, pmb_step_stats* s) {
     s->impact = c.impact;
     s->status = c.status;
     s->residual = c.residual;
+    s->residual_max = c.residual_max;
 }
 
 }  // namespace
@@ -497,6 +500,30 @@ int pmb_world_solve_timer(pmb_world* w, int enable, float* total_ms, uint32_t* l
     return r;
 }
 
+int pmb_prepare_mesh(const float* vertices, uint32_t vertex_count, const uint32_t* indices, uint32_t index_count,
+                     uint32_t* out_indices, float* out_planes, float* out_bounds, int* convex) {
+    if (!vertices || !indices || vertex_count == 0 || index_count % 3 || !out_indices || !out_planes || !out_bounds ||
+        !convex)
+        return PMB_ERROR_INVALID_ARGUMENT;
+    for (uint32_t k = 0; k < index_count; ++k)
+        if (indices[k] >= vertex_count) return PMB_ERROR_INVALID_ARGUMENT;
+    PreparedMesh pm = prepare_mesh(vertices, vertex_count, indices, index_count);
+    std::memcpy(out_indices, pm.indices.data(), 4 * size_t(index_count));
+    for (size_t t = 0; t < pm.planes.size(); ++t)
+        for (int k = 0; k < 4; ++k) out_planes[4 * t + k] = pm.planes[t][k];
+    const float b[10] = {pm.lo[0], pm.lo[1], pm.lo[2], pm.hi[0], pm.hi[1], pm.hi[2],
+                         pm.center[0], pm.center[1], pm.center[2], pm.radius};
+    std::memcpy(out_bounds, b, sizeof(b));
+    *convex = pm.convex ? 1 : 0;
+    return PMB_SUCCESS;
+}
+
+int pmb_kernel_launches(unsigned long long* count) {
+    if (!count) return PMB_ERROR_INVALID_ARGUMENT;
+    *count = g_kernel_launches;
+    return PMB_SUCCESS;
+}
+
 int pmb_world_capture(pmb_world* w, const pmb_step_desc* step, uint32_t steps) {
     if (!w || !step || steps == 0 || (steps & 1u)) return PMB_ERROR_INVALID_ARGUMENT;
     cudaSetDevice(w->device);
@@ -696,6 +723,7 @@ int pmb_math_eval(uint32_t kind, uint32_t count, const float* in, float* out) {
     }
     cudaMemcpy(din, in, 4 * size_t(count) * in_w[kind], cudaMemcpyHostToDevice);
     k_math_eval<<<(count + 127) / 128, 128>>>(kind, count, din, dout);
+    ++g_kernel_launches;
     cudaMemcpy(out, dout, 4 * size_t(count) * out_w[kind], cudaMemcpyDeviceToHost);
     int r = check(cudaGetLastError());
     cudaFree(din);

@@ -99,7 +99,9 @@ struct JointCtx {
     bool first;
     unsigned visit;
     float dt;
-    float residual;
+    double res_sq;
+    uint32_t res_n;
+    float res_max;
 };
 
 // geometry_constraints.slang:626-713
@@ -140,7 +142,12 @@ static __device__ void joint_row(JointCtx& c, const V6& ja, const V6& jb, float 
         }
     } else if (c.visit == kVisitAdvance) {
         c.impulse += fab(row_force(row, c.A->dx, c.B->dx, dt)) * dt;
-        if (stiffness >= kMaxPenalty) c.residual = fmx(c.residual, fab(row_error(row, c.A->dx, c.B->dx)));
+        if (stiffness >= kMaxPenalty) {
+            const float v = fab(row_error(row, c.A->dx, c.B->dx));
+            c.res_sq += double(v) * double(v);
+            c.res_n += 1;
+            c.res_max = fmx(c.res_max, v);
+        }
         store_row(c.rows[ri], row_advance(row, c.A->dx, c.B->dx));
     } else if (c.visit == kVisitImpact) {
         if (stiffness < kMaxPenalty) {
@@ -161,8 +168,9 @@ static __device__ void joint_row(JointCtx& c, const V6& ja, const V6& jb, float 
 // geometry_constraints.slang:715-926. prevA/prevB: start-of-tick poses.
 static __device__ float visit_joint(const Joint& o, JointRow* rows, const BodyView& A, const BodyView& B, V3 prev_xa,
                              Q4 prev_qa, V3 prev_xb, Q4 prev_qb, float4 pa0, float4 pb0, float dt, Blk* blk,
-                             bool first, unsigned visit, uint32_t* count_out, float* residual) {
-    JointCtx c{rows, &A, &B, blk, 0u, 0.0f, first, visit, dt, 0.0f};
+                             bool first, unsigned visit, uint32_t* count_out, double* res_sq = nullptr,
+                             uint32_t* res_n = nullptr, float* res_max = nullptr) {
+    JointCtx c{rows, &A, &B, blk, 0u, 0.0f, first, visit, dt, 0.0, 0u, 0.0f};
     V3 xa, xb;
     Q4 qa, qb;
     body_pose(A, xa, qa);
@@ -267,7 +275,9 @@ static __device__ float visit_joint(const Joint& o, JointRow* rows, const BodyVi
         }
     }
     if (count_out) *count_out = c.index;
-    if (residual) *residual = c.residual;
+    if (res_sq) *res_sq += c.res_sq;
+    if (res_n) *res_n += c.res_n;
+    if (res_max) *res_max = fmx(*res_max, c.res_max);
     return c.impulse;
 }
 

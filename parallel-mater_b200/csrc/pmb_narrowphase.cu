@@ -416,11 +416,14 @@ __global__ void k_cache_load(Dev d, StepParams sp) {
 
 void launch_narrowphase(const Dev& d, const StepParams& sp, cudaStream_t s) {
     k_narrow<<<blocks_for(d.cap_cand, 128), 128, 0, s>>>(d);
+    ++g_kernel_launches;
     prof_mark(s, "narrowphase");
     scan_u64(d.np_scan, d.np_scan, &d.ctr->n_cand, d.cap_cand, d.scan_tmp, s);
     k_compact<<<blocks_for(d.cap_cand), kBlock, 0, s>>>(d);
+    ++g_kernel_launches;
     prof_mark(s, "compact");
     k_cache_load<<<blocks_for(d.cap_pair, 128), 128, 0, s>>>(d, sp);
+    ++g_kernel_launches;
     prof_mark(s, "cache load");
 }
 

@@ -169,7 +169,7 @@ __global__ void k_prepare_joints(Dev d, StepParams sp) {
                 Blk scratch{};
                 uint32_t count = 0;
                 visit_joint(o, d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]), q4(d.q[b]),
-                            d.p0[a], d.p0[b], dt, &scratch, true, kVisitInit, &count, nullptr);
+                            d.p0[a], d.p0[b], dt, &scratch, true, kVisitInit, &count);
                 st.count = count;
             }
         }
@@ -402,8 +402,13 @@ __global__ void k_color_scatter(Dev d) {
 
 void launch_prepare(const Dev& d, const StepParams& sp, cudaStream_t s) {
     k_prepare_bodies<<<blocks_for(d.n), kBlock, 0, s>>>(d, sp);
+    ++g_kernel_launches;
     k_prepare_pairs<<<blocks_for(d.cap_pair, 128), 128, 0, s>>>(d, sp);
-    if (d.nj) k_prepare_joints<<<blocks_for(d.nj, 64), 64, 0, s>>>(d, sp);
+    ++g_kernel_launches;
+    if (d.nj) {
+        k_prepare_joints<<<blocks_for(d.nj, 64), 64, 0, s>>>(d, sp);
+        ++g_kernel_launches;
+    }
     launch_contact_jacobians(d, 0, s);
     prof_mark(s, "prepare");
 }
@@ -413,22 +418,33 @@ const void* color_kernel_ptr = reinterpret_cast<const void*>(&k_color);
 void launch_graph(const Dev& d, const StepParams& sp, cudaStream_t s, int coop_blocks) {
     uint32_t gb = blocks_for(d.cap_pair > d.nj ? d.cap_pair : d.nj);
     k_graph_degrees<<<gb, kBlock, 0, s>>>(d, sp);
+    ++g_kernel_launches;
     scan_u32(d.deg, d.inc_off, nullptr, d.n, nullptr, d.scan_tmp32, s);
     scan_u32(d.jdeg, d.jinc_off, nullptr, d.n, nullptr, d.scan_tmp32, s);
     k_graph_fill<<<gb, kBlock, 0, s>>>(d);
+    ++g_kernel_launches;
     k_graph_lists<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    ++g_kernel_launches;
     k_graph_roots<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    ++g_kernel_launches;
     scan_u32(d.rcount, d.roff, nullptr, d.n, nullptr, d.scan_tmp32, s);
     k_row_lists<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    ++g_kernel_launches;
     k_graph_impact<<<blocks_for(d.cap_pair), kBlock, 0, s>>>(d);
+    ++g_kernel_launches;
     k_graph_islands<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    ++g_kernel_launches;
     prof_mark(s, "graph lists+islands");
     void* args[] = {const_cast<Dev*>(&d)};
     cudaLaunchCooperativeKernel(color_kernel_ptr, dim3(coop_blocks), dim3(kBlock), args, 0, s);
+    ++g_kernel_launches;
     prof_mark(s, "colour fixpoint");
     k_color_count<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    ++g_kernel_launches;
     k_color_offsets<<<1, 32, 0, s>>>(d);
+    ++g_kernel_launches;
     k_color_scatter<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    ++g_kernel_launches;
     prof_mark(s, "colour buckets");
 }
 

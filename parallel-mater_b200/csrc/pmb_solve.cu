@@ -91,6 +91,7 @@ __global__ void k_contact_jacobians(Dev d, uint32_t phase) {
 }
 void launch_contact_jacobians(const Dev& d, uint32_t phase, cudaStream_t s) {
     k_contact_jacobians<<<blocks_for(d.cap_contact), kBlock, 0, s>>>(d, phase);
+    ++g_kernel_launches;
 }
 
 __device__ __forceinline__ void apply_pose_update(const Dev& d, uint32_t i, const V6& u) {
@@ -315,7 +316,7 @@ __device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float
                 if (phase == 0) {
                     BodyView A = load_body(d, a), B = load_body(d, b);
                     visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]),
-                                q4(d.q[b]), d.p0[a], d.p0[b], dt, &blk, first, kVisitAccumulate, nullptr, nullptr);
+                                q4(d.q[b]), d.p0[a], d.p0[b], dt, &blk, first, kVisitAccumulate, nullptr);
                 } else {
                     const Lite A = load_lite(d, a), B = load_lite(d, b);
                     for (uint32_t r = 0; r < js.count; ++r) {
@@ -385,13 +386,21 @@ __device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float
     }
 }
 
+// Residual accumulator of one dual pass (this build's addition): rows that
+// carry force or penetrate contribute |C_n| (force > 0) or C_n (penetration
+// only); hard joint rows contribute |C|. Reported as the RMS over those rows.
+struct Res {
+    double sq;
+    uint32_t n;
+    float mx;
+};
+
 // advance_duals for one contact point (geometry_constraints_solve.slang:
-// 494-532; the last-iteration block runs in k_contact_finalize). Returns
-// max(0, C_n) at the current displacements.
-__device__ float dual_contact(const Dev& d, uint32_t c, float dt, uint32_t phase) {
+// 494-532; the last-iteration block runs in k_contact_finalize).
+__device__ void dual_contact(const Dev& d, uint32_t c, float dt, uint32_t phase, Res& res) {
     const uint2 ab = d.c_bodies[c];
     const uint32_t a = ab.x, b = ab.y;
-    if (phase != 0 && d.impact[a] == 0 && d.impact[b] == 0) return 0.0f;
+    if (phase != 0 && d.impact[a] == 0 && d.impact[b] == 0) return;
     const Lite A = load_lite(d, a), B = load_lite(d, b);
     const float friction = sqrtf(d.p1[a].x * d.p1[b].x);
     const float beta = (1.0f / (fmx(d.p0[a].x + d.p0[b].x, 1.0e-6f) * dt * dt)) * 100.0f;
@@ -415,20 +424,26 @@ __device__ float dual_contact(const Dev& d, uint32_t c, float dt, uint32_t phase
     pen.w = stick ? 1.0f : 0.0f;
     d.c_lam[c] = lam;
     d.c_pen[c] = pen;
-    return fmx(0.0f, err[0]);
+    if (f.n > 0.0f || err[0] > 0.0f) {
+        const float v = f.n > 0.0f ? fab(err[0]) : err[0];
+        res.sq += double(v) * double(v);
+        res.n += 1;
+        res.mx = fmx(res.mx, v);
+    }
 }
 
-__device__ float dual_joint(const Dev& d, uint32_t j, uint32_t phase, float dt) {
+__device__ void dual_joint(const Dev& d, uint32_t j, uint32_t phase, float dt, Res& res) {
     JointState js = d.jstate[j];
-    if (js.count == 0 || !js.enabled) return 0.0f;
+    if (js.count == 0 || !js.enabled) return;
     const uint32_t a = js.dense_a, b = js.dense_b;
-    if (phase != 0 && d.impact[a] == 0 && d.impact[b] == 0) return 0.0f;
-    float impulse = 0.0f, res = 0.0f;
+    if (phase != 0 && d.impact[a] == 0 && d.impact[b] == 0) return;
+    float impulse = 0.0f;
     if (phase == 0) {
         BodyView A = load_body(d, a), B = load_body(d, b);
         Blk scratch;
         impulse = visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]),
-                              q4(d.q[b]), d.p0[a], d.p0[b], dt, &scratch, true, kVisitAdvance, nullptr, &res);
+                              q4(d.q[b]), d.p0[a], d.p0[b], dt, &scratch, true, kVisitAdvance, nullptr, &res.sq,
+                              &res.n, &res.mx);
     } else {
         const Lite A = load_lite(d, a), B = load_lite(d, b);
         for (uint32_t r = 0; r < js.count; ++r) {
@@ -445,7 +460,6 @@ __device__ float dual_joint(const Dev& d, uint32_t j, uint32_t phase, float dt) 
         js.enabled = 0;
     }
     d.jstate[j] = js;
-    return res;
 }
 
 __device__ __forceinline__ void atomic_max_pos(float* addr, float v) {
@@ -468,9 +482,11 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev d, StepParams sp
     const bool adaptive = phase == 0 && sp.tolerance > 0.0f;
     const uint32_t iters = adaptive ? min(max(sp.max_iterations, 1u), kMaxIterations) : min(budget, kMaxIterations);
     const uint32_t n_con = c->n_contacts;
+    __shared__ double wsq[kSolveThreads / 32];
+    __shared__ uint32_t wn[kSolveThreads / 32];
+    __shared__ float wmx[kSolveThreads / 32];
     const uint32_t group = (blockIdx.x * kSolveThreads + threadIdx.x) / kGroup;
     const uint32_t groups = gridDim.x * kGroupsPerBlock;
-    __shared__ float block_res;
     const bool timing = sp.debug_timing && phase == 0;
     auto now = [] {
         unsigned long long t;
@@ -493,25 +509,57 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev d, StepParams sp
             if (!grid_sync(c)) return;
             if (timing && it == 0 && col < 18 && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_release[col] = now();
         }
-        if (threadIdx.x == 0) block_res = 0.0f;
+        Res res{0.0, 0u, 0.0f};
+        for (uint32_t k = grid_stride_begin(); k < n_con; k += grid_stride()) dual_contact(d, k, dt, phase, res);
+        for (uint32_t j = grid_stride_begin(); j < d.nj; j += grid_stride()) dual_joint(d, j, phase, dt, res);
+        // Deterministic reduction: warp tree, warps in order, blocks in order.
+        for (int o = 16; o > 0; o >>= 1) {
+            res.sq += __shfl_xor_sync(0xffffffffu, res.sq, o);
+            res.n += __shfl_xor_sync(0xffffffffu, res.n, o);
+            res.mx = fmx(res.mx, __shfl_xor_sync(0xffffffffu, res.mx, o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            wsq[threadIdx.x >> 5] = res.sq;
+            wn[threadIdx.x >> 5] = res.n;
+            wmx[threadIdx.x >> 5] = res.mx;
+        }
         __syncthreads();
-        float res = 0.0f;
-        for (uint32_t k = grid_stride_begin(); k < n_con; k += grid_stride()) res = fmx(res, dual_contact(d, k, dt, phase));
-        for (uint32_t j = grid_stride_begin(); j < d.nj; j += grid_stride()) res = fmx(res, dual_joint(d, j, phase, dt));
-        for (int o = 16; o > 0; o >>= 1) res = fmx(res, __shfl_xor_sync(0xffffffffu, res, o));
-        if ((threadIdx.x & 31) == 0) atomic_max_pos(&block_res, res);
-        __syncthreads();
-        if (threadIdx.x == 0 && phase == 0) atomic_max_pos(&c->residual_trace[it], block_res);
+        if (threadIdx.x == 0) {
+            double bs = 0.0;
+            uint32_t bn = 0;
+            float bm = 0.0f;
+            for (int k = 0; k < kSolveThreads / 32; ++k) {
+                bs += wsq[k];
+                bn += wn[k];
+                bm = fmx(bm, wmx[k]);
+            }
+            c->res_sum[blockIdx.x] = bs;
+            c->res_cnt[blockIdx.x] = bn;
+            c->res_mx[blockIdx.x] = bm;
+        }
         if (timing && it == 0 && threadIdx.x == 0) atomicMax(&c->dbg_work[19], now());
         if (!grid_sync(c)) return;
         if (timing && it == 0 && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_release[19] = now();
+        double tsq = 0.0;
+        uint32_t tn = 0;
+        float tmx = 0.0f;
+        for (uint32_t k = 0; k < gridDim.x; ++k) {
+            tsq += ((volatile double*)c->res_sum)[k];
+            tn += ((volatile uint32_t*)c->res_cnt)[k];
+            tmx = fmx(tmx, ((volatile float*)c->res_mx)[k]);
+        }
+        const float rms = tn ? float(sqrt(tsq / double(tn))) : 0.0f;
+        if (phase == 0 && grid_stride_begin() == 0) c->residual_trace[it] = rms;
         bool last = it + 1 == iters;
-        if (adaptive && ((volatile float*)c->residual_trace)[it] <= sp.tolerance) last = true;
+        if (adaptive && rms <= sp.tolerance) last = true;
+        // Every block has read the partials before the next pass rewrites them.
+        if (!last && colors == 0 && !grid_sync(c)) return;
         if (last) {
             if (grid_stride_begin() == 0) {
                 if (phase == 0) {
                     c->iterations = it + 1;
-                    c->residual = ((volatile float*)c->residual_trace)[it];
+                    c->residual = rms;
+                    c->residual_max = tmx;
                 }
                 c->budget = it + 1;
             }
@@ -717,7 +765,7 @@ __global__ void k_impact_constraints(Dev d, StepParams sp, const float4* ov, con
         BodyView A = load_body(d, a), B = load_body(d, b);
         Blk scratch;
         visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]), q4(d.q[b]),
-                    d.p0[a], d.p0[b], dt, &scratch, true, kVisitImpact, nullptr, nullptr);
+                    d.p0[a], d.p0[b], dt, &scratch, true, kVisitImpact, nullptr);
     }
     const uint32_t n_act = d.ctr->n_act;
     for (uint32_t i = grid_stride_begin(); i < n_act; i += grid_stride()) {
@@ -794,9 +842,12 @@ void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, int co
     for (uint32_t phase = 0; phase < (sp.realtime ? 1u : 2u); ++phase) {
         if (phase != 0) {
             k_impact_setup<<<blocks_for(d.cap_pair), kBlock, 0, s>>>(d, sp, o.ox, o.oq, o.ov, o.ow);
+            ++g_kernel_launches;
             k_impact_bodies<<<blocks_for(d.n), kBlock, 0, s>>>(d, o.ox, o.oq, o.ov, o.ow);
+            ++g_kernel_launches;
             launch_contact_jacobians(d, 1, s);
             k_impact_constraints<<<pb, kBlock, 0, s>>>(d, sp, o.ov, o.ow);
+            ++g_kernel_launches;
             prof_mark(s, "impact setup");
         }
         Dev dd = d;
@@ -805,18 +856,29 @@ void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, int co
         void* args[] = {&dd, &spp, &ph};
         solve_timer_begin(s);
         cudaLaunchCooperativeKernel(solve_kernel_ptr, dim3(coop_blocks), dim3(kSolveThreads), args, solve_kernel_smem, s);
+        ++g_kernel_launches;
         solve_timer_end(s);
         prof_mark(s, phase ? "solve phase 1" : "solve phase 0");
         k_contact_finalize<<<blocks_for(d.cap_contact), kBlock, 0, s>>>(d, sp, phase);
+        ++g_kernel_launches;
         k_free_anchor<<<blocks_for(d.cap_pair > d.n ? d.cap_pair : d.n), kBlock, 0, s>>>(d, phase);
+        ++g_kernel_launches;
         k_free_mean<<<blocks_for(d.n), kBlock, 0, s>>>(d, phase);
+        ++g_kernel_launches;
         k_free_subtract<<<blocks_for(d.n), kBlock, 0, s>>>(d, phase);
+        ++g_kernel_launches;
         k_apply<<<blocks_for(d.n), kBlock, 0, s>>>(d, sp, phase, o.ox, o.oq, o.ov, o.ow);
-        if (phase == 0 && d.nj) k_project_hinges<<<1, 32, 0, s>>>(d, o.ox, o.oq);
+        ++g_kernel_launches;
+        if (phase == 0 && d.nj) {
+            k_project_hinges<<<1, 32, 0, s>>>(d, o.ox, o.oq);
+            ++g_kernel_launches;
+        }
         prof_mark(s, phase ? "finish phase 1" : "finish phase 0");
     }
     k_clamp_commit<<<blocks_for(d.n), kBlock, 0, s>>>(d, o.ox, o.oq, o.ov, o.ow);
+    ++g_kernel_launches;
     k_cache_save<<<blocks_for(d.cap_pair), kBlock, 0, s>>>(d, sp);
+    ++g_kernel_launches;
     prof_mark(s, "commit+cache save");
 }
 

@@ -45,6 +45,10 @@ struct Counters {
     uint32_t color_off[kMaxColors + 1];
     uint32_t color_cursor[kMaxColors];
     float residual_trace[kMaxIterations];
+    double res_sum[1024];  // per-block partial residual sums of the latest dual pass
+    uint32_t res_cnt[1024];
+    float res_mx[1024];
+    float residual_max;
     unsigned long long dbg_work[20], dbg_release[20], dbg_start;
     unsigned long long dbg_body[8];
     uint32_t dbg_rn;
@@ -221,6 +225,8 @@ int coop_blocks_for(const void* kernel, int threads, size_t smem);
 // Stage timing for diagnosis: records a CUDA event named `stage` when a
 // profiled step is being enqueued (never during graph capture).
 void prof_mark(cudaStream_t s, const char* stage);
+// Kernels enqueued by this library since the last reset (all stages).
+extern unsigned long long g_kernel_launches;
 // Dominant-kernel timing: brackets each solve launch with CUDA events when on.
 void solve_timer_begin(cudaStream_t s);
 void solve_timer_end(cudaStream_t s);

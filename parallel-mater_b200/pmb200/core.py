@@ -58,7 +58,8 @@ def lib():
             "pmb_world_set_stream": [vp, vp], "pmb_world_step": [vp, vp, vp],
             "pmb_world_capture": [vp, vp, u32], "pmb_world_replay": [vp],
             "pmb_world_profile_step": [vp, vp, vp, u32],
-            "pmb_world_solve_timer": [vp, i32, vp, vp],
+            "pmb_world_solve_timer": [vp, i32, vp, vp], "pmb_kernel_launches": [vp],
+            "pmb_prepare_mesh": [vp, u32, vp, u32, vp, vp, vp, vp],
             "pmb_world_get_states": [vp, vp], "pmb_world_set_states": [vp, vp],
             "pmb_world_last_stats": [vp, vp], "pmb_world_apply_impulse": [vp, u32, vp, vp],
             "pmb_world_candidate_pairs": [vp, vp, u32, vp],
@@ -203,6 +204,27 @@ class World:
         p = ctypes.c_void_p()
         _check(lib().pmb_world_device_states(self.h, ctypes.byref(p)), "device_states")
         return p.value
+
+
+def prepare_mesh(vertices, indices):
+    """Host mesh preparation of the library: (convex, indices, planes[T,4], bounds[10])."""
+    v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+    i = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+    out_i = np.zeros_like(i)
+    planes = np.zeros((len(i) // 3, 4), np.float32)
+    bounds = np.zeros(10, np.float32)
+    convex = ctypes.c_int()
+    _check(lib().pmb_prepare_mesh(v.ctypes.data, len(v), i.ctypes.data, len(i), out_i.ctypes.data,
+                                  planes.ctypes.data, bounds.ctypes.data, ctypes.byref(convex)),
+           "pmb_prepare_mesh")
+    return bool(convex.value), out_i, planes, bounds
+
+
+def kernel_launches() -> int:
+    """CUDA kernels enqueued by the library so far in this process."""
+    n = ctypes.c_ulonglong()
+    _check(lib().pmb_kernel_launches(ctypes.byref(n)), "pmb_kernel_launches")
+    return n.value
 
 
 _MATH_WIDTH = {0: (27, 7), 1: (7, 5), 2: (4, 6), 3: (42, 7)}

@@ -139,3 +139,17 @@ def test_snapshot_restore(gpu_available):
     for _ in range(3):
         w.step()
     assert np.array_equal(x1.view(np.uint8), w.states().view(np.uint8))
+
+
+def test_residual_schedule_matches_oracle(gpu_available):
+    """The residual-driven schedule stops at the same sweep, with the same
+    residual trace, on the GPU and the oracle."""
+    s = scenes.box_pile((6, 4, 6), seed=11, spacing=1.6)
+    w = core.World(s)
+    o = O.OracleWorld(s)
+    for f in range(40):
+        sg = w.step(residual_tolerance=2e-4, max_iterations=40)
+        so = o.step(residual_tolerance=2e-4, max_iterations=40)
+        assert sg["iterations"] == so["iterations"], f
+        np.testing.assert_allclose(w.residual_trace(), o.residual_trace(), rtol=1e-5, atol=1e-9)
+        assert abs(float(sg["residual_max"]) - float(so["residual_max"])) <= 1e-6 + 1e-5 * abs(float(so["residual_max"]))
