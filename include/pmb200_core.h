@@ -157,6 +157,25 @@ PMB_API int pmb_prepare_mesh(const float* vertices, uint32_t vertex_count, const
                              uint32_t index_count, uint32_t* out_indices, float* out_planes, float* out_bounds,
                              int* convex);
 
+/* First-fit colouring of a caller-supplied graph without allocating memory.
+ * No counterpart in the reference: it is this library's own entry point for
+ * callers that cannot call cudaMalloc -- a pm* driver working only in memory
+ * the application binds to it, or a real-time thread that must not stall on
+ * an allocation. All pointers are device pointers on `device`, owned by the
+ * caller: offsets[vertex_count + 1] and neighbors[] form an undirected
+ * adjacency (CSR), dynamic[v] != 0 marks vertices that take a colour; each
+ * dynamic vertex gets, in index order, the smallest colour absent among its
+ * lower-index dynamic neighbours (the tick's constraint-graph colouring);
+ * others get 0xffffffff. Enqueued on `stream` (cudaStream_t), then waited for.
+ * Working memory is a fixed array inside the library (one per GPU, held until
+ * the process exits) for at most 1,048,576 vertices; larger graphs return
+ * PMB_ERROR_CAPACITY_EXCEEDED, and so do graphs needing more than 256 colours.
+ * The first call on a device resolves that array's address, so make it before
+ * any stream capture. Calls share the array: calls that overlap on the GPU
+ * (other streams, other threads) race and must be serialised by the caller. */
+PMB_API int pmb_graph_color_noalloc(const uint32_t* offsets, const uint32_t* neighbors, const uint32_t* dynamic,
+                                    uint32_t vertex_count, uint32_t* colors, int32_t device, void* stream);
+
 /* Number of CUDA kernels this library has enqueued in this process. */
 PMB_API int pmb_kernel_launches(unsigned long long* count);
 
