@@ -100,7 +100,22 @@ typedef struct pmb_world_desc {
     uint32_t pair_capacity;      /* non-empty manifolds */
     uint32_t contact_capacity;   /* contact points */
     int32_t device;              /* CUDA ordinal */
+    /* Optional caller-owned device memory (both or neither, 256-byte
+     * aligned), sized by pmb_world_memory_requirements. When given, every
+     * device array of the world is carved from it and the world allocates no
+     * device memory; otherwise the world allocates its own. */
+    void* persistent_memory;
+    uint64_t persistent_bytes;
+    void* scratch_memory;
+    uint64_t scratch_bytes;
 } pmb_world_desc;
+
+/* Upper bounds for sizing caller-owned memory. Capacities of 0 select the
+ * defaults pmb_world_create would derive from body_count. */
+typedef struct pmb_world_capacity {
+    uint32_t body_count, joint_count, mesh_count, mesh_vertex_count, mesh_triangle_count;
+    uint32_t candidate_capacity, pair_capacity, contact_capacity;
+} pmb_world_capacity;
 
 /* profile: 1 = realtime v1 (8 sweeps, 5% damping), otherwise legacy
  * (requested_iterations, or base_iterations raised by joint iteration hints,
@@ -203,13 +218,76 @@ PMB_API int pmb_world_graph(pmb_world* world, uint32_t* colors, uint32_t* parent
 PMB_API int pmb_world_residual_trace(pmb_world* world, float* out, uint32_t capacity, uint32_t* count);
 
 /* Snapshot / restore of the complete dynamic state (states, contact cache,
- * warm-start history) into a second device buffer owned by the world. */
+ * warm-start history) into a second device buffer owned by the world.
+ * Worlds in caller-owned memory have none: PMB_ERROR_FEATURE_NOT_PRESENT. */
 PMB_API int pmb_world_snapshot(pmb_world* world);
 PMB_API int pmb_world_restore(pmb_world* world);
 
-/* Device pointer to the current states (pmb_state[body_count]) on the
- * world's device, for callers that keep inputs resident. */
-PMB_API int pmb_world_device_states(pmb_world* world, void** device_ptr);
+/* Bytes of persistent (state kept between ticks) and scratch (rebuilt by
+ * every tick) device memory a world within these bounds needs. The split
+ * follows the reference's PmSimulationMemoryRequirements
+ * (include/parallel_mater/parallel_mater.h:381-384). */
+PMB_API int pmb_world_memory_requirements(const pmb_world_capacity* capacity, uint64_t* persistent,
+                                          uint64_t* scratch);
+
+/* Per-body inputs for the next tick, which consumes and clears them
+ * (reference SimulationRuntime::apply_rigid_input,
+ * src/simulation/runtime_rigid.cu.inc:265-294, and pm_clear_rigid_inputs,
+ * src/slang/geometry.slang:2877-2886). values: 12 floats per body -- force,
+ * torque, linear impulse, angular impulse -- replacing the body's pending
+ * inputs; bodies must be distinct. Enqueued on the world's stream. */
+PMB_API int pmb_world_set_inputs(pmb_world* world, uint32_t count, const uint32_t* bodies, const float* values);
+
+/* Kinematic targets for the next tick (position and orientation of each
+ * record are used; reference set_kinematic_target, runtime_rigid.cu.inc:197-230).
+ * The predictor moves each kinematic body onto its target and derives its
+ * velocity from the motion. */
+PMB_API int pmb_world_set_targets(pmb_world* world, uint32_t count, const uint32_t* bodies,
+                                  const pmb_state* targets);
+
+/* Overwrite the states of bodies [first, first + count) (reference
+ * set_rigid_body_state, runtime_rigid.cu.inc:147-195): orientation
+ * normalised, velocity history, pending inputs and targets of those bodies
+ * cleared, rows of joints touching them restarted. */
+PMB_API int pmb_world_write_states(pmb_world* world, uint32_t first, uint32_t count, const pmb_state* states);
+
+/* Enqueue a copy of states [first, first + count) as pmb_state records into
+ * device memory `dst` (4-byte aligned) on the world's stream. */
+PMB_API int pmb_world_copy_states_to_device(pmb_world* world, uint32_t first, uint32_t count, void* dst);
+
+/* Joint state after the last tick (synchronous): flags bit 0 enabled, bit 1
+ * broken; applied impulse; number of solver rows. capacity >= joint_count. */
+PMB_API int pmb_world_joints(pmb_world* world, uint32_t* flags, float* applied, uint32_t* counts,
+                             uint32_t capacity);
+
+/* The CUDA stream (cudaStream_t) the world enqueues its work on. */
+PMB_API int pmb_world_stream(pmb_world* world, void** stream);
+
+/* ---- device services ----
+ * The pm* driver (libpm_b200_driver.so) reaches CUDA only through these, so
+ * that a single CUDA runtime serves the process. Pointers are CUDA device or
+ * managed pointers; streams and events are cudaStream_t / cudaEvent_t. */
+typedef struct pmb_device_info_t {
+    char name[256];
+    uint8_t uuid[16];
+    uint64_t total_memory;
+    uint32_t multiprocessors, compute_major, compute_minor, pci_device, driver_version;
+} pmb_device_info_t;
+PMB_API int pmb_device_count(int32_t* count);
+PMB_API int pmb_device_info(int32_t device, pmb_device_info_t* info);
+PMB_API int pmb_device_memory_info(int32_t device, uint64_t* free_bytes, uint64_t* total_bytes);
+/* host_visible != 0: managed memory (one pointer for host and device). */
+PMB_API int pmb_device_alloc(int32_t device, uint64_t bytes, int host_visible, void** out);
+PMB_API int pmb_device_free(int32_t device, void* ptr);
+PMB_API int pmb_stream_create(int32_t device, void** stream);
+PMB_API int pmb_stream_destroy(int32_t device, void* stream);
+PMB_API int pmb_stream_synchronize(int32_t device, void* stream);
+PMB_API int pmb_copy_async(int32_t device, void* dst, const void* src, uint64_t bytes, void* stream);
+PMB_API int pmb_event_create(int32_t device, void** event);
+PMB_API int pmb_event_destroy(int32_t device, void* event);
+PMB_API int pmb_event_record(int32_t device, void* event, void* stream);
+PMB_API int pmb_event_query(int32_t device, void* event, int* ready);
+PMB_API int pmb_event_elapsed_ms(int32_t device, void* start, void* end, float* ms);
 
 /* Core AVBD math on the device, one thread per record, for parity checks
  * against the CPU restatement. Host pointers; synchronous.

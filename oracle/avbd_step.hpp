@@ -706,7 +706,12 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
     w.saved.swap(saved);
     w.state = pred;
     w.epoch = epoch;
-    for (uint32_t i = 0; i < n; ++i) w.force[i] = w.torque[i] = w.impulse[i] = w.angular_impulse[i] = V3<R>{};
+    // pm_clear_rigid_inputs (geometry.slang:2877-2886): inputs and targets
+    // last one tick.
+    for (uint32_t i = 0; i < n; ++i) {
+        w.force[i] = w.torque[i] = w.impulse[i] = w.angular_impulse[i] = V3<R>{};
+        w.target_set[i] = 0;
+    }
     w.stats = st;
 }
 

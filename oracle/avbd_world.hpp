@@ -237,6 +237,9 @@ template <class R> struct World {
     std::vector<JointRt<R>> joints;
     std::vector<AvbdBody<R>> avbd;
     std::vector<V3<R>> force, torque, impulse, angular_impulse;
+    // Kinematic targets for the next tick (types.slang KinematicTarget).
+    std::vector<State<R>> target;
+    std::vector<uint8_t> target_set;
     std::vector<SavedPair<R>> saved;  // sorted by pair code
     uint64_t epoch{};
     // Last tick, for inspection by tests.
@@ -278,10 +281,28 @@ template <class R> inline V3<R> inv_inertia_world(const BodyDesc& b, Q4<R> q, V3
 template <class R> inline State<R> integrate(const World<R>& w, uint32_t i, V3<R> g, R dt) {
     const BodyDesc& b = w.body[i];
     State<R> prev = w.state[i], next = prev;
-    if (b.motion == kStatic || b.motion == kKinematic) {
-        // Kinematic targets are not driven by this restatement's inputs.
+    if (b.motion == kStatic) {
         next.v = {};
         next.w = {};
+        return next;
+    }
+    if (b.motion == kKinematic) {
+        // geometry.slang:545-581 with one remaining substep.
+        if (w.target_set[i]) {
+            const R fraction = R(1) / R(1);
+            const State<R>& t = w.target[i];
+            next.x = add(prev.x, mul(sub(t.x, prev.x), fraction));
+            Q4<R> tq = t.q;
+            const R od = prev.q.x * tq.x + prev.q.y * tq.y + prev.q.z * tq.z + prev.q.w * tq.w;
+            if (od < R(0)) tq = Q4<R>{-tq.x, -tq.y, -tq.z, -tq.w};
+            next.q = qnormalize(Q4<R>{prev.q.x + (tq.x - prev.q.x) * fraction, prev.q.y + (tq.y - prev.q.y) * fraction,
+                                      prev.q.z + (tq.z - prev.q.z) * fraction, prev.q.w + (tq.w - prev.q.w) * fraction});
+            next.v = mul(sub(next.x, prev.x), R(1) / dt);
+            next.w = delta_velocity(prev.q, next.q, dt);
+        } else {
+            next.v = {};
+            next.w = {};
+        }
         return next;
     }
     next.v = add(next.v, mul(add(g, mul(w.force[i], R(b.inv_mass))), dt));

@@ -40,6 +40,9 @@ def lib():
         L.oracle_get_states.argtypes = [vp, vp]
         L.oracle_set_states.argtypes = [vp, vp]
         L.oracle_apply_impulse.argtypes = [vp, u32, vp, vp]
+        L.oracle_set_inputs.argtypes = [vp, u32, vp, vp]
+        L.oracle_set_targets.argtypes = [vp, u32, vp, vp]
+        L.oracle_write_states.argtypes = [vp, u32, u32, vp]
         L.oracle_candidate_pairs.restype = u32
         L.oracle_candidate_pairs.argtypes = [vp, vp, u32]
         L.oracle_manifolds.restype = u32
@@ -115,6 +118,20 @@ class OracleWorld:
         lin = np.asarray(linear, np.float32)
         ang = np.asarray(angular, np.float32)
         lib().oracle_apply_impulse(self.h, body, lin.ctypes.data, ang.ctypes.data)
+
+    def set_inputs(self, bodies, values):
+        b = np.ascontiguousarray(bodies, np.uint32)
+        v = np.ascontiguousarray(values, np.float32).reshape(len(b), 12)
+        lib().oracle_set_inputs(self.h, len(b), b.ctypes.data, v.ctypes.data)
+
+    def set_targets(self, bodies, targets):
+        b = np.ascontiguousarray(bodies, np.uint32)
+        t = np.ascontiguousarray(targets)
+        lib().oracle_set_targets(self.h, len(b), b.ctypes.data, t.ctypes.data)
+
+    def write_states(self, first, states):
+        t = np.ascontiguousarray(states)
+        lib().oracle_write_states(self.h, first, len(t), t.ctypes.data)
 
     def candidate_pairs(self):
         n = lib().oracle_candidate_pairs(self.h, None, 0)

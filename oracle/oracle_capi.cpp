@@ -40,6 +40,8 @@ void build(World<R>& w, uint32_t n, const BodyDesc* bodies, const StateDesc* sta
     w.torque.assign(n, {});
     w.impulse.assign(n, {});
     w.angular_impulse.assign(n, {});
+    w.target.assign(n, State<R>{});
+    w.target_set.assign(n, 0);
     w.saved.clear();
     w.epoch = 0;
 }
@@ -102,6 +104,62 @@ void oracle_apply_impulse(void* hp, uint32_t body, const float* linear, const fl
         using R = std::decay_t<decltype(w.state[0].x.x)>;
         w.impulse[body] = add(w.impulse[body], v3<R>(linear));
         w.angular_impulse[body] = add(w.angular_impulse[body], v3<R>(angular));
+        return 0;
+    });
+}
+
+// Replace the pending inputs of the listed bodies (12 floats each: force,
+// torque, linear impulse, angular impulse). runtime_rigid.cu.inc:265-294
+// accumulates onto cleared accumulators; callers merge duplicates first.
+void oracle_set_inputs(void* hp, uint32_t count, const uint32_t* bodies, const float* values) {
+    with(static_cast<Handle*>(hp), [&](auto& w) {
+        using R = std::decay_t<decltype(w.state[0].x.x)>;
+        for (uint32_t k = 0; k < count; ++k) {
+            const float* v = values + 12 * size_t(k);
+            const uint32_t b = bodies[k];
+            w.force[b] = v3<R>(v);
+            w.torque[b] = v3<R>(v + 3);
+            w.impulse[b] = v3<R>(v + 6);
+            w.angular_impulse[b] = v3<R>(v + 9);
+        }
+        return 0;
+    });
+}
+
+// runtime_rigid.cu.inc:197-230: target orientation normalised.
+void oracle_set_targets(void* hp, uint32_t count, const uint32_t* bodies, const StateDesc* targets) {
+    with(static_cast<Handle*>(hp), [&](auto& w) {
+        using R = std::decay_t<decltype(w.state[0].x.x)>;
+        for (uint32_t k = 0; k < count; ++k) {
+            State<R> t = to_state<R>(targets[k]);
+            t.q = qnormalize(t.q);
+            w.target[bodies[k]] = t;
+            w.target_set[bodies[k]] = 1;
+        }
+        return 0;
+    });
+}
+
+// runtime_rigid.cu.inc:147-195: state replaced (orientation normalised),
+// AvbdBody, accumulators and target cleared, rows of joints on the body reset.
+void oracle_write_states(void* hp, uint32_t first, uint32_t count, const StateDesc* states) {
+    with(static_cast<Handle*>(hp), [&](auto& w) {
+        using R = std::decay_t<decltype(w.state[0].x.x)>;
+        for (uint32_t k = 0; k < count; ++k) {
+            const uint32_t b = first + k;
+            State<R> s = to_state<R>(states[k]);
+            s.q = qnormalize(s.q);
+            w.state[b] = s;
+            w.avbd[b] = AvbdBody<R>{};
+            w.force[b] = w.torque[b] = w.impulse[b] = w.angular_impulse[b] = V3<R>{};
+            w.target_set[b] = 0;
+        }
+        for (auto& j : w.joints) {
+            const bool touches = (j.d.body_a >= first && j.d.body_a - first < count) ||
+                                 (j.d.body_b >= first && j.d.body_b - first < count);
+            if (touches)
+                for (auto& row : j.rows) row = Row<R>{};
+        }
         return 0;
     });
 }

@@ -74,14 +74,34 @@ __global__ void k_integrate(Dev d, StepParams sp, float4* ox, float4* oq, float4
         float4 x = d.x[i], q = d.q[i], v = d.v[i], w = d.w[i];
         V3 nx = v3(x), nv = v3(v), nw = v3(w);
         Q4 nq = q4(q);
-        if (motion != kDynamic) {
+        if (motion == kKinematic) {
+            // Kinematic bodies follow a target set for this tick (one
+            // substep: the whole way), else stand still (geometry.slang:545-581).
+            const float4 tgt = d.tgt_x[i];
+            if (tgt.w != 0.0f) {
+                const float fraction = 1.0f;
+                nx = add(v3(x), mul(sub(v3(tgt), v3(x)), fraction));
+                Q4 t = q4(d.tgt_q[i]);
+                const Q4 p = q4(q);
+                const float od = p.x * t.x + p.y * t.y + p.z * t.z + p.w * t.w;
+                if (od < 0.0f) t = Q4{-t.x, -t.y, -t.z, -t.w};
+                nq = qnormalize(Q4{p.x + (t.x - p.x) * fraction, p.y + (t.y - p.y) * fraction,
+                                   p.z + (t.z - p.z) * fraction, p.w + (t.w - p.w) * fraction});
+                nv = mul(sub(nx, v3(x)), 1.0f / dt);
+                nw = delta_velocity(p, nq, dt);
+                d.tgt_x[i] = make_float4(0, 0, 0, 0);
+            } else {
+                nv = {0, 0, 0};
+                nw = {0, 0, 0};
+            }
+        } else if (motion != kDynamic) {
             nv = {0, 0, 0};
             nw = {0, 0, 0};
         } else {
             const float4 p0 = d.p0[i], p1 = d.p1[i], p2 = d.p2[i];
-            const V3 force{0, 0, 0};
+            const V3 force = v3(d.force[i]), torque = v3(d.torque[i]);
             nv = add(nv, mul(add(g, mul(force, p0.x)), dt));
-            nw = add(nw, mul(inv_inertia_world(p0, nq, V3{0, 0, 0}), dt));
+            nw = add(nw, mul(inv_inertia_world(p0, nq, torque), dt));
             nv = add(nv, mul(v3(d.lin_imp[i]), p0.x));
             nw = add(nw, inv_inertia_world(p0, nq, v3(d.ang_imp[i])));
             nv = mul(nv, 1.0f / (1.0f + p1.z * dt));
@@ -92,8 +112,8 @@ __global__ void k_integrate(Dev d, StepParams sp, float4* ox, float4* oq, float4
             Q4 dq = qmul(Q4{nw.x, nw.y, nw.z, 0.0f}, nq);
             nq = qnormalize(Q4{nq.x + 0.5f * dq.x * dt, nq.y + 0.5f * dq.y * dt, nq.z + 0.5f * dq.z * dt,
                                nq.w + 0.5f * dq.w * dt});
-            d.lin_imp[i] = make_float4(0, 0, 0, 0);
-            d.ang_imp[i] = make_float4(0, 0, 0, 0);
+            const float4 z = make_float4(0, 0, 0, 0);
+            d.force[i] = d.torque[i] = d.lin_imp[i] = d.ang_imp[i] = z;
         }
         // The predicted state is both the AVBD target and the initial solved
         // state (bodies the solve does not move keep it).
@@ -125,6 +145,64 @@ __global__ void k_integrate(Dev d, StepParams sp, float4* ox, float4* oq, float4
             atomicMax(reinterpret_cast<int*>(&d.ctr->hs), __float_as_int(m));
         }
     }
+}
+
+// Sparse record writes between ticks (host staging -> per-body arrays).
+// kind 0: force, torque, linear impulse, angular impulse (replaces the
+// body's pending inputs, src/simulation/runtime_rigid.cu.inc:265-294);
+// kind 1: kinematic target position + normalised orientation (:197-230);
+// kind 2: full state with normalised orientation, clearing the body's
+// velocity history, pending inputs and target (:147-195). All of them are
+// consumed and cleared by the next predictor, as pm_clear_rigid_inputs
+// (src/slang/geometry.slang:2877-2886) does at the end of the reference tick.
+__global__ void k_scatter_records(Dev d, uint32_t kind, uint32_t count) {
+    for (uint32_t k = grid_stride_begin(); k < count; k += grid_stride()) {
+        const uint32_t b = d.io_index[k];
+        if (b >= d.n) continue;
+        const float4* r = d.io_rec + 4 * size_t(k);
+        if (kind == 0) {
+            d.force[b] = r[0];
+            d.torque[b] = r[1];
+            d.lin_imp[b] = r[2];
+            d.ang_imp[b] = r[3];
+        } else if (kind == 1) {
+            d.tgt_x[b] = make_float4(r[0].x, r[0].y, r[0].z, 1.0f);
+            d.tgt_q[b] = f4(qnormalize(q4(r[1])));
+        } else {
+            d.x[b] = make_float4(r[0].x, r[0].y, r[0].z, 0.0f);
+            d.q[b] = f4(qnormalize(q4(r[1])));
+            d.v[b] = make_float4(r[2].x, r[2].y, r[2].z, 0.0f);
+            d.w[b] = make_float4(r[3].x, r[3].y, r[3].z, 0.0f);
+            d.prev_vel[b] = make_float4(0, 0, 0, 0);
+            const float4 z = make_float4(0, 0, 0, 0);
+            d.force[b] = d.torque[b] = d.lin_imp[b] = d.ang_imp[b] = z;
+            d.tgt_x[b] = z;
+        }
+    }
+}
+void launch_scatter_records(const Dev& d, uint32_t kind, uint32_t count, cudaStream_t s) {
+    if (count == 0) return;
+    k_scatter_records<<<blocks_for(count), kBlock, 0, s>>>(d, kind, count);
+    ++g_kernel_launches;
+}
+
+// States [first, first + count) as packed 13-float records (position,
+// orientation xyzw, linear and angular velocity) at dst.
+__global__ void k_pack_states(Dev d, uint32_t first, uint32_t count, float* dst) {
+    for (uint32_t k = grid_stride_begin(); k < count; k += grid_stride()) {
+        const uint32_t b = first + k;
+        const float4 x = d.x[b], q = d.q[b], v = d.v[b], w = d.w[b];
+        float* o = dst + 13 * size_t(k);
+        o[0] = x.x; o[1] = x.y; o[2] = x.z;
+        o[3] = q.x; o[4] = q.y; o[5] = q.z; o[6] = q.w;
+        o[7] = v.x; o[8] = v.y; o[9] = v.z;
+        o[10] = w.x; o[11] = w.y; o[12] = w.z;
+    }
+}
+void launch_pack_states(const Dev& d, uint32_t first, uint32_t count, float* dst, cudaStream_t s) {
+    if (count == 0) return;
+    k_pack_states<<<blocks_for(count), kBlock, 0, s>>>(d, first, count, dst);
+    ++g_kernel_launches;
 }
 
 void launch_integrate(const Dev& d, const StepParams& sp, cudaStream_t s, const SolveBuffers& o) {

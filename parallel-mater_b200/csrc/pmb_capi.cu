@@ -3,6 +3,7 @@
 // upload, the tick sequence, graph capture, inspection and snapshots.
 #include <algorithm>
 #include <cstdio>
+#include <cmath>
 #include <cstring>
 #include <new>
 #include <string>
@@ -70,6 +71,12 @@ struct pmb_world {
     SolveBuffers out{};
     std::vector<void*> allocs;
     std::vector<std::pair<void*, size_t>> dynamic_state;  // snapshot set
+    // Caller-bound memory (persistent, scratch): when set, every device array
+    // is carved from it and nothing is allocated. counting: only sum sizes.
+    char* arena[2]{};
+    size_t arena_size[2]{}, arena_used[2]{};
+    bool counting{};
+    std::vector<pmb_joint> host_joints;
     std::vector<void*> snapshot;
     int coop_solve{}, coop_color{};
     cudaGraphExec_t graph{};
@@ -79,17 +86,33 @@ struct pmb_world {
 
 namespace {
 
-template <class T> int alloc(pmb_world* w, T*& p, size_t count) {
+enum { kPersistent = 0, kScratch = 1 };
+constexpr size_t kArenaAlign = 256;
+
+template <class T> int alloc(pmb_world* w, T*& p, size_t count, int cls) {
     p = nullptr;
     if (count == 0) count = 1;
-    if (cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * count) != cudaSuccess) return PMB_ERROR_OUT_OF_DEVICE_MEMORY;
-    w->allocs.push_back(p);
-    cudaMemsetAsync(p, 0, sizeof(T) * count, w->stream);
+    const size_t bytes = sizeof(T) * count;
+    const size_t padded = (bytes + kArenaAlign - 1) & ~(kArenaAlign - 1);
+    if (w->counting) {
+        w->arena_used[cls] += padded;
+        return PMB_SUCCESS;
+    }
+    if (w->arena[cls]) {
+        if (w->arena_used[cls] + padded > w->arena_size[cls]) return PMB_ERROR_CAPACITY_EXCEEDED;
+        p = reinterpret_cast<T*>(w->arena[cls] + w->arena_used[cls]);
+        w->arena_used[cls] += padded;
+    } else {
+        if (cudaMalloc(reinterpret_cast<void**>(&p), bytes) != cudaSuccess) return PMB_ERROR_OUT_OF_DEVICE_MEMORY;
+        w->allocs.push_back(p);
+    }
+    cudaMemsetAsync(p, 0, bytes, w->stream);
     return PMB_SUCCESS;
 }
+// Persistent arrays that make up the dynamic state (snapshot set).
 template <class T> int alloc_state(pmb_world* w, T*& p, size_t count) {
-    int r = alloc(w, p, count);
-    if (r == PMB_SUCCESS) w->dynamic_state.push_back({p, sizeof(T) * (count ? count : 1)});
+    int r = alloc(w, p, count, kPersistent);
+    if (r == PMB_SUCCESS && !w->counting) w->dynamic_state.push_back({p, sizeof(T) * (count ? count : 1)});
     return r;
 }
 
@@ -187,6 +210,85 @@ void fill_stats(const Counters& c, pmb_step_stats* s) {
     s->residual_max = c.residual_max;
 }
 
+struct Sizes {
+    uint32_t n, nm, nj;
+    size_t verts, planes, dis;
+    uint32_t cap_cand, cap_pair, cap_contact;
+};
+struct Extra {
+    float4 *lo, *hi, *sph;  // mesh bounds, read once at creation
+    uint64_t* dis;
+};
+
+// The world's device layout. The same sequence runs in counting mode to size
+// caller-bound memory, so every array of a world comes from here.
+int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
+    const uint32_t n = z.n, nm = z.nm, nj = z.nj;
+    const uint32_t grid_size = next_pow2(std::max(2u * n, 1024u));
+    const size_t cap_cand = z.cap_cand, cap_pair = z.cap_pair, cap_contact = z.cap_contact;
+    int r = PMB_SUCCESS;
+#define ALLOCP(p, c) if (r == PMB_SUCCESS) r = alloc(w, p, c, kPersistent)
+#define ALLOC(p, c) if (r == PMB_SUCCESS) r = alloc(w, p, c, kScratch)
+#define ALLOCS(p, c) if (r == PMB_SUCCESS) r = alloc_state(w, p, c)
+    ALLOCP(d.motion, n); ALLOCP(d.mesh, n); ALLOCP(d.p0, n); ALLOCP(d.p1, n); ALLOCP(d.p2, n);
+    ALLOCP(d.expand, n); ALLOCP(d.rotb, n);
+    ALLOCS(d.x, n); ALLOCS(d.q, n); ALLOCS(d.v, n); ALLOCS(d.w, n);
+    ALLOC(d.tx, n); ALLOC(d.tq, n); ALLOC(d.tv, n); ALLOC(d.tw, n);
+    ALLOC(w->out.ox, n); ALLOC(w->out.oq, n); ALLOC(w->out.ov, n); ALLOC(w->out.ow, n);
+    ALLOCS(d.force, n); ALLOCS(d.torque, n); ALLOCS(d.lin_imp, n); ALLOCS(d.ang_imp, n);
+    ALLOCS(d.tgt_x, n); ALLOCS(d.tgt_q, n);
+    ALLOC(d.io_index, n); ALLOC(d.io_rec, 4 * size_t(n));
+    ALLOCP(d.m_vo, nm); ALLOCP(d.m_vc, nm); ALLOCP(d.m_to, nm); ALLOCP(d.m_tc, nm); ALLOCP(d.m_convex, nm);
+    ALLOCP(d.m_verts, z.verts); ALLOCP(d.m_planes, z.planes);
+    ALLOC(d.dxl, n); ALLOC(d.dxa, n); ALLOC(d.dq, n); ALLOC(d.inA, n); ALLOC(d.inB, n);
+    ALLOCS(d.prev_vel, n); ALLOCS(d.color, n);
+    ALLOC(d.parent, n); ALLOC(d.impact, n); ALLOC(d.anchored, n); ALLOC(d.mean, n);
+    ALLOC(d.lo, n); ALLOC(d.hi, n); ALLOC(d.is_large, n); ALLOC(d.large_list, n);
+    ALLOC(d.bucket_count, grid_size + 1); ALLOC(d.bucket_off, grid_size + 1); ALLOC(d.bucket_cursor, grid_size);
+    ALLOC(d.grid_body, n); ALLOC(d.grid_cell, n);
+    ALLOC(d.cand_count, n + 1); ALLOC(d.cand_off, n + 1);
+    ALLOC(d.cand_a, cap_cand); ALLOC(d.cand_b, cap_cand);
+    ALLOC(d.np_count, cap_cand); ALLOC(d.np_scan, cap_cand + 1); ALLOC(d.np_stage, cap_cand);
+    ALLOC(d.st_n, cap_contact); ALLOC(d.st_p, cap_contact);
+    ALLOC(d.act_a, cap_pair); ALLOC(d.act_b, cap_pair); ALLOC(d.act_code, cap_pair);
+    ALLOC(d.act_off, cap_pair + 1); ALLOC(d.act_cnt, cap_pair); ALLOC(d.act_impact, cap_pair);
+    ALLOC(d.c_pair, cap_contact); ALLOC(d.c_bodies, cap_contact); ALLOC(d.c_jac, 9 * cap_contact);
+    ALLOC(d.c_n, cap_contact); ALLOC(d.c_p, cap_contact); ALLOC(d.c_e, cap_contact);
+    ALLOC(d.c_aa, cap_contact); ALLOC(d.c_ab, cap_contact); ALLOC(d.c_lam, cap_contact);
+    ALLOC(d.c_pen, cap_contact); ALLOC(d.c_accf, cap_contact);
+    for (int side = 0; side < 2; ++side) {
+        uint32_t** code = side ? &d.out_code : &d.sv_code;
+        uint32_t** off = side ? &d.out_off : &d.sv_off;
+        uint32_t** cnt = side ? &d.out_cnt : &d.sv_cnt;
+        uint32_t** np = side ? &d.out_n_pairs : &d.sv_n_pairs;
+        float4** f[7] = {side ? &d.out_local : &d.sv_local, side ? &d.out_normal : &d.sv_normal,
+                         side ? &d.out_fimp : &d.sv_fimp, side ? &d.out_lam : &d.sv_lam,
+                         side ? &d.out_pen : &d.sv_pen, side ? &d.out_aa : &d.sv_aa, side ? &d.out_ab : &d.sv_ab};
+        float** dtp = side ? &d.out_dt : &d.sv_dt;
+        ALLOCS(*code, cap_pair); ALLOCS(*off, cap_pair); ALLOCS(*cnt, cap_pair); ALLOCS(*np, 1);
+        for (auto* p : f) ALLOCS(*p, cap_contact);
+        ALLOCS(*dtp, 1);
+    }
+    ALLOC(d.deg, n); ALLOC(d.inc_off, n + 1); ALLOC(d.inc_cursor, n); ALLOC(d.inc_list, 2 * cap_pair);
+    ALLOC(d.jdeg, n); ALLOC(d.jinc_off, n + 1); ALLOC(d.jinc_cursor, n); ALLOC(d.jinc_list, 2 * size_t(nj) + 2);
+    ALLOC(d.corder, n);
+    ALLOC(d.rcount, n); ALLOC(d.roff, n + 1); ALLOC(d.blist, 2 * cap_contact); ALLOC(d.bother, 2 * cap_contact);
+    ALLOCP(d.joints, nj); ALLOCS(d.jstate, nj); ALLOCS(d.jrows, size_t(nj) * 18);
+    {
+        // Scan scratch: one slot per 2048-element tile of the longest scan plus the total.
+        size_t longest = std::max<size_t>({cap_cand, grid_size, n, cap_pair});
+        size_t tiles = (longest + 2047) / 2048 + 2;
+        ALLOC(d.scan_tmp, tiles); ALLOC(d.scan_tmp32, tiles);
+    }
+    ALLOCP(d.ctr, 1);
+    ALLOC(e.lo, nm); ALLOC(e.hi, nm); ALLOC(e.sph, nm);
+    ALLOCP(e.dis, z.dis);
+#undef ALLOCP
+#undef ALLOC
+#undef ALLOCS
+    return r;
+}
+
 }  // namespace
 
 extern "C" {
@@ -201,10 +303,21 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     for (uint32_t i = 0; i < desc->body_count; ++i)
         if (desc->bodies[i].mesh >= desc->mesh_count || desc->bodies[i].motion > 2) return PMB_ERROR_INVALID_ARGUMENT;
     for (uint32_t j = 0; j < desc->joint_count; ++j)
-        if (desc->joints[j].type > 7) return PMB_ERROR_INVALID_ARGUMENT;
+        if (desc->joints[j].type > 7 || desc->joints[j].body_a >= desc->body_count ||
+            desc->joints[j].body_b >= desc->body_count)
+            return PMB_ERROR_INVALID_ARGUMENT;
+    if ((desc->persistent_memory == nullptr) != (desc->scratch_memory == nullptr) ||
+        (reinterpret_cast<uintptr_t>(desc->persistent_memory) % kArenaAlign) != 0 ||
+        (reinterpret_cast<uintptr_t>(desc->scratch_memory) % kArenaAlign) != 0)
+        return PMB_ERROR_INVALID_ARGUMENT;
     pmb_world* w = new (std::nothrow) pmb_world;
     if (!w) return PMB_ERROR_OUT_OF_DEVICE_MEMORY;
     w->device = desc->device;
+    w->arena[kPersistent] = static_cast<char*>(desc->persistent_memory);
+    w->arena_size[kPersistent] = size_t(desc->persistent_bytes);
+    w->arena[kScratch] = static_cast<char*>(desc->scratch_memory);
+    w->arena_size[kScratch] = size_t(desc->scratch_bytes);
+    if (desc->joint_count) w->host_joints.assign(desc->joints, desc->joints + desc->joint_count);
     cudaSetDevice(w->device);
     if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete w;
@@ -263,61 +376,6 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
         msph[m] = make_float4(pm.center[0], pm.center[1], pm.center[2], pm.radius);
     }
 
-    int r = PMB_SUCCESS;
-#define ALLOC(p, c) if (r == PMB_SUCCESS) r = alloc(w, p, c)
-#define ALLOCS(p, c) if (r == PMB_SUCCESS) r = alloc_state(w, p, c)
-    ALLOC(d.motion, n); ALLOC(d.mesh, n); ALLOC(d.p0, n); ALLOC(d.p1, n); ALLOC(d.p2, n);
-    ALLOC(d.expand, n); ALLOC(d.rotb, n);
-    ALLOCS(d.x, n); ALLOCS(d.q, n); ALLOCS(d.v, n); ALLOCS(d.w, n);
-    ALLOC(d.tx, n); ALLOC(d.tq, n); ALLOC(d.tv, n); ALLOC(d.tw, n);
-    ALLOC(w->out.ox, n); ALLOC(w->out.oq, n); ALLOC(w->out.ov, n); ALLOC(w->out.ow, n);
-    ALLOCS(d.lin_imp, n); ALLOCS(d.ang_imp, n);
-    ALLOC(d.m_vo, nm); ALLOC(d.m_vc, nm); ALLOC(d.m_to, nm); ALLOC(d.m_tc, nm); ALLOC(d.m_convex, nm);
-    ALLOC(d.m_verts, verts.size()); ALLOC(d.m_planes, planes.size());
-    ALLOC(d.dxl, n); ALLOC(d.dxa, n); ALLOC(d.dq, n); ALLOC(d.inA, n); ALLOC(d.inB, n);
-    ALLOCS(d.prev_vel, n); ALLOCS(d.color, n);
-    ALLOC(d.parent, n); ALLOC(d.impact, n); ALLOC(d.anchored, n); ALLOC(d.mean, n);
-    ALLOC(d.lo, n); ALLOC(d.hi, n); ALLOC(d.is_large, n); ALLOC(d.large_list, n);
-    ALLOC(d.bucket_count, d.grid_size + 1); ALLOC(d.bucket_off, d.grid_size + 1); ALLOC(d.bucket_cursor, d.grid_size);
-    ALLOC(d.grid_body, n); ALLOC(d.grid_cell, n);
-    ALLOC(d.cand_count, n + 1); ALLOC(d.cand_off, n + 1);
-    ALLOC(d.cand_a, d.cap_cand); ALLOC(d.cand_b, d.cap_cand);
-    ALLOC(d.np_count, d.cap_cand); ALLOC(d.np_scan, d.cap_cand + 1); ALLOC(d.np_stage, d.cap_cand);
-    ALLOC(d.st_n, d.cap_stage); ALLOC(d.st_p, d.cap_stage);
-    ALLOC(d.act_a, d.cap_pair); ALLOC(d.act_b, d.cap_pair); ALLOC(d.act_code, d.cap_pair);
-    ALLOC(d.act_off, d.cap_pair + 1); ALLOC(d.act_cnt, d.cap_pair); ALLOC(d.act_impact, d.cap_pair);
-    ALLOC(d.c_pair, d.cap_contact); ALLOC(d.c_bodies, d.cap_contact); ALLOC(d.c_jac, 9 * size_t(d.cap_contact));
-    ALLOC(d.c_n, d.cap_contact); ALLOC(d.c_p, d.cap_contact); ALLOC(d.c_e, d.cap_contact);
-    ALLOC(d.c_aa, d.cap_contact); ALLOC(d.c_ab, d.cap_contact); ALLOC(d.c_lam, d.cap_contact);
-    ALLOC(d.c_pen, d.cap_contact); ALLOC(d.c_accf, d.cap_contact);
-    for (int side = 0; side < 2; ++side) {
-        uint32_t** code = side ? &d.out_code : &d.sv_code;
-        uint32_t** off = side ? &d.out_off : &d.sv_off;
-        uint32_t** cnt = side ? &d.out_cnt : &d.sv_cnt;
-        uint32_t** np = side ? &d.out_n_pairs : &d.sv_n_pairs;
-        float4** f[7] = {side ? &d.out_local : &d.sv_local, side ? &d.out_normal : &d.sv_normal,
-                         side ? &d.out_fimp : &d.sv_fimp, side ? &d.out_lam : &d.sv_lam,
-                         side ? &d.out_pen : &d.sv_pen, side ? &d.out_aa : &d.sv_aa, side ? &d.out_ab : &d.sv_ab};
-        float** dtp = side ? &d.out_dt : &d.sv_dt;
-        ALLOCS(*code, d.cap_pair); ALLOCS(*off, d.cap_pair); ALLOCS(*cnt, d.cap_pair); ALLOCS(*np, 1);
-        for (auto* p : f) ALLOCS(*p, d.cap_contact);
-        ALLOCS(*dtp, 1);
-    }
-    ALLOC(d.deg, n); ALLOC(d.inc_off, n + 1); ALLOC(d.inc_cursor, n); ALLOC(d.inc_list, 2 * size_t(d.cap_pair));
-    ALLOC(d.jdeg, n); ALLOC(d.jinc_off, n + 1); ALLOC(d.jinc_cursor, n); ALLOC(d.jinc_list, 2 * size_t(nj) + 2);
-    ALLOC(d.corder, n);
-    ALLOC(d.rcount, n); ALLOC(d.roff, n + 1); ALLOC(d.blist, 2 * size_t(d.cap_contact)); ALLOC(d.bother, 2 * size_t(d.cap_contact));
-    ALLOC(d.joints, nj); ALLOCS(d.jstate, nj); ALLOCS(d.jrows, size_t(nj) * 18);
-    {
-        // Scan scratch: one slot per 2048-element tile of the longest scan plus the total.
-        size_t longest = std::max<size_t>({d.cap_cand, d.grid_size, n, d.cap_pair});
-        size_t tiles = (longest + 2047) / 2048 + 2;
-        ALLOC(d.scan_tmp, tiles); ALLOC(d.scan_tmp32, tiles);
-    }
-    ALLOC(d.ctr, 1);
-    float4 *dlo = nullptr, *dhi = nullptr, *dsph = nullptr;
-    ALLOC(dlo, nm); ALLOC(dhi, nm); ALLOC(dsph, nm);
-    uint64_t* dis = nullptr;
     std::vector<uint64_t> dis_keys;
     for (uint32_t j = 0; j < nj; ++j) {
         const pmb_joint& o = desc->joints[j];
@@ -328,11 +386,25 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     }
     std::sort(dis_keys.begin(), dis_keys.end());
     dis_keys.erase(std::unique(dis_keys.begin(), dis_keys.end()), dis_keys.end());
-    ALLOC(dis, dis_keys.size());
+    const Sizes z{n, nm, nj, verts.size(), planes.size(), dis_keys.size(), d.cap_cand, d.cap_pair, d.cap_contact};
+    if (w->arena[kPersistent]) {
+        // Bound memory must hold the whole layout before anything is carved.
+        pmb_world probe;
+        probe.counting = true;
+        Extra ex{};
+        allocate_world(&probe, probe.d, z, ex);
+        if (probe.arena_used[kPersistent] > w->arena_size[kPersistent] ||
+            probe.arena_used[kScratch] > w->arena_size[kScratch]) {
+            pmb_world_destroy(w);
+            return PMB_ERROR_CAPACITY_EXCEEDED;
+        }
+    }
+    Extra ex{};
+    int r = allocate_world(w, d, z, ex);
+    float4 *dlo = ex.lo, *dhi = ex.hi, *dsph = ex.sph;
+    uint64_t* dis = ex.dis;
     d.dis_keys = reinterpret_cast<uint32_t*>(dis);
     d.n_dis = uint32_t(dis_keys.size());
-#undef ALLOC
-#undef ALLOCS
     if (r != PMB_SUCCESS) {
         pmb_world_destroy(w);
         return r;
@@ -396,7 +468,10 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     cudaFuncSetAttribute(solve_kernel_ptr, cudaFuncAttributeMaxDynamicSharedMemorySize, int(solve_kernel_smem));
     w->coop_solve = coop_blocks_for(solve_kernel_ptr, solve_kernel_threads, solve_kernel_smem);
     w->coop_color = coop_blocks_for(color_kernel_ptr, kBlock, 0);
+    // A world in caller-bound memory allocates nothing, so it has no
+    // snapshot storage (pmb_world_snapshot reports FEATURE_NOT_PRESENT).
     for (auto& p : w->dynamic_state) {
+        if (w->arena[kPersistent]) break;
         void* snap = nullptr;
         if (cudaMalloc(&snap, p.second) != cudaSuccess) {
             pmb_world_destroy(w);
@@ -685,6 +760,7 @@ int pmb_world_residual_trace(pmb_world* w, float* out, uint32_t capacity, uint32
 
 int pmb_world_snapshot(pmb_world* w) {
     if (!w) return PMB_ERROR_INVALID_ARGUMENT;
+    if (w->snapshot.size() != w->dynamic_state.size()) return PMB_ERROR_FEATURE_NOT_PRESENT;
     cudaSetDevice(w->device);
     w->snapshot_parity = w->step_parity;
     for (size_t k = 0; k < w->dynamic_state.size(); ++k)
@@ -695,6 +771,7 @@ int pmb_world_snapshot(pmb_world* w) {
 
 int pmb_world_restore(pmb_world* w) {
     if (!w) return PMB_ERROR_INVALID_ARGUMENT;
+    if (w->snapshot.size() != w->dynamic_state.size()) return PMB_ERROR_FEATURE_NOT_PRESENT;
     cudaSetDevice(w->device);
     if (w->step_parity != w->snapshot_parity) swap_cache(w);
     for (size_t k = 0; k < w->dynamic_state.size(); ++k)
@@ -703,9 +780,137 @@ int pmb_world_restore(pmb_world* w) {
     return check(cudaStreamSynchronize(w->stream));
 }
 
-int pmb_world_device_states(pmb_world* w, void** device_ptr) {
-    if (!w || !device_ptr) return PMB_ERROR_INVALID_ARGUMENT;
-    *device_ptr = w->d.x;
+namespace {
+bool finite3(const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
+bool valid_quaternion(const float* q) {
+    if (!std::isfinite(q[0]) || !std::isfinite(q[1]) || !std::isfinite(q[2]) || !std::isfinite(q[3])) return false;
+    const float size = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+    return size > kEps * kEps;
+}
+// Stage sparse per-body records (4 float4 each) and scatter them on the
+// world's stream. Pageable sources are staged by the copy before it returns.
+int stage_records(pmb_world* w, uint32_t kind, uint32_t count, const uint32_t* bodies, const float4* recs) {
+    if (count == 0) return PMB_SUCCESS;
+    cudaSetDevice(w->device);
+    cudaMemcpyAsync(w->d.io_index, bodies, 4 * size_t(count), cudaMemcpyHostToDevice, w->stream);
+    cudaMemcpyAsync(w->d.io_rec, recs, 64 * size_t(count), cudaMemcpyHostToDevice, w->stream);
+    launch_scatter_records(w->d, kind, count, w->stream);
+    return check(cudaGetLastError());
+}
+bool unique_bodies(uint32_t n, uint32_t count, const uint32_t* bodies) {
+    std::vector<uint8_t> seen(n, 0);
+    for (uint32_t k = 0; k < count; ++k) {
+        if (bodies[k] >= n || seen[bodies[k]]) return false;
+        seen[bodies[k]] = 1;
+    }
+    return true;
+}
+}  // namespace
+
+int pmb_world_set_inputs(pmb_world* w, uint32_t count, const uint32_t* bodies, const float* values) {
+    if (!w || (count && (!bodies || !values)) || count > w->d.n || !unique_bodies(w->d.n, count, bodies))
+        return PMB_ERROR_INVALID_ARGUMENT;
+    std::vector<float4> rec(4 * size_t(count));
+    for (uint32_t k = 0; k < count; ++k) {
+        const float* v = values + 12 * size_t(k);
+        for (int f = 0; f < 4; ++f) {
+            if (!finite3(v + 3 * f)) return PMB_ERROR_INVALID_ARGUMENT;
+            rec[4 * k + f] = make_float4(v[3 * f], v[3 * f + 1], v[3 * f + 2], 0.0f);
+        }
+    }
+    return stage_records(w, 0, count, bodies, rec.data());
+}
+
+int pmb_world_set_targets(pmb_world* w, uint32_t count, const uint32_t* bodies, const pmb_state* targets) {
+    if (!w || (count && (!bodies || !targets)) || count > w->d.n || !unique_bodies(w->d.n, count, bodies))
+        return PMB_ERROR_INVALID_ARGUMENT;
+    std::vector<float4> rec(4 * size_t(count));
+    for (uint32_t k = 0; k < count; ++k) {
+        const pmb_state& t = targets[k];
+        if (!finite3(t.x) || !valid_quaternion(t.q) || !finite3(t.v) || !finite3(t.w))
+            return PMB_ERROR_INVALID_ARGUMENT;
+        rec[4 * k] = make_float4(t.x[0], t.x[1], t.x[2], 0.0f);
+        rec[4 * k + 1] = make_float4(t.q[0], t.q[1], t.q[2], t.q[3]);
+    }
+    return stage_records(w, 1, count, bodies, rec.data());
+}
+
+int pmb_world_write_states(pmb_world* w, uint32_t first, uint32_t count, const pmb_state* states) {
+    if (!w || (count && !states) || first > w->d.n || count > w->d.n - first) return PMB_ERROR_INVALID_ARGUMENT;
+    std::vector<uint32_t> idx(count);
+    std::vector<float4> rec(4 * size_t(count));
+    for (uint32_t k = 0; k < count; ++k) {
+        const pmb_state& t = states[k];
+        if (!finite3(t.x) || !valid_quaternion(t.q) || !finite3(t.v) || !finite3(t.w))
+            return PMB_ERROR_INVALID_ARGUMENT;
+        idx[k] = first + k;
+        rec[4 * k] = make_float4(t.x[0], t.x[1], t.x[2], 0.0f);
+        rec[4 * k + 1] = make_float4(t.q[0], t.q[1], t.q[2], t.q[3]);
+        rec[4 * k + 2] = make_float4(t.v[0], t.v[1], t.v[2], 0.0f);
+        rec[4 * k + 3] = make_float4(t.w[0], t.w[1], t.w[2], 0.0f);
+    }
+    int r = stage_records(w, 2, count, idx.data(), rec.data());
+    if (r != PMB_SUCCESS) return r;
+    // Joints touching a rewritten body restart their rows from zero.
+    for (uint32_t j = 0; j < uint32_t(w->host_joints.size()); ++j) {
+        const pmb_joint& o = w->host_joints[j];
+        const bool touches = (o.body_a >= first && o.body_a - first < count) ||
+                             (o.body_b >= first && o.body_b - first < count);
+        if (touches) cudaMemsetAsync(w->d.jrows + 18 * size_t(j), 0, 18 * sizeof(JointRow), w->stream);
+    }
+    return check(cudaGetLastError());
+}
+
+int pmb_world_copy_states_to_device(pmb_world* w, uint32_t first, uint32_t count, void* dst) {
+    if (!w || (count && !dst) || first > w->d.n || count > w->d.n - first ||
+        (reinterpret_cast<uintptr_t>(dst) & 3u))
+        return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    launch_pack_states(w->d, first, count, static_cast<float*>(dst), w->stream);
+    return check(cudaGetLastError());
+}
+
+int pmb_world_memory_requirements(const pmb_world_capacity* c, uint64_t* persistent, uint64_t* scratch) {
+    if (!c || !persistent || !scratch || c->body_count == 0) return PMB_ERROR_INVALID_ARGUMENT;
+    const uint32_t n = c->body_count;
+    pmb_world probe;
+    probe.counting = true;
+    const Sizes z{n,
+                  std::max(1u, c->mesh_count),
+                  c->joint_count,
+                  size_t(c->mesh_vertex_count),
+                  2 * size_t(c->mesh_triangle_count),
+                  size_t(c->joint_count),
+                  c->candidate_capacity ? c->candidate_capacity : 64u * n + 4096u,
+                  c->pair_capacity ? c->pair_capacity : 24u * n + 1024u,
+                  c->contact_capacity ? c->contact_capacity : 64u * n + 4096u};
+    Extra ex{};
+    allocate_world(&probe, probe.d, z, ex);
+    *persistent = probe.arena_used[kPersistent];
+    *scratch = probe.arena_used[kScratch];
+    return PMB_SUCCESS;
+}
+
+int pmb_world_joints(pmb_world* w, uint32_t* flags, float* applied, uint32_t* counts, uint32_t capacity) {
+    if (!w || capacity < w->d.nj) return PMB_ERROR_INVALID_ARGUMENT;
+    const uint32_t nj = w->d.nj;
+    if (nj == 0) return PMB_SUCCESS;
+    cudaSetDevice(w->device);
+    std::vector<JointState> js(nj);
+    cudaMemcpyAsync(js.data(), w->d.jstate, sizeof(JointState) * nj, cudaMemcpyDeviceToHost, w->stream);
+    int r = check(cudaStreamSynchronize(w->stream));
+    if (r != PMB_SUCCESS) return r;
+    for (uint32_t j = 0; j < nj; ++j) {
+        if (flags) flags[j] = js[j].enabled | (js[j].broken << 1);
+        if (applied) applied[j] = js[j].applied;
+        if (counts) counts[j] = js[j].count;
+    }
+    return PMB_SUCCESS;
+}
+
+int pmb_world_stream(pmb_world* w, void** stream) {
+    if (!w || !stream) return PMB_ERROR_INVALID_ARGUMENT;
+    *stream = w->stream;
     return PMB_SUCCESS;
 }
 

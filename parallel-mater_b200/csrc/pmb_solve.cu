@@ -723,7 +723,6 @@ __global__ void k_project_hinges(Dev d, float4* ox, const float4* oq) {
 __global__ void k_impact_setup(Dev d, StepParams sp, const float4* ox, const float4* oq, const float4* ov,
                                const float4* ow) {
     if (d.ctr->impact == 0) return;
-    const float dt = sp.dt;
     const uint32_t n_act = d.ctr->n_act;
     // impact_gaps (uses the phase-0 displacements)
     for (uint32_t i = grid_stride_begin(); i < n_act; i += grid_stride()) {

@@ -112,7 +112,12 @@ struct Dev {
     // state: current (start of tick) and target (predicted, then solved)
     float4 *x, *q, *v, *w;
     float4 *tx, *tq, *tv, *tw;
-    float4 *lin_imp, *ang_imp;
+    // per-tick inputs, cleared by the predictor that consumes them
+    float4 *force, *torque, *lin_imp, *ang_imp;
+    float4 *tgt_x, *tgt_q;  // kinematic target (w of tgt_x: 1 = set)
+    // host-to-device staging for sparse per-body records
+    uint32_t* io_index;
+    float4* io_rec;  // 4 per record
     // meshes
     uint32_t *m_vo, *m_vc, *m_to, *m_tc, *m_convex;
     float4* m_verts;
@@ -234,6 +239,10 @@ extern const void* solve_kernel_ptr;
 extern const int solve_kernel_threads;
 extern const size_t solve_kernel_smem;
 void launch_contact_jacobians(const Dev& d, uint32_t phase, cudaStream_t s);
+// Sparse per-body record writes staged in io_index / io_rec (kind 0: inputs,
+// 1: kinematic targets, 2: states), and AoS state packing into `dst`.
+void launch_scatter_records(const Dev& d, uint32_t kind, uint32_t count, cudaStream_t s);
+void launch_pack_states(const Dev& d, uint32_t first, uint32_t count, float* dst, cudaStream_t s);
 extern const void* color_kernel_ptr;
 
 inline uint32_t blocks_for(uint32_t n, int threads = kBlock) {

@@ -36,7 +36,15 @@ class WorldDesc(ctypes.Structure):
                 ("index_offsets", ctypes.c_void_p), ("indices", ctypes.c_void_p),
                 ("joint_count", ctypes.c_uint32), ("joints", ctypes.c_void_p),
                 ("candidate_capacity", ctypes.c_uint32), ("pair_capacity", ctypes.c_uint32),
-                ("contact_capacity", ctypes.c_uint32), ("device", ctypes.c_int32)]
+                ("contact_capacity", ctypes.c_uint32), ("device", ctypes.c_int32),
+                ("persistent_memory", ctypes.c_void_p), ("persistent_bytes", ctypes.c_uint64),
+                ("scratch_memory", ctypes.c_void_p), ("scratch_bytes", ctypes.c_uint64)]
+
+
+class WorldCapacity(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint32) for k in ("body_count", "joint_count", "mesh_count", "mesh_vertex_count",
+                                                "mesh_triangle_count", "candidate_capacity", "pair_capacity",
+                                                "contact_capacity")]
 
 
 _lib = None
@@ -66,7 +74,12 @@ def lib():
             "pmb_world_manifolds": [vp, vp, vp, vp, u32, vp],
             "pmb_world_graph": [vp, vp, vp], "pmb_world_residual_trace": [vp, vp, u32, vp],
             "pmb_world_snapshot": [vp], "pmb_world_restore": [vp],
-            "pmb_world_device_states": [vp, vp], "pmb_math_eval": [u32, u32, vp, vp],
+            "pmb_math_eval": [u32, u32, vp, vp],
+            "pmb_world_memory_requirements": [vp, vp, vp],
+            "pmb_world_set_inputs": [vp, u32, vp, vp], "pmb_world_set_targets": [vp, u32, vp, vp],
+            "pmb_world_write_states": [vp, u32, u32, vp],
+            "pmb_world_copy_states_to_device": [vp, u32, u32, vp], "pmb_world_stream": [vp, vp],
+            "pmb_world_joints": [vp, vp, vp, vp, u32],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -74,6 +87,17 @@ def lib():
             f.restype = None if name == "pmb_world_destroy" else i32
         _lib = L
     return _lib
+
+
+def memory_requirements(body_count, joint_count=0, mesh_count=1, mesh_vertex_count=0, mesh_triangle_count=0,
+                        candidate_capacity=0, pair_capacity=0, contact_capacity=0):
+    """(persistent, scratch) bytes of caller-owned memory for a world within these bounds."""
+    c = WorldCapacity(body_count, joint_count, mesh_count, mesh_vertex_count, mesh_triangle_count,
+                      candidate_capacity, pair_capacity, contact_capacity)
+    p, s = ctypes.c_uint64(), ctypes.c_uint64()
+    _check(lib().pmb_world_memory_requirements(ctypes.byref(c), ctypes.byref(p), ctypes.byref(s)),
+           "pmb_world_memory_requirements")
+    return p.value, s.value
 
 
 def _check(rc, what):
@@ -200,10 +224,30 @@ class World:
     def restore(self):
         _check(lib().pmb_world_restore(self.h), "restore")
 
-    def device_states_ptr(self):
-        p = ctypes.c_void_p()
-        _check(lib().pmb_world_device_states(self.h, ctypes.byref(p)), "device_states")
-        return p.value
+    def joints(self):
+        j = len(self.scene.joints)
+        flags = np.zeros(max(j, 1), np.uint32)
+        applied = np.zeros(max(j, 1), np.float32)
+        counts = np.zeros(max(j, 1), np.uint32)
+        _check(lib().pmb_world_joints(self.h, flags.ctypes.data, applied.ctypes.data, counts.ctypes.data,
+                                      max(j, 1)), "pmb_world_joints")
+        return flags[:j], applied[:j], counts[:j]
+
+    def set_inputs(self, bodies, values):
+        """values: [k, 12] float32 (force, torque, linear, angular impulse)."""
+        b = np.ascontiguousarray(bodies, np.uint32)
+        v = np.ascontiguousarray(values, np.float32).reshape(len(b), 12)
+        _check(lib().pmb_world_set_inputs(self.h, len(b), _p(b), _p(v)), "pmb_world_set_inputs")
+
+    def set_targets(self, bodies, targets):
+        b = np.ascontiguousarray(bodies, np.uint32)
+        t = np.ascontiguousarray(targets, STATE_DTYPE)
+        _check(lib().pmb_world_set_targets(self.h, len(b), _p(b), _p(t)), "pmb_world_set_targets")
+
+    def write_states(self, first, states):
+        t = np.ascontiguousarray(states, STATE_DTYPE)
+        _check(lib().pmb_world_write_states(self.h, first, len(t), _p(t)), "pmb_world_write_states")
+
 
 
 def prepare_mesh(vertices, indices):

@@ -101,7 +101,7 @@ class _Builder:
 
     def body(self, mesh, motion, x, q=(0, 0, 0, 1), v=(0, 0, 0), w=(0, 0, 0), mass=1.0,
              inertia=(1, 1, 1), friction=0.5, restitution=0.0, margin=0.005,
-             max_speed=100.0) -> int:
+             max_speed=100.0, linear_damping=0.0, angular_damping=0.0) -> int:
         b = np.zeros((), BODY_DTYPE)
         b["motion"], b["mesh"] = motion, mesh
         if motion == DYNAMIC:
@@ -109,6 +109,7 @@ class _Builder:
             b["inv_inertia"] = np.float32(1.0) / np.asarray(inertia, np.float32)
         b["friction"], b["restitution"], b["margin"] = friction, restitution, margin
         b["max_linear_speed"] = b["max_angular_speed"] = max_speed
+        b["linear_damping"], b["angular_damping"] = linear_damping, angular_damping
         s = np.zeros((), STATE_DTYPE)
         s["x"], s["q"], s["v"], s["w"] = x, q, v, w
         self.bodies.append(b)
@@ -300,6 +301,20 @@ def chains(count=512, links=64, seed=3, radius=0.05, length=0.4, spacing=1.0,
                      inertia=box_inertia(end_mass, box_half), friction=0.5)
         b.joint(POINT, prev, box, prev_anchor, (0.0, box_half[1], 0.0))
     return b.build(f"chains{count}x{links}", iterations, profile)
+
+
+def cube_pair(profile=REALTIME) -> Scene:
+    """A static unit cube at y = -1 and a dynamic one at y = 2 (mass 1,
+    inertia 1/6, friction 0.5, damping 0.05, speed limits 100, margin 5 mm):
+    the scene the reference's command-API test steps
+    (tests/api/command_api_tests.cpp:338-456)."""
+    b = _Builder()
+    m = b.mesh(*box_mesh((0.5, 0.5, 0.5)))
+    common = dict(mass=1.0, inertia=(1.0 / 6.0,) * 3, friction=0.5, margin=0.005, max_speed=100.0,
+                  linear_damping=0.05, angular_damping=0.05)
+    b.body(m, STATIC, (0.0, -1.0, 0.0), **common)
+    b.body(m, DYNAMIC, (0.0, 2.0, 0.0), **common)
+    return b.build("cube pair", 10, profile)
 
 
 def config(index: int) -> Scene:
