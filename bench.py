@@ -37,7 +37,7 @@ METRIC = "steps/sec at 64k boxes to equal residual: learned warm-start vs plain 
 GRID = (64, 32, 32)
 SEED = 4
 SETTLED = os.path.join(ROOT, "tests", "golden", "settled_pile_64x32x32.npz")
-PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_solve_pile65k_traffic.json")
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "k_solve_pile65k.md")
 
 
 def parse():
@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--tolerance", type=float, default=1e-4)
     ap.add_argument("--max-iterations", type=int, default=64)
     ap.add_argument("--cpu-ticks", type=int, default=1, help="ticks timed by the CPU baseline leg")
+    ap.add_argument("--contact-capacity", type=int, default=0,
+                    help="contact-point capacity of the world (0: the library default, 64 per body)")
     return ap.parse_args()
 
 
@@ -162,7 +164,7 @@ def gpu_arm(args):
     scene = load_scene()
     n_dyn = int((scene.bodies["motion"] == scenes.DYNAMIC).sum())
     desc = scene.step_desc(residual_tolerance=args.tolerance, max_iterations=args.max_iterations)
-    world = core.World(scene, device=local)
+    world = core.World(scene, device=local, contact_capacity=args.contact_capacity)
     stream = torch.cuda.current_stream()
     world.set_stream(stream.cuda_stream)
 
@@ -214,10 +216,14 @@ def gpu_arm(args):
         peak, peak_src = float(peaks["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
         peak, peak_src = 6650.0, "fallback"
+    # DRAM bytes per k_solve launch from the committed ncu capture of this
+    # workload (dram__bytes_read.sum + dram__bytes_write.sum).
     traffic = None
     try:
-        with open(PROFILE_TRAFFIC) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch")
+        with open(PROFILE_SUMMARY) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    traffic = float(line.split(":")[1])
     except (OSError, ValueError):
         pass
 

@@ -242,7 +242,7 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     ALLOCP(d.m_verts, z.verts); ALLOCP(d.m_planes, z.planes);
     ALLOC(d.dxl, n); ALLOC(d.dxa, n); ALLOC(d.dq, n); ALLOC(d.inA, n); ALLOC(d.inB, n);
     ALLOCS(d.prev_vel, n); ALLOCS(d.color, n);
-    ALLOC(d.parent, n); ALLOC(d.impact, n); ALLOC(d.anchored, n); ALLOC(d.mean, n);
+    ALLOC(d.parent, n); ALLOC(d.impact, n); ALLOC(d.anchored, n); ALLOC(d.mean, n); ALLOC(d.island_end, n);
     ALLOC(d.lo, n); ALLOC(d.hi, n); ALLOC(d.is_large, n); ALLOC(d.large_list, n);
     ALLOC(d.bucket_count, grid_size + 1); ALLOC(d.bucket_off, grid_size + 1); ALLOC(d.bucket_cursor, grid_size);
     ALLOC(d.grid_body, n); ALLOC(d.grid_cell, n);

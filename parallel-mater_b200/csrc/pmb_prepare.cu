@@ -34,6 +34,7 @@ __global__ void k_prepare_bodies(Dev d, StepParams sp) {
         d.parent[i] = i;
         d.impact[i] = 0;
         d.anchored[i] = 0;
+        d.island_end[i] = 0;
         d.mean[i] = make_float4(0, 0, 0, 0);
         d.dq[i] = make_float4(0, 0, 0, 1);
         d.dxa[i] = make_float4(0, 0, 0, 0);
@@ -311,6 +312,7 @@ __global__ void k_graph_islands(Dev d) {
     for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
         if (d.motion[i] != kDynamic) continue;
         const uint32_t r = d.parent[i];
+        atomicMax(&d.island_end[r], i);
         if (r != i) d.impact[i] = d.impact[r];
         if (r == i && (d.deg[i] > 0 || d.jdeg[i] > 0)) atomicAdd(&d.ctr->islands, 1u);
     }

@@ -632,20 +632,42 @@ __global__ void k_free_anchor(Dev d, uint32_t phase) {
     }
 }
 
+// One warp per island root: the members, found 32 indices at a time between
+// the root (the island's lowest index) and the island's largest index, are
+// summed by every lane in ascending index order -- the reference's serial
+// root loop (geometry_constraints_solve.slang:617-698) without its scan over
+// all bodies.
 __global__ void k_free_mean(Dev d, uint32_t phase) {
-    for (uint32_t r = grid_stride_begin(); r < d.n; r += grid_stride()) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t r = warp; r < d.n; r += warps) {
         if (d.motion[r] != kDynamic || d.parent[r] != r) continue;
         if ((phase != 0 && d.impact[r] == 0) || (d.deg[r] == 0 && d.jdeg[r] == 0)) continue;
         if (d.anchored[r]) continue;
+        const uint32_t end = d.island_end[r];
         V3 weighted{0, 0, 0};
         float total = 0.0f;
-        for (uint32_t i = r; i < d.n; ++i) {
-            if (d.motion[i] != kDynamic || d.parent[i] != r) continue;
-            const float mass = 1.0f / fmx(d.p0[i].x, 1.0e-12f);
-            weighted = add(weighted, mul(v3(d.dxl[i]), mass));
-            total += mass;
+        for (uint32_t base = r; base <= end; base += 32u) {
+            const uint32_t i = base + lane;
+            const bool member = i <= end && d.motion[i] == kDynamic && d.parent[i] == r;
+            float mass = 0.0f;
+            float4 l = make_float4(0, 0, 0, 0);
+            if (member) {
+                mass = 1.0f / fmx(d.p0[i].x, 1.0e-12f);
+                l = d.dxl[i];
+            }
+            uint32_t mask = __ballot_sync(0xffffffffu, member);
+            while (mask) {
+                const int k = __ffs(mask) - 1;
+                mask &= mask - 1u;
+                const float mk = __shfl_sync(0xffffffffu, mass, k);
+                const V3 lk{__shfl_sync(0xffffffffu, l.x, k), __shfl_sync(0xffffffffu, l.y, k),
+                            __shfl_sync(0xffffffffu, l.z, k)};
+                weighted = add(weighted, mul(lk, mk));
+                total += mk;
+            }
         }
-        if (total > 0.0f) d.mean[r] = f4(mul(weighted, 1.0f / total));
+        if (lane == 0 && total > 0.0f) d.mean[r] = f4(mul(weighted, 1.0f / total));
     }
 }
 
@@ -862,7 +884,7 @@ void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, int co
         ++g_kernel_launches;
         k_free_anchor<<<blocks_for(d.cap_pair > d.n ? d.cap_pair : d.n), kBlock, 0, s>>>(d, phase);
         ++g_kernel_launches;
-        k_free_mean<<<blocks_for(d.n), kBlock, 0, s>>>(d, phase);
+        k_free_mean<<<std::min<uint32_t>(blocks_for(32u * d.n, 256), 148u * 8u), 256, 0, s>>>(d, phase);
         ++g_kernel_launches;
         k_free_subtract<<<blocks_for(d.n), kBlock, 0, s>>>(d, phase);
         ++g_kernel_launches;

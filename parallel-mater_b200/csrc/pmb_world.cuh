@@ -127,6 +127,7 @@ struct Dev {
     float4 *inA, *inB;  // inertia block: (m/dt2, h33, h43, h44), (h53, h54, h55, -)
     float4* prev_vel;   // xyz + history flag in w
     uint32_t *color, *parent, *impact, *anchored;
+    uint32_t* island_end;  // largest member index of each island (at its root)
     float4* mean;       // free-island mean displacement (roots)
     // broadphase
     float4 *lo, *hi;
