@@ -121,12 +121,17 @@ typedef struct pmb_world_capacity {
  * (requested_iterations, or base_iterations raised by joint iteration hints,
  * plus the velocity impact phase). residual_tolerance > 0 switches to the
  * residual-driven schedule: sweep until the residual is at or below the
- * tolerance, at most max_iterations sweeps. warm_start: 0 plain, 1 learned. */
+ * tolerance, at most max_iterations sweeps. warm_start selects where each
+ * contact's normal row (lambda, penalty) starts: 0 plain (the reference's
+ * cached-and-decayed warm start), 1 learned (the world's MLP predictor, when
+ * one is attached; plain otherwise), 2 the table set by
+ * pmb_world_set_warm_table. */
 typedef struct pmb_step_desc {
     float dt, gravity[3];
     uint32_t profile, requested_iterations, base_iterations;
     float residual_tolerance;
     uint32_t max_iterations;
+    uint32_t warm_start;
 } pmb_step_desc;
 
 /* residual: RMS, over contact normal rows that carry force or penetrate and
@@ -259,6 +264,54 @@ PMB_API int pmb_world_copy_states_to_device(pmb_world* world, uint32_t first, ui
  * broken; applied impulse; number of solver rows. capacity >= joint_count. */
 PMB_API int pmb_world_joints(pmb_world* world, uint32_t* flags, float* applied, uint32_t* counts,
                              uint32_t capacity);
+
+/* (lambda, penalty) of the first `rows` rows (1: normal; 3: normal and both
+ * friction rows) of every contact point after the last tick, in contact
+ * order, `rows` values per point (synchronous). Counts are returned even when
+ * the output pointers are null or the capacity is too small. */
+PMB_API int pmb_world_contact_duals(pmb_world* world, uint32_t rows, float* lambda, float* penalty,
+                                    uint32_t capacity, uint32_t* count);
+
+/* Per-contact start values for ticks run with warm_start = 2: row x of
+ * contact point c (in contact order) starts from (lambda[rows*c+x],
+ * penalty[rows*c+x]) for c < count and x < rows. A penalty <= 0 keeps the
+ * plain penalty; a negative normal lambda or a NaN friction lambda keeps the
+ * plain lambda. Copied to the device (synchronous). */
+PMB_API int pmb_world_set_warm_table(pmb_world* world, uint32_t rows, const float* lambda, const float* penalty,
+                                     uint32_t count);
+
+/* ---- learned warm start ----
+ * An 8 -> 64 -> 64 -> 2 MLP (BF16 tensor-core kernels, FP32 accumulation and
+ * FP32 master weights) predicting each contact's converged normal-row
+ * (lambda, penalty) from its features at the start of the tick. It has no
+ * counterpart in the reference: the reference's warm start is the cached,
+ * decayed dual (constraint_math.slang:30-37), which stays the default
+ * (warm_start = 0) and the fallback for non-finite predictions.
+ * Parameter vector (PMB_MLP_PARAMS floats, row-major): W1[64][16],
+ * W2[64][80], W3[16][80]; biases live in column 8 of W1 and column 64 of W2
+ * and W3 (constant-one inputs); rows 2..15 of W3 and padding columns are 0. */
+#define PMB_MLP_PARAMS 7424u
+
+/* Attach a predictor to a world (device buffers allocated once): params, or
+ * a deterministic initialisation from seed when params is null. Resets the
+ * optimiser. Not available for worlds in caller-owned memory. */
+PMB_API int pmb_world_mlp_attach(pmb_world* world, const float* params, uint32_t seed);
+/* Online training: when enabled, every tick ends with steps_per_tick Adam
+ * steps (learning_rate) on that tick's contacts, target = the converged
+ * normal-row (lambda, penalty), loss = mean squared error of the normalised
+ * pair. */
+PMB_API int pmb_world_mlp_train(pmb_world* world, int enable, float learning_rate, uint32_t steps_per_tick);
+/* Current master parameters and the last training step's loss (either
+ * pointer may be null; synchronous). */
+PMB_API int pmb_world_mlp_params(pmb_world* world, float* params, float* last_loss);
+/* One forward and backward pass over `rows` given rows (features: 8 per row,
+ * targets: 2 per row, weights: loss weight per row), host buffers; returns
+ * the outputs (2 per row), the gradient of the weighted squared-error loss
+ * with respect to every parameter, and the loss. For checking the device
+ * kernels against a CPU restatement. */
+PMB_API int pmb_mlp_forward_backward(int32_t device, uint32_t rows, const float* features, const float* targets,
+                                     const float* weights, const float* params, float* outputs, float* grads,
+                                     float* loss);
 
 /* The CUDA stream (cudaStream_t) the world enqueues its work on. */
 PMB_API int pmb_world_stream(pmb_world* world, void** stream);

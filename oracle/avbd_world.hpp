@@ -67,6 +67,7 @@ struct StepDesc {
     uint32_t base_iterations;
     float residual_tolerance;       // > 0: stop sweeping once the residual is below it
     uint32_t max_iterations;        // cap for the residual-driven loop
+    uint32_t warm_start;            // 0: plain (the only source the oracle models)
 };
 struct StepStats {
     uint32_t candidate_pairs, active_pairs, contacts, colors, islands, iterations, impact, status;

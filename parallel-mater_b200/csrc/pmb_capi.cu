@@ -12,6 +12,7 @@
 #include "../../include/pmb200_core.h"
 #include "pmb_joint.cuh"
 #include "pmb_mesh.hpp"
+#include "pmb_mlp.cuh"
 
 namespace pmb {
 __global__ void k_math_eval(uint32_t kind, uint32_t count, const float* in, float* out);
@@ -82,6 +83,17 @@ struct pmb_world {
     cudaGraphExec_t graph{};
     uint32_t step_parity{}, snapshot_parity{};
     Counters host_ctr{};
+    // Learned warm start (allocated by pmb_world_mlp_attach).
+    struct Mlp {
+        bool attached{}, train{};
+        float lr{1e-3f};
+        uint32_t steps_per_tick{1}, grid{};
+        uint64_t adam_t{};
+        float *params{}, *m{}, *v{}, *grad{}, *partial{};
+        uint8_t *img{}, *x{};
+        MlpMeta* meta{};
+        std::vector<void*> allocs;
+    } mlp;
 };
 
 namespace {
@@ -133,6 +145,7 @@ StepParams params_from(const pmb_step_desc& s) {
     p.budget_request = p.realtime ? 8u : (s.requested_iterations ? s.requested_iterations : s.base_iterations);
     p.tolerance = s.residual_tolerance;
     p.max_iterations = s.max_iterations;
+    p.warm_start = s.warm_start;
     return p;
 }
 
@@ -154,8 +167,30 @@ void enqueue_step(pmb_world* w, const StepParams& sp) {
     launch_broadphase(d, s);
     launch_narrowphase(d, sp, s);
     launch_prepare(d, sp, s);
+    auto& mlp = w->mlp;
+    const bool learned = mlp.attached && sp.warm_start == 1;
+    if (mlp.attached && (learned || mlp.train)) launch_mlp_features(d, sp, mlp.x, mlp.meta, s);
+    if (learned)
+        launch_mlp_tiles(false, mlp.x, mlp.meta, mlp.img, 0, 0, &d.ctr->n_contacts, d.c_lam, d.c_pen, nullptr,
+                         nullptr, &d.ctr->status, kStBarrierTimeout, mlp.grid, s);
+    prof_mark(s, "mlp features+inference");
     launch_graph(d, sp, s, w->coop_color);
     launch_solve_all(d, sp, s, w->coop_solve, w->out);
+    if (mlp.attached && mlp.train) {
+        // Online training on this tick's converged normal rows.
+        launch_mlp_targets(d, mlp.meta, s);
+        for (uint32_t k = 0; k < mlp.steps_per_tick; ++k) {
+            launch_mlp_tiles(true, mlp.x, mlp.meta, mlp.img, 0, 0, &d.ctr->n_contacts, nullptr, nullptr, nullptr,
+                             mlp.partial, &d.ctr->status, kStBarrierTimeout, mlp.grid, s);
+            ++mlp.adam_t;
+            const float b1 = 0.9f, b2 = 0.999f;
+            const float c1 = 1.0f - std::pow(b1, float(mlp.adam_t)), c2 = 1.0f - std::pow(b2, float(mlp.adam_t));
+            launch_mlp_reduce_adam(mlp.partial, mlp.grid, mlp.grad, mlp.params, mlp.m, mlp.v, mlp.lr, b1, b2, c1, c2,
+                                   1e-8f, s);
+            launch_mlp_images(mlp.params, mlp.img, s);
+        }
+        prof_mark(s, "mlp training");
+    }
     // The cache written this tick is read by the next one.
     std::swap(d.sv_code, d.out_code);
     std::swap(d.sv_off, d.out_off);
@@ -238,6 +273,7 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     ALLOCS(d.force, n); ALLOCS(d.torque, n); ALLOCS(d.lin_imp, n); ALLOCS(d.ang_imp, n);
     ALLOCS(d.tgt_x, n); ALLOCS(d.tgt_q, n);
     ALLOC(d.io_index, n); ALLOC(d.io_rec, 4 * size_t(n));
+    ALLOC(d.warm_table, 2 * cap_contact);
     ALLOCP(d.m_vo, nm); ALLOCP(d.m_vc, nm); ALLOCP(d.m_to, nm); ALLOCP(d.m_tc, nm); ALLOCP(d.m_convex, nm);
     ALLOCP(d.m_verts, z.verts); ALLOCP(d.m_planes, z.planes);
     ALLOC(d.dxl, n); ALLOC(d.dxa, n); ALLOC(d.dq, n); ALLOC(d.inA, n); ALLOC(d.inB, n);
@@ -289,6 +325,40 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     return r;
 }
 
+}  // namespace
+
+namespace {
+// Deterministic initial weights: He-uniform hidden layers from a counter-based
+// hash of (seed, index), small output layer, zero biases and padding.
+float init_uniform(uint32_t seed, uint32_t i) {
+    uint64_t z = (uint64_t(seed) << 32) ^ (uint64_t(i) * 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return float((z >> 40) * (1.0 / 16777216.0)) * 2.0f - 1.0f;
+}
+void init_params(uint32_t seed, std::vector<float>& p) {
+    p.assign(kMlpParams, 0.0f);
+    const float a1 = std::sqrt(6.0f / float(kMlpFeatures)), a2 = std::sqrt(6.0f / float(kMlpHidden)),
+                a3 = 0.1f * std::sqrt(6.0f / float(kMlpHidden));
+    for (uint32_t j = 0; j < kMlpHidden; ++j) {
+        for (uint32_t f = 0; f < kMlpFeatures; ++f)
+            p[kMlpW1 + j * kMlpIn + f] = a1 * init_uniform(seed, kMlpW1 + j * kMlpIn + f);
+        for (uint32_t k = 0; k < kMlpHidden; ++k)
+            p[kMlpW2 + j * kMlpHiddenK + k] = a2 * init_uniform(seed, kMlpW2 + j * kMlpHiddenK + k);
+    }
+    for (uint32_t o = 0; o < kMlpOut; ++o)
+        for (uint32_t k = 0; k < kMlpHidden; ++k)
+            p[kMlpW3 + o * kMlpHiddenK + k] = a3 * init_uniform(seed, kMlpW3 + o * kMlpHiddenK + k);
+}
+template <class T> int mlp_alloc(pmb_world* w, T*& p, size_t count) {
+    p = nullptr;
+    if (cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * std::max<size_t>(count, 1)) != cudaSuccess)
+        return PMB_ERROR_OUT_OF_DEVICE_MEMORY;
+    w->mlp.allocs.push_back(p);
+    cudaMemsetAsync(p, 0, sizeof(T) * std::max<size_t>(count, 1), w->stream);
+    return PMB_SUCCESS;
+}
 }  // namespace
 
 extern "C" {
@@ -490,6 +560,7 @@ void pmb_world_destroy(pmb_world* w) {
     if (w->graph) cudaGraphExecDestroy(w->graph);
     for (void* p : w->allocs) cudaFree(p);
     for (void* p : w->snapshot) cudaFree(p);
+    for (void* p : w->mlp.allocs) cudaFree(p);
     if (w->own_stream && w->stream) cudaStreamDestroy(w->stream);
     delete w;
 }
@@ -906,6 +977,166 @@ int pmb_world_joints(pmb_world* w, uint32_t* flags, float* applied, uint32_t* co
         if (counts) counts[j] = js[j].count;
     }
     return PMB_SUCCESS;
+}
+
+int pmb_world_contact_duals(pmb_world* w, uint32_t rows, float* lambda, float* penalty, uint32_t capacity,
+                            uint32_t* count) {
+    if (!w || rows < 1 || rows > 3) return PMB_ERROR_INVALID_ARGUMENT;
+    pmb_step_stats st;
+    int r = pmb_world_last_stats(w, &st);
+    if (r) return r;
+    const uint32_t nc = w->host_ctr.n_contacts;
+    if (count) *count = nc;
+    if (!lambda || !penalty || capacity < nc || nc == 0) return PMB_SUCCESS;
+    std::vector<float4> lam(nc), pen(nc);
+    cudaMemcpyAsync(lam.data(), w->d.c_lam, 16 * size_t(nc), cudaMemcpyDeviceToHost, w->stream);
+    cudaMemcpyAsync(pen.data(), w->d.c_pen, 16 * size_t(nc), cudaMemcpyDeviceToHost, w->stream);
+    r = check(cudaStreamSynchronize(w->stream));
+    if (r) return r;
+    for (uint32_t c = 0; c < nc; ++c) {
+        const float l[3] = {lam[c].x, lam[c].y, lam[c].z}, k[3] = {pen[c].x, pen[c].y, pen[c].z};
+        for (uint32_t x = 0; x < rows; ++x) {
+            lambda[rows * size_t(c) + x] = l[x];
+            penalty[rows * size_t(c) + x] = k[x];
+        }
+    }
+    return PMB_SUCCESS;
+}
+
+int pmb_world_set_warm_table(pmb_world* w, uint32_t rows, const float* lambda, const float* penalty,
+                             uint32_t count) {
+    if (!w || rows < 1 || rows > 3 || (count && (!lambda || !penalty)) || count > w->d.cap_contact)
+        return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    std::vector<float4> t(2 * size_t(count));
+    for (uint32_t c = 0; c < count; ++c) {
+        float l[3] = {-1.0f, std::nanf(""), std::nanf("")}, k[3] = {0.0f, 0.0f, 0.0f};
+        for (uint32_t x = 0; x < rows; ++x) {
+            l[x] = lambda[rows * size_t(c) + x];
+            k[x] = penalty[rows * size_t(c) + x];
+        }
+        t[2 * size_t(c)] = make_float4(l[0], l[1], l[2], 0.0f);
+        t[2 * size_t(c) + 1] = make_float4(k[0], k[1], k[2], 0.0f);
+    }
+    if (count) cudaMemcpyAsync(w->d.warm_table, t.data(), 32 * size_t(count), cudaMemcpyHostToDevice, w->stream);
+    w->d.warm_count = count;
+    w->d.warm_rows = rows;
+    return check(cudaStreamSynchronize(w->stream));
+}
+
+
+int pmb_world_mlp_attach(pmb_world* w, const float* params, uint32_t seed) {
+    if (!w) return PMB_ERROR_INVALID_ARGUMENT;
+    if (w->arena[kPersistent]) return PMB_ERROR_FEATURE_NOT_PRESENT;
+    cudaSetDevice(w->device);
+    auto& m = w->mlp;
+    if (!m.attached) {
+        if (mlp_configure_kernels() != 0) return PMB_ERROR_DEVICE_LOST;
+        const size_t tiles = (size_t(w->d.cap_contact) + kMlpTile - 1) / kMlpTile;
+        m.grid = mlp_grid(uint32_t(tiles));
+        int r = PMB_SUCCESS;
+        if (!r) r = mlp_alloc(w, m.params, kMlpParams);
+        if (!r) r = mlp_alloc(w, m.m, kMlpParams);
+        if (!r) r = mlp_alloc(w, m.v, kMlpParams);
+        if (!r) r = mlp_alloc(w, m.grad, kMlpParams + 1);
+        if (!r) r = mlp_alloc(w, m.partial, size_t(m.grid) * (kMlpParams + 1));
+        if (!r) r = mlp_alloc(w, m.img, kImgBytes);
+        if (!r) r = mlp_alloc(w, m.x, tiles * 4096);
+        if (!r) r = mlp_alloc(w, m.meta, tiles * kMlpTile);
+        if (r) return r;
+        m.attached = true;
+    }
+    std::vector<float> host;
+    if (params)
+        host.assign(params, params + kMlpParams);
+    else
+        init_params(seed, host);
+    cudaMemcpyAsync(m.params, host.data(), sizeof(float) * kMlpParams, cudaMemcpyHostToDevice, w->stream);
+    cudaMemsetAsync(m.m, 0, sizeof(float) * kMlpParams, w->stream);
+    cudaMemsetAsync(m.v, 0, sizeof(float) * kMlpParams, w->stream);
+    m.adam_t = 0;
+    launch_mlp_images(m.params, m.img, w->stream);
+    return check(cudaStreamSynchronize(w->stream));
+}
+
+int pmb_world_mlp_train(pmb_world* w, int enable, float learning_rate, uint32_t steps_per_tick) {
+    if (!w || !w->mlp.attached || !(learning_rate >= 0.0f) || steps_per_tick == 0) return PMB_ERROR_INVALID_ARGUMENT;
+    w->mlp.train = enable != 0;
+    w->mlp.lr = learning_rate;
+    w->mlp.steps_per_tick = steps_per_tick;
+    return PMB_SUCCESS;
+}
+
+int pmb_world_mlp_params(pmb_world* w, float* params, float* last_loss) {
+    if (!w || !w->mlp.attached) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    if (params)
+        cudaMemcpyAsync(params, w->mlp.params, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost, w->stream);
+    if (last_loss)
+        cudaMemcpyAsync(last_loss, w->mlp.grad + kMlpParams, sizeof(float), cudaMemcpyDeviceToHost, w->stream);
+    return check(cudaStreamSynchronize(w->stream));
+}
+
+int pmb_mlp_forward_backward(int32_t device, uint32_t rows, const float* features, const float* targets,
+                             const float* weights, const float* params, float* outputs, float* grads, float* loss) {
+    if (!features || !targets || !weights || !params || rows == 0) return PMB_ERROR_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return PMB_ERROR_NO_DEVICE;
+    if (device < 0 || device >= ndev) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(device);
+    if (mlp_configure_kernels() != 0) return PMB_ERROR_DEVICE_LOST;
+    const uint32_t tiles = (rows + kMlpTile - 1) / kMlpTile, grid = mlp_grid(tiles);
+    std::vector<void*> owned;
+    auto get = [&](size_t bytes) -> void* {
+        void* p = nullptr;
+        if (cudaMalloc(&p, std::max<size_t>(bytes, 16)) != cudaSuccess) return nullptr;
+        owned.push_back(p);
+        return p;
+    };
+    float* d_feat = static_cast<float*>(get(sizeof(float) * kMlpFeatures * rows));
+    float* d_y = static_cast<float*>(get(sizeof(float) * 2 * rows));
+    float* d_w = static_cast<float*>(get(sizeof(float) * rows));
+    float* d_p = static_cast<float*>(get(sizeof(float) * kMlpParams));
+    float* d_out = static_cast<float*>(get(sizeof(float) * 2 * rows));
+    float* d_grad = static_cast<float*>(get(sizeof(float) * (kMlpParams + 1)));
+    float* d_part = static_cast<float*>(get(sizeof(float) * grid * (kMlpParams + 1)));
+    uint8_t* d_img = static_cast<uint8_t*>(get(kImgBytes));
+    uint8_t* d_x = static_cast<uint8_t*>(get(size_t(tiles) * 4096));
+    MlpMeta* d_meta = static_cast<MlpMeta*>(get(sizeof(MlpMeta) * tiles * kMlpTile));
+    uint32_t* d_status = static_cast<uint32_t*>(get(sizeof(uint32_t)));
+    int r = PMB_SUCCESS;
+    for (void* p : owned)
+        if (!p) r = PMB_ERROR_OUT_OF_DEVICE_MEMORY;
+    if (owned.size() != 11) r = PMB_ERROR_OUT_OF_DEVICE_MEMORY;
+    uint32_t status = 0;
+    if (r == PMB_SUCCESS) {
+        cudaStream_t s = nullptr;
+        cudaMemcpy(d_feat, features, sizeof(float) * kMlpFeatures * rows, cudaMemcpyHostToDevice);
+        cudaMemcpy(d_y, targets, sizeof(float) * 2 * rows, cudaMemcpyHostToDevice);
+        cudaMemcpy(d_w, weights, sizeof(float) * rows, cudaMemcpyHostToDevice);
+        cudaMemcpy(d_p, params, sizeof(float) * kMlpParams, cudaMemcpyHostToDevice);
+        cudaMemset(d_status, 0, sizeof(uint32_t));
+        launch_mlp_images(d_p, d_img, s);
+        launch_mlp_pack_rows(d_feat, d_y, d_w, rows, d_x, d_meta, tiles, s);
+        launch_mlp_tiles(true, d_x, d_meta, d_img, rows, tiles, nullptr, nullptr, nullptr, d_out, d_part, d_status,
+                         1u, grid, s);
+        launch_mlp_reduce_adam(d_part, grid, d_grad, nullptr, nullptr, nullptr, 0.0f, 0.9f, 0.999f, 1.0f, 1.0f, 1e-8f,
+                               s);
+        r = check(cudaDeviceSynchronize());
+        if (r == PMB_SUCCESS) {
+            cudaMemcpy(&status, d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+            if (outputs) cudaMemcpy(outputs, d_out, sizeof(float) * 2 * rows, cudaMemcpyDeviceToHost);
+            std::vector<float> g(kMlpParams + 1);
+            cudaMemcpy(g.data(), d_grad, sizeof(float) * (kMlpParams + 1), cudaMemcpyDeviceToHost);
+            if (grads) std::memcpy(grads, g.data(), sizeof(float) * kMlpParams);
+            if (loss) *loss = g[kMlpParams];
+            r = check(cudaGetLastError());
+        }
+    }
+    for (void* p : owned)
+        if (p) cudaFree(p);
+    if (r == PMB_SUCCESS && status) r = PMB_ERROR_DEVICE_LOST;
+    return r;
 }
 
 int pmb_world_stream(pmb_world* w, void** stream) {

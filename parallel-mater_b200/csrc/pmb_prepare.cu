@@ -141,10 +141,22 @@ __global__ void k_prepare_pairs(Dev d, StepParams sp) {
                 du[0] = du[1] = du[2] = {0.0f, penalty};
             }
             for (int x = 0; x < 3; ++x) du[x] = warm_start(du[x], kMaxPenalty);
+            const float plain_lambda = du[0].lambda;
+            if (sp.warm_start == 2 && c < d.warm_count) {
+                // Per row: a negative lambda or a non-positive penalty keeps
+                // the plain value of that half (friction lambdas are signed;
+                // NaN keeps them).
+                const float4 tl = d.warm_table[2 * size_t(c)], tk = d.warm_table[2 * size_t(c) + 1];
+                const float tla[3] = {tl.x, tl.y, tl.z}, tka[3] = {tk.x, tk.y, tk.z};
+                for (uint32_t x = 0; x < d.warm_rows; ++x) {
+                    if (x == 0 ? tla[0] >= 0.0f : tla[x] == tla[x]) du[x].lambda = tla[x];
+                    if (tka[x] > 0.0f) du[x].penalty = tka[x];
+                }
+            }
             d.c_lam[c] = make_float4(du[0].lambda, du[1].lambda, du[2].lambda, lam.w);
             d.c_pen[c] = make_float4(du[0].penalty, du[1].penalty, du[2].penalty, 0.0f);
             const float impact_fraction = p4.w;
-            bool fresh = (!cached || du[0].lambda <= 1.0e-6f || (impact_fraction > 0.0f && impact_fraction < 1.0f)) &&
+            bool fresh = (!cached || plain_lambda <= 1.0e-6f || (impact_fraction > 0.0f && impact_fraction < 1.0f)) &&
                          speed < -0.1f && pen >= -1.0e-5f;
             float prev_pen = pen + speed * dt;
             impact = impact || fresh || prev_pen > skin + 1.0e-4f;

@@ -63,6 +63,7 @@ struct StepParams {
     float tolerance;
     uint32_t max_iterations;
     uint32_t debug_timing;  // record solve-kernel timestamps for iteration 0
+    uint32_t warm_start;    // 0 plain, 1 learned, 2 table
 };
 
 struct JointRow {  // constraint_math.slang AvbdRow, packed for the device
@@ -115,6 +116,9 @@ struct Dev {
     // per-tick inputs, cleared by the predictor that consumes them
     float4 *force, *torque, *lin_imp, *ang_imp;
     float4 *tgt_x, *tgt_q;  // kinematic target (w of tgt_x: 1 = set)
+    // warm-start table: per contact point, lambda (x, y, z rows) and penalty
+    float4* warm_table;  // 2 per contact: lambda, penalty
+    uint32_t warm_count, warm_rows;
     // host-to-device staging for sparse per-body records
     uint32_t* io_index;
     float4* io_rec;  // 4 per record
@@ -245,6 +249,21 @@ void launch_contact_jacobians(const Dev& d, uint32_t phase, cudaStream_t s);
 void launch_scatter_records(const Dev& d, uint32_t kind, uint32_t count, cudaStream_t s);
 void launch_pack_states(const Dev& d, uint32_t first, uint32_t count, float* dst, cudaStream_t s);
 extern const void* color_kernel_ptr;
+// Learned warm start (pmb_mlp.cu).
+struct MlpMeta;
+size_t mlp_smem_bytes();
+int mlp_configure_kernels();
+uint32_t mlp_grid(uint32_t tiles);
+void launch_mlp_images(const float* params, uint8_t* img, cudaStream_t s);
+void launch_mlp_features(const Dev& d, const StepParams& sp, uint8_t* x, MlpMeta* meta, cudaStream_t s);
+void launch_mlp_targets(const Dev& d, MlpMeta* meta, cudaStream_t s);
+void launch_mlp_pack_rows(const float* feat, const float* y, const float* w, uint32_t n, uint8_t* x, MlpMeta* meta,
+                          uint32_t tiles, cudaStream_t s);
+void launch_mlp_tiles(bool train, const uint8_t* x, const MlpMeta* meta, const uint8_t* img, uint32_t rows,
+                      uint32_t tiles, const uint32_t* rows_ptr, float4* lam, float4* pen, float* out, float* partial,
+                      uint32_t* status, uint32_t status_bit, uint32_t grid, cudaStream_t s);
+void launch_mlp_reduce_adam(const float* partial, uint32_t parts, float* grad, float* params, float* m, float* v,
+                            float lr, float b1, float b2, float c1, float c2, float eps, cudaStream_t s);
 
 inline uint32_t blocks_for(uint32_t n, int threads = kBlock) {
     uint32_t b = (n + threads - 1) / threads;

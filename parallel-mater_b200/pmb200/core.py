@@ -80,6 +80,11 @@ def lib():
             "pmb_world_write_states": [vp, u32, u32, vp],
             "pmb_world_copy_states_to_device": [vp, u32, u32, vp], "pmb_world_stream": [vp, vp],
             "pmb_world_joints": [vp, vp, vp, vp, u32],
+            "pmb_world_contact_duals": [vp, u32, vp, vp, u32, vp],
+            "pmb_world_mlp_attach": [vp, vp, u32], "pmb_world_mlp_train": [vp, i32, ctypes.c_float, u32],
+            "pmb_world_mlp_params": [vp, vp, vp],
+            "pmb_mlp_forward_backward": [i32, u32, vp, vp, vp, vp, vp, vp, vp],
+            "pmb_world_set_warm_table": [vp, u32, vp, vp, u32],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -98,6 +103,25 @@ def memory_requirements(body_count, joint_count=0, mesh_count=1, mesh_vertex_cou
     _check(lib().pmb_world_memory_requirements(ctypes.byref(c), ctypes.byref(p), ctypes.byref(s)),
            "pmb_world_memory_requirements")
     return p.value, s.value
+
+
+MLP_PARAMS = 7424
+
+
+def mlp_forward_backward(features, targets, weights, params, device=0):
+    """GPU forward + backward of the warm-start MLP over given rows:
+    (outputs [n,2], gradient [7424], loss)."""
+    f = np.ascontiguousarray(features, np.float32).reshape(-1, 8)
+    n = len(f)
+    y = np.ascontiguousarray(targets, np.float32).reshape(n, 2)
+    w = np.ascontiguousarray(weights, np.float32).reshape(n)
+    p = np.ascontiguousarray(params, np.float32).reshape(MLP_PARAMS)
+    out = np.zeros((n, 2), np.float32)
+    g = np.zeros(MLP_PARAMS, np.float32)
+    loss = ctypes.c_float()
+    _check(lib().pmb_mlp_forward_backward(device, n, _p(f), _p(y), _p(w), _p(p), _p(out), _p(g), ctypes.byref(loss)),
+           "pmb_mlp_forward_backward")
+    return out, g, loss.value
 
 
 def _check(rc, what):
@@ -232,6 +256,38 @@ class World:
         _check(lib().pmb_world_joints(self.h, flags.ctypes.data, applied.ctypes.data, counts.ctypes.data,
                                       max(j, 1)), "pmb_world_joints")
         return flags[:j], applied[:j], counts[:j]
+
+    def mlp_attach(self, params=None, seed=1):
+        p = None if params is None else np.ascontiguousarray(params, np.float32)
+        _check(lib().pmb_world_mlp_attach(self.h, _p(p), seed), "pmb_world_mlp_attach")
+
+    def mlp_train(self, enable=True, lr=1e-3, steps_per_tick=1):
+        _check(lib().pmb_world_mlp_train(self.h, 1 if enable else 0, lr, steps_per_tick), "pmb_world_mlp_train")
+
+    def mlp_params(self):
+        """(master parameters, last training loss)."""
+        p = np.zeros(MLP_PARAMS, np.float32)
+        loss = ctypes.c_float()
+        _check(lib().pmb_world_mlp_params(self.h, p.ctypes.data, ctypes.byref(loss)), "pmb_world_mlp_params")
+        return p, loss.value
+
+    def contact_duals(self, rows=1):
+        """(lambda, penalty) of the first `rows` rows of every contact point
+        after the last tick, shape [contacts, rows]."""
+        n = ctypes.c_uint32()
+        _check(lib().pmb_world_contact_duals(self.h, rows, None, None, 0, ctypes.byref(n)), "contact_duals")
+        lam = np.zeros((max(n.value, 1), rows), np.float32)
+        pen = np.zeros((max(n.value, 1), rows), np.float32)
+        _check(lib().pmb_world_contact_duals(self.h, rows, lam.ctypes.data, pen.ctypes.data, n.value,
+                                             ctypes.byref(n)), "contact_duals")
+        return lam[:n.value], pen[:n.value]
+
+    def set_warm_table(self, lam, pen):
+        lam = np.ascontiguousarray(lam, np.float32)
+        pen = np.ascontiguousarray(pen, np.float32)
+        rows = 1 if lam.ndim == 1 else lam.shape[1]
+        _check(lib().pmb_world_set_warm_table(self.h, rows, lam.ctypes.data, pen.ctypes.data, len(lam)),
+               "set_warm_table")
 
     def set_inputs(self, bodies, values):
         """values: [k, 12] float32 (force, torque, linear, angular impulse)."""

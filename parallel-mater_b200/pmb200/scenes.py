@@ -49,7 +49,8 @@ assert JOINT_DTYPE.itemsize == 220
 
 STEP_DTYPE = np.dtype([
     ("dt", "<f4"), ("gravity", "<f4", 3), ("profile", "<u4"), ("requested_iterations", "<u4"),
-    ("base_iterations", "<u4"), ("residual_tolerance", "<f4"), ("max_iterations", "<u4")])
+    ("base_iterations", "<u4"), ("residual_tolerance", "<f4"), ("max_iterations", "<u4"),
+    ("warm_start", "<u4")])
 
 STATS_DTYPE = np.dtype([
     ("candidate_pairs", "<u4"), ("active_pairs", "<u4"), ("contacts", "<u4"), ("colors", "<u4"),
@@ -78,7 +79,7 @@ class Scene:
         return len(self.bodies)
 
     def step_desc(self, *, dt=DT, profile=None, iterations=None, residual_tolerance=0.0,
-                  max_iterations=0) -> np.ndarray:
+                  max_iterations=0, warm_start=0) -> np.ndarray:
         s = np.zeros((), STEP_DTYPE)
         s["dt"] = dt
         s["gravity"] = (0.0, -9.81, 0.0)
@@ -87,6 +88,7 @@ class Scene:
         s["base_iterations"] = 10
         s["residual_tolerance"] = residual_tolerance
         s["max_iterations"] = max_iterations
+        s["warm_start"] = warm_start
         return s
 
 

@@ -1,0 +1,67 @@
+# SPDX-License-Identifier: MIT
+"""The warm-start MLP's tensor-core kernels against the CPU restatement.
+
+- Forward outputs and every parameter gradient of the BF16 tcgen05 kernels
+  (pmb_mlp_forward_backward) match oracle/mlp.py with BF16 rounding at the
+  same points. Accumulation order inside the tensor cores differs from the
+  oracle's float64 sums and ReLU masks can flip for pre-activations within
+  rounding of zero, so the comparison is norm-wise: relative error <= 1e-2
+  for the outputs and for each weight matrix's gradient.
+- Batches that are not a multiple of the 128-row tile and batches spanning
+  several tiles per CTA accumulate correctly.
+- Online training inside the tick lowers the loss, and ticks run with the
+  learned warm start reach the residual tolerance like plain ticks.
+"""
+import numpy as np
+import pytest
+
+import mlp as M
+from pmb200 import core, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize("n", [128, 1000, 40000])
+def test_forward_backward_matches_oracle(gpu_available, n):
+    rng = np.random.default_rng(n)
+    f = rng.uniform(-1.0, 1.0, (n, M.FEATURES)).astype(np.float32)
+    y = rng.uniform(-0.5, 1.5, (n, 2)).astype(np.float32)
+    w = np.full(n, 1.0 / n, np.float32)
+    p = M.init_params(n % 97)
+    out, g, loss = core.mlp_forward_backward(f, y, w, p)
+    o_ref, g_ref, loss_ref = M.forward_backward(f, y, w, p)
+    assert _rel(out, o_ref) < 1e-2
+    assert abs(loss - loss_ref) <= 1e-2 * abs(loss_ref)
+    for lo, hi in ((M.W1, M.W2), (M.W2, M.W3), (M.W3, M.PARAMS)):
+        assert _rel(g[lo:hi], g_ref[lo:hi]) < 1e-2, (n, lo)
+    # padding parameters stay exactly zero
+    w1 = g[M.W1:M.W2].reshape(M.HIDDEN, M.IN)
+    w3 = g[M.W3:].reshape(M.OUT_N, M.HIDDEN_K)
+    assert not w1[:, M.FEATURES + 1:].any() and not w3[M.OUT:].any()
+
+
+def test_online_training_and_learned_ticks(gpu_available):
+    scene = scenes.box_pile((8, 6, 8), seed=12, spacing=1.3)
+    w = core.World(scene)
+    kw = dict(residual_tolerance=2e-4, max_iterations=48)
+    for _ in range(60):
+        w.step(**kw)
+    w.mlp_attach(seed=3)
+    w.mlp_train(True, lr=3e-3, steps_per_tick=4)
+    losses = []
+    for _ in range(40):
+        st = w.step(**kw)
+        assert st["status"] == 0
+        losses.append(w.mlp_params()[1])
+    assert np.isfinite(losses).all()
+    assert np.mean(losses[-5:]) < 0.5 * np.mean(losses[:3]), losses
+    w.mlp_train(False)
+    for _ in range(10):
+        st = w.step(warm_start=1, **kw)
+        assert st["status"] == 0
+        assert st["residual"] <= 2e-4 or st["iterations"] == 48
+    assert np.isfinite(w.states()["x"]).all()
