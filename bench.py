@@ -12,10 +12,14 @@ run with the residual-driven schedule: sweep until the contact residual (RMS
 over active normal rows) is at or below --tolerance, at most --max-iterations
 sweeps. Inputs are synthetic (seeded); no dataset is involved.
 
-GPU arm (default): `value` is steps/s with the state resident in HBM, timed
-with CUDA events on the world's stream (max over ranks); `e2e` is the same
-metric through the C ABI with host buffers (state upload from pinned host
-memory, tick, state download each step). Multi-GPU runs independent replicas
+GPU arm (default): the warm-start MLP is first trained online on
+--train-frames plain ticks (untimed); then, from the same settled snapshot,
+--steps ticks are timed with the plain warm start and --steps with the
+learned one. `value` is the learned arm's steps/s with the state resident in
+HBM, timed with CUDA events on the world's stream (max over ranks); the plain
+arm's steps/s and both arms' sweep counts are in `config`. `e2e` is the
+learned arm through the C ABI with host buffers (state upload from pinned
+host memory, tick, state download each step). Multi-GPU runs independent replicas
 (the coupled pile does not shard). Reference arm (--impl reference): the CPU
 restatement of the reference's serial Slang CPU driver (oracle/, one core),
 on the same state and schedule, over a bounded number of ticks.
@@ -51,6 +55,9 @@ def parse():
     ap.add_argument("--cpu-ticks", type=int, default=1, help="ticks timed by the CPU baseline leg")
     ap.add_argument("--contact-capacity", type=int, default=0,
                     help="contact-point capacity of the world (0: the library default, 64 per body)")
+    ap.add_argument("--train-frames", type=int, default=200, help="plain ticks of online MLP training")
+    ap.add_argument("--mlp-lr", type=float, default=3e-3)
+    ap.add_argument("--mlp-steps", type=int, default=4, help="Adam steps per training frame")
     return ap.parse_args()
 
 
@@ -149,6 +156,22 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def timed_ticks(world, desc, steps, stream, torch):
+    """CUDA-event time (ms) of `steps` ticks enqueued on the world's stream."""
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(steps):
+        world.step(desc, stats=False)
+    end.record(stream)
+    torch.cuda.synchronize()
+    return start.elapsed_time(end)
+
+
+def replay_stats(world, desc, steps):
+    world.restore()
+    return [world.step(desc) for _ in range(steps)]
+
+
 def gpu_arm(args):
     import torch
     import torch.distributed as dist
@@ -163,7 +186,8 @@ def gpu_arm(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     scene = load_scene()
     n_dyn = int((scene.bodies["motion"] == scenes.DYNAMIC).sum())
-    desc = scene.step_desc(residual_tolerance=args.tolerance, max_iterations=args.max_iterations)
+    plain = scene.step_desc(residual_tolerance=args.tolerance, max_iterations=args.max_iterations)
+    learned = scene.step_desc(residual_tolerance=args.tolerance, max_iterations=args.max_iterations, warm_start=1)
     world = core.World(scene, device=local, contact_capacity=args.contact_capacity)
     stream = torch.cuda.current_stream()
     world.set_stream(stream.cuda_stream)
@@ -172,48 +196,55 @@ def gpu_arm(args):
         if world_size > 1:
             dist.barrier()
 
-    # ---- device-resident timing
+    def max_over_ranks(x):
+        t = torch.tensor([x], device="cuda")
+        if world_size > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     for _ in range(args.warmup):
-        world.step(desc, stats=False)
+        world.step(plain, stats=False)
     world.snapshot()
+
+    # ---- online training of the warm-start MLP on plain ticks (untimed)
+    t0 = time.perf_counter()
+    world.mlp_attach(seed=1)
+    world.mlp_train(True, lr=args.mlp_lr, steps_per_tick=args.mlp_steps)
+    for _ in range(args.train_frames):
+        world.step(plain, stats=False)
+    _, mlp_loss, mlp_plain_loss, mlp_gate = world.mlp_params()
+    world.mlp_train(False)
+    train_s = time.perf_counter() - t0
+
+    # ---- plain arm, device-resident, from the settled snapshot
+    world.restore()
+    barrier()
+    torch.cuda.synchronize()
+    plain_ms = max_over_ranks(timed_ticks(world, plain, args.steps, stream, torch))
+    plain_stats = replay_stats(world, plain, args.steps)
+
+    # ---- learned arm: the headline number
+    world.restore()
     barrier()
     torch.cuda.synchronize()
     world.solve_timer(True)
     launches0 = core.kernel_launches()
     sampler = ClockSampler(local)
     sampler.start()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    start.record(stream)
-    iters, contacts, stats_all = [], [], []
-    for _ in range(args.steps):
-        world.step(desc, stats=False)
-    end.record(stream)
-    torch.cuda.synchronize()
+    learned_ms = max_over_ranks(timed_ticks(world, learned, args.steps, stream, torch))
     barrier()
     clocks = sampler.stop()
     launches = core.kernel_launches() - launches0
     solve_ms, solve_launches = world.solve_timer(False)
-    elapsed = start.elapsed_time(end)
-    t = torch.tensor([elapsed], device="cuda")
-    if world_size > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    elapsed_max = float(t.item())
-    value = world_size * args.steps / (elapsed_max * 1e-3)
-    # Per-tick statistics of the same ticks, replayed from the snapshot
-    # (outside the timed region) for the roofline's algorithmic bytes.
-    world.restore()
-    for _ in range(args.steps):
-        st = world.step(desc)
-        stats_all.append(st)
-        iters.append(int(st["iterations"]))
-        contacts.append(int(st["contacts"]))
-    alg_bytes = sum(solve_bytes(st, n_dyn) for st in stats_all)
+    learned_stats = replay_stats(world, learned, args.steps)
+    value = world_size * args.steps / (learned_ms * 1e-3)
+    plain_value = world_size * args.steps / (plain_ms * 1e-3)
+
+    alg_bytes = sum(solve_bytes(st, n_dyn) for st in learned_stats)
     achieved = alg_bytes / (solve_ms * 1e-3) / 1e9 if solve_ms > 0 else None
-    peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peaks = json.load(f)
-        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+            peak, peak_src = float(json.load(f)["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
         peak, peak_src = 6650.0, "fallback"
     # DRAM bytes per k_solve launch from the committed ncu capture of this
@@ -227,7 +258,7 @@ def gpu_arm(args):
     except (OSError, ValueError):
         pass
 
-    # ---- end to end through the C ABI with host buffers
+    # ---- end to end through the C ABI with host buffers (learned arm)
     world.restore()
     host = torch.empty((scene.n, 13), dtype=torch.float32, pin_memory=True)
     host_np = host.numpy().view(scenes.STATE_DTYPE).reshape(-1)
@@ -237,36 +268,46 @@ def gpu_arm(args):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         world.set_states(host_np)            # h2d: the step's input states
-        world.step(desc, stats=False)
+        world.step(learned, stats=False)
         host_np[:] = world.states()          # d2h: the step's result
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], device="cuda")
-    if world_size > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world_size * args.steps / float(te.item())
+    e2e_value = world_size * args.steps / max_over_ranks(time.perf_counter() - t0)
     state_bytes = scene.n * 52
 
     cpu = None
     if rank == 0 and world_size == 1 and args.cpu_ticks > 0:
-        cv, cst = cpu_baseline(scene, desc, args.cpu_ticks)
+        cv, cst = cpu_baseline(scene, plain, args.cpu_ticks)
         cpu = {"value": cv, "unit": "steps/s", "cores": 1, "kind": "port",
-               "sample": f"{args.cpu_ticks} tick(s) of the same settled pile, same schedule; serial CPU "
-                         f"restatement (oracle/), {int(cst['iterations'])} sweeps"}
+               "sample": f"{args.cpu_ticks} tick(s) of the same settled pile, same schedule, plain warm start; "
+                         f"serial CPU restatement (oracle/), {int(cst['iterations'])} sweeps"}
+
+    def mean(stats, key):
+        return float(np.mean([int(st[key]) for st in stats]))
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world_size,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed_max / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": learned_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": "box pile 64x32x32 (65,536 boxes + ground and walls), settled state, "
-                                   "legacy AVBD profile, residual-driven schedule, plain warm start",
+                                   "legacy AVBD profile, residual-driven schedule; learned warm start "
+                                   "(BF16 tcgen05 MLP, penalty prediction) vs plain",
                        "bodies": scene.n, "tolerance": args.tolerance,
                        "max_iterations": args.max_iterations,
-                       "iterations_mean": float(np.mean(iters)), "contacts_mean": float(np.mean(contacts)),
+                       "plain_steps_per_s": plain_value, "learned_over_plain": value / plain_value,
+                       "iterations_mean_learned": mean(learned_stats, "iterations"),
+                       "iterations_mean_plain": mean(plain_stats, "iterations"),
+                       "residual_max_learned": max(float(st["residual"]) for st in learned_stats),
+                       "residual_max_plain": max(float(st["residual"]) for st in plain_stats),
+                       "contacts_mean": mean(learned_stats, "contacts"),
+                       "mlp_training": {"frames": args.train_frames, "adam_lr": args.mlp_lr,
+                                        "steps_per_frame": args.mlp_steps, "seconds": round(train_s, 2),
+                                        "loss_over_plain_loss": mlp_loss / mlp_plain_loss if mlp_plain_loss else None,
+                                        "gate_open": bool(mlp_gate)},
                        "parallelism": f"replicas x{world_size}",
                        "l2": "inputs larger than L2: per-tick working set ~%d MB (126 MB L2)" % int(
-                           (np.mean(contacts) * (8 + 9) * 16 + scene.n * 400 + 1.2e6 * 24) / 1e6)},
+                           (mean(learned_stats, "contacts") * (8 + 9) * 16 + scene.n * 400 + 1.2e6 * 24) / 1e6)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "kernel": "k_solve", "launches": solve_launches,

@@ -283,7 +283,9 @@ PMB_API int pmb_world_set_warm_table(pmb_world* world, uint32_t rows, const floa
 /* ---- learned warm start ----
  * An 8 -> 64 -> 64 -> 2 MLP (BF16 tensor-core kernels, FP32 accumulation and
  * FP32 master weights) predicting each contact's converged normal-row
- * (lambda, penalty) from its features at the start of the tick. It has no
+ * (lambda, penalty) from its features at the start of the tick, as a
+ * log-space correction of the plain warm start (an all-zero output layer,
+ * the initial state, reproduces the plain warm start). It has no
  * counterpart in the reference: the reference's warm start is the cached,
  * decayed dual (constraint_math.slang:30-37), which stays the default
  * (warm_start = 0) and the fallback for non-finite predictions.
@@ -296,14 +298,31 @@ PMB_API int pmb_world_set_warm_table(pmb_world* world, uint32_t rows, const floa
  * a deterministic initialisation from seed when params is null. Resets the
  * optimiser. Not available for worlds in caller-owned memory. */
 PMB_API int pmb_world_mlp_attach(pmb_world* world, const float* params, uint32_t seed);
+/* What learned ticks take from the predictor: bit 0 the normal lambda, bit 1
+ * the normal penalty, bit 2 lambda corrections averaged over each
+ * manifold's points (keeping the carried-over split of the pair's force).
+ * Default 2 (penalty only): on the settled 65,536-box pile the predicted
+ * penalty cuts the sweeps to the residual tolerance while predicted lambdas,
+ * per point or averaged, add sweeps. */
+PMB_API int pmb_world_mlp_apply_mode(pmb_world* world, uint32_t mode);
 /* Online training: when enabled, every tick ends with steps_per_tick Adam
  * steps (learning_rate) on that tick's contacts, target = the converged
  * normal-row (lambda, penalty), loss = mean squared error of the normalised
  * pair. */
 PMB_API int pmb_world_mlp_train(pmb_world* world, int enable, float learning_rate, uint32_t steps_per_tick);
-/* Current master parameters and the last training step's loss (either
- * pointer may be null; synchronous). */
-PMB_API int pmb_world_mlp_params(pmb_world* world, float* params, float* last_loss);
+/* Current master parameters, the last training step's loss, the loss the
+ * plain warm start (a zero correction) has on the same rows, and the gate:
+ * learned ticks apply predictions only while the gate is open (1), which
+ * online training sets after each tick's first step from loss < 0.9 x plain
+ * loss; attaching given parameters opens it. Null pointers are skipped;
+ * synchronous. */
+PMB_API int pmb_world_mlp_params(pmb_world* world, float* params, float* last_loss, float* plain_loss,
+                                 float* gate);
+/* The last tick's MLP rows (synchronous): 8 features per contact (as stored,
+ * BF16 values widened to float) and 4 metadata floats (y0, y1, weight,
+ * scale: after a training tick y0/y1 are the targets, otherwise the plain
+ * warm start in the model's log space). For inspection and tests. */
+PMB_API int pmb_world_mlp_rows(pmb_world* world, float* features, float* meta, uint32_t capacity, uint32_t* count);
 /* One forward and backward pass over `rows` given rows (features: 8 per row,
  * targets: 2 per row, weights: loss weight per row), host buffers; returns
  * the outputs (2 per row), the gradient of the weighted squared-error loss

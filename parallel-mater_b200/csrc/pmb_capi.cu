@@ -89,7 +89,8 @@ struct pmb_world {
         float lr{1e-3f};
         uint32_t steps_per_tick{1}, grid{};
         uint64_t adam_t{};
-        float *params{}, *m{}, *v{}, *grad{}, *partial{};
+        float *params{}, *m{}, *v{}, *grad{}, *partial{}, *gate{}, *out{};
+        uint32_t mode{2};
         uint8_t *img{}, *x{};
         MlpMeta* meta{};
         std::vector<void*> allocs;
@@ -170,9 +171,11 @@ void enqueue_step(pmb_world* w, const StepParams& sp) {
     auto& mlp = w->mlp;
     const bool learned = mlp.attached && sp.warm_start == 1;
     if (mlp.attached && (learned || mlp.train)) launch_mlp_features(d, sp, mlp.x, mlp.meta, s);
-    if (learned)
-        launch_mlp_tiles(false, mlp.x, mlp.meta, mlp.img, 0, 0, &d.ctr->n_contacts, d.c_lam, d.c_pen, nullptr,
-                         nullptr, &d.ctr->status, kStBarrierTimeout, mlp.grid, s);
+    if (learned) {
+        launch_mlp_tiles(false, mlp.x, mlp.meta, mlp.img, 0, 0, &d.ctr->n_contacts, mlp.out, nullptr, &d.ctr->status,
+                         kStBarrierTimeout, mlp.grid, s);
+        launch_mlp_apply(d, mlp.meta, mlp.out, mlp.mode, mlp.gate, s);
+    }
     prof_mark(s, "mlp features+inference");
     launch_graph(d, sp, s, w->coop_color);
     launch_solve_all(d, sp, s, w->coop_solve, w->out);
@@ -180,13 +183,15 @@ void enqueue_step(pmb_world* w, const StepParams& sp) {
         // Online training on this tick's converged normal rows.
         launch_mlp_targets(d, mlp.meta, s);
         for (uint32_t k = 0; k < mlp.steps_per_tick; ++k) {
-            launch_mlp_tiles(true, mlp.x, mlp.meta, mlp.img, 0, 0, &d.ctr->n_contacts, nullptr, nullptr, nullptr,
-                             mlp.partial, &d.ctr->status, kStBarrierTimeout, mlp.grid, s);
+            launch_mlp_tiles(true, mlp.x, mlp.meta, mlp.img, 0, 0, &d.ctr->n_contacts, nullptr, mlp.partial,
+                             &d.ctr->status, kStBarrierTimeout, mlp.grid, s);
             ++mlp.adam_t;
             const float b1 = 0.9f, b2 = 0.999f;
             const float c1 = 1.0f - std::pow(b1, float(mlp.adam_t)), c2 = 1.0f - std::pow(b2, float(mlp.adam_t));
+            // The gate follows the first step of each tick: its loss is
+            // measured before the model has seen this tick's targets.
             launch_mlp_reduce_adam(mlp.partial, mlp.grid, mlp.grad, mlp.params, mlp.m, mlp.v, mlp.lr, b1, b2, c1, c2,
-                                   1e-8f, s);
+                                   1e-8f, k == 0 ? mlp.gate : nullptr, s);
             launch_mlp_images(mlp.params, mlp.img, s);
         }
         prof_mark(s, "mlp training");
@@ -329,7 +334,8 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
 
 namespace {
 // Deterministic initial weights: He-uniform hidden layers from a counter-based
-// hash of (seed, index), small output layer, zero biases and padding.
+// hash of (seed, index); zero output layer (the predictor starts out as the
+// plain warm start), zero biases and padding.
 float init_uniform(uint32_t seed, uint32_t i) {
     uint64_t z = (uint64_t(seed) << 32) ^ (uint64_t(i) * 0x9E3779B97F4A7C15ull);
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -339,8 +345,7 @@ float init_uniform(uint32_t seed, uint32_t i) {
 }
 void init_params(uint32_t seed, std::vector<float>& p) {
     p.assign(kMlpParams, 0.0f);
-    const float a1 = std::sqrt(6.0f / float(kMlpFeatures)), a2 = std::sqrt(6.0f / float(kMlpHidden)),
-                a3 = 0.1f * std::sqrt(6.0f / float(kMlpHidden));
+    const float a1 = std::sqrt(6.0f / float(kMlpFeatures)), a2 = std::sqrt(6.0f / float(kMlpHidden)), a3 = 0.0f;
     for (uint32_t j = 0; j < kMlpHidden; ++j) {
         for (uint32_t f = 0; f < kMlpFeatures; ++f)
             p[kMlpW1 + j * kMlpIn + f] = a1 * init_uniform(seed, kMlpW1 + j * kMlpIn + f);
@@ -1038,8 +1043,10 @@ int pmb_world_mlp_attach(pmb_world* w, const float* params, uint32_t seed) {
         if (!r) r = mlp_alloc(w, m.params, kMlpParams);
         if (!r) r = mlp_alloc(w, m.m, kMlpParams);
         if (!r) r = mlp_alloc(w, m.v, kMlpParams);
-        if (!r) r = mlp_alloc(w, m.grad, kMlpParams + 1);
-        if (!r) r = mlp_alloc(w, m.partial, size_t(m.grid) * (kMlpParams + 1));
+        if (!r) r = mlp_alloc(w, m.grad, kMlpPartial);
+        if (!r) r = mlp_alloc(w, m.partial, size_t(m.grid) * kMlpPartial);
+        if (!r) r = mlp_alloc(w, m.gate, 1);
+        if (!r) r = mlp_alloc(w, m.out, tiles * kMlpTile * 2);
         if (!r) r = mlp_alloc(w, m.img, kImgBytes);
         if (!r) r = mlp_alloc(w, m.x, tiles * 4096);
         if (!r) r = mlp_alloc(w, m.meta, tiles * kMlpTile);
@@ -1054,9 +1061,19 @@ int pmb_world_mlp_attach(pmb_world* w, const float* params, uint32_t seed) {
     cudaMemcpyAsync(m.params, host.data(), sizeof(float) * kMlpParams, cudaMemcpyHostToDevice, w->stream);
     cudaMemsetAsync(m.m, 0, sizeof(float) * kMlpParams, w->stream);
     cudaMemsetAsync(m.v, 0, sizeof(float) * kMlpParams, w->stream);
+    // Given parameters apply at once; a fresh model waits for training to
+    // show it beats the plain warm start.
+    const float open = params ? 1.0f : 0.0f;
+    cudaMemcpyAsync(m.gate, &open, sizeof(float), cudaMemcpyHostToDevice, w->stream);
     m.adam_t = 0;
     launch_mlp_images(m.params, m.img, w->stream);
     return check(cudaStreamSynchronize(w->stream));
+}
+
+int pmb_world_mlp_apply_mode(pmb_world* w, uint32_t mode) {
+    if (!w || !w->mlp.attached || mode == 0 || mode > 7) return PMB_ERROR_INVALID_ARGUMENT;
+    w->mlp.mode = mode;
+    return PMB_SUCCESS;
 }
 
 int pmb_world_mlp_train(pmb_world* w, int enable, float learning_rate, uint32_t steps_per_tick) {
@@ -1067,14 +1084,39 @@ int pmb_world_mlp_train(pmb_world* w, int enable, float learning_rate, uint32_t 
     return PMB_SUCCESS;
 }
 
-int pmb_world_mlp_params(pmb_world* w, float* params, float* last_loss) {
+int pmb_world_mlp_params(pmb_world* w, float* params, float* last_loss, float* plain_loss, float* gate) {
     if (!w || !w->mlp.attached) return PMB_ERROR_INVALID_ARGUMENT;
     cudaSetDevice(w->device);
     if (params)
         cudaMemcpyAsync(params, w->mlp.params, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost, w->stream);
     if (last_loss)
         cudaMemcpyAsync(last_loss, w->mlp.grad + kMlpParams, sizeof(float), cudaMemcpyDeviceToHost, w->stream);
+    if (plain_loss)
+        cudaMemcpyAsync(plain_loss, w->mlp.grad + kMlpParams + 1, sizeof(float), cudaMemcpyDeviceToHost, w->stream);
+    if (gate) cudaMemcpyAsync(gate, w->mlp.gate, sizeof(float), cudaMemcpyDeviceToHost, w->stream);
     return check(cudaStreamSynchronize(w->stream));
+}
+
+int pmb_world_mlp_rows(pmb_world* w, float* features, float* meta, uint32_t capacity, uint32_t* count) {
+    if (!w || !w->mlp.attached) return PMB_ERROR_INVALID_ARGUMENT;
+    pmb_step_stats st;
+    int r = pmb_world_last_stats(w, &st);
+    if (r) return r;
+    const uint32_t nc = w->host_ctr.n_contacts;
+    if (count) *count = nc;
+    if (!features || !meta || capacity < nc || nc == 0) return PMB_SUCCESS;
+    const uint32_t tiles = (nc + kMlpTile - 1) / kMlpTile;
+    std::vector<uint16_t> x(size_t(tiles) * 2048);
+    cudaMemcpyAsync(x.data(), w->mlp.x, size_t(tiles) * 4096, cudaMemcpyDeviceToHost, w->stream);
+    cudaMemcpyAsync(meta, w->mlp.meta, sizeof(MlpMeta) * size_t(nc), cudaMemcpyDeviceToHost, w->stream);
+    r = check(cudaStreamSynchronize(w->stream));
+    if (r) return r;
+    for (uint32_t c = 0; c < nc; ++c)
+        for (uint32_t k = 0; k < kMlpFeatures; ++k) {
+            const uint32_t bits = uint32_t(x[(size_t(c / kMlpTile) * 4096 + tile_offset(c % kMlpTile, k)) / 2]) << 16;
+            std::memcpy(&features[kMlpFeatures * size_t(c) + k], &bits, 4);
+        }
+    return PMB_SUCCESS;
 }
 
 int pmb_mlp_forward_backward(int32_t device, uint32_t rows, const float* features, const float* targets,
@@ -1098,8 +1140,8 @@ int pmb_mlp_forward_backward(int32_t device, uint32_t rows, const float* feature
     float* d_w = static_cast<float*>(get(sizeof(float) * rows));
     float* d_p = static_cast<float*>(get(sizeof(float) * kMlpParams));
     float* d_out = static_cast<float*>(get(sizeof(float) * 2 * rows));
-    float* d_grad = static_cast<float*>(get(sizeof(float) * (kMlpParams + 1)));
-    float* d_part = static_cast<float*>(get(sizeof(float) * grid * (kMlpParams + 1)));
+    float* d_grad = static_cast<float*>(get(sizeof(float) * kMlpPartial));
+    float* d_part = static_cast<float*>(get(sizeof(float) * grid * kMlpPartial));
     uint8_t* d_img = static_cast<uint8_t*>(get(kImgBytes));
     uint8_t* d_x = static_cast<uint8_t*>(get(size_t(tiles) * 4096));
     MlpMeta* d_meta = static_cast<MlpMeta*>(get(sizeof(MlpMeta) * tiles * kMlpTile));
@@ -1118,16 +1160,15 @@ int pmb_mlp_forward_backward(int32_t device, uint32_t rows, const float* feature
         cudaMemset(d_status, 0, sizeof(uint32_t));
         launch_mlp_images(d_p, d_img, s);
         launch_mlp_pack_rows(d_feat, d_y, d_w, rows, d_x, d_meta, tiles, s);
-        launch_mlp_tiles(true, d_x, d_meta, d_img, rows, tiles, nullptr, nullptr, nullptr, d_out, d_part, d_status,
-                         1u, grid, s);
+        launch_mlp_tiles(true, d_x, d_meta, d_img, rows, tiles, nullptr, d_out, d_part, d_status, 1u, grid, s);
         launch_mlp_reduce_adam(d_part, grid, d_grad, nullptr, nullptr, nullptr, 0.0f, 0.9f, 0.999f, 1.0f, 1.0f, 1e-8f,
-                               s);
+                               nullptr, s);
         r = check(cudaDeviceSynchronize());
         if (r == PMB_SUCCESS) {
             cudaMemcpy(&status, d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost);
             if (outputs) cudaMemcpy(outputs, d_out, sizeof(float) * 2 * rows, cudaMemcpyDeviceToHost);
-            std::vector<float> g(kMlpParams + 1);
-            cudaMemcpy(g.data(), d_grad, sizeof(float) * (kMlpParams + 1), cudaMemcpyDeviceToHost);
+            std::vector<float> g(kMlpPartial);
+            cudaMemcpy(g.data(), d_grad, sizeof(float) * kMlpPartial, cudaMemcpyDeviceToHost);
             if (grads) std::memcpy(grads, g.data(), sizeof(float) * kMlpParams);
             if (loss) *loss = g[kMlpParams];
             r = check(cudaGetLastError());

@@ -142,9 +142,7 @@ struct MlpArgs {
     uint32_t rows;           // valid rows (contacts)
     uint32_t tiles;
     const uint32_t* rows_ptr;  // when set, the row count is read here (device counter)
-    float4* lam;             // inference: written warm start (may be null)
-    float4* pen;
-    float* out;              // optional raw outputs [rows][2]
+    float* out;              // raw outputs [rows][2] (inference: required)
     float* partial;          // training: [gridDim.x][kMlpParams + 1]
     uint32_t* status;        // status word; status_bit is set when a wait times out
     uint32_t status_bit;
@@ -213,7 +211,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_tiles(MlpArgs a) {
     const uint32_t sH1 = smem_u32(sm + kSmH1), sH2 = smem_u32(sm + kSmH2), sDO = smem_u32(sm + kSmDO),
                    sDZ2 = smem_u32(sm + kSmDZ2), sDZ1 = smem_u32(sm + kSmDZ1);
     uint32_t mma_phase = 0;
-    float loss = 0.0f;
+    float loss = 0.0f, base = 0.0f;  // weighted squared error; the same for a zero prediction
     uint32_t it = 0;
     bool pending = false;  // a prefetch is in flight into the other buffer
     for (uint32_t tile = first; tile < a.tiles && ok; tile += gridDim.x, ++it) {
@@ -303,24 +301,13 @@ __global__ void __launch_bounds__(128, 1) k_mlp_tiles(MlpArgs a) {
             a.out[2 * size_t(c_row)] = o[0];
             a.out[2 * size_t(c_row) + 1] = o[1];
         }
-        if (!kTrain) {
-            if (valid && a.lam) {
-                // Normal-row warm start: lambda = max(0, o0) * scale,
-                // penalty = 10^(10 * clamp(o1, 0, 1)) within [1, 1e10].
-                const float lam = fmaxf(o[0], 0.0f) * meta.scale;
-                const float pen = fminf(fmaxf(exp10f(10.0f * fminf(fmaxf(o[1], 0.0f), 1.0f)), 1.0f), 1.0e10f);
-                if (isfinite(lam) && isfinite(pen)) {
-                    reinterpret_cast<float*>(a.lam + c_row)[0] = lam;
-                    reinterpret_cast<float*>(a.pen + c_row)[0] = pen;
-                }
-            }
-            continue;
-        }
+        if (!kTrain) continue;
 
         // ---- backward: squared error on (lambda, penalty), row weights in meta
         const float w = valid ? meta.weight : 0.0f;
         const float e0 = valid ? o[0] - meta.y0 : 0.0f, e1 = valid ? o[1] - meta.y1 : 0.0f;
         loss += w * (e0 * e0 + e1 * e1);
+        if (valid) base += w * (meta.y0 * meta.y0 + meta.y1 * meta.y1);
         {
             const float d[8] = {2.0f * w * e0, 2.0f * w * e1, 0, 0, 0, 0, 0, 0};
             store8(sm + kSmDO, tile_offset(row, 0), d);
@@ -395,7 +382,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_tiles(MlpArgs a) {
 
     if (kTrain) {
         // Partial gradients of this CTA (zero when it had no tile).
-        float* p = a.partial + size_t(blockIdx.x) * (kMlpParams + 1);
+        float* p = a.partial + size_t(blockIdx.x) * kMlpPartial;
         const bool any = it > 0 && ok;
         float v[16] = {};
         if (any) tmem_ld16(tmem + lane_base + kTmDW3, v);
@@ -417,6 +404,14 @@ __global__ void __launch_bounds__(128, 1) k_mlp_tiles(MlpArgs a) {
             for (int k = 0; k < 128; ++k) s += red[k];
             p[kMlpParams] = s;
         }
+        __syncthreads();
+        red[row] = base;
+        __syncthreads();
+        if (tid == 0) {
+            float s = 0.0f;
+            for (int k = 0; k < 128; ++k) s += red[k];
+            p[kMlpParams + 1] = s;
+        }
     }
     if (!ok) {
         // Leave no bulk copy in flight: wait (bounded) for the prefetch of
@@ -432,16 +427,22 @@ __global__ void __launch_bounds__(128, 1) k_mlp_tiles(MlpArgs a) {
 }
 
 // ---------------------------------------------------------------- features
-// One row per contact point, written into its tile's canonical position:
-//  0 normal error at the start of the tick / 1 cm
+// One row per contact point, written into its tile's canonical position
+// (each feature scaled to order one and clipped to [-5, 5]):
+//  0 normal error at the start of the tick / 0.1 m
 //  1 closing speed (m/s)
-//  2 plain warm-start lambda / scale, scale = |g| m_eff (m_eff = 1/(w_a+w_b))
-//  3 log10(plain warm-start penalty) / 10
-//  4 w_b / (w_a + w_b)
+//  2 log1p(plain warm-start lambda / scale) / 2, scale = |g| m_eff,
+//    m_eff = 1/(w_a+w_b)
+//  3 (log10(plain warm-start penalty) - 6.5) / 0.3
+//  4 2 w_b / (w_a + w_b) - 1
 //  5 1 if the contact was matched in the cache
 //  6 normal . up (up = -g/|g|)
-//  7 log10(m_eff) / 4
+//  7 (log10(m_eff) - 2.7) / 0.25
 //  8 constant one (bias)
+// The row's metadata keeps the plain warm start in the model's log space in
+// FP32 (y0 = log1p(lambda / scale), y1 = log10(penalty)) and the scale: the
+// network predicts scaled corrections of them (see kLamOut, kPenOut), so an
+// all-zero output layer reproduces the plain warm start exactly.
 __global__ void k_mlp_features(Dev d, StepParams sp, uint8_t* x, MlpMeta* meta) {
     const uint32_t nc = d.ctr->n_contacts;
     const uint32_t tiles = (nc + kMlpTile - 1) / kMlpTile;
@@ -459,17 +460,19 @@ __global__ void k_mlp_features(Dev d, StepParams sp, uint8_t* x, MlpMeta* meta) 
             const float meff = wsum > 0.0f ? 1.0f / wsum : 1.0f;
             const float scale = fmaxf(g * meff, 1.0e-6f);
             const float4 e = d.c_e[c], lam = d.c_lam[c], pen = d.c_pen[c], n = d.c_n[c], aa = d.c_aa[c];
-            f[0] = e.x * 100.0f;
+            const float llam = log1pf(fmaxf(lam.x, 0.0f) / scale), lpen = log10f(fmaxf(pen.x, 1.0f));
+            f[0] = e.x * 10.0f;
             f[1] = e.w;
-            f[2] = lam.x / scale;
-            f[3] = log10f(fmaxf(pen.x, 1.0f)) * 0.1f;
-            f[4] = wsum > 0.0f ? wb / wsum : 0.5f;
+            f[2] = llam * 0.5f;
+            f[3] = (lpen - 6.5f) * (1.0f / 0.3f);
+            f[4] = wsum > 0.0f ? 2.0f * wb / wsum - 1.0f : 0.0f;
             f[5] = aa.w != 0.0f ? 1.0f : 0.0f;
             f[6] = n.x * up.x + n.y * up.y + n.z * up.z;
-            f[7] = log10f(meff) * 0.25f;
+            f[7] = (log10f(meff) - 2.7f) * 4.0f;
+            for (int k = 0; k < 8; ++k) f[k] = isfinite(f[k]) ? fminf(fmaxf(f[k], -5.0f), 5.0f) : 0.0f;
             f[8] = 1.0f;
-            for (int k = 0; k < 8; ++k)
-                if (!isfinite(f[k])) f[k] = 0.0f;
+            m.y0 = llam;
+            m.y1 = lpen;
             m.scale = scale;
         }
         const uint32_t tile = c / kMlpTile, r = c % kMlpTile;
@@ -480,7 +483,10 @@ __global__ void k_mlp_features(Dev d, StepParams sp, uint8_t* x, MlpMeta* meta) 
     }
 }
 
-// Training targets from the tick's converged normal rows.
+// Training targets from the tick's converged normal rows: the scaled
+// corrections that turn the plain warm start into the converged
+// (lambda, penalty): y0 = kLamOut * (log1p(lambda / scale) - plain),
+// y1 = kPenOut * (log10(penalty) - plain).
 __global__ void k_mlp_targets(Dev d, MlpMeta* meta) {
     const uint32_t nc = d.ctr->n_contacts;
     const float w = nc ? 1.0f / float(nc) : 0.0f;
@@ -488,11 +494,43 @@ __global__ void k_mlp_targets(Dev d, MlpMeta* meta) {
         MlpMeta m = meta[c];
         const float lam = reinterpret_cast<const float*>(d.c_lam + c)[0];
         const float pen = reinterpret_cast<const float*>(d.c_pen + c)[0];
-        m.y0 = lam / m.scale;
-        m.y1 = log10f(fmaxf(pen, 1.0f)) * 0.1f;
+        m.y0 = kLamOut * (log1pf(fmaxf(lam, 0.0f) / m.scale) - m.y0);
+        m.y1 = kPenOut * (log10f(fmaxf(pen, 1.0f)) - m.y1);
         m.weight = (isfinite(m.y0) && isfinite(m.y1)) ? w : 0.0f;
         if (m.weight == 0.0f) m.y0 = m.y1 = 0.0f;
         meta[c] = m;
+    }
+}
+
+// Learned warm start from the network's outputs (scaled corrections of the
+// plain warm start in log space, meta.y0/y1 from k_mlp_features):
+//   lambda  = scale * expm1(y0 + o0 / kLamOut)   (mode bit 0)
+//   penalty = 10^(y1 + o1 / kPenOut)             (mode bit 1)
+// With mode bit 2 the lambda correction of every point of a manifold is the
+// mean of its points' corrections, so the split of the pair's normal force
+// between its points stays the one the plain warm start carries over.
+// Nothing changes while the gate is closed or for non-finite values.
+__global__ void k_mlp_apply(Dev d, const MlpMeta* meta, const float* out, uint32_t mode, const float* gate) {
+    if (gate && *gate == 0.0f) return;
+    const uint32_t n_act = d.ctr->n_act;
+    for (uint32_t i = grid_stride_begin(); i < n_act; i += grid_stride()) {
+        const uint32_t off = d.act_off[i], cnt = d.act_cnt[i];
+        float mean0 = 0.0f;
+        for (uint32_t p = 0; p < cnt; ++p) mean0 += out[2 * size_t(off + p)];
+        mean0 /= float(cnt > 0 ? cnt : 1);
+        for (uint32_t p = 0; p < cnt; ++p) {
+            const uint32_t c = off + p;
+            const MlpMeta m = meta[c];
+            const float o0 = (mode & 4u) ? mean0 : out[2 * size_t(c)], o1 = out[2 * size_t(c) + 1];
+            if (mode & 1u) {
+                const float lam = fmaxf(m.scale * expm1f(m.y0 + o0 * (1.0f / kLamOut)), 0.0f);
+                if (isfinite(lam)) reinterpret_cast<float*>(d.c_lam + c)[0] = lam;
+            }
+            if (mode & 2u) {
+                const float pen = fminf(fmaxf(exp10f(m.y1 + o1 * (1.0f / kPenOut)), 1.0f), 1.0e10f);
+                if (isfinite(pen)) reinterpret_cast<float*>(d.c_pen + c)[0] = pen;
+            }
+        }
     }
 }
 
@@ -536,19 +574,29 @@ __global__ void k_mlp_images(const float* params, uint8_t* img) {
 }
 
 // Sum of the CTAs' partial gradients in CTA order, then one Adam step on the
-// FP32 master weights (lr = 0 only sums).
+// FP32 master weights (lr = 0 only sums). With gate set, also opens the
+// learned warm start when this step's loss (measured before the update) is
+// below 0.9 of the loss of the plain warm start (a zero correction).
 __global__ void k_mlp_reduce_adam(const float* partial, uint32_t parts, float* grad, float* params, float* m,
-                                  float* v, float lr, float b1, float b2, float c1, float c2, float eps) {
-    for (uint32_t i = grid_stride_begin(); i <= kMlpParams; i += grid_stride()) {
+                                  float* v, float lr, float b1, float b2, float c1, float c2, float eps, float* gate) {
+    for (uint32_t i = grid_stride_begin(); i < kMlpPartial; i += grid_stride()) {
         float s = 0.0f;
-        for (uint32_t p = 0; p < parts; ++p) s += partial[size_t(p) * (kMlpParams + 1) + i];
+        for (uint32_t p = 0; p < parts; ++p) s += partial[size_t(p) * kMlpPartial + i];
         grad[i] = s;
-        if (i == kMlpParams || lr == 0.0f) continue;
+        if (i >= kMlpParams || lr == 0.0f) continue;
         const float mi = b1 * m[i] + (1.0f - b1) * s;
         const float vi = b2 * v[i] + (1.0f - b2) * s * s;
         m[i] = mi;
         v[i] = vi;
         params[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+    if (gate && blockIdx.x == 0 && threadIdx.x == 0) {
+        float loss = 0.0f, zero = 0.0f;
+        for (uint32_t p = 0; p < parts; ++p) {
+            loss += partial[size_t(p) * kMlpPartial + kMlpParams];
+            zero += partial[size_t(p) * kMlpPartial + kMlpParams + 1];
+        }
+        *gate = (zero > 0.0f && loss < 0.9f * zero) ? 1.0f : 0.0f;
     }
 }
 
@@ -595,9 +643,9 @@ void launch_mlp_pack_rows(const float* feat, const float* y, const float* w, uin
 }
 
 void launch_mlp_tiles(bool train, const uint8_t* x, const MlpMeta* meta, const uint8_t* img, uint32_t rows,
-                      uint32_t tiles, const uint32_t* rows_ptr, float4* lam, float4* pen, float* out, float* partial,
-                      uint32_t* status, uint32_t status_bit, uint32_t grid, cudaStream_t s) {
-    MlpArgs a{x, meta, img, rows, tiles, rows_ptr, lam, pen, out, partial, status, status_bit};
+                      uint32_t tiles, const uint32_t* rows_ptr, float* out, float* partial, uint32_t* status,
+                      uint32_t status_bit, uint32_t grid, cudaStream_t s) {
+    MlpArgs a{x, meta, img, rows, tiles, rows_ptr, out, partial, status, status_bit};
     if (train)
         k_mlp_tiles<true><<<grid, 128, kSmBytes, s>>>(a);
     else
@@ -605,10 +653,16 @@ void launch_mlp_tiles(bool train, const uint8_t* x, const MlpMeta* meta, const u
     ++g_kernel_launches;
 }
 
+void launch_mlp_apply(const Dev& d, const MlpMeta* meta, const float* out, uint32_t mode, const float* gate,
+                      cudaStream_t s) {
+    k_mlp_apply<<<blocks_for(d.cap_pair), kBlock, 0, s>>>(d, meta, out, mode, gate);
+    ++g_kernel_launches;
+}
+
 void launch_mlp_reduce_adam(const float* partial, uint32_t parts, float* grad, float* params, float* m, float* v,
-                            float lr, float b1, float b2, float c1, float c2, float eps, cudaStream_t s) {
-    k_mlp_reduce_adam<<<(kMlpParams + 256) / 256, 256, 0, s>>>(partial, parts, grad, params, m, v, lr, b1, b2, c1,
-                                                                c2, eps);
+                            float lr, float b1, float b2, float c1, float c2, float eps, float* gate, cudaStream_t s) {
+    k_mlp_reduce_adam<<<(kMlpPartial + 255) / 256, 256, 0, s>>>(partial, parts, grad, params, m, v, lr, b1, b2, c1,
+                                                                 c2, eps, gate);
     ++g_kernel_launches;
 }
 

@@ -26,6 +26,13 @@ constexpr uint32_t kMlpW1 = 0;
 constexpr uint32_t kMlpW2 = kMlpW1 + kMlpHidden * kMlpIn;
 constexpr uint32_t kMlpW3 = kMlpW2 + kMlpHidden * kMlpHiddenK;
 constexpr uint32_t kMlpParams = kMlpW3 + kMlpOutN * kMlpHiddenK;  // 7424
+// A CTA's partial vector: the gradient, the weighted squared error and the
+// weighted squared error of a zero prediction (the plain warm start).
+constexpr uint32_t kMlpPartial = kMlpParams + 2;
+// Output scaling: o0 = kLamOut * correction of log1p(lambda / scale),
+// o1 = kPenOut * correction of log10(penalty).
+constexpr float kLamOut = 4.0f;
+constexpr float kPenOut = 100.0f;
 
 // BF16 weight images in the tensor cores' shared-memory layout (no swizzle,
 // K-major core matrices of 8 rows x 16 bytes), copied into shared memory

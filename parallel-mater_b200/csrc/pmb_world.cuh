@@ -260,10 +260,12 @@ void launch_mlp_targets(const Dev& d, MlpMeta* meta, cudaStream_t s);
 void launch_mlp_pack_rows(const float* feat, const float* y, const float* w, uint32_t n, uint8_t* x, MlpMeta* meta,
                           uint32_t tiles, cudaStream_t s);
 void launch_mlp_tiles(bool train, const uint8_t* x, const MlpMeta* meta, const uint8_t* img, uint32_t rows,
-                      uint32_t tiles, const uint32_t* rows_ptr, float4* lam, float4* pen, float* out, float* partial,
-                      uint32_t* status, uint32_t status_bit, uint32_t grid, cudaStream_t s);
+                      uint32_t tiles, const uint32_t* rows_ptr, float* out, float* partial, uint32_t* status,
+                      uint32_t status_bit, uint32_t grid, cudaStream_t s);
+void launch_mlp_apply(const Dev& d, const MlpMeta* meta, const float* out, uint32_t mode, const float* gate,
+                      cudaStream_t s);
 void launch_mlp_reduce_adam(const float* partial, uint32_t parts, float* grad, float* params, float* m, float* v,
-                            float lr, float b1, float b2, float c1, float c2, float eps, cudaStream_t s);
+                            float lr, float b1, float b2, float c1, float c2, float eps, float* gate, cudaStream_t s);
 
 inline uint32_t blocks_for(uint32_t n, int threads = kBlock) {
     uint32_t b = (n + threads - 1) / threads;

@@ -82,7 +82,7 @@ def lib():
             "pmb_world_joints": [vp, vp, vp, vp, u32],
             "pmb_world_contact_duals": [vp, u32, vp, vp, u32, vp],
             "pmb_world_mlp_attach": [vp, vp, u32], "pmb_world_mlp_train": [vp, i32, ctypes.c_float, u32],
-            "pmb_world_mlp_params": [vp, vp, vp],
+            "pmb_world_mlp_params": [vp, vp, vp, vp, vp], "pmb_world_mlp_apply_mode": [vp, u32], "pmb_world_mlp_rows": [vp, vp, vp, u32, vp],
             "pmb_mlp_forward_backward": [i32, u32, vp, vp, vp, vp, vp, vp, vp],
             "pmb_world_set_warm_table": [vp, u32, vp, vp, u32],
         }
@@ -261,15 +261,29 @@ class World:
         p = None if params is None else np.ascontiguousarray(params, np.float32)
         _check(lib().pmb_world_mlp_attach(self.h, _p(p), seed), "pmb_world_mlp_attach")
 
+    def mlp_apply_mode(self, mode):
+        _check(lib().pmb_world_mlp_apply_mode(self.h, mode), "pmb_world_mlp_apply_mode")
+
     def mlp_train(self, enable=True, lr=1e-3, steps_per_tick=1):
         _check(lib().pmb_world_mlp_train(self.h, 1 if enable else 0, lr, steps_per_tick), "pmb_world_mlp_train")
 
     def mlp_params(self):
-        """(master parameters, last training loss)."""
+        """(master parameters, last training loss, plain warm start's loss on
+        the same rows, gate)."""
         p = np.zeros(MLP_PARAMS, np.float32)
-        loss = ctypes.c_float()
-        _check(lib().pmb_world_mlp_params(self.h, p.ctypes.data, ctypes.byref(loss)), "pmb_world_mlp_params")
-        return p, loss.value
+        loss, plain, gate = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        _check(lib().pmb_world_mlp_params(self.h, p.ctypes.data, ctypes.byref(loss), ctypes.byref(plain),
+                                          ctypes.byref(gate)), "pmb_world_mlp_params")
+        return p, loss.value, plain.value, gate.value
+
+    def mlp_rows(self):
+        """(features [n, 8], meta [n, 4]) of the last tick's contacts."""
+        n = ctypes.c_uint32()
+        _check(lib().pmb_world_mlp_rows(self.h, None, None, 0, ctypes.byref(n)), "mlp_rows")
+        f = np.zeros((max(n.value, 1), 8), np.float32)
+        m = np.zeros((max(n.value, 1), 4), np.float32)
+        _check(lib().pmb_world_mlp_rows(self.h, f.ctypes.data, m.ctypes.data, n.value, ctypes.byref(n)), "mlp_rows")
+        return f[:n.value], m[:n.value]
 
     def contact_duals(self, rows=1):
         """(lambda, penalty) of the first `rows` rows of every contact point
