@@ -108,6 +108,16 @@ typedef struct pmb_world_desc {
     uint64_t persistent_bytes;
     void* scratch_memory;
     uint64_t scratch_bytes;
+    /* Optional batch of independent scenes stepped together (scene_count >
+     * 1): body_scene[i] is body i's scene, non-decreasing (each scene's
+     * bodies contiguous); bodies of different scenes never collide; joints
+     * stay within a scene. Every scene sweeps its own budget: the tick's
+     * rule applied per scene, with scene_iterations[s] (optional, 0 = none)
+     * as the scene's requested iterations. The residual-driven schedule
+     * does not apply to batches. */
+    uint32_t scene_count;
+    const uint32_t* body_scene;
+    const uint32_t* scene_iterations;
 } pmb_world_desc;
 
 /* Upper bounds for sizing caller-owned memory. Capacities of 0 select the
@@ -331,6 +341,13 @@ PMB_API int pmb_world_mlp_rows(pmb_world* world, float* features, float* meta, u
 PMB_API int pmb_mlp_forward_backward(int32_t device, uint32_t rows, const float* features, const float* targets,
                                      const float* weights, const float* params, float* outputs, float* grads,
                                      float* loss);
+
+/* Per-scene results of the last tick of a batched world (synchronous): RMS
+ * and largest row violation of the scene's last sweep (the tick's residual
+ * definition), sweeps run, contact points. Null pointers are skipped;
+ * capacity >= scene_count. */
+PMB_API int pmb_world_scene_stats(pmb_world* world, float* residual, float* residual_max, uint32_t* iterations,
+                                  uint32_t* contacts, uint32_t capacity);
 
 /* The CUDA stream (cudaStream_t) the world enqueues its work on. */
 PMB_API int pmb_world_stream(pmb_world* world, void** stream);

@@ -29,11 +29,13 @@ __device__ __forceinline__ uint32_t expand10(uint32_t v) {
     v = (v | (v << 2)) & 0x09249249u;
     return v;
 }
-__device__ __forceinline__ uint32_t cell_bucket(int cx, int cy, int cz, uint32_t size) {
+// Bucket of a grid cell; in a batched world the scene is part of the key.
+__device__ __forceinline__ uint32_t cell_bucket(int cx, int cy, int cz, uint32_t size, uint32_t scene) {
     uint32_t m = expand10(uint32_t(cx)) | (expand10(uint32_t(cy)) << 1) | (expand10(uint32_t(cz)) << 2);
     uint32_t hi = (uint32_t(cx) >> 10) * 73856093u ^ (uint32_t(cy) >> 10) * 19349663u ^ (uint32_t(cz) >> 10) * 83492791u;
-    return (m ^ hi) & (size - 1u);
+    return (m ^ hi ^ (scene * 0x9E3779B1u)) & (size - 1u);
 }
+__device__ __forceinline__ uint32_t scene_of(const Dev& d, uint32_t i) { return batched(d) ? d.scene_of[i] : 0u; }
 __device__ __forceinline__ int4 cell_of(float4 lo, float4 hi, float hs) {
     V3 c = mul(add(v3(lo), v3(hi)), 0.5f);
     return make_int4(int(floorf(c.x / hs)), int(floorf(c.y / hs)), int(floorf(c.z / hs)), 0);
@@ -217,7 +219,7 @@ __global__ void k_grid_count(Dev d) {
         if (d.is_large[i] != 0) continue;
         int4 c = cell_of(d.lo[i], d.hi[i], hs);
         d.grid_cell[i] = c;
-        atomicAdd(&d.bucket_count[cell_bucket(c.x, c.y, c.z, d.grid_size)], 1u);
+        atomicAdd(&d.bucket_count[cell_bucket(c.x, c.y, c.z, d.grid_size, scene_of(d, i))], 1u);
     }
 }
 
@@ -225,7 +227,7 @@ __global__ void k_grid_scatter(Dev d) {
     for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
         if (d.is_large[i] != 0) continue;
         int4 c = d.grid_cell[i];
-        uint32_t b = cell_bucket(c.x, c.y, c.z, d.grid_size);
+        uint32_t b = cell_bucket(c.x, c.y, c.z, d.grid_size, scene_of(d, i));
         uint32_t slot = d.bucket_off[b] + atomicAdd(&d.bucket_cursor[b], 1u);
         d.grid_body[slot] = i;
     }
@@ -265,13 +267,19 @@ template <bool kWrite> __device__ uint32_t visit_candidates(const Dev& d, uint32
         if (kWrite && count < cap) out[count] = b;
         ++count;
     };
-    const uint32_t nl = d.ctr->n_large;
-    for (uint32_t k = 0; k < nl; ++k) {
-        uint32_t b = d.large_list[k];
+    const bool multi = batched(d);
+    const uint32_t scene = scene_of(d, a);
+    // Large bodies (all of them, or this scene's).
+    const uint32_t l0 = multi ? d.scene_large_off[scene] : 0u;
+    const uint32_t l1 = multi ? d.scene_large_off[scene + 1] : d.ctr->n_large;
+    const uint32_t* large = multi ? d.scene_large_list : d.large_list;
+    for (uint32_t k = l0; k < l1; ++k) {
+        uint32_t b = large[k];
         if (candidate(d, a, b, alo, ahi)) emit(b);
     }
     if (d.is_large[a] == 1) {
-        for (uint32_t b = 0; b < d.n; ++b)
+        const uint32_t b0 = multi ? d.scene_body_off[scene] : 0u, b1 = multi ? d.scene_body_off[scene + 1] : d.n;
+        for (uint32_t b = b0; b < b1; ++b)
             if (d.is_large[b] == 0 && candidate(d, a, b, alo, ahi)) emit(b);
         return count;
     }
@@ -280,16 +288,31 @@ template <bool kWrite> __device__ uint32_t visit_candidates(const Dev& d, uint32
         for (int dy = -1; dy <= 1; ++dy)
             for (int dx = -1; dx <= 1; ++dx) {
                 int cx = c.x + dx, cy = c.y + dy, cz = c.z + dz;
-                uint32_t bk = cell_bucket(cx, cy, cz, d.grid_size);
+                uint32_t bk = cell_bucket(cx, cy, cz, d.grid_size, scene);
                 uint32_t s = d.bucket_off[bk], e = d.bucket_off[bk + 1];
                 for (uint32_t k = s; k < e; ++k) {
                     uint32_t b = d.grid_body[k];
                     int4 cb = d.grid_cell[b];
                     if (cb.x != cx || cb.y != cy || cb.z != cz) continue;
+                    if (multi && d.scene_of[b] != scene) continue;
                     if (candidate(d, a, b, alo, ahi)) emit(b);
                 }
             }
     return count;
+}
+
+// Per-scene large-body lists (batched worlds): count, offsets, scatter.
+__global__ void k_scene_large_count(Dev d) {
+    const uint32_t nl = d.ctr->n_large;
+    for (uint32_t k = grid_stride_begin(); k < nl; k += grid_stride())
+        atomicAdd(&d.scene_large_count[d.scene_of[d.large_list[k]]], 1u);
+}
+__global__ void k_scene_large_scatter(Dev d) {
+    const uint32_t nl = d.ctr->n_large;
+    for (uint32_t k = grid_stride_begin(); k < nl; k += grid_stride()) {
+        const uint32_t b = d.large_list[k], s = d.scene_of[b];
+        d.scene_large_list[d.scene_large_off[s] + atomicAdd(&d.scene_large_cursor[s], 1u)] = b;
+    }
 }
 
 __global__ void k_query_count(Dev d) {
@@ -330,6 +353,15 @@ __global__ void k_clamp_count(uint32_t* count, uint32_t cap) {
 }
 
 void launch_broadphase(const Dev& d, cudaStream_t s) {
+    if (d.n_scenes > 1) {
+        cudaMemsetAsync(d.scene_large_count, 0, sizeof(uint32_t) * (d.n_scenes + 1), s);
+        cudaMemsetAsync(d.scene_large_cursor, 0, sizeof(uint32_t) * d.n_scenes, s);
+        k_scene_large_count<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+        ++g_kernel_launches;
+        scan_u32(d.scene_large_count, d.scene_large_off, nullptr, d.n_scenes, nullptr, d.scan_tmp32, s);
+        k_scene_large_scatter<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+        ++g_kernel_launches;
+    }
     cudaMemsetAsync(d.bucket_count, 0, sizeof(uint32_t) * (d.grid_size + 1), s);
     cudaMemsetAsync(d.bucket_cursor, 0, sizeof(uint32_t) * d.grid_size, s);
     k_grid_count<<<blocks_for(d.n), kBlock, 0, s>>>(d);

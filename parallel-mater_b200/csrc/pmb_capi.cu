@@ -178,6 +178,7 @@ void enqueue_step(pmb_world* w, const StepParams& sp) {
     }
     prof_mark(s, "mlp features+inference");
     launch_graph(d, sp, s, w->coop_color);
+    launch_scene_budgets(d, sp, s);
     launch_solve_all(d, sp, s, w->coop_solve, w->out);
     if (mlp.attached && mlp.train) {
         // Online training on this tick's converged normal rows.
@@ -251,7 +252,7 @@ void fill_stats(const Counters& c, pmb_step_stats* s) {
 }
 
 struct Sizes {
-    uint32_t n, nm, nj;
+    uint32_t n, nm, nj, scenes;
     size_t verts, planes, dis;
     uint32_t cap_cand, cap_pair, cap_contact;
 };
@@ -324,6 +325,13 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     ALLOCP(d.ctr, 1);
     ALLOC(e.lo, nm); ALLOC(e.hi, nm); ALLOC(e.sph, nm);
     ALLOCP(e.dis, z.dis);
+    if (z.scenes > 1) {
+        const uint32_t ns = z.scenes;
+        ALLOCP(d.scene_of, n); ALLOCP(d.scene_body_off, ns + 1); ALLOCP(d.scene_iters, ns); ALLOCP(d.scene_jiters, ns);
+        ALLOC(d.scene_large_count, ns + 1); ALLOC(d.scene_large_off, ns + 1); ALLOC(d.scene_large_cursor, ns);
+        ALLOC(d.scene_large_list, n); ALLOC(d.scene_budget, ns);
+        ALLOC(d.scene_res_sq, ns); ALLOC(d.scene_res_mx, ns); ALLOC(d.scene_res_n, ns);
+    }
 #undef ALLOCP
 #undef ALLOC
 #undef ALLOCS
@@ -381,6 +389,15 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
         if (desc->joints[j].type > 7 || desc->joints[j].body_a >= desc->body_count ||
             desc->joints[j].body_b >= desc->body_count)
             return PMB_ERROR_INVALID_ARGUMENT;
+    if (desc->scene_count > 1) {
+        if (!desc->body_scene || desc->scene_count > desc->body_count) return PMB_ERROR_INVALID_ARGUMENT;
+        for (uint32_t i = 0; i < desc->body_count; ++i)
+            if (desc->body_scene[i] >= desc->scene_count || (i && desc->body_scene[i] < desc->body_scene[i - 1]))
+                return PMB_ERROR_INVALID_ARGUMENT;
+        for (uint32_t j = 0; j < desc->joint_count; ++j)
+            if (desc->body_scene[desc->joints[j].body_a] != desc->body_scene[desc->joints[j].body_b])
+                return PMB_ERROR_INVALID_ARGUMENT;
+    }
     if ((desc->persistent_memory == nullptr) != (desc->scratch_memory == nullptr) ||
         (reinterpret_cast<uintptr_t>(desc->persistent_memory) % kArenaAlign) != 0 ||
         (reinterpret_cast<uintptr_t>(desc->scratch_memory) % kArenaAlign) != 0)
@@ -461,7 +478,9 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     }
     std::sort(dis_keys.begin(), dis_keys.end());
     dis_keys.erase(std::unique(dis_keys.begin(), dis_keys.end()), dis_keys.end());
-    const Sizes z{n, nm, nj, verts.size(), planes.size(), dis_keys.size(), d.cap_cand, d.cap_pair, d.cap_contact};
+    const uint32_t ns = desc->scene_count > 1 ? desc->scene_count : 0u;
+    d.n_scenes = ns;
+    const Sizes z{n, nm, nj, ns, verts.size(), planes.size(), dis_keys.size(), d.cap_cand, d.cap_pair, d.cap_contact};
     if (w->arena[kPersistent]) {
         // Bound memory must hold the whole layout before anything is carved.
         pmb_world probe;
@@ -525,6 +544,17 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     up(dhi, mhi.data(), 16 * nm);
     up(dsph, msph.data(), 16 * nm);
     if (nj) up(d.joints, desc->joints, sizeof(Joint) * nj);
+    std::vector<uint32_t> scene_off, scene_iters;
+    if (ns > 1) {
+        scene_off.assign(ns + 1, 0);
+        for (uint32_t i = 0; i < n; ++i) ++scene_off[desc->body_scene[i] + 1];
+        for (uint32_t k = 0; k < ns; ++k) scene_off[k + 1] += scene_off[k];
+        scene_iters.assign(ns, 0);
+        if (desc->scene_iterations) scene_iters.assign(desc->scene_iterations, desc->scene_iterations + ns);
+        up(d.scene_of, desc->body_scene, 4 * size_t(n));
+        up(d.scene_body_off, scene_off.data(), 4 * size_t(ns + 1));
+        up(d.scene_iters, scene_iters.data(), 4 * size_t(ns));
+    }
     if (!dis_keys.empty()) up(dis, dis_keys.data(), 8 * dis_keys.size());
     std::vector<uint32_t> colors(n, kInvalid);
     up(d.color, colors.data(), 4 * n);
@@ -954,6 +984,7 @@ int pmb_world_memory_requirements(const pmb_world_capacity* c, uint64_t* persist
     const Sizes z{n,
                   std::max(1u, c->mesh_count),
                   c->joint_count,
+                  0u,
                   size_t(c->mesh_vertex_count),
                   2 * size_t(c->mesh_triangle_count),
                   size_t(c->joint_count),
@@ -1178,6 +1209,44 @@ int pmb_mlp_forward_backward(int32_t device, uint32_t rows, const float* feature
         if (p) cudaFree(p);
     if (r == PMB_SUCCESS && status) r = PMB_ERROR_DEVICE_LOST;
     return r;
+}
+
+int pmb_world_scene_stats(pmb_world* w, float* residual, float* residual_max, uint32_t* iterations,
+                          uint32_t* contacts, uint32_t capacity) {
+    if (!w || w->d.n_scenes <= 1 || capacity < w->d.n_scenes) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    const uint32_t ns = w->d.n_scenes;
+    std::vector<float> sq(ns), mx(ns);
+    std::vector<uint32_t> cnt(ns), bud(ns);
+    cudaMemcpyAsync(sq.data(), w->d.scene_res_sq, 4 * size_t(ns), cudaMemcpyDeviceToHost, w->stream);
+    cudaMemcpyAsync(mx.data(), w->d.scene_res_mx, 4 * size_t(ns), cudaMemcpyDeviceToHost, w->stream);
+    cudaMemcpyAsync(cnt.data(), w->d.scene_res_n, 4 * size_t(ns), cudaMemcpyDeviceToHost, w->stream);
+    cudaMemcpyAsync(bud.data(), w->d.scene_budget, 4 * size_t(ns), cudaMemcpyDeviceToHost, w->stream);
+    std::vector<uint32_t> per_scene;
+    if (contacts) {
+        // Contact points per scene from the last tick's pairs.
+        pmb_step_stats st;
+        int r = pmb_world_last_stats(w, &st);
+        if (r) return r;
+        const uint32_t na = w->host_ctr.n_act;
+        std::vector<uint32_t> a(na), c(na), scene(w->d.n);
+        cudaMemcpyAsync(a.data(), w->d.act_a, 4 * size_t(na), cudaMemcpyDeviceToHost, w->stream);
+        cudaMemcpyAsync(c.data(), w->d.act_cnt, 4 * size_t(na), cudaMemcpyDeviceToHost, w->stream);
+        cudaMemcpyAsync(scene.data(), w->d.scene_of, 4 * size_t(w->d.n), cudaMemcpyDeviceToHost, w->stream);
+        r = check(cudaStreamSynchronize(w->stream));
+        if (r) return r;
+        per_scene.assign(ns, 0);
+        for (uint32_t k = 0; k < na; ++k) per_scene[scene[a[k]]] += c[k];
+    }
+    int r = check(cudaStreamSynchronize(w->stream));
+    if (r) return r;
+    for (uint32_t k = 0; k < ns; ++k) {
+        if (residual) residual[k] = cnt[k] ? std::sqrt(sq[k] / float(cnt[k])) : 0.0f;
+        if (residual_max) residual_max[k] = mx[k];
+        if (iterations) iterations[k] = bud[k];
+        if (contacts) contacts[k] = per_scene[k];
+    }
+    return PMB_SUCCESS;
 }
 
 int pmb_world_stream(pmb_world* w, void** stream) {

@@ -240,7 +240,33 @@ __global__ void k_graph_degrees(Dev d, StepParams sp) {
         if (db) atomicAdd(&d.jdeg[b], 1u);
         if (da && db) uf_unite(d.parent, a, b);
         if (!sp.realtime && sp.requested == 0) atomicMax(&d.ctr->joint_iters, d.joints[j].solver_iterations);
+        if (batched(d)) atomicMax(&d.scene_jiters[d.scene_of[a]], d.joints[j].solver_iterations);
     }
+}
+
+// Sweeps of every scene of a batched world, with the whole-world rule of
+// k_solve applied per scene: the realtime profile sweeps 8 times; legacy
+// sweeps the scene's requested iterations (or the tick's), else the base
+// budget raised by the scene's largest joint iteration hint. Also clears the
+// scene's residual accumulators and joint hints for the next tick.
+__global__ void k_scene_budgets(Dev d, StepParams sp) {
+    for (uint32_t s = grid_stride_begin(); s < d.n_scenes; s += grid_stride()) {
+        const uint32_t req = d.scene_iters[s] ? d.scene_iters[s] : sp.requested;
+        uint32_t budget = sp.realtime ? 8u : (req ? req : sp.budget_request);
+        if (!sp.realtime && req == 0) budget = max(budget, d.scene_jiters[s]);
+        budget = min(max(budget, 1u), kMaxIterations);
+        d.scene_budget[s] = budget;
+        d.scene_jiters[s] = 0;
+        d.scene_res_sq[s] = 0.0f;
+        d.scene_res_mx[s] = 0.0f;
+        d.scene_res_n[s] = 0;
+        atomicMax(&d.ctr->budget_max, budget);
+    }
+}
+void launch_scene_budgets(const Dev& d, const StepParams& sp, cudaStream_t s) {
+    if (d.n_scenes <= 1) return;
+    k_scene_budgets<<<blocks_for(d.n_scenes), kBlock, 0, s>>>(d, sp);
+    ++g_kernel_launches;
 }
 
 __global__ void k_graph_fill(Dev d) {

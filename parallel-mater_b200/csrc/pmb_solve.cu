@@ -397,10 +397,20 @@ struct Res {
 
 // advance_duals for one contact point (geometry_constraints_solve.slang:
 // 494-532; the last-iteration block runs in k_contact_finalize).
-__device__ void dual_contact(const Dev& d, uint32_t c, float dt, uint32_t phase, Res& res) {
+__device__ void dual_contact(const Dev& d, uint32_t c, float dt, uint32_t phase, Res& res, uint32_t it) {
     const uint2 ab = d.c_bodies[c];
     const uint32_t a = ab.x, b = ab.y;
     if (phase != 0 && d.impact[a] == 0 && d.impact[b] == 0) return;
+    // Batched worlds: a scene past its budget is finished; its last sweep
+    // feeds the scene's residual.
+    uint32_t scene = 0;
+    bool scene_last = false;
+    if (batched(d)) {
+        scene = d.scene_of[a];
+        const uint32_t budget = d.scene_budget[scene];
+        if (it >= budget) return;
+        scene_last = phase == 0 && it + 1 == budget;  // the tick's residual is the pose phase's
+    }
     const Lite A = load_lite(d, a), B = load_lite(d, b);
     const float friction = sqrtf(d.p1[a].x * d.p1[b].x);
     const float beta = (1.0f / (fmx(d.p0[a].x + d.p0[b].x, 1.0e-6f) * dt * dt)) * 100.0f;
@@ -429,21 +439,47 @@ __device__ void dual_contact(const Dev& d, uint32_t c, float dt, uint32_t phase,
         res.sq += double(v) * double(v);
         res.n += 1;
         res.mx = fmx(res.mx, v);
+        if (scene_last) {
+            atomicAdd(&d.scene_res_sq[scene], v * v);
+            atomicAdd(&d.scene_res_n[scene], 1u);
+            atomicMax(reinterpret_cast<int*>(&d.scene_res_mx[scene]), __float_as_int(v));
+        }
     }
 }
 
-__device__ void dual_joint(const Dev& d, uint32_t j, uint32_t phase, float dt, Res& res) {
+__device__ void dual_joint(const Dev& d, uint32_t j, uint32_t phase, float dt, Res& res, uint32_t it) {
     JointState js = d.jstate[j];
     if (js.count == 0 || !js.enabled) return;
     const uint32_t a = js.dense_a, b = js.dense_b;
     if (phase != 0 && d.impact[a] == 0 && d.impact[b] == 0) return;
+    uint32_t scene = 0;
+    bool scene_last = false;
+    if (batched(d)) {
+        scene = d.scene_of[a];
+        const uint32_t budget = d.scene_budget[scene];
+        if (it >= budget) return;
+        scene_last = it + 1 == budget;
+    }
     float impulse = 0.0f;
     if (phase == 0) {
         BodyView A = load_body(d, a), B = load_body(d, b);
         Blk scratch;
+        // A batched world also needs this joint's own residual for its scene.
+        Res jr{0.0, 0u, 0.0f};
+        Res& sink = batched(d) ? jr : res;
         impulse = visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]),
-                              q4(d.q[b]), d.p0[a], d.p0[b], dt, &scratch, true, kVisitAdvance, nullptr, &res.sq,
-                              &res.n, &res.mx);
+                              q4(d.q[b]), d.p0[a], d.p0[b], dt, &scratch, true, kVisitAdvance, nullptr, &sink.sq,
+                              &sink.n, &sink.mx);
+        if (batched(d)) {
+            res.sq += jr.sq;
+            res.n += jr.n;
+            res.mx = fmx(res.mx, jr.mx);
+        }
+        if (scene_last && jr.n) {
+            atomicAdd(&d.scene_res_sq[scene], float(jr.sq));
+            atomicAdd(&d.scene_res_n[scene], jr.n);
+            atomicMax(reinterpret_cast<int*>(&d.scene_res_mx[scene]), __float_as_int(fmx(jr.mx, 0.0f)));
+        }
     } else {
         const Lite A = load_lite(d, a), B = load_lite(d, b);
         for (uint32_t r = 0; r < js.count; ++r) {
@@ -479,8 +515,11 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev d, StepParams sp
     uint32_t budget = sp.budget_request;
     if (!sp.realtime && sp.requested == 0) budget = max(budget, c->joint_iters);
     if (phase != 0 && sp.tolerance > 0.0f) budget = c->budget;
-    const bool adaptive = phase == 0 && sp.tolerance > 0.0f;
-    const uint32_t iters = adaptive ? min(max(sp.max_iterations, 1u), kMaxIterations) : min(budget, kMaxIterations);
+    // Batched worlds sweep every scene its own budget (no residual-driven stop).
+    const bool adaptive = phase == 0 && sp.tolerance > 0.0f && !batched(d);
+    const uint32_t iters = batched(d) ? min(c->budget_max, kMaxIterations)
+                                      : adaptive ? min(max(sp.max_iterations, 1u), kMaxIterations)
+                                                 : min(budget, kMaxIterations);
     const uint32_t n_con = c->n_contacts;
     __shared__ double wsq[kSolveThreads / 32];
     __shared__ uint32_t wn[kSolveThreads / 32];
@@ -500,6 +539,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev d, StepParams sp
             for (uint32_t k = b0 + group; k < b1; k += groups) {
                 const uint32_t i = d.corder[k];
                 if (phase != 0 && d.impact[i] == 0) continue;
+                if (batched(d) && it >= d.scene_budget[d.scene_of[i]]) continue;
                 solve_body_group(d, i, phase, dt, sm, gmask, gl, gbase, timing && it == 0 && col + 1 == colors);
             }
             if (timing && it == 0 && col < 18) {
@@ -510,8 +550,8 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev d, StepParams sp
             if (timing && it == 0 && col < 18 && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_release[col] = now();
         }
         Res res{0.0, 0u, 0.0f};
-        for (uint32_t k = grid_stride_begin(); k < n_con; k += grid_stride()) dual_contact(d, k, dt, phase, res);
-        for (uint32_t j = grid_stride_begin(); j < d.nj; j += grid_stride()) dual_joint(d, j, phase, dt, res);
+        for (uint32_t k = grid_stride_begin(); k < n_con; k += grid_stride()) dual_contact(d, k, dt, phase, res, it);
+        for (uint32_t j = grid_stride_begin(); j < d.nj; j += grid_stride()) dual_joint(d, j, phase, dt, res, it);
         // Deterministic reduction: warp tree, warps in order, blocks in order.
         for (int o = 16; o > 0; o >>= 1) {
             res.sq += __shfl_xor_sync(0xffffffffu, res.sq, o);

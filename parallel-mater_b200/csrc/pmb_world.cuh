@@ -41,6 +41,7 @@ struct Counters {
     uint32_t impact, status, changed, rounds;
     uint32_t bar_count, bar_gen, budget, joint_iters;
     float hs, residual, pad1, pad2;
+    uint32_t budget_max;  // batched scenes: the largest scene budget of the tick
     uint32_t color_count[kMaxColors];
     uint32_t color_off[kMaxColors + 1];
     uint32_t color_cursor[kMaxColors];
@@ -116,6 +117,19 @@ struct Dev {
     // per-tick inputs, cleared by the predictor that consumes them
     float4 *force, *torque, *lin_imp, *ang_imp;
     float4 *tgt_x, *tgt_q;  // kinematic target (w of tgt_x: 1 = set)
+    // Batched independent scenes (n_scenes > 1): bodies of scene s are the
+    // contiguous range [scene_body_off[s], scene_body_off[s+1]). Bodies of
+    // different scenes never pair: grid buckets are keyed by scene, large
+    // bodies are listed per scene, and every scene sweeps its own budget.
+    uint32_t n_scenes;
+    uint32_t* scene_of;          // per body
+    uint32_t* scene_body_off;    // n_scenes + 1
+    uint32_t *scene_large_count, *scene_large_off, *scene_large_cursor, *scene_large_list;
+    uint32_t* scene_iters;       // requested iterations per scene (0: base, raised by joint hints)
+    uint32_t* scene_jiters;      // per tick: largest joint iteration hint
+    uint32_t* scene_budget;      // per tick: the scene's sweeps
+    float *scene_res_sq, *scene_res_mx;  // per tick: residual of the scene's last sweep
+    uint32_t* scene_res_n;
     // warm-start table: per contact point, lambda (x, y, z rows) and penalty
     float4* warm_table;  // 2 per contact: lambda, penalty
     uint32_t warm_count, warm_rows;
@@ -219,6 +233,8 @@ __device__ __forceinline__ bool grid_sync(Counters* c) {
 
 // Host-side stage launchers (defined in the .cu files).
 void launch_broadphase(const Dev& d, cudaStream_t s);
+void launch_scene_budgets(const Dev& d, const StepParams& sp, cudaStream_t s);
+__device__ __forceinline__ bool batched(const Dev& d) { return d.n_scenes > 1; }
 void launch_narrowphase(const Dev& d, const StepParams& sp, cudaStream_t s);
 void launch_prepare(const Dev& d, const StepParams& sp, cudaStream_t s);
 void launch_graph(const Dev& d, const StepParams& sp, cudaStream_t s, int coop_blocks);

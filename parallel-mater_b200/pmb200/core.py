@@ -38,7 +38,9 @@ class WorldDesc(ctypes.Structure):
                 ("candidate_capacity", ctypes.c_uint32), ("pair_capacity", ctypes.c_uint32),
                 ("contact_capacity", ctypes.c_uint32), ("device", ctypes.c_int32),
                 ("persistent_memory", ctypes.c_void_p), ("persistent_bytes", ctypes.c_uint64),
-                ("scratch_memory", ctypes.c_void_p), ("scratch_bytes", ctypes.c_uint64)]
+                ("scratch_memory", ctypes.c_void_p), ("scratch_bytes", ctypes.c_uint64),
+                ("scene_count", ctypes.c_uint32), ("body_scene", ctypes.c_void_p),
+                ("scene_iterations", ctypes.c_void_p)]
 
 
 class WorldCapacity(ctypes.Structure):
@@ -80,6 +82,7 @@ def lib():
             "pmb_world_write_states": [vp, u32, u32, vp],
             "pmb_world_copy_states_to_device": [vp, u32, u32, vp], "pmb_world_stream": [vp, vp],
             "pmb_world_joints": [vp, vp, vp, vp, u32],
+            "pmb_world_scene_stats": [vp, vp, vp, vp, vp, u32],
             "pmb_world_contact_duals": [vp, u32, vp, vp, u32, vp],
             "pmb_world_mlp_attach": [vp, vp, u32], "pmb_world_mlp_train": [vp, i32, ctypes.c_float, u32],
             "pmb_world_mlp_params": [vp, vp, vp, vp, vp], "pmb_world_mlp_apply_mode": [vp, u32], "pmb_world_mlp_rows": [vp, vp, vp, u32, vp],
@@ -147,6 +150,14 @@ class World:
         b, st, vo, v, io, i, j = self._keep
         d = WorldDesc(len(b), _p(b), _p(st), len(vo) - 1, _p(vo), _p(v), _p(io), _p(i), len(j), _p(j),
                       candidate_capacity, pair_capacity, contact_capacity, device)
+        if s.body_scene is not None:
+            bs = np.ascontiguousarray(s.body_scene, np.uint32)
+            si = np.ascontiguousarray(s.scene_iterations if s.scene_iterations is not None
+                                      else np.zeros(int(bs.max()) + 1), np.uint32)
+            self._keep += [bs, si]
+            d.scene_count = len(si)
+            d.body_scene = _p(bs)
+            d.scene_iterations = _p(si)
         h = ctypes.c_void_p()
         _check(L.pmb_world_create(ctypes.byref(d), ctypes.byref(h)), "pmb_world_create")
         self.h = h
@@ -256,6 +267,14 @@ class World:
         _check(lib().pmb_world_joints(self.h, flags.ctypes.data, applied.ctypes.data, counts.ctypes.data,
                                       max(j, 1)), "pmb_world_joints")
         return flags[:j], applied[:j], counts[:j]
+
+    def scene_stats(self):
+        """Per scene of a batched world: (residual RMS, residual max, sweeps, contact points)."""
+        ns = len(self.scene.scene_iterations)
+        rms, mx = np.zeros(ns, np.float32), np.zeros(ns, np.float32)
+        its, cts = np.zeros(ns, np.uint32), np.zeros(ns, np.uint32)
+        _check(lib().pmb_world_scene_stats(self.h, _p(rms), _p(mx), _p(its), _p(cts), ns), "pmb_world_scene_stats")
+        return rms, mx, its, cts
 
     def mlp_attach(self, params=None, seed=1):
         p = None if params is None else np.ascontiguousarray(params, np.float32)

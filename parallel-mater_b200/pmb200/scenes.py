@@ -73,6 +73,8 @@ class Scene:
     name: str = ""
     iterations: int = 10
     profile: int = LEGACY
+    body_scene: np.ndarray | None = None        # batched worlds: scene of each body (u32, contiguous)
+    scene_iterations: np.ndarray | None = None  # batched worlds: requested iterations per scene
 
     @property
     def n(self) -> int:
@@ -226,7 +228,7 @@ def pyramid(levels=10, seed=1, jitter=1e-3, friction=0.5, density=1000.0, iterat
 
 
 def box_pile(grid=(16, 16, 16), seed=2, spacing=1.8, iterations=10, profile=LEGACY,
-             wall_height=None) -> Scene:
+             wall_height=None, count=None) -> Scene:
     """Random boxes (edges U[0.5,1.5] per axis, density U[500,2000], friction
     U[0.3,0.8]) on a jittered grid (gx along x, gy layers along y, gz along z)
     above a static walled container sized to the grid footprint. Walls are
@@ -246,6 +248,7 @@ def box_pile(grid=(16, 16, 16), seed=2, spacing=1.8, iterations=10, profile=LEGA
         b.body(wall_x, STATIC, (s * (half_x + 0.5), 0.5 * wall_height, 0.0))
         b.body(wall_z, STATIC, (0.0, 0.5 * wall_height, s * (half_z + 0.5)))
     n = gx * gy * gz
+    limit = n if count is None else min(n, count)
     edges = rng.uniform(0.5, 1.5, (n, 3)).astype(np.float32)
     density = rng.uniform(500.0, 2000.0, n)
     friction = rng.uniform(0.3, 0.8, n).astype(np.float32)
@@ -254,6 +257,8 @@ def box_pile(grid=(16, 16, 16), seed=2, spacing=1.8, iterations=10, profile=LEGA
     for y in range(gy):
         for z in range(gz):
             for x in range(gx):
+                if k >= limit:
+                    break
                 half = 0.5 * edges[k]
                 m = b.mesh(*box_mesh(half))
                 mass = float(density[k] * np.prod(edges[k].astype(np.float64)))
@@ -317,6 +322,65 @@ def cube_pair(profile=REALTIME) -> Scene:
     b.body(m, STATIC, (0.0, -1.0, 0.0), **common)
     b.body(m, DYNAMIC, (0.0, 2.0, 0.0), **common)
     return b.build("cube pair", 10, profile)
+
+
+def batch(parts, name="batch") -> Scene:
+    """Independent scenes stepped as one batched world: bodies, meshes and
+    joints concatenated (indices offset), each body tagged with its scene.
+    All parts share one profile; each keeps its own requested iterations."""
+    profile = parts[0].profile
+    assert all(p.profile == profile for p in parts)
+    bodies, states, joints, verts, idx, scene = [], [], [], [], [], []
+    voff, ioff = [0], [0]
+    mesh_base = body_base = 0
+    for k, p in enumerate(parts):
+        b = p.bodies.copy()
+        b["mesh"] += mesh_base
+        bodies.append(b)
+        states.append(p.states)
+        if len(p.joints):
+            j = p.joints.copy()
+            j["body_a"] += body_base
+            j["body_b"] += body_base
+            joints.append(j)
+        for m in range(len(p.mesh_vertex_offsets) - 1):
+            v0, v1 = p.mesh_vertex_offsets[m], p.mesh_vertex_offsets[m + 1]
+            i0, i1 = p.mesh_index_offsets[m], p.mesh_index_offsets[m + 1]
+            verts.append(p.vertices[v0:v1])
+            idx.append(p.indices[i0:i1])
+            voff.append(voff[-1] + int(v1 - v0))
+            ioff.append(ioff[-1] + int(i1 - i0))
+        scene.append(np.full(p.n, k, np.uint32))
+        mesh_base += len(p.mesh_vertex_offsets) - 1
+        body_base += p.n
+    return Scene(np.concatenate(bodies), np.concatenate(states), np.array(voff, np.uint32),
+                 np.concatenate(verts).astype(np.float32), np.array(ioff, np.uint32),
+                 np.concatenate(idx).astype(np.uint32),
+                 np.concatenate(joints) if joints else np.zeros(0, JOINT_DTYPE), name,
+                 max(p.iterations for p in parts), profile, np.concatenate(scene),
+                 np.array([p.iterations for p in parts], np.uint32))
+
+
+def batched_scenes(count=1024, seed=5, smallest=16, largest=2048, profile=LEGACY):
+    """Config-5 mix: `count` independent scenes, body counts log-uniform in
+    [smallest, largest], each a random box pile (config-2 distributions, 10
+    iterations) or a set of joint chains (config-3 distributions, 16 links
+    and an end box per chain, 20 iterations), 50/50."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    sizes = np.exp(rng.uniform(math.log(smallest), math.log(largest), count)).astype(int)
+    kinds = rng.uniform(0.0, 1.0, count) < 0.5
+    parts = []
+    for k in range(count):
+        n = int(sizes[k])
+        sub = seed * 100000 + k
+        if kinds[k]:
+            side = max(1, int(round(n ** (1.0 / 3.0))))
+            layers = int(math.ceil(n / (side * side)))
+            parts.append(box_pile((side, layers, side), seed=sub, spacing=1.6, profile=profile,
+                                  wall_height=max(4.0, 0.75 * layers), count=n))
+        else:
+            parts.append(chains(count=max(1, n // 17), links=16, seed=sub, profile=profile))
+    return batch(parts, f"batch{count}")
 
 
 def config(index: int) -> Scene:

@@ -202,3 +202,22 @@ def test_chain_scene_shapes():
     flags, applied, counts = w.joints()
     assert (counts == 3).all() and (flags & 1).all()
     assert np.isfinite(w.states()["x"]).all()
+
+
+def test_scene_batch_concatenates_independent_scenes():
+    parts = [scenes.pyramid(levels=3), scenes.chains(count=2, links=3), scenes.box_pile((2, 2, 2), seed=1)]
+    b = scenes.batch(parts)
+    assert b.n == sum(p.n for p in parts)
+    assert list(np.bincount(b.body_scene)) == [p.n for p in parts]
+    assert list(b.scene_iterations) == [p.iterations for p in parts]
+    assert len(b.mesh_vertex_offsets) - 1 == sum(len(p.mesh_vertex_offsets) - 1 for p in parts)
+    # joints stay inside their scene
+    sa, sb = b.body_scene[b.joints["body_a"]], b.body_scene[b.joints["body_b"]]
+    assert np.array_equal(sa, sb) and (sa == 1).all()
+    # body k of part 1 keeps its mesh geometry
+    off = parts[0].n
+    m = b.bodies["mesh"][off]
+    m0 = parts[1].bodies["mesh"][0]
+    v = b.vertices[b.mesh_vertex_offsets[m]:b.mesh_vertex_offsets[m + 1]]
+    v0 = parts[1].vertices[parts[1].mesh_vertex_offsets[m0]:parts[1].mesh_vertex_offsets[m0 + 1]]
+    assert np.array_equal(v, v0)
