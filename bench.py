@@ -204,6 +204,8 @@ def gpu_arm(args):
 
     for _ in range(args.warmup):
         world.step(plain, stats=False)
+    # Pick the solve launch plan on this workload (state restored afterwards).
+    plan_v, plan_p, _ = world.autotune(plain, ticks=3)
     world.snapshot()
 
     # ---- online training of the warm-start MLP on plain ticks (untimed)
@@ -305,6 +307,8 @@ def gpu_arm(args):
                                         "steps_per_frame": args.mlp_steps, "seconds": round(train_s, 2),
                                         "loss_over_plain_loss": mlp_loss / mlp_plain_loss if mlp_plain_loss else None,
                                         "gate_open": bool(mlp_gate)},
+                       "launch_plan": {"solve_threads": [512, 384, 256][plan_v],
+                                       "lanes_per_body": "8/16/32 by colour" if plan_p == 0 else "8"},
                        "parallelism": f"replicas x{world_size}",
                        "l2": "inputs larger than L2: per-tick working set ~%d MB (126 MB L2)" % int(
                            (mean(learned_stats, "contacts") * (8 + 9) * 16 + scene.n * 400 + 1.2e6 * 24) / 1e6)},

@@ -349,6 +349,20 @@ PMB_API int pmb_mlp_forward_backward(int32_t device, uint32_t rows, const float*
 PMB_API int pmb_world_scene_stats(pmb_world* world, float* residual, float* residual_max, uint32_t* iterations,
                                   uint32_t* contacts, uint32_t capacity);
 
+/* ---- launch plan ----
+ * How the cooperative solve kernel is launched: solve_variant 0, 1, 2 = 512,
+ * 384, 256 threads per CTA (one CTA per SM; fewer threads leave each thread
+ * more registers); solve_policy 0 = 8, 16 or 32 lanes per body chosen per
+ * colour by its size, 1 = always 8. Every plan computes bit-identical
+ * results; only the speed differs. A new world starts with (1, 0). */
+PMB_API int pmb_world_set_launch_plan(pmb_world* world, uint32_t solve_variant, uint32_t solve_policy);
+/* Time `ticks` ticks of every plan from the current state (restored before
+ * each plan and at the end, so the world does not advance), keep the fastest
+ * and report it; `report` receives one line per plan. Needs snapshot
+ * storage (not for worlds in caller-owned memory). */
+PMB_API int pmb_world_autotune(pmb_world* world, const pmb_step_desc* step, uint32_t ticks,
+                               uint32_t* solve_variant, uint32_t* solve_policy, char* report, uint32_t capacity);
+
 /* The CUDA stream (cudaStream_t) the world enqueues its work on. */
 PMB_API int pmb_world_stream(pmb_world* world, void** stream);
 

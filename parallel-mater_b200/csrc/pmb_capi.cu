@@ -79,7 +79,7 @@ struct pmb_world {
     bool counting{};
     std::vector<pmb_joint> host_joints;
     std::vector<void*> snapshot;
-    int coop_solve{}, coop_color{};
+    int coop_solve[kSolveVariants]{}, coop_color{};
     cudaGraphExec_t graph{};
     uint32_t step_parity{}, snapshot_parity{};
     Counters host_ctr{};
@@ -570,8 +570,13 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     std::vector<float> sorted = expand;
     std::nth_element(sorted.begin(), sorted.begin() + n / 2, sorted.end());
     d.large_extent = 2.0f * sorted[n / 2] * 4.0f;
-    cudaFuncSetAttribute(solve_kernel_ptr, cudaFuncAttributeMaxDynamicSharedMemorySize, int(solve_kernel_smem));
-    w->coop_solve = coop_blocks_for(solve_kernel_ptr, solve_kernel_threads, solve_kernel_smem);
+    d.solve_variant = 1;  // 384 threads: the fastest plan on a settled 65k-box pile
+    d.solve_policy = 0;
+    for (uint32_t v = 0; v < kSolveVariants; ++v) {
+        const SolveVariant& sv = solve_variants[v];
+        cudaFuncSetAttribute(sv.ptr, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sv.smem));
+        w->coop_solve[v] = coop_blocks_for(sv.ptr, sv.threads, sv.smem);
+    }
     w->coop_color = coop_blocks_for(color_kernel_ptr, kBlock, 0);
     // A world in caller-bound memory allocates nothing, so it has no
     // snapshot storage (pmb_world_snapshot reports FEATURE_NOT_PRESENT).
@@ -1247,6 +1252,62 @@ int pmb_world_scene_stats(pmb_world* w, float* residual, float* residual_max, ui
         if (contacts) contacts[k] = per_scene[k];
     }
     return PMB_SUCCESS;
+}
+
+int pmb_world_set_launch_plan(pmb_world* w, uint32_t solve_variant, uint32_t solve_policy) {
+    if (!w || solve_variant >= kSolveVariants || solve_policy > 1) return PMB_ERROR_INVALID_ARGUMENT;
+    w->d.solve_variant = solve_variant;
+    w->d.solve_policy = solve_policy;
+    return PMB_SUCCESS;
+}
+
+int pmb_world_autotune(pmb_world* w, const pmb_step_desc* step, uint32_t ticks, uint32_t* solve_variant,
+                       uint32_t* solve_policy, char* report, uint32_t capacity) {
+    if (!w || !step || ticks == 0) return PMB_ERROR_INVALID_ARGUMENT;
+    if (w->snapshot.size() != w->dynamic_state.size()) return PMB_ERROR_FEATURE_NOT_PRESENT;
+    cudaSetDevice(w->device);
+    int r = pmb_world_snapshot(w);
+    if (r) return r;
+    const StepParams sp = params_from(*step);
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float best = 0.0f;
+    uint32_t bv = 0, bp = 0;
+    std::string text;
+    for (uint32_t v = 0; v < kSolveVariants && r == PMB_SUCCESS; ++v)
+        for (uint32_t p = 0; p < 2 && r == PMB_SUCCESS; ++p) {
+            r = pmb_world_restore(w);
+            if (r) break;
+            w->d.solve_variant = v;
+            w->d.solve_policy = p;
+            enqueue_step(w, sp);  // untimed: first launch of this plan
+            cudaEventRecord(a, w->stream);
+            for (uint32_t k = 0; k < ticks; ++k) enqueue_step(w, sp);
+            cudaEventRecord(b, w->stream);
+            r = check(cudaEventSynchronize(b));
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, a, b);
+            char line[128];
+            std::snprintf(line, sizeof(line), "solve %3d threads, widths %s: %8.3f ms/tick\n",
+                          solve_variants[v].threads, p ? "8      " : "8/16/32", ms / float(ticks));
+            text += line;
+            if ((v == 0 && p == 0) || ms < best) {
+                best = ms;
+                bv = v;
+                bp = p;
+            }
+        }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    const int rr = pmb_world_restore(w);
+    if (r == PMB_SUCCESS) r = rr;
+    w->d.solve_variant = bv;
+    w->d.solve_policy = bp;
+    if (solve_variant) *solve_variant = bv;
+    if (solve_policy) *solve_policy = bp;
+    if (report && capacity) std::snprintf(report, capacity, "%s", text.c_str());
+    return r;
 }
 
 int pmb_world_stream(pmb_world* w, void** stream) {

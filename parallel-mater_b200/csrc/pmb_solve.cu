@@ -10,6 +10,8 @@
 // last-iteration work (accumulated impulses, re-anchoring sliding contacts) is
 // applied after the loop from the final duals and the stick flag each dual
 // pass stores, which is the same arithmetic on the same values.
+#include <type_traits>
+
 #include "pmb_joint.cuh"
 
 namespace pmb {
@@ -110,42 +112,53 @@ __device__ __forceinline__ void apply_pose_update(const Dev& d, uint32_t i, cons
     d.dxa[i] = make_float4(2.0f * rel.x, 2.0f * rel.y, 2.0f * rel.z, 0.0f);
 }
 
-// Group-per-body primal: 8 lanes solve one body, 4 bodies per warp, so a
-// whole colour of a large pile is in flight at once. Lanes evaluate the
-// body's contact rows 8 at a time (coalesced SoA loads) and stage them in
-// shared memory; each lane owns 3-4 of the 27 entries of the packed 6x6 block
-// (21 Hessian, 6 gradient) and adds the staged rows to them in list order.
-// Every entry thus sees exactly the additions, in exactly the order, of the
-// serial per-body loop of geometry_constraints_solve.slang:339-400, and the
-// block is bit-identical to it; the LDL^T solve then runs in registers. The
-// crossing safeguard reuses the staged normal rows: its error term is the
-// same expression at the same displacements.
-constexpr int kGroup = 8;
+// Group-per-body primal: G lanes (G = 8, 16 or 32) solve one body. Lanes
+// evaluate the body's contact rows G at a time (coalesced SoA loads) and
+// stage them in shared memory; each lane owns ceil(27/G) of the 27 entries of
+// the packed 6x6 block (21 Hessian, 6 gradient) and adds the staged rows to
+// them in list order. Every entry thus sees exactly the additions, in exactly
+// the order, of the serial per-body loop of
+// geometry_constraints_solve.slang:339-400, whatever G is, and the block is
+// bit-identical to it; the LDL^T solve then runs in registers. The crossing
+// safeguard reuses the staged normal rows: its error term is the same
+// expression at the same displacements.
+//
+// G is chosen per colour: 8 lanes when the colour has more bodies than the
+// grid has 16-lane groups, else 16, or 32 when even 32-lane groups cover it.
+// The tail colours of a pile hold few but heavily loaded bodies (tens of
+// rows), and a colour ends when its slowest body does, so wider groups
+// there shorten the critical path.
 constexpr uint32_t kNormSlots = 32;
-constexpr int kSolveThreads = 512;
-constexpr int kGroupsPerBlock = kSolveThreads / kGroup;
-struct GroupRows {
-    float r[kGroup][3][8];      // chunk being accumulated: 3 rows of (jacobian[6], stiffness, force)
+template <int G> struct GroupRows {
+    float r[G][3][8];           // chunk being accumulated: 3 rows of (jacobian[6], stiffness, force)
     float nrow[kNormSlots][8];  // normal row: jacobian[6], raw penalty, trial force
-    uint32_t flag[kGroup];
+    uint32_t flag[G];
 };
+// Per-warp staging area: four 8-lane groups, two 16-lane groups or one
+// 32-lane group.
+constexpr size_t kWarpStage = 4 * sizeof(GroupRows<8>);
+static_assert(2 * sizeof(GroupRows<16>) <= kWarpStage && sizeof(GroupRows<32>) <= kWarpStage, "staging area");
 
 __device__ __forceinline__ void entry_ik(int e, int& i, int& k) {
     i = e >= 15 ? 5 : e >= 10 ? 4 : e >= 6 ? 3 : e >= 3 ? 2 : e >= 1 ? 1 : 0;
     k = e - i * (i + 1) / 2;
 }
 
-// Lane gl owns entries gl, gl+8, gl+16, gl+24 (those below 27).
-__device__ __forceinline__ void gather_block(const float ent[4], Blk& blk, uint32_t gmask, int gbase) {
+// Lane gl owns entries gl, gl+G, gl+2G, ... (those below 27).
+template <int G> struct Owned {
+    static constexpr int E = (27 + G - 1) / G;
+};
+template <int G>
+__device__ __forceinline__ void gather_block(const float* ent, Blk& blk, uint32_t gmask, int gbase) {
 #pragma unroll
-    for (int e = 0; e < 21; ++e) blk.h[e] = __shfl_sync(gmask, ent[e / 8], gbase + (e % 8));
+    for (int e = 0; e < 21; ++e) blk.h[e] = __shfl_sync(gmask, ent[e / G], gbase + (e % G));
 #pragma unroll
-    for (int r = 0; r < 6; ++r) blk.g[r] = __shfl_sync(gmask, ent[(21 + r) / 8], gbase + ((21 + r) % 8));
+    for (int r = 0; r < 6; ++r) blk.g[r] = __shfl_sync(gmask, ent[(21 + r) / G], gbase + ((21 + r) % G));
 }
-__device__ __forceinline__ void own_entries(const Blk& blk, int gl, float ent[4]) {
+template <int G> __device__ __forceinline__ void own_entries(const Blk& blk, int gl, float* ent) {
 #pragma unroll
-    for (int m = 0; m < 4; ++m) {
-        const int e = gl + 8 * m;
+    for (int m = 0; m < Owned<G>::E; ++m) {
+        const int e = gl + G * m;
         float v = 0.0f;
 #pragma unroll
         for (int q = 0; q < 21; ++q) v = e == q ? blk.h[q] : v;
@@ -155,37 +168,48 @@ __device__ __forceinline__ void own_entries(const Blk& blk, int gl, float ent[4]
     }
 }
 
-__device__ __forceinline__ void accumulate_chunk(float ent[4], int gl, const GroupRows& sm, uint32_t m) {
+template <int G>
+__device__ __forceinline__ void accumulate_chunk(float* ent, int gl, const GroupRows<G>& sm, uint32_t m) {
     // Products first (independent, pipelined loads), then the ordered adds.
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int e = gl + 8 * q;
+    for (int q = 0; q < Owned<G>::E; ++q) {
+        const int e = gl + G * q;
         if (e >= 27) continue;
         int ei = 0, ek = 0;
         const bool hess = e < 21;
         if (hess) entry_ik(e, ei, ek);
         else ei = e - 21;
-        float prod[kGroup][3];
+        if (G <= 8) {
+            float prod[G][3];
 #pragma unroll
-        for (int t = 0; t < kGroup; ++t)
+            for (int t = 0; t < G; ++t)
 #pragma unroll
-            for (int x = 0; x < 3; ++x) {
-                const float* row = sm.r[t][x];
-                prod[t][x] = hess ? row[6] * row[ei] * row[ek] : row[ei] * row[7];
-            }
+                for (int x = 0; x < 3; ++x) {
+                    const float* row = sm.r[t][x];
+                    prod[t][x] = hess ? row[6] * row[ei] * row[ek] : row[ei] * row[7];
+                }
 #pragma unroll
-        for (int t = 0; t < kGroup; ++t)
+            for (int t = 0; t < G; ++t)
 #pragma unroll
-            for (int x = 0; x < 3; ++x)
-                if (t < int(m)) ent[q] += prod[t][x];
+                for (int x = 0; x < 3; ++x)
+                    if (t < int(m)) ent[q] += prod[t][x];
+        } else {
+            for (int t = 0; t < int(m); ++t)
+#pragma unroll
+                for (int x = 0; x < 3; ++x) {
+                    const float* row = sm.r[t][x];
+                    ent[q] += hess ? row[6] * row[ei] * row[ek] : row[ei] * row[7];
+                }
+        }
     }
 }
 
-__device__ __forceinline__ void accumulate_crossing(float ent[4], int gl, const GroupRows& sm, uint32_t s0,
+template <int G>
+__device__ __forceinline__ void accumulate_crossing(float* ent, int gl, const GroupRows<G>& sm, uint32_t s0,
                                                     uint32_t m) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int e = gl + 8 * q;
+    for (int q = 0; q < Owned<G>::E; ++q) {
+        const int e = gl + G * q;
         if (e >= 27) continue;
         int ei = 0, ek = 0;
         if (e < 21) entry_ik(e, ei, ek);
@@ -200,9 +224,10 @@ __device__ __forceinline__ void accumulate_crossing(float ent[4], int gl, const 
 
 // Rows of one contact for body i into chunk slot `slot`; its normal row,
 // raw penalty and normal trial also go to nrow[nslot].
+template <int G>
 __device__ __forceinline__ void stage_contact(const Dev& d, const Lite& me, float my_friction, uint32_t code,
-                                              uint32_t other_body, uint32_t phase, float dt, GroupRows& sm, int slot,
-                                              int nslot) {
+                                              uint32_t other_body, uint32_t phase, float dt, GroupRows<G>& sm,
+                                              int slot, int nslot) {
     const uint32_t c = code & 0x7fffffffu;
     const bool first = (code >> 31) == 0;
     const Lite other = load_lite(d, other_body);
@@ -250,8 +275,9 @@ __device__ __forceinline__ unsigned long long gtimer() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-__device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float dt, GroupRows& sm, uint32_t gmask,
-                                 int gl, int gbase, bool trace = false) {
+template <int G>
+__device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float dt, GroupRows<G>& sm,
+                                 uint32_t gmask, int gl, int gbase, bool trace = false) {
     const unsigned long long t0 = trace ? gtimer() : 0ull;
     auto mark = [&](int k) {
         if (trace && gl == 0) atomicMax(&d.ctr->dbg_body[k], gtimer() - t0);
@@ -259,7 +285,7 @@ __device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float
     const Lite me = load_lite(d, i);
     const float my_friction = d.p1[i].x;
     const uint32_t ro = d.roff[i], rn = d.rcount[i];
-    float ent[4];
+    float ent[Owned<G>::E];
     {
         const float4 ia = d.inA[i], ib = d.inB[i];
         float H[21];
@@ -275,8 +301,8 @@ __device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float
         H[bidx(5, 4)] = ib.y;
         H[bidx(5, 5)] = ib.z;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int e = gl + 8 * q;
+        for (int q = 0; q < Owned<G>::E; ++q) {
+            const int e = gl + G * q;
             float v = 0.0f;
 #pragma unroll
             for (int k = 0; k < 21; ++k) v = e == k ? H[k] : v;
@@ -290,18 +316,18 @@ __device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float
             ent[q] = v;
         }
     }
-    for (uint32_t base = 0; base < rn; base += kGroup) {
+    for (uint32_t base = 0; base < rn; base += G) {
         const uint32_t sidx = base + gl;
         if (sidx < rn)
-            stage_contact(d, me, my_friction, d.blist[ro + sidx], d.bother[ro + sidx], phase, dt, sm, gl,
-                          sidx < kNormSlots ? int(sidx) : -1);
+            stage_contact<G>(d, me, my_friction, d.blist[ro + sidx], d.bother[ro + sidx], phase, dt, sm, gl,
+                             sidx < kNormSlots ? int(sidx) : -1);
         __syncwarp(gmask);
-        accumulate_chunk(ent, gl, sm, min(uint32_t(kGroup), rn - base));
+        accumulate_chunk<G>(ent, gl, sm, min(uint32_t(G), rn - base));
         __syncwarp(gmask);
     }
     mark(0);
     Blk blk;
-    gather_block(ent, blk, gmask, gbase);
+    gather_block<G>(ent, blk, gmask, gbase);
     mark(1);
     const uint32_t jcnt = d.jdeg[i];
     if (jcnt) {
@@ -336,13 +362,13 @@ __device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float
     if (!block_solve(blk, upd)) return;
     mark(2);
     // Crossing safeguard (geometry_constraints_solve.slang:433-475).
-    own_entries(blk, gl, ent);
+    own_entries<G>(blk, gl, ent);
     bool crossing = false;
-    for (uint32_t base = 0; base < rn; base += kGroup) {
+    for (uint32_t base = 0; base < rn; base += G) {
         const uint32_t sidx = base + gl;
         if (rn > kNormSlots && base >= kNormSlots && sidx < rn)
-            stage_contact(d, me, my_friction, d.blist[ro + sidx], d.bother[ro + sidx], phase, dt, sm, -1,
-                          int(sidx % kNormSlots));
+            stage_contact<G>(d, me, my_friction, d.blist[ro + sidx], d.bother[ro + sidx], phase, dt, sm, -1,
+                             int(sidx % kNormSlots));
         __syncwarp(gmask);
         uint32_t flag = 0;
         if (sidx < rn) {
@@ -357,13 +383,13 @@ __device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float
         __syncwarp(gmask);
         if (__any_sync(gmask, flag)) {
             crossing = true;
-            accumulate_crossing(ent, gl, sm, base % kNormSlots, min(uint32_t(kGroup), rn - base));
+            accumulate_crossing<G>(ent, gl, sm, base % kNormSlots, min(uint32_t(G), rn - base));
         }
         __syncwarp(gmask);
     }
     mark(3);
     if (crossing) {
-        gather_block(ent, blk, gmask, gbase);
+        gather_block<G>(ent, blk, gmask, gbase);
         V6 safe;
         if (block_solve(blk, safe)) upd = safe;
     }
@@ -502,14 +528,18 @@ __device__ __forceinline__ void atomic_max_pos(float* addr, float v) {
     atomicMax(reinterpret_cast<int*>(addr), __float_as_int(fmx(v, 0.0f)));
 }
 
-__global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev d, StepParams sp, uint32_t phase) {
+// T threads per CTA, one CTA per SM (cooperative): 512 threads cap a thread
+// at 128 registers, 384 at 168, 256 at 255 -- fewer resident warps against
+// fewer spills; the world picks one (pmb_world_autotune).
+template <int T>
+__global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t phase) {
+    constexpr int kSolveThreads = T;
     Counters* c = d.ctr;
     if (phase != 0 && c->impact == 0) return;
-    extern __shared__ GroupRows rows[];
+    extern __shared__ __align__(16) uint8_t stage_raw[];
     const int lane = threadIdx.x & 31;
-    const int gl = lane % kGroup, gbase = lane - gl;
-    const uint32_t gmask = 0xffu << gbase;
-    GroupRows& sm = rows[threadIdx.x / kGroup];
+    uint8_t* warp_stage = stage_raw + (threadIdx.x >> 5) * kWarpStage;
+    const uint32_t tid = blockIdx.x * kSolveThreads + threadIdx.x, nthreads = gridDim.x * kSolveThreads;
     const float dt = sp.dt;
     const uint32_t colors = c->colors;
     uint32_t budget = sp.budget_request;
@@ -524,8 +554,6 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev d, StepParams sp
     __shared__ double wsq[kSolveThreads / 32];
     __shared__ uint32_t wn[kSolveThreads / 32];
     __shared__ float wmx[kSolveThreads / 32];
-    const uint32_t group = (blockIdx.x * kSolveThreads + threadIdx.x) / kGroup;
-    const uint32_t groups = gridDim.x * kGroupsPerBlock;
     const bool timing = sp.debug_timing && phase == 0;
     auto now = [] {
         unsigned long long t;
@@ -536,12 +564,28 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev d, StepParams sp
     for (uint32_t it = 0; it < iters; ++it) {
         for (uint32_t col = 0; col < colors; ++col) {
             const uint32_t b0 = c->color_off[col], b1 = c->color_off[col + 1];
-            for (uint32_t k = b0 + group; k < b1; k += groups) {
-                const uint32_t i = d.corder[k];
-                if (phase != 0 && d.impact[i] == 0) continue;
-                if (batched(d) && it >= d.scene_budget[d.scene_of[i]]) continue;
-                solve_body_group(d, i, phase, dt, sm, gmask, gl, gbase, timing && it == 0 && col + 1 == colors);
-            }
+            const uint32_t nb = b1 - b0;
+            const bool last_colour = timing && it == 0 && col + 1 == colors;
+            auto sweep = [&](auto width) {
+                constexpr int G = decltype(width)::value;
+                const int gl = lane % G, gbase = lane - gl;
+                const uint32_t gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << gbase;
+                GroupRows<G>& sm = reinterpret_cast<GroupRows<G>*>(warp_stage)[gbase / G];
+                const uint32_t groups = nthreads / G;
+                for (uint32_t k = b0 + tid / G; k < b1; k += groups) {
+                    const uint32_t i = d.corder[k];
+                    if (phase != 0 && d.impact[i] == 0) continue;
+                    if (batched(d) && it >= d.scene_budget[d.scene_of[i]]) continue;
+                    solve_body_group<G>(d, i, phase, dt, sm, gmask, gl, gbase, last_colour);
+                }
+            };
+            // Widths: see the group-per-body comment; policy 1 keeps 8 lanes.
+            if (d.solve_policy == 0 && nb * 32u <= nthreads)
+                sweep(std::integral_constant<int, 32>{});
+            else if (d.solve_policy == 0 && nb * 16u <= nthreads)
+                sweep(std::integral_constant<int, 16>{});
+            else
+                sweep(std::integral_constant<int, 8>{});
             if (timing && it == 0 && col < 18) {
                 __syncthreads();
                 if (threadIdx.x == 0) atomicMax(&c->dbg_work[col], now());
@@ -608,9 +652,11 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev d, StepParams sp
     }
 }
 
-const void* solve_kernel_ptr = reinterpret_cast<const void*>(&k_solve);
-const int solve_kernel_threads = kSolveThreads;
-const size_t solve_kernel_smem = sizeof(GroupRows) * kGroupsPerBlock;
+const SolveVariant solve_variants[kSolveVariants] = {
+    {reinterpret_cast<const void*>(&k_solve<512>), 512, kWarpStage * (512 / 32)},
+    {reinterpret_cast<const void*>(&k_solve<384>), 384, kWarpStage * (384 / 32)},
+    {reinterpret_cast<const void*>(&k_solve<256>), 256, kWarpStage * (256 / 32)},
+};
 
 // Last-iteration contact work (geometry_constraints_solve.slang:533-561),
 // one thread per contact point.
@@ -898,7 +944,10 @@ __global__ void k_cache_save(Dev d, StepParams sp) {
     }
 }
 
-void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, int coop_blocks, const SolveBuffers& o) {
+void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, const int* coop_blocks,
+                      const SolveBuffers& o) {
+    const SolveVariant& sv = solve_variants[d.solve_variant < kSolveVariants ? d.solve_variant : 0];
+    const int coop = coop_blocks[d.solve_variant < kSolveVariants ? d.solve_variant : 0];
     const uint32_t pb = blocks_for(d.cap_pair > d.nj ? d.cap_pair : d.nj);
     for (uint32_t phase = 0; phase < (sp.realtime ? 1u : 2u); ++phase) {
         if (phase != 0) {
@@ -916,7 +965,7 @@ void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, int co
         StepParams spp = sp;
         void* args[] = {&dd, &spp, &ph};
         solve_timer_begin(s);
-        cudaLaunchCooperativeKernel(solve_kernel_ptr, dim3(coop_blocks), dim3(kSolveThreads), args, solve_kernel_smem, s);
+        cudaLaunchCooperativeKernel(sv.ptr, dim3(coop), dim3(sv.threads), args, sv.smem, s);
         ++g_kernel_launches;
         solve_timer_end(s);
         prof_mark(s, phase ? "solve phase 1" : "solve phase 0");

@@ -117,6 +117,9 @@ struct Dev {
     // per-tick inputs, cleared by the predictor that consumes them
     float4 *force, *torque, *lin_imp, *ang_imp;
     float4 *tgt_x, *tgt_q;  // kinematic target (w of tgt_x: 1 = set)
+    // Launch plan (pmb_world_autotune): solve kernel variant, colour width
+    // policy (0: 8/16/32 lanes per body by colour size, 1: always 8).
+    uint32_t solve_variant, solve_policy;
     // Batched independent scenes (n_scenes > 1): bodies of scene s are the
     // contiguous range [scene_body_off[s], scene_body_off[s+1]). Bodies of
     // different scenes never pair: grid buckets are keyed by scene, large
@@ -240,7 +243,8 @@ void launch_prepare(const Dev& d, const StepParams& sp, cudaStream_t s);
 void launch_graph(const Dev& d, const StepParams& sp, cudaStream_t s, int coop_blocks);
 struct SolveBuffers { float4 *ox, *oq, *ov, *ow; };
 void launch_integrate(const Dev& d, const StepParams& sp, cudaStream_t s, const SolveBuffers& o);
-void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, int coop_blocks, const SolveBuffers& o);
+void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, const int* coop_blocks,
+                      const SolveBuffers& o);
 void launch_body_constants(const Dev& d, const float4* lo, const float4* hi, const float4* sph, cudaStream_t s);
 void launch_finish(const Dev& d, const StepParams& sp, cudaStream_t s);
 void scan_u32(const uint32_t* in, uint32_t* out, const uint32_t* count_ptr, uint32_t capacity, uint32_t* total,
@@ -256,9 +260,14 @@ extern unsigned long long g_kernel_launches;
 // Dominant-kernel timing: brackets each solve launch with CUDA events when on.
 void solve_timer_begin(cudaStream_t s);
 void solve_timer_end(cudaStream_t s);
-extern const void* solve_kernel_ptr;
-extern const int solve_kernel_threads;
-extern const size_t solve_kernel_smem;
+// Cooperative solve kernel variants (threads per CTA) and their smem.
+struct SolveVariant {
+    const void* ptr;
+    int threads;
+    size_t smem;
+};
+constexpr uint32_t kSolveVariants = 3;
+extern const SolveVariant solve_variants[kSolveVariants];
 void launch_contact_jacobians(const Dev& d, uint32_t phase, cudaStream_t s);
 // Sparse per-body record writes staged in io_index / io_rec (kind 0: inputs,
 // 1: kinematic targets, 2: states), and AoS state packing into `dst`.

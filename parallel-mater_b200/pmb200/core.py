@@ -83,6 +83,7 @@ def lib():
             "pmb_world_copy_states_to_device": [vp, u32, u32, vp], "pmb_world_stream": [vp, vp],
             "pmb_world_joints": [vp, vp, vp, vp, u32],
             "pmb_world_scene_stats": [vp, vp, vp, vp, vp, u32],
+            "pmb_world_set_launch_plan": [vp, u32, u32], "pmb_world_autotune": [vp, vp, u32, vp, vp, vp, u32],
             "pmb_world_contact_duals": [vp, u32, vp, vp, u32, vp],
             "pmb_world_mlp_attach": [vp, vp, u32], "pmb_world_mlp_train": [vp, i32, ctypes.c_float, u32],
             "pmb_world_mlp_params": [vp, vp, vp, vp, vp], "pmb_world_mlp_apply_mode": [vp, u32], "pmb_world_mlp_rows": [vp, vp, vp, u32, vp],
@@ -267,6 +268,19 @@ class World:
         _check(lib().pmb_world_joints(self.h, flags.ctypes.data, applied.ctypes.data, counts.ctypes.data,
                                       max(j, 1)), "pmb_world_joints")
         return flags[:j], applied[:j], counts[:j]
+
+    def set_launch_plan(self, solve_variant=0, solve_policy=0):
+        _check(lib().pmb_world_set_launch_plan(self.h, solve_variant, solve_policy), "pmb_world_set_launch_plan")
+
+    def autotune(self, desc=None, ticks=3, **kw):
+        """Time every launch plan over `ticks` ticks (state restored), keep
+        the fastest; returns (solve_variant, solve_policy, report)."""
+        d = np.ascontiguousarray(self.scene.step_desc(**kw) if desc is None else desc)
+        v, p = ctypes.c_uint32(), ctypes.c_uint32()
+        buf = ctypes.create_string_buffer(4096)
+        _check(lib().pmb_world_autotune(self.h, d.ctypes.data, ticks, ctypes.byref(v), ctypes.byref(p), buf, 4096),
+               "pmb_world_autotune")
+        return v.value, p.value, buf.value.decode()
 
     def scene_stats(self):
         """Per scene of a batched world: (residual RMS, residual max, sweeps, contact points)."""

@@ -153,3 +153,29 @@ def test_residual_schedule_matches_oracle(gpu_available):
         assert sg["iterations"] == so["iterations"], f
         np.testing.assert_allclose(w.residual_trace(), o.residual_trace(), rtol=1e-5, atol=1e-9)
         assert abs(float(sg["residual_max"]) - float(so["residual_max"])) <= 1e-6 + 1e-5 * abs(float(so["residual_max"]))
+
+
+def test_launch_plans_are_bit_identical(gpu_available):
+    """Every solve launch plan (CTA size, lanes per body) computes the same
+    bits; the autotuner only picks among them and leaves the state as it
+    found it."""
+    s = scenes.box_pile((6, 4, 6), seed=13, spacing=1.6)
+    ref = None
+    for v in range(3):
+        for p in range(2):
+            w = core.World(s)
+            w.set_launch_plan(v, p)
+            for _ in range(12):
+                w.step()
+            x = w.states().view(np.uint8).copy()
+            if ref is None:
+                ref = x
+            assert np.array_equal(x, ref), (v, p)
+            w.close()
+    w = core.World(s)
+    for _ in range(5):
+        w.step()
+    before = w.states().view(np.uint8).copy()
+    v, p, report = w.autotune(ticks=2)
+    assert report.count("ms/tick") == 6
+    assert np.array_equal(w.states().view(np.uint8), before)
