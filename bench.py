@@ -58,6 +58,11 @@ def parse():
     ap.add_argument("--train-frames", type=int, default=200, help="plain ticks of online MLP training")
     ap.add_argument("--mlp-lr", type=float, default=3e-3)
     ap.add_argument("--mlp-steps", type=int, default=4, help="Adam steps per training frame")
+    ap.add_argument("--workload", default="pile65k", choices=["pile65k", "batched"],
+                    help="pile65k: the 65,536-box pile (default); batched: 1,024 independent scenes")
+    ap.add_argument("--scenes", type=int, default=1024, help="batched: scene count")
+    ap.add_argument("--settle", type=int, default=120, help="batched: plain ticks from the spawn before timing")
+    ap.add_argument("--cpu-scenes", type=int, default=48, help="batched: scenes in the CPU baseline sample")
     return ap.parse_args()
 
 
@@ -329,9 +334,260 @@ def gpu_arm(args):
         dist.destroy_process_group()
 
 
+BATCH_METRIC = "scene-steps/sec, 1,024 independent scenes (log-uniform 16-2048 bodies, piles and chains) per CUDA-graph tick"
+BATCH_SEED = 5
+BATCH_PROFILE = os.path.join(ROOT, "profiles", "k_solve_batch1024.md")
+
+
+def batch_cpu_sample(count, ids):
+    """CPU restatement (oracle/, one core) stepping each sampled scene on its
+    own for one tick from the spawn; a batched world evolves every scene
+    exactly as that scene stepped alone, so this is the same work."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from pmb200 import scenes
+    sizes, kinds = scenes.batched_plan(count, BATCH_SEED)
+    parts = [scenes.batched_part(k, sizes[k], kinds[k], BATCH_SEED) for k in ids]
+    bodies = sum(p.n for p in parts)
+    elapsed = 0.0
+    for p in parts:
+        w = O.OracleWorld(p)
+        t0 = time.perf_counter()
+        w.step(p.step_desc())
+        elapsed += time.perf_counter() - t0
+    return len(parts) / elapsed, bodies
+
+
+def batch_cpu_ids(count, want):
+    """A bounded CPU sample: every (count // want)-th scene."""
+    stride = max(1, count // max(1, want))
+    return list(range(0, count, stride))[:want]
+
+
+def reference_batched(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    ids = batch_cpu_ids(args.scenes, args.cpu_scenes)
+    value, bodies = batch_cpu_sample(args.scenes, ids)
+    line = {
+        "impl": "reference", "metric": BATCH_METRIC, "value": value, "unit": "scene-steps/s",
+        "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": 1e3 * args.scenes / value,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{args.scenes} independent scenes (config-5 mix, seed {BATCH_SEED}), first tick "
+                               "from the spawn, per-scene iterations (piles 10, chains 20)"},
+        "cpu_baseline": {"value": value, "unit": "scene-steps/s", "cores": 1, "kind": "port",
+                         "sample": f"{len(ids)} of {args.scenes} scenes ({bodies} bodies), one tick each, stepped "
+                                   "alone by the CPU restatement of the reference's serial Slang CPU driver"},
+        "e2e": {"value": value, "unit": "scene-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def gpu_batched(args):
+    """Config 5: the scenes are bin-packed over the ranks by body count; each
+    rank steps its shard as one batched world, one CUDA-graph replay per two
+    ticks, after settling from the spawn with the warm-start MLP trained
+    online on the last --train-frames settling ticks. Arms: plain and learned
+    warm start at the scenes' fixed iteration counts, from one snapshot."""
+    import torch
+    import torch.distributed as dist
+    from pmb200 import core, scenes, shard
+
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world_size > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    sizes, kinds = scenes.batched_plan(args.scenes, BATCH_SEED)
+    mine = scenes.shard_scenes(sizes, world_size)[rank]
+    scene = scenes.batched_scenes(args.scenes, BATCH_SEED, subset=mine)
+    n_scenes = len(mine)
+    dyn = scene.bodies["motion"] == scenes.DYNAMIC
+    n_dyn = np.bincount(scene.body_scene[dyn], minlength=n_scenes)
+    plain = scene.step_desc()
+    learned = scene.step_desc(warm_start=1)
+    world = core.World(scene, device=local, contact_capacity=args.contact_capacity)
+    stream = torch.cuda.Stream()             # a capturable (non-default) stream for the graph
+    world.set_stream(stream.cuda_stream)
+    steps = args.steps + (args.steps & 1)
+
+    def barrier():
+        if world_size > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        t = torch.tensor([x], device="cuda")
+        if world_size > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- settle from the spawn; MLP trained online on the last frames (untimed)
+    t0 = time.perf_counter()
+    train = min(args.train_frames, args.settle)
+    for _ in range(args.settle - train):
+        world.step(plain, stats=False)
+    world.mlp_attach(seed=1)
+    world.mlp_train(True, lr=args.mlp_lr, steps_per_tick=args.mlp_steps)
+    for _ in range(train):
+        world.step(plain, stats=False)
+    _, mlp_loss, mlp_plain_loss, mlp_gate = world.mlp_params()
+    world.mlp_train(False)
+    for _ in range(args.warmup):
+        world.step(plain, stats=False)
+    status = int(world.step(plain)["status"])
+    if status:
+        raise RuntimeError("batched world status: %s" % core.status_names(status))
+    settle_s = time.perf_counter() - t0
+    plan_v, plan_p, _ = world.autotune(plain, ticks=3)
+    world.snapshot()
+
+    def graph_arm(desc):
+        world.restore()
+        l0 = core.kernel_launches()
+        world.capture(steps=2, desc=desc)
+        per_replay = core.kernel_launches() - l0
+        world.restore()
+        world.replay()                       # untimed: first replay uploads the graph
+        world.restore()
+        barrier()
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(steps // 2):
+            world.replay()
+        end.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(start.elapsed_time(end)), per_replay * (steps // 2)
+
+    plain_ms, _ = graph_arm(plain)
+    sampler = ClockSampler(local)
+    sampler.start()
+    learned_ms, launches = graph_arm(learned)
+    barrier()
+    clocks = sampler.stop()
+
+    def scene_trace(desc, timer=False):
+        """Per tick and scene: residual RMS, residual max, sweeps, contacts."""
+        world.restore()
+        if timer:
+            world.solve_timer(True)
+        rms, mx, its, cts = [], [], [], []
+        for _ in range(steps):
+            st = world.step(desc)
+            if int(st["status"]):
+                raise RuntimeError("batched world status: %s" % core.status_names(int(st["status"])))
+            r, m, i, c = world.scene_stats()
+            rms.append(r), mx.append(m), its.append(i), cts.append(c)
+        solve = world.solve_timer(False) if timer else (0.0, 0)
+        return np.array(rms), np.array(mx), np.array(its), np.array(cts), solve
+
+    p_rms, p_mx, p_its, p_cts, _ = scene_trace(plain)
+    l_rms, l_mx, l_its, l_cts, (solve_ms, solve_launches) = scene_trace(learned, timer=True)
+    # phase-0 algorithmic bytes of k_solve (per sweep: 124 B per dynamic body,
+    # 384 B per contact point), summed over scenes and ticks
+    alg_bytes = float(np.sum(l_its * (124.0 * n_dyn[None, :] + 384.0 * l_cts)))
+    achieved = alg_bytes / (solve_ms * 1e-3) / 1e9 if solve_ms > 0 else None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak, peak_src = float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        peak, peak_src = 6650.0, "fallback"
+    traffic = None
+    try:
+        with open(BATCH_PROFILE) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    traffic = float(line.split(":")[1])
+    except (OSError, ValueError):
+        pass
+
+    # ---- end to end through the C ABI with host buffers (learned arm)
+    world.restore()
+    host = torch.empty((scene.n, 13), dtype=torch.float32, pin_memory=True)
+    host_np = host.numpy().view(scenes.STATE_DTYPE).reshape(-1)
+    host_np[:] = world.states()
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        world.set_states(host_np)
+        world.step(learned, stats=False)
+        host_np[:] = world.states()
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+
+    # per-scene metrics of every rank, in global scene order
+    per_scene = np.stack([p_rms.mean(0), l_rms.mean(0), p_mx.max(0), l_mx.max(0),
+                          p_its.mean(0), l_cts.mean(0), n_dyn], axis=1).astype(np.float64)
+    allm = shard.gather_by_scene(mine, per_scene, args.scenes, world_size)
+    bodies_all = shard.gather_by_scene(mine, np.bincount(scene.body_scene, minlength=n_scenes), args.scenes,
+                                       world_size)
+    total_bodies = int(bodies_all.sum())
+    cpu = None
+    if rank == 0 and world_size == 1 and args.cpu_scenes > 0:
+        ids = batch_cpu_ids(args.scenes, args.cpu_scenes)
+        cv, cb = batch_cpu_sample(args.scenes, ids)
+        cpu = {"value": cv, "unit": "scene-steps/s", "cores": 1, "kind": "port",
+               "sample": f"{len(ids)} of {args.scenes} scenes ({cb} bodies), first tick from the spawn, each "
+                         "stepped alone by the serial CPU restatement (oracle/)"}
+    if rank == 0:
+        value = args.scenes * steps / (learned_ms * 1e-3)
+        plain_value = args.scenes * steps / (plain_ms * 1e-3)
+        sweeps = float(np.sum(allm[:, 4] * allm[:, 6]))       # sweeps x dynamic bodies, per tick
+        ratio = allm[:, 1] / np.maximum(allm[:, 0], 1e-30)
+        has = allm[:, 0] > 0
+        line = {
+            "metric": BATCH_METRIC, "value": value, "unit": "scene-steps/s", "n_gpus": world_size,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": learned_ms / steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"{args.scenes} independent scenes, body counts log-uniform [16,2048], "
+                                   "box piles (10 sweeps) and joint chains (20 sweeps) 50/50, seed 5; legacy "
+                                   f"profile; {args.settle} settling ticks from the spawn, then timed",
+                       "bodies": total_bodies, "scenes_per_rank": n_scenes,
+                       "tick": "one CUDA graph replay per 2 ticks",
+                       "body_updates_per_s": sweeps * value / args.scenes,
+                       "plain_scene_steps_per_s": plain_value, "learned_over_plain": value / plain_value,
+                       "residual_rms_median_plain": float(np.median(allm[has, 0])) if has.any() else None,
+                       "residual_rms_median_learned": float(np.median(allm[has, 1])) if has.any() else None,
+                       "residual_max_plain": float(allm[:, 2].max()),
+                       "residual_max_learned": float(allm[:, 3].max()),
+                       "scenes_learned_at_or_below_plain": int(np.sum(ratio[has] <= 1.0)),
+                       "scenes_with_contacts": int(has.sum()),
+                       "mlp_training": {"frames": train, "adam_lr": args.mlp_lr, "steps_per_frame": args.mlp_steps,
+                                        "loss_over_plain_loss": mlp_loss / mlp_plain_loss if mlp_plain_loss else None,
+                                        "gate_open": bool(mlp_gate)},
+                       "settle_seconds": round(settle_s, 1),
+                       "launch_plan": {"solve_threads": [512, 384, 256][plan_v],
+                                       "lanes_per_body": "8/16/32 by colour" if plan_p == 0 else "8"},
+                       "parallelism": f"scenes bin-packed by body count over {world_size} GPU(s)",
+                       "l2": "inputs larger than L2 (per-tick working set several hundred MB)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "kernel": "k_solve", "launches": solve_launches,
+                         "kernel_ms_per_launch": solve_ms / max(1, solve_launches),
+                         "bytes": "phase-0 sweeps only (impact-phase sweeps timed but not counted)",
+                         "peak_source": peak_src},
+            "cpu_baseline": cpu,
+            "e2e": {"value": args.scenes * steps / e2e_s, "unit": "scene-steps/s",
+                    "h2d_bytes_per_step": total_bodies * 52, "d2h_bytes_per_step": total_bodies * 52},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    world.close()
+    if world_size > 1:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.workload == "batched":
+        (reference_batched if args.impl == "reference" else gpu_batched)(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         gpu_arm(args)

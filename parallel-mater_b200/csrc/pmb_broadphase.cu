@@ -247,7 +247,11 @@ __device__ __forceinline__ bool collision_disabled(const Dev& d, uint32_t a, uin
         if (keys[mid] < key) lo = mid + 1;
         else hi = mid;
     }
-    return lo < d.n_dis && keys[lo] == key;
+    // constrained_collision_disabled (geometry.slang:494-511): only joints
+    // that are not broken disable the pair.
+    for (; lo < d.n_dis && keys[lo] == key; ++lo)
+        if (d.jstate[d.dis_joint[lo]].broken == 0) return true;
+    return false;
 }
 
 // Candidate predicate: overlap (leaf b against query a), a != b, identity

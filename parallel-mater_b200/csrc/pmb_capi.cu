@@ -253,7 +253,7 @@ void fill_stats(const Counters& c, pmb_step_stats* s) {
 
 struct Sizes {
     uint32_t n, nm, nj, scenes;
-    size_t verts, planes, dis;
+    size_t verts, planes, dis, hinges, hinge_segs;
     uint32_t cap_cand, cap_pair, cap_contact;
 };
 struct Extra {
@@ -316,6 +316,7 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     ALLOC(d.corder, n);
     ALLOC(d.rcount, n); ALLOC(d.roff, n + 1); ALLOC(d.blist, 2 * cap_contact); ALLOC(d.bother, 2 * cap_contact);
     ALLOCP(d.joints, nj); ALLOCS(d.jstate, nj); ALLOCS(d.jrows, size_t(nj) * 18);
+    ALLOCP(d.hinge_list, z.hinges); ALLOCP(d.hinge_seg, z.hinge_segs + 1);
     {
         // Scan scratch: one slot per 2048-element tile of the longest scan plus the total.
         size_t longest = std::max<size_t>({cap_cand, grid_size, n, cap_pair});
@@ -324,7 +325,7 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     }
     ALLOCP(d.ctr, 1);
     ALLOC(e.lo, nm); ALLOC(e.hi, nm); ALLOC(e.sph, nm);
-    ALLOCP(e.dis, z.dis);
+    ALLOCP(e.dis, z.dis); ALLOCP(d.dis_joint, z.dis);
     if (z.scenes > 1) {
         const uint32_t ns = z.scenes;
         ALLOCP(d.scene_of, n); ALLOCP(d.scene_body_off, ns + 1); ALLOCP(d.scene_iters, ns); ALLOCP(d.scene_jiters, ns);
@@ -468,19 +469,46 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
         msph[m] = make_float4(pm.center[0], pm.center[1], pm.center[2], pm.radius);
     }
 
-    std::vector<uint64_t> dis_keys;
+    // Collision-disabling joints as (body pair key, joint) sorted by key then
+    // joint; a pair is filtered while any of its joints is unbroken.
+    std::vector<std::pair<uint64_t, uint32_t>> dis_entries;
     for (uint32_t j = 0; j < nj; ++j) {
         const pmb_joint& o = desc->joints[j];
         if (o.enabled && o.disable_collisions) {
             uint64_t a = std::min(o.body_a, o.body_b), b = std::max(o.body_a, o.body_b);
-            dis_keys.push_back((a << 32) | b);
+            dis_entries.push_back({(a << 32) | b, j});
         }
     }
-    std::sort(dis_keys.begin(), dis_keys.end());
-    dis_keys.erase(std::unique(dis_keys.begin(), dis_keys.end()), dis_keys.end());
+    std::sort(dis_entries.begin(), dis_entries.end());
+    std::vector<uint64_t> dis_keys(dis_entries.size());
+    std::vector<uint32_t> dis_joint(dis_entries.size());
+    for (size_t k = 0; k < dis_entries.size(); ++k) {
+        dis_keys[k] = dis_entries[k].first;
+        dis_joint[k] = dis_entries[k].second;
+    }
     const uint32_t ns = desc->scene_count > 1 ? desc->scene_count : 0u;
     d.n_scenes = ns;
-    const Sizes z{n, nm, nj, ns, verts.size(), planes.size(), dis_keys.size(), d.cap_cand, d.cap_pair, d.cap_contact};
+    // Hinge projection runs serially over hinge joints in index order; joints
+    // of different scenes touch disjoint bodies, so each scene's hinges form
+    // an independent segment.
+    std::vector<uint32_t> hinge_list, hinge_seg;
+    {
+        std::vector<std::pair<uint32_t, uint32_t>> hs;
+        for (uint32_t j = 0; j < nj; ++j)
+            if (desc->joints[j].type == kHinge) {
+                const uint32_t a = desc->joints[j].body_a;
+                hs.push_back({ns > 1 && a < n ? desc->body_scene[a] : 0u, j});
+            }
+        std::stable_sort(hs.begin(), hs.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+        for (size_t k = 0; k < hs.size(); ++k) {
+            if (k == 0 || hs[k].first != hs[k - 1].first) hinge_seg.push_back(uint32_t(k));
+            hinge_list.push_back(hs[k].second);
+        }
+        hinge_seg.push_back(uint32_t(hs.size()));
+    }
+    d.n_hinge_segs = uint32_t(hinge_seg.size() - 1);
+    const Sizes z{n, nm, nj, ns, verts.size(), planes.size(), dis_keys.size(), hinge_list.size(),
+                  hinge_seg.size() - 1, d.cap_cand, d.cap_pair, d.cap_contact};
     if (w->arena[kPersistent]) {
         // Bound memory must hold the whole layout before anything is carved.
         pmb_world probe;
@@ -544,6 +572,8 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     up(dhi, mhi.data(), 16 * nm);
     up(dsph, msph.data(), 16 * nm);
     if (nj) up(d.joints, desc->joints, sizeof(Joint) * nj);
+    up(d.hinge_list, hinge_list.data(), 4 * hinge_list.size());
+    up(d.hinge_seg, hinge_seg.data(), 4 * hinge_seg.size());
     std::vector<uint32_t> scene_off, scene_iters;
     if (ns > 1) {
         scene_off.assign(ns + 1, 0);
@@ -555,7 +585,10 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
         up(d.scene_body_off, scene_off.data(), 4 * size_t(ns + 1));
         up(d.scene_iters, scene_iters.data(), 4 * size_t(ns));
     }
-    if (!dis_keys.empty()) up(dis, dis_keys.data(), 8 * dis_keys.size());
+    if (!dis_keys.empty()) {
+        up(dis, dis_keys.data(), 8 * dis_keys.size());
+        up(d.dis_joint, dis_joint.data(), 4 * dis_joint.size());
+    }
     std::vector<uint32_t> colors(n, kInvalid);
     up(d.color, colors.data(), 4 * n);
     launch_body_constants(d, dlo, dhi, dsph, s);
@@ -992,6 +1025,8 @@ int pmb_world_memory_requirements(const pmb_world_capacity* c, uint64_t* persist
                   0u,
                   size_t(c->mesh_vertex_count),
                   2 * size_t(c->mesh_triangle_count),
+                  size_t(c->joint_count),
+                  size_t(c->joint_count),
                   size_t(c->joint_count),
                   c->candidate_capacity ? c->candidate_capacity : 64u * n + 4096u,
                   c->pair_capacity ? c->pair_capacity : 24u * n + 1024u,

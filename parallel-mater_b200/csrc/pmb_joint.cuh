@@ -181,24 +181,33 @@ static __device__ float visit_joint(const Joint& o, JointRow* rows, const BodyVi
     V3 arm_a = rotate(qa, la), arm_b = rotate(qb, lb);
     V3 error = sub(add(xb, arm_b), add(xa, arm_a));
     V3 old_error = sub(add(prev_xb, rotate(prev_qb, lb)), add(prev_xa, rotate(prev_qa, la)));
-    Q4 frame_a = qnormalize(qmul(qa, fa_l)), frame_b = qnormalize(qmul(qb, fb_l));
-    Q4 old_a = qnormalize(qmul(prev_qa, fa_l)), old_b = qnormalize(qmul(prev_qb, fb_l));
-    V3 twist = rotation_vector(qrelative(frame_a, frame_b, true));
-    V3 old_twist = rotation_vector(qrelative(old_a, old_b, true));
+    const Q4 frame_a = qnormalize(qmul(qa, fa_l)), old_a = qnormalize(qmul(prev_qa, fa_l));
     const uint32_t t = o.type;
-    bool swing = t == kHinge || t == kPiston || (t == kMotor && o.motor_angular != 0);
-    V3 free_axis = t == kHinge ? V3{0, 0, 1} : V3{1, 0, 0};
-    V3 swing_axis = inv_rotate(frame_a, rotate(frame_b, free_axis));
-    V3 old_swing = inv_rotate(old_a, rotate(old_b, free_axis));
-    V3 rotation = swing ? cross(free_axis, swing_axis) : twist;
-    V3 old_rotation = swing ? cross(free_axis, old_swing) : old_twist;
+    // A point joint has three linear lock rows and no angular row, so its
+    // visit skips the relative-rotation terms (same values for every row it
+    // does emit).
+    const bool angular_rows = t != kPoint;
+    const bool swing = t == kHinge || t == kPiston || (t == kMotor && o.motor_angular != 0);
+    const V3 free_axis = t == kHinge ? V3{0, 0, 1} : V3{1, 0, 0};
+    V3 twist{0, 0, 0}, old_twist{0, 0, 0}, swing_axis{0, 0, 0}, rotation{0, 0, 0}, old_rotation{0, 0, 0};
+    Q4 frame_b{0, 0, 0, 1}, old_b{0, 0, 0, 1};
+    if (angular_rows) {
+        frame_b = qnormalize(qmul(qb, fb_l));
+        old_b = qnormalize(qmul(prev_qb, fb_l));
+        twist = rotation_vector(qrelative(frame_a, frame_b, true));
+        old_twist = rotation_vector(qrelative(old_a, old_b, true));
+        swing_axis = inv_rotate(frame_a, rotate(frame_b, free_axis));
+        const V3 old_swing = inv_rotate(old_a, rotate(old_b, free_axis));
+        rotation = swing ? cross(free_axis, swing_axis) : twist;
+        old_rotation = swing ? cross(free_axis, old_swing) : old_twist;
+    }
     float lin_pen = 1.0f / (fmx(pa0.x + pb0.x, 1.0e-6f) * dt * dt);
     const bool generic = t == kGeneric || t == kGenericSpring;
     const bool motor_type = t == kMotor;
     for (unsigned axis = 0; axis < 3; ++axis) {
         V3 dir = rotate(frame_a, unit_axis(axis));
         V3 old_dir = rotate(old_a, unit_axis(axis));
-        for (unsigned av = 0; av < 2; ++av) {
+        for (unsigned av = 0; av < (angular_rows ? 2u : 1u); ++av) {
             bool angular = av != 0;
             bool lock = angular ? (t == kFixed || t == kSlider || (t == kHinge && axis != 2) ||
                                    (t == kPiston && axis != 0) ||
@@ -214,9 +223,11 @@ static __device__ float visit_joint(const Joint& o, JointRow* rows, const BodyVi
             const float* spr_c = angular ? o.ang_damping : o.lin_damping;
             float current = angular ? comp(rotation, axis) : dot(error, dir);
             float old_current = angular ? comp(old_rotation, axis) : dot(old_error, old_dir);
-            V3 ang_axis = swing ? rotate(frame_a, sub(mul(unit_axis(axis), dot(free_axis, swing_axis)),
-                                                      mul(free_axis, comp(swing_axis, axis))))
-                                : log_axis(frame_a, twist, axis);
+            V3 ang_axis{0, 0, 0};
+            if (angular)
+                ang_axis = swing ? rotate(frame_a, sub(mul(unit_axis(axis), dot(free_axis, swing_axis)),
+                                                       mul(free_axis, comp(swing_axis, axis))))
+                                 : log_axis(frame_a, twist, axis);
             V6 ja = angular ? jac(V3{0, 0, 0}, mul(ang_axis, -1.0f))
                             : jac(mul(dir, -1.0f), add(mul(cross(arm_a, dir), -1.0f), cross(dir, error)));
             V6 jb = angular ? jac(V3{0, 0, 0}, ang_axis) : jac(dir, cross(arm_b, dir));

@@ -806,13 +806,16 @@ __global__ void k_apply(Dev d, StepParams sp, uint32_t phase, float4* ox, float4
     }
 }
 
-// rigid_avbd_project_hinge_anchors (geometry_constraints_solve.slang:174-209),
-// serial over joints as in the reference.
+// rigid_avbd_project_hinge_anchors (geometry_constraints_solve.slang:174-209):
+// serial over the hinge joints in index order, as in the reference. One
+// thread per scene segment (scenes of a batched world share no bodies).
 __global__ void k_project_hinges(Dev d, float4* ox, const float4* oq) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    for (uint32_t j = 0; j < d.nj; ++j) {
+    const uint32_t seg = blockIdx.x * blockDim.x + threadIdx.x;
+    if (seg >= d.n_hinge_segs) return;
+    for (uint32_t h = d.hinge_seg[seg]; h < d.hinge_seg[seg + 1]; ++h) {
+        const uint32_t j = d.hinge_list[h];
         const JointState st = d.jstate[j];
-        if (st.count == 0 || !st.enabled || d.joints[j].type != kHinge) continue;
+        if (st.count == 0 || !st.enabled) continue;
         const uint32_t a = st.dense_a, b = st.dense_b;
         const float ima = d.motion[a] == kDynamic ? d.p0[a].x : 0.0f;
         const float imb = d.motion[b] == kDynamic ? d.p0[b].x : 0.0f;
@@ -979,8 +982,8 @@ void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, const 
         ++g_kernel_launches;
         k_apply<<<blocks_for(d.n), kBlock, 0, s>>>(d, sp, phase, o.ox, o.oq, o.ov, o.ow);
         ++g_kernel_launches;
-        if (phase == 0 && d.nj) {
-            k_project_hinges<<<1, 32, 0, s>>>(d, o.ox, o.oq);
+        if (phase == 0 && d.n_hinge_segs) {
+            k_project_hinges<<<blocks_for(d.n_hinge_segs), kBlock, 0, s>>>(d, o.ox, o.oq);
             ++g_kernel_launches;
         }
         prof_mark(s, phase ? "finish phase 1" : "finish phase 0");

@@ -190,7 +190,13 @@ struct Dev {
     JointState* jstate;
     JointRow* jrows;  // 18 per joint
     uint32_t* dis_keys;    // sorted (min<<32|max) keys of collision-disabling joints
+    uint32_t* dis_joint;   // the joint of each key (a pair may have several)
     uint32_t n_dis;
+    // hinge joints (ascending index) grouped by scene: segment k is
+    // hinge_list[hinge_seg[k] .. hinge_seg[k+1]); scenes share no bodies
+    uint32_t* hinge_list;
+    uint32_t* hinge_seg;
+    uint32_t n_hinge_segs;
     // scratch for scans
     uint64_t* scan_tmp;
     uint32_t* scan_tmp32;

@@ -271,6 +271,70 @@ def box_pile(grid=(16, 16, 16), seed=2, spacing=1.8, iterations=10, profile=LEGA
     return b.build(f"pile{gx}x{gy}x{gz}", iterations, profile)
 
 
+def joint_zoo(seed=6, profile=LEGACY, iterations=12, links=2) -> Scene:
+    """One rig per joint type -- fixed, point, hinge (angular limit on its
+    free axis), slider and piston (linear limit on the free axis; the piston
+    also an angular limit), generic (equality and range limits on linear and
+    angular axes), generic spring (springs on all six axes), motor (angular
+    and linear drives) -- each a static anchor and `links` dynamic 0.4 m
+    boxes in a chain started with seeded velocities, plus a point joint whose
+    breaking threshold is below the impulse that holds its box."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    b = _Builder()
+    box = b.mesh(*box_mesh((0.2, 0.2, 0.2)))
+    anchor = b.mesh(*box_mesh((0.1, 0.1, 0.1)))
+    inertia = (0.32 / 12.0,) * 3
+
+    def rig(kind, x0, setup=None, threshold=0.0):
+        prev, prev_anchor = b.body(anchor, STATIC, (x0, 6.0, 0.0)), (0.0, -0.15, 0.0)
+        for k in range(links):
+            v = tuple(float(x) for x in rng.uniform(-1.0, 1.0, 3))
+            w = tuple(float(x) for x in rng.uniform(-2.0, 2.0, 3))
+            body = b.body(box, DYNAMIC, (x0, 6.0 - 0.45 - 0.5 * k, 0.0), v=v, w=w, mass=1.0, inertia=inertia)
+            j = b.joint(kind, prev, body, prev_anchor, (0.0, 0.25, 0.0))
+            o = b.joints[j]
+            if setup:
+                setup(o)
+            o["breaking_threshold"] = threshold
+            prev, prev_anchor = body, (0.0, -0.25, 0.0)
+
+    def hinge(o):
+        o["ang_limit_axes"] = 4
+        o["ang_lower"], o["ang_upper"] = (0, 0, -0.5), (0, 0, 0.7)
+
+    def slider(o):
+        o["lin_limit_axes"] = 1
+        o["lin_lower"], o["lin_upper"] = (-0.2, 0, 0), (0.3, 0, 0)
+
+    def piston(o):
+        slider(o)
+        o["ang_limit_axes"] = 1
+        o["ang_lower"], o["ang_upper"] = (-0.4, 0, 0), (0.4, 0, 0)
+
+    def generic(o):
+        o["lin_limit_axes"], o["ang_limit_axes"] = 7, 3
+        o["lin_lower"], o["lin_upper"] = (-0.1, 0, 0), (0.2, 0, 0)
+        o["ang_lower"], o["ang_upper"] = (-0.3, 0.0, 0), (0.3, 0.0, 0)
+
+    def spring(o):
+        o["lin_spring_axes"] = o["ang_spring_axes"] = 7
+        o["lin_stiffness"], o["lin_damping"] = (200.0,) * 3, (5.0,) * 3
+        o["ang_stiffness"], o["ang_damping"] = (50.0,) * 3, (1.0,) * 3
+
+    def motor(o):
+        o["motor_angular"] = o["motor_linear"] = 1
+        o["motor_angular_velocity"], o["motor_angular_max_impulse"] = 2.0, 5.0
+        o["motor_linear_velocity"], o["motor_linear_max_impulse"] = 0.5, 3.0
+
+    kinds = [(FIXED, None), (POINT, None), (HINGE, hinge), (SLIDER, slider), (PISTON, piston),
+             (GENERIC, generic), (GENERIC_SPRING, spring), (MOTOR, motor)]
+    for k, (kind, setup) in enumerate(kinds):
+        rig(kind, (k - 4.0) * 2.0, setup)
+    rig(POINT, 8.0, threshold=0.12)
+    b.body(b.mesh(*box_mesh((12.0, 0.5, 4.0))), STATIC, (0.0, -0.5, 0.0))
+    return b.build("joint_zoo", iterations, profile)
+
+
 def chains(count=512, links=64, seed=3, radius=0.05, length=0.4, spacing=1.0,
            iterations=20, profile=LEGACY, link_density=1000.0) -> Scene:
     """``count`` chains of ``links`` capsule links joined by point joints,
@@ -361,26 +425,54 @@ def batch(parts, name="batch") -> Scene:
                  np.array([p.iterations for p in parts], np.uint32))
 
 
-def batched_scenes(count=1024, seed=5, smallest=16, largest=2048, profile=LEGACY):
-    """Config-5 mix: `count` independent scenes, body counts log-uniform in
-    [smallest, largest], each a random box pile (config-2 distributions, 10
-    iterations) or a set of joint chains (config-3 distributions, 16 links
-    and an end box per chain, 20 iterations), 50/50."""
+def batched_plan(count=1024, seed=5, smallest=16, largest=2048):
+    """Config-5 draw: body counts log-uniform in [smallest, largest] and the
+    kind of each scene (True: box pile, False: joint chains), 50/50."""
     rng = np.random.Generator(np.random.Philox(seed))
     sizes = np.exp(rng.uniform(math.log(smallest), math.log(largest), count)).astype(int)
     kinds = rng.uniform(0.0, 1.0, count) < 0.5
-    parts = []
-    for k in range(count):
-        n = int(sizes[k])
-        sub = seed * 100000 + k
-        if kinds[k]:
-            side = max(1, int(round(n ** (1.0 / 3.0))))
-            layers = int(math.ceil(n / (side * side)))
-            parts.append(box_pile((side, layers, side), seed=sub, spacing=1.6, profile=profile,
-                                  wall_height=max(4.0, 0.75 * layers), count=n))
-        else:
-            parts.append(chains(count=max(1, n // 17), links=16, seed=sub, profile=profile))
-    return batch(parts, f"batch{count}")
+    return sizes, kinds
+
+
+def batched_part(k, size, kind, seed=5, profile=LEGACY) -> Scene:
+    """Scene `k` of a config-5 batch: a random box pile (config-2
+    distributions, 10 iterations) of `size` boxes, or `size // 17` joint
+    chains (config-3 distributions, 16 links and an end box per chain, 20
+    iterations). Depends only on (k, size, kind, seed), so any subset of the
+    batch can be built on its own."""
+    n = int(size)
+    sub = seed * 100000 + int(k)
+    if kind:
+        side = max(1, int(round(n ** (1.0 / 3.0))))
+        layers = int(math.ceil(n / (side * side)))
+        return box_pile((side, layers, side), seed=sub, spacing=1.6, profile=profile,
+                        wall_height=max(4.0, 0.75 * layers), count=n)
+    return chains(count=max(1, n // 17), links=16, seed=sub, profile=profile)
+
+
+def batched_scenes(count=1024, seed=5, smallest=16, largest=2048, profile=LEGACY, subset=None):
+    """Config-5 mix: `count` independent scenes (batched_plan, batched_part)
+    as one batched world; `subset` (scene indices) builds only those."""
+    sizes, kinds = batched_plan(count, seed, smallest, largest)
+    ids = range(count) if subset is None else subset
+    parts = [batched_part(k, sizes[k], kinds[k], seed, profile) for k in ids]
+    return batch(parts, f"batch{count}" if subset is None else f"batch{count}[{len(parts)}]")
+
+
+def shard_scenes(weights, ranks):
+    """Independent scenes bin-packed over `ranks` GPUs by weight (body
+    count): longest-processing-time greedy -- heaviest scene first, each to
+    the least-loaded rank, ties to the lower rank. Returns one ascending list
+    of scene indices per rank; every scene appears exactly once."""
+    weights = np.asarray(weights, np.int64)
+    order = sorted(range(len(weights)), key=lambda k: (-int(weights[k]), k))
+    load = [0] * ranks
+    out = [[] for _ in range(ranks)]
+    for k in order:
+        r = min(range(ranks), key=lambda i: (load[i], i))
+        out[r].append(k)
+        load[r] += int(weights[k])
+    return [sorted(x) for x in out]
 
 
 def config(index: int) -> Scene:

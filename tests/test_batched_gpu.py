@@ -23,7 +23,9 @@ def _parts():
             scenes.box_pile((4, 3, 4), seed=21, spacing=1.6, count=40),
             scenes.chains(count=2, links=6, seed=4),
             scenes.box_pile((3, 3, 3), seed=22, spacing=1.6),
-            scenes.chains(count=1, links=9, seed=5, iterations=12)]
+            scenes.chains(count=1, links=9, seed=5, iterations=12),
+            scenes.joint_zoo(seed=8),
+            scenes.joint_zoo(seed=9, iterations=16)]
 
 
 def test_batch_equals_scenes_stepped_alone(gpu_available):
@@ -60,3 +62,28 @@ def test_batched_graph_replay_equals_steps(gpu_available):
     b.replay()
     b.replay()
     assert np.array_equal(a.states().view(np.uint8), b.states().view(np.uint8))
+
+
+def test_batched_learned_graph_replay_equals_steps(gpu_available):
+    """The learned warm start (features, tensor-core inference, apply) is
+    stream-ordered with no host decision, so a captured tick replays it
+    exactly; a trained MLP (gate open or not) is read from device memory."""
+    batch = scenes.batched_scenes(12, seed=5, smallest=16, largest=96)
+    a = core.World(batch)
+    b = core.World(batch)
+    for w in (a, b):
+        w.mlp_attach(seed=1)
+        w.mlp_train(True, lr=3e-3, steps_per_tick=2)
+        for _ in range(6):
+            w.step(stats=False)
+        w.mlp_train(False)
+    assert np.array_equal(a.mlp_params()[0], b.mlp_params()[0])
+    for _ in range(4):
+        st = a.step(warm_start=1)
+        assert st["status"] == 0
+    b.capture(steps=2, warm_start=1)
+    b.replay()
+    b.replay()
+    assert np.array_equal(a.states().view(np.uint8), b.states().view(np.uint8))
+    a.close()
+    b.close()

@@ -114,6 +114,29 @@ def test_small_pile_matches_oracle(gpu_available):
     print("pile worst |gpu-oracle| =", worst)
 
 
+def test_joint_zoo_matches_oracle(gpu_available):
+    """All eight joint types with limits, springs, motors, breaking and hinge
+    projection: poses within tolerance of the oracle, joint flags and row
+    counts equal every tick."""
+    s = scenes.joint_zoo()
+    w = core.World(s)
+    o = O.OracleWorld(s)
+    worst = 0.0
+    for f in range(60):
+        sg, so = w.step(), o.step()
+        assert sg["status"] == 0, core.status_names(int(sg["status"]))
+        assert sg["colors"] == so["colors"] and sg["islands"] == so["islands"], f
+        fg, ag, cg = w.joints()
+        fo, ao, co = o.joints()
+        assert np.array_equal(fg, fo) and np.array_equal(cg, co), f
+        xg, xo = w.states(), o.states()
+        err = max(np.abs(xg["x"] - xo["x"]).max(), np.abs(xg["q"] - xo["q"]).max(),
+                  np.abs(xg["v"] - xo["v"]).max())
+        worst = max(worst, err)
+        assert err < 2e-3, (f, err)
+    print("joint zoo worst |gpu-oracle| =", worst)
+
+
 def test_graph_replay_equals_steps(gpu_available):
     s = scenes.pyramid()
     a = core.World(s)

@@ -221,3 +221,21 @@ def test_scene_batch_concatenates_independent_scenes():
     v = b.vertices[b.mesh_vertex_offsets[m]:b.mesh_vertex_offsets[m + 1]]
     v0 = parts[1].vertices[parts[1].mesh_vertex_offsets[m0]:parts[1].mesh_vertex_offsets[m0 + 1]]
     assert np.array_equal(v, v0)
+
+
+def test_joint_zoo_runs_every_joint_type():
+    """Every joint type steps without non-finite state; the under-rated
+    point joints break, all others stay enabled and keep their rows."""
+    z = scenes.joint_zoo()
+    kinds = sorted(set(int(t) for t in z.joints["type"]))
+    assert kinds == list(range(8))
+    o = O.OracleWorld(z)
+    for _ in range(30):
+        st = o.step()
+        assert st["status"] == 0
+    x = o.states()
+    assert np.isfinite(x["x"]).all() and np.isfinite(x["q"]).all()
+    flags, applied, counts = o.joints()
+    breakable = z.joints["breaking_threshold"] > 0
+    assert (flags[breakable] & 2).all() and (counts[breakable] == 0).all()
+    assert (flags[~breakable] == 1).all() and (counts[~breakable] > 0).all()
