@@ -42,6 +42,7 @@ GRID = (64, 32, 32)
 SEED = 4
 SETTLED = os.path.join(ROOT, "tests", "golden", "settled_pile_64x32x32.npz")
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "k_solve_pile65k.md")
+LANE_POLICIES = ["8/16/32 by colour size", "8", "8/16/32 by body rows, heaviest first"]
 
 
 def parse():
@@ -313,7 +314,7 @@ def gpu_arm(args):
                                         "loss_over_plain_loss": mlp_loss / mlp_plain_loss if mlp_plain_loss else None,
                                         "gate_open": bool(mlp_gate)},
                        "launch_plan": {"solve_threads": [512, 384, 256][plan_v],
-                                       "lanes_per_body": "8/16/32 by colour" if plan_p == 0 else "8"},
+                                       "lanes_per_body": LANE_POLICIES[plan_p]},
                        "parallelism": f"replicas x{world_size}",
                        "l2": "inputs larger than L2: per-tick working set ~%d MB (126 MB L2)" % int(
                            (mean(learned_stats, "contacts") * (8 + 9) * 16 + scene.n * 400 + 1.2e6 * 24) / 1e6)},
@@ -562,7 +563,7 @@ def gpu_batched(args):
                                         "gate_open": bool(mlp_gate)},
                        "settle_seconds": round(settle_s, 1),
                        "launch_plan": {"solve_threads": [512, 384, 256][plan_v],
-                                       "lanes_per_body": "8/16/32 by colour" if plan_p == 0 else "8"},
+                                       "lanes_per_body": LANE_POLICIES[plan_p]},
                        "parallelism": f"scenes bin-packed by body count over {world_size} GPU(s)",
                        "l2": "inputs larger than L2 (per-tick working set several hundred MB)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

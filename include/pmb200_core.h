@@ -353,8 +353,10 @@ PMB_API int pmb_world_scene_stats(pmb_world* world, float* residual, float* resi
  * How the cooperative solve kernel is launched: solve_variant 0, 1, 2 = 512,
  * 384, 256 threads per CTA (one CTA per SM; fewer threads leave each thread
  * more registers); solve_policy 0 = 8, 16 or 32 lanes per body chosen per
- * colour by its size, 1 = always 8. Every plan computes bit-identical
- * results; only the speed differs. A new world starts with (1, 0). */
+ * colour by its size, 1 = always 8, 2 = per body by its contact rows (more
+ * than 16: 32 lanes, 9-16: 16, else 8; heaviest bodies first) unless 32-lane
+ * groups cover the whole colour. Every plan computes bit-identical results;
+ * only the speed differs. A new world starts with (1, 0). */
 PMB_API int pmb_world_set_launch_plan(pmb_world* world, uint32_t solve_variant, uint32_t solve_policy);
 /* Time `ticks` ticks of every plan from the current state (restored before
  * each plan and at the end, so the world does not advance), keep the fastest

@@ -291,6 +291,7 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     ALLOC(d.cand_count, n + 1); ALLOC(d.cand_off, n + 1);
     ALLOC(d.cand_a, cap_cand); ALLOC(d.cand_b, cap_cand);
     ALLOC(d.np_count, cap_cand); ALLOC(d.np_scan, cap_cand + 1); ALLOC(d.np_stage, cap_cand);
+    ALLOC(d.np_list, cap_cand);
     ALLOC(d.st_n, cap_contact); ALLOC(d.st_p, cap_contact);
     ALLOC(d.act_a, cap_pair); ALLOC(d.act_b, cap_pair); ALLOC(d.act_code, cap_pair);
     ALLOC(d.act_off, cap_pair + 1); ALLOC(d.act_cnt, cap_pair); ALLOC(d.act_impact, cap_pair);
@@ -1289,8 +1290,11 @@ int pmb_world_scene_stats(pmb_world* w, float* residual, float* residual_max, ui
     return PMB_SUCCESS;
 }
 
+constexpr uint32_t kSolvePolicies = 3;
+const char* const kPolicyNames[kSolvePolicies] = {"per colour", "8 lanes   ", "per body  "};
+
 int pmb_world_set_launch_plan(pmb_world* w, uint32_t solve_variant, uint32_t solve_policy) {
-    if (!w || solve_variant >= kSolveVariants || solve_policy > 1) return PMB_ERROR_INVALID_ARGUMENT;
+    if (!w || solve_variant >= kSolveVariants || solve_policy >= kSolvePolicies) return PMB_ERROR_INVALID_ARGUMENT;
     w->d.solve_variant = solve_variant;
     w->d.solve_policy = solve_policy;
     return PMB_SUCCESS;
@@ -1311,7 +1315,7 @@ int pmb_world_autotune(pmb_world* w, const pmb_step_desc* step, uint32_t ticks, 
     uint32_t bv = 0, bp = 0;
     std::string text;
     for (uint32_t v = 0; v < kSolveVariants && r == PMB_SUCCESS; ++v)
-        for (uint32_t p = 0; p < 2 && r == PMB_SUCCESS; ++p) {
+        for (uint32_t p = 0; p < kSolvePolicies && r == PMB_SUCCESS; ++p) {
             r = pmb_world_restore(w);
             if (r) break;
             w->d.solve_variant = v;
@@ -1325,7 +1329,7 @@ int pmb_world_autotune(pmb_world* w, const pmb_step_desc* step, uint32_t ticks, 
             cudaEventElapsedTime(&ms, a, b);
             char line[128];
             std::snprintf(line, sizeof(line), "solve %3d threads, widths %s: %8.3f ms/tick\n",
-                          solve_variants[v].threads, p ? "8      " : "8/16/32", ms / float(ticks));
+                          solve_variants[v].threads, kPolicyNames[p], ms / float(ticks));
             text += line;
             if ((v == 0 && p == 0) || ms < best) {
                 best = ms;

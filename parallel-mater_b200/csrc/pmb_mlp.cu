@@ -627,12 +627,12 @@ void launch_mlp_images(const float* params, uint8_t* img, cudaStream_t s) {
 }
 
 void launch_mlp_features(const Dev& d, const StepParams& sp, uint8_t* x, MlpMeta* meta, cudaStream_t s) {
-    k_mlp_features<<<blocks_for(d.cap_contact), kBlock, 0, s>>>(d, sp, x, meta);
+    k_mlp_features<<<cap_blocks(d.cap_contact), kBlock, 0, s>>>(d, sp, x, meta);
     ++g_kernel_launches;
 }
 
 void launch_mlp_targets(const Dev& d, MlpMeta* meta, cudaStream_t s) {
-    k_mlp_targets<<<blocks_for(d.cap_contact), kBlock, 0, s>>>(d, meta);
+    k_mlp_targets<<<cap_blocks(d.cap_contact), kBlock, 0, s>>>(d, meta);
     ++g_kernel_launches;
 }
 
@@ -655,7 +655,7 @@ void launch_mlp_tiles(bool train, const uint8_t* x, const MlpMeta* meta, const u
 
 void launch_mlp_apply(const Dev& d, const MlpMeta* meta, const float* out, uint32_t mode, const float* gate,
                       cudaStream_t s) {
-    k_mlp_apply<<<blocks_for(d.cap_pair), kBlock, 0, s>>>(d, meta, out, mode, gate);
+    k_mlp_apply<<<cap_blocks(d.cap_pair), kBlock, 0, s>>>(d, meta, out, mode, gate);
     ++g_kernel_launches;
 }
 

@@ -98,6 +98,36 @@ __device__ void reduce_face_patch(Man& m, float tol) {
     }
 }
 
+__device__ __forceinline__ bool same_plane(float4 a, float4 b) {
+    return __float_as_uint(a.x) == __float_as_uint(b.x) && __float_as_uint(a.y) == __float_as_uint(b.y) &&
+           __float_as_uint(a.z) == __float_as_uint(b.z) && __float_as_uint(a.w) == __float_as_uint(b.w);
+}
+
+// The separating-axis test of face_manifold alone: true exactly when some
+// reference-face plane separates the pair by more than `reach`, i.e. when
+// face_manifold's maximum separation exceeds reach and it returns an empty
+// manifold. Same arithmetic, stopping at the first separating plane.
+__device__ bool face_separated(const Pose& bs, const MeshRef& bm, const Pose& cs, const MeshRef& cm, float reach) {
+    for (uint32_t side = 0; side < 2; ++side) {
+        const MeshRef& rm = side == 0 ? cm : bm;
+        const Pose& rs = side == 0 ? cs : bs;
+        const MeshRef& im = side == 0 ? bm : cm;
+        const Pose& is = side == 0 ? bs : cs;
+        const V3 rel = sub(is.x, rs.x);
+        for (uint32_t f = 0; f < rm.nt; ++f) {
+            float4 pl = rm.planes[f];
+            if (f != 0 && same_plane(pl, rm.planes[f - 1])) continue;
+            V3 n = rotate(rs.q, v3(pl));
+            V3 in = inv_rotate(is.q, n);
+            float support = kFltMax;
+            for (uint32_t k = 0; k < im.nv; ++k) support = fminf(support, dot(in, pv(im, k)));
+            float sep = support + dot(n, rel) - pl.w;
+            if (sep > reach) return true;
+        }
+    }
+    return false;
+}
+
 // geometry.slang:1606-1745
 __device__ bool face_manifold(const Pose& bs, const MeshRef& bm, const Pose& cs, const MeshRef& cm, float margin,
                               float correction, Man& out) {
@@ -117,6 +147,9 @@ __device__ bool face_manifold(const Pose& bs, const MeshRef& bm, const Pose& cs,
         const V3 rel = sub(is.x, rs.x);
         for (uint32_t f = 0; f < rm.nt; ++f) {
             float4 pl = rm.planes[f];
+            // A plane equal to the one before it (a quad's second triangle)
+            // gives the same separation, which never wins the strict max.
+            if (f != 0 && same_plane(pl, rm.planes[f - 1])) continue;
             V3 n = rotate(rs.q, v3(pl));
             V3 in = inv_rotate(is.q, n);
             float support = kFltMax;
@@ -260,35 +293,69 @@ __device__ __forceinline__ float rotational_bound(Q4 prev, Q4 cur, float rotb) {
     return 2.0f * rotb * len(V3{d.x, d.y, d.z});
 }
 
-__global__ void __launch_bounds__(128) k_narrow(Dev d) {
+struct CandidateMotion {
+    Pose prev_a, prev_b, pred_a, pred_b;
+    float margin, corr;
+    bool swept;
+};
+__device__ __forceinline__ CandidateMotion candidate_motion(const Dev& d, uint32_t a, uint32_t b) {
+    CandidateMotion c;
+    const float4 pa2 = d.p2[a], pb2 = d.p2[b];
+    c.margin = pa2.z + pb2.z;
+    c.corr = pa2.w + pb2.w;
+    c.prev_a = {v3(d.x[a]), q4(d.q[a])};
+    c.prev_b = {v3(d.x[b]), q4(d.q[b])};
+    c.pred_a = {v3(d.tx[a]), q4(d.tq[a])};
+    c.pred_b = {v3(d.tx[b]), q4(d.tq[b])};
+    float moved = len(sub(sub(c.pred_a.x, c.prev_a.x), sub(c.pred_b.x, c.prev_b.x))) +
+                  rotational_bound(c.prev_a.q, c.pred_a.q, d.rotb[a]) +
+                  rotational_bound(c.prev_b.q, c.pred_b.q, d.rotb[b]);
+    c.swept = moved > c.margin;
+    return c;
+}
+
+// Pass 1, one thread per candidate: pairs that are not both convex, and
+// unswept pairs separated by a face plane, get an empty manifold here; the
+// rest go to the survivor list for pass 2. Light enough for full occupancy.
+__global__ void __launch_bounds__(256) k_narrow_sat(Dev d) {
     const uint32_t total = d.ctr->n_cand;
     for (uint32_t k = grid_stride_begin(); k < total; k += grid_stride()) {
         const uint32_t a = d.cand_a[k], b = d.cand_b[k];
         const uint32_t ma = d.mesh[a], mb = d.mesh[b];
-        uint32_t count = 0;
+        bool empty = !(d.m_convex[ma] && d.m_convex[mb]);
+        if (!empty) {
+            const CandidateMotion c = candidate_motion(d, a, b);
+            empty = !c.swept && face_separated(c.pred_a, mesh_ref(d, ma), c.pred_b, mesh_ref(d, mb), c.margin + c.corr);
+        }
+        if (empty) {
+            d.np_count[k] = 0;
+            d.np_scan[k] = 0ull;
+        } else {
+            d.np_list[atomicAdd(&d.ctr->n_surv, 1u)] = k;
+        }
+    }
+}
+
+// Pass 2, one thread per surviving candidate: the full face manifold
+// (swept variant first when the pair moved more than its margin).
+__global__ void __launch_bounds__(128) k_narrow(Dev d) {
+    const uint32_t total = d.ctr->n_surv;
+    for (uint32_t s = grid_stride_begin(); s < total; s += grid_stride()) {
+        const uint32_t k = d.np_list[s];
+        const uint32_t a = d.cand_a[k], b = d.cand_b[k];
+        const uint32_t ma = d.mesh[a], mb = d.mesh[b];
         Man m;
         m.count = 0;
-        const bool face = d.m_convex[ma] && d.m_convex[mb];
-        if (face) {
-            const MeshRef bm = mesh_ref(d, ma), cm = mesh_ref(d, mb);
-            const float4 pa2 = d.p2[a], pb2 = d.p2[b];
-            const float margin = pa2.z + pb2.z;
-            const float corr = pa2.w + pb2.w;
-            const Pose prev_a{v3(d.x[a]), q4(d.q[a])}, prev_b{v3(d.x[b]), q4(d.q[b])};
-            const Pose pred_a{v3(d.tx[a]), q4(d.tq[a])}, pred_b{v3(d.tx[b]), q4(d.tq[b])};
-            float moved = len(sub(sub(pred_a.x, prev_a.x), sub(pred_b.x, prev_b.x))) +
-                          rotational_bound(prev_a.q, pred_a.q, d.rotb[a]) +
-                          rotational_bound(prev_b.q, pred_b.q, d.rotb[b]);
-            bool swept = moved > margin;
-            bool ok = false;
-            if (swept) ok = swept_face_manifold(prev_a, pred_a, bm, prev_b, pred_b, cm, margin, m);
-            if (!ok) {
-                ok = face_manifold(pred_a, bm, pred_b, cm, margin, corr, m);
-                if (swept && m.count == 0) ok = false;
-            }
-            if (!ok) m.count = 0;
-            count = m.count;
+        const MeshRef bm = mesh_ref(d, ma), cm = mesh_ref(d, mb);
+        const CandidateMotion c = candidate_motion(d, a, b);
+        bool ok = false;
+        if (c.swept) ok = swept_face_manifold(c.prev_a, c.pred_a, bm, c.prev_b, c.pred_b, cm, c.margin, m);
+        if (!ok) {
+            ok = face_manifold(c.pred_a, bm, c.pred_b, cm, c.margin, c.corr, m);
+            if (c.swept && m.count == 0) ok = false;
         }
+        if (!ok) m.count = 0;
+        const uint32_t count = m.count;
         d.np_count[k] = count;
         d.np_scan[k] = count ? ((uint64_t(1) << 32) | count) : 0ull;
         if (count) {
@@ -415,14 +482,16 @@ __global__ void k_cache_load(Dev d, StepParams sp) {
 }
 
 void launch_narrowphase(const Dev& d, const StepParams& sp, cudaStream_t s) {
-    k_narrow<<<blocks_for(d.cap_cand, 128), 128, 0, s>>>(d);
+    k_narrow_sat<<<cap_blocks(d.cap_cand, 256), 256, 0, s>>>(d);
+    ++g_kernel_launches;
+    k_narrow<<<cap_blocks(d.cap_cand, 128), 128, 0, s>>>(d);
     ++g_kernel_launches;
     prof_mark(s, "narrowphase");
     scan_u64(d.np_scan, d.np_scan, &d.ctr->n_cand, d.cap_cand, d.scan_tmp, s);
-    k_compact<<<blocks_for(d.cap_cand), kBlock, 0, s>>>(d);
+    k_compact<<<cap_blocks(d.cap_cand), kBlock, 0, s>>>(d);
     ++g_kernel_launches;
     prof_mark(s, "compact");
-    k_cache_load<<<blocks_for(d.cap_pair, 128), 128, 0, s>>>(d, sp);
+    k_cache_load<<<cap_blocks(d.cap_pair, 128), 128, 0, s>>>(d, sp);
     ++g_kernel_launches;
     prof_mark(s, "cache load");
 }

@@ -415,35 +415,53 @@ __global__ void k_color_count(Dev d) {
     for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
         if (d.motion[i] != kDynamic) continue;
         const uint32_t col = d.color[i];
-        atomicAdd(&d.ctr->color_count[col], 1u);
+        atomicAdd(&d.ctr->color_count[col * kWidthClasses + width_class(d.rcount[i])], 1u);
         atomicMax(&d.ctr->colors, col + 1);
     }
 }
 
-__global__ void k_color_offsets(Dev d) {
-    if (threadIdx.x == 0) {
-        uint32_t s = 0;
-        for (uint32_t k = 0; k < kMaxColors; ++k) {
-            d.ctr->color_off[k] = s;
-            s += d.ctr->color_count[k];
-            d.ctr->color_count[k] = 0;
-        }
-        d.ctr->color_off[kMaxColors] = s;
+// Exclusive scan of the bucket counts (one block); counts become cursors.
+constexpr uint32_t kBuckets = kMaxColors * kWidthClasses;
+__global__ void __launch_bounds__(1024) k_color_offsets(Dev d) {
+    __shared__ uint32_t part[32];
+    const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint32_t v = t < kBuckets ? d.ctr->color_count[t] : 0u;
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= uint32_t(o)) x += y;
     }
+    if (lane == 31) part[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t p = part[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, p, o);
+            if (lane >= uint32_t(o)) p += y;
+        }
+        part[lane] = p;
+    }
+    __syncthreads();
+    const uint32_t incl = x + (warp ? part[warp - 1] : 0u);
+    if (t < kBuckets) {
+        d.ctr->color_off[t] = incl - v;
+        d.ctr->color_count[t] = 0;
+    }
+    if (t == kBuckets - 1) d.ctr->color_off[kBuckets] = incl;
 }
 
 __global__ void k_color_scatter(Dev d) {
     for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
         if (d.motion[i] != kDynamic) continue;
-        const uint32_t col = d.color[i];
-        d.corder[d.ctr->color_off[col] + atomicAdd(&d.ctr->color_count[col], 1u)] = i;
+        const uint32_t b = d.color[i] * kWidthClasses + width_class(d.rcount[i]);
+        d.corder[d.ctr->color_off[b] + atomicAdd(&d.ctr->color_count[b], 1u)] = i;
     }
 }
 
 void launch_prepare(const Dev& d, const StepParams& sp, cudaStream_t s) {
     k_prepare_bodies<<<blocks_for(d.n), kBlock, 0, s>>>(d, sp);
     ++g_kernel_launches;
-    k_prepare_pairs<<<blocks_for(d.cap_pair, 128), 128, 0, s>>>(d, sp);
+    k_prepare_pairs<<<cap_blocks(d.cap_pair, 128), 128, 0, s>>>(d, sp);
     ++g_kernel_launches;
     if (d.nj) {
         k_prepare_joints<<<blocks_for(d.nj, 64), 64, 0, s>>>(d, sp);
@@ -456,7 +474,7 @@ void launch_prepare(const Dev& d, const StepParams& sp, cudaStream_t s) {
 const void* color_kernel_ptr = reinterpret_cast<const void*>(&k_color);
 
 void launch_graph(const Dev& d, const StepParams& sp, cudaStream_t s, int coop_blocks) {
-    uint32_t gb = blocks_for(d.cap_pair > d.nj ? d.cap_pair : d.nj);
+    uint32_t gb = cap_blocks(d.cap_pair > d.nj ? d.cap_pair : d.nj);
     k_graph_degrees<<<gb, kBlock, 0, s>>>(d, sp);
     ++g_kernel_launches;
     scan_u32(d.deg, d.inc_off, nullptr, d.n, nullptr, d.scan_tmp32, s);
@@ -470,7 +488,7 @@ void launch_graph(const Dev& d, const StepParams& sp, cudaStream_t s, int coop_b
     scan_u32(d.rcount, d.roff, nullptr, d.n, nullptr, d.scan_tmp32, s);
     k_row_lists<<<blocks_for(d.n), kBlock, 0, s>>>(d);
     ++g_kernel_launches;
-    k_graph_impact<<<blocks_for(d.cap_pair), kBlock, 0, s>>>(d);
+    k_graph_impact<<<cap_blocks(d.cap_pair), kBlock, 0, s>>>(d);
     ++g_kernel_launches;
     k_graph_islands<<<blocks_for(d.n), kBlock, 0, s>>>(d);
     ++g_kernel_launches;
@@ -481,7 +499,8 @@ void launch_graph(const Dev& d, const StepParams& sp, cudaStream_t s, int coop_b
     prof_mark(s, "colour fixpoint");
     k_color_count<<<blocks_for(d.n), kBlock, 0, s>>>(d);
     ++g_kernel_launches;
-    k_color_offsets<<<1, 32, 0, s>>>(d);
+    static_assert(kBuckets <= 1024, "bucket scan is one block");
+    k_color_offsets<<<1, 1024, 0, s>>>(d);
     ++g_kernel_launches;
     k_color_scatter<<<blocks_for(d.n), kBlock, 0, s>>>(d);
     ++g_kernel_launches;

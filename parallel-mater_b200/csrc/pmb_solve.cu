@@ -92,7 +92,7 @@ __global__ void k_contact_jacobians(Dev d, uint32_t phase) {
     }
 }
 void launch_contact_jacobians(const Dev& d, uint32_t phase, cudaStream_t s) {
-    k_contact_jacobians<<<blocks_for(d.cap_contact), kBlock, 0, s>>>(d, phase);
+    k_contact_jacobians<<<cap_blocks(d.cap_contact), kBlock, 0, s>>>(d, phase);
     ++g_kernel_launches;
 }
 
@@ -539,7 +539,7 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
     extern __shared__ __align__(16) uint8_t stage_raw[];
     const int lane = threadIdx.x & 31;
     uint8_t* warp_stage = stage_raw + (threadIdx.x >> 5) * kWarpStage;
-    const uint32_t tid = blockIdx.x * kSolveThreads + threadIdx.x, nthreads = gridDim.x * kSolveThreads;
+    const uint32_t nthreads = gridDim.x * kSolveThreads;
     const float dt = sp.dt;
     const uint32_t colors = c->colors;
     uint32_t budget = sp.budget_request;
@@ -563,29 +563,49 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
     if (timing && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_start = now();
     for (uint32_t it = 0; it < iters; ++it) {
         for (uint32_t col = 0; col < colors; ++col) {
-            const uint32_t b0 = c->color_off[col], b1 = c->color_off[col + 1];
+            const uint32_t* off = c->color_off + col * kWidthClasses;
+            const uint32_t b0 = off[0], b1 = off[kWidthClasses];
             const uint32_t nb = b1 - b0;
             const bool last_colour = timing && it == 0 && col + 1 == colors;
-            auto sweep = [&](auto width) {
+            // Bodies [lo, hi) with G lanes each. Consecutive bodies go to
+            // consecutive CTAs (group rank = local group x grid + CTA), so the
+            // heavy bodies at the front of a colour spread over all SMs.
+            auto sweep = [&](auto width, uint32_t lo, uint32_t hi) {
                 constexpr int G = decltype(width)::value;
                 const int gl = lane % G, gbase = lane - gl;
                 const uint32_t gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << gbase;
                 GroupRows<G>& sm = reinterpret_cast<GroupRows<G>*>(warp_stage)[gbase / G];
                 const uint32_t groups = nthreads / G;
-                for (uint32_t k = b0 + tid / G; k < b1; k += groups) {
+                const uint32_t rank = (threadIdx.x / G) * gridDim.x + blockIdx.x;
+                for (uint32_t k = lo + rank; k < hi; k += groups) {
                     const uint32_t i = d.corder[k];
                     if (phase != 0 && d.impact[i] == 0) continue;
                     if (batched(d) && it >= d.scene_budget[d.scene_of[i]]) continue;
                     solve_body_group<G>(d, i, phase, dt, sm, gmask, gl, gbase, last_colour);
                 }
+                __syncwarp();
             };
-            // Widths: see the group-per-body comment; policy 1 keeps 8 lanes.
-            if (d.solve_policy == 0 && nb * 32u <= nthreads)
-                sweep(std::integral_constant<int, 32>{});
-            else if (d.solve_policy == 0 && nb * 16u <= nthreads)
-                sweep(std::integral_constant<int, 16>{});
-            else
-                sweep(std::integral_constant<int, 8>{});
+            using W32 = std::integral_constant<int, 32>;
+            using W16 = std::integral_constant<int, 16>;
+            using W8 = std::integral_constant<int, 8>;
+            // Widths (see the group-per-body comment): policy 0 one width per
+            // colour by its size, 1 eight lanes, 2 a width per body class
+            // (heaviest first) unless 32-lane groups cover the whole colour.
+            uint32_t r32 = b0, r16 = b0, r8 = b0;  // 32 lanes [b0, r32), 16 [r32, r16), 8 [r16, r8)
+            if (d.solve_policy != 1 && nb * 32u <= nthreads) {
+                r32 = r16 = r8 = b1;
+            } else if (d.solve_policy == 2) {
+                r32 = off[1];
+                r16 = off[2];
+                r8 = b1;
+            } else if (d.solve_policy == 0 && nb * 16u <= nthreads) {
+                r16 = r8 = b1;
+            } else {
+                r8 = b1;
+            }
+            sweep(W32{}, b0, r32);
+            sweep(W16{}, r32, r16);
+            sweep(W8{}, r16, r8);
             if (timing && it == 0 && col < 18) {
                 __syncthreads();
                 if (threadIdx.x == 0) atomicMax(&c->dbg_work[col], now());
@@ -951,10 +971,10 @@ void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, const 
                       const SolveBuffers& o) {
     const SolveVariant& sv = solve_variants[d.solve_variant < kSolveVariants ? d.solve_variant : 0];
     const int coop = coop_blocks[d.solve_variant < kSolveVariants ? d.solve_variant : 0];
-    const uint32_t pb = blocks_for(d.cap_pair > d.nj ? d.cap_pair : d.nj);
+    const uint32_t pb = cap_blocks(d.cap_pair > d.nj ? d.cap_pair : d.nj);
     for (uint32_t phase = 0; phase < (sp.realtime ? 1u : 2u); ++phase) {
         if (phase != 0) {
-            k_impact_setup<<<blocks_for(d.cap_pair), kBlock, 0, s>>>(d, sp, o.ox, o.oq, o.ov, o.ow);
+            k_impact_setup<<<cap_blocks(d.cap_pair), kBlock, 0, s>>>(d, sp, o.ox, o.oq, o.ov, o.ow);
             ++g_kernel_launches;
             k_impact_bodies<<<blocks_for(d.n), kBlock, 0, s>>>(d, o.ox, o.oq, o.ov, o.ow);
             ++g_kernel_launches;
@@ -972,9 +992,9 @@ void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, const 
         ++g_kernel_launches;
         solve_timer_end(s);
         prof_mark(s, phase ? "solve phase 1" : "solve phase 0");
-        k_contact_finalize<<<blocks_for(d.cap_contact), kBlock, 0, s>>>(d, sp, phase);
+        k_contact_finalize<<<cap_blocks(d.cap_contact), kBlock, 0, s>>>(d, sp, phase);
         ++g_kernel_launches;
-        k_free_anchor<<<blocks_for(d.cap_pair > d.n ? d.cap_pair : d.n), kBlock, 0, s>>>(d, phase);
+        k_free_anchor<<<cap_blocks(d.cap_pair > d.n ? d.cap_pair : d.n), kBlock, 0, s>>>(d, phase);
         ++g_kernel_launches;
         k_free_mean<<<std::min<uint32_t>(blocks_for(32u * d.n, 256), 148u * 8u), 256, 0, s>>>(d, phase);
         ++g_kernel_launches;
@@ -990,7 +1010,7 @@ void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, const 
     }
     k_clamp_commit<<<blocks_for(d.n), kBlock, 0, s>>>(d, o.ox, o.oq, o.ov, o.ow);
     ++g_kernel_launches;
-    k_cache_save<<<blocks_for(d.cap_pair), kBlock, 0, s>>>(d, sp);
+    k_cache_save<<<cap_blocks(d.cap_pair), kBlock, 0, s>>>(d, sp);
     ++g_kernel_launches;
     prof_mark(s, "commit+cache save");
 }

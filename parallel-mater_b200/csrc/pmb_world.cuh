@@ -21,6 +21,10 @@ namespace pmb {
 enum : uint32_t { kStatic = 0, kKinematic = 1, kDynamic = 2 };
 enum : uint32_t { kFixed, kPoint, kHinge, kSlider, kPiston, kGeneric, kGenericSpring, kMotor };
 constexpr uint32_t kMaxColors = 256;
+// Width classes of a colour's bodies by contact rows: more than 16 rows
+// (class 0, 32 lanes), 9-16 (class 1, 16 lanes), at most 8 (class 2, 8 lanes).
+constexpr uint32_t kWidthClasses = 3;
+__host__ __device__ inline uint32_t width_class(uint32_t rows) { return rows > 16u ? 0u : rows > 8u ? 1u : 2u; }
 constexpr uint32_t kMaxIterations = 256;
 constexpr int kBlock = 256;
 
@@ -42,9 +46,10 @@ struct Counters {
     uint32_t bar_count, bar_gen, budget, joint_iters;
     float hs, residual, pad1, pad2;
     uint32_t budget_max;  // batched scenes: the largest scene budget of the tick
-    uint32_t color_count[kMaxColors];
-    uint32_t color_off[kMaxColors + 1];
-    uint32_t color_cursor[kMaxColors];
+    uint32_t n_surv;      // narrowphase candidates left for the manifold pass
+    // Bodies bucketed by (colour, width class): bucket col * kWidthClasses + k.
+    uint32_t color_count[kMaxColors * kWidthClasses];
+    uint32_t color_off[kMaxColors * kWidthClasses + 1];
     float residual_trace[kMaxIterations];
     double res_sum[1024];  // per-block partial residual sums of the latest dual pass
     uint32_t res_cnt[1024];
@@ -163,6 +168,7 @@ struct Dev {
     uint32_t* np_count;
     uint64_t* np_scan;
     uint32_t* np_stage;
+    uint32_t* np_list;  // candidates surviving the separating-axis pass
     float4 *st_n, *st_p;
     // active pairs / contacts
     uint32_t *act_a, *act_b, *act_code, *act_off, *act_cnt, *act_impact;
@@ -301,6 +307,14 @@ void launch_mlp_reduce_adam(const float* partial, uint32_t parts, float* grad, f
 inline uint32_t blocks_for(uint32_t n, int threads = kBlock) {
     uint32_t b = (n + threads - 1) / threads;
     return b == 0 ? 1 : b;
+}
+// Grid for a grid-stride kernel sized by a capacity (most of which is
+// usually unused): at most enough blocks to fill a B200's 148 SMs.
+constexpr uint32_t kGridSms = 148;
+inline uint32_t cap_blocks(size_t cap, int threads = kBlock) {
+    const uint32_t full = kGridSms * (2048u / uint32_t(threads));
+    const uint32_t need = blocks_for(uint32_t(cap < 0xffffffffu ? cap : 0xffffffffu), threads);
+    return need < full ? need : full;
 }
 
 }  // namespace pmb

@@ -185,7 +185,7 @@ def test_launch_plans_are_bit_identical(gpu_available):
     s = scenes.box_pile((6, 4, 6), seed=13, spacing=1.6)
     ref = None
     for v in range(3):
-        for p in range(2):
+        for p in range(3):
             w = core.World(s)
             w.set_launch_plan(v, p)
             for _ in range(12):
@@ -200,5 +200,25 @@ def test_launch_plans_are_bit_identical(gpu_available):
         w.step()
     before = w.states().view(np.uint8).copy()
     v, p, report = w.autotune(ticks=2)
-    assert report.count("ms/tick") == 6
+    assert report.count("ms/tick") == 9
     assert np.array_equal(w.states().view(np.uint8), before)
+
+
+def test_launch_plans_are_bit_identical_on_the_settled_pile(gpu_available):
+    """The same on the settled 65,536-box pile, where colours are large
+    enough for the per-body width classes (8/16/32 lanes, heaviest first)."""
+    s = scenes.box_pile((64, 32, 32), seed=4)
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "settled_pile_64x32x32.npz"))
+    s.states = z["states"].astype(np.float32).view(scenes.STATE_DTYPE).reshape(-1).copy()
+    ref = None
+    for v, p in ((1, 0), (0, 1), (0, 2), (1, 2), (2, 2)):
+        w = core.World(s)
+        w.set_launch_plan(v, p)
+        for _ in range(4):
+            st = w.step()
+            assert st["status"] == 0
+        x = w.states().view(np.uint8).copy()
+        if ref is None:
+            ref = x
+        assert np.array_equal(x, ref), (v, p)
+        w.close()
