@@ -144,7 +144,10 @@ __global__ void k_integrate(Dev d, StepParams sp, float4* ox, float4* oq, float4
             d.large_list[slot] = i;
         } else {
             d.is_large[i] = 0;
-            atomicMax(reinterpret_cast<int*>(&d.ctr->hs), __float_as_int(m));
+            // Cell size: the largest small proxy (per scene in a batched
+            // world, so a scene of small links keeps small cells).
+            float* hs = batched(d) ? d.scene_hs + d.scene_of[i] : &d.ctr->hs;
+            atomicMax(reinterpret_cast<int*>(hs), __float_as_int(m));
         }
     }
 }
@@ -208,16 +211,17 @@ void launch_pack_states(const Dev& d, uint32_t first, uint32_t count, float* dst
 }
 
 void launch_integrate(const Dev& d, const StepParams& sp, cudaStream_t s, const SolveBuffers& o) {
+    if (d.n_scenes > 1) cudaMemsetAsync(d.scene_hs, 0, sizeof(float) * d.n_scenes, s);
     k_integrate<<<blocks_for(d.n), kBlock, 0, s>>>(d, sp, o.ox, o.oq, o.ov, o.ow);
     ++g_kernel_launches;
     prof_mark(s, "integrate+proxy");
 }
 
 __global__ void k_grid_count(Dev d) {
-    const float hs = d.ctr->hs > 0.0f ? d.ctr->hs : 1.0f;
     for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
         if (d.is_large[i] != 0) continue;
-        int4 c = cell_of(d.lo[i], d.hi[i], hs);
+        const float h = batched(d) ? d.scene_hs[d.scene_of[i]] : d.ctr->hs;
+        int4 c = cell_of(d.lo[i], d.hi[i], h > 0.0f ? h : 1.0f);
         d.grid_cell[i] = c;
         atomicAdd(&d.bucket_count[cell_bucket(c.x, c.y, c.z, d.grid_size, scene_of(d, i))], 1u);
     }
@@ -264,7 +268,13 @@ __device__ __forceinline__ bool candidate(const Dev& d, uint32_t a, uint32_t b, 
     return true;
 }
 
-template <bool kWrite> __device__ uint32_t visit_candidates(const Dev& d, uint32_t a, uint32_t* out, uint32_t cap) {
+// The candidates of query body a that lane gl of a kQueryLanes-lane group
+// finds: large bodies k = gl (mod lanes), then either every small body of
+// the scene (a large dynamic a) or the grid cells q = gl (mod lanes) of the
+// 27 around a's cell. The group's union is the reference's candidate set;
+// the write pass sorts it by identity.
+template <bool kWrite>
+__device__ uint32_t visit_candidates(const Dev& d, uint32_t a, uint32_t gl, uint32_t* out, uint32_t cap) {
     const float4 alo = d.lo[a], ahi = d.hi[a];
     uint32_t count = 0;
     auto emit = [&](uint32_t b) {
@@ -277,31 +287,29 @@ template <bool kWrite> __device__ uint32_t visit_candidates(const Dev& d, uint32
     const uint32_t l0 = multi ? d.scene_large_off[scene] : 0u;
     const uint32_t l1 = multi ? d.scene_large_off[scene + 1] : d.ctr->n_large;
     const uint32_t* large = multi ? d.scene_large_list : d.large_list;
-    for (uint32_t k = l0; k < l1; ++k) {
+    for (uint32_t k = l0 + gl; k < l1; k += kQueryLanes) {
         uint32_t b = large[k];
         if (candidate(d, a, b, alo, ahi)) emit(b);
     }
     if (d.is_large[a] == 1) {
         const uint32_t b0 = multi ? d.scene_body_off[scene] : 0u, b1 = multi ? d.scene_body_off[scene + 1] : d.n;
-        for (uint32_t b = b0; b < b1; ++b)
+        for (uint32_t b = b0 + gl; b < b1; b += kQueryLanes)
             if (d.is_large[b] == 0 && candidate(d, a, b, alo, ahi)) emit(b);
         return count;
     }
     const int4 c = d.grid_cell[a];
-    for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx) {
-                int cx = c.x + dx, cy = c.y + dy, cz = c.z + dz;
-                uint32_t bk = cell_bucket(cx, cy, cz, d.grid_size, scene);
-                uint32_t s = d.bucket_off[bk], e = d.bucket_off[bk + 1];
-                for (uint32_t k = s; k < e; ++k) {
-                    uint32_t b = d.grid_body[k];
-                    int4 cb = d.grid_cell[b];
-                    if (cb.x != cx || cb.y != cy || cb.z != cz) continue;
-                    if (multi && d.scene_of[b] != scene) continue;
-                    if (candidate(d, a, b, alo, ahi)) emit(b);
-                }
-            }
+    for (uint32_t q = gl; q < 27u; q += kQueryLanes) {
+        const int cx = c.x + int(q % 3u) - 1, cy = c.y + int((q / 3u) % 3u) - 1, cz = c.z + int(q / 9u) - 1;
+        uint32_t bk = cell_bucket(cx, cy, cz, d.grid_size, scene);
+        uint32_t s = d.bucket_off[bk], e = d.bucket_off[bk + 1];
+        for (uint32_t k = s; k < e; ++k) {
+            uint32_t b = d.grid_body[k];
+            int4 cb = d.grid_cell[b];
+            if (cb.x != cx || cb.y != cy || cb.z != cz) continue;
+            if (multi && d.scene_of[b] != scene) continue;
+            if (candidate(d, a, b, alo, ahi)) emit(b);
+        }
+    }
     return count;
 }
 
@@ -319,36 +327,51 @@ __global__ void k_scene_large_scatter(Dev d) {
     }
 }
 
+// kQueryLanes lanes per query body; each lane's count is kept for the
+// write pass.
 __global__ void k_query_count(Dev d) {
-    for (uint32_t a = grid_stride_begin(); a < d.n; a += grid_stride()) {
+    const uint32_t gl = threadIdx.x % kQueryLanes;
+    const uint32_t gmask = ((1u << kQueryLanes) - 1u) << (threadIdx.x & 31u & ~(kQueryLanes - 1u));
+    const uint32_t groups = grid_stride() / kQueryLanes;
+    for (uint32_t a = grid_stride_begin() / kQueryLanes; a < d.n; a += groups) {
         uint32_t c = 0;
-        if (d.motion[a] == kDynamic && d.is_large[a] != 2) c = visit_candidates<false>(d, a, nullptr, 0);
-        d.cand_count[a] = c;
+        if (d.motion[a] == kDynamic && d.is_large[a] != 2) c = visit_candidates<false>(d, a, gl, nullptr, 0);
+        d.cand_lane[size_t(a) * kQueryLanes + gl] = c;
+        for (uint32_t o = kQueryLanes / 2; o > 0; o >>= 1) c += __shfl_xor_sync(gmask, c, o);
+        if (gl == 0) d.cand_count[a] = c;
     }
 }
 
 __global__ void k_query_write(Dev d) {
     const uint32_t total = d.ctr->n_cand;
     if (grid_stride_begin() == 0 && total > d.cap_cand) atomicOr(&d.ctr->status, kStCandidateOverflow);
-    for (uint32_t a = grid_stride_begin(); a < d.n; a += grid_stride()) {
-        uint32_t c = d.cand_count[a];
-        if (c == 0) continue;
-        uint32_t off = d.cand_off[a];
-        if (off >= d.cap_cand) continue;
-        uint32_t cap = min(c, d.cap_cand - off);
+    const uint32_t gl = threadIdx.x % kQueryLanes;
+    const uint32_t gmask = ((1u << kQueryLanes) - 1u) << (threadIdx.x & 31u & ~(kQueryLanes - 1u));
+    const uint32_t groups = grid_stride() / kQueryLanes;
+    for (uint32_t a = grid_stride_begin() / kQueryLanes; a < d.n; a += groups) {
+        const uint32_t c = d.cand_count[a];
+        const uint32_t off = d.cand_off[a];
+        if (c == 0 || off >= d.cap_cand) continue;  // uniform over the group
+        const uint32_t cap = min(c, d.cap_cand - off);
+        uint32_t lane_off = 0;
+        for (uint32_t k = 0; k < gl; ++k) lane_off += d.cand_lane[size_t(a) * kQueryLanes + k];
         uint32_t* seg = d.cand_b + off;
-        visit_candidates<true>(d, a, seg, cap);
-        // Insertion sort by identity (dense index).
-        for (uint32_t i = 1; i < cap; ++i) {
-            uint32_t v = seg[i];
-            uint32_t j = i;
-            while (j > 0 && seg[j - 1] > v) {
-                seg[j] = seg[j - 1];
-                --j;
+        if (lane_off < cap) visit_candidates<true>(d, a, gl, seg + lane_off, cap - lane_off);
+        __syncwarp(gmask);
+        if (gl == 0) {
+            // Insertion sort by identity (dense index).
+            for (uint32_t i = 1; i < cap; ++i) {
+                uint32_t v = seg[i];
+                uint32_t j = i;
+                while (j > 0 && seg[j - 1] > v) {
+                    seg[j] = seg[j - 1];
+                    --j;
+                }
+                seg[j] = v;
             }
-            seg[j] = v;
         }
-        for (uint32_t i = 0; i < cap; ++i) d.cand_a[off + i] = a;
+        for (uint32_t i = gl; i < cap; i += kQueryLanes) d.cand_a[off + i] = a;
+        __syncwarp(gmask);
     }
 }
 
@@ -374,11 +397,11 @@ void launch_broadphase(const Dev& d, cudaStream_t s) {
     k_grid_scatter<<<blocks_for(d.n), kBlock, 0, s>>>(d);
     ++g_kernel_launches;
     prof_mark(s, "grid build");
-    k_query_count<<<blocks_for(d.n, 128), 128, 0, s>>>(d);
+    k_query_count<<<blocks_for(kQueryLanes * d.n, 128), 128, 0, s>>>(d);
     ++g_kernel_launches;
     prof_mark(s, "query count");
     scan_u32(d.cand_count, d.cand_off, nullptr, d.n, &d.ctr->n_cand, d.scan_tmp32, s);
-    k_query_write<<<blocks_for(d.n, 128), 128, 0, s>>>(d);
+    k_query_write<<<blocks_for(kQueryLanes * d.n, 128), 128, 0, s>>>(d);
     ++g_kernel_launches;
     k_clamp_count<<<1, 1, 0, s>>>(&d.ctr->n_cand, d.cap_cand);
     ++g_kernel_launches;

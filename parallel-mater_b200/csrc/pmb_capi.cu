@@ -288,7 +288,7 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     ALLOC(d.lo, n); ALLOC(d.hi, n); ALLOC(d.is_large, n); ALLOC(d.large_list, n);
     ALLOC(d.bucket_count, grid_size + 1); ALLOC(d.bucket_off, grid_size + 1); ALLOC(d.bucket_cursor, grid_size);
     ALLOC(d.grid_body, n); ALLOC(d.grid_cell, n);
-    ALLOC(d.cand_count, n + 1); ALLOC(d.cand_off, n + 1);
+    ALLOC(d.cand_count, n + 1); ALLOC(d.cand_off, n + 1); ALLOC(d.cand_lane, kQueryLanes * size_t(n));
     ALLOC(d.cand_a, cap_cand); ALLOC(d.cand_b, cap_cand);
     ALLOC(d.np_count, cap_cand); ALLOC(d.np_scan, cap_cand + 1); ALLOC(d.np_stage, cap_cand);
     ALLOC(d.np_list, cap_cand);
@@ -314,7 +314,7 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     }
     ALLOC(d.deg, n); ALLOC(d.inc_off, n + 1); ALLOC(d.inc_cursor, n); ALLOC(d.inc_list, 2 * cap_pair);
     ALLOC(d.jdeg, n); ALLOC(d.jinc_off, n + 1); ALLOC(d.jinc_cursor, n); ALLOC(d.jinc_list, 2 * size_t(nj) + 2);
-    ALLOC(d.corder, n);
+    ALLOC(d.corder, n); ALLOC(d.cdirty, 2 * size_t(n));
     ALLOC(d.rcount, n); ALLOC(d.roff, n + 1); ALLOC(d.blist, 2 * cap_contact); ALLOC(d.bother, 2 * cap_contact);
     ALLOCP(d.joints, nj); ALLOCS(d.jstate, nj); ALLOCS(d.jrows, size_t(nj) * 18);
     ALLOCP(d.hinge_list, z.hinges); ALLOCP(d.hinge_seg, z.hinge_segs + 1);
@@ -332,7 +332,7 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
         ALLOCP(d.scene_of, n); ALLOCP(d.scene_body_off, ns + 1); ALLOCP(d.scene_iters, ns); ALLOCP(d.scene_jiters, ns);
         ALLOC(d.scene_large_count, ns + 1); ALLOC(d.scene_large_off, ns + 1); ALLOC(d.scene_large_cursor, ns);
         ALLOC(d.scene_large_list, n); ALLOC(d.scene_budget, ns);
-        ALLOC(d.scene_res_sq, ns); ALLOC(d.scene_res_mx, ns); ALLOC(d.scene_res_n, ns);
+        ALLOC(d.scene_res_sq, ns); ALLOC(d.scene_res_mx, ns); ALLOC(d.scene_res_n, ns); ALLOC(d.scene_hs, ns);
     }
 #undef ALLOCP
 #undef ALLOC
@@ -611,7 +611,12 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
         cudaFuncSetAttribute(sv.ptr, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sv.smem));
         w->coop_solve[v] = coop_blocks_for(sv.ptr, sv.threads, sv.smem);
     }
-    w->coop_color = coop_blocks_for(color_kernel_ptr, kBlock, 0);
+    {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        w->coop_color = std::min(coop_blocks_for(color_kernel_ptr, kColorThreads, 0), std::max(1, sms));
+    }
     // A world in caller-bound memory allocates nothing, so it has no
     // snapshot storage (pmb_world_snapshot reports FEATURE_NOT_PRESENT).
     for (auto& p : w->dynamic_state) {
@@ -683,6 +688,9 @@ int pmb_world_profile_step(pmb_world* w, const pmb_step_desc* step, char* report
     cudaMemcpy(&hc, w->d.ctr, sizeof(Counters), cudaMemcpyDeviceToHost);
     {
         char line[160];
+        std::snprintf(line, sizeof(line), "colour fixpoint rounds %u, candidates %u, narrowphase survivors %u\n",
+                      hc.rounds, hc.n_cand, hc.n_surv);
+        text += line;
         std::snprintf(line, sizeof(line), "solve iteration 0 (us from kernel start): colours %u\n", hc.colors);
         text += line;
         for (uint32_t k = 0; k < 20; ++k) {

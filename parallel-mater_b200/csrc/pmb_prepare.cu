@@ -384,19 +384,49 @@ __device__ __forceinline__ uint32_t mex_lower(const Dev& d, uint32_t v, bool& ov
     return kMaxColors - 1;
 }
 
-__global__ void __launch_bounds__(kBlock) k_color(Dev d) {
+// Mark v's higher-indexed dynamic neighbours for the next round: only their
+// mex can depend on v's colour.
+__device__ __forceinline__ void mark_higher(const Dev& d, uint32_t v, uint8_t* next) {
+    const uint32_t so = d.inc_off[v], sn = d.deg[v];
+    for (uint32_t k = 0; k < sn; ++k) {
+        const uint32_t p = d.inc_list[so + k];
+        const uint32_t a = d.act_a[p], b = d.act_b[p];
+        const uint32_t u = a == v ? b : a;
+        if (u > v && d.motion[u] == kDynamic) next[u] = 1;
+    }
+    const uint32_t jo = d.jinc_off[v], jn = d.jdeg[v];
+    for (uint32_t k = 0; k < jn; ++k) {
+        const JointState st = d.jstate[d.jinc_list[jo + k]];
+        const uint32_t u = st.dense_a == v ? st.dense_b : st.dense_a;
+        if (u > v && d.motion[u] == kDynamic) next[u] = 1;
+    }
+}
+
+// Jacobi rounds towards the greedy colouring in index order (colour of v =
+// smallest colour absent among its lower-indexed neighbours), warm-started
+// from last tick's colours. Round 0 visits every body; later rounds only
+// those with a lower neighbour that changed in the round before (the only
+// bodies whose mex can change), so the fixpoint is the same.
+__global__ void __launch_bounds__(kColorThreads) k_color(Dev d) {
     Counters* c = d.ctr;
     for (uint32_t round = 0; round < d.n + 2; ++round) {
         const uint32_t before = ((volatile uint32_t*)&c->changed)[0];
         if (!grid_sync(c)) return;
+        uint8_t* cur = d.cdirty + size_t(round & 1u) * d.n;
+        uint8_t* next = d.cdirty + size_t((round + 1u) & 1u) * d.n;
         bool overflow = false;
         uint32_t changes = 0;
         for (uint32_t v = grid_stride_begin(); v < d.n; v += grid_stride()) {
+            if (round != 0) {
+                if (!cur[v]) continue;
+                cur[v] = 0;
+            }
             if (d.motion[v] != kDynamic) continue;
             uint32_t col = mex_lower(d, v, overflow);
             if (col != d.color[v]) {
                 ((volatile uint32_t*)d.color)[v] = col;
                 ++changes;
+                mark_higher(d, v, next);
             }
         }
         if (overflow) atomicOr(&c->status, kStColorOverflow);
@@ -493,8 +523,9 @@ void launch_graph(const Dev& d, const StepParams& sp, cudaStream_t s, int coop_b
     k_graph_islands<<<blocks_for(d.n), kBlock, 0, s>>>(d);
     ++g_kernel_launches;
     prof_mark(s, "graph lists+islands");
+    cudaMemsetAsync(d.cdirty, 0, 2 * size_t(d.n), s);
     void* args[] = {const_cast<Dev*>(&d)};
-    cudaLaunchCooperativeKernel(color_kernel_ptr, dim3(coop_blocks), dim3(kBlock), args, 0, s);
+    cudaLaunchCooperativeKernel(color_kernel_ptr, dim3(coop_blocks), dim3(kColorThreads), args, 0, s);
     ++g_kernel_launches;
     prof_mark(s, "colour fixpoint");
     k_color_count<<<blocks_for(d.n), kBlock, 0, s>>>(d);

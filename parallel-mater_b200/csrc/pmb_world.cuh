@@ -21,6 +21,10 @@ namespace pmb {
 enum : uint32_t { kStatic = 0, kKinematic = 1, kDynamic = 2 };
 enum : uint32_t { kFixed, kPoint, kHinge, kSlider, kPiston, kGeneric, kGenericSpring, kMotor };
 constexpr uint32_t kMaxColors = 256;
+constexpr uint32_t kQueryLanes = 8;  // broadphase query lanes per body
+// The colour fixpoint runs one 1024-thread CTA per SM: its ~30 rounds are
+// two grid barriers each, and a barrier's cost grows with the CTA count.
+constexpr int kColorThreads = 1024;
 // Width classes of a colour's bodies by contact rows: more than 16 rows
 // (class 0, 32 lanes), 9-16 (class 1, 16 lanes), at most 8 (class 2, 8 lanes).
 constexpr uint32_t kWidthClasses = 3;
@@ -137,6 +141,7 @@ struct Dev {
     uint32_t* scene_jiters;      // per tick: largest joint iteration hint
     uint32_t* scene_budget;      // per tick: the scene's sweeps
     float *scene_res_sq, *scene_res_mx;  // per tick: residual of the scene's last sweep
+    float* scene_hs;                     // per tick: the scene's broadphase cell size
     uint32_t* scene_res_n;
     // warm-start table: per contact point, lambda (x, y, z rows) and penalty
     float4* warm_table;  // 2 per contact: lambda, penalty
@@ -163,6 +168,7 @@ struct Dev {
     uint32_t* grid_body;
     int4* grid_cell;
     uint32_t *cand_count, *cand_off;
+    uint32_t* cand_lane;  // per query body, each query lane's candidate count
     uint32_t *cand_a, *cand_b;
     // narrowphase
     uint32_t* np_count;
@@ -188,6 +194,7 @@ struct Dev {
     uint32_t *deg, *inc_off, *inc_cursor, *inc_list;
     uint32_t *jdeg, *jinc_off, *jinc_cursor, *jinc_list;
     uint32_t* corder;
+    uint8_t* cdirty;  // colour rounds: two flag arrays of n (bodies to revisit)
     uint32_t *rcount, *roff, *blist;  // per-body flattened contact rows (bit 31: second body)
     uint32_t* bother;                 // the other body of each flattened row
     uint32_t *mem_count, *mem_off, *mem_cursor, *mem_list;
