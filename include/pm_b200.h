@@ -458,6 +458,25 @@ typedef struct PmConstraintState {
     float appliedImpulse;
 } PmConstraintState;
 
+/* ---- contact events (parallel_mater.h:759-774, 955-968) ---- */
+typedef struct PmFloat3 { float x; float y; float z; } PmFloat3;
+typedef struct PmDomainOutputHeader {
+    uint32_t activeCount;
+    uint32_t capacity;
+    uint64_t revision;
+} PmDomainOutputHeader;
+typedef enum PmContactEventType { PM_CONTACT_RIGID_RIGID = 0, PM_CONTACT_LIQUID_RIGID = 1 } PmContactEventType;
+typedef struct PmContactEvent {
+    PmContactEventType type;
+    uint32_t first;
+    uint32_t second;
+    PmFloat3 position;
+    PmFloat3 normal;
+    float penetration;
+    float normalImpulse;
+    PmFloat3 frictionImpulse;
+} PmContactEvent;
+
 /* ---- barriers and synchronisation (parallel_mater.h:1032-1078) ---- */
 #define PM_STAGE_HOST_BIT UINT64_C(0x1)
 #define PM_STAGE_TRANSFER_BIT UINT64_C(0x2)
@@ -637,6 +656,8 @@ typedef void(PMAPI_CALL* PFN_pmDestroyPhysicsPipeline)(PmDevice device, PmPhysic
 typedef PmResult(PMAPI_CALL* PFN_pmCmdCopyConstraintStates)(PmCommandBuffer commandBuffer, PmSimulation simulation,
                                                             uint32_t firstConstraint, uint32_t count,
                                                             const PmBufferRange* pDestination);
+typedef PmResult(PMAPI_CALL* PFN_pmCmdCopyContactEvents)(PmCommandBuffer commandBuffer, PmSimulation simulation,
+                                                         const PmBufferRange* pDestination);
 typedef PmResult(PMAPI_CALL* PFN_pmCreateCommandPool)(PmDevice device, const PmCommandPoolCreateInfo* pInfo,
                                                       PmCommandPool* pPool);
 typedef void(PMAPI_CALL* PFN_pmDestroyCommandPool)(PmDevice device, PmCommandPool pool);

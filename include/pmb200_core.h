@@ -118,6 +118,8 @@ typedef struct pmb_world_desc {
     uint32_t scene_count;
     const uint32_t* body_scene;
     const uint32_t* scene_iterations;
+    /* Contact events kept per tick when a step asks for them (0: none). */
+    uint32_t event_capacity;
 } pmb_world_desc;
 
 /* Upper bounds for sizing caller-owned memory. Capacities of 0 select the
@@ -125,6 +127,7 @@ typedef struct pmb_world_desc {
 typedef struct pmb_world_capacity {
     uint32_t body_count, joint_count, mesh_count, mesh_vertex_count, mesh_triangle_count;
     uint32_t candidate_capacity, pair_capacity, contact_capacity;
+    uint32_t event_capacity;
 } pmb_world_capacity;
 
 /* profile: 1 = realtime v1 (8 sweeps, 5% damping), otherwise legacy
@@ -142,6 +145,7 @@ typedef struct pmb_step_desc {
     float residual_tolerance;
     uint32_t max_iterations;
     uint32_t warm_start;
+    uint32_t collect_events; /* nonzero: record this tick's contact events */
 } pmb_step_desc;
 
 /* residual: RMS, over contact normal rows that carry force or penetrate and
@@ -272,6 +276,22 @@ PMB_API int pmb_world_copy_states_to_device(pmb_world* world, uint32_t first, ui
 
 /* Joint state after the last tick (synchronous): flags bit 0 enabled, bit 1
  * broken; applied impulse; number of solver rows. capacity >= joint_count. */
+/* One contact point of the last tick that collected events, in active-pair
+ * order (pm_prepare_parallel_contact_events, geometry.slang:2902-2939, and
+ * the impulses of pm_save_rigid_contact_cache, :3028-3043): the pair's
+ * bodies (dense indices, query body first), the point and normal, the
+ * penetration (>= 0) and the normal and friction impulses of the tick. */
+typedef struct pmb_contact_event {
+    uint32_t body, collider;
+    float position[3], normal[3];
+    float penetration, normal_impulse;
+    float friction_impulse[3];
+} pmb_contact_event;
+/* Copies at most `capacity` events of the last tick into `out` (host
+ * memory); `count` receives the tick's event count (min(contact points,
+ * event capacity); 0 when the tick did not collect). */
+PMB_API int pmb_world_contact_events(pmb_world* world, pmb_contact_event* out, uint32_t capacity, uint32_t* count);
+
 PMB_API int pmb_world_joints(pmb_world* world, uint32_t* flags, float* applied, uint32_t* counts,
                              uint32_t capacity);
 

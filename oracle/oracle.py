@@ -48,6 +48,8 @@ def lib():
         L.oracle_manifolds.restype = u32
         L.oracle_manifolds.argtypes = [vp, vp, vp, vp, u32]
         L.oracle_graph.argtypes = [vp, vp, vp]
+        L.oracle_contact_events.restype = u32
+        L.oracle_contact_events.argtypes = [vp, vp, u32]
         L.oracle_residual_trace.restype = u32
         L.oracle_residual_trace.argtypes = [vp, vp, u32]
         L.oracle_aabbs.argtypes = [vp, vp, vp]
@@ -147,6 +149,14 @@ class OracleWorld:
         contacts = np.zeros((max(n, 1), 8, 22), np.float32)
         lib().oracle_manifolds(self.h, codes.ctypes.data, counts.ctypes.data, contacts.ctypes.data, n)
         return codes[:n], counts[:n], contacts[:n]
+
+    def contact_events(self, capacity=1 << 20):
+        """The latest tick's contact events as the reference reports them
+        (records of pmb200.core.EVENT_DTYPE)."""
+        from pmb200.core import EVENT_DTYPE
+        out = np.zeros(capacity, EVENT_DTYPE)
+        n = lib().oracle_contact_events(self.h, out.ctypes.data, capacity)
+        return out[:n]
 
     def graph(self):
         colors = np.zeros(self.scene.n, np.uint32)

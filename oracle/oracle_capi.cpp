@@ -2,6 +2,7 @@
 // ORACLE — test infrastructure only. C ABI over the CPU restatement so the
 // Python tests, smoke() and bench.py's cpu_baseline leg can drive it. The
 // product library never links or loads this file.
+#include <cstring>
 #include <cstdlib>
 #include <memory>
 #include <new>
@@ -194,6 +195,40 @@ uint32_t oracle_manifolds(void* hp, uint32_t* codes, uint32_t* counts, float* co
             }
         }
         return n;
+    });
+}
+
+// Contact events of the latest tick as the reference writes them
+// (pm_prepare_parallel_contact_events, geometry.slang:2902-2939: every point
+// of every active pair in order, up to the capacity, penetration clamped at
+// 0; impulses from pm_save_rigid_contact_cache, :3028-3043: accumulated for
+// persistent contacts, else the reported ones). 13 words per event: body,
+// collider (as float bit patterns of uint32), position, normal,
+// penetration, normal impulse, friction impulse. Returns the event count.
+uint32_t oracle_contact_events(void* hp, float* out, uint32_t capacity) {
+    return with(static_cast<Handle*>(hp), [&](auto& w) {
+        uint32_t cursor = 0;
+        const uint32_t n = w.n;
+        for (uint32_t k = 0; k < w.active_pairs.size(); ++k) {
+            const auto& m = w.manifolds[k];
+            const uint32_t a = w.active_pairs[k] / n, b = w.active_pairs[k] % n;
+            for (uint32_t p = 0; p < m.count; ++p, ++cursor) {
+                if (cursor >= capacity || !out) continue;
+                const auto& c = m.c[p];
+                float* o = out + size_t(cursor) * 13;
+                std::memcpy(&o[0], &a, 4);
+                std::memcpy(&o[1], &b, 4);
+                const float v[11] = {float(c.point.x), float(c.point.y), float(c.point.z), float(c.normal.x),
+                                     float(c.normal.y), float(c.normal.z),
+                                     float(c.penetration > 0 ? c.penetration : 0),
+                                     float(c.persistent ? c.acc_n : c.rep_n),
+                                     float(c.persistent ? c.acc_f.x : c.rep_f.x),
+                                     float(c.persistent ? c.acc_f.y : c.rep_f.y),
+                                     float(c.persistent ? c.acc_f.z : c.rep_f.z)};
+                for (int q = 0; q < 11; ++q) o[2 + q] = v[q];
+            }
+        }
+        return cursor < capacity ? cursor : capacity;
     });
 }
 

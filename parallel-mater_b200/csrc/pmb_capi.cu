@@ -147,6 +147,7 @@ StepParams params_from(const pmb_step_desc& s) {
     p.tolerance = s.residual_tolerance;
     p.max_iterations = s.max_iterations;
     p.warm_start = s.warm_start;
+    p.collect_events = s.collect_events;
     return p;
 }
 
@@ -255,6 +256,7 @@ struct Sizes {
     uint32_t n, nm, nj, scenes;
     size_t verts, planes, dis, hinges, hinge_segs;
     uint32_t cap_cand, cap_pair, cap_contact;
+    uint32_t events;
 };
 struct Extra {
     float4 *lo, *hi, *sph;  // mesh bounds, read once at creation
@@ -315,6 +317,7 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     ALLOC(d.deg, n); ALLOC(d.inc_off, n + 1); ALLOC(d.inc_cursor, n); ALLOC(d.inc_list, 2 * cap_pair);
     ALLOC(d.jdeg, n); ALLOC(d.jinc_off, n + 1); ALLOC(d.jinc_cursor, n); ALLOC(d.jinc_list, 2 * size_t(nj) + 2);
     ALLOC(d.corder, n); ALLOC(d.cdirty, 2 * size_t(n));
+    ALLOCP(d.events, z.events);
     ALLOC(d.rcount, n); ALLOC(d.roff, n + 1); ALLOC(d.blist, 2 * cap_contact); ALLOC(d.bother, 2 * cap_contact);
     ALLOCP(d.joints, nj); ALLOCS(d.jstate, nj); ALLOCS(d.jrows, size_t(nj) * 18);
     ALLOCP(d.hinge_list, z.hinges); ALLOCP(d.hinge_seg, z.hinge_segs + 1);
@@ -508,8 +511,9 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
         hinge_seg.push_back(uint32_t(hs.size()));
     }
     d.n_hinge_segs = uint32_t(hinge_seg.size() - 1);
+    d.event_capacity = desc->event_capacity;
     const Sizes z{n, nm, nj, ns, verts.size(), planes.size(), dis_keys.size(), hinge_list.size(),
-                  hinge_seg.size() - 1, d.cap_cand, d.cap_pair, d.cap_contact};
+                  hinge_seg.size() - 1, d.cap_cand, d.cap_pair, d.cap_contact, desc->event_capacity};
     if (w->arena[kPersistent]) {
         // Bound memory must hold the whole layout before anything is carved.
         pmb_world probe;
@@ -1039,12 +1043,31 @@ int pmb_world_memory_requirements(const pmb_world_capacity* c, uint64_t* persist
                   size_t(c->joint_count),
                   c->candidate_capacity ? c->candidate_capacity : 64u * n + 4096u,
                   c->pair_capacity ? c->pair_capacity : 24u * n + 1024u,
-                  c->contact_capacity ? c->contact_capacity : 64u * n + 4096u};
+                  c->contact_capacity ? c->contact_capacity : 64u * n + 4096u,
+                  c->event_capacity};
     Extra ex{};
     allocate_world(&probe, probe.d, z, ex);
     *persistent = probe.arena_used[kPersistent];
     *scratch = probe.arena_used[kScratch];
     return PMB_SUCCESS;
+}
+
+int pmb_world_contact_events(pmb_world* w, pmb_contact_event* out, uint32_t capacity, uint32_t* count) {
+    if (!w || !count || (capacity && !out)) return PMB_ERROR_INVALID_ARGUMENT;
+    static_assert(sizeof(pmb_contact_event) == sizeof(ContactEvent), "event record");
+    cudaSetDevice(w->device);
+    uint32_t n = 0;
+    cudaMemcpyAsync(&n, &w->d.ctr->n_events, sizeof(n), cudaMemcpyDeviceToHost, w->stream);
+    int r = check(cudaStreamSynchronize(w->stream));
+    if (r != PMB_SUCCESS) return r;
+    n = std::min(n, w->d.event_capacity);
+    *count = n;
+    const uint32_t m = std::min(n, capacity);
+    if (m) {
+        cudaMemcpyAsync(out, w->d.events, sizeof(ContactEvent) * size_t(m), cudaMemcpyDeviceToHost, w->stream);
+        r = check(cudaStreamSynchronize(w->stream));
+    }
+    return r;
 }
 
 int pmb_world_joints(pmb_world* w, uint32_t* flags, float* applied, uint32_t* counts, uint32_t capacity) {

@@ -967,6 +967,34 @@ __global__ void k_cache_save(Dev d, StepParams sp) {
     }
 }
 
+// Contact events of the tick (geometry.slang:2902-2939 and :3028-3043): one
+// per contact point in active-pair order, up to the capacity. Points,
+// normals and penetrations are the narrowphase's (unchanged since); the
+// impulses are those the cache save stores (convex pairs are persistent).
+__global__ void k_contact_events(Dev d) {
+    const uint32_t n = min(d.ctr->n_contacts, d.event_capacity);
+    if (grid_stride_begin() == 0) d.ctr->n_events = n;
+    for (uint32_t c = grid_stride_begin(); c < n; c += grid_stride()) {
+        const uint2 ab = d.c_bodies[c];
+        const float4 nn = d.c_n[c], p = d.c_p[c], f = d.c_accf[c];
+        ContactEvent e;
+        e.body = ab.x;
+        e.collider = ab.y;
+        e.position[0] = p.x;
+        e.position[1] = p.y;
+        e.position[2] = p.z;
+        e.normal[0] = nn.x;
+        e.normal[1] = nn.y;
+        e.normal[2] = nn.z;
+        e.penetration = fmx(0.0f, nn.w);
+        e.normal_impulse = d.c_lam[c].w;
+        e.friction_impulse[0] = f.x;
+        e.friction_impulse[1] = f.y;
+        e.friction_impulse[2] = f.z;
+        d.events[c] = e;
+    }
+}
+
 void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, const int* coop_blocks,
                       const SolveBuffers& o) {
     const SolveVariant& sv = solve_variants[d.solve_variant < kSolveVariants ? d.solve_variant : 0];
@@ -1012,6 +1040,10 @@ void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, const 
     ++g_kernel_launches;
     k_cache_save<<<cap_blocks(d.cap_pair), kBlock, 0, s>>>(d, sp);
     ++g_kernel_launches;
+    if (sp.collect_events && d.event_capacity) {
+        k_contact_events<<<cap_blocks(d.event_capacity), kBlock, 0, s>>>(d);
+        ++g_kernel_launches;
+    }
     prof_mark(s, "commit+cache save");
 }
 

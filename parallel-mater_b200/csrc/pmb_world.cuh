@@ -51,6 +51,7 @@ struct Counters {
     float hs, residual, pad1, pad2;
     uint32_t budget_max;  // batched scenes: the largest scene budget of the tick
     uint32_t n_surv;      // narrowphase candidates left for the manifold pass
+    uint32_t n_events;    // contact events recorded by the tick
     // Bodies bucketed by (colour, width class): bucket col * kWidthClasses + k.
     uint32_t color_count[kMaxColors * kWidthClasses];
     uint32_t color_off[kMaxColors * kWidthClasses + 1];
@@ -74,7 +75,16 @@ struct StepParams {
     uint32_t max_iterations;
     uint32_t debug_timing;  // record solve-kernel timestamps for iteration 0
     uint32_t warm_start;    // 0 plain, 1 learned, 2 table
+    uint32_t collect_events;
 };
+
+struct ContactEvent {  // pmb_contact_event
+    uint32_t body, collider;
+    float position[3], normal[3];
+    float penetration, normal_impulse;
+    float friction_impulse[3];
+};
+static_assert(sizeof(ContactEvent) == 52, "event record");
 
 struct JointRow {  // constraint_math.slang AvbdRow, packed for the device
     float a[6], b[6];
@@ -195,6 +205,8 @@ struct Dev {
     uint32_t *jdeg, *jinc_off, *jinc_cursor, *jinc_list;
     uint32_t* corder;
     uint8_t* cdirty;  // colour rounds: two flag arrays of n (bodies to revisit)
+    ContactEvent* events;
+    uint32_t event_capacity;
     uint32_t *rcount, *roff, *blist;  // per-body flattened contact rows (bit 31: second body)
     uint32_t* bother;                 // the other body of each flattened row
     uint32_t *mem_count, *mem_off, *mem_cursor, *mem_list;

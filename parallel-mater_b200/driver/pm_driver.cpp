@@ -174,6 +174,7 @@ PmPhysicalDeviceFeatures supported_features() {
     f.timestampQueries = PM_TRUE;
     f.statisticsQueries = PM_TRUE;
     f.memoryBudget = PM_TRUE;
+    f.contactEvents = PM_TRUE;
     return f;
 }
 

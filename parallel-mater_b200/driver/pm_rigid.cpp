@@ -247,6 +247,7 @@ PmResult ensure_world(PmSimulation_T* s) {
     desc.candidate_capacity = s->capacity.candidate_capacity;
     desc.pair_capacity = s->capacity.pair_capacity;
     desc.contact_capacity = s->capacity.contact_capacity;
+    desc.event_capacity = s->capacity.event_capacity;
     desc.device = device->ordinal;
     desc.persistent_memory = static_cast<char*>(s->binding.persistentMemory->ptr) + s->binding.persistentOffset;
     desc.persistent_bytes = s->requirements.persistent.size;
@@ -305,6 +306,8 @@ PmResult PMAPI_CALL pmCreateSimulation(PmDevice device, const PmSimulationCreate
     // mesh per body with room to spare.
     c.mesh_vertex_count = 4096u + 16u * n;
     c.mesh_triangle_count = 8192u + 32u * n;
+    // Contact events kept per tick (resources.cpp:212, contact_capacity).
+    c.event_capacity = std::max(1u, info->contactCapacity);
     uint64_t persistent = 0, scratch = 0;
     if (pmb_world_memory_requirements(&c, &persistent, &scratch) != PMB_SUCCESS) {
         delete created;
@@ -545,8 +548,6 @@ PmResult PMAPI_CALL pmCmdStepSimulation(PmCommandBuffer buffer, PmSimulation sim
         (step->flags & ~PmFlags(PM_STEP_COLLECT_CONTACT_EVENTS_BIT)) != 0u)
         return PM_ERROR_INVALID_ARGUMENT;
     if (!realtime_timestep(step->timestep) || step->substeps != 1u) return PM_ERROR_INVALID_ARGUMENT;
-    // Contact events are not produced by this driver (the feature bit is off).
-    if (step->flags & PM_STEP_COLLECT_CONTACT_EVENTS_BIT) return PM_ERROR_FEATURE_NOT_PRESENT;
     const PmStepInfo copied = *step;
     const uint32_t iterations = buffer->bound_pipeline->rigid.rigidIterations;
     const PmResult recorded = record_simulation(buffer, simulation, [simulation, copied, iterations]() -> PmResult {
@@ -582,6 +583,7 @@ PmResult PMAPI_CALL pmCmdStepSimulation(PmCommandBuffer buffer, PmSimulation sim
                 sd.profile = 1u;  // realtime v1
                 sd.requested_iterations = iterations;
                 sd.base_iterations = iterations;
+                sd.collect_events = (copied.flags & PM_STEP_COLLECT_CONTACT_EVENTS_BIT) ? 1u : 0u;
                 pmb_step_stats stats{};
                 r = from_core(pmb_world_step(w, &sd, &stats));
                 if (r == PM_SUCCESS) {
@@ -629,6 +631,67 @@ PmResult PMAPI_CALL pmCmdCopyRigidStates(PmCommandBuffer buffer, PmSimulation si
             k += run;
         }
         return PM_SUCCESS;
+    });
+}
+
+// pmCmdCopyContactEvents (reference src/api/domains.cpp:1692-1746): a
+// PmDomainOutputHeader {events, simulation contact capacity, steps taken}
+// followed by the last tick's rigid-rigid events, bodies as application
+// slots. Capacity-exceeded when the range cannot hold them all.
+PmResult PMAPI_CALL pmCmdCopyContactEvents(PmCommandBuffer buffer, PmSimulation simulation,
+                                           const PmBufferRange* destination) {
+    const PmResult state = require_recording(buffer);
+    if (state != PM_SUCCESS) return state;
+    if (!destination || !destination->buffer || destination->buffer->device != buffer->device ||
+        destination->size < sizeof(PmDomainOutputHeader) ||
+        !range_fits(destination->offset, destination->size, destination->buffer->size) || !simulation ||
+        simulation->device != buffer->device)
+        return PM_ERROR_INVALID_ARGUMENT;
+    const PmBufferRange copied = *destination;
+    PmDevice_T* device = buffer->device;
+    return record_simulation(buffer, simulation, [simulation, copied, device]() -> PmResult {
+        if (!copied.buffer->ptr) return PM_ERROR_INVALID_STATE;
+        std::vector<pmb_contact_event> events;
+        if (simulation->world) {
+            uint32_t n = 0;
+            int rc = pmb_world_contact_events(simulation->world, nullptr, 0, &n);
+            if (rc == PMB_SUCCESS && n) {
+                events.resize(n);
+                rc = pmb_world_contact_events(simulation->world, events.data(), n, &n);
+            }
+            if (rc != PMB_SUCCESS) return from_core(rc);
+        }
+        std::vector<uint32_t> slot_of_dense(simulation->dense_of_slot.size(), PM_INVALID_INDEX);
+        for (uint32_t slot = 0; slot < simulation->dense_of_slot.size(); ++slot)
+            if (simulation->dense_of_slot[slot] != PM_INVALID_INDEX)
+                slot_of_dense[simulation->dense_of_slot[slot]] = slot;
+        const auto slot = [&](uint32_t dense) {
+            return dense < slot_of_dense.size() ? slot_of_dense[dense] : PM_INVALID_INDEX;
+        };
+        const PmDeviceSize required =
+            sizeof(PmDomainOutputHeader) + PmDeviceSize(events.size()) * sizeof(PmContactEvent);
+        if (required > copied.size) return PM_ERROR_CAPACITY_EXCEEDED;
+        std::vector<char> staging(static_cast<size_t>(required));
+        const PmDomainOutputHeader header{uint32_t(events.size()), simulation->capacity.event_capacity,
+                                          simulation->submitted_steps};
+        std::memcpy(staging.data(), &header, sizeof(header));
+        for (size_t k = 0; k < events.size(); ++k) {
+            const pmb_contact_event& e = events[k];
+            PmContactEvent t{};
+            t.type = PM_CONTACT_RIGID_RIGID;
+            t.first = slot(e.body);
+            t.second = slot(e.collider);
+            t.position = {e.position[0], e.position[1], e.position[2]};
+            t.normal = {e.normal[0], e.normal[1], e.normal[2]};
+            t.penetration = e.penetration;
+            t.normalImpulse = e.normal_impulse;
+            t.frictionImpulse = {e.friction_impulse[0], e.friction_impulse[1], e.friction_impulse[2]};
+            std::memcpy(staging.data() + sizeof(header) + k * sizeof(PmContactEvent), &t, sizeof(t));
+        }
+        int rc = pmb_copy_async(device->ordinal, copied.buffer->ptr + copied.offset, staging.data(),
+                                uint64_t(required), device->stream);
+        if (rc == PMB_SUCCESS) rc = pmb_stream_synchronize(device->ordinal, device->stream);
+        return from_core(rc);
     });
 }
 
@@ -712,6 +775,7 @@ PFN_pmVoidFunction lookup_rigid(const char* name) {
     PM_ENTRY(pmCmdStepSimulation)
     PM_ENTRY(pmCmdCopyRigidStates)
     PM_ENTRY(pmCmdCopyConstraintStates)
+    PM_ENTRY(pmCmdCopyContactEvents)
 #undef PM_ENTRY
     return nullptr;
 }

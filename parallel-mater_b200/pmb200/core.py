@@ -40,13 +40,18 @@ class WorldDesc(ctypes.Structure):
                 ("persistent_memory", ctypes.c_void_p), ("persistent_bytes", ctypes.c_uint64),
                 ("scratch_memory", ctypes.c_void_p), ("scratch_bytes", ctypes.c_uint64),
                 ("scene_count", ctypes.c_uint32), ("body_scene", ctypes.c_void_p),
-                ("scene_iterations", ctypes.c_void_p)]
+                ("scene_iterations", ctypes.c_void_p), ("event_capacity", ctypes.c_uint32)]
+
+
+EVENT_DTYPE = np.dtype([("body", "<u4"), ("collider", "<u4"), ("position", "<f4", 3), ("normal", "<f4", 3),
+                        ("penetration", "<f4"), ("normal_impulse", "<f4"), ("friction_impulse", "<f4", 3)])
+assert EVENT_DTYPE.itemsize == 52
 
 
 class WorldCapacity(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint32) for k in ("body_count", "joint_count", "mesh_count", "mesh_vertex_count",
                                                 "mesh_triangle_count", "candidate_capacity", "pair_capacity",
-                                                "contact_capacity")]
+                                                "contact_capacity", "event_capacity")]
 
 
 _lib = None
@@ -89,6 +94,7 @@ def lib():
             "pmb_world_mlp_params": [vp, vp, vp, vp, vp], "pmb_world_mlp_apply_mode": [vp, u32], "pmb_world_mlp_rows": [vp, vp, vp, u32, vp],
             "pmb_mlp_forward_backward": [i32, u32, vp, vp, vp, vp, vp, vp, vp],
             "pmb_world_set_warm_table": [vp, u32, vp, vp, u32],
+            "pmb_world_contact_events": [vp, vp, u32, vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -141,7 +147,7 @@ class World:
     """A rigid world resident on one GPU, stepped by the CUDA kernels."""
 
     def __init__(self, scene: Scene, device=0, candidate_capacity=0, pair_capacity=0,
-                 contact_capacity=0):
+                 contact_capacity=0, event_capacity=0):
         self.scene = scene
         L = lib()
         s = scene
@@ -151,6 +157,7 @@ class World:
         b, st, vo, v, io, i, j = self._keep
         d = WorldDesc(len(b), _p(b), _p(st), len(vo) - 1, _p(vo), _p(v), _p(io), _p(i), len(j), _p(j),
                       candidate_capacity, pair_capacity, contact_capacity, device)
+        d.event_capacity = event_capacity
         if s.body_scene is not None:
             bs = np.ascontiguousarray(s.body_scene, np.uint32)
             si = np.ascontiguousarray(s.scene_iterations if s.scene_iterations is not None
@@ -253,6 +260,17 @@ class World:
         _check(lib().pmb_world_residual_trace(self.h, out.ctypes.data, 256, ctypes.byref(n)),
                "residual_trace")
         return out[:n.value]
+
+    def contact_events(self):
+        """The last tick's contact events (EVENT_DTYPE records), or an empty
+        array when that tick did not collect them."""
+        n = ctypes.c_uint32()
+        _check(lib().pmb_world_contact_events(self.h, None, 0, ctypes.byref(n)), "pmb_world_contact_events")
+        out = np.zeros(n.value, EVENT_DTYPE)
+        if n.value:
+            _check(lib().pmb_world_contact_events(self.h, out.ctypes.data, n.value, ctypes.byref(n)),
+                   "pmb_world_contact_events")
+        return out
 
     def snapshot(self):
         _check(lib().pmb_world_snapshot(self.h), "snapshot")

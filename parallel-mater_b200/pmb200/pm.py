@@ -90,6 +90,12 @@ BufferView = S("PmBufferView", [("range", BufferRange), ("format", i32), ("count
 GeometryCreateInfo = S("PmGeometryCreateInfo", [
     ("sType", i32), ("pNext", vp), ("vertices", BufferView), ("indices", BufferView),
     ("queueFamilyIndex", u32)])
+# PmContactEvent (parallel_mater.h:959-968)
+PM_EVENT_DTYPE = np.dtype([("type", "<u4"), ("first", "<u4"), ("second", "<u4"), ("position", "<f4", 3),
+                           ("normal", "<f4", 3), ("penetration", "<f4"), ("normalImpulse", "<f4"),
+                           ("frictionImpulse", "<f4", 3)])
+assert PM_EVENT_DTYPE.itemsize == 56
+
 SimulationCreateInfo = S("PmSimulationCreateInfo", [
     ("sType", i32), ("pNext", vp), ("queueFamilyIndex", u32), ("rigidBodyCapacity", u32),
     ("constraintCapacity", u32), ("contactCapacity", u32), ("fluidCount", u32), ("pFluidCapacities", vp),
@@ -190,6 +196,7 @@ SIGNATURES = {
     "pmCreatePhysicsPipeline": (R, [P, P, P]),
     "pmDestroyPhysicsPipeline": (V, [P, P]),
     "pmCmdCopyConstraintStates": (R, [P, P, u32, u32, P]),
+    "pmCmdCopyContactEvents": (R, [P, P, P]),
     "pmCreateCommandPool": (R, [P, P, P]),
     "pmDestroyCommandPool": (V, [P, P]),
     "pmResetCommandPool": (R, [P, P]),
@@ -285,7 +292,7 @@ class RigidSession:
     """A Scene driven through the pm* API on one device (realtime profile,
     dt = 1/60 s, one substep, as the reference's command path requires)."""
 
-    def __init__(self, scene: Scene, physical_index=0, iterations=8):
+    def __init__(self, scene: Scene, physical_index=0, iterations=8, contact_capacity=4096):
         self.scene = scene
         boot = Api()
         inst = vp()
@@ -319,7 +326,8 @@ class RigidSession:
         self._buffers = []
         self.geometries = [self._geometry(m) for m in range(len(scene.mesh_vertex_offsets) - 1)]
         # simulation
-        sci = SimulationCreateInfo(ST_SIMULATION, None, 0, scene.n, max(len(scene.joints), 0), 0)
+        sci = SimulationCreateInfo(ST_SIMULATION, None, 0, scene.n, max(len(scene.joints), 0), contact_capacity)
+        self.contact_capacity = contact_capacity
         sim = vp()
         check(self.api.pmCreateSimulation(dev, ref(sci), ref(sim)), "pmCreateSimulation")
         self.sim = sim
@@ -345,6 +353,9 @@ class RigidSession:
         # state read-back buffer in host-visible memory
         self.state_bytes = 52 * scene.n
         self.state_mem, self.state_buf, self.state_ptr = self._mapped_buffer(self.state_bytes)
+        # contact-event read-back: PmDomainOutputHeader + PmContactEvent records
+        self.event_bytes = 16 + 56 * contact_capacity
+        self.event_mem, self.event_buf, self.event_ptr = self._mapped_buffer(self.event_bytes)
         fence = vp()
         check(self.api.pmCreateFence(dev, 0, ref(fence)), "pmCreateFence")
         self.fence = fence
@@ -472,12 +483,16 @@ class RigidSession:
         return SUCCESS
 
     # ---- public
-    def step(self, gravity=(0.0, -9.81, 0.0), inputs=None, targets=None, states=True, statistics=False):
+    def step(self, gravity=(0.0, -9.81, 0.0), inputs=None, targets=None, states=True, statistics=False,
+             events=False, copy_events=None):
         """One tick; returns the submission result. inputs: list of
         (body, force, torque, linear impulse, angular impulse); targets:
         {body: state record}. statistics: wrap the step in a step-statistics
-        query, read afterwards with step_statistics()."""
-        step = StepInfo(1.0 / 60.0, 1, (f32 * 3)(*gravity), 0)
+        query, read afterwards with step_statistics(). events: collect the
+        tick's contact events; copy_events (default: events) records
+        pmCmdCopyContactEvents after the step (read with contact_events())."""
+        copy_events = events if copy_events is None else copy_events
+        step = StepInfo(1.0 / 60.0, 1, (f32 * 3)(*gravity), 1 if events else 0)
         if statistics and getattr(self, "query_pool", None) is None:
             qp = vp()
             check(self.api.pmCreateQueryPool(self.dev, ref(QueryPoolCreateInfo(ST_QUERY_POOL, None,
@@ -505,7 +520,18 @@ class RigidSession:
                 rng = BufferRange(self.state_buf, 0, self.state_bytes)
                 check(self.api.pmCmdCopyRigidStates(self.cb, self.sim, 0, self.scene.n, ref(rng)),
                       "pmCmdCopyRigidStates")
+            if copy_events:
+                rng = BufferRange(self.event_buf, 0, self.event_bytes)
+                check(self.api.pmCmdCopyContactEvents(self.cb, self.sim, ref(rng)), "pmCmdCopyContactEvents")
         return self._record(rec)
+
+    def contact_events(self):
+        """(activeCount, capacity, revision), PM_EVENT_DTYPE records of the
+        last pmCmdCopyContactEvents."""
+        raw = bytes((C.c_uint8 * self.event_bytes).from_address(self.event_ptr))
+        count, capacity, revision = np.frombuffer(raw[:16], np.dtype([("n", "<u4"), ("c", "<u4"), ("r", "<u8")]))[0]
+        return (int(count), int(capacity), int(revision)), np.frombuffer(raw[16:16 + 56 * int(count)],
+                                                                         PM_EVENT_DTYPE).copy()
 
     def set_states(self, first, states):
         arr = (RigidState * len(states))(*[_state(s) for s in states])

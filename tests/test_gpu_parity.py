@@ -222,3 +222,25 @@ def test_launch_plans_are_bit_identical_on_the_settled_pile(gpu_available):
             ref = x
         assert np.array_equal(x, ref), (v, p)
         w.close()
+
+
+def test_contact_events_match_oracle(gpu_available):
+    """Contact events (every point of every active pair in order, penetration
+    clamped at 0, the tick's normal and friction impulses): bodies, points,
+    normals and penetrations equal the oracle's bits; impulses agree within
+    the solver's float tolerance."""
+    s = scenes.box_pile((4, 3, 4), seed=21, spacing=1.6, count=40)
+    w = core.World(s, event_capacity=100000)
+    o = O.OracleWorld(s)
+    for t in range(40):
+        w.step(collect_events=1)
+        o.step()
+        g, r = w.contact_events(), o.contact_events()
+        assert len(g) == len(r), t
+        for k in ("body", "collider", "position", "normal", "penetration"):
+            assert np.array_equal(g[k].view(np.uint32), r[k].view(np.uint32)), (t, k)
+        for k in ("normal_impulse", "friction_impulse"):
+            assert np.allclose(g[k], r[k], rtol=2e-3, atol=2e-4), (t, k)
+    w.step()
+    assert len(w.contact_events()) == 0
+    w.close()

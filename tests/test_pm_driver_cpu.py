@@ -79,7 +79,7 @@ def test_every_rigid_command_resolves_and_other_domains_do_not(drv):
     try:
         for name in pm.SIGNATURES:
             assert drv.pm_driverGetInstanceProcAddr(inst, name.encode()), name
-        for name in ("pmCmdWriteFluidParticles", "pmCreateFluid", "pmCmdWriteCloth", "pmCmdCopyContactEvents",
+        for name in ("pmCmdWriteFluidParticles", "pmCreateFluid", "pmCmdWriteCloth", "pmCmdCopyDebugData",
                      "pmImportNativeDevice", "pmCmdWriteSmoke", "pmNotACommand"):
             assert not drv.pm_driverGetInstanceProcAddr(inst, name.encode()), name
     finally:

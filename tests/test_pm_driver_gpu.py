@@ -213,7 +213,12 @@ def test_error_codes(gpu_available):
         two = pm.StepInfo(1.0 / 60.0, 2, (ctypes.c_float * 3)(0, -9.81, 0), 0)
         assert a.pmCmdStepSimulation(cb, s.sim, ctypes.byref(two)) == pm.ERROR_INVALID_ARGUMENT
         events = pm.StepInfo(1.0 / 60.0, 1, (ctypes.c_float * 3)(0, -9.81, 0), 1)
-        assert a.pmCmdStepSimulation(cb, s.sim, ctypes.byref(events)) == pm.ERROR_FEATURE_NOT_PRESENT
+        assert a.pmCmdStepSimulation(cb, s.sim, ctypes.byref(events)) == 0
+        other = pm.StepInfo(1.0 / 60.0, 1, (ctypes.c_float * 3)(0, -9.81, 0), 2)
+        assert a.pmCmdStepSimulation(cb, s.sim, ctypes.byref(other)) == pm.ERROR_INVALID_ARGUMENT
+        assert a.pmCmdCopyContactEvents(cb, s.sim, None) == pm.ERROR_INVALID_ARGUMENT
+        short = pm.BufferRange(s.event_buf, 0, 8)
+        assert a.pmCmdCopyContactEvents(cb, s.sim, ctypes.byref(short)) == pm.ERROR_INVALID_ARGUMENT
         # an input on the static body fails when the submission executes
         bad = pm.RigidInput(0, (ctypes.c_float * 3)(1, 0, 0))
         assert a.pmCmdApplyRigidInputs(cb, s.sim, 1, ctypes.byref(bad)) == 0
@@ -231,3 +236,40 @@ def test_error_codes(gpu_available):
                                    ctypes.byref(mem)) == pm.ERROR_FEATURE_NOT_PRESENT
     finally:
         s.close()
+
+
+def test_contact_events_through_the_api_match_the_core_world(gpu_available):
+    """pmCmdCopyContactEvents: header (events, contact capacity, steps taken)
+    and one record per contact point, bodies as slots; the records carry the
+    bits of the core world's events for the same ticks, and capacity bounds
+    the count."""
+    scene = pm.canonical_scene(scenes.pyramid(levels=5, seed=2, profile=scenes.REALTIME))
+    s = pm.RigidSession(scene, contact_capacity=4096)
+    w = core.World(scene, event_capacity=4096)
+    try:
+        for t in range(12):
+            assert s.step(events=True) == 0
+            st = w.step(collect_events=1)
+            (count, capacity, revision), ev = s.contact_events()
+            want = w.contact_events()
+            assert capacity == 4096 and revision == t + 1
+            assert count == len(want) == int(st["contacts"]) > 0
+            assert (ev["type"] == 0).all()
+            assert np.array_equal(ev["first"], want["body"]) and np.array_equal(ev["second"], want["collider"])
+            for a, b in (("position", "position"), ("normal", "normal"), ("penetration", "penetration"),
+                         ("normalImpulse", "normal_impulse"), ("frictionImpulse", "friction_impulse")):
+                assert np.array_equal(ev[a].view(np.uint32), want[b].view(np.uint32)), (t, a)
+        assert s.step(events=False, copy_events=True) == 0
+        (count, _, revision), _ = s.contact_events()
+        assert count == 0 and revision == 13
+    finally:
+        s.close()
+        w.close()
+    small = pm.RigidSession(scene, contact_capacity=5)
+    try:
+        for _ in range(3):
+            assert small.step(events=True) == 0
+        (count, capacity, _), ev = small.contact_events()
+        assert count == 5 and capacity == 5
+    finally:
+        small.close()
