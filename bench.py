@@ -15,8 +15,9 @@ sweeps. Inputs are synthetic (seeded); no dataset is involved.
 GPU arm (default): the warm-start MLP is first trained online on
 --train-frames plain ticks (untimed); then, from the same settled snapshot,
 --steps ticks are timed with the plain warm start and --steps with the
-learned one. `value` is the learned arm's steps/s with the state resident in
-HBM, timed with CUDA events on the world's stream (max over ranks); the plain
+learned one, each as CUDA-graph replays of two ticks. `value` is the learned
+arm's steps/s with the state resident in HBM, timed with CUDA events on the
+world's stream (max over ranks); the plain
 arm's steps/s and both arms' sweep counts are in `config`. `e2e` is the
 learned arm through the C ABI with host buffers (state upload from pinned
 host memory, tick, state download each step). Multi-GPU runs independent replicas
@@ -162,15 +163,26 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
-def timed_ticks(world, desc, steps, stream, torch):
-    """CUDA-event time (ms) of `steps` ticks enqueued on the world's stream."""
+def graph_ticks(world, desc, steps, stream, torch, core, before=None):
+    """CUDA-event time (ms) of `steps` ticks (even) as CUDA-graph replays of
+    two ticks on the world's stream, from the world's snapshot, and the
+    kernels they launch. The graph is captured and replayed once untimed
+    first; `before` runs right before the timed replays."""
+    world.restore()
+    l0 = core.kernel_launches()
+    world.capture(steps=2, desc=desc)
+    per_replay = core.kernel_launches() - l0
+    world.replay()
+    world.restore()
+    if before:
+        before()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record(stream)
-    for _ in range(steps):
-        world.step(desc, stats=False)
+    for _ in range(steps // 2):
+        world.replay()
     end.record(stream)
     torch.cuda.synchronize()
-    return start.elapsed_time(end)
+    return start.elapsed_time(end), per_replay * (steps // 2)
 
 
 def replay_stats(world, desc, steps):
@@ -195,8 +207,9 @@ def gpu_arm(args):
     plain = scene.step_desc(residual_tolerance=args.tolerance, max_iterations=args.max_iterations)
     learned = scene.step_desc(residual_tolerance=args.tolerance, max_iterations=args.max_iterations, warm_start=1)
     world = core.World(scene, device=local, contact_capacity=args.contact_capacity)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()             # a capturable (non-default) stream for the graph
     world.set_stream(stream.cuda_stream)
+    steps = args.steps + (args.steps & 1)
 
     def barrier():
         if world_size > 1:
@@ -224,32 +237,29 @@ def gpu_arm(args):
     world.mlp_train(False)
     train_s = time.perf_counter() - t0
 
-    # ---- plain arm, device-resident, from the settled snapshot (clocks are
-    # sampled over both timed arms)
-    world.restore()
-    barrier()
-    torch.cuda.synchronize()
+    # ---- plain arm, device-resident, from the settled snapshot, as CUDA-graph
+    # replays (clocks are sampled over both timed arms)
+    sync = lambda: (barrier(), torch.cuda.synchronize())
     sampler = ClockSampler(local)
     sampler.start()
-    plain_ms = max_over_ranks(timed_ticks(world, plain, args.steps, stream, torch))
+    plain_ms, _ = graph_ticks(world, plain, steps, stream, torch, core, before=sync)
+    plain_ms = max_over_ranks(plain_ms)
 
     # ---- learned arm: the headline number
-    world.restore()
-    barrier()
-    torch.cuda.synchronize()
-    world.solve_timer(True)
-    launches0 = core.kernel_launches()
     torch.cuda.nvtx.range_push("learned_arm")
-    learned_ms = max_over_ranks(timed_ticks(world, learned, args.steps, stream, torch))
+    learned_ms, launches = graph_ticks(world, learned, steps, stream, torch, core, before=sync)
     torch.cuda.nvtx.range_pop()
+    learned_ms = max_over_ranks(learned_ms)
     barrier()
     clocks = sampler.stop()
-    launches = core.kernel_launches() - launches0
+    # per-tick statistics and the solve kernel's event time (plain launches)
+    world.restore()
+    world.solve_timer(True)
+    learned_stats = [world.step(learned) for _ in range(steps)]
     solve_ms, solve_launches = world.solve_timer(False)
-    learned_stats = replay_stats(world, learned, args.steps)
-    plain_stats = replay_stats(world, plain, args.steps)
-    value = world_size * args.steps / (learned_ms * 1e-3)
-    plain_value = world_size * args.steps / (plain_ms * 1e-3)
+    plain_stats = replay_stats(world, plain, steps)
+    value = world_size * steps / (learned_ms * 1e-3)
+    plain_value = world_size * steps / (plain_ms * 1e-3)
 
     alg_bytes = sum(solve_bytes(st, n_dyn) for st in learned_stats)
     achieved = alg_bytes / (solve_ms * 1e-3) / 1e9 if solve_ms > 0 else None
@@ -277,12 +287,12 @@ def gpu_arm(args):
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         world.set_states(host_np)            # h2d: the step's input states
         world.step(learned, stats=False)
         host_np[:] = world.states()          # d2h: the step's result
     torch.cuda.synchronize()
-    e2e_value = world_size * args.steps / max_over_ranks(time.perf_counter() - t0)
+    e2e_value = world_size * steps / max_over_ranks(time.perf_counter() - t0)
     state_bytes = scene.n * 52
 
     cpu = None
@@ -298,7 +308,7 @@ def gpu_arm(args):
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world_size,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": learned_ms / args.steps,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": learned_ms / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": "box pile 64x32x32 (65,536 boxes + ground and walls), settled state, "
@@ -319,6 +329,7 @@ def gpu_arm(args):
                        "launch_plan": {"solve_threads": [512, 384, 256][plan_v],
                                        "lanes_per_body": LANE_POLICIES[plan_p]},
                        "parallelism": f"replicas x{world_size}",
+                       "tick": "CUDA graph replays (one graph = two ticks); e2e: one pmb_world_step per tick",
                        "l2": "inputs larger than L2: per-tick working set ~%d MB (126 MB L2)" % int(
                            (mean(learned_stats, "contacts") * (8 + 9) * 16 + scene.n * 400 + 1.2e6 * 24) / 1e6)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -562,6 +573,7 @@ def gpu_batched(args):
                        "residual_max_plain": float(allm[:, 2].max()),
                        "residual_max_learned": float(allm[:, 3].max()),
                        "scenes_learned_at_or_below_plain": int(np.sum(ratio[has] <= 1.0)),
+                       "scenes_learned_above_10x_plain": int(np.sum(allm[has, 3] > 10.0 * np.maximum(allm[has, 2], 1e-6))),
                        "scenes_with_contacts": int(has.sum()),
                        "mlp_training": {"frames": train, "adam_lr": args.mlp_lr, "steps_per_frame": args.mlp_steps,
                                         "loss_over_plain_loss": mlp_loss / mlp_plain_loss if mlp_plain_loss else None,

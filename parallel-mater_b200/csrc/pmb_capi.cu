@@ -293,7 +293,7 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     ALLOC(d.cand_count, n + 1); ALLOC(d.cand_off, n + 1); ALLOC(d.cand_lane, kQueryLanes * size_t(n));
     ALLOC(d.cand_a, cap_cand); ALLOC(d.cand_b, cap_cand);
     ALLOC(d.np_count, cap_cand); ALLOC(d.np_scan, cap_cand + 1); ALLOC(d.np_stage, cap_cand);
-    ALLOC(d.np_list, cap_cand);
+    ALLOC(d.np_list, cap_cand); ALLOC(d.np_sat, cap_cand);
     ALLOC(d.st_n, cap_contact); ALLOC(d.st_p, cap_contact);
     ALLOC(d.act_a, cap_pair); ALLOC(d.act_b, cap_pair); ALLOC(d.act_code, cap_pair);
     ALLOC(d.act_off, cap_pair + 1); ALLOC(d.act_cnt, cap_pair); ALLOC(d.act_impact, cap_pair);
@@ -317,6 +317,7 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     ALLOC(d.deg, n); ALLOC(d.inc_off, n + 1); ALLOC(d.inc_cursor, n); ALLOC(d.inc_list, 2 * cap_pair);
     ALLOC(d.jdeg, n); ALLOC(d.jinc_off, n + 1); ALLOC(d.jinc_cursor, n); ALLOC(d.jinc_list, 2 * size_t(nj) + 2);
     ALLOC(d.corder, n); ALLOC(d.cdirty, 2 * size_t(n));
+    ALLOC(d.nbr, 2 * cap_pair + 2 * size_t(nj) + 2); ALLOC(d.nlow, n); ALLOC(d.nhigh, n);
     ALLOCP(d.events, z.events);
     ALLOC(d.rcount, n); ALLOC(d.roff, n + 1); ALLOC(d.blist, 2 * cap_contact); ALLOC(d.bother, 2 * cap_contact);
     ALLOCP(d.joints, nj); ALLOCS(d.jstate, nj); ALLOCS(d.jrows, size_t(nj) * 18);

@@ -521,13 +521,19 @@ __global__ void k_mlp_apply(Dev d, const MlpMeta* meta, const float* out, uint32
         for (uint32_t p = 0; p < cnt; ++p) {
             const uint32_t c = off + p;
             const MlpMeta m = meta[c];
+            // Trust region: a prediction moves the plain warm start by at most
+            // kMaxCorrection in its log space (a factor of 10 in penalty), so
+            // an input unlike the training contacts cannot soften or stiffen a
+            // contact without bound.
             const float o0 = (mode & 4u) ? mean0 : out[2 * size_t(c)], o1 = out[2 * size_t(c) + 1];
             if (mode & 1u) {
-                const float lam = fmaxf(m.scale * expm1f(m.y0 + o0 * (1.0f / kLamOut)), 0.0f);
+                const float dl = fminf(fmaxf(o0 * (1.0f / kLamOut), -kMaxCorrection), kMaxCorrection);
+                const float lam = fmaxf(m.scale * expm1f(m.y0 + dl), 0.0f);
                 if (isfinite(lam)) reinterpret_cast<float*>(d.c_lam + c)[0] = lam;
             }
             if (mode & 2u) {
-                const float pen = fminf(fmaxf(exp10f(m.y1 + o1 * (1.0f / kPenOut)), 1.0f), 1.0e10f);
+                const float dk = fminf(fmaxf(o1 * (1.0f / kPenOut), -kMaxCorrection), kMaxCorrection);
+                const float pen = fminf(fmaxf(exp10f(m.y1 + dk), 1.0f), 1.0e10f);
                 if (isfinite(pen)) reinterpret_cast<float*>(d.c_pen + c)[0] = pen;
             }
         }

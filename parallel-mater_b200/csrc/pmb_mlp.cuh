@@ -33,6 +33,8 @@ constexpr uint32_t kMlpPartial = kMlpParams + 2;
 // o1 = kPenOut * correction of log10(penalty).
 constexpr float kLamOut = 4.0f;
 constexpr float kPenOut = 100.0f;
+// Largest applied correction in those log spaces (1 = a decade of penalty).
+constexpr float kMaxCorrection = 1.0f;
 
 // BF16 weight images in the tensor cores' shared-memory layout (no swizzle,
 // K-major core matrices of 8 rows x 16 bytes), copied into shared memory

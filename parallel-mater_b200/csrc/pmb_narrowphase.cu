@@ -103,11 +103,21 @@ __device__ __forceinline__ bool same_plane(float4 a, float4 b) {
            __float_as_uint(a.z) == __float_as_uint(b.z) && __float_as_uint(a.w) == __float_as_uint(b.w);
 }
 
-// The separating-axis test of face_manifold alone: true exactly when some
-// reference-face plane separates the pair by more than `reach`, i.e. when
-// face_manifold's maximum separation exceeds reach and it returns an empty
-// manifold. Same arithmetic, stopping at the first separating plane.
-__device__ bool face_separated(const Pose& bs, const MeshRef& bm, const Pose& cs, const MeshRef& cm, float reach) {
+// The separating-axis test of face_manifold (geometry.slang:1606-1640): the
+// largest separation over every reference-face plane of both meshes (support
+// = min over the other mesh's vertices), the face and side that give it. A
+// plane equal to the one before it (a quad's second triangle) gives the same
+// separation, which never wins the strict max, and is skipped. With
+// `stop_above`, returns as soon as a separation exceeds it (the pair then
+// has an empty manifold, whatever the later planes give).
+struct FaceSat {
+    float best;
+    uint32_t ref_face;
+    bool ref_body;
+};
+__device__ FaceSat face_sat(const Pose& bs, const MeshRef& bm, const Pose& cs, const MeshRef& cm,
+                            float stop_above = kFltMax) {
+    FaceSat r{-kFltMax, 0u, false};
     for (uint32_t side = 0; side < 2; ++side) {
         const MeshRef& rm = side == 0 ? cm : bm;
         const Pose& rs = side == 0 ? cs : bs;
@@ -122,46 +132,30 @@ __device__ bool face_separated(const Pose& bs, const MeshRef& bm, const Pose& cs
             float support = kFltMax;
             for (uint32_t k = 0; k < im.nv; ++k) support = fminf(support, dot(in, pv(im, k)));
             float sep = support + dot(n, rel) - pl.w;
-            if (sep > reach) return true;
+            if (sep > r.best) {
+                r.best = sep;
+                r.ref_face = f;
+                r.ref_body = side != 0;
+                if (sep > stop_above) return r;
+            }
         }
     }
-    return false;
+    return r;
 }
 
-// geometry.slang:1606-1745
+// geometry.slang:1606-1745. `sat`: the pair's separating-axis result when the
+// caller already has it.
 __device__ bool face_manifold(const Pose& bs, const MeshRef& bm, const Pose& cs, const MeshRef& cm, float margin,
-                              float correction, Man& out) {
+                              float correction, Man& out, const FaceSat* sat = nullptr) {
     out.count = 0;
     out.impact = 1.0f;
     out.normal = {0, 0, 0};
     const float rest = fmn(margin, 1.0e-3f);
     const float reach = margin + correction;
-    float best = -kFltMax;
-    uint32_t ref_face = 0;
-    bool ref_body = false;
-    for (uint32_t side = 0; side < 2; ++side) {
-        const MeshRef& rm = side == 0 ? cm : bm;
-        const Pose& rs = side == 0 ? cs : bs;
-        const MeshRef& im = side == 0 ? bm : cm;
-        const Pose& is = side == 0 ? bs : cs;
-        const V3 rel = sub(is.x, rs.x);
-        for (uint32_t f = 0; f < rm.nt; ++f) {
-            float4 pl = rm.planes[f];
-            // A plane equal to the one before it (a quad's second triangle)
-            // gives the same separation, which never wins the strict max.
-            if (f != 0 && same_plane(pl, rm.planes[f - 1])) continue;
-            V3 n = rotate(rs.q, v3(pl));
-            V3 in = inv_rotate(is.q, n);
-            float support = kFltMax;
-            for (uint32_t k = 0; k < im.nv; ++k) support = fminf(support, dot(in, pv(im, k)));
-            float sep = support + dot(n, rel) - pl.w;
-            if (sep > best) {
-                best = sep;
-                ref_face = f;
-                ref_body = side != 0;
-            }
-        }
-    }
+    const FaceSat fs = sat ? *sat : face_sat(bs, bm, cs, cm);
+    const float best = fs.best;
+    const uint32_t ref_face = fs.ref_face;
+    const bool ref_body = fs.ref_body;
     if (best > reach) return true;
     const MeshRef& rm = ref_body ? bm : cm;
     const Pose& rs = ref_body ? bs : cs;
@@ -316,22 +310,30 @@ __device__ __forceinline__ CandidateMotion candidate_motion(const Dev& d, uint32
 
 // Pass 1, one thread per candidate: pairs that are not both convex, and
 // unswept pairs separated by a face plane, get an empty manifold here; the
-// rest go to the survivor list for pass 2. Light enough for full occupancy.
+// rest go to the survivor list for pass 2 with their separating-axis result.
+// Light enough for full occupancy.
 __global__ void __launch_bounds__(256) k_narrow_sat(Dev d) {
     const uint32_t total = d.ctr->n_cand;
     for (uint32_t k = grid_stride_begin(); k < total; k += grid_stride()) {
         const uint32_t a = d.cand_a[k], b = d.cand_b[k];
         const uint32_t ma = d.mesh[a], mb = d.mesh[b];
         bool empty = !(d.m_convex[ma] && d.m_convex[mb]);
+        FaceSat fs{0.0f, kInvalid, false};  // kInvalid face: no result kept (swept pair)
         if (!empty) {
             const CandidateMotion c = candidate_motion(d, a, b);
-            empty = !c.swept && face_separated(c.pred_a, mesh_ref(d, ma), c.pred_b, mesh_ref(d, mb), c.margin + c.corr);
+            if (!c.swept) {
+                const float reach = c.margin + c.corr;
+                fs = face_sat(c.pred_a, mesh_ref(d, ma), c.pred_b, mesh_ref(d, mb), reach);
+                empty = fs.best > reach;
+            }
         }
         if (empty) {
             d.np_count[k] = 0;
             d.np_scan[k] = 0ull;
         } else {
-            d.np_list[atomicAdd(&d.ctr->n_surv, 1u)] = k;
+            const uint32_t slot = atomicAdd(&d.ctr->n_surv, 1u);
+            d.np_list[slot] = k;
+            d.np_sat[slot] = make_uint2(__float_as_uint(fs.best), fs.ref_face | (fs.ref_body ? 0x80000000u : 0u));
         }
     }
 }
@@ -342,6 +344,7 @@ __global__ void __launch_bounds__(128) k_narrow(Dev d) {
     const uint32_t total = d.ctr->n_surv;
     for (uint32_t s = grid_stride_begin(); s < total; s += grid_stride()) {
         const uint32_t k = d.np_list[s];
+        const uint2 sat = d.np_sat[s];
         const uint32_t a = d.cand_a[k], b = d.cand_b[k];
         const uint32_t ma = d.mesh[a], mb = d.mesh[b];
         Man m;
@@ -351,7 +354,9 @@ __global__ void __launch_bounds__(128) k_narrow(Dev d) {
         bool ok = false;
         if (c.swept) ok = swept_face_manifold(c.prev_a, c.pred_a, bm, c.prev_b, c.pred_b, cm, c.margin, m);
         if (!ok) {
-            ok = face_manifold(c.pred_a, bm, c.pred_b, cm, c.margin, c.corr, m);
+            // An unswept pair's separating-axis result comes from pass 1.
+            const FaceSat fs{__uint_as_float(sat.x), sat.y & 0x7fffffffu, (sat.y >> 31) != 0};
+            ok = face_manifold(c.pred_a, bm, c.pred_b, cm, c.margin, c.corr, m, c.swept ? nullptr : &fs);
             if (c.swept && m.count == 0) ok = false;
         }
         if (!ok) m.count = 0;

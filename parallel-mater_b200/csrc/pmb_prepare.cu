@@ -359,24 +359,10 @@ __global__ void k_graph_islands(Dev d) {
 // Colour fixpoint (persistent cooperative kernel).
 __device__ __forceinline__ uint32_t mex_lower(const Dev& d, uint32_t v, bool& overflow) {
     uint64_t mask[4] = {0, 0, 0, 0};
-    const uint32_t so = d.inc_off[v], sn = d.deg[v];
-    for (uint32_t k = 0; k < sn; ++k) {
-        const uint32_t p = d.inc_list[so + k];
-        const uint32_t a = d.act_a[p], b = d.act_b[p];
-        const uint32_t u = a == v ? b : a;
-        if (u < v && d.motion[u] == kDynamic) {
-            uint32_t c = ((volatile uint32_t*)d.color)[u];
-            if (c < kMaxColors) mask[c >> 6] |= 1ull << (c & 63);
-        }
-    }
-    const uint32_t jo = d.jinc_off[v], jn = d.jdeg[v];
-    for (uint32_t k = 0; k < jn; ++k) {
-        const JointState st = d.jstate[d.jinc_list[jo + k]];
-        const uint32_t u = st.dense_a == v ? st.dense_b : st.dense_a;
-        if (u < v && d.motion[u] == kDynamic) {
-            uint32_t c = ((volatile uint32_t*)d.color)[u];
-            if (c < kMaxColors) mask[c >> 6] |= 1ull << (c & 63);
-        }
+    const uint32_t base = d.inc_off[v] + d.jinc_off[v], nl = d.nlow[v];
+    for (uint32_t k = 0; k < nl; ++k) {
+        const uint32_t c = ((volatile uint32_t*)d.color)[d.nbr[base + k]];
+        if (c < kMaxColors) mask[c >> 6] |= 1ull << (c & 63);
     }
     for (int w = 0; w < 4; ++w)
         if (~mask[w]) return uint32_t(w * 64 + __ffsll((long long)~mask[w]) - 1);
@@ -384,22 +370,41 @@ __device__ __forceinline__ uint32_t mex_lower(const Dev& d, uint32_t v, bool& ov
     return kMaxColors - 1;
 }
 
+// Each body's dynamic neighbours through contacts and joints, for the colour
+// rounds: lower-indexed ones from the front of its segment (nlow of them),
+// higher-indexed ones from the back (nhigh). Segment base = inc_off + jinc_off
+// (room for deg + jdeg entries).
+__global__ void k_neighbour_lists(Dev d) {
+    for (uint32_t v = grid_stride_begin(); v < d.n; v += grid_stride()) {
+        if (d.motion[v] != kDynamic) continue;
+        const uint32_t base = d.inc_off[v] + d.jinc_off[v], len = d.deg[v] + d.jdeg[v];
+        uint32_t lo = 0, hi = 0;
+        auto add = [&](uint32_t u) {
+            if (d.motion[u] != kDynamic || u == v) return;
+            if (u < v) d.nbr[base + lo++] = u;
+            else d.nbr[base + len - 1 - hi++] = u;
+        };
+        const uint32_t so = d.inc_off[v], sn = d.deg[v];
+        for (uint32_t k = 0; k < sn; ++k) {
+            const uint32_t p = d.inc_list[so + k];
+            const uint32_t a = d.act_a[p], b = d.act_b[p];
+            add(a == v ? b : a);
+        }
+        const uint32_t jo = d.jinc_off[v], jn = d.jdeg[v];
+        for (uint32_t k = 0; k < jn; ++k) {
+            const JointState st = d.jstate[d.jinc_list[jo + k]];
+            add(st.dense_a == v ? st.dense_b : st.dense_a);
+        }
+        d.nlow[v] = lo;
+        d.nhigh[v] = hi;
+    }
+}
+
 // Mark v's higher-indexed dynamic neighbours for the next round: only their
 // mex can depend on v's colour.
 __device__ __forceinline__ void mark_higher(const Dev& d, uint32_t v, uint8_t* next) {
-    const uint32_t so = d.inc_off[v], sn = d.deg[v];
-    for (uint32_t k = 0; k < sn; ++k) {
-        const uint32_t p = d.inc_list[so + k];
-        const uint32_t a = d.act_a[p], b = d.act_b[p];
-        const uint32_t u = a == v ? b : a;
-        if (u > v && d.motion[u] == kDynamic) next[u] = 1;
-    }
-    const uint32_t jo = d.jinc_off[v], jn = d.jdeg[v];
-    for (uint32_t k = 0; k < jn; ++k) {
-        const JointState st = d.jstate[d.jinc_list[jo + k]];
-        const uint32_t u = st.dense_a == v ? st.dense_b : st.dense_a;
-        if (u > v && d.motion[u] == kDynamic) next[u] = 1;
-    }
+    const uint32_t end = d.inc_off[v] + d.jinc_off[v] + d.deg[v] + d.jdeg[v];
+    for (uint32_t k = end - d.nhigh[v]; k < end; ++k) next[d.nbr[k]] = 1;
 }
 
 // Jacobi rounds towards the greedy colouring in index order (colour of v =
@@ -523,6 +528,8 @@ void launch_graph(const Dev& d, const StepParams& sp, cudaStream_t s, int coop_b
     k_graph_islands<<<blocks_for(d.n), kBlock, 0, s>>>(d);
     ++g_kernel_launches;
     prof_mark(s, "graph lists+islands");
+    k_neighbour_lists<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    ++g_kernel_launches;
     cudaMemsetAsync(d.cdirty, 0, 2 * size_t(d.n), s);
     void* args[] = {const_cast<Dev*>(&d)};
     cudaLaunchCooperativeKernel(color_kernel_ptr, dim3(coop_blocks), dim3(kColorThreads), args, 0, s);

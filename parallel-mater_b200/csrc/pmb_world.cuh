@@ -185,6 +185,7 @@ struct Dev {
     uint64_t* np_scan;
     uint32_t* np_stage;
     uint32_t* np_list;  // candidates surviving the separating-axis pass
+    uint2* np_sat;      // their separation (float bits) and reference face (bit 31: side)
     float4 *st_n, *st_p;
     // active pairs / contacts
     uint32_t *act_a, *act_b, *act_code, *act_off, *act_cnt, *act_impact;
@@ -205,6 +206,7 @@ struct Dev {
     uint32_t *jdeg, *jinc_off, *jinc_cursor, *jinc_list;
     uint32_t* corder;
     uint8_t* cdirty;  // colour rounds: two flag arrays of n (bodies to revisit)
+    uint32_t *nbr, *nlow, *nhigh;  // dynamic neighbours per body (k_neighbour_lists)
     ContactEvent* events;
     uint32_t event_capacity;
     uint32_t *rcount, *roff, *blist;  // per-body flattened contact rows (bit 31: second body)
