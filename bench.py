@@ -43,7 +43,8 @@ GRID = (64, 32, 32)
 SEED = 4
 SETTLED = os.path.join(ROOT, "tests", "golden", "settled_pile_64x32x32.npz")
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "k_solve_pile65k.md")
-LANE_POLICIES = ["8/16/32 by colour size", "8", "8/16/32 by body rows, heaviest first"]
+LANE_POLICIES = ["8/16/32 by colour size", "8", "8/16/32 by body rows, heaviest first",
+                 "8/16/32 by colour size, bodies claimed dynamically"]
 
 
 def parse():

@@ -375,7 +375,8 @@ PMB_API int pmb_world_scene_stats(pmb_world* world, float* residual, float* resi
  * more registers); solve_policy 0 = 8, 16 or 32 lanes per body chosen per
  * colour by its size, 1 = always 8, 2 = per body by its contact rows (more
  * than 16: 32 lanes, 9-16: 16, else 8; heaviest bodies first) unless 32-lane
- * groups cover the whole colour. Every plan computes bit-identical results;
+ * groups cover the whole colour, 3 = widths as 0 with the colour's bodies
+ * claimed dynamically from a counter. Every plan computes bit-identical results;
  * only the speed differs. A new world starts with (1, 0). */
 PMB_API int pmb_world_set_launch_plan(pmb_world* world, uint32_t solve_variant, uint32_t solve_policy);
 /* Time `ticks` ticks of every plan from the current state (restored before

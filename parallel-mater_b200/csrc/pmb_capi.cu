@@ -708,6 +708,15 @@ int pmb_world_profile_step(pmb_world* w, const pmb_step_desc* step, char* report
                       hc.dbg_rn, hc.dbg_body[0] * 1e-3, hc.dbg_body[1] * 1e-3, hc.dbg_body[2] * 1e-3, hc.dbg_body[3] * 1e-3,
                       hc.dbg_body[4] * 1e-3);
         text += line;
+        if (hc.dbg_sum[6]) {
+            const double nb = double(hc.dbg_sum[6]);
+            std::snprintf(line, sizeof(line),
+                          "  colour 0 mean over %.0f bodies (mean rn %.1f): stage %.1f gather %.1f solve %.1f crossing "
+                          "%.1f solve2 %.1f us\n",
+                          nb, hc.dbg_sum[7] / nb, hc.dbg_sum[0] * 1e-3 / nb, hc.dbg_sum[1] * 1e-3 / nb,
+                          hc.dbg_sum[2] * 1e-3 / nb, hc.dbg_sum[3] * 1e-3 / nb, hc.dbg_sum[4] * 1e-3 / nb);
+            text += line;
+        }
     }
     g_prof = Prof{};
     std::snprintf(report, capacity, "%s", text.c_str());
@@ -1322,8 +1331,8 @@ int pmb_world_scene_stats(pmb_world* w, float* residual, float* residual_max, ui
     return PMB_SUCCESS;
 }
 
-constexpr uint32_t kSolvePolicies = 3;
-const char* const kPolicyNames[kSolvePolicies] = {"per colour", "8 lanes   ", "per body  "};
+constexpr uint32_t kSolvePolicies = 4;
+const char* const kPolicyNames[kSolvePolicies] = {"per colour", "8 lanes   ", "per body  ", "claimed   "};
 
 int pmb_world_set_launch_plan(pmb_world* w, uint32_t solve_variant, uint32_t solve_policy) {
     if (!w || solve_variant >= kSolveVariants || solve_policy >= kSolvePolicies) return PMB_ERROR_INVALID_ARGUMENT;

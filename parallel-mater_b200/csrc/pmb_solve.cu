@@ -277,10 +277,13 @@ __device__ __forceinline__ unsigned long long gtimer() {
 }
 template <int G>
 __device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float dt, GroupRows<G>& sm,
-                                 uint32_t gmask, int gl, int gbase, bool trace = false) {
+                                 uint32_t gmask, int gl, int gbase, uint32_t trace = 0) {
+    // trace 1: slowest body of the colour per stage; 2: stage times summed
+    // over the colour's bodies (profiling only).
     const unsigned long long t0 = trace ? gtimer() : 0ull;
     auto mark = [&](int k) {
-        if (trace && gl == 0) atomicMax(&d.ctr->dbg_body[k], gtimer() - t0);
+        if (trace == 1 && gl == 0) atomicMax(&d.ctr->dbg_body[k], gtimer() - t0);
+        if (trace == 2 && gl == 0) atomicAdd(&d.ctr->dbg_sum[k], gtimer() - t0);
     };
     const Lite me = load_lite(d, i);
     const float my_friction = d.p1[i].x;
@@ -394,7 +397,11 @@ __device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float
         if (block_solve(blk, safe)) upd = safe;
     }
     mark(4);
-    if (trace && gl == 0) atomicMax(&d.ctr->dbg_rn, rn);
+    if (trace == 1 && gl == 0) atomicMax(&d.ctr->dbg_rn, rn);
+    if (trace == 2 && gl == 0) {
+        atomicAdd(&d.ctr->dbg_sum[6], 1ull);
+        atomicAdd(&d.ctr->dbg_sum[7], (unsigned long long)rn);
+    }
     if (gl == 0) {
         if (phase == 0) {
             apply_pose_update(d, i, upd);
@@ -566,31 +573,54 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
             const uint32_t* off = c->color_off + col * kWidthClasses;
             const uint32_t b0 = off[0], b1 = off[kWidthClasses];
             const uint32_t nb = b1 - b0;
-            const bool last_colour = timing && it == 0 && col + 1 == colors;
+            const uint32_t trace = !timing || it != 0 ? 0u : col + 1 == colors ? 1u : col == 0 ? 2u : 0u;
             // Bodies [lo, hi) with G lanes each. Consecutive bodies go to
             // consecutive CTAs (group rank = local group x grid + CTA), so the
             // heavy bodies at the front of a colour spread over all SMs.
+            // Policy 3 hands the bodies out dynamically instead: each group
+            // takes the next unclaimed body of the colour from a counter
+            // (claiming its following one while it solves), so groups that
+            // drew light bodies take more of them.
+            const uint32_t step = it * colors + col;
+            uint32_t* claim = &c->claim[step & 1u];
+            if (d.solve_policy == 3 && blockIdx.x == 0 && threadIdx.x == 0) c->claim[(step + 1u) & 1u] = 0u;
             auto sweep = [&](auto width, uint32_t lo, uint32_t hi) {
                 constexpr int G = decltype(width)::value;
+                if (lo >= hi) return;
                 const int gl = lane % G, gbase = lane - gl;
                 const uint32_t gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << gbase;
                 GroupRows<G>& sm = reinterpret_cast<GroupRows<G>*>(warp_stage)[gbase / G];
-                const uint32_t groups = nthreads / G;
-                const uint32_t rank = (threadIdx.x / G) * gridDim.x + blockIdx.x;
-                for (uint32_t k = lo + rank; k < hi; k += groups) {
+                auto body = [&](uint32_t k) {
                     const uint32_t i = d.corder[k];
-                    if (phase != 0 && d.impact[i] == 0) continue;
-                    if (batched(d) && it >= d.scene_budget[d.scene_of[i]]) continue;
-                    solve_body_group<G>(d, i, phase, dt, sm, gmask, gl, gbase, last_colour);
+                    if (phase != 0 && d.impact[i] == 0) return;
+                    if (batched(d) && it >= d.scene_budget[d.scene_of[i]]) return;
+                    solve_body_group<G>(d, i, phase, dt, sm, gmask, gl, gbase, trace);
+                };
+                // One call site of the body solve for both assignments (each
+                // inlined copy adds its own stack frame).
+                const bool dynamic = d.solve_policy == 3;
+                const uint32_t groups = nthreads / G;
+                uint32_t k = lo + (threadIdx.x / G) * gridDim.x + blockIdx.x;
+                if (dynamic) {
+                    uint32_t t = 0;
+                    if (gl == 0) t = atomicAdd(claim, 1u);
+                    k = lo + __shfl_sync(gmask, t, gbase);
+                }
+                while (k < hi) {
+                    uint32_t next = 0;
+                    if (dynamic && gl == 0) next = atomicAdd(claim, 1u);
+                    body(k);
+                    if (dynamic) k = lo + __shfl_sync(gmask, next, gbase);
+                    else k += groups;
                 }
                 __syncwarp();
             };
             using W32 = std::integral_constant<int, 32>;
             using W16 = std::integral_constant<int, 16>;
             using W8 = std::integral_constant<int, 8>;
-            // Widths (see the group-per-body comment): policy 0 one width per
-            // colour by its size, 1 eight lanes, 2 a width per body class
-            // (heaviest first) unless 32-lane groups cover the whole colour.
+            // Widths (see the group-per-body comment): policy 0 (and 3) one
+            // width per colour by its size, 1 eight lanes, 2 a width per body
+            // class (heaviest first) unless 32-lane groups cover the colour.
             uint32_t r32 = b0, r16 = b0, r8 = b0;  // 32 lanes [b0, r32), 16 [r32, r16), 8 [r16, r8)
             if (d.solve_policy != 1 && nb * 32u <= nthreads) {
                 r32 = r16 = r8 = b1;
@@ -598,7 +628,7 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
                 r32 = off[1];
                 r16 = off[2];
                 r8 = b1;
-            } else if (d.solve_policy == 0 && nb * 16u <= nthreads) {
+            } else if ((d.solve_policy == 0 || d.solve_policy == 3) && nb * 16u <= nthreads) {
                 r16 = r8 = b1;
             } else {
                 r8 = b1;
@@ -660,6 +690,7 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
         if (!last && colors == 0 && !grid_sync(c)) return;
         if (last) {
             if (grid_stride_begin() == 0) {
+                c->claim[0] = c->claim[1] = 0u;  // every block is past its last claim
                 if (phase == 0) {
                     c->iterations = it + 1;
                     c->residual = rms;

@@ -52,6 +52,7 @@ struct Counters {
     uint32_t budget_max;  // batched scenes: the largest scene budget of the tick
     uint32_t n_surv;      // narrowphase candidates left for the manifold pass
     uint32_t n_events;    // contact events recorded by the tick
+    uint32_t claim[2];    // solve policy 3: next unclaimed body of the colour (alternating)
     // Bodies bucketed by (colour, width class): bucket col * kWidthClasses + k.
     uint32_t color_count[kMaxColors * kWidthClasses];
     uint32_t color_off[kMaxColors * kWidthClasses + 1];
@@ -62,6 +63,7 @@ struct Counters {
     float residual_max;
     unsigned long long dbg_work[20], dbg_release[20], dbg_start;
     unsigned long long dbg_body[8];
+    unsigned long long dbg_sum[8];  // colour 0 of the first sweep: stage sums, bodies, rows
     uint32_t dbg_rn;
 };
 

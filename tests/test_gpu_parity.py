@@ -185,7 +185,7 @@ def test_launch_plans_are_bit_identical(gpu_available):
     s = scenes.box_pile((6, 4, 6), seed=13, spacing=1.6)
     ref = None
     for v in range(3):
-        for p in range(3):
+        for p in range(4):
             w = core.World(s)
             w.set_launch_plan(v, p)
             for _ in range(12):
@@ -200,7 +200,7 @@ def test_launch_plans_are_bit_identical(gpu_available):
         w.step()
     before = w.states().view(np.uint8).copy()
     v, p, report = w.autotune(ticks=2)
-    assert report.count("ms/tick") == 9
+    assert report.count("ms/tick") == 12
     assert np.array_equal(w.states().view(np.uint8), before)
 
 
@@ -211,7 +211,7 @@ def test_launch_plans_are_bit_identical_on_the_settled_pile(gpu_available):
     z = np.load(os.path.join(os.path.dirname(__file__), "golden", "settled_pile_64x32x32.npz"))
     s.states = z["states"].astype(np.float32).view(scenes.STATE_DTYPE).reshape(-1).copy()
     ref = None
-    for v, p in ((1, 0), (0, 1), (0, 2), (1, 2), (2, 2)):
+    for v, p in ((1, 0), (0, 1), (0, 2), (1, 2), (2, 2), (1, 3), (0, 3)):
         w = core.World(s)
         w.set_launch_plan(v, p)
         for _ in range(4):
