@@ -256,7 +256,9 @@ def gpu_arm(args):
     # per-tick statistics and the solve kernel's event time (plain launches)
     world.restore()
     world.solve_timer(True)
+    torch.cuda.nvtx.range_push("learned_stats")
     learned_stats = [world.step(learned) for _ in range(steps)]
+    torch.cuda.nvtx.range_pop()
     solve_ms, solve_launches = world.solve_timer(False)
     plain_stats = replay_stats(world, plain, steps)
     value = world_size * steps / (learned_ms * 1e-3)
@@ -291,7 +293,7 @@ def gpu_arm(args):
     for _ in range(steps):
         world.set_states(host_np)            # h2d: the step's input states
         world.step(learned, stats=False)
-        host_np[:] = world.states()          # d2h: the step's result
+        world.states(out=host_np)            # d2h: the step's result
     torch.cuda.synchronize()
     e2e_value = world_size * steps / max_over_ranks(time.perf_counter() - t0)
     state_bytes = scene.n * 52
@@ -533,7 +535,7 @@ def gpu_batched(args):
     for _ in range(steps):
         world.set_states(host_np)
         world.step(learned, stats=False)
-        host_np[:] = world.states()
+        world.states(out=host_np)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
 

@@ -204,6 +204,22 @@ __global__ void k_pack_states(Dev d, uint32_t first, uint32_t count, float* dst)
         o[10] = w.x; o[11] = w.y; o[12] = w.z;
     }
 }
+// The inverse for every body: x, q, v, w exactly as given (no
+// renormalisation, unlike the record writes).
+__global__ void k_unpack_states(Dev d, uint32_t count, const float* src) {
+    for (uint32_t b = grid_stride_begin(); b < count; b += grid_stride()) {
+        const float* o = src + 13 * size_t(b);
+        d.x[b] = make_float4(o[0], o[1], o[2], 0.0f);
+        d.q[b] = make_float4(o[3], o[4], o[5], o[6]);
+        d.v[b] = make_float4(o[7], o[8], o[9], 0.0f);
+        d.w[b] = make_float4(o[10], o[11], o[12], 0.0f);
+    }
+}
+void launch_unpack_states(const Dev& d, uint32_t count, const float* src, cudaStream_t s) {
+    if (count == 0) return;
+    k_unpack_states<<<blocks_for(count), kBlock, 0, s>>>(d, count, src);
+    ++g_kernel_launches;
+}
 void launch_pack_states(const Dev& d, uint32_t first, uint32_t count, float* dst, cudaStream_t s) {
     if (count == 0) return;
     k_pack_states<<<blocks_for(count), kBlock, 0, s>>>(d, first, count, dst);

@@ -801,39 +801,27 @@ int pmb_world_last_stats(pmb_world* w, pmb_step_stats* out) {
     return PMB_SUCCESS;
 }
 
+// Whole-world state transfer through the record staging buffer (64 B per
+// body): one packing kernel and one copy each way, straight from or into the
+// caller's host memory (pinned memory makes both copies DMA transfers).
 int pmb_world_get_states(pmb_world* w, pmb_state* out) {
     if (!w || !out) return PMB_ERROR_INVALID_ARGUMENT;
+    static_assert(sizeof(pmb_state) == 52, "state record");
     cudaSetDevice(w->device);
     const uint32_t n = w->d.n;
-    std::vector<float4> x(n), q(n), v(n), wv(n);
-    cudaMemcpyAsync(x.data(), w->d.x, 16 * n, cudaMemcpyDeviceToHost, w->stream);
-    cudaMemcpyAsync(q.data(), w->d.q, 16 * n, cudaMemcpyDeviceToHost, w->stream);
-    cudaMemcpyAsync(v.data(), w->d.v, 16 * n, cudaMemcpyDeviceToHost, w->stream);
-    cudaMemcpyAsync(wv.data(), w->d.w, 16 * n, cudaMemcpyDeviceToHost, w->stream);
-    int r = check(cudaStreamSynchronize(w->stream));
-    if (r != PMB_SUCCESS) return r;
-    for (uint32_t i = 0; i < n; ++i) {
-        out[i] = {{x[i].x, x[i].y, x[i].z}, {q[i].x, q[i].y, q[i].z, q[i].w}, {v[i].x, v[i].y, v[i].z},
-                  {wv[i].x, wv[i].y, wv[i].z}};
-    }
-    return PMB_SUCCESS;
+    float* staging = reinterpret_cast<float*>(w->d.io_rec);
+    launch_pack_states(w->d, 0, n, staging, w->stream);
+    cudaMemcpyAsync(out, staging, sizeof(pmb_state) * size_t(n), cudaMemcpyDeviceToHost, w->stream);
+    return check(cudaStreamSynchronize(w->stream));
 }
 
 int pmb_world_set_states(pmb_world* w, const pmb_state* in) {
     if (!w || !in) return PMB_ERROR_INVALID_ARGUMENT;
     cudaSetDevice(w->device);
     const uint32_t n = w->d.n;
-    std::vector<float4> x(n), q(n), v(n), wv(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        x[i] = make_float4(in[i].x[0], in[i].x[1], in[i].x[2], 0);
-        q[i] = make_float4(in[i].q[0], in[i].q[1], in[i].q[2], in[i].q[3]);
-        v[i] = make_float4(in[i].v[0], in[i].v[1], in[i].v[2], 0);
-        wv[i] = make_float4(in[i].w[0], in[i].w[1], in[i].w[2], 0);
-    }
-    cudaMemcpyAsync(w->d.x, x.data(), 16 * n, cudaMemcpyHostToDevice, w->stream);
-    cudaMemcpyAsync(w->d.q, q.data(), 16 * n, cudaMemcpyHostToDevice, w->stream);
-    cudaMemcpyAsync(w->d.v, v.data(), 16 * n, cudaMemcpyHostToDevice, w->stream);
-    cudaMemcpyAsync(w->d.w, wv.data(), 16 * n, cudaMemcpyHostToDevice, w->stream);
+    float* staging = reinterpret_cast<float*>(w->d.io_rec);
+    cudaMemcpyAsync(staging, in, sizeof(pmb_state) * size_t(n), cudaMemcpyHostToDevice, w->stream);
+    launch_unpack_states(w->d, n, staging, w->stream);
     return check(cudaStreamSynchronize(w->stream));
 }
 

@@ -307,6 +307,7 @@ void launch_contact_jacobians(const Dev& d, uint32_t phase, cudaStream_t s);
 // Sparse per-body record writes staged in io_index / io_rec (kind 0: inputs,
 // 1: kinematic targets, 2: states), and AoS state packing into `dst`.
 void launch_scatter_records(const Dev& d, uint32_t kind, uint32_t count, cudaStream_t s);
+void launch_unpack_states(const Dev& d, uint32_t count, const float* src, cudaStream_t s);
 void launch_pack_states(const Dev& d, uint32_t first, uint32_t count, float* dst, cudaStream_t s);
 extern const void* color_kernel_ptr;
 // Learned warm start (pmb_mlp.cu).

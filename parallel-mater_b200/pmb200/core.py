@@ -214,8 +214,13 @@ class World:
         _check(lib().pmb_world_last_stats(self.h, out.ctypes.data), "pmb_world_last_stats")
         return out
 
-    def states(self):
-        out = np.zeros(self.scene.n, STATE_DTYPE)
+    def states(self, out=None):
+        """All body states (STATE_DTYPE); `out`: a contiguous array of n
+        records to fill instead of a new one (pinned memory makes the copy a
+        DMA transfer)."""
+        if out is None:
+            out = np.empty(self.scene.n, STATE_DTYPE)
+        assert out.dtype == STATE_DTYPE and out.size == self.scene.n and out.flags.c_contiguous
         _check(lib().pmb_world_get_states(self.h, out.ctypes.data), "pmb_world_get_states")
         return out
 
