@@ -87,3 +87,22 @@ def test_batched_learned_graph_replay_equals_steps(gpu_available):
     assert np.array_equal(a.states().view(np.uint8), b.states().view(np.uint8))
     a.close()
     b.close()
+
+
+def test_batched_plans_are_bit_identical(gpu_available):
+    """A batched world with joints (chains, every joint type) gives the same
+    bits under every solve launch plan (CTA size, lanes per body, static or
+    claimed body assignment)."""
+    batch = scenes.batch(_parts())
+    ref = None
+    for v, p in ((1, 0), (1, 3), (0, 2), (2, 1), (0, 3)):
+        w = core.World(batch)
+        w.set_launch_plan(v, p)
+        for _ in range(20):
+            st = w.step()
+            assert st["status"] == 0, core.status_names(int(st["status"]))
+        x = w.states().view(np.uint8).copy()
+        if ref is None:
+            ref = x
+        assert np.array_equal(x, ref), (v, p)
+        w.close()
