@@ -292,7 +292,10 @@ class RigidSession:
     """A Scene driven through the pm* API on one device (realtime profile,
     dt = 1/60 s, one substep, as the reference's command path requires)."""
 
-    def __init__(self, scene: Scene, physical_index=0, iterations=8, contact_capacity=4096):
+    def __init__(self, scene: Scene, physical_index=0, iterations=8, contact_capacity=4096, body_infos=None):
+        """body_infos: optional {body: {PmRigidBodyInfo field: value}} written
+        over the fields derived from the scene (e.g. mass and a zero inertia
+        diagonal, which asks the driver for the mesh's box inertia)."""
         self.scene = scene
         boot = Api()
         inst = vp()
@@ -359,8 +362,18 @@ class RigidSession:
         fence = vp()
         check(self.api.pmCreateFence(dev, 0, ref(fence)), "pmCreateFence")
         self.fence = fence
+        # constraint-state read-back
+        self.constraint_count = len(scene.joints)
+        self.cstate_bytes = 12 * max(1, self.constraint_count)
+        self.cstate_mem, self.cstate_buf, self.cstate_ptr = self._mapped_buffer(self.cstate_bytes)
         # bodies and constraints
         self.body_infos = self._bodies()
+        for i, fields in (body_infos or {}).items():
+            for key, value in fields.items():
+                if key == "inertiaDiagonal":
+                    self.body_infos[i].inertiaDiagonal[:] = [float(v) for v in value]
+                else:
+                    setattr(self.body_infos[i], key, value)
         self._record(lambda: [
             *[check(self.api.pmCmdBuildGeometry(cb, g), "pmCmdBuildGeometry") for g in self.geometries],
             check(self.api.pmCmdWriteRigidBodies(cb, sim, 0, scene.n, self.body_infos), "pmCmdWriteRigidBodies"),
@@ -433,14 +446,14 @@ class RigidSession:
             x.collisionMargin = float(b["margin"][i])
         return infos
 
-    def _write_constraints(self):
+    def _write_constraints(self, active=None):
         j = self.scene.joints
         if len(j) == 0:
             return
         infos = (RigidConstraintInfo * len(j))()
         for k in range(len(j)):
             c, x = j[k], infos[k]
-            x.active = 1
+            x.active = 1 if active is None else int(bool(active[k]))
             x.type = int(c["type"])
             x.bodyA, x.bodyB = int(c["body_a"]), int(c["body_b"])
             x.frameA.position[:] = [float(v) for v in c["anchor_a"]]
@@ -532,6 +545,23 @@ class RigidSession:
         count, capacity, revision = np.frombuffer(raw[:16], np.dtype([("n", "<u4"), ("c", "<u4"), ("r", "<u8")]))[0]
         return (int(count), int(capacity), int(revision)), np.frombuffer(raw[16:16 + 56 * int(count)],
                                                                          PM_EVENT_DTYPE).copy()
+
+    def write_constraints(self, active):
+        """Rewrite every constraint slot with the given active flags
+        (pmCmdWriteRigidConstraints: removing or re-adding joints)."""
+        return self._record(lambda: self._write_constraints(active))
+
+    def copy_constraint_states(self):
+        """Records pmCmdCopyConstraintStates of every slot; returns the
+        (enabled, broken, appliedImpulse) records."""
+        n = self.constraint_count
+        if n == 0:
+            return np.zeros(0, np.dtype([("enabled", "<u4"), ("broken", "<u4"), ("applied", "<f4")]))
+        rc = self._record(lambda: check(self.api.pmCmdCopyConstraintStates(
+            self.cb, self.sim, 0, n, ref(BufferRange(self.cstate_buf, 0, 12 * n))), "pmCmdCopyConstraintStates"))
+        check(rc, "copy constraint states")
+        raw = bytes((C.c_uint8 * (12 * n)).from_address(self.cstate_ptr))
+        return np.frombuffer(raw, np.dtype([("enabled", "<u4"), ("broken", "<u4"), ("applied", "<f4")])).copy()
 
     def set_states(self, first, states):
         arr = (RigidState * len(states))(*[_state(s) for s in states])
