@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(256) k_narrow_sat(Dev d) {
 
 // Pass 2, one thread per surviving candidate: the full face manifold
 // (swept variant first when the pair moved more than its margin).
-__global__ void __launch_bounds__(128) k_narrow(Dev d) {
+__global__ void __launch_bounds__(128, 6) k_narrow(Dev d) {
     const uint32_t total = d.ctr->n_surv;
     for (uint32_t s = grid_stride_begin(); s < total; s += grid_stride()) {
         const uint32_t k = d.np_list[s];

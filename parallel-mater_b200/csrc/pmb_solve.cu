@@ -130,7 +130,10 @@ __device__ __forceinline__ void apply_pose_update(const Dev& d, uint32_t i, cons
 // there shorten the critical path.
 constexpr uint32_t kNormSlots = 32;
 template <int G> struct GroupRows {
-    float r[G][3][8];           // chunk being accumulated: 3 rows of (jacobian[6], stiffness, force)
+    // Chunk being accumulated: 3 rows of (jacobian[6], stiffness, force,
+    // stiffness x jacobian[6]); the last six are the Hessian products' first
+    // factors, formed once per row instead of once per entry.
+    float r[G][3][14];
     float nrow[kNormSlots][8];  // normal row: jacobian[6], raw penalty, trial force
     uint32_t flag[G];
 };
@@ -186,7 +189,7 @@ __device__ __forceinline__ void accumulate_chunk(float* ent, int gl, const Group
 #pragma unroll
                 for (int x = 0; x < 3; ++x) {
                     const float* row = sm.r[t][x];
-                    prod[t][x] = hess ? row[6] * row[ei] * row[ek] : row[ei] * row[7];
+                    prod[t][x] = hess ? row[8 + ei] * row[ek] : row[ei] * row[7];
                 }
 #pragma unroll
             for (int t = 0; t < G; ++t)
@@ -198,7 +201,7 @@ __device__ __forceinline__ void accumulate_chunk(float* ent, int gl, const Group
 #pragma unroll
                 for (int x = 0; x < 3; ++x) {
                     const float* row = sm.r[t][x];
-                    ent[q] += hess ? row[6] * row[ei] * row[ek] : row[ei] * row[7];
+                    ent[q] += hess ? row[8 + ei] * row[ek] : row[ei] * row[7];
                 }
         }
     }
@@ -267,6 +270,8 @@ __device__ __forceinline__ void stage_contact(const Dev& d, const Lite& me, floa
         for (int k = 0; k < 6; ++k) sm.r[slot][x][k] = row.v[k];
         sm.r[slot][x][6] = st[x];
         sm.r[slot][x][7] = forces[x];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) sm.r[slot][x][8 + k] = st[x] * row.v[k];  // = (stiffness x J_i), as before
     }
 }
 
