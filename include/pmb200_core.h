@@ -274,8 +274,19 @@ PMB_API int pmb_world_write_states(pmb_world* world, uint32_t first, uint32_t co
  * device memory `dst` (4-byte aligned) on the world's stream. */
 PMB_API int pmb_world_copy_states_to_device(pmb_world* world, uint32_t first, uint32_t count, void* dst);
 
-/* Joint state after the last tick (synchronous): flags bit 0 enabled, bit 1
- * broken; applied impulse; number of solver rows. capacity >= joint_count. */
+/* Work telemetry of the latest tick, in the reference's realtime work phases
+ * (realtime_telemetry.hpp: boundary, predict, index, candidates, domain,
+ * coupling, commit): kernel dispatches and thread blocks enqueued per phase,
+ * algorithmic bytes per phase (the per-body and per-contact costs of the
+ * kernels), grid-wide barriers (colour rounds and sweeps), sweeps and
+ * spatial-index builds. Feeds PM_QUERY_REALTIME_STEP_STATISTICS. */
+typedef struct pmb_tick_telemetry {
+    uint64_t tick;
+    uint64_t dispatches[7], workgroups[7], bytes_moved[7], barriers[7];
+    uint64_t sweeps, spatial_builds;
+} pmb_tick_telemetry;
+PMB_API int pmb_world_tick_telemetry(pmb_world* world, pmb_tick_telemetry* out);
+
 /* One contact point of the last tick that collected events, in active-pair
  * order (pm_prepare_parallel_contact_events, geometry.slang:2902-2939, and
  * the impulses of pm_save_rigid_contact_cache, :3028-3043): the pair's
@@ -292,6 +303,8 @@ typedef struct pmb_contact_event {
  * event capacity); 0 when the tick did not collect). */
 PMB_API int pmb_world_contact_events(pmb_world* world, pmb_contact_event* out, uint32_t capacity, uint32_t* count);
 
+/* Joint state after the last tick (synchronous): flags bit 0 enabled, bit 1
+ * broken; applied impulse; number of solver rows. capacity >= joint_count. */
 PMB_API int pmb_world_joints(pmb_world* world, uint32_t* flags, float* applied, uint32_t* counts,
                              uint32_t capacity);
 

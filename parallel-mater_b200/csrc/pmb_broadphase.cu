@@ -65,7 +65,7 @@ __global__ void k_body_constants(Dev d, const float4* mesh_lo, const float4* mes
 }
 void launch_body_constants(const Dev& d, const float4* lo, const float4* hi, const float4* sph, cudaStream_t s) {
     k_body_constants<<<blocks_for(d.n), kBlock, 0, s>>>(d, lo, hi, sph);
-    ++g_kernel_launches;
+    note_launch(blocks_for(d.n));
 }
 
 __global__ void k_integrate(Dev d, StepParams sp, float4* ox, float4* oq, float4* ov, float4* ow) {
@@ -188,7 +188,7 @@ __global__ void k_scatter_records(Dev d, uint32_t kind, uint32_t count) {
 void launch_scatter_records(const Dev& d, uint32_t kind, uint32_t count, cudaStream_t s) {
     if (count == 0) return;
     k_scatter_records<<<blocks_for(count), kBlock, 0, s>>>(d, kind, count);
-    ++g_kernel_launches;
+    note_launch(blocks_for(count));
 }
 
 // States [first, first + count) as packed 13-float records (position,
@@ -218,18 +218,18 @@ __global__ void k_unpack_states(Dev d, uint32_t count, const float* src) {
 void launch_unpack_states(const Dev& d, uint32_t count, const float* src, cudaStream_t s) {
     if (count == 0) return;
     k_unpack_states<<<blocks_for(count), kBlock, 0, s>>>(d, count, src);
-    ++g_kernel_launches;
+    note_launch(blocks_for(count));
 }
 void launch_pack_states(const Dev& d, uint32_t first, uint32_t count, float* dst, cudaStream_t s) {
     if (count == 0) return;
     k_pack_states<<<blocks_for(count), kBlock, 0, s>>>(d, first, count, dst);
-    ++g_kernel_launches;
+    note_launch(blocks_for(count));
 }
 
 void launch_integrate(const Dev& d, const StepParams& sp, cudaStream_t s, const SolveBuffers& o) {
     if (d.n_scenes > 1) cudaMemsetAsync(d.scene_hs, 0, sizeof(float) * d.n_scenes, s);
     k_integrate<<<blocks_for(d.n), kBlock, 0, s>>>(d, sp, o.ox, o.oq, o.ov, o.ow);
-    ++g_kernel_launches;
+    note_launch(blocks_for(d.n));
     prof_mark(s, "integrate+proxy");
 }
 
@@ -400,27 +400,28 @@ void launch_broadphase(const Dev& d, cudaStream_t s) {
         cudaMemsetAsync(d.scene_large_count, 0, sizeof(uint32_t) * (d.n_scenes + 1), s);
         cudaMemsetAsync(d.scene_large_cursor, 0, sizeof(uint32_t) * d.n_scenes, s);
         k_scene_large_count<<<blocks_for(d.n), kBlock, 0, s>>>(d);
-        ++g_kernel_launches;
+        note_launch(blocks_for(d.n));
         scan_u32(d.scene_large_count, d.scene_large_off, nullptr, d.n_scenes, nullptr, d.scan_tmp32, s);
         k_scene_large_scatter<<<blocks_for(d.n), kBlock, 0, s>>>(d);
-        ++g_kernel_launches;
+        note_launch(blocks_for(d.n));
     }
     cudaMemsetAsync(d.bucket_count, 0, sizeof(uint32_t) * (d.grid_size + 1), s);
     cudaMemsetAsync(d.bucket_cursor, 0, sizeof(uint32_t) * d.grid_size, s);
     k_grid_count<<<blocks_for(d.n), kBlock, 0, s>>>(d);
-    ++g_kernel_launches;
+    note_launch(blocks_for(d.n));
     scan_u32(d.bucket_count, d.bucket_off, nullptr, d.grid_size, nullptr, d.scan_tmp32, s);
     k_grid_scatter<<<blocks_for(d.n), kBlock, 0, s>>>(d);
-    ++g_kernel_launches;
+    note_launch(blocks_for(d.n));
     prof_mark(s, "grid build");
+    set_phase(kPhCandidates);
     k_query_count<<<blocks_for(kQueryLanes * d.n, 128), 128, 0, s>>>(d);
-    ++g_kernel_launches;
+    note_launch(blocks_for(kQueryLanes * d.n, 128));
     prof_mark(s, "query count");
     scan_u32(d.cand_count, d.cand_off, nullptr, d.n, &d.ctr->n_cand, d.scan_tmp32, s);
     k_query_write<<<blocks_for(kQueryLanes * d.n, 128), 128, 0, s>>>(d);
-    ++g_kernel_launches;
+    note_launch(blocks_for(kQueryLanes * d.n, 128));
     k_clamp_count<<<1, 1, 0, s>>>(&d.ctr->n_cand, d.cap_cand);
-    ++g_kernel_launches;
+    note_launch(1);
     prof_mark(s, "query write");
 }
 

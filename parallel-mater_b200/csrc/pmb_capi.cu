@@ -24,6 +24,8 @@ struct Prof {
 };
 static Prof g_prof;
 unsigned long long g_kernel_launches = 0;
+thread_local LaunchLedger* g_ledger = nullptr;
+thread_local int g_phase = 0;
 
 void prof_mark(cudaStream_t s, const char* stage) {
     if (!g_prof.on) return;
@@ -83,6 +85,8 @@ struct pmb_world {
     cudaGraphExec_t graph{};
     uint32_t step_parity{}, snapshot_parity{};
     Counters host_ctr{};
+    LaunchLedger ledger{};          // launches of the latest enqueued tick
+    uint64_t ticks_enqueued{};
     // Learned warm start (allocated by pmb_world_mlp_attach).
     struct Mlp {
         bool attached{}, train{};
@@ -163,11 +167,17 @@ __global__ void k_reset_counters(Counters* c) {
 void enqueue_step(pmb_world* w, const StepParams& sp) {
     cudaStream_t s = w->stream;
     Dev& d = w->d;
+    w->ledger = LaunchLedger{};
+    g_ledger = &w->ledger;
+    set_phase(kPhBoundary);
     k_reset_counters<<<1, 256, 0, s>>>(d.ctr);
-    ++g_kernel_launches;
+    note_launch(1);
+    set_phase(kPhPredict);
     launch_integrate(d, sp, s, w->out);
-    launch_broadphase(d, s);
+    set_phase(kPhIndex);
+    launch_broadphase(d, s);  // switches to the candidate phase for the query
     launch_narrowphase(d, sp, s);
+    set_phase(kPhDomain);
     launch_prepare(d, sp, s);
     auto& mlp = w->mlp;
     const bool learned = mlp.attached && sp.warm_start == 1;
@@ -181,6 +191,7 @@ void enqueue_step(pmb_world* w, const StepParams& sp) {
     launch_graph(d, sp, s, w->coop_color);
     launch_scene_budgets(d, sp, s);
     launch_solve_all(d, sp, s, w->coop_solve, w->out);
+    set_phase(kPhDomain);
     if (mlp.attached && mlp.train) {
         // Online training on this tick's converged normal rows.
         launch_mlp_targets(d, mlp.meta, s);
@@ -198,6 +209,8 @@ void enqueue_step(pmb_world* w, const StepParams& sp) {
         }
         prof_mark(s, "mlp training");
     }
+    g_ledger = nullptr;
+    ++w->ticks_enqueued;
     // The cache written this tick is read by the next one.
     std::swap(d.sv_code, d.out_code);
     std::swap(d.sv_off, d.out_off);
@@ -1050,6 +1063,35 @@ int pmb_world_memory_requirements(const pmb_world_capacity* c, uint64_t* persist
     return PMB_SUCCESS;
 }
 
+// Telemetry of the latest tick: the host's launch ledger plus counts the
+// device recorded (colour rounds, sweeps, colours, contacts), with the
+// algorithmic byte model of each phase.
+int pmb_world_tick_telemetry(pmb_world* w, pmb_tick_telemetry* out) {
+    if (!w || !out) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(w->device);
+    Counters c;
+    cudaMemcpyAsync(&c, w->d.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, w->stream);
+    const int r = check(cudaStreamSynchronize(w->stream));
+    if (r != PMB_SUCCESS) return r;
+    *out = pmb_tick_telemetry{};
+    out->tick = w->ticks_enqueued;
+    for (int p = 0; p < kPhases; ++p) {
+        out->dispatches[p] = w->ledger.dispatches[p];
+        out->workgroups[p] = w->ledger.workgroups[p];
+    }
+    const uint64_t n = w->d.n, con = c.n_contacts;
+    const uint64_t sweeps = uint64_t(c.iterations) + (c.impact ? uint64_t(c.budget) : 0u);
+    out->sweeps = sweeps;
+    out->spatial_builds = 1;
+    out->barriers[kPhDomain] = 2ull * c.rounds + sweeps * (uint64_t(c.colors) + 1u);
+    out->bytes_moved[kPhPredict] = 250u * n;
+    out->bytes_moved[kPhIndex] = 100u * n;
+    out->bytes_moved[kPhCandidates] = 8ull * c.n_cand + 64u * con;
+    out->bytes_moved[kPhDomain] = 604u * con + sweeps * (124u * n + 384u * con);
+    out->bytes_moved[kPhCommit] = 200u * n + 250u * con;
+    return PMB_SUCCESS;
+}
+
 int pmb_world_contact_events(pmb_world* w, pmb_contact_event* out, uint32_t capacity, uint32_t* count) {
     if (!w || !count || (capacity && !out)) return PMB_ERROR_INVALID_ARGUMENT;
     static_assert(sizeof(pmb_contact_event) == sizeof(ContactEvent), "event record");
@@ -1398,7 +1440,7 @@ int pmb_math_eval(uint32_t kind, uint32_t count, const float* in, float* out) {
     }
     cudaMemcpy(din, in, 4 * size_t(count) * in_w[kind], cudaMemcpyHostToDevice);
     k_math_eval<<<(count + 127) / 128, 128>>>(kind, count, din, dout);
-    ++g_kernel_launches;
+    note_launch((count + 127) / 128);
     cudaMemcpy(out, dout, 4 * size_t(count) * out_w[kind], cudaMemcpyDeviceToHost);
     int r = check(cudaGetLastError());
     cudaFree(din);

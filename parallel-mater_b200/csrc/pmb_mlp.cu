@@ -629,23 +629,23 @@ uint32_t mlp_grid(uint32_t tiles) {
 
 void launch_mlp_images(const float* params, uint8_t* img, cudaStream_t s) {
     k_mlp_images<<<(kMlpParams + 255) / 256, 256, 0, s>>>(params, img);
-    ++g_kernel_launches;
+    note_launch((kMlpParams + 255) / 256);
 }
 
 void launch_mlp_features(const Dev& d, const StepParams& sp, uint8_t* x, MlpMeta* meta, cudaStream_t s) {
     k_mlp_features<<<cap_blocks(d.cap_contact), kBlock, 0, s>>>(d, sp, x, meta);
-    ++g_kernel_launches;
+    note_launch(cap_blocks(d.cap_contact));
 }
 
 void launch_mlp_targets(const Dev& d, MlpMeta* meta, cudaStream_t s) {
     k_mlp_targets<<<cap_blocks(d.cap_contact), kBlock, 0, s>>>(d, meta);
-    ++g_kernel_launches;
+    note_launch(cap_blocks(d.cap_contact));
 }
 
 void launch_mlp_pack_rows(const float* feat, const float* y, const float* w, uint32_t n, uint8_t* x, MlpMeta* meta,
                           uint32_t tiles, cudaStream_t s) {
     k_mlp_pack_rows<<<blocks_for(tiles * kMlpTile), kBlock, 0, s>>>(feat, y, w, n, x, meta, tiles);
-    ++g_kernel_launches;
+    note_launch(blocks_for(tiles * kMlpTile));
 }
 
 void launch_mlp_tiles(bool train, const uint8_t* x, const MlpMeta* meta, const uint8_t* img, uint32_t rows,
@@ -656,20 +656,20 @@ void launch_mlp_tiles(bool train, const uint8_t* x, const MlpMeta* meta, const u
         k_mlp_tiles<true><<<grid, 128, kSmBytes, s>>>(a);
     else
         k_mlp_tiles<false><<<grid, 128, kSmBytes, s>>>(a);
-    ++g_kernel_launches;
+    note_launch(grid);
 }
 
 void launch_mlp_apply(const Dev& d, const MlpMeta* meta, const float* out, uint32_t mode, const float* gate,
                       cudaStream_t s) {
     k_mlp_apply<<<cap_blocks(d.cap_pair), kBlock, 0, s>>>(d, meta, out, mode, gate);
-    ++g_kernel_launches;
+    note_launch(cap_blocks(d.cap_pair));
 }
 
 void launch_mlp_reduce_adam(const float* partial, uint32_t parts, float* grad, float* params, float* m, float* v,
                             float lr, float b1, float b2, float c1, float c2, float eps, float* gate, cudaStream_t s) {
     k_mlp_reduce_adam<<<(kMlpPartial + 255) / 256, 256, 0, s>>>(partial, parts, grad, params, m, v, lr, b1, b2, c1,
                                                                  c2, eps, gate);
-    ++g_kernel_launches;
+    note_launch((kMlpPartial + 255) / 256);
 }
 
 }  // namespace pmb

@@ -488,17 +488,17 @@ __global__ void k_cache_load(Dev d, StepParams sp) {
 
 void launch_narrowphase(const Dev& d, const StepParams& sp, cudaStream_t s) {
     k_narrow_sat<<<cap_blocks(d.cap_cand, 256), 256, 0, s>>>(d);
-    ++g_kernel_launches;
+    note_launch(cap_blocks(d.cap_cand, 256));
     prof_mark(s, "narrowphase SAT");
     k_narrow<<<cap_blocks(d.cap_cand, 128), 128, 0, s>>>(d);
-    ++g_kernel_launches;
+    note_launch(cap_blocks(d.cap_cand, 128));
     prof_mark(s, "narrowphase manifolds");
     scan_u64(d.np_scan, d.np_scan, &d.ctr->n_cand, d.cap_cand, d.scan_tmp, s);
     k_compact<<<cap_blocks(d.cap_cand), kBlock, 0, s>>>(d);
-    ++g_kernel_launches;
+    note_launch(cap_blocks(d.cap_cand));
     prof_mark(s, "compact");
     k_cache_load<<<cap_blocks(d.cap_pair, 128), 128, 0, s>>>(d, sp);
-    ++g_kernel_launches;
+    note_launch(cap_blocks(d.cap_pair, 128));
     prof_mark(s, "cache load");
 }
 

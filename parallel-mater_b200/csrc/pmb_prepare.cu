@@ -266,7 +266,7 @@ __global__ void k_scene_budgets(Dev d, StepParams sp) {
 void launch_scene_budgets(const Dev& d, const StepParams& sp, cudaStream_t s) {
     if (d.n_scenes <= 1) return;
     k_scene_budgets<<<blocks_for(d.n_scenes), kBlock, 0, s>>>(d, sp);
-    ++g_kernel_launches;
+    note_launch(blocks_for(d.n_scenes));
 }
 
 __global__ void k_graph_fill(Dev d) {
@@ -495,12 +495,12 @@ __global__ void k_color_scatter(Dev d) {
 
 void launch_prepare(const Dev& d, const StepParams& sp, cudaStream_t s) {
     k_prepare_bodies<<<blocks_for(d.n), kBlock, 0, s>>>(d, sp);
-    ++g_kernel_launches;
+    note_launch(blocks_for(d.n));
     k_prepare_pairs<<<cap_blocks(d.cap_pair, 128), 128, 0, s>>>(d, sp);
-    ++g_kernel_launches;
+    note_launch(cap_blocks(d.cap_pair, 128));
     if (d.nj) {
         k_prepare_joints<<<blocks_for(d.nj, 64), 64, 0, s>>>(d, sp);
-        ++g_kernel_launches;
+        note_launch(blocks_for(d.nj, 64));
     }
     launch_contact_jacobians(d, 0, s);
     prof_mark(s, "prepare");
@@ -511,37 +511,37 @@ const void* color_kernel_ptr = reinterpret_cast<const void*>(&k_color);
 void launch_graph(const Dev& d, const StepParams& sp, cudaStream_t s, int coop_blocks) {
     uint32_t gb = cap_blocks(d.cap_pair > d.nj ? d.cap_pair : d.nj);
     k_graph_degrees<<<gb, kBlock, 0, s>>>(d, sp);
-    ++g_kernel_launches;
+    note_launch(gb);
     scan_u32(d.deg, d.inc_off, nullptr, d.n, nullptr, d.scan_tmp32, s);
     scan_u32(d.jdeg, d.jinc_off, nullptr, d.n, nullptr, d.scan_tmp32, s);
     k_graph_fill<<<gb, kBlock, 0, s>>>(d);
-    ++g_kernel_launches;
+    note_launch(gb);
     k_graph_lists<<<blocks_for(d.n), kBlock, 0, s>>>(d);
-    ++g_kernel_launches;
+    note_launch(blocks_for(d.n));
     k_graph_roots<<<blocks_for(d.n), kBlock, 0, s>>>(d);
-    ++g_kernel_launches;
+    note_launch(blocks_for(d.n));
     scan_u32(d.rcount, d.roff, nullptr, d.n, nullptr, d.scan_tmp32, s);
     k_row_lists<<<blocks_for(d.n), kBlock, 0, s>>>(d);
-    ++g_kernel_launches;
+    note_launch(blocks_for(d.n));
     k_graph_impact<<<cap_blocks(d.cap_pair), kBlock, 0, s>>>(d);
-    ++g_kernel_launches;
+    note_launch(cap_blocks(d.cap_pair));
     k_graph_islands<<<blocks_for(d.n), kBlock, 0, s>>>(d);
-    ++g_kernel_launches;
+    note_launch(blocks_for(d.n));
     prof_mark(s, "graph lists+islands");
     k_neighbour_lists<<<blocks_for(d.n), kBlock, 0, s>>>(d);
-    ++g_kernel_launches;
+    note_launch(blocks_for(d.n));
     cudaMemsetAsync(d.cdirty, 0, 2 * size_t(d.n), s);
     void* args[] = {const_cast<Dev*>(&d)};
     cudaLaunchCooperativeKernel(color_kernel_ptr, dim3(coop_blocks), dim3(kColorThreads), args, 0, s);
-    ++g_kernel_launches;
+    note_launch(coop_blocks);
     prof_mark(s, "colour fixpoint");
     k_color_count<<<blocks_for(d.n), kBlock, 0, s>>>(d);
-    ++g_kernel_launches;
+    note_launch(blocks_for(d.n));
     static_assert(kBuckets <= 1024, "bucket scan is one block");
     k_color_offsets<<<1, 1024, 0, s>>>(d);
-    ++g_kernel_launches;
+    note_launch(1);
     k_color_scatter<<<blocks_for(d.n), kBlock, 0, s>>>(d);
-    ++g_kernel_launches;
+    note_launch(blocks_for(d.n));
     prof_mark(s, "colour buckets");
 }
 

@@ -107,13 +107,13 @@ static void scan_impl(const T* in, T* out, const uint32_t* count_ptr, uint32_t c
     uint32_t tiles = (capacity + kScanTile - 1) / kScanTile;
     if (tiles == 0) tiles = 1;
     k_tile_sums<T><<<tiles, kScanThreads, 0, s>>>(in, count_ptr, capacity, tmp);
-    ++g_kernel_launches;
+    note_launch(tiles);
     k_scan_tiles<T><<<1, kScanThreads, 0, s>>>(tmp, tiles, tmp + tiles);
-    ++g_kernel_launches;
+    note_launch(1);
     k_scan_apply<T><<<tiles, kScanThreads, 0, s>>>(in, out, count_ptr, capacity, tmp);
-    ++g_kernel_launches;
+    note_launch(tiles);
     k_scan_total<T><<<1, 1, 0, s>>>(out, count_ptr, capacity, tmp + tiles);
-    ++g_kernel_launches;
+    note_launch(1);
 }
 
 // out must hold capacity + 1 entries; out[count] receives the total and, when
@@ -128,7 +128,7 @@ void scan_u32(const uint32_t* in, uint32_t* out, const uint32_t* count_ptr, uint
     scan_impl<uint32_t>(in, out, count_ptr, capacity, tmp, s);
     if (total) {
         k_copy_total<<<1, 1, 0, s>>>(out, count_ptr, capacity, total);
-        ++g_kernel_launches;
+        note_launch(1);
     }
 }
 

@@ -93,7 +93,7 @@ __global__ void k_contact_jacobians(Dev d, uint32_t phase) {
 }
 void launch_contact_jacobians(const Dev& d, uint32_t phase, cudaStream_t s) {
     k_contact_jacobians<<<cap_blocks(d.cap_contact), kBlock, 0, s>>>(d, phase);
-    ++g_kernel_launches;
+    note_launch(cap_blocks(d.cap_contact));
 }
 
 __device__ __forceinline__ void apply_pose_update(const Dev& d, uint32_t i, const V6& u) {
@@ -1039,12 +1039,12 @@ void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, const 
     for (uint32_t phase = 0; phase < (sp.realtime ? 1u : 2u); ++phase) {
         if (phase != 0) {
             k_impact_setup<<<cap_blocks(d.cap_pair), kBlock, 0, s>>>(d, sp, o.ox, o.oq, o.ov, o.ow);
-            ++g_kernel_launches;
+            note_launch(cap_blocks(d.cap_pair));
             k_impact_bodies<<<blocks_for(d.n), kBlock, 0, s>>>(d, o.ox, o.oq, o.ov, o.ow);
-            ++g_kernel_launches;
+            note_launch(blocks_for(d.n));
             launch_contact_jacobians(d, 1, s);
             k_impact_constraints<<<pb, kBlock, 0, s>>>(d, sp, o.ov, o.ow);
-            ++g_kernel_launches;
+            note_launch(pb);
             prof_mark(s, "impact setup");
         }
         Dev dd = d;
@@ -1053,32 +1053,33 @@ void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, const 
         void* args[] = {&dd, &spp, &ph};
         solve_timer_begin(s);
         cudaLaunchCooperativeKernel(sv.ptr, dim3(coop), dim3(sv.threads), args, sv.smem, s);
-        ++g_kernel_launches;
+        note_launch(coop);
         solve_timer_end(s);
         prof_mark(s, phase ? "solve phase 1" : "solve phase 0");
         k_contact_finalize<<<cap_blocks(d.cap_contact), kBlock, 0, s>>>(d, sp, phase);
-        ++g_kernel_launches;
+        note_launch(cap_blocks(d.cap_contact));
         k_free_anchor<<<cap_blocks(d.cap_pair > d.n ? d.cap_pair : d.n), kBlock, 0, s>>>(d, phase);
-        ++g_kernel_launches;
+        note_launch(cap_blocks(d.cap_pair > d.n ? d.cap_pair : d.n));
         k_free_mean<<<std::min<uint32_t>(blocks_for(32u * d.n, 256), 148u * 8u), 256, 0, s>>>(d, phase);
-        ++g_kernel_launches;
+        note_launch(std::min<uint32_t>(blocks_for(32u * d.n, 256), 148u * 8u));
         k_free_subtract<<<blocks_for(d.n), kBlock, 0, s>>>(d, phase);
-        ++g_kernel_launches;
+        note_launch(blocks_for(d.n));
         k_apply<<<blocks_for(d.n), kBlock, 0, s>>>(d, sp, phase, o.ox, o.oq, o.ov, o.ow);
-        ++g_kernel_launches;
+        note_launch(blocks_for(d.n));
         if (phase == 0 && d.n_hinge_segs) {
             k_project_hinges<<<blocks_for(d.n_hinge_segs), kBlock, 0, s>>>(d, o.ox, o.oq);
-            ++g_kernel_launches;
+            note_launch(blocks_for(d.n_hinge_segs));
         }
         prof_mark(s, phase ? "finish phase 1" : "finish phase 0");
     }
+    set_phase(kPhCommit);
     k_clamp_commit<<<blocks_for(d.n), kBlock, 0, s>>>(d, o.ox, o.oq, o.ov, o.ow);
-    ++g_kernel_launches;
+    note_launch(blocks_for(d.n));
     k_cache_save<<<cap_blocks(d.cap_pair), kBlock, 0, s>>>(d, sp);
-    ++g_kernel_launches;
+    note_launch(cap_blocks(d.cap_pair));
     if (sp.collect_events && d.event_capacity) {
         k_contact_events<<<cap_blocks(d.event_capacity), kBlock, 0, s>>>(d);
-        ++g_kernel_launches;
+        note_launch(cap_blocks(d.event_capacity));
     }
     prof_mark(s, "commit+cache save");
 }

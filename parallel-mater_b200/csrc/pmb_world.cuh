@@ -292,6 +292,25 @@ int coop_blocks_for(const void* kernel, int threads, size_t smem);
 void prof_mark(cudaStream_t s, const char* stage);
 // Kernels enqueued by this library since the last reset (all stages).
 extern unsigned long long g_kernel_launches;
+// Launch ledger of the tick being enqueued on this thread (telemetry):
+// dispatches and thread blocks per work phase, in the reference's phase
+// order (boundary, predict, index, candidates, domain, coupling, commit).
+constexpr int kPhases = 7;
+enum : int { kPhBoundary, kPhPredict, kPhIndex, kPhCandidates, kPhDomain, kPhCoupling, kPhCommit };
+struct LaunchLedger {
+    unsigned long long dispatches[kPhases];
+    unsigned long long workgroups[kPhases];
+};
+extern thread_local LaunchLedger* g_ledger;
+extern thread_local int g_phase;
+inline void set_phase(int phase) { g_phase = phase; }
+inline void note_launch(unsigned long long blocks) {
+    ++g_kernel_launches;
+    if (g_ledger) {
+        ++g_ledger->dispatches[g_phase];
+        g_ledger->workgroups[g_phase] += blocks;
+    }
+}
 // Dominant-kernel timing: brackets each solve launch with CUDA events when on.
 void solve_timer_begin(cudaStream_t s);
 void solve_timer_end(cudaStream_t s);

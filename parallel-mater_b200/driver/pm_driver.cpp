@@ -995,8 +995,6 @@ PmResult PMAPI_CALL pmCreateQueryPool(PmDevice device, const PmQueryPoolCreateIn
         (info->queryType != PM_QUERY_TIMESTAMP && info->queryType != PM_QUERY_STEP_STATISTICS &&
          info->queryType != PM_QUERY_REALTIME_STEP_STATISTICS))
         return PM_ERROR_INVALID_ARGUMENT;
-    // The realtime telemetry ledger is not produced by this driver.
-    if (info->queryType == PM_QUERY_REALTIME_STEP_STATISTICS) return PM_ERROR_FEATURE_NOT_PRESENT;
     auto* created = new (std::nothrow) PmQueryPool_T;
     if (!created) return PM_ERROR_OUT_OF_HOST_MEMORY;
     created->device = device;
@@ -1033,6 +1031,7 @@ PmResult PMAPI_CALL pmCmdResetQueryPool(PmCommandBuffer buffer, PmQueryPool pool
         for (uint32_t i = first; i < first + count; ++i) {
             pool->slots[i].available = false;
             pool->slots[i].statistics = {};
+            pool->slots[i].realtime = {};
         }
         return PM_SUCCESS;
     });
@@ -1056,16 +1055,19 @@ PmResult PMAPI_CALL pmCmdWriteTimestamp(PmCommandBuffer buffer, PmStageFlags, Pm
 PmResult PMAPI_CALL pmCmdBeginStatisticsQuery(PmCommandBuffer buffer, PmQueryPool pool, uint32_t query) {
     const PmResult state = require_recording(buffer);
     if (state != PM_SUCCESS) return state;
-    if (!pool || pool->device != buffer->device || pool->type != PM_QUERY_STEP_STATISTICS ||
+    if (!pool || pool->device != buffer->device ||
+        (pool->type != PM_QUERY_STEP_STATISTICS && pool->type != PM_QUERY_REALTIME_STEP_STATISTICS) ||
         query >= pool->slots.size() || buffer->statistics_open)
         return PM_ERROR_INVALID_ARGUMENT;
     buffer->statistics_open = true;
     buffer->statistics_pool = pool;
     buffer->statistics_query = query;
     buffer->statistics_simulation = nullptr;
+    buffer->statistics_step_count = 0;
     return record_query(buffer, pool, query, 1u, [pool, query]() -> PmResult {
         std::lock_guard<std::mutex> lock(pool->mutex);
         pool->slots[query].statistics = {};
+        pool->slots[query].realtime = {};
         pool->slots[query].available = false;
         return PM_SUCCESS;
     });
@@ -1074,18 +1076,30 @@ PmResult PMAPI_CALL pmCmdBeginStatisticsQuery(PmCommandBuffer buffer, PmQueryPoo
 PmResult PMAPI_CALL pmCmdEndStatisticsQuery(PmCommandBuffer buffer, PmQueryPool pool, uint32_t query) {
     const PmResult state = require_recording(buffer);
     if (state != PM_SUCCESS) return state;
-    if (!pool || pool->device != buffer->device || pool->type != PM_QUERY_STEP_STATISTICS ||
+    // A realtime statistics query brackets exactly one step
+    // (reference src/api/queries.cpp:159-172).
+    if (!pool || pool->device != buffer->device ||
+        (pool->type != PM_QUERY_STEP_STATISTICS && pool->type != PM_QUERY_REALTIME_STEP_STATISTICS) ||
         query >= pool->slots.size() || !buffer->statistics_open || buffer->statistics_pool != pool ||
-        buffer->statistics_query != query || !buffer->statistics_simulation)
+        buffer->statistics_query != query || !buffer->statistics_simulation ||
+        (pool->type == PM_QUERY_REALTIME_STEP_STATISTICS && buffer->statistics_step_count != 1u))
         return PM_ERROR_INVALID_ARGUMENT;
     PmSimulation_T* simulation = buffer->statistics_simulation;
     buffer->statistics_open = false;
     buffer->statistics_pool = nullptr;
     buffer->statistics_simulation = nullptr;
+    buffer->statistics_step_count = 0;
     return record_query(buffer, pool, query, 1u, [pool, query, simulation]() -> PmResult {
         std::lock_guard<std::mutex> lock(pool->mutex);
-        fill_statistics(simulation, pool->slots[query].statistics);
-        pool->slots[query].available = true;
+        auto& slot = pool->slots[query];
+        fill_statistics(simulation, slot.statistics);
+        if (pool->type == PM_QUERY_REALTIME_STEP_STATISTICS) {
+            const PmResult r = fill_realtime_statistics(simulation, slot.realtime);
+            if (r != PM_SUCCESS) return r;
+            slot.realtime.step = slot.statistics;
+            slot.realtime.step.stepCount = 1;  // query-local, as the reference reports it
+        }
+        slot.available = true;
         return PM_SUCCESS;
     });
 }
@@ -1095,7 +1109,9 @@ PmResult PMAPI_CALL pmGetQueryPoolResults(PmDevice device, PmQueryPool pool, uin
     if (!device || !pool || pool->device != device || count == 0u || !data || first > pool->slots.size() ||
         count > pool->slots.size() - first)
         return PM_ERROR_INVALID_ARGUMENT;
-    const size_t value_size = pool->type == PM_QUERY_TIMESTAMP ? sizeof(uint64_t) : sizeof(PmStepStatistics);
+    const size_t value_size = pool->type == PM_QUERY_TIMESTAMP                   ? sizeof(uint64_t)
+                              : pool->type == PM_QUERY_REALTIME_STEP_STATISTICS ? sizeof(PmRealtimeStepStatistics)
+                                                                                : sizeof(PmStepStatistics);
     const size_t record_size = value_size + ((flags & PM_QUERY_RESULT_WITH_AVAILABILITY_BIT) ? sizeof(uint64_t) : 0);
     if (stride < record_size || data_size < record_size + size_t(count - 1u) * size_t(stride))
         return PM_ERROR_INVALID_ARGUMENT;
@@ -1126,6 +1142,8 @@ PmResult PMAPI_CALL pmGetQueryPoolResults(PmDevice device, PmQueryPool pool, uin
                     return PM_ERROR_DEVICE_LOST;
                 const uint64_t ns = uint64_t(double(ms) * 1.0e6);
                 std::memcpy(dst, &ns, sizeof(ns));
+            } else if (pool->type == PM_QUERY_REALTIME_STEP_STATISTICS) {
+                std::memcpy(dst, &slot.realtime, sizeof(PmRealtimeStepStatistics));
             } else {
                 std::memcpy(dst, &slot.statistics, sizeof(PmStepStatistics));
             }

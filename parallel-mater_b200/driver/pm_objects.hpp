@@ -204,6 +204,7 @@ struct PmCommandBuffer_T {
     PmQueryPool_T* statistics_pool{};
     uint32_t statistics_query{};
     PmSimulation_T* statistics_simulation{};
+    uint32_t statistics_step_count{};  // steps recorded inside an open statistics query
     pmd::CompletionPtr completion;
 };
 
@@ -228,6 +229,7 @@ struct PmQueryPool_T {
         bool available{};
         void* event{};  // timestamps
         PmStepStatistics statistics{};
+        PmRealtimeStepStatistics realtime{};
         pmd::CompletionPtr completion;
     };
     std::vector<Slot> slots;
@@ -257,5 +259,6 @@ PmResult record_query(PmCommandBuffer_T* buffer, PmQueryPool_T* pool, uint32_t f
 PFN_pmVoidFunction lookup_rigid(const char* name);
 // Statistics of a simulation's last tick, for step-statistics queries.
 void fill_statistics(PmSimulation_T* simulation, PmStepStatistics& out);
+PmResult fill_realtime_statistics(PmSimulation_T* simulation, PmRealtimeStepStatistics& out);
 
 }  // namespace pmd

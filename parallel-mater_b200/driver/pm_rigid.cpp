@@ -548,6 +548,9 @@ PmResult PMAPI_CALL pmCmdStepSimulation(PmCommandBuffer buffer, PmSimulation sim
         (step->flags & ~PmFlags(PM_STEP_COLLECT_CONTACT_EVENTS_BIT)) != 0u)
         return PM_ERROR_INVALID_ARGUMENT;
     if (!realtime_timestep(step->timestep) || step->substeps != 1u) return PM_ERROR_INVALID_ARGUMENT;
+    if (buffer->statistics_open && buffer->statistics_pool->type == PM_QUERY_REALTIME_STEP_STATISTICS &&
+        buffer->statistics_step_count != 0u)
+        return PM_ERROR_INVALID_ARGUMENT;  // one step per realtime statistics query (resources.cpp:1243-1246)
     const PmStepInfo copied = *step;
     const uint32_t iterations = buffer->bound_pipeline->rigid.rigidIterations;
     const PmResult recorded = record_simulation(buffer, simulation, [simulation, copied, iterations]() -> PmResult {
@@ -599,7 +602,10 @@ PmResult PMAPI_CALL pmCmdStepSimulation(PmCommandBuffer buffer, PmSimulation sim
         }
         return r;
     });
-    if (recorded == PM_SUCCESS && buffer->statistics_open) buffer->statistics_simulation = simulation;
+    if (recorded == PM_SUCCESS && buffer->statistics_open) {
+        buffer->statistics_simulation = simulation;
+        ++buffer->statistics_step_count;
+    }
     return recorded;
 }
 
@@ -756,6 +762,50 @@ void fill_statistics(PmSimulation_T* s, PmStepStatistics& out) {
     out.overflowCount = uint64_t(__builtin_popcount(s->last.status & overflow));
     out.executionResult = s->execution_result.load();
     out.earlyExitCount = 0;
+}
+
+// Realtime step statistics (reference src/api/queries.cpp:215-250): the
+// latest tick's telemetry from the core library, in the reference's work
+// phases. The tick issues one queue submission, reads nothing back and waits
+// for nothing inside itself; one spatial index is built and published.
+PmResult fill_realtime_statistics(PmSimulation_T* s, PmRealtimeStepStatistics& out) {
+    out = {};
+    out.schemaVersion = 1;
+    out.profileVersion = 1;
+    out.budgetVersion = 1;
+    out.phaseCount = PM_REALTIME_WORK_PHASE_COUNT;
+    out.tick = s->submitted_steps;
+    if (!s->world) return PM_SUCCESS;
+    pmb_tick_telemetry t{};
+    const int rc = pmb_world_tick_telemetry(s->world, &t);
+    if (rc != PMB_SUCCESS) return from_core(rc);
+    for (int p = 0; p < PM_REALTIME_WORK_PHASE_COUNT; ++p) {
+        PmRealtimeWorkStatistics& w = out.phases[p];
+        w.dispatches = t.dispatches[p];
+        w.workgroups = t.workgroups[p];
+        w.bytesMoved = t.bytes_moved[p];
+        w.barriers = t.barriers[p];
+    }
+    out.phases[PM_REALTIME_WORK_PHASE_INDEX].spatialIndexBuilds = t.spatial_builds;
+    out.phases[PM_REALTIME_WORK_PHASE_INDEX].spatialIndexPublications = t.spatial_builds;
+    out.phases[PM_REALTIME_WORK_PHASE_DOMAIN].numericalIterations = t.sweeps;
+    out.phases[PM_REALTIME_WORK_PHASE_BOUNDARY].queueSubmissions = 1;
+    for (const auto& w : out.phases) {
+        out.total.dispatches += w.dispatches;
+        out.total.workgroups += w.workgroups;
+        out.total.bytesMoved += w.bytesMoved;
+        out.total.spatialIndexBuilds += w.spatialIndexBuilds;
+        out.total.spatialIndexRefits += w.spatialIndexRefits;
+        out.total.spatialIndexPublications += w.spatialIndexPublications;
+        out.total.numericalIterations += w.numericalIterations;
+        out.total.barriers += w.barriers;
+        out.total.queueSubmissions += w.queueSubmissions;
+        out.total.intraTickHostReadbacks += w.intraTickHostReadbacks;
+        out.total.intraTickHostWaits += w.intraTickHostWaits;
+    }
+    out.timeAdvances = s->execution_result.load() == PM_SUCCESS ? 1u : 0u;
+    out.domainIterations[0] = t.sweeps;  // rigid contact and joint sweeps
+    return PM_SUCCESS;
 }
 
 PFN_pmVoidFunction lookup_rigid(const char* name) {

@@ -40,7 +40,7 @@ TIMEOUT_INFINITE = 2**64 - 1
 INVALID_INDEX = 2**32 - 1
 FORMAT_R32_UINT, FORMAT_R32G32B32_SFLOAT = 1, 3
 STAGE_ALL_COMMANDS = 0x1E
-QUERY_TIMESTAMP, QUERY_STEP_STATISTICS = 0, 1
+QUERY_TIMESTAMP, QUERY_STEP_STATISTICS, QUERY_REALTIME_STEP_STATISTICS = 0, 1, 2
 QUERY_RESULT_WAIT = 1
 
 
@@ -151,6 +151,16 @@ StepStatistics = S("PmStepStatistics", [(n, u64) for n in (
     "stepCount", "substepsExecuted", "poseIterations", "impactIterations", "peakContactCount",
     "peakActiveBodies", "peakAwakeBodies", "peakParticleCount", "scratchHighWaterBytes",
     "overflowCount")] + [("executionResult", i32), ("earlyExitCount", u32)])
+REALTIME_PHASES = ("boundary", "predict", "index", "candidates", "domain", "coupling", "commit")
+RealtimeWorkStatistics = S("PmRealtimeWorkStatistics", [(n, u64) for n in (
+    "dispatches", "workgroups", "bytesMoved", "spatialIndexBuilds", "spatialIndexRefits",
+    "spatialIndexPublications", "numericalIterations", "barriers", "queueSubmissions",
+    "intraTickHostReadbacks", "intraTickHostWaits")])
+RealtimeStepStatistics = S("PmRealtimeStepStatistics", [
+    ("step", StepStatistics), ("schemaVersion", u32), ("profileVersion", u32), ("budgetVersion", u32),
+    ("phaseCount", u32), ("tick", u64), ("total", RealtimeWorkStatistics),
+    ("phases", RealtimeWorkStatistics * len(REALTIME_PHASES)), ("timeAdvances", u64),
+    ("domainIterations", u64 * 6), ("couplingEdgeCount", u64), ("couplingSweeps", u64)])
 ConstraintState = S("PmConstraintState", [("enabled", u32), ("broken", u32), ("appliedImpulse", f32)])
 
 R = i32  # PmResult
@@ -353,6 +363,7 @@ class RigidSession:
         cb = vp()
         check(self.api.pmAllocateCommandBuffers(dev, pool, 1, ref(cb)), "pmAllocateCommandBuffers")
         self.cb = cb
+        self.query_pools = {}
         # state read-back buffer in host-visible memory
         self.state_bytes = 52 * scene.n
         self.state_mem, self.state_buf, self.state_ptr = self._mapped_buffer(self.state_bytes)
@@ -501,17 +512,19 @@ class RigidSession:
         """One tick; returns the submission result. inputs: list of
         (body, force, torque, linear impulse, angular impulse); targets:
         {body: state record}. statistics: wrap the step in a step-statistics
-        query, read afterwards with step_statistics(). events: collect the
+        query, read afterwards with step_statistics(); "realtime" uses a
+        realtime query instead (realtime_statistics()). events: collect the
         tick's contact events; copy_events (default: events) records
         pmCmdCopyContactEvents after the step (read with contact_events())."""
         copy_events = events if copy_events is None else copy_events
         step = StepInfo(1.0 / 60.0, 1, (f32 * 3)(*gravity), 1 if events else 0)
-        if statistics and getattr(self, "query_pool", None) is None:
+        kind = QUERY_REALTIME_STEP_STATISTICS if statistics == "realtime" else QUERY_STEP_STATISTICS
+        if statistics and self.query_pools.get(kind) is None:
             qp = vp()
-            check(self.api.pmCreateQueryPool(self.dev, ref(QueryPoolCreateInfo(ST_QUERY_POOL, None,
-                                                                               QUERY_STEP_STATISTICS, 1)),
+            check(self.api.pmCreateQueryPool(self.dev, ref(QueryPoolCreateInfo(ST_QUERY_POOL, None, kind, 1)),
                                              ref(qp)), "pmCreateQueryPool")
-            self.query_pool = qp
+            self.query_pools[kind] = qp
+        pool = self.query_pools.get(kind)
 
         def rec():
             check(self.api.pmCmdBindPhysicsPipeline(self.cb, self.pipeline), "pmCmdBindPhysicsPipeline")
@@ -524,11 +537,11 @@ class RigidSession:
                 t = _state(s)
                 check(self.api.pmCmdSetKinematicTargets(self.cb, self.sim, b, 1, ref(t)), "pmCmdSetKinematicTargets")
             if statistics:
-                check(self.api.pmCmdResetQueryPool(self.cb, self.query_pool, 0, 1), "pmCmdResetQueryPool")
-                check(self.api.pmCmdBeginStatisticsQuery(self.cb, self.query_pool, 0), "pmCmdBeginStatisticsQuery")
+                check(self.api.pmCmdResetQueryPool(self.cb, pool, 0, 1), "pmCmdResetQueryPool")
+                check(self.api.pmCmdBeginStatisticsQuery(self.cb, pool, 0), "pmCmdBeginStatisticsQuery")
             check(self.api.pmCmdStepSimulation(self.cb, self.sim, ref(step)), "pmCmdStepSimulation")
             if statistics:
-                check(self.api.pmCmdEndStatisticsQuery(self.cb, self.query_pool, 0), "pmCmdEndStatisticsQuery")
+                check(self.api.pmCmdEndStatisticsQuery(self.cb, pool, 0), "pmCmdEndStatisticsQuery")
             if states:
                 rng = BufferRange(self.state_buf, 0, self.state_bytes)
                 check(self.api.pmCmdCopyRigidStates(self.cb, self.sim, 0, self.scene.n, ref(rng)),
@@ -569,9 +582,19 @@ class RigidSession:
                                           "pmCmdSetRigidStates"))
 
     def step_statistics(self):
+        """PmStepStatistics of the last step(statistics=True)."""
         out = StepStatistics()
-        check(self.api.pmGetQueryPoolResults(self.dev, self.query_pool, 0, 1, C.sizeof(out), ref(out),
-                                             C.sizeof(out), QUERY_RESULT_WAIT), "pmGetQueryPoolResults")
+        check(self.api.pmGetQueryPoolResults(self.dev, self.query_pools[QUERY_STEP_STATISTICS], 0, 1,
+                                             C.sizeof(out), ref(out), C.sizeof(out), QUERY_RESULT_WAIT),
+              "pmGetQueryPoolResults")
+        return out
+
+    def realtime_statistics(self):
+        """PmRealtimeStepStatistics of the last step(statistics="realtime")."""
+        out = RealtimeStepStatistics()
+        check(self.api.pmGetQueryPoolResults(self.dev, self.query_pools[QUERY_REALTIME_STEP_STATISTICS], 0, 1,
+                                             C.sizeof(out), ref(out), C.sizeof(out), QUERY_RESULT_WAIT),
+              "pmGetQueryPoolResults")
         return out
 
     def states(self):
@@ -589,8 +612,8 @@ class RigidSession:
         a = self.api
         a.pmDeviceWaitIdle(self.dev)
         a.pmDestroyFence(self.dev, self.fence)
-        if getattr(self, "query_pool", None) is not None:
-            a.pmDestroyQueryPool(self.dev, self.query_pool)
+        for qp in self.query_pools.values():
+            a.pmDestroyQueryPool(self.dev, qp)
         a.pmDestroyCommandPool(self.dev, self.pool)
         a.pmDestroyPhysicsPipeline(self.dev, self.pipeline)
         a.pmDestroySimulation(self.dev, self.sim)

@@ -54,6 +54,59 @@ def test_reference_command_flow(gpu_available):
         s.close()
 
 
+def test_realtime_step_statistics(gpu_available):
+    """PM_QUERY_REALTIME_STEP_STATISTICS brackets one step and reports its
+    work ledger with the invariants the reference's realtime tests check
+    (tests/api/native_realtime_runtime_tests.cpp:550-555): one time advance,
+    one spatial index built and published, no host readback inside the tick;
+    the total is the sum of the phases and the dispatch count is every kernel
+    the tick launched (the first step also creates the world, whose set-up
+    launches are not part of a tick)."""
+    scene = pm.canonical_scene(scenes.pyramid(levels=5, seed=2, profile=scenes.REALTIME))
+    s = pm.RigidSession(scene, iterations=8)
+    try:
+        assert s.step(states=False) == pm.SUCCESS
+        for t in range(3):
+            before = core.kernel_launches()
+            assert s.step(statistics="realtime", states=False) == pm.SUCCESS
+            launched = core.kernel_launches() - before
+            r = s.realtime_statistics()
+            assert (r.schemaVersion, r.profileVersion, r.budgetVersion, r.phaseCount) == (1, 1, 1, 7)
+            assert r.tick == t + 2 and r.step.stepCount == 1 and r.step.executionResult == 0
+            assert r.timeAdvances == 1
+            assert r.total.spatialIndexBuilds == 1 and r.total.spatialIndexPublications == 1
+            assert r.total.intraTickHostReadbacks == 0 and r.total.intraTickHostWaits == 0
+            assert r.total.queueSubmissions == 1
+            assert r.domainIterations[0] == r.phases[4].numericalIterations >= 8
+            assert list(r.domainIterations)[1:] == [0] * 5 and r.couplingEdgeCount == 0
+            for f, _ in pm.RealtimeWorkStatistics._fields_:
+                assert getattr(r.total, f) == sum(getattr(p, f) for p in r.phases), f
+            assert r.total.dispatches == launched
+            by_phase = {name: r.phases[k] for k, name in enumerate(pm.REALTIME_PHASES)}
+            for name in ("predict", "index", "candidates", "domain", "commit"):
+                assert by_phase[name].dispatches > 0 and by_phase[name].workgroups > 0, name
+                assert by_phase[name].bytesMoved > 0, name
+            assert by_phase["coupling"].dispatches == 0
+            assert by_phase["domain"].barriers > 0
+        # A realtime query brackets exactly one step: a second step inside
+        # the open query, or an end with no step, is rejected at recording.
+        a, cb, qp = s.api, s.cb, s.query_pools[pm.QUERY_REALTIME_STEP_STATISTICS]
+        step = pm.StepInfo(1.0 / 60.0, 1, (ctypes.c_float * 3)(0, -9.81, 0), 0)
+        assert a.pmBeginCommandBuffer(cb, ctypes.byref(pm.CommandBufferBeginInfo(pm.ST_BEGIN, None, 0))) == 0
+        assert a.pmCmdBindPhysicsPipeline(cb, s.pipeline) == 0
+        assert a.pmCmdResetQueryPool(cb, qp, 0, 1) == 0
+        assert a.pmCmdBeginStatisticsQuery(cb, qp, 0) == 0
+        assert a.pmCmdEndStatisticsQuery(cb, qp, 0) == pm.ERROR_INVALID_ARGUMENT
+        assert a.pmCmdStepSimulation(cb, s.sim, ctypes.byref(step)) == 0
+        assert a.pmCmdStepSimulation(cb, s.sim, ctypes.byref(step)) == pm.ERROR_INVALID_ARGUMENT
+        assert a.pmCmdEndStatisticsQuery(cb, qp, 0) == 0
+        assert a.pmEndCommandBuffer(cb) == 0
+        assert s.submit() == pm.SUCCESS
+        assert s.realtime_statistics().tick == 5
+    finally:
+        s.close()
+
+
 def _run_api_vs_oracle(scene, ticks, per_tick=None):
     scene = pm.canonical_scene(scene)
     s = pm.RigidSession(scene)
@@ -230,10 +283,10 @@ def test_error_codes(gpu_available):
         sci = pm.SimulationCreateInfo(pm.ST_SIMULATION, None, 0, 4, 0, 0, 1)
         sim = ctypes.c_void_p()
         assert a.pmCreateSimulation(dev, ctypes.byref(sci), ctypes.byref(sim)) == pm.ERROR_INVALID_ARGUMENT
-        # binding twice
+        # an unknown query type
         mem = ctypes.c_void_p()
-        assert a.pmCreateQueryPool(dev, ctypes.byref(pm.QueryPoolCreateInfo(pm.ST_QUERY_POOL, None, 2, 1)),
-                                   ctypes.byref(mem)) == pm.ERROR_FEATURE_NOT_PRESENT
+        assert a.pmCreateQueryPool(dev, ctypes.byref(pm.QueryPoolCreateInfo(pm.ST_QUERY_POOL, None, 3, 1)),
+                                   ctypes.byref(mem)) == pm.ERROR_INVALID_ARGUMENT
     finally:
         s.close()
 
