@@ -23,6 +23,30 @@ template <class R> inline bool collision_disabled(const World<R>& w, uint32_t a,
     return false;
 }
 
+// pm_build_fixed_collision_groups (geometry.slang:3102-3136): bodies joined
+// through enabled, unbroken, collision-disabling fixed joints form a group
+// whose root is its smallest dense index; a pair inside one group is not a
+// candidate (:902-904). Empty when the world has no joints (the filter then
+// gets no group buffer, production_realtime_backend.cu.inc:7684-7687).
+template <class R> inline std::vector<uint32_t> fixed_groups(const World<R>& w) {
+    std::vector<uint32_t> root;
+    if (w.joints.empty()) return root;
+    root.resize(w.n);
+    for (uint32_t i = 0; i < w.n; ++i) root[i] = i;
+    auto find = [&](uint32_t b) {
+        while (root[b] != b) b = root[b];
+        return b;
+    };
+    for (auto& j : w.joints) {
+        if (!j.alive || !j.d.enabled || j.broken || !j.d.disable_collisions || j.d.type != kFixed) continue;
+        if (j.d.body_a >= w.n || j.d.body_b >= w.n) continue;
+        const uint32_t a = find(j.d.body_a), b = find(j.d.body_b);
+        if (a != b) root[std::max(a, b)] = std::min(a, b);
+    }
+    for (uint32_t i = 0; i < w.n; ++i) root[i] = find(i);
+    return root;
+}
+
 // Sorted candidate pairs (a dynamic query body, b any other leaf whose swept
 // proxy overlaps a's). A uniform grid keyed on AABB centre lists candidates;
 // the predicate and the (a, b) order are the reference's.
@@ -56,6 +80,7 @@ template <class R> inline std::vector<uint32_t> broadphase(const World<R>& w) {
     };
     std::map<std::array<int64_t, 3>, std::vector<uint32_t>> grid;
     for (uint32_t i : small) grid[key(i, 0, 0, 0)].push_back(i);
+    const std::vector<uint32_t> group = fixed_groups(w);
     std::vector<uint32_t> cand;
     for (uint32_t a = 0; a < n; ++a) {
         if (!dynamic(w, a)) continue;
@@ -64,6 +89,7 @@ template <class R> inline std::vector<uint32_t> broadphase(const World<R>& w) {
             if (b == a) return;
             if (!overlaps(w.aabb_lo[b], w.aabb_hi[b], w.aabb_lo[a], w.aabb_hi[a])) return;
             if (dynamic(w, b) && !(a < b)) return;
+            if (!group.empty() && group[a] == group[b]) return;
             if (collision_disabled(w, a, b)) return;
             cand.push_back(b);
         };

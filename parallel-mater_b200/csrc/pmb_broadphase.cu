@@ -275,13 +275,55 @@ __device__ __forceinline__ bool collision_disabled(const Dev& d, uint32_t a, uin
 }
 
 // Candidate predicate: overlap (leaf b against query a), a != b, identity
-// order between two dynamic bodies, no collision-disabling joint.
+// order between two dynamic bodies, different fixed collision groups, no
+// collision-disabling joint (geometry.slang:897-913).
 __device__ __forceinline__ bool candidate(const Dev& d, uint32_t a, uint32_t b, float4 alo, float4 ahi) {
     if (b == a || d.is_large[b] == 2) return false;
     if (!aabb_overlap(d.lo[b], d.hi[b], alo, ahi)) return false;
     if (d.motion[b] == kDynamic && !(a < b)) return false;
+    if (d.n_fixed && d.fixed_root[a] == d.fixed_root[b]) return false;
     if (collision_disabled(d, a, b)) return false;
     return true;
+}
+
+__device__ __forceinline__ uint32_t group_root(const volatile uint32_t* root, uint32_t b, uint32_t n) {
+    for (uint32_t hop = 0; hop < n; ++hop) {
+        const uint32_t p = root[b];
+        if (p == b) break;
+        b = p;
+    }
+    return b;
+}
+
+// Fixed collision groups (pm_build_fixed_collision_groups,
+// geometry.slang:3102-3136): the groups are the connected components of the
+// unbroken fixed joints that disable collisions, and each body's root is the
+// smallest body of its component. One block: the unions run concurrently,
+// every link hangs the larger of two roots under the smaller with a
+// compare-and-swap, so a tree's root is always its smallest member and the
+// result does not depend on the order the joints are taken in. Each loop is
+// bounded by the body count (a failed swap means another union progressed).
+__global__ void __launch_bounds__(1024) k_fixed_groups(Dev d) {
+    volatile uint32_t* root = d.fixed_root;
+    for (uint32_t i = threadIdx.x; i < d.n; i += blockDim.x) root[i] = i;
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < d.n_fixed; k += blockDim.x) {
+        const uint32_t j = d.fixed_list[k];
+        if (d.jstate[j].broken) continue;
+        uint32_t a = d.joints[j].body_a, b = d.joints[j].body_b;
+        for (uint32_t attempt = 0; attempt <= d.n; ++attempt) {
+            a = group_root(root, a, d.n);
+            b = group_root(root, b, d.n);
+            if (a == b) break;
+            const uint32_t hi = a > b ? a : b, lo = a > b ? b : a;
+            if (atomicCAS(d.fixed_root + hi, hi, lo) == hi) break;
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < d.n; i += blockDim.x) {
+        const uint32_t r = group_root(root, i, d.n);
+        root[i] = r;
+    }
 }
 
 // The candidates of query body a that lane gl of a kQueryLanes-lane group
@@ -414,6 +456,10 @@ void launch_broadphase(const Dev& d, cudaStream_t s) {
     note_launch(blocks_for(d.n));
     prof_mark(s, "grid build");
     set_phase(kPhCandidates);
+    if (d.n_fixed) {
+        k_fixed_groups<<<1, 1024, 0, s>>>(d);
+        note_launch(1);
+    }
     k_query_count<<<blocks_for(kQueryLanes * d.n, 128), 128, 0, s>>>(d);
     note_launch(blocks_for(kQueryLanes * d.n, 128));
     prof_mark(s, "query count");

@@ -270,6 +270,7 @@ struct Sizes {
     size_t verts, planes, dis, hinges, hinge_segs;
     uint32_t cap_cand, cap_pair, cap_contact;
     uint32_t events;
+    size_t fixed;  // fixed collision-disabling joints
 };
 struct Extra {
     float4 *lo, *hi, *sph;  // mesh bounds, read once at creation
@@ -344,6 +345,7 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     ALLOCP(d.ctr, 1);
     ALLOC(e.lo, nm); ALLOC(e.hi, nm); ALLOC(e.sph, nm);
     ALLOCP(e.dis, z.dis); ALLOCP(d.dis_joint, z.dis);
+    ALLOCP(d.fixed_list, z.fixed); ALLOC(d.fixed_root, z.fixed ? size_t(n) : 0);
     if (z.scenes > 1) {
         const uint32_t ns = z.scenes;
         ALLOCP(d.scene_of, n); ALLOCP(d.scene_body_off, ns + 1); ALLOCP(d.scene_iters, ns); ALLOCP(d.scene_jiters, ns);
@@ -498,6 +500,13 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
         }
     }
     std::sort(dis_entries.begin(), dis_entries.end());
+    // Fixed joints that disable collisions join their bodies' collision groups.
+    std::vector<uint32_t> fixed_list;
+    for (uint32_t j = 0; j < nj; ++j) {
+        const pmb_joint& o = desc->joints[j];
+        if (o.type == kFixed && o.enabled && o.disable_collisions && o.body_a < n && o.body_b < n)
+            fixed_list.push_back(j);
+    }
     std::vector<uint64_t> dis_keys(dis_entries.size());
     std::vector<uint32_t> dis_joint(dis_entries.size());
     for (size_t k = 0; k < dis_entries.size(); ++k) {
@@ -527,7 +536,8 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     d.n_hinge_segs = uint32_t(hinge_seg.size() - 1);
     d.event_capacity = desc->event_capacity;
     const Sizes z{n, nm, nj, ns, verts.size(), planes.size(), dis_keys.size(), hinge_list.size(),
-                  hinge_seg.size() - 1, d.cap_cand, d.cap_pair, d.cap_contact, desc->event_capacity};
+                  hinge_seg.size() - 1, d.cap_cand, d.cap_pair, d.cap_contact, desc->event_capacity,
+                  fixed_list.size()};
     if (w->arena[kPersistent]) {
         // Bound memory must hold the whole layout before anything is carved.
         pmb_world probe;
@@ -546,6 +556,7 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     uint64_t* dis = ex.dis;
     d.dis_keys = reinterpret_cast<uint32_t*>(dis);
     d.n_dis = uint32_t(dis_keys.size());
+    d.n_fixed = uint32_t(fixed_list.size());
     if (r != PMB_SUCCESS) {
         pmb_world_destroy(w);
         return r;
@@ -608,6 +619,7 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
         up(dis, dis_keys.data(), 8 * dis_keys.size());
         up(d.dis_joint, dis_joint.data(), 4 * dis_joint.size());
     }
+    if (!fixed_list.empty()) up(d.fixed_list, fixed_list.data(), 4 * fixed_list.size());
     std::vector<uint32_t> colors(n, kInvalid);
     up(d.color, colors.data(), 4 * n);
     launch_body_constants(d, dlo, dhi, dsph, s);
@@ -1055,7 +1067,8 @@ int pmb_world_memory_requirements(const pmb_world_capacity* c, uint64_t* persist
                   c->candidate_capacity ? c->candidate_capacity : 64u * n + 4096u,
                   c->pair_capacity ? c->pair_capacity : 24u * n + 1024u,
                   c->contact_capacity ? c->contact_capacity : 64u * n + 4096u,
-                  c->event_capacity};
+                  c->event_capacity,
+                  size_t(c->joint_count)};
     Extra ex{};
     allocate_world(&probe, probe.d, z, ex);
     *persistent = probe.arena_used[kPersistent];

@@ -221,6 +221,11 @@ struct Dev {
     uint32_t* dis_keys;    // sorted (min<<32|max) keys of collision-disabling joints
     uint32_t* dis_joint;   // the joint of each key (a pair may have several)
     uint32_t n_dis;
+    // fixed collision groups: fixed, collision-disabling joints (ascending)
+    // and each body's group root, rebuilt every tick from the joints' state
+    uint32_t* fixed_list;
+    uint32_t* fixed_root;
+    uint32_t n_fixed;
     // hinge joints (ascending index) grouped by scene: segment k is
     // hinge_list[hinge_seg[k] .. hinge_seg[k+1]); scenes share no bodies
     uint32_t* hinge_list;

@@ -375,6 +375,34 @@ def chains(count=512, links=64, seed=3, radius=0.05, length=0.4, spacing=1.0,
     return b.build(f"chains{count}x{links}", iterations, profile)
 
 
+def welded_groups(profile=LEGACY, iterations=10, disable_bc=True) -> Scene:
+    """Fixed collision groups. Bars A, B, C (1.2 m long) in a row 0.5 m apart,
+    welded A-B and B-C by collision-disabling fixed joints: A and C overlap
+    but share a group, so they never touch. Boxes D and E overlap each other
+    and are each welded to the static post P: the post joins them into one
+    group. A free box F rests on C (an ordinary contact with a group member).
+    disable_bc=False leaves the B-C weld colliding, which splits the first
+    group, so A-C and B-C become candidate pairs."""
+    b = _Builder()
+    _ground(b, 4.0, 4.0)
+    bar = b.mesh(*box_mesh((0.6, 0.1, 0.1)))
+    small = b.mesh(*box_mesh((0.2, 0.1, 0.1)))
+    post = b.mesh(*box_mesh((0.1, 1.0, 0.1)))
+    cube = b.mesh(*box_mesh((0.15, 0.15, 0.15)))
+    bar_inertia = box_inertia(1.0, (0.6, 0.1, 0.1))
+    small_inertia = box_inertia(0.5, (0.2, 0.1, 0.1))
+    bars = [b.body(bar, DYNAMIC, (-1.0 + 0.5 * k, 0.3, 0.0), mass=1.0, inertia=bar_inertia) for k in range(3)]
+    b.joint(FIXED, bars[0], bars[1], (0.25, 0.0, 0.0), (-0.25, 0.0, 0.0))
+    b.joint(FIXED, bars[1], bars[2], (0.25, 0.0, 0.0), (-0.25, 0.0, 0.0), disable_collisions=disable_bc)
+    p = b.body(post, STATIC, (2.0, 1.0, 0.0))
+    d = b.body(small, DYNAMIC, (2.25, 1.5, 0.0), mass=0.5, inertia=small_inertia)
+    e = b.body(small, DYNAMIC, (2.3, 1.55, 0.0), mass=0.5, inertia=small_inertia)
+    b.joint(FIXED, p, d, (0.15, 0.5, 0.0), (-0.1, 0.0, 0.0))
+    b.joint(FIXED, p, e, (0.15, 0.55, 0.0), (-0.15, 0.0, 0.0))
+    b.body(cube, DYNAMIC, (0.1, 0.56, 0.0), mass=0.5, inertia=box_inertia(0.5, (0.15,) * 3))
+    return b.build("welded groups", iterations, profile)
+
+
 def cube_pair(profile=REALTIME) -> Scene:
     """A static unit cube at y = -1 and a dynamic one at y = 2 (mass 1,
     inertia 1/6, friction 0.5, damping 0.05, speed limits 100, margin 5 mm):

@@ -137,6 +137,24 @@ def test_joint_zoo_matches_oracle(gpu_available):
     print("joint zoo worst |gpu-oracle| =", worst)
 
 
+def test_fixed_collision_groups_match_oracle(gpu_available):
+    """Fixed collision groups on the GPU: the candidate pairs equal the
+    oracle's every tick (no pair inside a group), and poses follow it."""
+    s = scenes.welded_groups()
+    w = core.World(s)
+    o = O.OracleWorld(s)
+    for f in range(60):
+        sg, so = w.step(), o.step()
+        assert sg["status"] == 0 and so["status"] == 0
+        assert np.array_equal(w.candidate_pairs(), o.candidate_pairs()), f
+        assert sg["contacts"] == so["contacts"], f
+        xg, xo = w.states(), o.states()
+        err = max(np.abs(xg[k] - xo[k]).max() for k in ("x", "q", "v"))
+        assert err < 1e-4, (f, err)
+    codes = set(int(c) for c in w.candidate_pairs())
+    assert 1 * s.n + 3 not in codes and 5 * s.n + 6 not in codes
+
+
 def test_graph_replay_equals_steps(gpu_available):
     s = scenes.pyramid()
     a = core.World(s)

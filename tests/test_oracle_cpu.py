@@ -239,3 +239,26 @@ def test_joint_zoo_runs_every_joint_type():
     breakable = z.joints["breaking_threshold"] > 0
     assert (flags[breakable] & 2).all() and (counts[breakable] == 0).all()
     assert (flags[~breakable] == 1).all() and (counts[~breakable] > 0).all()
+
+
+def test_fixed_collision_groups_filter_candidates():
+    """Bodies joined by collision-disabling fixed joints share a collision
+    group (pm_build_fixed_collision_groups, geometry.slang:3102-3136) and no
+    pair inside a group is a candidate (:902-904): A-C of the welded bars and
+    D-E (joined through a static post) stay out, the outsider resting on C
+    stays in. Letting the B-C weld collide splits the bars' group."""
+    for disable_bc in (True, False):
+        s = scenes.welded_groups(disable_bc=disable_bc)
+        o = O.OracleWorld(s)
+        assert o.step()["status"] == 0
+        pairs = {(int(c) // s.n, int(c) % s.n) for c in o.candidate_pairs()}
+        assert ((1, 3) in pairs) == (not disable_bc)
+        assert ((2, 3) in pairs) == (not disable_bc)
+        assert (1, 2) not in pairs and (5, 6) not in pairs
+        assert (3, 7) in pairs
+    o = O.OracleWorld(scenes.welded_groups())
+    for _ in range(60):
+        assert o.step()["status"] == 0
+    x = o.states()["x"]
+    # the welded bars settle on the ground where they were put
+    assert np.allclose(x[1:4, 0], [-1.0, -0.5, 0.0], atol=1e-3) and np.allclose(x[1:4, 1], 0.101, atol=2e-3)
