@@ -1,0 +1,536 @@
+// SPDX-License-Identifier: MIT
+// Oracle (test infrastructure): the general triangle-mesh narrowphase of the
+// reference, restated for pairs the convex face path does not take.
+//
+// Reference: src/slang/geometry.slang
+//   hinge contact frames            :373-377, :404-492
+//   closest points (Ericson)        :949-1105, bounds overlap :1107-1116
+//   contact speed / rest offset     :1272-1290
+//   shell metadata                  :1308-1357
+//   triangle ranges                 :1359-1584
+//   swept-pair test                 :1586-1604
+//   feature normal                  :1855-1908
+//   BVH pair traversal              :2156-2299 (rigid_collide_meshes)
+//   bounds transforms               src/slang/math.slang:43-49, :142-190
+// What is restated: the unswept triangle ranges over the BVH traversal of
+// rigid_collide_meshes (swept bounds when the pair requires them), and the
+// per-body hinge frame fields those ranges read. Not restated: the swept
+// triangle ranges (:1921-2155), so a pair that needs continuous contact only
+// gets its end-pose contacts, and guided contacts (produced only there).
+#pragma once
+#include <vector>
+
+#include "avbd_world.hpp"
+
+namespace oracle {
+
+// The fields of HingeContactFrame (geometry.slang:143-157) the unswept ranges
+// read, and the body's reference point (the hinge anchor of a non-axial
+// hinge member, else its position).
+template <class R> struct HingeFrame {
+    V3<R> anchor, reference;
+    bool present{}, axial{}, fixed_member{}, static_body{};
+};
+
+// geometry.slang:404-492 (the anchor and flags; axis, guide mass and moment
+// only feed guided contacts). `joints_of_body`: the body's joints in
+// ascending index.
+template <class R>
+inline HingeFrame<R> hinge_frame(const World<R>& w, const std::vector<State<R>>& st, uint32_t i,
+                                 const std::vector<uint32_t>& joints_of_body) {
+    HingeFrame<R> f;
+    f.static_body = w.body[i].motion == kStatic;
+    if (!(w.body[i].inv_mass > 0.0f)) {
+        f.reference = st[i].x;
+        return f;
+    }
+    uint32_t incident = 0;
+    for (uint32_t ji : joints_of_body) {
+        const auto& j = w.joints[ji];
+        if (!j.alive || !j.d.enabled || j.broken) continue;
+        const bool is_a = j.d.body_a == i, is_b = j.d.body_b == i;
+        if (!is_a && !is_b) continue;
+        ++incident;
+        if (j.d.type == kFixed) f.fixed_member = true;
+        const bool axial = j.d.type == kPiston || j.d.type == kSlider;
+        const uint32_t other = is_a ? j.d.body_b : j.d.body_a;
+        const bool static_anchor = other < w.n && w.body[other].motion == kStatic;
+        if (f.present || (j.d.type != kHinge && !(axial && static_anchor && !(j.d.breaking_threshold > 0.0f))))
+            continue;
+        const float* la = is_a ? j.d.anchor_a : j.d.anchor_b;
+        f.anchor = add(st[i].x, rotate(st[i].q, v3<R>(la)));
+        f.present = true;
+        f.axial = static_anchor && axial;
+        if (static_anchor) {
+            const float* lo = is_a ? j.d.anchor_b : j.d.anchor_a;
+            f.anchor = add(st[other].x, rotate(st[other].q, v3<R>(lo)));
+        }
+    }
+    if (f.axial && incident != 1u) {
+        f.axial = false;
+        f.present = false;
+    }
+    f.reference = f.present && !f.axial ? f.anchor : st[i].x;
+    return f;
+}
+
+// Every body's frame at the given poses.
+template <class R> inline std::vector<HingeFrame<R>> hinge_frames(const World<R>& w, const std::vector<State<R>>& st) {
+    std::vector<std::vector<uint32_t>> by_body(w.n);
+    for (uint32_t j = 0; j < w.joints.size(); ++j) {
+        const auto& d = w.joints[j].d;
+        if (d.body_a < w.n) by_body[d.body_a].push_back(j);
+        if (d.body_b < w.n && d.body_b != d.body_a) by_body[d.body_b].push_back(j);
+    }
+    std::vector<HingeFrame<R>> out(w.n);
+    for (uint32_t i = 0; i < w.n; ++i) out[i] = hinge_frame(w, st, i, by_body[i]);
+    return out;
+}
+
+// geometry.slang:373-377
+template <class R> inline bool guided_pair(const HingeFrame<R>& a, const HingeFrame<R>& b) {
+    return (a.axial && b.static_body) || (b.axial && a.static_body);
+}
+
+// geometry.slang:949-997
+template <class R> inline void closest_segments(V3<R> p0, V3<R> p1, V3<R> q0, V3<R> q1, V3<R>& on_p, V3<R>& on_q) {
+    const V3<R> d0 = sub(p1, p0), d1 = sub(q1, q0), r = sub(p0, q0);
+    const R a = dot(d0, d0), e = dot(d1, d1);
+    R s = 0, t = 0;
+    if (a <= R(1.0e-12) && e <= R(1.0e-12)) {
+        on_p = p0;
+        on_q = q0;
+        return;
+    }
+    if (a <= R(1.0e-12)) {
+        t = clampv(dot(d1, r) / e, R(0), R(1));
+    } else {
+        const R c = dot(d0, r);
+        if (e <= R(1.0e-12)) {
+            s = clampv(-c / a, R(0), R(1));
+        } else {
+            const R b = dot(d0, d1), f = dot(d1, r);
+            const R den = a * e - b * b;
+            if (ab(den) > kEps<R>() * a * e) s = clampv((b * f - c * e) / den, R(0), R(1));
+            t = (b * s + f) / e;
+            if (t < R(0)) {
+                t = 0;
+                s = clampv(-c / a, R(0), R(1));
+            } else if (t > R(1)) {
+                t = 1;
+                s = clampv((b - c) / a, R(0), R(1));
+            }
+        }
+    }
+    on_p = add(p0, mul(d0, s));
+    on_q = add(q0, mul(d1, t));
+}
+
+// geometry.slang:1000-1031 (Voronoi regions of a triangle; the interior
+// witness is the plane projection of p)
+template <class R> inline V3<R> closest_on_triangle(V3<R> p, V3<R> a, V3<R> b, V3<R> c) {
+    const V3<R> ab_ = sub(b, a), ac = sub(c, a), ap = sub(p, a);
+    const R d1 = dot(ab_, ap), d2 = dot(ac, ap);
+    if (d1 <= R(0) && d2 <= R(0)) return a;
+    const V3<R> bp = sub(p, b);
+    const R d3 = dot(ab_, bp), d4 = dot(ac, bp);
+    if (d3 >= R(0) && d4 <= d3) return b;
+    const R vc = d1 * d4 - d3 * d2;
+    if (vc <= R(0) && d1 >= R(0) && d3 <= R(0)) return add(a, mul(ab_, d1 / (d1 - d3)));
+    const V3<R> cp = sub(p, c);
+    const R d5 = dot(ab_, cp), d6 = dot(ac, cp);
+    if (d6 >= R(0) && d5 <= d6) return c;
+    const R vb = d5 * d2 - d1 * d6;
+    if (vb <= R(0) && d2 >= R(0) && d6 <= R(0)) return add(a, mul(ac, d2 / (d2 - d6)));
+    const R va = d3 * d6 - d5 * d4;
+    if (va <= R(0) && d4 - d3 >= R(0) && d5 - d6 >= R(0))
+        return add(b, mul(sub(c, b), (d4 - d3) / ((d4 - d3) + (d5 - d6))));
+    const V3<R> nrm = cross(ab_, ac);
+    return sub(p, mul(nrm, dot(ap, nrm) / len2(nrm)));
+}
+
+// geometry.slang:1033-1055
+template <class R> inline bool point_in_triangle(V3<R> p, V3<R> a, V3<R> b, V3<R> c, V3<R> nrm) {
+    const R tol = R(-1.0e-5) * len2(nrm);
+    return dot(cross(sub(b, a), sub(p, a)), nrm) >= tol && dot(cross(sub(c, b), sub(p, b)), nrm) >= tol &&
+           dot(cross(sub(a, c), sub(p, c)), nrm) >= tol;
+}
+template <class R> inline bool segment_hits_triangle(V3<R> p, V3<R> q, V3<R> a, V3<R> b, V3<R> c, V3<R>& hit) {
+    hit = V3<R>{};
+    const V3<R> nrm = cross(sub(b, a), sub(c, a));
+    const V3<R> dir = sub(q, p);
+    const R den = dot(nrm, dir);
+    if (len2(nrm) <= kEps<R>() * kEps<R>() || ab(den) <= kEps<R>()) return false;
+    const R amount = dot(nrm, sub(a, p)) / den;
+    if (amount < R(0) || amount > R(1)) return false;
+    hit = add(p, mul(dir, amount));
+    return point_in_triangle(hit, a, b, c, nrm);
+}
+
+// geometry.slang:1057-1105: an edge crossing the other triangle is a zero-
+// distance witness; else the closest of vertex-face and edge-edge pairs.
+template <class R>
+inline void closest_triangle_pair(const V3<R> av[3], const V3<R> bv[3], V3<R>& best_a, V3<R>& best_b) {
+    V3<R> hit{};
+    for (uint32_t e = 0; e < 3; ++e)
+        if (segment_hits_triangle(av[e], av[(e + 1) % 3], bv[0], bv[1], bv[2], hit)) {
+            best_a = best_b = hit;
+            return;
+        }
+    for (uint32_t e = 0; e < 3; ++e)
+        if (segment_hits_triangle(bv[e], bv[(e + 1) % 3], av[0], av[1], av[2], hit)) {
+            best_a = best_b = hit;
+            return;
+        }
+    R best = R(3.402823466e38);
+    auto consider = [&](V3<R> p, V3<R> q) {
+        const R s = len2(sub(p, q));
+        if (s < best) {
+            best = s;
+            best_a = p;
+            best_b = q;
+        }
+    };
+    for (uint32_t i = 0; i < 3; ++i) consider(av[i], closest_on_triangle(av[i], bv[0], bv[1], bv[2]));
+    for (uint32_t i = 0; i < 3; ++i) consider(closest_on_triangle(bv[i], av[0], av[1], av[2]), bv[i]);
+    for (uint32_t i = 0; i < 3; ++i)
+        for (uint32_t j = 0; j < 3; ++j) {
+            V3<R> on_a, on_b;
+            closest_segments(av[i], av[(i + 1) % 3], bv[j], bv[(j + 1) % 3], on_a, on_b);
+            consider(on_a, on_b);
+        }
+}
+
+// math.slang:43-49
+template <class R> inline bool bounds_overlap(V3<R> alo, V3<R> ahi, V3<R> blo, V3<R> bhi) {
+    return alo.x <= bhi.x && ahi.x >= blo.x && alo.y <= bhi.y && ahi.y >= blo.y && alo.z <= bhi.z && ahi.z >= blo.z;
+}
+
+// geometry.slang:1107-1116
+template <class R> inline bool triangle_bounds_overlap(const V3<R> a[3], const V3<R> b[3], R margin) {
+    const V3<R> ex{margin, margin, margin};
+    const V3<R> alo = sub(vmin(a[0], vmin(a[1], a[2])), ex), ahi = add(vmax(a[0], vmax(a[1], a[2])), ex);
+    const V3<R> blo = vmin(b[0], vmin(b[1], b[2])), bhi = vmax(b[0], vmax(b[1], b[2]));
+    return bounds_overlap(alo, ahi, blo, bhi);
+}
+
+// math.slang:142-190: box bounds of a local AABB under a pose, grown by a
+// margin, unioned with the previous pose's when swept.
+template <class R> struct BoundsXf { V3<R> x, ax, ay, az; };
+template <class R> inline BoundsXf<R> bounds_xf(const State<R>& s) {
+    return {s.x, rotate(s.q, V3<R>{1, 0, 0}), rotate(s.q, V3<R>{0, 1, 0}), rotate(s.q, V3<R>{0, 0, 1})};
+}
+template <class R>
+inline void xf_bounds(V3<R> llo, V3<R> lhi, const BoundsXf<R>& t, R margin, V3<R>& lo, V3<R>& hi) {
+    const V3<R> c = mul(add(llo, lhi), R(0.5)), h = mul(sub(lhi, llo), R(0.5));
+    const V3<R> wc = add(t.x, add(mul(t.ax, c.x), add(mul(t.ay, c.y), mul(t.az, c.z))));
+    const V3<R> wh{ab(t.ax.x) * h.x + ab(t.ay.x) * h.y + ab(t.az.x) * h.z,
+                   ab(t.ax.y) * h.x + ab(t.ay.y) * h.y + ab(t.az.y) * h.z,
+                   ab(t.ax.z) * h.x + ab(t.ay.z) * h.y + ab(t.az.z) * h.z};
+    const V3<R> ex{margin, margin, margin};
+    lo = sub(sub(wc, wh), ex);
+    hi = add(add(wc, wh), ex);
+}
+template <class R>
+inline void motion_bounds(V3<R> llo, V3<R> lhi, const BoundsXf<R>& prev, const BoundsXf<R>& cur, bool swept, R margin,
+                          V3<R>& lo, V3<R>& hi) {
+    xf_bounds(llo, lhi, cur, margin, lo, hi);
+    if (!swept) return;
+    V3<R> plo, phi;
+    xf_bounds(llo, lhi, prev, margin, plo, phi);
+    lo = vmin(lo, plo);
+    hi = vmax(hi, phi);
+}
+
+template <class R> inline V3<R> xf_point(const State<R>& s, V3<R> p) { return add(s.x, rotate(s.q, p)); }
+
+// geometry.slang:1272-1290
+template <class R> inline R normal_speed(const State<R>& a, const State<R>& b, V3<R> p, V3<R> n) {
+    const V3<R> va = add(a.v, cross(a.w, sub(p, a.x)));
+    const V3<R> vb = add(b.v, cross(b.w, sub(p, b.x)));
+    return dot(sub(va, vb), n);
+}
+template <class R>
+inline bool reaches_rest_offset(const State<R>& a, const State<R>& b, V3<R> p, V3<R> n, R dist, R rest, R dt) {
+    if (dist <= rest + R(1.0e-5)) return true;
+    const R speed = normal_speed(a, b, p, n);
+    if (speed > R(1.0e-5)) return false;
+    return -speed * dt + rest + R(1.0e-5) >= dist;
+}
+
+// geometry.slang:1292-1306
+template <class R> inline V3<R> advect_triangle_point(V3<R> p, const V3<R> from[3], const V3<R> to[3]) {
+    const V3<R> e1 = sub(from[1], from[0]), e2 = sub(from[2], from[0]);
+    const V3<R> nrm = cross(e1, e2);
+    const R sq = len2(nrm);
+    if (sq <= R(1.0e-20)) return to[0];
+    const V3<R> rel = sub(p, from[0]);
+    const R v = dot(cross(rel, e2), nrm) / sq;
+    const R w2 = dot(cross(e1, rel), nrm) / sq;
+    return add(to[0], add(mul(sub(to[1], to[0]), v), mul(sub(to[2], to[0]), w2)));
+}
+
+// geometry.slang:1308-1322: the certified outward direction carried to the
+// posed triangle (unit for a certified face, quarter length for an interior
+// open-surface face, zero when uncertified).
+template <class R> inline V3<R> shell_outward(const Mesh<R>& m, uint32_t t, V3<R> a, V3<R> b, V3<R> c) {
+    if (m.shell.empty()) return {};
+    const V3<R> out = m.shell[t];
+    const R sq = len2(out);
+    if (sq < R(0.01)) return {};
+    const V3<R> la = m.verts[m.idx[3 * t]], lb = m.verts[m.idx[3 * t + 1]], lc = m.verts[m.idx[3 * t + 2]];
+    const R sign = dot(cross(sub(lb, la), sub(lc, la)), out) >= R(0) ? R(1) : R(-1);
+    return mul(normalized_or(cross(sub(b, a), sub(c, a)), V3<R>{}), sign * (sq > R(0.5) ? R(1) : R(0.25)));
+}
+
+// geometry.slang:1324-1337
+template <class R> inline bool shell_contact_facing(V3<R> n, V3<R> oa, V3<R> ob) {
+    const R sa = len2(oa), sb = len2(ob);
+    return (sa < R(0.01) || (sa > R(0.5) ? dot(n, oa) < R(-1.0e-3) : ab(dot(n, oa)) > R(2.5e-4))) &&
+           (sb < R(0.01) || (sb > R(0.5) ? dot(n, ob) > R(1.0e-3) : ab(dot(n, ob)) > R(2.5e-4)));
+}
+
+// geometry.slang:1339-1357 (every plane of a convex mesh; its deduplicated
+// plane list gives the same answer)
+template <class R> inline bool point_inside_convex(const Mesh<R>& m, const State<R>& s, V3<R> p) {
+    if (!m.convex) return false;
+    const V3<R> l = inv_rotate(s.q, sub(p, s.x));
+    for (const auto& pl : m.planes)
+        if (dot(pl.n, l) > pl.d + R(1.0e-5)) return false;
+    return true;
+}
+
+// geometry.slang:1855-1908
+template <class R>
+inline V3<R> triangle_feature_normal(const V3<R> a[3], const V3<R> b[3], V3<R> pa, V3<R> pb, V3<R> fallback) {
+    const V3<R> delta = sub(pa, pb);
+    V3<R> nrm = normalized_or(delta, fallback);
+    const V3<R> faces[2] = {normalized_or(cross(sub(a[1], a[0]), sub(a[2], a[0])), nrm),
+                            normalized_or(cross(sub(b[1], b[0]), sub(b[2], b[0])), nrm)};
+    const V3<R>* tri[2] = {a, b};
+    const V3<R> pts[2] = {pa, pb};
+    R align_best = R(-1);
+    V3<R> interior_n{};
+    for (uint32_t side = 0; side < 2; ++side) {
+        const V3<R>* v = tri[side];
+        const V3<R> raw = cross(sub(v[1], v[0]), sub(v[2], v[0]));
+        const R tol = R(1.0e-5) * len2(raw);
+        bool interior = tol > R(0);
+        for (uint32_t e = 0; e < 3; ++e)
+            interior = interior && dot(cross(sub(v[(e + 1) % 3], v[e]), sub(pts[side], v[e])), raw) > tol;
+        const R align = ab(dot(faces[side], nrm));
+        if (interior && align > align_best) {
+            align_best = align;
+            const R proj = dot(delta, faces[side]);
+            const R dir = ab(proj) > kEps<R>() ? proj : dot(fallback, faces[side]);
+            interior_n = dir >= R(0) ? faces[side] : mul(faces[side], R(-1));
+        }
+    }
+    if (align_best >= R(0)) return interior_n;
+    R best_err = R(4) * kEps<R>() * kEps<R>();
+    if (len2(delta) > kEps<R>() * kEps<R>())
+        for (uint32_t side = 0; side < 2; ++side) {
+            const R proj = dot(delta, faces[side]);
+            const R err = len2(sub(delta, mul(faces[side], proj)));
+            if (err < best_err) {
+                best_err = err;
+                nrm = proj >= R(0) ? faces[side] : mul(faces[side], R(-1));
+            }
+        }
+    return nrm;
+}
+
+// geometry.slang:1359-1584: contacts of triangle range [af, af+ac) of the
+// body against [bf, bf+bc) of the collider at the current poses.
+template <class R>
+inline void collide_triangle_ranges(const Mesh<R>& am, const State<R>& aprev, const State<R>& as,
+                                    const HingeFrame<R>& ah, uint32_t af, uint32_t ac, const Mesh<R>& bm,
+                                    const State<R>& bprev, const State<R>& bs, const HingeFrame<R>& bh, uint32_t bf,
+                                    uint32_t bc, R margin, R dt, Manifold<R>& out) {
+    if (guided_pair(ah, bh)) return;
+    const R rest = mn(margin, R(1.0e-3));
+    const bool interior_a = ah.static_body && point_inside_convex(am, aprev, bprev.x);
+    const bool interior_b = bh.static_body && point_inside_convex(bm, bprev, aprev.x);
+    const uint32_t a_tris = uint32_t(am.idx.size() / 3), b_tris = uint32_t(bm.idx.size() / 3);
+    for (uint32_t i = 0; i < ac; ++i) {
+        const uint32_t at = af + i;
+        if (at >= a_tris) break;
+        V3<R> A[3];
+        for (uint32_t k = 0; k < 3; ++k) A[k] = xf_point(as, am.verts[am.idx[3 * at + k]]);
+        for (uint32_t j = 0; j < bc; ++j) {
+            const uint32_t bt = bf + j;
+            if (bt >= b_tris) break;
+            V3<R> B[3];
+            for (uint32_t k = 0; k < 3; ++k) B[k] = xf_point(bs, bm.verts[bm.idx[3 * bt + k]]);
+            if (!triangle_bounds_overlap(A, B, margin)) continue;
+            const V3<R> out_a = shell_outward(am, at, A[0], A[1], A[2]);
+            const V3<R> out_b = shell_outward(bm, bt, B[0], B[1], B[2]);
+            const V3<R> c_out_a = ah.static_body && interior_a ? V3<R>{} : out_a;
+            const V3<R> c_out_b = bh.static_body && interior_b ? V3<R>{} : out_b;
+            if (dot(out_a, out_b) > R(0.9999)) continue;
+            V3<R> pa, pb;
+            closest_triangle_pair(A, B, pa, pb);
+            const V3<R> delta = sub(pa, pb);
+            const R sq = len2(delta);
+            if (sq > margin * margin) continue;
+            const V3<R> cn = normalized_or(cross(sub(B[1], B[0]), sub(B[2], B[0])), V3<R>{0, 1, 0});
+            V3<R> fallback = dot(cn, sub(ah.reference, pb)) >= R(0) ? cn : mul(cn, R(-1));
+            if (len2(c_out_b) > R(0.5)) fallback = c_out_b;
+            const R dist = std::sqrt(mx(sq, R(0)));
+            const V3<R> point = mul(add(pa, pb), R(0.5));
+            const V3<R> proj = sub(pa, mul(cn, dot(sub(pa, B[0]), cn)));
+            const bool on_face = len2(sub(proj, closest_on_triangle(proj, B[0], B[1], B[2]))) <= R(1.0e-10);
+            const V3<R> nrm = (dist <= R(1.0e-5) || on_face) ? fallback : normalized_or(delta, fallback);
+            if (on_face && len2(out_a) < R(0.01) && len2(out_b) > R(0.5) && bm.convex) {
+                const V3<R> face_a = normalized_or(cross(sub(A[1], A[0]), sub(A[2], A[0])), V3<R>{});
+                if (ab(dot(face_a, nrm)) < R(1.0e-3)) {
+                    const R depth = mx(R(0), -mn(dot(sub(A[0], B[0]), nrm),
+                                                 mn(dot(sub(A[1], B[0]), nrm), dot(sub(A[2], B[0]), nrm))));
+                    const V3<R> laxis = inv_rotate(bs.q, face_a);
+                    const R off = dot(sub(bs.x, A[0]), face_a);
+                    R lo = R(3.402823466e38), hi = R(-3.402823466e38);
+                    for (const auto& v : bm.verts) {
+                        const R pr = dot(v, laxis) + off;
+                        lo = mn(lo, pr);
+                        hi = mx(hi, pr);
+                    }
+                    const R alt = mx(R(0), mn(-lo, hi));
+                    if (alt + R(1.0e-5) < depth) continue;
+                }
+            }
+            const R separation = on_face && len2(c_out_b) > R(0.5) ? dot(delta, nrm) : dist;
+            if (!reaches_rest_offset(as, bs, point, nrm, separation, rest, dt)) continue;
+            Contact<R> c{};
+            c.normal = nrm;
+            c.point = point;
+            c.penetration = rest - separation + R(1.0e-5);
+            bool recovered = false;
+            if (!am.convex && !bm.convex && dist <= R(1.0e-5)) {
+                V3<R> oA[3], oB[3];
+                for (uint32_t k = 0; k < 3; ++k) {
+                    oA[k] = xf_point(aprev, am.verts[am.idx[3 * at + k]]);
+                    oB[k] = xf_point(bprev, bm.verts[bm.idx[3 * bt + k]]);
+                }
+                V3<R> opa, opb;
+                closest_triangle_pair(oA, oB, opa, opb);
+                V3<R> od = sub(opa, opb);
+                if (len2(od) > R(1.0e-10)) {
+                    V3<R> iA[3], iB[3];
+                    R low = 0, high = 1;
+                    const R gap = mn(rest, R(0.5) * std::sqrt(len2(od)));
+                    for (uint32_t it = 0; it < 10; ++it) {
+                        const R time = R(0.5) * (low + high);
+                        for (uint32_t k = 0; k < 3; ++k) {
+                            iA[k] = add(oA[k], mul(sub(A[k], oA[k]), time));
+                            iB[k] = add(oB[k], mul(sub(B[k], oB[k]), time));
+                        }
+                        V3<R> p, q;
+                        closest_triangle_pair(iA, iB, p, q);
+                        if (len2(sub(p, q)) > gap * gap)
+                            low = time;
+                        else
+                            high = time;
+                    }
+                    for (uint32_t k = 0; k < 3; ++k) {
+                        iA[k] = add(oA[k], mul(sub(A[k], oA[k]), low));
+                        iB[k] = add(oB[k], mul(sub(B[k], oB[k]), low));
+                    }
+                    closest_triangle_pair(iA, iB, opa, opb);
+                    od = sub(opa, opb);
+                    c.normal = triangle_feature_normal(iA, iB, opa, opb, normalized_or(od, fallback));
+                    const V3<R> cpa = advect_triangle_point(opa, iA, A);
+                    const V3<R> cpb = advect_triangle_point(opb, iB, B);
+                    c.point = mul(add(cpa, cpb), R(0.5));
+                    c.penetration = rest - dot(sub(cpa, cpb), c.normal) + R(1.0e-5);
+                    recovered = true;
+                }
+            }
+            if (dist <= R(1.0e-5)) {
+                if (!recovered && (ah.fixed_member || bh.fixed_member || on_face)) {
+                    const R depth = mx(R(0), -mn(dot(sub(A[0], pb), nrm),
+                                                 mn(dot(sub(A[1], pb), nrm), dot(sub(A[2], pb), nrm))));
+                    c.penetration = mn(margin, depth + rest) + R(1.0e-5);
+                } else if (!recovered) {
+                    c.penetration = margin + R(1.0e-5);
+                }
+            }
+            if (!shell_contact_facing(c.normal, c_out_a, c_out_b)) continue;
+            c.impact_fraction = R(1);
+            c.init_speed = normal_speed(as, bs, c.point, c.normal);
+            add_contact(out, c, mx(R(2) * margin, R(1.0e-4)));
+        }
+    }
+}
+
+// geometry.slang:1586-1604
+template <class R>
+inline bool requires_swept(const State<R>& pa, const State<R>& a, const Mesh<R>& am, const State<R>& pb,
+                           const State<R>& b, const Mesh<R>& bm, R threshold) {
+    if (!am.convex || !bm.convex) threshold = mn(threshold, R(1.0e-3));
+    const V3<R> rel = sub(sub(a.x, pa.x), sub(b.x, pb.x));
+    return len(rel) + rotational_motion_bound(pa, a, am) + rotational_motion_bound(pb, b, bm) > threshold;
+}
+
+// geometry.slang:2156-2299 without the swept ranges: BVH pair traversal
+// (stack of 64 pairs, children pushed right before left), the unswept
+// triangle ranges at each overlapping leaf pair; a traversal that would
+// overflow the stack restarts as one pass over all triangle pairs.
+template <class R>
+inline void collide_meshes(const World<R>& w, uint32_t a, uint32_t b, const std::vector<State<R>>& prev,
+                           const std::vector<State<R>>& cur, const HingeFrame<R>& ah, const HingeFrame<R>& bh, R dt,
+                           Manifold<R>& out) {
+    out = Manifold<R>{};
+    const Mesh<R>& am = w.meshes[w.body[a].mesh];
+    const Mesh<R>& bm = w.meshes[w.body[b].mesh];
+    const R margin = R(w.body[a].margin) + R(w.body[b].margin);
+    const bool swept = guided_pair(ah, bh) || requires_swept(prev[a], cur[a], am, prev[b], cur[b], bm, margin);
+    const BoundsXf<R> pxa = swept ? bounds_xf(prev[a]) : BoundsXf<R>{}, pxb = swept ? bounds_xf(prev[b]) : BoundsXf<R>{};
+    const BoundsXf<R> xa = bounds_xf(cur[a]), xb = bounds_xf(cur[b]);
+    V3<R> alo, ahi, blo, bhi;
+    motion_bounds(am.lo, am.hi, pxa, xa, swept, margin, alo, ahi);
+    motion_bounds(bm.lo, bm.hi, pxb, xb, swept, R(0), blo, bhi);
+    if (!bounds_overlap(alo, ahi, blo, bhi)) return;
+    constexpr uint32_t kStack = 64;
+    uint32_t sa[kStack] = {}, sb[kStack] = {};
+    uint32_t size = 1;
+    bool overflow = am.bvh.empty() || bm.bvh.empty();
+    while (size > 0 && !overflow) {
+        --size;
+        const uint32_t na = sa[size], nb = sb[size];
+        const BvhNode<R>& A = am.bvh[na];
+        const BvhNode<R>& B = bm.bvh[nb];
+        motion_bounds(A.lo, A.hi, pxa, xa, swept, margin, alo, ahi);
+        motion_bounds(B.lo, B.hi, pxb, xb, swept, R(0), blo, bhi);
+        if (!bounds_overlap(alo, ahi, blo, bhi)) continue;
+        const bool la = A.count != 0, lb = B.count != 0;
+        if (la && lb) {
+            collide_triangle_ranges(am, prev[a], cur[a], ah, A.first, A.count, bm, prev[b], cur[b], bh, B.first,
+                                    B.count, margin, dt, out);
+            continue;
+        }
+        const uint32_t need = la || lb ? 2u : 4u;
+        if (size + need > kStack) {
+            overflow = true;
+            break;
+        }
+        if (la) {
+            sa[size] = na; sb[size++] = B.right;
+            sa[size] = na; sb[size++] = B.left;
+        } else if (lb) {
+            sa[size] = A.right; sb[size++] = nb;
+            sa[size] = A.left; sb[size++] = nb;
+        } else {
+            sa[size] = A.right; sb[size++] = B.right;
+            sa[size] = A.right; sb[size++] = B.left;
+            sa[size] = A.left; sb[size++] = B.right;
+            sa[size] = A.left; sb[size++] = B.left;
+        }
+    }
+    if (overflow) {
+        out = Manifold<R>{};
+        collide_triangle_ranges(am, prev[a], cur[a], ah, 0, uint32_t(am.idx.size() / 3), bm, prev[b], cur[b], bh, 0,
+                                uint32_t(bm.idx.size() / 3), margin, dt, out);
+    }
+}
+
+}  // namespace oracle

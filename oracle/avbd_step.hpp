@@ -3,6 +3,7 @@
 // the reference's order (production_realtime_backend.cu.inc:2642-2654 predict,
 // :2656+ spatial build, :7664-7866 emit_rigid_solve).
 #pragma once
+#include "avbd_mesh.hpp"
 #include "avbd_world.hpp"
 
 namespace oracle {
@@ -141,31 +142,31 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
     w.candidate_pairs = broadphase(w);
     st.candidate_pairs = uint32_t(w.candidate_pairs.size());
 
-    // ---- face narrowphase + finalize (geometry.slang:2741-2873)
+    // ---- face narrowphase, triangle-mesh narrowphase, finalize
+    // (geometry.slang:2741-2873, :2156-2299)
     w.active_pairs.clear();
     w.manifolds.clear();
+    const std::vector<HingeFrame<R>> frames = hinge_frames(w, pred);
     for (uint32_t code : w.candidate_pairs) {
         uint32_t a = code / n, b = code % n;
         const Mesh<R>& bm = w.meshes[w.body[a].mesh];
         const Mesh<R>& cm = w.meshes[w.body[b].mesh];
         R margin = R(w.body[a].margin) + R(w.body[b].margin);
         Manifold<R> m{};
-        if (face_capable(bm) && face_capable(cm)) {
+        bool face = false;
+        if (face_capable(bm) && face_capable(cm) && !guided_pair(frames[a], frames[b])) {
             R corr = correction_reach(w.body[a], bm) + correction_reach(w.body[b], cm);
             R moved = len(sub(sub(pred[a].x, prev[a].x), sub(pred[b].x, prev[b].x))) +
                       rotational_motion_bound(prev[a], pred[a], bm) + rotational_motion_bound(prev[b], pred[b], cm);
             bool swept = moved > margin;
-            bool face = false;
             if (swept) face = swept_face_manifold(prev[a], pred[a], bm, prev[b], pred[b], cm, margin, m);
             if (!face) {
                 face = face_manifold(pred[a], bm, pred[b], cm, margin, corr, m);
                 if (swept && m.count == 0) face = false;
             }
-            // A pair the face path declines goes to the general triangle-mesh
-            // path in the reference; that path is outside this restatement,
-            // so such a pair keeps an empty manifold.
-            if (!face) m = Manifold<R>{};
         }
+        // A pair the face path declines goes to the triangle-mesh path.
+        if (!face) collide_meshes(w, a, b, prev, pred, frames[a], frames[b], dt, m);
         if (m.count == 0) continue;
         bool persistent = face_capable(bm) && (!dynamic(w, b) || face_capable(cm));
         for (uint32_t p = 0; p < m.count; ++p) {

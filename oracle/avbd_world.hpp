@@ -77,10 +77,16 @@ struct StepStats {
 // ------------------------------------------------------------ world types
 template <class R> struct State { V3<R> x; Q4<R> q; V3<R> v, w; };
 template <class R> struct Plane { V3<R> n; R d{}; };
+template <class R> struct BvhNode {
+    V3<R> lo, hi;
+    uint32_t first{}, count{}, left{}, right{};  // count != 0: a leaf
+};
 template <class R> struct Mesh {
     std::vector<V3<R>> verts;
     std::vector<uint32_t> idx;      // BVH-reordered triangle order
     std::vector<Plane<R>> planes;   // one per triangle when convex
+    std::vector<BvhNode<R>> bvh;    // nodes in build (pre-)order, root first
+    std::vector<V3<R>> shell;       // certified outward normal per triangle, or empty
     bool convex{};
     V3<R> lo, hi, center;
     R radius{};
@@ -186,6 +192,9 @@ inline bool convex_planes(const std::vector<V3<R>>& v, const std::vector<uint32_
 
 // runtime_deformables.cu.inc:103-270: median-split BVH (<=4 triangles per
 // leaf) whose leaf order becomes the stored triangle order; bounds, sphere.
+template <class R>
+inline std::vector<V3<R>> shell_normals(const std::vector<V3<R>>& v, const std::vector<uint32_t>& idx);
+
 template <class R> inline Mesh<R> prepare_mesh(const float* verts, uint32_t nv, const uint32_t* idx, uint32_t ni) {
     Mesh<R> m;
     m.verts.resize(nv);
@@ -198,7 +207,7 @@ template <class R> inline Mesh<R> prepare_mesh(const float* verts, uint32_t nv, 
     auto centroid = [&](uint32_t t) {
         return mul(add(add(m.verts[idx[3 * t]], m.verts[idx[3 * t + 1]]), m.verts[idx[3 * t + 2]]), R(1) / R(3));
     };
-    std::function<void(uint32_t, uint32_t)> build = [&](uint32_t b, uint32_t e) {
+    std::function<uint32_t(uint32_t, uint32_t)> build = [&](uint32_t b, uint32_t e) -> uint32_t {
         V3<R> lo{R(3.402823466e38), R(3.402823466e38), R(3.402823466e38)};
         V3<R> hi = mul(lo, R(-1));
         for (uint32_t i = b; i < e; ++i)
@@ -206,7 +215,13 @@ template <class R> inline Mesh<R> prepare_mesh(const float* verts, uint32_t nv, 
                 lo = vmin(lo, m.verts[idx[3 * order[i] + c]]);
                 hi = vmax(hi, m.verts[idx[3 * order[i] + c]]);
             }
-        if (e - b <= 4) return;
+        const uint32_t node = uint32_t(m.bvh.size());
+        m.bvh.push_back(BvhNode<R>{lo, hi, 0, 0, 0, 0});
+        if (e - b <= 4) {
+            m.bvh[node].first = b;
+            m.bvh[node].count = e - b;
+            return node;
+        }
         V3<R> ext = sub(hi, lo);
         unsigned axis = ext.x >= ext.y && ext.x >= ext.z ? 0 : (ext.y >= ext.z ? 1 : 2);
         std::stable_sort(order.begin() + b, order.begin() + e, [&](uint32_t p, uint32_t q) {
@@ -214,14 +229,18 @@ template <class R> inline Mesh<R> prepare_mesh(const float* verts, uint32_t nv, 
             return fp < fq || (fp == fq && p < q);
         });
         uint32_t mid = b + (e - b) / 2;
-        build(b, mid);
-        build(mid, e);
+        const uint32_t left = build(b, mid);
+        const uint32_t right = build(mid, e);
+        m.bvh[node].left = left;
+        m.bvh[node].right = right;
+        return node;
     };
-    build(0, nt);
+    if (nt) build(0, nt);
     m.idx.resize(ni);
     for (uint32_t t = 0; t < nt; ++t)
         for (uint32_t c = 0; c < 3; ++c) m.idx[3 * t + c] = idx[3 * order[t] + c];
     m.convex = convex_planes(m.verts, m.idx, m.planes);
+    m.shell = shell_normals(m.verts, m.idx);
     m.center = mul(add(m.lo, m.hi), R(0.5));
     R r2 = 0;
     for (auto& p : m.verts) r2 = std::max(r2, len2(sub(p, m.center)));
@@ -322,6 +341,122 @@ template <class R> inline State<R> integrate(const World<R>& w, uint32_t i, V3<R
 }
 
 // geometry.slang:513-522
+// runtime_domains.cu.inc:1111-1235: a certified outward normal per triangle.
+// Triangles are grouped into components through shared (exactly welded)
+// positions; a closed convex component takes its planes' normals; a closed,
+// consistently wound component takes its winding normal signed by its volume;
+// an open component certifies a triangle only when the whole component lies
+// on one side of it (then the outward side), marks an interior triangle of an
+// open surface with a quarter-length normal and leaves boundary triangles
+// unrestricted (zero). Empty when no triangle got a normal.
+template <class R>
+inline std::vector<V3<R>> shell_normals(const std::vector<V3<R>>& v, const std::vector<uint32_t>& idx) {
+    const uint32_t nv = uint32_t(v.size()), nt = uint32_t(idx.size() / 3);
+    std::map<std::array<R, 3>, uint32_t> weld;
+    std::vector<uint32_t> remap(nv), parent(nv);
+    for (uint32_t i = 0; i < nv; ++i) {
+        remap[i] = weld.emplace(std::array<R, 3>{v[i].x, v[i].y, v[i].z}, i).first->second;
+        parent[i] = i;
+    }
+    auto root = [&](uint32_t i) {
+        while (parent[i] != i) {
+            parent[i] = parent[parent[i]];
+            i = parent[i];
+        }
+        return i;
+    };
+    for (uint32_t t = 0; t < nt; ++t)
+        for (uint32_t c = 1; c < 3; ++c) {
+            const uint32_t a = root(remap[idx[3 * t]]), b = root(remap[idx[3 * t + c]]);
+            parent[b] = a;
+        }
+    std::map<uint32_t, std::vector<uint32_t>> comps;
+    for (uint32_t t = 0; t < nt; ++t) comps[root(remap[idx[3 * t]])].push_back(t);
+    std::vector<V3<R>> normals(nt);
+    bool found = false;
+    for (const auto& kv : comps) {
+        const std::vector<uint32_t>& tris = kv.second;
+        std::map<uint32_t, uint32_t> local;
+        std::vector<V3<R>> pts;
+        std::vector<uint32_t> faces;
+        for (uint32_t t : tris)
+            for (uint32_t c = 0; c < 3; ++c) {
+                const uint32_t vert = remap[idx[3 * t + c]];
+                auto ins = local.emplace(vert, uint32_t(pts.size()));
+                if (ins.second) pts.push_back(v[vert]);
+                faces.push_back(ins.first->second);
+            }
+        std::vector<Plane<R>> planes;
+        if (convex_planes(pts, faces, planes)) {
+            found = true;
+            for (size_t i = 0; i < tris.size(); ++i) normals[tris[i]] = planes[i].n;
+            continue;
+        }
+        // Closed and consistently wound: every edge used twice, in opposite
+        // directions; the signed volume fixes the outward sign.
+        std::map<std::pair<uint32_t, uint32_t>, std::pair<unsigned, int>> edges;
+        double volume = 0.0;
+        for (size_t f = 0; f < faces.size(); f += 3) {
+            for (size_t c = 0; c < 3; ++c) {
+                const uint32_t a = faces[f + c], b = faces[f + (c + 1) % 3];
+                auto& e = edges[{std::min(a, b), std::max(a, b)}];
+                ++e.first;
+                e.second += a < b ? 1 : -1;
+            }
+            double q[3][3];
+            for (size_t c = 0; c < 3; ++c) {
+                const V3<R> p = pts[faces[f + c]];
+                q[c][0] = double(p.x) - double(pts[0].x);
+                q[c][1] = double(p.y) - double(pts[0].y);
+                q[c][2] = double(p.z) - double(pts[0].z);
+            }
+            volume += q[0][0] * (q[1][1] * q[2][2] - q[1][2] * q[2][1]) +
+                      q[0][1] * (q[1][2] * q[2][0] - q[1][0] * q[2][2]) +
+                      q[0][2] * (q[1][0] * q[2][1] - q[1][1] * q[2][0]);
+        }
+        bool closed = volume != 0.0 && std::isfinite(volume);
+        for (const auto& e : edges) closed = closed && e.second.first == 2u && e.second.second == 0;
+        if (!closed) {
+            R scale = 0;
+            for (const auto& p : pts) scale = std::max(scale, len(sub(p, pts[0])));
+            const R tol = std::max(R(1.0e-7), scale * R(1.0e-5));
+            for (size_t i = 0; i < tris.size(); ++i) {
+                const V3<R> a = pts[faces[3 * i]];
+                const V3<R> nrm =
+                    normalized_or(cross(sub(pts[faces[3 * i + 1]], a), sub(pts[faces[3 * i + 2]], a)), V3<R>{});
+                R lo = 0, hi = 0;
+                for (const auto& p : pts) {
+                    const R dist = dot(nrm, sub(p, a));
+                    lo = std::min(lo, dist);
+                    hi = std::max(hi, dist);
+                }
+                if (hi <= tol && lo < -tol) {
+                    normals[tris[i]] = nrm;
+                } else if (lo >= -tol && hi > tol) {
+                    normals[tris[i]] = mul(nrm, R(-1));
+                } else {
+                    bool interior = true;
+                    for (size_t c = 0; c < 3; ++c) {
+                        const uint32_t f0 = faces[3 * i + c], f1 = faces[3 * i + (c + 1) % 3];
+                        const auto& e = edges.at({std::min(f0, f1), std::max(f0, f1)});
+                        interior = interior && e.first == 2u && e.second == 0;
+                    }
+                    if (!interior) continue;
+                    normals[tris[i]] = mul(nrm, R(0.25));
+                }
+                found = true;
+            }
+            continue;
+        }
+        found = true;
+        for (size_t i = 0; i < tris.size(); ++i) {
+            const V3<R> a = pts[faces[3 * i]], b = pts[faces[3 * i + 1]], c = pts[faces[3 * i + 2]];
+            normals[tris[i]] = mul(normalized_or(cross(sub(b, a), sub(c, a)), V3<R>{}), volume > 0.0 ? R(1) : R(-1));
+        }
+    }
+    return found ? normals : std::vector<V3<R>>{};
+}
+
 template <class R> inline R correction_reach(const BodyDesc& b, const Mesh<R>& m) {
     if (b.motion != kDynamic) return R(0);
     V3<R> e = sub(m.hi, m.lo);

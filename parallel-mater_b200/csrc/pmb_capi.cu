@@ -176,6 +176,7 @@ void enqueue_step(pmb_world* w, const StepParams& sp) {
     launch_integrate(d, sp, s, w->out);
     set_phase(kPhIndex);
     launch_broadphase(d, s);  // switches to the candidate phase for the query
+    launch_hinge_frames(d, s);
     launch_narrowphase(d, sp, s);
     set_phase(kPhDomain);
     launch_prepare(d, sp, s);
@@ -265,12 +266,20 @@ void fill_stats(const Counters& c, pmb_step_stats* s) {
     s->residual_max = c.residual_max;
 }
 
+// The float whose bits are u (index fields packed into float4 records).
+float host_bits(uint32_t u) {
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
 struct Sizes {
     uint32_t n, nm, nj, scenes;
     size_t verts, planes, dis, hinges, hinge_segs;
     uint32_t cap_cand, cap_pair, cap_contact;
     uint32_t events;
     size_t fixed;  // fixed collision-disabling joints
+    size_t bvh_nodes, shell_normals;
 };
 struct Extra {
     float4 *lo, *hi, *sph;  // mesh bounds, read once at creation
@@ -298,6 +307,10 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     ALLOC(d.warm_table, 2 * cap_contact);
     ALLOCP(d.m_vo, nm); ALLOCP(d.m_vc, nm); ALLOCP(d.m_to, nm); ALLOCP(d.m_tc, nm); ALLOCP(d.m_convex, nm);
     ALLOCP(d.m_verts, z.verts); ALLOCP(d.m_planes, z.planes);
+    ALLOCP(d.m_solid, nm); ALLOCP(d.m_bo, nm); ALLOCP(d.m_so, nm); ALLOCP(d.m_lo, nm); ALLOCP(d.m_hi, nm);
+    ALLOCP(d.m_bvh, 3 * z.bvh_nodes); ALLOCP(d.m_shell, z.shell_normals);
+    ALLOCP(d.jb_off, nj ? size_t(n) + 1 : 0); ALLOCP(d.jb_list, 2 * size_t(nj)); ALLOC(d.frame, nj ? size_t(n) : 0);
+    ALLOC(d.np_mesh, cap_cand);
     ALLOC(d.dxl, n); ALLOC(d.dxa, n); ALLOC(d.dq, n); ALLOC(d.inA, n); ALLOC(d.inB, n);
     ALLOCS(d.prev_vel, n); ALLOCS(d.color, n);
     ALLOC(d.parent, n); ALLOC(d.impact, n); ALLOC(d.anchored, n); ALLOC(d.mean, n); ALLOC(d.island_end, n);
@@ -449,8 +462,8 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     d.grid_size = next_pow2(std::max(2u * n, 1024u));
 
     // ---- meshes (host preparation, then upload)
-    std::vector<uint32_t> m_vo(nm), m_vc(nm), m_to(nm), m_tc(nm), m_convex(nm);
-    std::vector<float4> verts, planes, mlo(nm), mhi(nm), msph(nm);
+    std::vector<uint32_t> m_vo(nm), m_vc(nm), m_to(nm), m_tc(nm), m_convex(nm), m_solid(nm), m_bo(nm), m_so(nm);
+    std::vector<float4> verts, planes, mlo(nm), mhi(nm), msph(nm), bvh, shell;
     for (uint32_t m = 0; m < nm; ++m) {
         const uint32_t v0 = desc->vertex_offsets[m], v1 = desc->vertex_offsets[m + 1];
         const uint32_t i0 = desc->index_offsets[m], i1 = desc->index_offsets[m + 1];
@@ -472,6 +485,15 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
         m_to[m] = uint32_t(planes.size());
         m_tc[m] = nt;
         m_convex[m] = pm.convex && (i1 - i0) <= 96 ? 1u : 0u;
+        m_solid[m] = pm.convex ? 1u : 0u;
+        m_bo[m] = uint32_t(bvh.size() / 3);
+        for (const BvhNodeHost& nd : pm.bvh) {
+            bvh.push_back(make_float4(nd.lo[0], nd.lo[1], nd.lo[2], host_bits(nd.first)));
+            bvh.push_back(make_float4(nd.hi[0], nd.hi[1], nd.hi[2], host_bits(nd.count)));
+            bvh.push_back(make_float4(host_bits(nd.left), host_bits(nd.right), 0, 0));
+        }
+        m_so[m] = pm.shell.empty() ? kInvalid : uint32_t(shell.size());
+        for (const auto& sn : pm.shell) shell.push_back(make_float4(sn[0], sn[1], sn[2], 0));
         for (uint32_t t = 0; t < nt; ++t)
             planes.push_back(pm.convex ? make_float4(pm.planes[t][0], pm.planes[t][1], pm.planes[t][2], pm.planes[t][3])
                                        : make_float4(0, 0, 0, 0));
@@ -537,7 +559,7 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     d.event_capacity = desc->event_capacity;
     const Sizes z{n, nm, nj, ns, verts.size(), planes.size(), dis_keys.size(), hinge_list.size(),
                   hinge_seg.size() - 1, d.cap_cand, d.cap_pair, d.cap_contact, desc->event_capacity,
-                  fixed_list.size()};
+                  fixed_list.size(), bvh.size() / 3, shell.size()};
     if (w->arena[kPersistent]) {
         // Bound memory must hold the whole layout before anything is carved.
         pmb_world probe;
@@ -620,6 +642,31 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
         up(d.dis_joint, dis_joint.data(), 4 * dis_joint.size());
     }
     if (!fixed_list.empty()) up(d.fixed_list, fixed_list.data(), 4 * fixed_list.size());
+    up(d.m_solid, m_solid.data(), 4 * size_t(nm));
+    up(d.m_bo, m_bo.data(), 4 * size_t(nm));
+    up(d.m_so, m_so.data(), 4 * size_t(nm));
+    up(d.m_lo, mlo.data(), 16 * size_t(nm));
+    up(d.m_hi, mhi.data(), 16 * size_t(nm));
+    if (!bvh.empty()) up(d.m_bvh, bvh.data(), 16 * bvh.size());
+    if (!shell.empty()) up(d.m_shell, shell.data(), 16 * shell.size());
+    if (nj) {
+        // Each body's joints in ascending index (a joint on one body twice
+        // is listed once), for the per-tick hinge contact frames.
+        std::vector<uint32_t> jb_off(n + 1, 0), jb_list;
+        std::vector<std::vector<uint32_t>> by_body(n);
+        for (uint32_t j = 0; j < nj; ++j) {
+            const pmb_joint& o = desc->joints[j];
+            if (o.body_a < n) by_body[o.body_a].push_back(j);
+            if (o.body_b < n && o.body_b != o.body_a) by_body[o.body_b].push_back(j);
+        }
+        for (uint32_t i = 0; i < n; ++i) {
+            jb_off[i] = uint32_t(jb_list.size());
+            jb_list.insert(jb_list.end(), by_body[i].begin(), by_body[i].end());
+        }
+        jb_off[n] = uint32_t(jb_list.size());
+        up(d.jb_off, jb_off.data(), 4 * size_t(n + 1));
+        if (!jb_list.empty()) up(d.jb_list, jb_list.data(), 4 * jb_list.size());
+    }
     std::vector<uint32_t> colors(n, kInvalid);
     up(d.color, colors.data(), 4 * n);
     launch_body_constants(d, dlo, dhi, dsph, s);
@@ -1068,7 +1115,9 @@ int pmb_world_memory_requirements(const pmb_world_capacity* c, uint64_t* persist
                   c->pair_capacity ? c->pair_capacity : 24u * n + 1024u,
                   c->contact_capacity ? c->contact_capacity : 64u * n + 4096u,
                   c->event_capacity,
-                  size_t(c->joint_count)};
+                  size_t(c->joint_count),
+                  2 * size_t(c->mesh_triangle_count) + std::max(1u, c->mesh_count),
+                  size_t(c->mesh_triangle_count)};
     Extra ex{};
     allocate_world(&probe, probe.d, z, ex);
     *persistent = probe.arena_used[kPersistent];

@@ -6,8 +6,9 @@
 // closed-convex-plane certificate of runtime_domains.cu.inc:1061-1108 (weld
 // exact duplicate positions, every welded edge used twice, one outward plane
 // per triangle, every vertex within tolerance behind it); AABB and bounding
-// sphere about the AABB centre. Compiled with -ffp-contract=off so the plane
-// arithmetic is the reference's FP32 sequence.
+// sphere about the AABB centre; the BVH nodes; the certified outward shell
+// normals of runtime_domains.cu.inc:1111-1235. Compiled with
+// -ffp-contract=off so the plane arithmetic is the reference's FP32 sequence.
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -72,6 +73,119 @@ bool convex_planes(const std::vector<F3>& v, const std::vector<uint32_t>& idx, s
     return true;
 }
 
+// A certified outward normal per triangle (zero where uncertified, a quarter
+// length for an interior triangle of an open surface). Triangles form
+// components through exactly welded positions; a closed convex component
+// takes its planes' normals; a closed, consistently wound one its winding
+// normals signed by its volume; an open one certifies a triangle with the
+// whole component on one side of it. Empty when nothing was certified.
+std::vector<std::array<float, 3>> shell_normals(const std::vector<F3>& v, const std::vector<uint32_t>& idx) {
+    const uint32_t nv = uint32_t(v.size()), nt = uint32_t(idx.size() / 3);
+    std::map<std::array<float, 3>, uint32_t> weld;
+    std::vector<uint32_t> remap(nv), parent(nv);
+    for (uint32_t i = 0; i < nv; ++i) {
+        remap[i] = weld.emplace(std::array<float, 3>{v[i].x, v[i].y, v[i].z}, i).first->second;
+        parent[i] = i;
+    }
+    auto root = [&](uint32_t i) {
+        while (parent[i] != i) {
+            parent[i] = parent[parent[i]];
+            i = parent[i];
+        }
+        return i;
+    };
+    for (uint32_t t = 0; t < nt; ++t)
+        for (uint32_t c = 1; c < 3; ++c) {
+            const uint32_t a = root(remap[idx[3 * t]]), b = root(remap[idx[3 * t + c]]);
+            parent[b] = a;
+        }
+    std::map<uint32_t, std::vector<uint32_t>> comps;
+    for (uint32_t t = 0; t < nt; ++t) comps[root(remap[idx[3 * t]])].push_back(t);
+    std::vector<std::array<float, 3>> normals(nt, std::array<float, 3>{0.0f, 0.0f, 0.0f});
+    bool found = false;
+    auto put = [&](uint32_t t, F3 n) { normals[t] = {n.x, n.y, n.z}; };
+    for (const auto& kv : comps) {
+        const std::vector<uint32_t>& tris = kv.second;
+        std::map<uint32_t, uint32_t> local;
+        std::vector<F3> pts;
+        std::vector<uint32_t> faces;
+        for (uint32_t t : tris)
+            for (uint32_t c = 0; c < 3; ++c) {
+                const uint32_t vert = remap[idx[3 * t + c]];
+                auto ins = local.emplace(vert, uint32_t(pts.size()));
+                if (ins.second) pts.push_back(v[vert]);
+                faces.push_back(ins.first->second);
+            }
+        std::vector<std::array<float, 4>> planes;
+        if (convex_planes(pts, faces, planes)) {
+            found = true;
+            for (size_t i = 0; i < tris.size(); ++i) put(tris[i], F3{planes[i][0], planes[i][1], planes[i][2]});
+            continue;
+        }
+        std::map<std::pair<uint32_t, uint32_t>, std::pair<unsigned, int>> edges;
+        double volume = 0.0;
+        for (size_t f = 0; f < faces.size(); f += 3) {
+            for (size_t c = 0; c < 3; ++c) {
+                const uint32_t a = faces[f + c], b = faces[f + (c + 1) % 3];
+                auto& e = edges[{std::min(a, b), std::max(a, b)}];
+                ++e.first;
+                e.second += a < b ? 1 : -1;
+            }
+            double q[3][3];
+            for (size_t c = 0; c < 3; ++c) {
+                const F3 p = pts[faces[f + c]];
+                q[c][0] = double(p.x) - pts[0].x;
+                q[c][1] = double(p.y) - pts[0].y;
+                q[c][2] = double(p.z) - pts[0].z;
+            }
+            volume += q[0][0] * (q[1][1] * q[2][2] - q[1][2] * q[2][1]) +
+                      q[0][1] * (q[1][2] * q[2][0] - q[1][0] * q[2][2]) +
+                      q[0][2] * (q[1][0] * q[2][1] - q[1][1] * q[2][0]);
+        }
+        bool closed = volume != 0.0 && std::isfinite(volume);
+        for (const auto& e : edges) closed = closed && e.second.first == 2u && e.second.second == 0;
+        if (!closed) {
+            float scale = 0.0f;
+            for (const auto& p : pts) scale = std::max(scale, len(sub(p, pts[0])));
+            const float tol = std::max(1.0e-7f, scale * 1.0e-5f);
+            for (size_t i = 0; i < tris.size(); ++i) {
+                const F3 a = pts[faces[3 * i]];
+                const F3 nrm =
+                    normalized_or(cross(sub(pts[faces[3 * i + 1]], a), sub(pts[faces[3 * i + 2]], a)), F3{0, 0, 0});
+                float lo = 0.0f, hi = 0.0f;
+                for (const auto& p : pts) {
+                    const float dist = dot(nrm, sub(p, a));
+                    lo = std::min(lo, dist);
+                    hi = std::max(hi, dist);
+                }
+                if (hi <= tol && lo < -tol) {
+                    put(tris[i], nrm);
+                } else if (lo >= -tol && hi > tol) {
+                    put(tris[i], mul(nrm, -1.0f));
+                } else {
+                    bool interior = true;
+                    for (size_t c = 0; c < 3; ++c) {
+                        const uint32_t f0 = faces[3 * i + c], f1 = faces[3 * i + (c + 1) % 3];
+                        const auto& e = edges.at({std::min(f0, f1), std::max(f0, f1)});
+                        interior = interior && e.first == 2u && e.second == 0;
+                    }
+                    if (!interior) continue;
+                    put(tris[i], mul(nrm, 0.25f));
+                }
+                found = true;
+            }
+            continue;
+        }
+        found = true;
+        for (size_t i = 0; i < tris.size(); ++i) {
+            const F3 a = pts[faces[3 * i]], b = pts[faces[3 * i + 1]], c = pts[faces[3 * i + 2]];
+            put(tris[i], mul(normalized_or(cross(sub(b, a), sub(c, a)), F3{0, 0, 0}), volume > 0.0 ? 1.0f : -1.0f));
+        }
+    }
+    if (!found) normals.clear();
+    return normals;
+}
+
 }  // namespace
 
 PreparedMesh prepare_mesh(const float* verts, uint32_t nv, const uint32_t* idx, uint32_t ni) {
@@ -89,7 +203,7 @@ PreparedMesh prepare_mesh(const float* verts, uint32_t nv, const uint32_t* idx, 
     auto centroid = [&](uint32_t t) {
         return mul(add(add(v[idx[3 * t]], v[idx[3 * t + 1]]), v[idx[3 * t + 2]]), 1.0f / 3.0f);
     };
-    std::function<void(uint32_t, uint32_t)> build = [&](uint32_t b, uint32_t e) {
+    std::function<uint32_t(uint32_t, uint32_t)> build = [&](uint32_t b, uint32_t e) -> uint32_t {
         F3 nlo{3.402823466e38f, 3.402823466e38f, 3.402823466e38f};
         F3 nhi = mul(nlo, -1.0f);
         for (uint32_t i = b; i < e; ++i)
@@ -98,7 +212,13 @@ PreparedMesh prepare_mesh(const float* verts, uint32_t nv, const uint32_t* idx, 
                 nlo = {std::fmin(nlo.x, p.x), std::fmin(nlo.y, p.y), std::fmin(nlo.z, p.z)};
                 nhi = {std::fmax(nhi.x, p.x), std::fmax(nhi.y, p.y), std::fmax(nhi.z, p.z)};
             }
-        if (e - b <= 4) return;
+        const uint32_t node = uint32_t(m.bvh.size());
+        m.bvh.push_back(BvhNodeHost{{nlo.x, nlo.y, nlo.z}, {nhi.x, nhi.y, nhi.z}, 0, 0, 0, 0});
+        if (e - b <= 4) {
+            m.bvh[node].first = b;
+            m.bvh[node].count = e - b;
+            return node;
+        }
         F3 ext = sub(nhi, nlo);
         int axis = ext.x >= ext.y && ext.x >= ext.z ? 0 : (ext.y >= ext.z ? 1 : 2);
         std::stable_sort(order.begin() + b, order.begin() + e, [&](uint32_t p, uint32_t q) {
@@ -106,15 +226,19 @@ PreparedMesh prepare_mesh(const float* verts, uint32_t nv, const uint32_t* idx, 
             return fp < fq || (fp == fq && p < q);
         });
         uint32_t mid = b + (e - b) / 2;
-        build(b, mid);
-        build(mid, e);
+        const uint32_t left = build(b, mid);
+        const uint32_t right = build(mid, e);
+        m.bvh[node].left = left;
+        m.bvh[node].right = right;
+        return node;
     };
-    build(0, nt);
+    if (nt) build(0, nt);
     std::vector<uint32_t> re(ni);
     for (uint32_t t = 0; t < nt; ++t)
         for (uint32_t c = 0; c < 3; ++c) re[3 * t + c] = idx[3 * order[t] + c];
     m.indices = re;
     m.convex = convex_planes(v, re, m.planes);
+    m.shell = shell_normals(v, re);
     F3 center = mul(add(lo, hi), 0.5f);
     float r2 = 0;
     for (auto& p : v) r2 = std::max(r2, dot(sub(p, center), sub(p, center)));

@@ -1,0 +1,637 @@
+// SPDX-License-Identifier: MIT
+// Triangle-mesh narrowphase: the candidate pairs the convex face path does
+// not take (a mesh that is not convex or has more than 96 indices, or a
+// convex pair whose face manifold came out empty), as the reference's
+// rigid_collide_meshes (geometry.slang:2156-2299) runs them: a traversal of
+// the two meshes' BVHs in pairs, children pushed right before left on a
+// 64-entry stack (a deeper traversal restarts as one pass over all triangle
+// pairs), and at each overlapping pair of leaves the triangle-range contacts
+// of :1359-1584 -- closest points of the two triangles (:949-1105), the
+// certified shell normals that orient and filter them (:1308-1337), the
+// rest-offset reach test (:1272-1290), the intersection recovery of two
+// non-convex meshes (:1292-1306, :1855-1908) -- merged into at most eight
+// contacts (:1129-1220). The swept triangle ranges (:1921-2155) are not
+// built: a pair that needs continuous contact gets its end-pose contacts.
+//
+// One thread per pair on the path, which is rare: everything stays in
+// registers and local memory. Per-body hinge contact frames (:404-492) are
+// computed once per tick before the narrowphase; the face path uses them to
+// skip guided pairs (:373-377).
+#include "pmb_world.cuh"
+
+namespace pmb {
+
+namespace {
+
+constexpr uint32_t kStack = 64;
+
+struct MeshPose { V3 x; Q4 q; V3 v, w; };
+
+struct MeshMan {
+    uint32_t count;
+    V3 p[8], n[8];
+    float pen[8];
+};
+
+// geometry.slang:1129-1220, the unguided merge: a point within `spacing` of a
+// kept one replaces it when deeper; a ninth point replaces the shallowest.
+__device__ void mm_add(MeshMan& m, V3 p, V3 n, float pen, float spacing) {
+    const float s2 = spacing * spacing;
+    for (uint32_t i = 0; i < m.count; ++i)
+        if (len2(sub(m.p[i], p)) < s2) {
+            if (pen - m.pen[i] > 0.0f) {
+                m.p[i] = p;
+                m.n[i] = n;
+                m.pen[i] = pen;
+            }
+            return;
+        }
+    if (m.count < 8) {
+        m.p[m.count] = p;
+        m.n[m.count] = n;
+        m.pen[m.count] = pen;
+        ++m.count;
+        return;
+    }
+    uint32_t sh = 0;
+    for (uint32_t i = 1; i < m.count; ++i)
+        if (m.pen[i] < m.pen[sh]) sh = i;
+    if (pen > m.pen[sh]) {
+        m.p[sh] = p;
+        m.n[sh] = n;
+        m.pen[sh] = pen;
+    }
+}
+
+struct Tri { V3 v[3]; };
+
+__device__ __forceinline__ V3 xf(const MeshPose& s, V3 p) { return add(s.x, rotate(s.q, p)); }
+
+struct MeshView {
+    const float4* verts;
+    const float4* planes;  // nt planes, then nt packed triangles
+    const float4* bvh;
+    const float4* shell;   // nullptr: no certified normals
+    uint32_t nv, nt, nodes;
+    bool solid;
+    V3 lo, hi;
+};
+
+__device__ MeshView mesh_view(const Dev& d, uint32_t m) {
+    MeshView v;
+    v.verts = d.m_verts + d.m_vo[m];
+    v.planes = d.m_planes + d.m_to[m];
+    v.nv = d.m_vc[m];
+    v.nt = d.m_tc[m];
+    v.bvh = d.m_bvh + 3 * size_t(d.m_bo[m]);
+    v.nodes = v.nt ? 1u : 0u;  // non-zero: the mesh has a BVH (its root is node 0)
+    v.shell = d.m_so[m] == kInvalid ? nullptr : d.m_shell + d.m_so[m];
+    v.solid = d.m_solid[m] != 0;
+    v.lo = v3(d.m_lo[m]);
+    v.hi = v3(d.m_hi[m]);
+    return v;
+}
+
+__device__ __forceinline__ uint3 tri_index(const MeshView& m, uint32_t t) {
+    const float4 k = m.planes[m.nt + t];
+    return make_uint3(__float_as_uint(k.x), __float_as_uint(k.y), __float_as_uint(k.z));
+}
+__device__ __forceinline__ Tri posed_tri(const MeshView& m, uint32_t t, const MeshPose& s) {
+    const uint3 k = tri_index(m, t);
+    return {{xf(s, v3(m.verts[k.x])), xf(s, v3(m.verts[k.y])), xf(s, v3(m.verts[k.z]))}};
+}
+
+// geometry.slang:949-997
+__device__ void closest_segments(V3 p0, V3 p1, V3 q0, V3 q1, V3& on_p, V3& on_q) {
+    const V3 d0 = sub(p1, p0), d1 = sub(q1, q0), r = sub(p0, q0);
+    const float a = dot(d0, d0), e = dot(d1, d1);
+    float s = 0.0f, t = 0.0f;
+    if (a <= 1.0e-12f && e <= 1.0e-12f) {
+        on_p = p0;
+        on_q = q0;
+        return;
+    }
+    if (a <= 1.0e-12f) {
+        t = fclamp(dot(d1, r) / e, 0.0f, 1.0f);
+    } else {
+        const float c = dot(d0, r);
+        if (e <= 1.0e-12f) {
+            s = fclamp(-c / a, 0.0f, 1.0f);
+        } else {
+            const float b = dot(d0, d1), f = dot(d1, r);
+            const float den = a * e - b * b;
+            if (fab(den) > kEps * a * e) s = fclamp((b * f - c * e) / den, 0.0f, 1.0f);
+            t = (b * s + f) / e;
+            if (t < 0.0f) {
+                t = 0.0f;
+                s = fclamp(-c / a, 0.0f, 1.0f);
+            } else if (t > 1.0f) {
+                t = 1.0f;
+                s = fclamp((b - c) / a, 0.0f, 1.0f);
+            }
+        }
+    }
+    on_p = add(p0, mul(d0, s));
+    on_q = add(q0, mul(d1, t));
+}
+
+// geometry.slang:1000-1031
+__device__ V3 closest_on_triangle(V3 p, V3 a, V3 b, V3 c) {
+    const V3 ab = sub(b, a), ac = sub(c, a), ap = sub(p, a);
+    const float d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0.0f && d2 <= 0.0f) return a;
+    const V3 bp = sub(p, b);
+    const float d3 = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3 >= 0.0f && d4 <= d3) return b;
+    const float vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) return add(a, mul(ab, d1 / (d1 - d3)));
+    const V3 cp = sub(p, c);
+    const float d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= 0.0f && d5 <= d6) return c;
+    const float vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) return add(a, mul(ac, d2 / (d2 - d6)));
+    const float va = d3 * d6 - d5 * d4;
+    if (va <= 0.0f && d4 - d3 >= 0.0f && d5 - d6 >= 0.0f)
+        return add(b, mul(sub(c, b), (d4 - d3) / ((d4 - d3) + (d5 - d6))));
+    const V3 n = cross(ab, ac);
+    return sub(p, mul(n, dot(ap, n) / len2(n)));
+}
+
+// geometry.slang:1033-1055
+__device__ bool segment_hits_triangle(V3 p, V3 q, const Tri& t, V3& hit) {
+    hit = V3{0.0f, 0.0f, 0.0f};
+    const V3 n = cross(sub(t.v[1], t.v[0]), sub(t.v[2], t.v[0]));
+    const V3 dir = sub(q, p);
+    const float den = dot(n, dir);
+    if (len2(n) <= kEps * kEps || fab(den) <= kEps) return false;
+    const float amount = dot(n, sub(t.v[0], p)) / den;
+    if (amount < 0.0f || amount > 1.0f) return false;
+    hit = add(p, mul(dir, amount));
+    const float tol = -1.0e-5f * len2(n);
+    return dot(cross(sub(t.v[1], t.v[0]), sub(hit, t.v[0])), n) >= tol &&
+           dot(cross(sub(t.v[2], t.v[1]), sub(hit, t.v[1])), n) >= tol &&
+           dot(cross(sub(t.v[0], t.v[2]), sub(hit, t.v[2])), n) >= tol;
+}
+
+// geometry.slang:1057-1105
+__device__ void closest_triangle_pair(const Tri& A, const Tri& B, V3& best_a, V3& best_b) {
+    V3 hit;
+    for (uint32_t e = 0; e < 3; ++e)
+        if (segment_hits_triangle(A.v[e], A.v[(e + 1) % 3], B, hit)) {
+            best_a = best_b = hit;
+            return;
+        }
+    for (uint32_t e = 0; e < 3; ++e)
+        if (segment_hits_triangle(B.v[e], B.v[(e + 1) % 3], A, hit)) {
+            best_a = best_b = hit;
+            return;
+        }
+    float best = 3.402823466e+38f;
+    auto consider = [&](V3 p, V3 q) {
+        const float s = len2(sub(p, q));
+        if (s < best) {
+            best = s;
+            best_a = p;
+            best_b = q;
+        }
+    };
+    for (uint32_t i = 0; i < 3; ++i) consider(A.v[i], closest_on_triangle(A.v[i], B.v[0], B.v[1], B.v[2]));
+    for (uint32_t i = 0; i < 3; ++i) consider(closest_on_triangle(B.v[i], A.v[0], A.v[1], A.v[2]), B.v[i]);
+    for (uint32_t i = 0; i < 3; ++i)
+        for (uint32_t j = 0; j < 3; ++j) {
+            V3 on_a, on_b;
+            closest_segments(A.v[i], A.v[(i + 1) % 3], B.v[j], B.v[(j + 1) % 3], on_a, on_b);
+            consider(on_a, on_b);
+        }
+}
+
+__device__ __forceinline__ bool bounds_overlap(V3 alo, V3 ahi, V3 blo, V3 bhi) {
+    return alo.x <= bhi.x && ahi.x >= blo.x && alo.y <= bhi.y && ahi.y >= blo.y && alo.z <= bhi.z && ahi.z >= blo.z;
+}
+
+// math.slang:142-190
+struct BoundsXf { V3 x, ax, ay, az; };
+__device__ __forceinline__ BoundsXf bounds_xf(const MeshPose& s) {
+    return {s.x, rotate(s.q, V3{1.0f, 0.0f, 0.0f}), rotate(s.q, V3{0.0f, 1.0f, 0.0f}),
+            rotate(s.q, V3{0.0f, 0.0f, 1.0f})};
+}
+__device__ void xf_bounds(V3 llo, V3 lhi, const BoundsXf& t, float margin, V3& lo, V3& hi) {
+    const V3 c = mul(add(llo, lhi), 0.5f), h = mul(sub(lhi, llo), 0.5f);
+    const V3 wc = add(t.x, add(mul(t.ax, c.x), add(mul(t.ay, c.y), mul(t.az, c.z))));
+    const V3 wh{fab(t.ax.x) * h.x + fab(t.ay.x) * h.y + fab(t.az.x) * h.z,
+                fab(t.ax.y) * h.x + fab(t.ay.y) * h.y + fab(t.az.y) * h.z,
+                fab(t.ax.z) * h.x + fab(t.ay.z) * h.y + fab(t.az.z) * h.z};
+    const V3 ex{margin, margin, margin};
+    lo = sub(sub(wc, wh), ex);
+    hi = add(add(wc, wh), ex);
+}
+__device__ void motion_bounds(V3 llo, V3 lhi, const BoundsXf& prev, const BoundsXf& cur, bool swept, float margin,
+                              V3& lo, V3& hi) {
+    xf_bounds(llo, lhi, cur, margin, lo, hi);
+    if (!swept) return;
+    V3 plo, phi;
+    xf_bounds(llo, lhi, prev, margin, plo, phi);
+    lo = vmin(lo, plo);
+    hi = vmax(hi, phi);
+}
+
+// geometry.slang:1272-1290
+__device__ __forceinline__ float normal_speed(const MeshPose& a, const MeshPose& b, V3 p, V3 n) {
+    const V3 va = add(a.v, cross(a.w, sub(p, a.x)));
+    const V3 vb = add(b.v, cross(b.w, sub(p, b.x)));
+    return dot(sub(va, vb), n);
+}
+__device__ bool reaches_rest_offset(const MeshPose& a, const MeshPose& b, V3 p, V3 n, float dist, float rest,
+                                    float dt) {
+    if (dist <= rest + 1.0e-5f) return true;
+    const float speed = normal_speed(a, b, p, n);
+    if (speed > 1.0e-5f) return false;
+    return -speed * dt + rest + 1.0e-5f >= dist;
+}
+
+// geometry.slang:1292-1306
+__device__ V3 advect_triangle_point(V3 p, const Tri& from, const Tri& to) {
+    const V3 e1 = sub(from.v[1], from.v[0]), e2 = sub(from.v[2], from.v[0]);
+    const V3 n = cross(e1, e2);
+    const float sq = len2(n);
+    if (sq <= 1.0e-20f) return to.v[0];
+    const V3 rel = sub(p, from.v[0]);
+    const float v = dot(cross(rel, e2), n) / sq;
+    const float w = dot(cross(e1, rel), n) / sq;
+    return add(to.v[0], add(mul(sub(to.v[1], to.v[0]), v), mul(sub(to.v[2], to.v[0]), w)));
+}
+
+// geometry.slang:1308-1322
+__device__ V3 shell_outward(const MeshView& m, uint32_t t, const Tri& T) {
+    if (!m.shell) return V3{0.0f, 0.0f, 0.0f};
+    const V3 out = v3(m.shell[t]);
+    const float sq = len2(out);
+    if (sq < 0.01f) return V3{0.0f, 0.0f, 0.0f};
+    const uint3 k = tri_index(m, t);
+    const V3 la = v3(m.verts[k.x]), lb = v3(m.verts[k.y]), lc = v3(m.verts[k.z]);
+    const float sign = dot(cross(sub(lb, la), sub(lc, la)), out) >= 0.0f ? 1.0f : -1.0f;
+    return mul(normalized_or(cross(sub(T.v[1], T.v[0]), sub(T.v[2], T.v[0])), V3{0.0f, 0.0f, 0.0f}),
+               sign * (sq > 0.5f ? 1.0f : 0.25f));
+}
+
+// geometry.slang:1324-1337
+__device__ __forceinline__ bool shell_contact_facing(V3 n, V3 oa, V3 ob) {
+    const float sa = len2(oa), sb = len2(ob);
+    return (sa < 0.01f || (sa > 0.5f ? dot(n, oa) < -1.0e-3f : fab(dot(n, oa)) > 2.5e-4f)) &&
+           (sb < 0.01f || (sb > 0.5f ? dot(n, ob) > 1.0e-3f : fab(dot(n, ob)) > 2.5e-4f));
+}
+
+// geometry.slang:1339-1357 over every plane of a convex mesh.
+__device__ bool point_inside_convex(const MeshView& m, const MeshPose& s, V3 p) {
+    if (!m.solid) return false;
+    const V3 l = inv_rotate(s.q, sub(p, s.x));
+    for (uint32_t t = 0; t < m.nt; ++t) {
+        const float4 pl = m.planes[t];
+        if (dot(v3(pl), l) > pl.w + 1.0e-5f) return false;
+    }
+    return true;
+}
+
+// geometry.slang:1855-1908
+__device__ V3 triangle_feature_normal(const Tri& A, const Tri& B, V3 pa, V3 pb, V3 fallback) {
+    const V3 delta = sub(pa, pb);
+    V3 n = normalized_or(delta, fallback);
+    const V3 faces[2] = {normalized_or(cross(sub(A.v[1], A.v[0]), sub(A.v[2], A.v[0])), n),
+                         normalized_or(cross(sub(B.v[1], B.v[0]), sub(B.v[2], B.v[0])), n)};
+    const Tri* tri[2] = {&A, &B};
+    const V3 pts[2] = {pa, pb};
+    float align_best = -1.0f;
+    V3 interior_n{0.0f, 0.0f, 0.0f};
+    for (uint32_t side = 0; side < 2; ++side) {
+        const Tri& t = *tri[side];
+        const V3 raw = cross(sub(t.v[1], t.v[0]), sub(t.v[2], t.v[0]));
+        const float tol = 1.0e-5f * len2(raw);
+        bool interior = tol > 0.0f;
+        for (uint32_t e = 0; e < 3; ++e)
+            interior = interior && dot(cross(sub(t.v[(e + 1) % 3], t.v[e]), sub(pts[side], t.v[e])), raw) > tol;
+        const float align = fab(dot(faces[side], n));
+        if (interior && align > align_best) {
+            align_best = align;
+            const float proj = dot(delta, faces[side]);
+            const float dir = fab(proj) > kEps ? proj : dot(fallback, faces[side]);
+            interior_n = dir >= 0.0f ? faces[side] : mul(faces[side], -1.0f);
+        }
+    }
+    if (align_best >= 0.0f) return interior_n;
+    float best_err = 4.0f * kEps * kEps;
+    if (len2(delta) > kEps * kEps)
+        for (uint32_t side = 0; side < 2; ++side) {
+            const float proj = dot(delta, faces[side]);
+            const float err = len2(sub(delta, mul(faces[side], proj)));
+            if (err < best_err) {
+                best_err = err;
+                n = proj >= 0.0f ? faces[side] : mul(faces[side], -1.0f);
+            }
+        }
+    return n;
+}
+
+struct Frame {
+    V3 reference;
+    uint32_t flags;
+};
+
+__device__ __forceinline__ Frame frame_of(const Dev& d, uint32_t i) {
+    if (d.nj) {
+        const float4 f = d.frame[i];
+        return {v3(f), __float_as_uint(f.w)};
+    }
+    return {v3(d.tx[i]), d.motion[i] == kStatic ? kFrameStatic : 0u};
+}
+
+
+// geometry.slang:1359-1584
+__device__ void collide_ranges(const MeshView& am, const MeshPose& aprev, const MeshPose& as, const Frame& fa,
+                               uint32_t af, uint32_t ac, const MeshView& bm, const MeshPose& bprev,
+                               const MeshPose& bs, const Frame& fb, uint32_t bf, uint32_t bc, float margin, float dt,
+                               MeshMan& out) {
+    if (frames_guided(fa.flags, fb.flags)) return;
+    const float rest = fmn(margin, 1.0e-3f);
+    const bool a_static = (fa.flags & kFrameStatic) != 0, b_static = (fb.flags & kFrameStatic) != 0;
+    const bool interior_a = a_static && point_inside_convex(am, aprev, bprev.x);
+    const bool interior_b = b_static && point_inside_convex(bm, bprev, aprev.x);
+    for (uint32_t i = 0; i < ac; ++i) {
+        const uint32_t at = af + i;
+        if (at >= am.nt) break;
+        const Tri A = posed_tri(am, at, as);
+        for (uint32_t j = 0; j < bc; ++j) {
+            const uint32_t bt = bf + j;
+            if (bt >= bm.nt) break;
+            const Tri B = posed_tri(bm, bt, bs);
+            {
+                const V3 ex{margin, margin, margin};
+                const V3 alo = sub(vmin(A.v[0], vmin(A.v[1], A.v[2])), ex);
+                const V3 ahi = add(vmax(A.v[0], vmax(A.v[1], A.v[2])), ex);
+                const V3 blo = vmin(B.v[0], vmin(B.v[1], B.v[2])), bhi = vmax(B.v[0], vmax(B.v[1], B.v[2]));
+                if (!bounds_overlap(alo, ahi, blo, bhi)) continue;
+            }
+            const V3 out_a = shell_outward(am, at, A), out_b = shell_outward(bm, bt, B);
+            const V3 zero{0.0f, 0.0f, 0.0f};
+            const V3 c_out_a = a_static && interior_a ? zero : out_a;
+            const V3 c_out_b = b_static && interior_b ? zero : out_b;
+            if (dot(out_a, out_b) > 0.9999f) continue;
+            V3 pa, pb;
+            closest_triangle_pair(A, B, pa, pb);
+            const V3 delta = sub(pa, pb);
+            const float sq = len2(delta);
+            if (sq > margin * margin) continue;
+            const V3 cn = normalized_or(cross(sub(B.v[1], B.v[0]), sub(B.v[2], B.v[0])), V3{0.0f, 1.0f, 0.0f});
+            V3 fallback = dot(cn, sub(fa.reference, pb)) >= 0.0f ? cn : mul(cn, -1.0f);
+            if (len2(c_out_b) > 0.5f) fallback = c_out_b;
+            const float dist = sqrtf(fmx(sq, 0.0f));
+            const V3 point = mul(add(pa, pb), 0.5f);
+            const V3 proj = sub(pa, mul(cn, dot(sub(pa, B.v[0]), cn)));
+            const bool on_face = len2(sub(proj, closest_on_triangle(proj, B.v[0], B.v[1], B.v[2]))) <= 1.0e-10f;
+            const V3 nrm = (dist <= 1.0e-5f || on_face) ? fallback : normalized_or(delta, fallback);
+            if (on_face && len2(out_a) < 0.01f && len2(out_b) > 0.5f && bm.solid) {
+                const V3 face_a = normalized_or(cross(sub(A.v[1], A.v[0]), sub(A.v[2], A.v[0])), zero);
+                if (fab(dot(face_a, nrm)) < 1.0e-3f) {
+                    const float depth = fmx(0.0f, -fmn(dot(sub(A.v[0], B.v[0]), nrm),
+                                                       fmn(dot(sub(A.v[1], B.v[0]), nrm), dot(sub(A.v[2], B.v[0]), nrm))));
+                    const V3 laxis = inv_rotate(bs.q, face_a);
+                    const float off = dot(sub(bs.x, A.v[0]), face_a);
+                    float lo = 3.402823466e+38f, hi = -3.402823466e+38f;
+                    for (uint32_t v = 0; v < bm.nv; ++v) {
+                        const float pr = dot(v3(bm.verts[v]), laxis) + off;
+                        lo = fmn(lo, pr);
+                        hi = fmx(hi, pr);
+                    }
+                    const float alt = fmx(0.0f, fmn(-lo, hi));
+                    if (alt + 1.0e-5f < depth) continue;
+                }
+            }
+            const float separation = on_face && len2(c_out_b) > 0.5f ? dot(delta, nrm) : dist;
+            if (!reaches_rest_offset(as, bs, point, nrm, separation, rest, dt)) continue;
+            V3 c_n = nrm, c_p = point;
+            float c_pen = rest - separation + 1.0e-5f;
+            bool recovered = false;
+            if (!am.solid && !bm.solid && dist <= 1.0e-5f) {
+                const Tri oA = posed_tri(am, at, aprev), oB = posed_tri(bm, bt, bprev);
+                V3 opa, opb;
+                closest_triangle_pair(oA, oB, opa, opb);
+                V3 od = sub(opa, opb);
+                if (len2(od) > 1.0e-10f) {
+                    Tri iA, iB;
+                    float low = 0.0f, high = 1.0f;
+                    const float gap = fmn(rest, 0.5f * sqrtf(len2(od)));
+                    for (uint32_t it = 0; it < 10; ++it) {
+                        const float time = 0.5f * (low + high);
+                        for (uint32_t k = 0; k < 3; ++k) {
+                            iA.v[k] = add(oA.v[k], mul(sub(A.v[k], oA.v[k]), time));
+                            iB.v[k] = add(oB.v[k], mul(sub(B.v[k], oB.v[k]), time));
+                        }
+                        V3 p, q;
+                        closest_triangle_pair(iA, iB, p, q);
+                        if (len2(sub(p, q)) > gap * gap)
+                            low = time;
+                        else
+                            high = time;
+                    }
+                    for (uint32_t k = 0; k < 3; ++k) {
+                        iA.v[k] = add(oA.v[k], mul(sub(A.v[k], oA.v[k]), low));
+                        iB.v[k] = add(oB.v[k], mul(sub(B.v[k], oB.v[k]), low));
+                    }
+                    closest_triangle_pair(iA, iB, opa, opb);
+                    od = sub(opa, opb);
+                    c_n = triangle_feature_normal(iA, iB, opa, opb, normalized_or(od, fallback));
+                    const V3 cpa = advect_triangle_point(opa, iA, A);
+                    const V3 cpb = advect_triangle_point(opb, iB, B);
+                    c_p = mul(add(cpa, cpb), 0.5f);
+                    c_pen = rest - dot(sub(cpa, cpb), c_n) + 1.0e-5f;
+                    recovered = true;
+                }
+            }
+            if (dist <= 1.0e-5f) {
+                const bool fixed_member = ((fa.flags | fb.flags) & kFrameFixedMember) != 0;
+                if (!recovered && (fixed_member || on_face)) {
+                    const float depth = fmx(0.0f, -fmn(dot(sub(A.v[0], pb), nrm),
+                                                       fmn(dot(sub(A.v[1], pb), nrm), dot(sub(A.v[2], pb), nrm))));
+                    c_pen = fmn(margin, depth + rest) + 1.0e-5f;
+                } else if (!recovered) {
+                    c_pen = margin + 1.0e-5f;
+                }
+            }
+            if (!shell_contact_facing(c_n, c_out_a, c_out_b)) continue;
+            mm_add(out, c_p, c_n, c_pen, fmx(2.0f * margin, 1.0e-4f));
+        }
+    }
+}
+
+__device__ __forceinline__ void node_of(const MeshView& m, uint32_t k, V3& lo, V3& hi, uint32_t& first,
+                                        uint32_t& count, uint32_t& left, uint32_t& right) {
+    const float4 a = m.bvh[3 * k], b = m.bvh[3 * k + 1], c = m.bvh[3 * k + 2];
+    lo = v3(a);
+    hi = v3(b);
+    first = __float_as_uint(a.w);
+    count = __float_as_uint(b.w);
+    left = __float_as_uint(c.x);
+    right = __float_as_uint(c.y);
+}
+
+__device__ __forceinline__ float rot_bound(Q4 prev, Q4 cur, const MeshView& m) {
+    const Q4 dq = qrelative(prev, cur, false);
+    const float s = len(V3{dq.x, dq.y, dq.z});
+    const V3 ma{fmx(fab(m.lo.x), fab(m.hi.x)), fmx(fab(m.lo.y), fab(m.hi.y)), fmx(fab(m.lo.z), fab(m.hi.z))};
+    return 2.0f * len(ma) * s;
+}
+
+// geometry.slang:2156-2299 without the swept ranges.
+__device__ void collide_meshes(const MeshView& am, const MeshPose& aprev, const MeshPose& as, const Frame& fa,
+                               const MeshView& bm, const MeshPose& bprev, const MeshPose& bs, const Frame& fb,
+                               float margin, float dt, MeshMan& out) {
+    out.count = 0;
+    float threshold = margin;
+    if (!am.solid || !bm.solid) threshold = fmn(threshold, 1.0e-3f);
+    const V3 rel = sub(sub(as.x, aprev.x), sub(bs.x, bprev.x));
+    const bool swept = frames_guided(fa.flags, fb.flags) ||
+                       len(rel) + rot_bound(aprev.q, as.q, am) + rot_bound(bprev.q, bs.q, bm) > threshold;
+    const BoundsXf zero_xf{};
+    const BoundsXf pxa = swept ? bounds_xf(aprev) : zero_xf, pxb = swept ? bounds_xf(bprev) : zero_xf;
+    const BoundsXf xa = bounds_xf(as), xb = bounds_xf(bs);
+    V3 alo, ahi, blo, bhi;
+    motion_bounds(am.lo, am.hi, pxa, xa, swept, margin, alo, ahi);
+    motion_bounds(bm.lo, bm.hi, pxb, xb, swept, 0.0f, blo, bhi);
+    if (!bounds_overlap(alo, ahi, blo, bhi)) return;
+    uint32_t sa[kStack], sb[kStack];
+    sa[0] = 0;
+    sb[0] = 0;
+    uint32_t size = 1;
+    bool overflow = am.nodes == 0 || bm.nodes == 0;
+    while (size > 0 && !overflow) {
+        --size;
+        const uint32_t na = sa[size], nb = sb[size];
+        uint32_t af, ac, al, ar, bf, bc, bl, br;
+        V3 nlo, nhi, mlo, mhi;
+        node_of(am, na, nlo, nhi, af, ac, al, ar);
+        node_of(bm, nb, mlo, mhi, bf, bc, bl, br);
+        motion_bounds(nlo, nhi, pxa, xa, swept, margin, alo, ahi);
+        motion_bounds(mlo, mhi, pxb, xb, swept, 0.0f, blo, bhi);
+        if (!bounds_overlap(alo, ahi, blo, bhi)) continue;
+        const bool la = ac != 0, lb = bc != 0;
+        if (la && lb) {
+            collide_ranges(am, aprev, as, fa, af, ac, bm, bprev, bs, fb, bf, bc, margin, dt, out);
+            continue;
+        }
+        const uint32_t need = la || lb ? 2u : 4u;
+        if (size + need > kStack) {
+            overflow = true;
+            break;
+        }
+        if (la) {
+            sa[size] = na; sb[size++] = br;
+            sa[size] = na; sb[size++] = bl;
+        } else if (lb) {
+            sa[size] = ar; sb[size++] = nb;
+            sa[size] = al; sb[size++] = nb;
+        } else {
+            sa[size] = ar; sb[size++] = br;
+            sa[size] = ar; sb[size++] = bl;
+            sa[size] = al; sb[size++] = br;
+            sa[size] = al; sb[size++] = bl;
+        }
+    }
+    if (overflow) {
+        out.count = 0;
+        collide_ranges(am, aprev, as, fa, 0, am.nt, bm, bprev, bs, fb, 0, bm.nt, margin, dt, out);
+    }
+}
+
+// Hinge contact frames (geometry.slang:404-492) at the predicted poses: the
+// first hinge joint, or unbreakable slider/piston to a static body, gives the
+// frame; a fixed joint marks a fixed member; an axial frame needs the body's
+// only joint. One thread per body.
+__global__ void k_hinge_frames(Dev d) {
+    for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
+        uint32_t flags = d.motion[i] == kStatic ? kFrameStatic : 0u;
+        const V3 x = v3(d.tx[i]);
+        const Q4 q = q4(d.tq[i]);
+        if (!(d.p0[i].x > 0.0f)) {
+            d.frame[i] = f4(x, __uint_as_float(flags));
+            continue;
+        }
+        uint32_t incident = 0;
+        bool present = false, axial = false, fixed_member = false;
+        V3 anchor{0.0f, 0.0f, 0.0f};
+        for (uint32_t k = d.jb_off[i]; k < d.jb_off[i + 1]; ++k) {
+            const uint32_t j = d.jb_list[k];
+            const Joint& o = d.joints[j];
+            if (!o.enabled || d.jstate[j].broken) continue;
+            const bool is_a = o.body_a == i;
+            ++incident;
+            if (o.type == kFixed) fixed_member = true;
+            const bool ax = o.type == kPiston || o.type == kSlider;
+            const uint32_t other = is_a ? o.body_b : o.body_a;
+            const bool static_anchor = other < d.n && d.motion[other] == kStatic;
+            if (present || (o.type != kHinge && !(ax && static_anchor && !(o.breaking_threshold > 0.0f)))) continue;
+            const float* la = is_a ? o.anchor_a : o.anchor_b;
+            anchor = add(x, rotate(q, V3{la[0], la[1], la[2]}));
+            present = true;
+            axial = static_anchor && ax;
+            if (static_anchor) {
+                const float* lo = is_a ? o.anchor_b : o.anchor_a;
+                anchor = add(v3(d.tx[other]), rotate(q4(d.tq[other]), V3{lo[0], lo[1], lo[2]}));
+            }
+        }
+        if (axial && incident != 1u) axial = present = false;
+        flags |= (present ? kFramePresent : 0u) | (axial ? kFrameAxial : 0u) | (fixed_member ? kFrameFixedMember : 0u);
+        d.frame[i] = f4(present && !axial ? anchor : x, __uint_as_float(flags));
+    }
+}
+
+__device__ __forceinline__ MeshPose pose_prev(const Dev& d, uint32_t i) {
+    return {v3(d.x[i]), q4(d.q[i]), v3(d.v[i]), v3(d.w[i])};
+}
+__device__ __forceinline__ MeshPose pose_pred(const Dev& d, uint32_t i) {
+    return {v3(d.tx[i]), q4(d.tq[i]), v3(d.tv[i]), v3(d.tw[i])};
+}
+
+// One thread per candidate on the triangle-mesh path; contacts are staged
+// like the face path's (per-contact normals).
+__global__ void __launch_bounds__(64) k_narrow_mesh(Dev d, StepParams sp) {
+    const uint32_t total = d.ctr->n_mesh;
+    for (uint32_t s = grid_stride_begin(); s < total; s += grid_stride()) {
+        const uint32_t k = d.np_mesh[s];
+        const uint32_t a = d.cand_a[k], b = d.cand_b[k];
+        const MeshView am = mesh_view(d, d.mesh[a]), bm = mesh_view(d, d.mesh[b]);
+        const float margin = d.p2[a].z + d.p2[b].z;
+        MeshMan m;
+        collide_meshes(am, pose_prev(d, a), pose_pred(d, a), frame_of(d, a), bm, pose_prev(d, b), pose_pred(d, b),
+                       frame_of(d, b), margin, sp.dt, m);
+        const uint32_t count = m.count;
+        d.np_count[k] = count;
+        d.np_scan[k] = count ? ((uint64_t(1) << 32) | count) : 0ull;
+        if (!count) continue;
+        const uint32_t slot = atomicAdd(&d.ctr->n_stage, count);
+        if (slot + count > d.cap_stage) {
+            atomicOr(&d.ctr->status, kStContactOverflow);
+            d.np_scan[k] = 0ull;
+            d.np_count[k] = 0;
+            continue;
+        }
+        d.np_stage[k] = slot;
+        for (uint32_t p = 0; p < count; ++p) {
+            d.st_n[slot + p] = f4(m.n[p], m.pen[p]);
+            d.st_p[slot + p] = f4(m.p[p], 1.0f);
+        }
+    }
+}
+
+}  // namespace
+
+void launch_hinge_frames(const Dev& d, cudaStream_t s) {
+    if (!d.nj) return;
+    k_hinge_frames<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+    note_launch(blocks_for(d.n));
+}
+
+void launch_mesh_narrowphase(const Dev& d, const StepParams& sp, cudaStream_t s) {
+    k_narrow_mesh<<<kGridSms, 64, 0, s>>>(d, sp);
+    note_launch(kGridSms);
+}
+
+}  // namespace pmb

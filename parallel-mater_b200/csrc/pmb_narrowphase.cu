@@ -11,9 +11,9 @@
 // reduction (geometry.slang:1129-1270, 1606-1745), with the translation-only
 // swept variant first for pairs that moved more than their margin
 // (:1586-1604, :1751-1853) and the selection of pm_prepare_rigid_face_manifolds
-// (:2741-2803). A pair the face path declines would take the reference's
-// general triangle-mesh path; that path is not part of this build and such a
-// pair keeps an empty manifold.
+// (:2741-2803). A pair the face path declines (not both face-capable, or an
+// empty face manifold) goes to the triangle-mesh path (pmb_meshpath.cu); a
+// guided pair skips the face path.
 //
 // Manifolds are staged by atomic allocation, then placed in pair order by a
 // 64-bit scan (high word: non-empty pair rank, low word: contact offset), so
@@ -308,18 +308,30 @@ __device__ __forceinline__ CandidateMotion candidate_motion(const Dev& d, uint32
     return c;
 }
 
-// Pass 1, one thread per candidate: pairs that are not both convex, and
-// unswept pairs separated by a face plane, get an empty manifold here; the
-// rest go to the survivor list for pass 2 with their separating-axis result.
-// Light enough for full occupancy.
+__device__ __forceinline__ void to_mesh_path(const Dev& d, uint32_t k) {
+    const uint32_t slot = atomicAdd(&d.ctr->n_mesh, 1u);
+    d.np_mesh[slot] = k;
+    d.np_count[k] = 0;
+    d.np_scan[k] = 0ull;
+}
+
+// Pass 1, one thread per candidate: pairs that are not both face-capable, and
+// guided pairs, go to the triangle-mesh path; unswept pairs separated by a
+// face plane get an empty manifold here; the rest go to the survivor list for
+// pass 2 with their separating-axis result. Light enough for full occupancy.
 __global__ void __launch_bounds__(256) k_narrow_sat(Dev d) {
     const uint32_t total = d.ctr->n_cand;
     for (uint32_t k = grid_stride_begin(); k < total; k += grid_stride()) {
         const uint32_t a = d.cand_a[k], b = d.cand_b[k];
         const uint32_t ma = d.mesh[a], mb = d.mesh[b];
-        bool empty = !(d.m_convex[ma] && d.m_convex[mb]);
+        if (!(d.m_convex[ma] && d.m_convex[mb]) ||
+            (d.nj && frames_guided(__float_as_uint(d.frame[a].w), __float_as_uint(d.frame[b].w)))) {
+            to_mesh_path(d, k);
+            continue;
+        }
+        bool empty = false;
         FaceSat fs{0.0f, kInvalid, false};  // kInvalid face: no result kept (swept pair)
-        if (!empty) {
+        {
             const CandidateMotion c = candidate_motion(d, a, b);
             if (!c.swept) {
                 const float reach = c.margin + c.corr;
@@ -359,7 +371,10 @@ __global__ void __launch_bounds__(128, 6) k_narrow(Dev d) {
             ok = face_manifold(c.pred_a, bm, c.pred_b, cm, c.margin, c.corr, m, c.swept ? nullptr : &fs);
             if (c.swept && m.count == 0) ok = false;
         }
-        if (!ok) m.count = 0;
+        if (!ok) {
+            to_mesh_path(d, k);
+            continue;
+        }
         const uint32_t count = m.count;
         d.np_count[k] = count;
         d.np_scan[k] = count ? ((uint64_t(1) << 32) | count) : 0ull;
@@ -493,6 +508,8 @@ void launch_narrowphase(const Dev& d, const StepParams& sp, cudaStream_t s) {
     k_narrow<<<cap_blocks(d.cap_cand, 128), 128, 0, s>>>(d);
     note_launch(cap_blocks(d.cap_cand, 128));
     prof_mark(s, "narrowphase manifolds");
+    launch_mesh_narrowphase(d, sp, s);
+    prof_mark(s, "narrowphase meshes");
     scan_u64(d.np_scan, d.np_scan, &d.ctr->n_cand, d.cap_cand, d.scan_tmp, s);
     k_compact<<<cap_blocks(d.cap_cand), kBlock, 0, s>>>(d);
     note_launch(cap_blocks(d.cap_cand));

@@ -52,6 +52,7 @@ struct Counters {
     uint32_t budget_max;  // batched scenes: the largest scene budget of the tick
     uint32_t n_surv;      // narrowphase candidates left for the manifold pass
     uint32_t n_events;    // contact events recorded by the tick
+    uint32_t n_mesh;      // candidates left for the triangle-mesh path
     uint32_t claim[2];    // solve policy 3: next unclaimed body of the colour (alternating)
     // Bodies bucketed by (colour, width class): bucket col * kWidthClasses + k.
     uint32_t color_count[kMaxColors * kWidthClasses];
@@ -165,6 +166,19 @@ struct Dev {
     uint32_t *m_vo, *m_vc, *m_to, *m_tc, *m_convex;
     float4* m_verts;
     float4* m_planes;
+    // triangle-mesh path: convex at any size; first BVH node; first shell
+    // normal (kInvalid: the mesh has none); local bounds; BVH nodes as three
+    // float4 (lo, first), (hi, count), (left, right); a certified outward
+    // normal per triangle
+    uint32_t *m_solid, *m_bo, *m_so;
+    float4 *m_lo, *m_hi;
+    float4* m_bvh;
+    float4* m_shell;
+    // hinge contact frames of the tick (reference point; flags in w) and
+    // each body's joints in ascending index
+    float4* frame;
+    uint32_t *jb_off, *jb_list;
+    uint32_t* np_mesh;  // candidates for the triangle-mesh path
     // AVBD body state
     float4 *dxl, *dxa, *dq;
     float4 *inA, *inB;  // inertia block: (m/dt2, h33, h43, h44), (h53, h54, h55, -)
@@ -279,6 +293,17 @@ void launch_broadphase(const Dev& d, cudaStream_t s);
 void launch_scene_budgets(const Dev& d, const StepParams& sp, cudaStream_t s);
 __device__ __forceinline__ bool batched(const Dev& d) { return d.n_scenes > 1; }
 void launch_narrowphase(const Dev& d, const StepParams& sp, cudaStream_t s);
+// Per-body hinge contact frames of the tick (worlds with joints) and the
+// triangle-mesh narrowphase over the candidates the face path left to it.
+void launch_hinge_frames(const Dev& d, cudaStream_t s);
+void launch_mesh_narrowphase(const Dev& d, const StepParams& sp, cudaStream_t s);
+// Hinge contact frame flags (d.frame[i].w bits).
+constexpr uint32_t kFramePresent = 1u, kFrameAxial = 2u, kFrameFixedMember = 4u, kFrameStatic = 8u;
+// rigid_guided_pair (geometry.slang:373-377): a body guided along a static
+// rail meets a static body.
+__host__ __device__ __forceinline__ bool frames_guided(uint32_t fa, uint32_t fb) {
+    return ((fa & kFrameAxial) && (fb & kFrameStatic)) || ((fb & kFrameAxial) && (fa & kFrameStatic));
+}
 void launch_prepare(const Dev& d, const StepParams& sp, cudaStream_t s);
 void launch_graph(const Dev& d, const StepParams& sp, cudaStream_t s, int coop_blocks);
 struct SolveBuffers { float4 *ox, *oq, *ov, *ow; };

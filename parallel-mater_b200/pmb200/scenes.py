@@ -375,6 +375,76 @@ def chains(count=512, links=64, seed=3, radius=0.05, length=0.4, spacing=1.0,
     return b.build(f"chains{count}x{links}", iterations, profile)
 
 
+def prism_mesh(polygon, half_z):
+    """A closed prism: the simple polygon ``polygon`` (x, y pairs, counter-
+    clockwise) extruded over z in [-half_z, half_z], caps ear-clipped, every
+    triangle wound outward. Concave polygons give concave meshes."""
+    p = [(float(x), float(y)) for x, y in polygon]
+    m = len(p)
+    v = np.array([[x, y, -half_z] for x, y in p] + [[x, y, half_z] for x, y in p], np.float32)
+
+    def cross2(o, a, b):
+        return (a[0] - o[0]) * (b[1] - o[1]) - (a[1] - o[1]) * (b[0] - o[0])
+
+    def inside(q, a, b, c):
+        return cross2(a, b, q) > 0 and cross2(b, c, q) > 0 and cross2(c, a, q) > 0
+
+    ring, cap = list(range(m)), []
+    while len(ring) > 3:
+        for k in range(len(ring)):
+            i0, i1, i2 = ring[k - 1], ring[k], ring[(k + 1) % len(ring)]
+            a, b, c = p[i0], p[i1], p[i2]
+            if cross2(a, b, c) <= 0:
+                continue
+            if any(inside(p[j], a, b, c) for j in ring if j not in (i0, i1, i2)):
+                continue
+            cap.append((i0, i1, i2))
+            ring.pop(k)
+            break
+        else:
+            raise ValueError("polygon is not simple and counter-clockwise")
+    cap.append(tuple(ring))
+    tris = []
+    for a, b, c in cap:
+        tris += [m + a, m + b, m + c]   # +z cap: counter-clockwise seen from +z
+        tris += [a, c, b]               # -z cap
+    for k in range(m):
+        k1 = (k + 1) % m
+        tris += [k, k1, m + k1, k, m + k1, m + k]   # side quad, outward for a CCW polygon
+    return v, np.array(tris, np.uint32)
+
+
+def mesh_mix(profile=LEGACY, iterations=10, seed=11) -> Scene:
+    """Pairs the convex face path does not take: three boxes dropped into a
+    static U-shaped trough (a closed concave prism), an L-shaped body (concave)
+    resting on the ground with another dropped on it, and a capsule of 64
+    triangles (convex but above the face path's 96 indices) lying down.
+    Collision margins of 4 cm let the unswept contacts catch the falls."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    b = _Builder()
+    _ground(b, 5.0, 5.0)
+    margin = 0.04
+    trough = b.mesh(*prism_mesh([(-1, 0), (1, 0), (1, 1), (0.8, 1), (0.8, 0.2), (-0.8, 0.2), (-0.8, 1), (-1, 1)],
+                                1.0))
+    b.body(trough, STATIC, (0.0, 0.0, 0.0), margin=margin)
+    cube = b.mesh(*box_mesh((0.15, 0.15, 0.15)))
+    for k in range(3):
+        x = float(rng.uniform(-0.4, 0.4))
+        b.body(cube, DYNAMIC, (x, 0.6 + 0.35 * k, float(rng.uniform(-0.3, 0.3))), mass=1.0,
+               inertia=box_inertia(1.0, (0.15,) * 3), margin=margin)
+    ell = [(0, 0), (0.6, 0), (0.6, 0.2), (0.2, 0.2), (0.2, 0.6), (0, 0.6)]
+    cx, cy = 0.2, 0.2
+    lmesh = b.mesh(*prism_mesh([(x - cx, y - cy) for x, y in ell], 0.15))
+    l_inertia = box_inertia(2.0, (0.3, 0.3, 0.15))
+    b.body(lmesh, DYNAMIC, (2.5, cy + 0.001, 0.0), mass=2.0, inertia=l_inertia, margin=margin)
+    b.body(lmesh, DYNAMIC, (2.55, cy + 0.9, 0.05), mass=2.0, inertia=l_inertia, margin=margin)
+    cap = b.mesh(*capsule_mesh(0.2, 0.8, segments=16))
+    s = math.sqrt(0.5)
+    b.body(cap, DYNAMIC, (-2.5, 0.25, 0.0), q=(0.0, 0.0, s, s), mass=1.5,
+           inertia=box_inertia(1.5, (0.2, 0.6, 0.2)), margin=margin)
+    return b.build("mesh mix", iterations, profile)
+
+
 def welded_groups(profile=LEGACY, iterations=10, disable_bc=True) -> Scene:
     """Fixed collision groups. Bars A, B, C (1.2 m long) in a row 0.5 m apart,
     welded A-B and B-C by collision-disabling fixed joints: A and C overlap

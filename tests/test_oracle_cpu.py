@@ -262,3 +262,29 @@ def test_fixed_collision_groups_filter_candidates():
     x = o.states()["x"]
     # the welded bars settle on the ground where they were put
     assert np.allclose(x[1:4, 0], [-1.0, -0.5, 0.0], atol=1e-3) and np.allclose(x[1:4, 1], 0.101, atol=2e-3)
+
+
+def test_triangle_mesh_path_holds_concave_and_large_meshes():
+    """Pairs the convex face path does not take go to the triangle-mesh path
+    (geometry.slang:2156-2299, :1359-1584): boxes dropped into a concave
+    trough come to rest on its floor between its walls, a concave L rests on
+    the ground with another on top of it, a 64-triangle capsule lies on the
+    ground on one of its faces."""
+    s = scenes.mesh_mix()
+    o = O.OracleWorld(s)
+    for _ in range(150):
+        st = o.step()
+        assert st["status"] == 0
+    x = o.states()["x"]
+    assert np.isfinite(x).all()
+    floor = 0.2 + 0.15
+    assert np.all(np.abs(x[2:5, 1] - floor) < 5e-3), x[2:5, 1]
+    assert np.all(np.abs(x[2:5, 0]) < 0.8 - 0.15 + 1e-2)
+    assert abs(x[5, 1] - 0.2) < 5e-3 and x[6, 1] > 0.1
+    assert abs(x[7, 1] - 0.2 * np.cos(np.pi / 16)) < 5e-3
+    # every pair with contacts has at most eight, and the trough's floor
+    # carries the three boxes
+    codes, counts, _ = o.manifolds()
+    assert counts.max() <= 8
+    pairs = {(int(c) // s.n, int(c) % s.n) for c in codes}
+    assert {(2, 1), (3, 1), (4, 1)} <= pairs
