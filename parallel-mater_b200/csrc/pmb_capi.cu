@@ -765,8 +765,9 @@ int pmb_world_profile_step(pmb_world* w, const pmb_step_desc* step, char* report
     cudaMemcpy(&hc, w->d.ctr, sizeof(Counters), cudaMemcpyDeviceToHost);
     {
         char line[160];
-        std::snprintf(line, sizeof(line), "colour fixpoint rounds %u, candidates %u, narrowphase survivors %u\n",
-                      hc.rounds, hc.n_cand, hc.n_surv);
+        std::snprintf(line, sizeof(line),
+                      "colour fixpoint rounds %u, candidates %u, narrowphase survivors %u, triangle-mesh pairs %u\n",
+                      hc.rounds, hc.n_cand, hc.n_surv, hc.n_mesh);
         text += line;
         std::snprintf(line, sizeof(line), "solve iteration 0 (us from kernel start): colours %u\n", hc.colors);
         text += line;

@@ -13,11 +13,12 @@
 // contacts (:1129-1220). The swept triangle ranges (:1921-2155) are not
 // built: a pair that needs continuous contact gets its end-pose contacts.
 //
-// One thread per pair on the path, which is rare: everything stays in
-// registers and local memory. Per-body hinge contact frames (:404-492) are
-// computed once per tick before the narrowphase; the face path uses them to
-// skip guided pairs (:373-377).
-#include "pmb_world.cuh"
+// One warp per pair on the path: the traversal runs identically in every
+// lane and the triangle pairs of each pair of leaves are spread over the
+// lanes, their contacts merged in the reference's order. Per-body hinge
+// contact frames (:404-492) are computed once per tick before the
+// narrowphase; the face path uses them to skip guided pairs (:373-377).
+#include "pmb_meshpath.cuh"
 
 namespace pmb {
 
@@ -205,36 +206,6 @@ __device__ void closest_triangle_pair(const Tri& A, const Tri& B, V3& best_a, V3
         }
 }
 
-__device__ __forceinline__ bool bounds_overlap(V3 alo, V3 ahi, V3 blo, V3 bhi) {
-    return alo.x <= bhi.x && ahi.x >= blo.x && alo.y <= bhi.y && ahi.y >= blo.y && alo.z <= bhi.z && ahi.z >= blo.z;
-}
-
-// math.slang:142-190
-struct BoundsXf { V3 x, ax, ay, az; };
-__device__ __forceinline__ BoundsXf bounds_xf(const MeshPose& s) {
-    return {s.x, rotate(s.q, V3{1.0f, 0.0f, 0.0f}), rotate(s.q, V3{0.0f, 1.0f, 0.0f}),
-            rotate(s.q, V3{0.0f, 0.0f, 1.0f})};
-}
-__device__ void xf_bounds(V3 llo, V3 lhi, const BoundsXf& t, float margin, V3& lo, V3& hi) {
-    const V3 c = mul(add(llo, lhi), 0.5f), h = mul(sub(lhi, llo), 0.5f);
-    const V3 wc = add(t.x, add(mul(t.ax, c.x), add(mul(t.ay, c.y), mul(t.az, c.z))));
-    const V3 wh{fab(t.ax.x) * h.x + fab(t.ay.x) * h.y + fab(t.az.x) * h.z,
-                fab(t.ax.y) * h.x + fab(t.ay.y) * h.y + fab(t.az.y) * h.z,
-                fab(t.ax.z) * h.x + fab(t.ay.z) * h.y + fab(t.az.z) * h.z};
-    const V3 ex{margin, margin, margin};
-    lo = sub(sub(wc, wh), ex);
-    hi = add(add(wc, wh), ex);
-}
-__device__ void motion_bounds(V3 llo, V3 lhi, const BoundsXf& prev, const BoundsXf& cur, bool swept, float margin,
-                              V3& lo, V3& hi) {
-    xf_bounds(llo, lhi, cur, margin, lo, hi);
-    if (!swept) return;
-    V3 plo, phi;
-    xf_bounds(llo, lhi, prev, margin, plo, phi);
-    lo = vmin(lo, plo);
-    hi = vmax(hi, phi);
-}
-
 // geometry.slang:1272-1290
 __device__ __forceinline__ float normal_speed(const MeshPose& a, const MeshPose& b, V3 p, V3 n) {
     const V3 va = add(a.v, cross(a.w, sub(p, a.x)));
@@ -345,121 +316,195 @@ __device__ __forceinline__ Frame frame_of(const Dev& d, uint32_t i) {
 }
 
 
-// geometry.slang:1359-1584
-__device__ void collide_ranges(const MeshView& am, const MeshPose& aprev, const MeshPose& as, const Frame& fa,
-                               uint32_t af, uint32_t ac, const MeshView& bm, const MeshPose& bprev,
-                               const MeshPose& bs, const Frame& fb, uint32_t bf, uint32_t bc, float margin, float dt,
-                               MeshMan& out) {
-    if (frames_guided(fa.flags, fb.flags)) return;
-    const float rest = fmn(margin, 1.0e-3f);
+// The pair-invariant inputs of the triangle ranges (geometry.slang:1359-1379).
+struct RangeCtx {
+    const MeshView* am;
+    const MeshView* bm;
+    MeshPose aprev, as, bprev, bs;
+    Frame fa, fb;
+    float margin, rest, dt;
+    bool interior_a, interior_b, skip;
+};
+
+__device__ RangeCtx range_ctx(const MeshView& am, const MeshPose& aprev, const MeshPose& as, const Frame& fa,
+                              const MeshView& bm, const MeshPose& bprev, const MeshPose& bs, const Frame& fb,
+                              float margin, float dt) {
+    RangeCtx c{&am, &bm, aprev, as, bprev, bs, fa, fb, margin, fmn(margin, 1.0e-3f), dt, false, false, false};
+    c.skip = frames_guided(fa.flags, fb.flags);
     const bool a_static = (fa.flags & kFrameStatic) != 0, b_static = (fb.flags & kFrameStatic) != 0;
-    const bool interior_a = a_static && point_inside_convex(am, aprev, bprev.x);
-    const bool interior_b = b_static && point_inside_convex(bm, bprev, aprev.x);
-    for (uint32_t i = 0; i < ac; ++i) {
-        const uint32_t at = af + i;
-        if (at >= am.nt) break;
-        const Tri A = posed_tri(am, at, as);
-        for (uint32_t j = 0; j < bc; ++j) {
-            const uint32_t bt = bf + j;
-            if (bt >= bm.nt) break;
-            const Tri B = posed_tri(bm, bt, bs);
-            {
-                const V3 ex{margin, margin, margin};
-                const V3 alo = sub(vmin(A.v[0], vmin(A.v[1], A.v[2])), ex);
-                const V3 ahi = add(vmax(A.v[0], vmax(A.v[1], A.v[2])), ex);
-                const V3 blo = vmin(B.v[0], vmin(B.v[1], B.v[2])), bhi = vmax(B.v[0], vmax(B.v[1], B.v[2]));
-                if (!bounds_overlap(alo, ahi, blo, bhi)) continue;
+    c.interior_a = !c.skip && a_static && point_inside_convex(am, aprev, bprev.x);
+    c.interior_b = !c.skip && b_static && point_inside_convex(bm, bprev, aprev.x);
+    return c;
+}
+
+// The contact of triangle `at` of the body against triangle `bt` of the
+// collider (the loop body of geometry.slang:1380-1583); false: none.
+__device__ bool triangle_pair_contact(const RangeCtx& c, uint32_t at, uint32_t bt, V3& c_p, V3& c_n, float& c_pen) {
+    const MeshView& am = *c.am;
+    const MeshView& bm = *c.bm;
+    const float margin = c.margin, rest = c.rest;
+    const Tri A = posed_tri(am, at, c.as);
+    const Tri B = posed_tri(bm, bt, c.bs);
+    {
+        const V3 ex{margin, margin, margin};
+        const V3 alo = sub(vmin(A.v[0], vmin(A.v[1], A.v[2])), ex);
+        const V3 ahi = add(vmax(A.v[0], vmax(A.v[1], A.v[2])), ex);
+        const V3 blo = vmin(B.v[0], vmin(B.v[1], B.v[2])), bhi = vmax(B.v[0], vmax(B.v[1], B.v[2]));
+        if (!bounds_overlap(alo, ahi, blo, bhi)) return false;
+    }
+    const bool a_static = (c.fa.flags & kFrameStatic) != 0, b_static = (c.fb.flags & kFrameStatic) != 0;
+    const V3 out_a = shell_outward(am, at, A), out_b = shell_outward(bm, bt, B);
+    const V3 zero{0.0f, 0.0f, 0.0f};
+    const V3 c_out_a = a_static && c.interior_a ? zero : out_a;
+    const V3 c_out_b = b_static && c.interior_b ? zero : out_b;
+    if (dot(out_a, out_b) > 0.9999f) return false;
+    V3 pa, pb;
+    closest_triangle_pair(A, B, pa, pb);
+    const V3 delta = sub(pa, pb);
+    const float sq = len2(delta);
+    if (sq > margin * margin) return false;
+    const V3 cn = normalized_or(cross(sub(B.v[1], B.v[0]), sub(B.v[2], B.v[0])), V3{0.0f, 1.0f, 0.0f});
+    V3 fallback = dot(cn, sub(c.fa.reference, pb)) >= 0.0f ? cn : mul(cn, -1.0f);
+    if (len2(c_out_b) > 0.5f) fallback = c_out_b;
+    const float dist = sqrtf(fmx(sq, 0.0f));
+    const V3 point = mul(add(pa, pb), 0.5f);
+    const V3 proj = sub(pa, mul(cn, dot(sub(pa, B.v[0]), cn)));
+    const bool on_face = len2(sub(proj, closest_on_triangle(proj, B.v[0], B.v[1], B.v[2]))) <= 1.0e-10f;
+    const V3 nrm = (dist <= 1.0e-5f || on_face) ? fallback : normalized_or(delta, fallback);
+    if (on_face && len2(out_a) < 0.01f && len2(out_b) > 0.5f && bm.solid) {
+        const V3 face_a = normalized_or(cross(sub(A.v[1], A.v[0]), sub(A.v[2], A.v[0])), zero);
+        if (fab(dot(face_a, nrm)) < 1.0e-3f) {
+            const float depth = fmx(0.0f, -fmn(dot(sub(A.v[0], B.v[0]), nrm),
+                                               fmn(dot(sub(A.v[1], B.v[0]), nrm), dot(sub(A.v[2], B.v[0]), nrm))));
+            const V3 laxis = inv_rotate(c.bs.q, face_a);
+            const float off = dot(sub(c.bs.x, A.v[0]), face_a);
+            float lo = 3.402823466e+38f, hi = -3.402823466e+38f;
+            for (uint32_t v = 0; v < bm.nv; ++v) {
+                const float pr = dot(v3(bm.verts[v]), laxis) + off;
+                lo = fmn(lo, pr);
+                hi = fmx(hi, pr);
             }
-            const V3 out_a = shell_outward(am, at, A), out_b = shell_outward(bm, bt, B);
-            const V3 zero{0.0f, 0.0f, 0.0f};
-            const V3 c_out_a = a_static && interior_a ? zero : out_a;
-            const V3 c_out_b = b_static && interior_b ? zero : out_b;
-            if (dot(out_a, out_b) > 0.9999f) continue;
-            V3 pa, pb;
-            closest_triangle_pair(A, B, pa, pb);
-            const V3 delta = sub(pa, pb);
-            const float sq = len2(delta);
-            if (sq > margin * margin) continue;
-            const V3 cn = normalized_or(cross(sub(B.v[1], B.v[0]), sub(B.v[2], B.v[0])), V3{0.0f, 1.0f, 0.0f});
-            V3 fallback = dot(cn, sub(fa.reference, pb)) >= 0.0f ? cn : mul(cn, -1.0f);
-            if (len2(c_out_b) > 0.5f) fallback = c_out_b;
-            const float dist = sqrtf(fmx(sq, 0.0f));
-            const V3 point = mul(add(pa, pb), 0.5f);
-            const V3 proj = sub(pa, mul(cn, dot(sub(pa, B.v[0]), cn)));
-            const bool on_face = len2(sub(proj, closest_on_triangle(proj, B.v[0], B.v[1], B.v[2]))) <= 1.0e-10f;
-            const V3 nrm = (dist <= 1.0e-5f || on_face) ? fallback : normalized_or(delta, fallback);
-            if (on_face && len2(out_a) < 0.01f && len2(out_b) > 0.5f && bm.solid) {
-                const V3 face_a = normalized_or(cross(sub(A.v[1], A.v[0]), sub(A.v[2], A.v[0])), zero);
-                if (fab(dot(face_a, nrm)) < 1.0e-3f) {
-                    const float depth = fmx(0.0f, -fmn(dot(sub(A.v[0], B.v[0]), nrm),
-                                                       fmn(dot(sub(A.v[1], B.v[0]), nrm), dot(sub(A.v[2], B.v[0]), nrm))));
-                    const V3 laxis = inv_rotate(bs.q, face_a);
-                    const float off = dot(sub(bs.x, A.v[0]), face_a);
-                    float lo = 3.402823466e+38f, hi = -3.402823466e+38f;
-                    for (uint32_t v = 0; v < bm.nv; ++v) {
-                        const float pr = dot(v3(bm.verts[v]), laxis) + off;
-                        lo = fmn(lo, pr);
-                        hi = fmx(hi, pr);
-                    }
-                    const float alt = fmx(0.0f, fmn(-lo, hi));
-                    if (alt + 1.0e-5f < depth) continue;
-                }
-            }
-            const float separation = on_face && len2(c_out_b) > 0.5f ? dot(delta, nrm) : dist;
-            if (!reaches_rest_offset(as, bs, point, nrm, separation, rest, dt)) continue;
-            V3 c_n = nrm, c_p = point;
-            float c_pen = rest - separation + 1.0e-5f;
-            bool recovered = false;
-            if (!am.solid && !bm.solid && dist <= 1.0e-5f) {
-                const Tri oA = posed_tri(am, at, aprev), oB = posed_tri(bm, bt, bprev);
-                V3 opa, opb;
-                closest_triangle_pair(oA, oB, opa, opb);
-                V3 od = sub(opa, opb);
-                if (len2(od) > 1.0e-10f) {
-                    Tri iA, iB;
-                    float low = 0.0f, high = 1.0f;
-                    const float gap = fmn(rest, 0.5f * sqrtf(len2(od)));
-                    for (uint32_t it = 0; it < 10; ++it) {
-                        const float time = 0.5f * (low + high);
-                        for (uint32_t k = 0; k < 3; ++k) {
-                            iA.v[k] = add(oA.v[k], mul(sub(A.v[k], oA.v[k]), time));
-                            iB.v[k] = add(oB.v[k], mul(sub(B.v[k], oB.v[k]), time));
-                        }
-                        V3 p, q;
-                        closest_triangle_pair(iA, iB, p, q);
-                        if (len2(sub(p, q)) > gap * gap)
-                            low = time;
-                        else
-                            high = time;
-                    }
-                    for (uint32_t k = 0; k < 3; ++k) {
-                        iA.v[k] = add(oA.v[k], mul(sub(A.v[k], oA.v[k]), low));
-                        iB.v[k] = add(oB.v[k], mul(sub(B.v[k], oB.v[k]), low));
-                    }
-                    closest_triangle_pair(iA, iB, opa, opb);
-                    od = sub(opa, opb);
-                    c_n = triangle_feature_normal(iA, iB, opa, opb, normalized_or(od, fallback));
-                    const V3 cpa = advect_triangle_point(opa, iA, A);
-                    const V3 cpb = advect_triangle_point(opb, iB, B);
-                    c_p = mul(add(cpa, cpb), 0.5f);
-                    c_pen = rest - dot(sub(cpa, cpb), c_n) + 1.0e-5f;
-                    recovered = true;
-                }
-            }
-            if (dist <= 1.0e-5f) {
-                const bool fixed_member = ((fa.flags | fb.flags) & kFrameFixedMember) != 0;
-                if (!recovered && (fixed_member || on_face)) {
-                    const float depth = fmx(0.0f, -fmn(dot(sub(A.v[0], pb), nrm),
-                                                       fmn(dot(sub(A.v[1], pb), nrm), dot(sub(A.v[2], pb), nrm))));
-                    c_pen = fmn(margin, depth + rest) + 1.0e-5f;
-                } else if (!recovered) {
-                    c_pen = margin + 1.0e-5f;
-                }
-            }
-            if (!shell_contact_facing(c_n, c_out_a, c_out_b)) continue;
-            mm_add(out, c_p, c_n, c_pen, fmx(2.0f * margin, 1.0e-4f));
+            const float alt = fmx(0.0f, fmn(-lo, hi));
+            if (alt + 1.0e-5f < depth) return false;
         }
     }
+    const float separation = on_face && len2(c_out_b) > 0.5f ? dot(delta, nrm) : dist;
+    if (!reaches_rest_offset(c.as, c.bs, point, nrm, separation, rest, c.dt)) return false;
+    c_n = nrm;
+    c_p = point;
+    c_pen = rest - separation + 1.0e-5f;
+    bool recovered = false;
+    if (!am.solid && !bm.solid && dist <= 1.0e-5f) {
+        const Tri oA = posed_tri(am, at, c.aprev), oB = posed_tri(bm, bt, c.bprev);
+        V3 opa, opb;
+        closest_triangle_pair(oA, oB, opa, opb);
+        V3 od = sub(opa, opb);
+        if (len2(od) > 1.0e-10f) {
+            Tri iA, iB;
+            float low = 0.0f, high = 1.0f;
+            const float gap = fmn(rest, 0.5f * sqrtf(len2(od)));
+            for (uint32_t it = 0; it < 10; ++it) {
+                const float time = 0.5f * (low + high);
+                for (uint32_t k = 0; k < 3; ++k) {
+                    iA.v[k] = add(oA.v[k], mul(sub(A.v[k], oA.v[k]), time));
+                    iB.v[k] = add(oB.v[k], mul(sub(B.v[k], oB.v[k]), time));
+                }
+                V3 p, q;
+                closest_triangle_pair(iA, iB, p, q);
+                if (len2(sub(p, q)) > gap * gap)
+                    low = time;
+                else
+                    high = time;
+            }
+            for (uint32_t k = 0; k < 3; ++k) {
+                iA.v[k] = add(oA.v[k], mul(sub(A.v[k], oA.v[k]), low));
+                iB.v[k] = add(oB.v[k], mul(sub(B.v[k], oB.v[k]), low));
+            }
+            closest_triangle_pair(iA, iB, opa, opb);
+            od = sub(opa, opb);
+            c_n = triangle_feature_normal(iA, iB, opa, opb, normalized_or(od, fallback));
+            const V3 cpa = advect_triangle_point(opa, iA, A);
+            const V3 cpb = advect_triangle_point(opb, iB, B);
+            c_p = mul(add(cpa, cpb), 0.5f);
+            c_pen = rest - dot(sub(cpa, cpb), c_n) + 1.0e-5f;
+            recovered = true;
+        }
+    }
+    if (dist <= 1.0e-5f) {
+        const bool fixed_member = ((c.fa.flags | c.fb.flags) & kFrameFixedMember) != 0;
+        if (!recovered && (fixed_member || on_face)) {
+            const float depth = fmx(0.0f, -fmn(dot(sub(A.v[0], pb), nrm),
+                                               fmn(dot(sub(A.v[1], pb), nrm), dot(sub(A.v[2], pb), nrm))));
+            c_pen = fmn(margin, depth + rest) + 1.0e-5f;
+        } else if (!recovered) {
+            c_pen = margin + 1.0e-5f;
+        }
+    }
+    return shell_contact_facing(c_n, c_out_a, c_out_b);
+}
+
+// geometry.slang:1359-1584 over a list of range pairs, one warp: the
+// triangle pairs of all the listed ranges, in the reference's order (range
+// pairs in list order; body triangle outer, collider triangle inner), are
+// spread over the lanes 32 at a time and their contacts merged in that order.
+// Every lane keeps the same manifold; warp-uniform control flow throughout.
+constexpr uint32_t kLeafBatch = 32;
+struct RangeList {
+    uint32_t af[kLeafBatch], ac[kLeafBatch], bf[kLeafBatch], bc[kLeafBatch];
+    uint32_t count;
+};
+
+__device__ void warp_ranges(const RangeCtx& c, const RangeList& r, uint32_t lane, MeshMan& out) {
+    if (c.skip) return;
+    uint32_t total = 0;
+    for (uint32_t i = 0; i < r.count; ++i) total += r.ac[i] * r.bc[i];
+    const float spacing = fmx(2.0f * c.margin, 1.0e-4f);
+    uint32_t item = 0, item_base = 0;  // the range pair holding flat index `base + lane` starts the search here
+    for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t f = base + lane;
+        bool valid = false;
+        V3 p{0.0f, 0.0f, 0.0f}, n{0.0f, 0.0f, 0.0f};
+        float pen = 0.0f;
+        if (f < total) {
+            uint32_t i = item, first = item_base;
+            while (f >= first + r.ac[i] * r.bc[i]) {
+                first += r.ac[i] * r.bc[i];
+                ++i;
+            }
+            const uint32_t local = f - first;
+            const uint32_t at = r.af[i] + local / r.bc[i], bt = r.bf[i] + local % r.bc[i];
+            valid = at < c.am->nt && bt < c.bm->nt && triangle_pair_contact(c, at, bt, p, n, pen);
+        }
+        // Advance the search start to the range pair of this chunk's first index.
+        while (item < r.count && base + 32 >= item_base + r.ac[item] * r.bc[item]) {
+            item_base += r.ac[item] * r.bc[item];
+            ++item;
+        }
+        uint32_t mask = __ballot_sync(0xffffffffu, valid);
+        while (mask) {
+            const int src = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const V3 sp{__shfl_sync(0xffffffffu, p.x, src), __shfl_sync(0xffffffffu, p.y, src),
+                        __shfl_sync(0xffffffffu, p.z, src)};
+            const V3 sn{__shfl_sync(0xffffffffu, n.x, src), __shfl_sync(0xffffffffu, n.y, src),
+                        __shfl_sync(0xffffffffu, n.z, src)};
+            const float spen = __shfl_sync(0xffffffffu, pen, src);
+            mm_add(out, sp, sn, spen, spacing);
+        }
+    }
+}
+
+// Contacts of one range pair (the full pass after a stack overflow is a
+// single range pair over all triangles).
+__device__ void warp_range(const RangeCtx& c, uint32_t af, uint32_t ac, uint32_t bf, uint32_t bc, uint32_t lane,
+                           MeshMan& out) {
+    RangeList r;
+    r.af[0] = af;
+    r.ac[0] = ac;
+    r.bf[0] = bf;
+    r.bc[0] = bc;
+    r.count = 1;
+    warp_ranges(c, r, lane, out);
 }
 
 __device__ __forceinline__ void node_of(const MeshView& m, uint32_t k, V3& lo, V3& hi, uint32_t& first,
@@ -473,30 +518,28 @@ __device__ __forceinline__ void node_of(const MeshView& m, uint32_t k, V3& lo, V
     right = __float_as_uint(c.y);
 }
 
-__device__ __forceinline__ float rot_bound(Q4 prev, Q4 cur, const MeshView& m) {
-    const Q4 dq = qrelative(prev, cur, false);
-    const float s = len(V3{dq.x, dq.y, dq.z});
-    const V3 ma{fmx(fab(m.lo.x), fab(m.hi.x)), fmx(fab(m.lo.y), fab(m.hi.y)), fmx(fab(m.lo.z), fab(m.hi.z))};
-    return 2.0f * len(ma) * s;
-}
-
-// geometry.slang:2156-2299 without the swept ranges.
+// geometry.slang:2156-2299 without the swept ranges, one warp per pair:
+// every lane runs the (cheap, bounds-only) traversal identically, and the
+// triangle pairs of each overlapping leaf pair are shared out by warp_ranges.
 __device__ void collide_meshes(const MeshView& am, const MeshPose& aprev, const MeshPose& as, const Frame& fa,
                                const MeshView& bm, const MeshPose& bprev, const MeshPose& bs, const Frame& fb,
-                               float margin, float dt, MeshMan& out) {
+                               float margin, float dt, uint32_t lane, MeshMan& out) {
     out.count = 0;
-    float threshold = margin;
-    if (!am.solid || !bm.solid) threshold = fmn(threshold, 1.0e-3f);
-    const V3 rel = sub(sub(as.x, aprev.x), sub(bs.x, bprev.x));
-    const bool swept = frames_guided(fa.flags, fb.flags) ||
-                       len(rel) + rot_bound(aprev.q, as.q, am) + rot_bound(bprev.q, bs.q, bm) > threshold;
+    const bool swept = mesh_pair_swept(aprev.x, aprev.q, as.x, as.q, am.lo, am.hi, am.solid, bprev.x, bprev.q, bs.x,
+                                       bs.q, bm.lo, bm.hi, bm.solid, margin, frames_guided(fa.flags, fb.flags));
     const BoundsXf zero_xf{};
-    const BoundsXf pxa = swept ? bounds_xf(aprev) : zero_xf, pxb = swept ? bounds_xf(bprev) : zero_xf;
-    const BoundsXf xa = bounds_xf(as), xb = bounds_xf(bs);
+    const BoundsXf pxa = swept ? bounds_xf(aprev.x, aprev.q) : zero_xf;
+    const BoundsXf pxb = swept ? bounds_xf(bprev.x, bprev.q) : zero_xf;
+    const BoundsXf xa = bounds_xf(as.x, as.q), xb = bounds_xf(bs.x, bs.q);
     V3 alo, ahi, blo, bhi;
     motion_bounds(am.lo, am.hi, pxa, xa, swept, margin, alo, ahi);
     motion_bounds(bm.lo, bm.hi, pxb, xb, swept, 0.0f, blo, bhi);
     if (!bounds_overlap(alo, ahi, blo, bhi)) return;
+    const RangeCtx ctx = range_ctx(am, aprev, as, fa, bm, bprev, bs, fb, margin, dt);
+    // Overlapping leaf pairs are collected in visit order and their triangle
+    // pairs evaluated a batch at a time; merging stays in visit order.
+    RangeList leaves;
+    leaves.count = 0;
     uint32_t sa[kStack], sb[kStack];
     sa[0] = 0;
     sb[0] = 0;
@@ -514,7 +557,14 @@ __device__ void collide_meshes(const MeshView& am, const MeshPose& aprev, const 
         if (!bounds_overlap(alo, ahi, blo, bhi)) continue;
         const bool la = ac != 0, lb = bc != 0;
         if (la && lb) {
-            collide_ranges(am, aprev, as, fa, af, ac, bm, bprev, bs, fb, bf, bc, margin, dt, out);
+            leaves.af[leaves.count] = af;
+            leaves.ac[leaves.count] = ac;
+            leaves.bf[leaves.count] = bf;
+            leaves.bc[leaves.count] = bc;
+            if (++leaves.count == kLeafBatch) {
+                warp_ranges(ctx, leaves, lane, out);
+                leaves.count = 0;
+            }
             continue;
         }
         const uint32_t need = la || lb ? 2u : 4u;
@@ -537,7 +587,9 @@ __device__ void collide_meshes(const MeshView& am, const MeshPose& aprev, const 
     }
     if (overflow) {
         out.count = 0;
-        collide_ranges(am, aprev, as, fa, 0, am.nt, bm, bprev, bs, fb, 0, bm.nt, margin, dt, out);
+        warp_range(ctx, 0, am.nt, 0, bm.nt, lane, out);
+    } else if (leaves.count) {
+        warp_ranges(ctx, leaves, lane, out);
     }
 }
 
@@ -590,18 +642,21 @@ __device__ __forceinline__ MeshPose pose_pred(const Dev& d, uint32_t i) {
     return {v3(d.tx[i]), q4(d.tq[i]), v3(d.tv[i]), v3(d.tw[i])};
 }
 
-// One thread per candidate on the triangle-mesh path; contacts are staged
-// like the face path's (per-contact normals).
-__global__ void __launch_bounds__(64) k_narrow_mesh(Dev d, StepParams sp) {
+// One warp per candidate on the triangle-mesh path; lane 0 stages the
+// contacts like the face path's (per-contact normals).
+__global__ void __launch_bounds__(128) k_narrow_mesh(Dev d, StepParams sp) {
     const uint32_t total = d.ctr->n_mesh;
-    for (uint32_t s = grid_stride_begin(); s < total; s += grid_stride()) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < total; s += warps) {
         const uint32_t k = d.np_mesh[s];
         const uint32_t a = d.cand_a[k], b = d.cand_b[k];
         const MeshView am = mesh_view(d, d.mesh[a]), bm = mesh_view(d, d.mesh[b]);
         const float margin = d.p2[a].z + d.p2[b].z;
         MeshMan m;
         collide_meshes(am, pose_prev(d, a), pose_pred(d, a), frame_of(d, a), bm, pose_prev(d, b), pose_pred(d, b),
-                       frame_of(d, b), margin, sp.dt, m);
+                       frame_of(d, b), margin, sp.dt, lane, m);
+        if (lane != 0) continue;
         const uint32_t count = m.count;
         d.np_count[k] = count;
         d.np_scan[k] = count ? ((uint64_t(1) << 32) | count) : 0ull;
@@ -630,8 +685,8 @@ void launch_hinge_frames(const Dev& d, cudaStream_t s) {
 }
 
 void launch_mesh_narrowphase(const Dev& d, const StepParams& sp, cudaStream_t s) {
-    k_narrow_mesh<<<kGridSms, 64, 0, s>>>(d, sp);
-    note_launch(kGridSms);
+    k_narrow_mesh<<<4 * kGridSms, 128, 0, s>>>(d, sp);
+    note_launch(4 * kGridSms);
 }
 
 }  // namespace pmb

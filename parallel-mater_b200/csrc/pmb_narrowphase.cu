@@ -18,7 +18,7 @@
 // Manifolds are staged by atomic allocation, then placed in pair order by a
 // 64-bit scan (high word: non-empty pair rank, low word: contact offset), so
 // pairs and contacts come out in the reference's active-pair order.
-#include "pmb_world.cuh"
+#include "pmb_meshpath.cuh"
 
 namespace pmb {
 
@@ -308,11 +308,13 @@ __device__ __forceinline__ CandidateMotion candidate_motion(const Dev& d, uint32
     return c;
 }
 
+// A candidate the face path leaves to the triangle-mesh path, queued for the
+// mesh kernel with an empty manifold until then.
 __device__ __forceinline__ void to_mesh_path(const Dev& d, uint32_t k) {
-    const uint32_t slot = atomicAdd(&d.ctr->n_mesh, 1u);
-    d.np_mesh[slot] = k;
     d.np_count[k] = 0;
     d.np_scan[k] = 0ull;
+    const uint32_t slot = atomicAdd(&d.ctr->n_mesh, 1u);
+    d.np_mesh[slot] = k;
 }
 
 // Pass 1, one thread per candidate: pairs that are not both face-capable, and
@@ -324,8 +326,8 @@ __global__ void __launch_bounds__(256) k_narrow_sat(Dev d) {
     for (uint32_t k = grid_stride_begin(); k < total; k += grid_stride()) {
         const uint32_t a = d.cand_a[k], b = d.cand_b[k];
         const uint32_t ma = d.mesh[a], mb = d.mesh[b];
-        if (!(d.m_convex[ma] && d.m_convex[mb]) ||
-            (d.nj && frames_guided(__float_as_uint(d.frame[a].w), __float_as_uint(d.frame[b].w)))) {
+        const bool guided = d.nj && frames_guided(__float_as_uint(d.frame[a].w), __float_as_uint(d.frame[b].w));
+        if (!(d.m_convex[ma] && d.m_convex[mb]) || guided) {
             to_mesh_path(d, k);
             continue;
         }
@@ -372,7 +374,14 @@ __global__ void __launch_bounds__(128, 6) k_narrow(Dev d) {
             if (c.swept && m.count == 0) ok = false;
         }
         if (!ok) {
-            to_mesh_path(d, k);
+            // Most declined pairs lie beyond the pair margin: their root
+            // bounds (the mesh path's first test) settle them here.
+            if (mesh_pair_bounds_overlap(d, a, b, false)) {
+                to_mesh_path(d, k);
+            } else {
+                d.np_count[k] = 0;
+                d.np_scan[k] = 0ull;
+            }
             continue;
         }
         const uint32_t count = m.count;
