@@ -12,11 +12,13 @@
 //   feature normal                  :1855-1908
 //   BVH pair traversal              :2156-2299 (rigid_collide_meshes)
 //   bounds transforms               src/slang/math.slang:43-49, :142-190
-// What is restated: the unswept triangle ranges over the BVH traversal of
-// rigid_collide_meshes (swept bounds when the pair requires them), and the
-// per-body hinge frame fields those ranges read. Not restated: the swept
-// triangle ranges (:1921-2155), so a pair that needs continuous contact only
-// gets its end-pose contacts, and guided contacts (produced only there).
+//   swept triangle ranges           :1921-2155
+// What is restated: the BVH traversal of rigid_collide_meshes with the
+// unswept triangle ranges and, for a pair that moved more than its
+// threshold, the swept ranges (conservative advancement) after them at each
+// leaf pair; the per-body hinge frame fields those ranges read. Not restated:
+// guided contacts (a body on an unbreakable slider or piston to a static body
+// against a static body), which such pairs therefore do not get.
 #pragma once
 #include <vector>
 
@@ -462,6 +464,134 @@ inline void collide_triangle_ranges(const Mesh<R>& am, const State<R>& aprev, co
     }
 }
 
+// geometry.slang:1921-2154 (the unguided pairs): conservative advancement
+// of each triangle pair along its linear vertex paths from the previous to
+// the current pose, up to 32 steps; the first pose within the rest offset
+// gives a contact whose depth is the distance still to close this tick and
+// whose impact fraction is the time reached (zero when it started in contact).
+template <class R>
+inline void collide_triangle_ranges_swept(const Mesh<R>& am, const State<R>& aprev, const State<R>& as,
+                                          V3<R> prev_ref_a, const HingeFrame<R>& ah, uint32_t af, uint32_t ac,
+                                          const Mesh<R>& bm, const State<R>& bprev, const State<R>& bs,
+                                          const HingeFrame<R>& bh, uint32_t bf, uint32_t bc, R margin, R dt,
+                                          Manifold<R>& out) {
+    if (guided_pair(ah, bh)) return;  // guided contacts are not restated
+    const R rest = mn(margin, R(1.0e-3));
+    const bool interior_a = ah.static_body && point_inside_convex(am, aprev, bprev.x);
+    const bool interior_b = bh.static_body && point_inside_convex(bm, bprev, aprev.x);
+    const uint32_t a_tris = uint32_t(am.idx.size() / 3), b_tris = uint32_t(bm.idx.size() / 3);
+    for (uint32_t i = 0; i < ac; ++i) {
+        const uint32_t at = af + i;
+        if (at >= a_tris) break;
+        V3<R> PA[3], CA[3];
+        for (uint32_t k = 0; k < 3; ++k) {
+            const V3<R> l = am.verts[am.idx[3 * at + k]];
+            PA[k] = xf_point(aprev, l);
+            CA[k] = xf_point(as, l);
+        }
+        V3<R> alo = vmin(PA[0], CA[0]), ahi = vmax(PA[0], CA[0]);
+        for (uint32_t k = 1; k < 3; ++k) {
+            alo = vmin(alo, vmin(PA[k], CA[k]));
+            ahi = vmax(ahi, vmax(PA[k], CA[k]));
+        }
+        for (uint32_t j = 0; j < bc; ++j) {
+            const uint32_t bt = bf + j;
+            if (bt >= b_tris) break;
+            V3<R> PB[3], CB[3];
+            for (uint32_t k = 0; k < 3; ++k) {
+                const V3<R> l = bm.verts[bm.idx[3 * bt + k]];
+                PB[k] = xf_point(bprev, l);
+                CB[k] = xf_point(bs, l);
+            }
+            V3<R> blo = vmin(PB[0], CB[0]), bhi = vmax(PB[0], CB[0]);
+            for (uint32_t k = 1; k < 3; ++k) {
+                blo = vmin(blo, vmin(PB[k], CB[k]));
+                bhi = vmax(bhi, vmax(PB[k], CB[k]));
+            }
+            const V3<R> ex{margin, margin, margin};
+            if (!bounds_overlap(sub(alo, ex), add(ahi, ex), blo, bhi)) continue;
+            V3<R> DA[3], DB[3];
+            R abs_speed = 0;
+            for (uint32_t k = 0; k < 3; ++k) {
+                DA[k] = sub(CA[k], PA[k]);
+                DB[k] = sub(CB[k], PB[k]);
+                abs_speed = mx(abs_speed, len(DA[k]));
+            }
+            R col_speed = 0;
+            for (uint32_t k = 0; k < 3; ++k) col_speed = mx(col_speed, len(DB[k]));
+            abs_speed += col_speed;
+            const V3<R> common = DB[0];
+            R rel_a = 0, rel_b = 0;
+            for (uint32_t k = 0; k < 3; ++k) {
+                rel_a = mx(rel_a, len(sub(DA[k], common)));
+                rel_b = mx(rel_b, len(sub(DB[k], common)));
+            }
+            const R bound = mn(abs_speed, rel_a + rel_b);
+            if (bound <= kEps<R>()) continue;
+            R time = 0;
+            bool starts_near = false;
+            V3<R> sep_n{};
+            bool have_sep = false;
+            for (uint32_t it = 0; it < 32; ++it) {
+                V3<R> A[3], B[3];
+                for (uint32_t k = 0; k < 3; ++k) {
+                    A[k] = add(PA[k], mul(DA[k], time));
+                    B[k] = add(PB[k], mul(DB[k], time));
+                }
+                V3<R> pa, pb;
+                closest_triangle_pair(A, B, pa, pb);
+                const V3<R> delta = sub(pa, pb);
+                const R dist = std::sqrt(mx(R(0), len2(delta)));
+                const R offset = rest;
+                if (it == 0) {
+                    starts_near = dist <= offset + R(5.0e-5);
+                    // A gap wider than the largest relative motion of the tick
+                    // (and 0.1 mm) cannot close: the advancement would end
+                    // without contact.
+                    if (dist > offset + R(1.0e-5) + bound + R(1.0e-4)) break;
+                }
+                if (dist <= offset + R(1.0e-5)) {
+                    const V3<R> cn = normalized_or(cross(sub(B[1], B[0]), sub(B[2], B[0])), V3<R>{0, 1, 0});
+                    const V3<R> center = add(aprev.x, mul(sub(as.x, aprev.x), time));
+                    V3<R> fallback = dot(cn, sub(center, pb)) >= R(0) ? cn : mul(cn, R(-1));
+                    if (ah.present) {
+                        const V3<R> ref = add(prev_ref_a, mul(sub(ah.reference, prev_ref_a), time));
+                        fallback = dot(cn, sub(ref, pb)) >= R(0) ? cn : mul(cn, R(-1));
+                    }
+                    const V3<R> out_a = shell_outward(am, at, A[0], A[1], A[2]);
+                    const V3<R> out_b = shell_outward(bm, bt, B[0], B[1], B[2]);
+                    const V3<R> c_out_a = ah.static_body && interior_a ? V3<R>{} : out_a;
+                    const V3<R> c_out_b = bh.static_body && interior_b ? V3<R>{} : out_b;
+                    if (dot(out_a, out_b) > R(0.9999)) break;
+                    if (len2(c_out_b) > R(0.5))
+                        fallback = c_out_b;
+                    else if (len2(c_out_a) > R(0.5))
+                        fallback = mul(c_out_a, R(-1));
+                    const V3<R> nrm = triangle_feature_normal(A, B, pa, pb, have_sep ? sep_n : fallback);
+                    if (!shell_contact_facing(nrm, c_out_a, c_out_b)) break;
+                    const V3<R> point = mul(add(pa, pb), R(0.5));
+                    const R speed = normal_speed(as, bs, point, nrm);
+                    if (speed > R(1.0e-5)) break;
+                    const R remaining = -speed * dt * (R(1) - time) - dist;
+                    Contact<R> c{};
+                    c.normal = nrm;
+                    c.point = point;
+                    c.penetration = mx(R(0), remaining + offset) + R(1.0e-5);
+                    c.impact_fraction = starts_near ? R(0) : time;
+                    c.init_speed = speed;
+                    add_contact(out, c, mx(margin * R(2), R(1.0e-4)));
+                    break;
+                }
+                sep_n = triangle_feature_normal(A, B, pa, pb, normalized_or(delta, V3<R>{0, 1, 0}));
+                have_sep = true;
+                const R adv = (dist - offset) / (bound + kEps<R>()) * R(0.9);
+                time += mx(adv, R(1.0e-5));
+                if (time > R(1)) break;
+            }
+        }
+    }
+}
+
 // geometry.slang:1586-1604
 template <class R>
 inline bool requires_swept(const State<R>& pa, const State<R>& a, const Mesh<R>& am, const State<R>& pb,
@@ -477,8 +607,8 @@ inline bool requires_swept(const State<R>& pa, const State<R>& a, const Mesh<R>&
 // overflow the stack restarts as one pass over all triangle pairs.
 template <class R>
 inline void collide_meshes(const World<R>& w, uint32_t a, uint32_t b, const std::vector<State<R>>& prev,
-                           const std::vector<State<R>>& cur, const HingeFrame<R>& ah, const HingeFrame<R>& bh, R dt,
-                           Manifold<R>& out) {
+                           const std::vector<State<R>>& cur, const HingeFrame<R>& ah, const HingeFrame<R>& bh,
+                           V3<R> prev_ref_a, R dt, Manifold<R>& out) {
     out = Manifold<R>{};
     const Mesh<R>& am = w.meshes[w.body[a].mesh];
     const Mesh<R>& bm = w.meshes[w.body[b].mesh];
@@ -506,6 +636,9 @@ inline void collide_meshes(const World<R>& w, uint32_t a, uint32_t b, const std:
         if (la && lb) {
             collide_triangle_ranges(am, prev[a], cur[a], ah, A.first, A.count, bm, prev[b], cur[b], bh, B.first,
                                     B.count, margin, dt, out);
+            if (swept)
+                collide_triangle_ranges_swept(am, prev[a], cur[a], prev_ref_a, ah, A.first, A.count, bm, prev[b],
+                                              cur[b], bh, B.first, B.count, margin, dt, out);
             continue;
         }
         const uint32_t need = la || lb ? 2u : 4u;
@@ -528,8 +661,11 @@ inline void collide_meshes(const World<R>& w, uint32_t a, uint32_t b, const std:
     }
     if (overflow) {
         out = Manifold<R>{};
-        collide_triangle_ranges(am, prev[a], cur[a], ah, 0, uint32_t(am.idx.size() / 3), bm, prev[b], cur[b], bh, 0,
-                                uint32_t(bm.idx.size() / 3), margin, dt, out);
+        const uint32_t na = uint32_t(am.idx.size() / 3), nb = uint32_t(bm.idx.size() / 3);
+        collide_triangle_ranges(am, prev[a], cur[a], ah, 0, na, bm, prev[b], cur[b], bh, 0, nb, margin, dt, out);
+        if (swept)
+            collide_triangle_ranges_swept(am, prev[a], cur[a], prev_ref_a, ah, 0, na, bm, prev[b], cur[b], bh, 0, nb,
+                                          margin, dt, out);
     }
 }
 

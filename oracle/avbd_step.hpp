@@ -147,6 +147,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
     w.active_pairs.clear();
     w.manifolds.clear();
     const std::vector<HingeFrame<R>> frames = hinge_frames(w, pred);
+    const std::vector<HingeFrame<R>> prev_frames = hinge_frames(w, prev);
     for (uint32_t code : w.candidate_pairs) {
         uint32_t a = code / n, b = code % n;
         const Mesh<R>& bm = w.meshes[w.body[a].mesh];
@@ -166,7 +167,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
             }
         }
         // A pair the face path declines goes to the triangle-mesh path.
-        if (!face) collide_meshes(w, a, b, prev, pred, frames[a], frames[b], dt, m);
+        if (!face) collide_meshes(w, a, b, prev, pred, frames[a], frames[b], prev_frames[a].reference, dt, m);
         if (m.count == 0) continue;
         bool persistent = face_capable(bm) && (!dynamic(w, b) || face_capable(cm));
         for (uint32_t p = 0; p < m.count; ++p) {

@@ -310,6 +310,7 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     ALLOCP(d.m_solid, nm); ALLOCP(d.m_bo, nm); ALLOCP(d.m_so, nm); ALLOCP(d.m_lo, nm); ALLOCP(d.m_hi, nm);
     ALLOCP(d.m_bvh, 3 * z.bvh_nodes); ALLOCP(d.m_shell, z.shell_normals);
     ALLOCP(d.jb_off, nj ? size_t(n) + 1 : 0); ALLOCP(d.jb_list, 2 * size_t(nj)); ALLOC(d.frame, nj ? size_t(n) : 0);
+    ALLOC(d.frame_prev, nj ? size_t(n) : 0);
     ALLOC(d.np_mesh, cap_cand);
     ALLOC(d.dxl, n); ALLOC(d.dxa, n); ALLOC(d.dq, n); ALLOC(d.inA, n); ALLOC(d.inB, n);
     ALLOCS(d.prev_vel, n); ALLOCS(d.color, n);

@@ -10,12 +10,15 @@
 // certified shell normals that orient and filter them (:1308-1337), the
 // rest-offset reach test (:1272-1290), the intersection recovery of two
 // non-convex meshes (:1292-1306, :1855-1908) -- merged into at most eight
-// contacts (:1129-1220). The swept triangle ranges (:1921-2155) are not
-// built: a pair that needs continuous contact gets its end-pose contacts.
+// contacts (:1129-1220); for a pair that moved more than its threshold, the
+// swept triangle ranges (:1921-2155, conservative advancement) after the
+// unswept ones at each leaf pair. Guided contacts (a body on an unbreakable
+// slider or piston to a static body, against a static body) are not built:
+// such pairs get no contacts.
 //
-// One warp per pair on the path: the traversal runs identically in every
-// lane and the triangle pairs of each pair of leaves are spread over the
-// lanes, their contacts merged in the reference's order. Per-body hinge
+// One block per pair on the path: the traversal runs identically in every
+// thread and the triangle pairs of each batch of leaf pairs are spread over
+// the threads, their contacts merged in the reference's order. Per-body hinge
 // contact frames (:404-492) are computed once per tick before the
 // narrowphase; the face path uses them to skip guided pairs (:373-377).
 #include "pmb_meshpath.cuh"
@@ -31,37 +34,32 @@ struct MeshPose { V3 x; Q4 q; V3 v, w; };
 struct MeshMan {
     uint32_t count;
     V3 p[8], n[8];
-    float pen[8];
+    float pen[8], impact[8];
 };
 
 // geometry.slang:1129-1220, the unguided merge: a point within `spacing` of a
 // kept one replaces it when deeper; a ninth point replaces the shallowest.
-__device__ void mm_add(MeshMan& m, V3 p, V3 n, float pen, float spacing) {
+__device__ void mm_put(MeshMan& m, uint32_t i, V3 p, V3 n, float pen, float impact) {
+    m.p[i] = p;
+    m.n[i] = n;
+    m.pen[i] = pen;
+    m.impact[i] = impact;
+}
+__device__ void mm_add(MeshMan& m, V3 p, V3 n, float pen, float impact, float spacing) {
     const float s2 = spacing * spacing;
     for (uint32_t i = 0; i < m.count; ++i)
         if (len2(sub(m.p[i], p)) < s2) {
-            if (pen - m.pen[i] > 0.0f) {
-                m.p[i] = p;
-                m.n[i] = n;
-                m.pen[i] = pen;
-            }
+            if (pen - m.pen[i] > 0.0f) mm_put(m, i, p, n, pen, impact);
             return;
         }
     if (m.count < 8) {
-        m.p[m.count] = p;
-        m.n[m.count] = n;
-        m.pen[m.count] = pen;
-        ++m.count;
+        mm_put(m, m.count++, p, n, pen, impact);
         return;
     }
     uint32_t sh = 0;
     for (uint32_t i = 1; i < m.count; ++i)
         if (m.pen[i] < m.pen[sh]) sh = i;
-    if (pen > m.pen[sh]) {
-        m.p[sh] = p;
-        m.n[sh] = n;
-        m.pen[sh] = pen;
-    }
+    if (pen > m.pen[sh]) mm_put(m, sh, p, n, pen, impact);
 }
 
 struct Tri { V3 v[3]; };
@@ -175,7 +173,7 @@ __device__ bool segment_hits_triangle(V3 p, V3 q, const Tri& t, V3& hit) {
 }
 
 // geometry.slang:1057-1105
-__device__ void closest_triangle_pair(const Tri& A, const Tri& B, V3& best_a, V3& best_b) {
+__device__ __noinline__ void closest_triangle_pair(const Tri& A, const Tri& B, V3& best_a, V3& best_b) {
     V3 hit;
     for (uint32_t e = 0; e < 3; ++e)
         if (segment_hits_triangle(A.v[e], A.v[(e + 1) % 3], B, hit)) {
@@ -264,7 +262,7 @@ __device__ bool point_inside_convex(const MeshView& m, const MeshPose& s, V3 p) 
 }
 
 // geometry.slang:1855-1908
-__device__ V3 triangle_feature_normal(const Tri& A, const Tri& B, V3 pa, V3 pb, V3 fallback) {
+__device__ __noinline__ V3 triangle_feature_normal(const Tri& A, const Tri& B, V3 pa, V3 pb, V3 fallback) {
     const V3 delta = sub(pa, pb);
     V3 n = normalized_or(delta, fallback);
     const V3 faces[2] = {normalized_or(cross(sub(A.v[1], A.v[0]), sub(A.v[2], A.v[0])), n),
@@ -322,14 +320,16 @@ struct RangeCtx {
     const MeshView* bm;
     MeshPose aprev, as, bprev, bs;
     Frame fa, fb;
+    V3 prev_ref_a;  // the body's reference point at the previous pose
     float margin, rest, dt;
-    bool interior_a, interior_b, skip;
+    bool interior_a, interior_b, skip, swept;
 };
 
 __device__ RangeCtx range_ctx(const MeshView& am, const MeshPose& aprev, const MeshPose& as, const Frame& fa,
-                              const MeshView& bm, const MeshPose& bprev, const MeshPose& bs, const Frame& fb,
-                              float margin, float dt) {
-    RangeCtx c{&am, &bm, aprev, as, bprev, bs, fa, fb, margin, fmn(margin, 1.0e-3f), dt, false, false, false};
+                              V3 prev_ref_a, const MeshView& bm, const MeshPose& bprev, const MeshPose& bs,
+                              const Frame& fb, float margin, float dt, bool swept) {
+    RangeCtx c{&am,   &bm,   aprev, as, bprev, bs, fa, fb, prev_ref_a, margin, fmn(margin, 1.0e-3f),
+               dt,    false, false, false, swept};
     c.skip = frames_guided(fa.flags, fb.flags);
     const bool a_static = (fa.flags & kFrameStatic) != 0, b_static = (fb.flags & kFrameStatic) != 0;
     c.interior_a = !c.skip && a_static && point_inside_convex(am, aprev, bprev.x);
@@ -339,7 +339,7 @@ __device__ RangeCtx range_ctx(const MeshView& am, const MeshPose& aprev, const M
 
 // The contact of triangle `at` of the body against triangle `bt` of the
 // collider (the loop body of geometry.slang:1380-1583); false: none.
-__device__ bool triangle_pair_contact(const RangeCtx& c, uint32_t at, uint32_t bt, V3& c_p, V3& c_n, float& c_pen) {
+__device__ __noinline__ bool triangle_pair_contact(const RangeCtx& c, uint32_t at, uint32_t bt, V3& c_p, V3& c_n, float& c_pen) {
     const MeshView& am = *c.am;
     const MeshView& bm = *c.bm;
     const float margin = c.margin, rest = c.rest;
@@ -443,68 +443,191 @@ __device__ bool triangle_pair_contact(const RangeCtx& c, uint32_t at, uint32_t b
     return shell_contact_facing(c_n, c_out_a, c_out_b);
 }
 
-// geometry.slang:1359-1584 over a list of range pairs, one warp: the
-// triangle pairs of all the listed ranges, in the reference's order (range
-// pairs in list order; body triangle outer, collider triangle inner), are
-// spread over the lanes 32 at a time and their contacts merged in that order.
-// Every lane keeps the same manifold; warp-uniform control flow throughout.
+// The swept contact of triangle `at` against `bt` (the loop body of
+// geometry.slang:1963-2151 for an unguided pair): conservative advancement
+// along the vertices' linear paths, up to 32 steps; false: none.
+__device__ __noinline__ bool triangle_pair_swept_contact(const RangeCtx& c, uint32_t at, uint32_t bt, V3& c_p, V3& c_n,
+                                            float& c_pen, float& c_impact) {
+    const MeshView& am = *c.am;
+    const MeshView& bm = *c.bm;
+    const float margin = c.margin, offset = c.rest;
+    const Tri PA = posed_tri(am, at, c.aprev), CA = posed_tri(am, at, c.as);
+    const Tri PB = posed_tri(bm, bt, c.bprev), CB = posed_tri(bm, bt, c.bs);
+    V3 alo = vmin(PA.v[0], CA.v[0]), ahi = vmax(PA.v[0], CA.v[0]);
+    V3 blo = vmin(PB.v[0], CB.v[0]), bhi = vmax(PB.v[0], CB.v[0]);
+    for (uint32_t k = 1; k < 3; ++k) {
+        alo = vmin(alo, vmin(PA.v[k], CA.v[k]));
+        ahi = vmax(ahi, vmax(PA.v[k], CA.v[k]));
+        blo = vmin(blo, vmin(PB.v[k], CB.v[k]));
+        bhi = vmax(bhi, vmax(PB.v[k], CB.v[k]));
+    }
+    const V3 ex{margin, margin, margin};
+    if (!bounds_overlap(sub(alo, ex), add(ahi, ex), blo, bhi)) return false;
+    Tri DA, DB;
+    float abs_speed = 0.0f;
+    for (uint32_t k = 0; k < 3; ++k) {
+        DA.v[k] = sub(CA.v[k], PA.v[k]);
+        DB.v[k] = sub(CB.v[k], PB.v[k]);
+        abs_speed = fmx(abs_speed, len(DA.v[k]));
+    }
+    float col_speed = 0.0f;
+    for (uint32_t k = 0; k < 3; ++k) col_speed = fmx(col_speed, len(DB.v[k]));
+    abs_speed += col_speed;
+    const V3 common = DB.v[0];
+    float rel_a = 0.0f, rel_b = 0.0f;
+    for (uint32_t k = 0; k < 3; ++k) {
+        rel_a = fmx(rel_a, len(sub(DA.v[k], common)));
+        rel_b = fmx(rel_b, len(sub(DB.v[k], common)));
+    }
+    const float bound = fmn(abs_speed, rel_a + rel_b);
+    if (bound <= kEps) return false;
+    const bool a_static = (c.fa.flags & kFrameStatic) != 0, b_static = (c.fb.flags & kFrameStatic) != 0;
+    const V3 zero{0.0f, 0.0f, 0.0f};
+    float time = 0.0f;
+    bool starts_near = false, have_sep = false;
+    V3 sep_n = zero;
+    for (uint32_t it = 0; it < 32; ++it) {
+        Tri A, B;
+        for (uint32_t k = 0; k < 3; ++k) {
+            A.v[k] = add(PA.v[k], mul(DA.v[k], time));
+            B.v[k] = add(PB.v[k], mul(DB.v[k], time));
+        }
+        V3 pa, pb;
+        closest_triangle_pair(A, B, pa, pb);
+        const V3 delta = sub(pa, pb);
+        const float dist = sqrtf(fmx(0.0f, len2(delta)));
+        if (it == 0) {
+            starts_near = dist <= offset + 5.0e-5f;
+            // No point of either triangle moves more than `bound` relative to
+            // the other during the tick: a gap wider than that (and 0.1 mm)
+            // cannot close, and the advancement would end without contact.
+            if (dist > offset + 1.0e-5f + bound + 1.0e-4f) return false;
+        }
+        if (dist <= offset + 1.0e-5f) {
+            const V3 cn = normalized_or(cross(sub(B.v[1], B.v[0]), sub(B.v[2], B.v[0])), V3{0.0f, 1.0f, 0.0f});
+            const V3 center = add(c.aprev.x, mul(sub(c.as.x, c.aprev.x), time));
+            V3 fallback = dot(cn, sub(center, pb)) >= 0.0f ? cn : mul(cn, -1.0f);
+            if (c.fa.flags & kFramePresent) {
+                const V3 ref = add(c.prev_ref_a, mul(sub(c.fa.reference, c.prev_ref_a), time));
+                fallback = dot(cn, sub(ref, pb)) >= 0.0f ? cn : mul(cn, -1.0f);
+            }
+            const V3 out_a = shell_outward(am, at, A), out_b = shell_outward(bm, bt, B);
+            const V3 c_out_a = a_static && c.interior_a ? zero : out_a;
+            const V3 c_out_b = b_static && c.interior_b ? zero : out_b;
+            if (dot(out_a, out_b) > 0.9999f) return false;
+            if (len2(c_out_b) > 0.5f)
+                fallback = c_out_b;
+            else if (len2(c_out_a) > 0.5f)
+                fallback = mul(c_out_a, -1.0f);
+            const V3 nrm = triangle_feature_normal(A, B, pa, pb, have_sep ? sep_n : fallback);
+            if (!shell_contact_facing(nrm, c_out_a, c_out_b)) return false;
+            const V3 point = mul(add(pa, pb), 0.5f);
+            const float speed = normal_speed(c.as, c.bs, point, nrm);
+            if (speed > 1.0e-5f) return false;
+            const float remaining = -speed * c.dt * (1.0f - time) - dist;
+            c_n = nrm;
+            c_p = point;
+            c_pen = fmx(0.0f, remaining + offset) + 1.0e-5f;
+            c_impact = starts_near ? 0.0f : time;
+            return true;
+        }
+        sep_n = triangle_feature_normal(A, B, pa, pb, normalized_or(delta, V3{0.0f, 1.0f, 0.0f}));
+        have_sep = true;
+        const float adv = (dist - offset) / (bound + kEps) * 0.9f;
+        time += fmx(adv, 1.0e-5f);
+        if (time > 1.0f) return false;
+    }
+    return false;
+}
+
+// geometry.slang:1359-1584 and :1921-2155 over a list of range pairs, one
+// block: the triangle pairs of all the listed ranges, in the reference's
+// order (range pairs in list order; unswept before swept; body triangle
+// outer, collider triangle inner), are spread over the threads a chunk at a
+// time and their contacts merged in that order by thread 0, which keeps the
+// manifold. Block-uniform control flow throughout.
 constexpr uint32_t kLeafBatch = 32;
 struct RangeList {
     uint32_t af[kLeafBatch], ac[kLeafBatch], bf[kLeafBatch], bc[kLeafBatch];
     uint32_t count;
 };
 
-__device__ void warp_ranges(const RangeCtx& c, const RangeList& r, uint32_t lane, MeshMan& out) {
+constexpr uint32_t kMeshThreads = 128;  // threads per pair on the mesh path
+
+// Thread 0's BVH pair traversal: the stack and the batch of leaf pairs.
+struct Traversal {
+    uint32_t sa[kStack], sb[kStack];
+    uint32_t size;
+    bool overflow;
+    RangeList leaves;
+};
+
+// Per-chunk results of the block's threads, merged in order by thread 0, and
+// the traversal state.
+struct ChunkResults {
+    float4 p[kMeshThreads];   // point, impact fraction
+    float4 n[kMeshThreads];   // normal, depth
+    uint32_t valid[kMeshThreads];
+    Traversal walk;
+};
+
+__device__ void block_ranges(const RangeCtx& c, const RangeList& r, uint32_t tid, ChunkResults& sm, MeshMan& out) {
     if (c.skip) return;
+    // Each range pair contributes its unswept triangle pairs, then (a swept
+    // pair) its swept ones: the reference's order at a leaf pair.
+    const uint32_t kinds = c.swept ? 2u : 1u;
     uint32_t total = 0;
-    for (uint32_t i = 0; i < r.count; ++i) total += r.ac[i] * r.bc[i];
+    for (uint32_t i = 0; i < r.count; ++i) total += kinds * r.ac[i] * r.bc[i];
     const float spacing = fmx(2.0f * c.margin, 1.0e-4f);
-    uint32_t item = 0, item_base = 0;  // the range pair holding flat index `base + lane` starts the search here
-    for (uint32_t base = 0; base < total; base += 32) {
-        const uint32_t f = base + lane;
+    uint32_t item = 0, item_base = 0;  // the range pair holding flat index `base` starts the search here
+    for (uint32_t base = 0; base < total; base += kMeshThreads) {
+        const uint32_t f = base + tid;
         bool valid = false;
         V3 p{0.0f, 0.0f, 0.0f}, n{0.0f, 0.0f, 0.0f};
-        float pen = 0.0f;
+        float pen = 0.0f, impact = 1.0f;
         if (f < total) {
             uint32_t i = item, first = item_base;
-            while (f >= first + r.ac[i] * r.bc[i]) {
-                first += r.ac[i] * r.bc[i];
+            while (f >= first + kinds * r.ac[i] * r.bc[i]) {
+                first += kinds * r.ac[i] * r.bc[i];
                 ++i;
             }
-            const uint32_t local = f - first;
+            const uint32_t size = r.ac[i] * r.bc[i];
+            const uint32_t local = (f - first) % size;
+            const bool swept_item = f - first >= size;
             const uint32_t at = r.af[i] + local / r.bc[i], bt = r.bf[i] + local % r.bc[i];
-            valid = at < c.am->nt && bt < c.bm->nt && triangle_pair_contact(c, at, bt, p, n, pen);
+            if (at < c.am->nt && bt < c.bm->nt)
+                valid = swept_item ? triangle_pair_swept_contact(c, at, bt, p, n, pen, impact)
+                                   : triangle_pair_contact(c, at, bt, p, n, pen);
         }
-        // Advance the search start to the range pair of this chunk's first index.
-        while (item < r.count && base + 32 >= item_base + r.ac[item] * r.bc[item]) {
-            item_base += r.ac[item] * r.bc[item];
+        // Advance the search start to the range pair of the next chunk's first index.
+        while (item < r.count && base + kMeshThreads >= item_base + kinds * r.ac[item] * r.bc[item]) {
+            item_base += kinds * r.ac[item] * r.bc[item];
             ++item;
         }
-        uint32_t mask = __ballot_sync(0xffffffffu, valid);
-        while (mask) {
-            const int src = __ffs(mask) - 1;
-            mask &= mask - 1;
-            const V3 sp{__shfl_sync(0xffffffffu, p.x, src), __shfl_sync(0xffffffffu, p.y, src),
-                        __shfl_sync(0xffffffffu, p.z, src)};
-            const V3 sn{__shfl_sync(0xffffffffu, n.x, src), __shfl_sync(0xffffffffu, n.y, src),
-                        __shfl_sync(0xffffffffu, n.z, src)};
-            const float spen = __shfl_sync(0xffffffffu, pen, src);
-            mm_add(out, sp, sn, spen, spacing);
+        sm.valid[tid] = valid ? 1u : 0u;
+        sm.p[tid] = f4(p, impact);
+        sm.n[tid] = f4(n, pen);
+        __syncthreads();
+        if (tid == 0) {
+            const uint32_t count = total - base < kMeshThreads ? total - base : kMeshThreads;
+            for (uint32_t k = 0; k < count; ++k)
+                if (sm.valid[k]) mm_add(out, v3(sm.p[k]), v3(sm.n[k]), sm.n[k].w, sm.p[k].w, spacing);
         }
+        __syncthreads();
     }
 }
 
 // Contacts of one range pair (the full pass after a stack overflow is a
 // single range pair over all triangles).
-__device__ void warp_range(const RangeCtx& c, uint32_t af, uint32_t ac, uint32_t bf, uint32_t bc, uint32_t lane,
-                           MeshMan& out) {
+__device__ void block_range(const RangeCtx& c, uint32_t af, uint32_t ac, uint32_t bf, uint32_t bc, uint32_t tid,
+                            ChunkResults& sm, MeshMan& out) {
     RangeList r;
     r.af[0] = af;
     r.ac[0] = ac;
     r.bf[0] = bf;
     r.bc[0] = bc;
     r.count = 1;
-    warp_ranges(c, r, lane, out);
+    block_ranges(c, r, tid, sm, out);
 }
 
 __device__ __forceinline__ void node_of(const MeshView& m, uint32_t k, V3& lo, V3& hi, uint32_t& first,
@@ -518,12 +641,13 @@ __device__ __forceinline__ void node_of(const MeshView& m, uint32_t k, V3& lo, V
     right = __float_as_uint(c.y);
 }
 
-// geometry.slang:2156-2299 without the swept ranges, one warp per pair:
-// every lane runs the (cheap, bounds-only) traversal identically, and the
-// triangle pairs of each overlapping leaf pair are shared out by warp_ranges.
+// geometry.slang:2156-2299, one block per pair: every thread runs the
+// (cheap, bounds-only) traversal identically, and the triangle pairs of each
+// batch of overlapping leaf pairs are shared out by block_ranges.
 __device__ void collide_meshes(const MeshView& am, const MeshPose& aprev, const MeshPose& as, const Frame& fa,
-                               const MeshView& bm, const MeshPose& bprev, const MeshPose& bs, const Frame& fb,
-                               float margin, float dt, uint32_t lane, MeshMan& out) {
+                               V3 prev_ref_a, const MeshView& bm, const MeshPose& bprev, const MeshPose& bs,
+                               const Frame& fb, float margin, float dt, uint32_t tid, ChunkResults& sm,
+                               MeshMan& out) {
     out.count = 0;
     const bool swept = mesh_pair_swept(aprev.x, aprev.q, as.x, as.q, am.lo, am.hi, am.solid, bprev.x, bprev.q, bs.x,
                                        bs.q, bm.lo, bm.hi, bm.solid, margin, frames_guided(fa.flags, fb.flags));
@@ -535,103 +659,121 @@ __device__ void collide_meshes(const MeshView& am, const MeshPose& aprev, const 
     motion_bounds(am.lo, am.hi, pxa, xa, swept, margin, alo, ahi);
     motion_bounds(bm.lo, bm.hi, pxb, xb, swept, 0.0f, blo, bhi);
     if (!bounds_overlap(alo, ahi, blo, bhi)) return;
-    const RangeCtx ctx = range_ctx(am, aprev, as, fa, bm, bprev, bs, fb, margin, dt);
-    // Overlapping leaf pairs are collected in visit order and their triangle
-    // pairs evaluated a batch at a time; merging stays in visit order.
-    RangeList leaves;
-    leaves.count = 0;
-    uint32_t sa[kStack], sb[kStack];
-    sa[0] = 0;
-    sb[0] = 0;
-    uint32_t size = 1;
-    bool overflow = am.nodes == 0 || bm.nodes == 0;
-    while (size > 0 && !overflow) {
-        --size;
-        const uint32_t na = sa[size], nb = sb[size];
-        uint32_t af, ac, al, ar, bf, bc, bl, br;
-        V3 nlo, nhi, mlo, mhi;
-        node_of(am, na, nlo, nhi, af, ac, al, ar);
-        node_of(bm, nb, mlo, mhi, bf, bc, bl, br);
-        motion_bounds(nlo, nhi, pxa, xa, swept, margin, alo, ahi);
-        motion_bounds(mlo, mhi, pxb, xb, swept, 0.0f, blo, bhi);
-        if (!bounds_overlap(alo, ahi, blo, bhi)) continue;
-        const bool la = ac != 0, lb = bc != 0;
-        if (la && lb) {
-            leaves.af[leaves.count] = af;
-            leaves.ac[leaves.count] = ac;
-            leaves.bf[leaves.count] = bf;
-            leaves.bc[leaves.count] = bc;
-            if (++leaves.count == kLeafBatch) {
-                warp_ranges(ctx, leaves, lane, out);
-                leaves.count = 0;
+    const RangeCtx ctx = range_ctx(am, aprev, as, fa, prev_ref_a, bm, bprev, bs, fb, margin, dt, swept);
+    // Thread 0 walks the BVH pair stack (in shared memory) and collects the
+    // overlapping leaf pairs in visit order; each batch is evaluated by the
+    // whole block, merging in visit order.
+    Traversal& t = sm.walk;
+    if (tid == 0) {
+        t.sa[0] = 0;
+        t.sb[0] = 0;
+        t.size = 1;
+        t.overflow = am.nodes == 0 || bm.nodes == 0;
+        t.leaves.count = 0;
+    }
+    __syncthreads();
+    bool overflow = false;
+    for (;;) {
+        if (tid == 0) {
+            t.leaves.count = 0;
+            while (t.size > 0 && !t.overflow && t.leaves.count < kLeafBatch) {
+                const uint32_t na = t.sa[--t.size], nb = t.sb[t.size];
+                uint32_t af, ac, al, ar, bf, bc, bl, br;
+                V3 nlo, nhi, mlo, mhi;
+                node_of(am, na, nlo, nhi, af, ac, al, ar);
+                node_of(bm, nb, mlo, mhi, bf, bc, bl, br);
+                motion_bounds(nlo, nhi, pxa, xa, swept, margin, alo, ahi);
+                motion_bounds(mlo, mhi, pxb, xb, swept, 0.0f, blo, bhi);
+                if (!bounds_overlap(alo, ahi, blo, bhi)) continue;
+                const bool la = ac != 0, lb = bc != 0;
+                if (la && lb) {
+                    const uint32_t k = t.leaves.count++;
+                    t.leaves.af[k] = af;
+                    t.leaves.ac[k] = ac;
+                    t.leaves.bf[k] = bf;
+                    t.leaves.bc[k] = bc;
+                    continue;
+                }
+                const uint32_t need = la || lb ? 2u : 4u;
+                if (t.size + need > kStack) {
+                    t.overflow = true;
+                    break;
+                }
+                uint32_t z = t.size;
+                if (la) {
+                    t.sa[z] = na; t.sb[z++] = br;
+                    t.sa[z] = na; t.sb[z++] = bl;
+                } else if (lb) {
+                    t.sa[z] = ar; t.sb[z++] = nb;
+                    t.sa[z] = al; t.sb[z++] = nb;
+                } else {
+                    t.sa[z] = ar; t.sb[z++] = br;
+                    t.sa[z] = ar; t.sb[z++] = bl;
+                    t.sa[z] = al; t.sb[z++] = br;
+                    t.sa[z] = al; t.sb[z++] = bl;
+                }
+                t.size = z;
             }
-            continue;
         }
-        const uint32_t need = la || lb ? 2u : 4u;
-        if (size + need > kStack) {
-            overflow = true;
-            break;
-        }
-        if (la) {
-            sa[size] = na; sb[size++] = br;
-            sa[size] = na; sb[size++] = bl;
-        } else if (lb) {
-            sa[size] = ar; sb[size++] = nb;
-            sa[size] = al; sb[size++] = nb;
-        } else {
-            sa[size] = ar; sb[size++] = br;
-            sa[size] = ar; sb[size++] = bl;
-            sa[size] = al; sb[size++] = br;
-            sa[size] = al; sb[size++] = bl;
-        }
+        __syncthreads();
+        overflow = t.overflow;
+        const bool more = t.size > 0;
+        const uint32_t batch = t.leaves.count;
+        __syncthreads();  // every thread has the state before thread 0 moves on
+        if (overflow) break;
+        if (batch) block_ranges(ctx, t.leaves, tid, sm, out);  // reads the batch, ends with a barrier
+        if (!more) break;
     }
     if (overflow) {
         out.count = 0;
-        warp_range(ctx, 0, am.nt, 0, bm.nt, lane, out);
-    } else if (leaves.count) {
-        warp_ranges(ctx, leaves, lane, out);
+        block_range(ctx, 0, am.nt, 0, bm.nt, tid, sm, out);
     }
+    __syncthreads();  // the traversal state is reused by the block's next pair
 }
 
-// Hinge contact frames (geometry.slang:404-492) at the predicted poses: the
-// first hinge joint, or unbreakable slider/piston to a static body, gives the
-// frame; a fixed joint marks a fixed member; an axial frame needs the body's
-// only joint. One thread per body.
+// The frame of body i at one set of poses (pos/rot: the predicted or the
+// previous positions and orientations of every body): reference point, flags.
+__device__ float4 hinge_frame_at(const Dev& d, uint32_t i, const float4* pos, const float4* rot) {
+    uint32_t flags = d.motion[i] == kStatic ? kFrameStatic : 0u;
+    const V3 x = v3(pos[i]);
+    const Q4 q = q4(rot[i]);
+    if (!(d.p0[i].x > 0.0f)) return f4(x, __uint_as_float(flags));
+    uint32_t incident = 0;
+    bool present = false, axial = false, fixed_member = false;
+    V3 anchor{0.0f, 0.0f, 0.0f};
+    for (uint32_t k = d.jb_off[i]; k < d.jb_off[i + 1]; ++k) {
+        const uint32_t j = d.jb_list[k];
+        const Joint& o = d.joints[j];
+        if (!o.enabled || d.jstate[j].broken) continue;
+        const bool is_a = o.body_a == i;
+        ++incident;
+        if (o.type == kFixed) fixed_member = true;
+        const bool ax = o.type == kPiston || o.type == kSlider;
+        const uint32_t other = is_a ? o.body_b : o.body_a;
+        const bool static_anchor = other < d.n && d.motion[other] == kStatic;
+        if (present || (o.type != kHinge && !(ax && static_anchor && !(o.breaking_threshold > 0.0f)))) continue;
+        const float* la = is_a ? o.anchor_a : o.anchor_b;
+        anchor = add(x, rotate(q, V3{la[0], la[1], la[2]}));
+        present = true;
+        axial = static_anchor && ax;
+        if (static_anchor) {
+            const float* lo = is_a ? o.anchor_b : o.anchor_a;
+            anchor = add(v3(pos[other]), rotate(q4(rot[other]), V3{lo[0], lo[1], lo[2]}));
+        }
+    }
+    if (axial && incident != 1u) axial = present = false;
+    flags |= (present ? kFramePresent : 0u) | (axial ? kFrameAxial : 0u) | (fixed_member ? kFrameFixedMember : 0u);
+    return f4(present && !axial ? anchor : x, __uint_as_float(flags));
+}
+
+// Hinge contact frames (geometry.slang:404-492) at the predicted and at the
+// previous poses: the first hinge joint, or unbreakable slider/piston to a
+// static body, gives the frame; a fixed joint marks a fixed member; an axial
+// frame needs the body's only joint. One thread per body.
 __global__ void k_hinge_frames(Dev d) {
     for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
-        uint32_t flags = d.motion[i] == kStatic ? kFrameStatic : 0u;
-        const V3 x = v3(d.tx[i]);
-        const Q4 q = q4(d.tq[i]);
-        if (!(d.p0[i].x > 0.0f)) {
-            d.frame[i] = f4(x, __uint_as_float(flags));
-            continue;
-        }
-        uint32_t incident = 0;
-        bool present = false, axial = false, fixed_member = false;
-        V3 anchor{0.0f, 0.0f, 0.0f};
-        for (uint32_t k = d.jb_off[i]; k < d.jb_off[i + 1]; ++k) {
-            const uint32_t j = d.jb_list[k];
-            const Joint& o = d.joints[j];
-            if (!o.enabled || d.jstate[j].broken) continue;
-            const bool is_a = o.body_a == i;
-            ++incident;
-            if (o.type == kFixed) fixed_member = true;
-            const bool ax = o.type == kPiston || o.type == kSlider;
-            const uint32_t other = is_a ? o.body_b : o.body_a;
-            const bool static_anchor = other < d.n && d.motion[other] == kStatic;
-            if (present || (o.type != kHinge && !(ax && static_anchor && !(o.breaking_threshold > 0.0f)))) continue;
-            const float* la = is_a ? o.anchor_a : o.anchor_b;
-            anchor = add(x, rotate(q, V3{la[0], la[1], la[2]}));
-            present = true;
-            axial = static_anchor && ax;
-            if (static_anchor) {
-                const float* lo = is_a ? o.anchor_b : o.anchor_a;
-                anchor = add(v3(d.tx[other]), rotate(q4(d.tq[other]), V3{lo[0], lo[1], lo[2]}));
-            }
-        }
-        if (axial && incident != 1u) axial = present = false;
-        flags |= (present ? kFramePresent : 0u) | (axial ? kFrameAxial : 0u) | (fixed_member ? kFrameFixedMember : 0u);
-        d.frame[i] = f4(present && !axial ? anchor : x, __uint_as_float(flags));
+        d.frame[i] = hinge_frame_at(d, i, d.tx, d.tq);
+        d.frame_prev[i] = hinge_frame_at(d, i, d.x, d.q);
     }
 }
 
@@ -642,21 +784,22 @@ __device__ __forceinline__ MeshPose pose_pred(const Dev& d, uint32_t i) {
     return {v3(d.tx[i]), q4(d.tq[i]), v3(d.tv[i]), v3(d.tw[i])};
 }
 
-// One warp per candidate on the triangle-mesh path; lane 0 stages the
+// One block per candidate on the triangle-mesh path; thread 0 stages the
 // contacts like the face path's (per-contact normals).
-__global__ void __launch_bounds__(128) k_narrow_mesh(Dev d, StepParams sp) {
+__global__ void __launch_bounds__(kMeshThreads, 4) k_narrow_mesh(Dev d, StepParams sp) {
+    __shared__ ChunkResults sm;
     const uint32_t total = d.ctr->n_mesh;
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < total; s += warps) {
+    const uint32_t tid = threadIdx.x;
+    for (uint32_t s = blockIdx.x; s < total; s += gridDim.x) {
         const uint32_t k = d.np_mesh[s];
         const uint32_t a = d.cand_a[k], b = d.cand_b[k];
         const MeshView am = mesh_view(d, d.mesh[a]), bm = mesh_view(d, d.mesh[b]);
         const float margin = d.p2[a].z + d.p2[b].z;
         MeshMan m;
-        collide_meshes(am, pose_prev(d, a), pose_pred(d, a), frame_of(d, a), bm, pose_prev(d, b), pose_pred(d, b),
-                       frame_of(d, b), margin, sp.dt, lane, m);
-        if (lane != 0) continue;
+        const V3 prev_ref_a = d.nj ? v3(d.frame_prev[a]) : v3(d.x[a]);
+        collide_meshes(am, pose_prev(d, a), pose_pred(d, a), frame_of(d, a), prev_ref_a, bm, pose_prev(d, b),
+                       pose_pred(d, b), frame_of(d, b), margin, sp.dt, tid, sm, m);
+        if (tid != 0) continue;
         const uint32_t count = m.count;
         d.np_count[k] = count;
         d.np_scan[k] = count ? ((uint64_t(1) << 32) | count) : 0ull;
@@ -671,7 +814,7 @@ __global__ void __launch_bounds__(128) k_narrow_mesh(Dev d, StepParams sp) {
         d.np_stage[k] = slot;
         for (uint32_t p = 0; p < count; ++p) {
             d.st_n[slot + p] = f4(m.n[p], m.pen[p]);
-            d.st_p[slot + p] = f4(m.p[p], 1.0f);
+            d.st_p[slot + p] = f4(m.p[p], m.impact[p]);
         }
     }
 }
@@ -685,8 +828,8 @@ void launch_hinge_frames(const Dev& d, cudaStream_t s) {
 }
 
 void launch_mesh_narrowphase(const Dev& d, const StepParams& sp, cudaStream_t s) {
-    k_narrow_mesh<<<4 * kGridSms, 128, 0, s>>>(d, sp);
-    note_launch(4 * kGridSms);
+    k_narrow_mesh<<<8 * kGridSms, kMeshThreads, 0, s>>>(d, sp);
+    note_launch(8 * kGridSms);
 }
 
 }  // namespace pmb

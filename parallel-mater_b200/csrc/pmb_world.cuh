@@ -176,7 +176,7 @@ struct Dev {
     float4* m_shell;
     // hinge contact frames of the tick (reference point; flags in w) and
     // each body's joints in ascending index
-    float4* frame;
+    float4 *frame, *frame_prev;  // at the predicted and at the previous poses
     uint32_t *jb_off, *jb_list;
     uint32_t* np_mesh;  // candidates for the triangle-mesh path
     // AVBD body state

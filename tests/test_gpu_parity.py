@@ -155,11 +155,13 @@ def test_fixed_collision_groups_match_oracle(gpu_available):
     assert 1 * s.n + 3 not in codes and 5 * s.n + 6 not in codes
 
 
-def test_triangle_mesh_path_matches_oracle(gpu_available):
+@pytest.mark.parametrize("margin", [0.04, 0.005])
+def test_triangle_mesh_path_matches_oracle(gpu_available, margin):
     """The triangle-mesh narrowphase on the GPU (concave trough and L bodies,
-    a 64-triangle capsule): candidate pairs, contact counts and manifolds
-    equal the oracle's every tick; poses follow it."""
-    s = scenes.mesh_mix()
+    a 64-triangle capsule; with 5 mm margins the falls take the swept
+    ranges): candidate pairs, contact counts and manifolds equal the oracle's
+    every tick; poses follow it."""
+    s = scenes.mesh_mix(margin=margin)
     w = core.World(s)
     o = O.OracleWorld(s)
     worst = 0.0

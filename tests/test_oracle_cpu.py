@@ -288,3 +288,9 @@ def test_triangle_mesh_path_holds_concave_and_large_meshes():
     assert counts.max() <= 8
     pairs = {(int(c) // s.n, int(c) % s.n) for c in codes}
     assert {(2, 1), (3, 1), (4, 1)} <= pairs
+    # With 5 mm margins the first box falls 4.7 cm per tick onto the trough
+    # floor: only the swept triangle ranges (:1921-2155) stop it there.
+    o = O.OracleWorld(scenes.mesh_mix(margin=0.005))
+    for _ in range(150):
+        assert o.step()["status"] == 0
+    assert abs(o.states()["x"][2, 1] - floor) < 5e-3
