@@ -312,6 +312,12 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     ALLOCP(d.jb_off, nj ? size_t(n) + 1 : 0); ALLOCP(d.jb_list, 2 * size_t(nj)); ALLOC(d.frame, nj ? size_t(n) : 0);
     ALLOC(d.frame_prev, nj ? size_t(n) : 0);
     ALLOC(d.np_mesh, cap_cand);
+    d.cap_mesh = uint32_t(cap_pair);
+    d.cap_mesh_leaves = d.cap_mesh_items = uint32_t(cap_contact);
+    ALLOC(d.mp_leaves, cap_pair); ALLOC(d.mp_items, cap_pair); ALLOC(d.mp_flags, cap_pair);
+    ALLOC(d.mp_leaf_off, cap_pair + 1); ALLOC(d.mp_item_off, cap_pair + 1);
+    ALLOC(d.ml_rec, cap_contact); ALLOC(d.ml_item, cap_contact); ALLOC(d.ml_pair, cap_contact);
+    ALLOC(d.mi_valid, cap_contact); ALLOC(d.mi_p, cap_contact); ALLOC(d.mi_n, cap_contact);
     ALLOC(d.dxl, n); ALLOC(d.dxa, n); ALLOC(d.dq, n); ALLOC(d.inA, n); ALLOC(d.inB, n);
     ALLOCS(d.prev_vel, n); ALLOCS(d.color, n);
     ALLOC(d.parent, n); ALLOC(d.impact, n); ALLOC(d.anchored, n); ALLOC(d.mean, n); ALLOC(d.island_end, n);
@@ -767,8 +773,9 @@ int pmb_world_profile_step(pmb_world* w, const pmb_step_desc* step, char* report
     {
         char line[160];
         std::snprintf(line, sizeof(line),
-                      "colour fixpoint rounds %u, candidates %u, narrowphase survivors %u, triangle-mesh pairs %u\n",
-                      hc.rounds, hc.n_cand, hc.n_surv, hc.n_mesh);
+                      "colour fixpoint rounds %u, candidates %u, narrowphase survivors %u, triangle-mesh pairs %u "
+                      "(leaf pairs %u, triangle-pair items %u)\n",
+                      hc.rounds, hc.n_cand, hc.n_surv, hc.n_mesh, hc.n_mesh_leaves, hc.n_mesh_items);
         text += line;
         std::snprintf(line, sizeof(line), "solve iteration 0 (us from kernel start): colours %u\n", hc.colors);
         text += line;

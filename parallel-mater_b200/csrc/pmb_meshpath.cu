@@ -325,16 +325,14 @@ struct RangeCtx {
     bool interior_a, interior_b, skip, swept;
 };
 
-__device__ RangeCtx range_ctx(const MeshView& am, const MeshPose& aprev, const MeshPose& as, const Frame& fa,
-                              V3 prev_ref_a, const MeshView& bm, const MeshPose& bprev, const MeshPose& bs,
-                              const Frame& fb, float margin, float dt, bool swept) {
-    RangeCtx c{&am,   &bm,   aprev, as, bprev, bs, fa, fb, prev_ref_a, margin, fmn(margin, 1.0e-3f),
-               dt,    false, false, false, swept};
-    c.skip = frames_guided(fa.flags, fb.flags);
-    const bool a_static = (fa.flags & kFrameStatic) != 0, b_static = (fb.flags & kFrameStatic) != 0;
-    c.interior_a = !c.skip && a_static && point_inside_convex(am, aprev, bprev.x);
-    c.interior_b = !c.skip && b_static && point_inside_convex(bm, bprev, aprev.x);
-    return c;
+
+__device__ __forceinline__ RangeCtx range_ctx_flat(const MeshView& am, const MeshPose& aprev, const MeshPose& as,
+                                                   const Frame& fa, V3 prev_ref_a, const MeshView& bm,
+                                                   const MeshPose& bprev, const MeshPose& bs, const Frame& fb,
+                                                   float margin, float dt, bool swept, bool interior_a,
+                                                   bool interior_b) {
+    return RangeCtx{&am,   &bm,        aprev,      as,    bprev, bs, fa, fb, prev_ref_a, margin, fmn(margin, 1.0e-3f),
+                    dt,    interior_a, interior_b, false, swept};
 }
 
 // The contact of triangle `at` of the body against triangle `bt` of the
@@ -540,96 +538,28 @@ __device__ __noinline__ bool triangle_pair_swept_contact(const RangeCtx& c, uint
     return false;
 }
 
-// geometry.slang:1359-1584 and :1921-2155 over a list of range pairs, one
-// block: the triangle pairs of all the listed ranges, in the reference's
-// order (range pairs in list order; unswept before swept; body triangle
-// outer, collider triangle inner), are spread over the threads a chunk at a
-// time and their contacts merged in that order by thread 0, which keeps the
-// manifold. Block-uniform control flow throughout.
-constexpr uint32_t kLeafBatch = 32;
-struct RangeList {
-    uint32_t af[kLeafBatch], ac[kLeafBatch], bf[kLeafBatch], bc[kLeafBatch];
-    uint32_t count;
-};
-
-constexpr uint32_t kMeshThreads = 128;  // threads per pair on the mesh path
-
-// Thread 0's BVH pair traversal: the stack and the batch of leaf pairs.
-struct Traversal {
-    uint32_t sa[kStack], sb[kStack];
-    uint32_t size;
-    bool overflow;
-    RangeList leaves;
-};
-
-// Per-chunk results of the block's threads, merged in order by thread 0, and
-// the traversal state.
-struct ChunkResults {
-    float4 p[kMeshThreads];   // point, impact fraction
-    float4 n[kMeshThreads];   // normal, depth
-    uint32_t valid[kMeshThreads];
-    Traversal walk;
-};
-
-__device__ void block_ranges(const RangeCtx& c, const RangeList& r, uint32_t tid, ChunkResults& sm, MeshMan& out) {
-    if (c.skip) return;
-    // Each range pair contributes its unswept triangle pairs, then (a swept
-    // pair) its swept ones: the reference's order at a leaf pair.
-    const uint32_t kinds = c.swept ? 2u : 1u;
-    uint32_t total = 0;
-    for (uint32_t i = 0; i < r.count; ++i) total += kinds * r.ac[i] * r.bc[i];
-    const float spacing = fmx(2.0f * c.margin, 1.0e-4f);
-    uint32_t item = 0, item_base = 0;  // the range pair holding flat index `base` starts the search here
-    for (uint32_t base = 0; base < total; base += kMeshThreads) {
-        const uint32_t f = base + tid;
-        bool valid = false;
-        V3 p{0.0f, 0.0f, 0.0f}, n{0.0f, 0.0f, 0.0f};
-        float pen = 0.0f, impact = 1.0f;
-        if (f < total) {
-            uint32_t i = item, first = item_base;
-            while (f >= first + kinds * r.ac[i] * r.bc[i]) {
-                first += kinds * r.ac[i] * r.bc[i];
-                ++i;
-            }
-            const uint32_t size = r.ac[i] * r.bc[i];
-            const uint32_t local = (f - first) % size;
-            const bool swept_item = f - first >= size;
-            const uint32_t at = r.af[i] + local / r.bc[i], bt = r.bf[i] + local % r.bc[i];
-            if (at < c.am->nt && bt < c.bm->nt)
-                valid = swept_item ? triangle_pair_swept_contact(c, at, bt, p, n, pen, impact)
-                                   : triangle_pair_contact(c, at, bt, p, n, pen);
-        }
-        // Advance the search start to the range pair of the next chunk's first index.
-        while (item < r.count && base + kMeshThreads >= item_base + kinds * r.ac[item] * r.bc[item]) {
-            item_base += kinds * r.ac[item] * r.bc[item];
-            ++item;
-        }
-        sm.valid[tid] = valid ? 1u : 0u;
-        sm.p[tid] = f4(p, impact);
-        sm.n[tid] = f4(n, pen);
-        __syncthreads();
-        if (tid == 0) {
-            const uint32_t count = total - base < kMeshThreads ? total - base : kMeshThreads;
-            for (uint32_t k = 0; k < count; ++k)
-                if (sm.valid[k]) mm_add(out, v3(sm.p[k]), v3(sm.n[k]), sm.n[k].w, sm.p[k].w, spacing);
-        }
-        __syncthreads();
-    }
+__device__ __forceinline__ MeshPose pose_prev(const Dev& d, uint32_t i) {
+    return {v3(d.x[i]), q4(d.q[i]), v3(d.v[i]), v3(d.w[i])};
+}
+__device__ __forceinline__ MeshPose pose_pred(const Dev& d, uint32_t i) {
+    return {v3(d.tx[i]), q4(d.tq[i]), v3(d.tv[i]), v3(d.tw[i])};
 }
 
-// Contacts of one range pair (the full pass after a stack overflow is a
-// single range pair over all triangles).
-__device__ void block_range(const RangeCtx& c, uint32_t af, uint32_t ac, uint32_t bf, uint32_t bc, uint32_t tid,
-                            ChunkResults& sm, MeshMan& out) {
-    RangeList r;
-    r.af[0] = af;
-    r.ac[0] = ac;
-    r.bf[0] = bf;
-    r.bc[0] = bc;
-    r.count = 1;
-    block_ranges(c, r, tid, sm, out);
-}
+// The mesh path runs flat over the whole tick rather than per pair:
+//   1. walk (count): one thread per pair -- swept test, root bounds, the BVH
+//      pair traversal of geometry.slang:2156-2299 (children pushed right before
+//      left on a 64-entry stack; an overflow makes the pair one range over all
+//      triangles); counts its overlapping leaf pairs and triangle-pair items
+//      (unswept, then swept for a swept pair, per leaf pair);
+//   2. exclusive scans of both counts;
+//   3. walk (write): the same traversal records each leaf pair and where its
+//      items start;
+//   4. items: one thread per triangle pair evaluates its contact;
+//   5. merge: one thread per pair merges its items' contacts in item order,
+//      which is the reference's order, and stages them.
+constexpr uint32_t kPairSwept = 1u, kPairInteriorA = 2u, kPairInteriorB = 4u;
 
+// A BVH node: bounds, (first, count) of a leaf's triangles, children.
 __device__ __forceinline__ void node_of(const MeshView& m, uint32_t k, V3& lo, V3& hi, uint32_t& first,
                                         uint32_t& count, uint32_t& left, uint32_t& right) {
     const float4 a = m.bvh[3 * k], b = m.bvh[3 * k + 1], c = m.bvh[3 * k + 2];
@@ -641,94 +571,213 @@ __device__ __forceinline__ void node_of(const MeshView& m, uint32_t k, V3& lo, V
     right = __float_as_uint(c.y);
 }
 
-// geometry.slang:2156-2299, one block per pair: every thread runs the
-// (cheap, bounds-only) traversal identically, and the triangle pairs of each
-// batch of overlapping leaf pairs are shared out by block_ranges.
-__device__ void collide_meshes(const MeshView& am, const MeshPose& aprev, const MeshPose& as, const Frame& fa,
-                               V3 prev_ref_a, const MeshView& bm, const MeshPose& bprev, const MeshPose& bs,
-                               const Frame& fb, float margin, float dt, uint32_t tid, ChunkResults& sm,
-                               MeshMan& out) {
-    out.count = 0;
-    const bool swept = mesh_pair_swept(aprev.x, aprev.q, as.x, as.q, am.lo, am.hi, am.solid, bprev.x, bprev.q, bs.x,
-                                       bs.q, bm.lo, bm.hi, bm.solid, margin, frames_guided(fa.flags, fb.flags));
+struct PairSetup {
+    MeshView am, bm;
+    MeshPose aprev, as, bprev, bs;
+    Frame fa, fb;
+    V3 prev_ref_a;
+    float margin;
+};
+
+__device__ PairSetup pair_setup(const Dev& d, uint32_t k) {
+    const uint32_t a = d.cand_a[k], b = d.cand_b[k];
+    PairSetup p;
+    p.am = mesh_view(d, d.mesh[a]);
+    p.bm = mesh_view(d, d.mesh[b]);
+    p.aprev = pose_prev(d, a);
+    p.as = pose_pred(d, a);
+    p.bprev = pose_prev(d, b);
+    p.bs = pose_pred(d, b);
+    p.fa = frame_of(d, a);
+    p.fb = frame_of(d, b);
+    p.prev_ref_a = d.nj ? v3(d.frame_prev[a]) : v3(d.x[a]);
+    p.margin = d.p2[a].z + d.p2[b].z;
+    return p;
+}
+
+// Steps 1 and 3. kWrite: record the leaf pairs from leaf_base on, their
+// items from item_base on.
+template <bool kWrite>
+__device__ void mesh_walk(const Dev& d, const PairSetup& p, uint32_t pair, bool swept, uint32_t leaf_base,
+                          uint32_t item_base, uint32_t& leaves, uint32_t& items) {
+    leaves = items = 0;
+    const uint32_t kinds = swept ? 2u : 1u;
     const BoundsXf zero_xf{};
-    const BoundsXf pxa = swept ? bounds_xf(aprev.x, aprev.q) : zero_xf;
-    const BoundsXf pxb = swept ? bounds_xf(bprev.x, bprev.q) : zero_xf;
-    const BoundsXf xa = bounds_xf(as.x, as.q), xb = bounds_xf(bs.x, bs.q);
-    V3 alo, ahi, blo, bhi;
-    motion_bounds(am.lo, am.hi, pxa, xa, swept, margin, alo, ahi);
-    motion_bounds(bm.lo, bm.hi, pxb, xb, swept, 0.0f, blo, bhi);
-    if (!bounds_overlap(alo, ahi, blo, bhi)) return;
-    const RangeCtx ctx = range_ctx(am, aprev, as, fa, prev_ref_a, bm, bprev, bs, fb, margin, dt, swept);
-    // Thread 0 walks the BVH pair stack (in shared memory) and collects the
-    // overlapping leaf pairs in visit order; each batch is evaluated by the
-    // whole block, merging in visit order.
-    Traversal& t = sm.walk;
-    if (tid == 0) {
-        t.sa[0] = 0;
-        t.sb[0] = 0;
-        t.size = 1;
-        t.overflow = am.nodes == 0 || bm.nodes == 0;
-        t.leaves.count = 0;
-    }
-    __syncthreads();
-    bool overflow = false;
-    for (;;) {
-        if (tid == 0) {
-            t.leaves.count = 0;
-            while (t.size > 0 && !t.overflow && t.leaves.count < kLeafBatch) {
-                const uint32_t na = t.sa[--t.size], nb = t.sb[t.size];
-                uint32_t af, ac, al, ar, bf, bc, bl, br;
-                V3 nlo, nhi, mlo, mhi;
-                node_of(am, na, nlo, nhi, af, ac, al, ar);
-                node_of(bm, nb, mlo, mhi, bf, bc, bl, br);
-                motion_bounds(nlo, nhi, pxa, xa, swept, margin, alo, ahi);
-                motion_bounds(mlo, mhi, pxb, xb, swept, 0.0f, blo, bhi);
-                if (!bounds_overlap(alo, ahi, blo, bhi)) continue;
-                const bool la = ac != 0, lb = bc != 0;
-                if (la && lb) {
-                    const uint32_t k = t.leaves.count++;
-                    t.leaves.af[k] = af;
-                    t.leaves.ac[k] = ac;
-                    t.leaves.bf[k] = bf;
-                    t.leaves.bc[k] = bc;
-                    continue;
-                }
-                const uint32_t need = la || lb ? 2u : 4u;
-                if (t.size + need > kStack) {
-                    t.overflow = true;
-                    break;
-                }
-                uint32_t z = t.size;
-                if (la) {
-                    t.sa[z] = na; t.sb[z++] = br;
-                    t.sa[z] = na; t.sb[z++] = bl;
-                } else if (lb) {
-                    t.sa[z] = ar; t.sb[z++] = nb;
-                    t.sa[z] = al; t.sb[z++] = nb;
-                } else {
-                    t.sa[z] = ar; t.sb[z++] = br;
-                    t.sa[z] = ar; t.sb[z++] = bl;
-                    t.sa[z] = al; t.sb[z++] = br;
-                    t.sa[z] = al; t.sb[z++] = bl;
-                }
-                t.size = z;
-            }
+    const BoundsXf pxa = swept ? bounds_xf(p.aprev.x, p.aprev.q) : zero_xf;
+    const BoundsXf pxb = swept ? bounds_xf(p.bprev.x, p.bprev.q) : zero_xf;
+    const BoundsXf xa = bounds_xf(p.as.x, p.as.q), xb = bounds_xf(p.bs.x, p.bs.q);
+    auto emit = [&](uint32_t af, uint32_t ac, uint32_t bf, uint32_t bc) {
+        if (kWrite && leaf_base + leaves < d.cap_mesh_leaves) {
+            d.ml_rec[leaf_base + leaves] = make_uint4(af, ac, bf, bc);
+            d.ml_item[leaf_base + leaves] = item_base + items;
+            d.ml_pair[leaf_base + leaves] = pair;
         }
-        __syncthreads();
-        overflow = t.overflow;
-        const bool more = t.size > 0;
-        const uint32_t batch = t.leaves.count;
-        __syncthreads();  // every thread has the state before thread 0 moves on
-        if (overflow) break;
-        if (batch) block_ranges(ctx, t.leaves, tid, sm, out);  // reads the batch, ends with a barrier
-        if (!more) break;
+        ++leaves;
+        items += kinds * ac * bc;
+    };
+    uint32_t sa[kStack], sb[kStack];
+    sa[0] = 0;
+    sb[0] = 0;
+    uint32_t size = 1;
+    bool overflow = p.am.nodes == 0 || p.bm.nodes == 0;
+    while (size > 0 && !overflow) {
+        --size;
+        const uint32_t na = sa[size], nb = sb[size];
+        uint32_t af, ac, al, ar, bf, bc, bl, br;
+        V3 nlo, nhi, mlo, mhi, alo, ahi, blo, bhi;
+        node_of(p.am, na, nlo, nhi, af, ac, al, ar);
+        node_of(p.bm, nb, mlo, mhi, bf, bc, bl, br);
+        motion_bounds(nlo, nhi, pxa, xa, swept, p.margin, alo, ahi);
+        motion_bounds(mlo, mhi, pxb, xb, swept, 0.0f, blo, bhi);
+        if (!bounds_overlap(alo, ahi, blo, bhi)) continue;
+        const bool la = ac != 0, lb = bc != 0;
+        if (la && lb) {
+            emit(af, ac, bf, bc);
+            continue;
+        }
+        const uint32_t need = la || lb ? 2u : 4u;
+        if (size + need > kStack) {
+            overflow = true;
+            break;
+        }
+        if (la) {
+            sa[size] = na; sb[size++] = br;
+            sa[size] = na; sb[size++] = bl;
+        } else if (lb) {
+            sa[size] = ar; sb[size++] = nb;
+            sa[size] = al; sb[size++] = nb;
+        } else {
+            sa[size] = ar; sb[size++] = br;
+            sa[size] = ar; sb[size++] = bl;
+            sa[size] = al; sb[size++] = br;
+            sa[size] = al; sb[size++] = bl;
+        }
     }
     if (overflow) {
-        out.count = 0;
-        block_range(ctx, 0, am.nt, 0, bm.nt, tid, sm, out);
+        // The reference clears the manifold and runs every triangle pair.
+        leaves = items = 0;
+        emit(0, p.am.nt, 0, p.bm.nt);
     }
-    __syncthreads();  // the traversal state is reused by the block's next pair
+}
+
+__global__ void k_mesh_walk_count(Dev d) {
+    const uint32_t total = min(d.ctr->n_mesh, d.cap_mesh);
+    for (uint32_t s = grid_stride_begin(); s < total; s += grid_stride()) {
+        const PairSetup p = pair_setup(d, d.np_mesh[s]);
+        uint32_t leaves = 0, items = 0, flags = 0;
+        const bool guided = frames_guided(p.fa.flags, p.fb.flags);
+        const bool swept = mesh_pair_swept(p.aprev.x, p.aprev.q, p.as.x, p.as.q, p.am.lo, p.am.hi, p.am.solid,
+                                           p.bprev.x, p.bprev.q, p.bs.x, p.bs.q, p.bm.lo, p.bm.hi, p.bm.solid,
+                                           p.margin, guided);
+        const BoundsXf zero_xf{};
+        V3 alo, ahi, blo, bhi;
+        motion_bounds(p.am.lo, p.am.hi, swept ? bounds_xf(p.aprev.x, p.aprev.q) : zero_xf,
+                      bounds_xf(p.as.x, p.as.q), swept, p.margin, alo, ahi);
+        motion_bounds(p.bm.lo, p.bm.hi, swept ? bounds_xf(p.bprev.x, p.bprev.q) : zero_xf,
+                      bounds_xf(p.bs.x, p.bs.q), swept, 0.0f, blo, bhi);
+        // A guided pair gets no contacts here (its ranges return at once).
+        if (!guided && bounds_overlap(alo, ahi, blo, bhi)) {
+            mesh_walk<false>(d, p, s, swept, 0, 0, leaves, items);
+            flags = swept ? kPairSwept : 0u;
+            if ((p.fa.flags & kFrameStatic) && point_inside_convex(p.am, p.aprev, p.bprev.x)) flags |= kPairInteriorA;
+            if ((p.fb.flags & kFrameStatic) && point_inside_convex(p.bm, p.bprev, p.aprev.x)) flags |= kPairInteriorB;
+        }
+        d.mp_leaves[s] = leaves;
+        d.mp_items[s] = items;
+        d.mp_flags[s] = flags;
+    }
+    if (grid_stride_begin() == 0 && d.ctr->n_mesh > d.cap_mesh) atomicOr(&d.ctr->status, kStPairOverflow);
+}
+
+__global__ void k_mesh_walk_write(Dev d) {
+    const uint32_t total = min(d.ctr->n_mesh, d.cap_mesh);
+    for (uint32_t s = grid_stride_begin(); s < total; s += grid_stride()) {
+        if (!d.mp_leaves[s]) continue;
+        const PairSetup p = pair_setup(d, d.np_mesh[s]);
+        uint32_t leaves, items;
+        mesh_walk<true>(d, p, s, (d.mp_flags[s] & kPairSwept) != 0, d.mp_leaf_off[s], d.mp_item_off[s], leaves,
+                        items);
+    }
+    if (grid_stride_begin() == 0 &&
+        (d.ctr->n_mesh_leaves > d.cap_mesh_leaves || d.ctr->n_mesh_items > d.cap_mesh_items))
+        atomicOr(&d.ctr->status, kStContactOverflow);
+}
+
+// One warp per leaf pair (a leaf pair has at most 2 x 4 x 4 items; the
+// single range of an overflowed traversal has more and loops), one lane per
+// triangle-pair item.
+__global__ void __launch_bounds__(128, 4) k_mesh_items(Dev d, StepParams sp) {
+    const uint32_t leaves_total = min(d.ctr->n_mesh_leaves, d.cap_mesh_leaves);
+    const uint32_t items_total = min(d.ctr->n_mesh_items, d.cap_mesh_items);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < leaves_total; j += warps) {
+        const uint32_t s = d.ml_pair[j];
+        const uint4 rec = d.ml_rec[j];
+        const uint32_t flags = d.mp_flags[s];
+        const bool swept = (flags & kPairSwept) != 0;
+        const uint32_t size = rec.y * rec.w, count = (swept ? 2u : 1u) * size, base = d.ml_item[j];
+        if (!size) continue;
+        const PairSetup p = pair_setup(d, d.np_mesh[s]);
+        const RangeCtx c = range_ctx_flat(p.am, p.aprev, p.as, p.fa, p.prev_ref_a, p.bm, p.bprev, p.bs, p.fb, p.margin,
+                                          sp.dt, swept, (flags & kPairInteriorA) != 0, (flags & kPairInteriorB) != 0);
+        for (uint32_t local = lane; local < count; local += 32) {
+            const uint32_t f = base + local;
+            if (f >= items_total) break;
+            const uint32_t t = local % size;
+            const uint32_t at = rec.x + t / rec.w, bt = rec.z + t % rec.w;
+            V3 cp{0.0f, 0.0f, 0.0f}, cn{0.0f, 0.0f, 0.0f};
+            float pen = 0.0f, impact = 1.0f;
+            bool valid = false;
+            if (at < p.am.nt && bt < p.bm.nt)
+                valid = local >= size ? triangle_pair_swept_contact(c, at, bt, cp, cn, pen, impact)
+                                      : triangle_pair_contact(c, at, bt, cp, cn, pen);
+            d.mi_valid[f] = valid ? 1u : 0u;
+            d.mi_p[f] = f4(cp, impact);
+            d.mi_n[f] = f4(cn, pen);
+        }
+    }
+}
+
+// One thread per pair: its items' contacts merged in item order (the
+// reference's), then staged like the face path's.
+__global__ void k_mesh_merge(Dev d, StepParams sp) {
+    const uint32_t pairs = min(d.ctr->n_mesh, d.cap_mesh);
+    const uint32_t total = min(d.ctr->n_mesh_items, d.cap_mesh_items);
+    for (uint32_t s = grid_stride_begin(); s < pairs; s += grid_stride()) {
+        const uint32_t k = d.np_mesh[s];
+        const uint32_t i0 = d.mp_item_off[s], i1 = d.mp_item_off[s + 1];
+        MeshMan m;
+        m.count = 0;
+        if (i1 > total) {
+            // Items past the capacity were not evaluated (overflow reported).
+            d.np_count[k] = 0;
+            d.np_scan[k] = 0ull;
+            continue;
+        }
+        const float spacing = fmx(2.0f * (d.p2[d.cand_a[k]].z + d.p2[d.cand_b[k]].z), 1.0e-4f);
+        for (uint32_t f = i0; f < i1; ++f) {
+            if (!d.mi_valid[f]) continue;
+            const float4 pv = d.mi_p[f], nv = d.mi_n[f];
+            mm_add(m, v3(pv), v3(nv), nv.w, pv.w, spacing);
+        }
+        const uint32_t count = m.count;
+        d.np_count[k] = count;
+        d.np_scan[k] = count ? ((uint64_t(1) << 32) | count) : 0ull;
+        if (!count) continue;
+        const uint32_t slot = atomicAdd(&d.ctr->n_stage, count);
+        if (slot + count > d.cap_stage) {
+            atomicOr(&d.ctr->status, kStContactOverflow);
+            d.np_scan[k] = 0ull;
+            d.np_count[k] = 0;
+            continue;
+        }
+        d.np_stage[k] = slot;
+        for (uint32_t p = 0; p < count; ++p) {
+            d.st_n[slot + p] = f4(m.n[p], m.pen[p]);
+            d.st_p[slot + p] = f4(m.p[p], m.impact[p]);
+        }
+    }
 }
 
 // The frame of body i at one set of poses (pos/rot: the predicted or the
@@ -777,47 +826,6 @@ __global__ void k_hinge_frames(Dev d) {
     }
 }
 
-__device__ __forceinline__ MeshPose pose_prev(const Dev& d, uint32_t i) {
-    return {v3(d.x[i]), q4(d.q[i]), v3(d.v[i]), v3(d.w[i])};
-}
-__device__ __forceinline__ MeshPose pose_pred(const Dev& d, uint32_t i) {
-    return {v3(d.tx[i]), q4(d.tq[i]), v3(d.tv[i]), v3(d.tw[i])};
-}
-
-// One block per candidate on the triangle-mesh path; thread 0 stages the
-// contacts like the face path's (per-contact normals).
-__global__ void __launch_bounds__(kMeshThreads, 4) k_narrow_mesh(Dev d, StepParams sp) {
-    __shared__ ChunkResults sm;
-    const uint32_t total = d.ctr->n_mesh;
-    const uint32_t tid = threadIdx.x;
-    for (uint32_t s = blockIdx.x; s < total; s += gridDim.x) {
-        const uint32_t k = d.np_mesh[s];
-        const uint32_t a = d.cand_a[k], b = d.cand_b[k];
-        const MeshView am = mesh_view(d, d.mesh[a]), bm = mesh_view(d, d.mesh[b]);
-        const float margin = d.p2[a].z + d.p2[b].z;
-        MeshMan m;
-        const V3 prev_ref_a = d.nj ? v3(d.frame_prev[a]) : v3(d.x[a]);
-        collide_meshes(am, pose_prev(d, a), pose_pred(d, a), frame_of(d, a), prev_ref_a, bm, pose_prev(d, b),
-                       pose_pred(d, b), frame_of(d, b), margin, sp.dt, tid, sm, m);
-        if (tid != 0) continue;
-        const uint32_t count = m.count;
-        d.np_count[k] = count;
-        d.np_scan[k] = count ? ((uint64_t(1) << 32) | count) : 0ull;
-        if (!count) continue;
-        const uint32_t slot = atomicAdd(&d.ctr->n_stage, count);
-        if (slot + count > d.cap_stage) {
-            atomicOr(&d.ctr->status, kStContactOverflow);
-            d.np_scan[k] = 0ull;
-            d.np_count[k] = 0;
-            continue;
-        }
-        d.np_stage[k] = slot;
-        for (uint32_t p = 0; p < count; ++p) {
-            d.st_n[slot + p] = f4(m.n[p], m.pen[p]);
-            d.st_p[slot + p] = f4(m.p[p], m.impact[p]);
-        }
-    }
-}
 
 }  // namespace
 
@@ -828,8 +836,22 @@ void launch_hinge_frames(const Dev& d, cudaStream_t s) {
 }
 
 void launch_mesh_narrowphase(const Dev& d, const StepParams& sp, cudaStream_t s) {
-    k_narrow_mesh<<<8 * kGridSms, kMeshThreads, 0, s>>>(d, sp);
-    note_launch(8 * kGridSms);
+    const uint32_t pairs_grid = cap_blocks(d.cap_mesh, 128);
+    k_mesh_walk_count<<<pairs_grid, 128, 0, s>>>(d);
+    note_launch(pairs_grid);
+    prof_mark(s, "mesh walk");
+    scan_u32(d.mp_leaves, d.mp_leaf_off, &d.ctr->n_mesh, d.cap_mesh, &d.ctr->n_mesh_leaves, d.scan_tmp32, s);
+    scan_u32(d.mp_items, d.mp_item_off, &d.ctr->n_mesh, d.cap_mesh, &d.ctr->n_mesh_items, d.scan_tmp32, s);
+    prof_mark(s, "mesh scans");
+    k_mesh_walk_write<<<pairs_grid, 128, 0, s>>>(d);
+    note_launch(pairs_grid);
+    prof_mark(s, "mesh leaf pairs");
+    const uint32_t items_grid = cap_blocks(32 * size_t(d.cap_mesh_leaves), 128);
+    k_mesh_items<<<items_grid, 128, 0, s>>>(d, sp);
+    note_launch(items_grid);
+    prof_mark(s, "mesh triangle pairs");
+    k_mesh_merge<<<pairs_grid, 128, 0, s>>>(d, sp);
+    note_launch(pairs_grid);
 }
 
 }  // namespace pmb

@@ -53,6 +53,7 @@ struct Counters {
     uint32_t n_surv;      // narrowphase candidates left for the manifold pass
     uint32_t n_events;    // contact events recorded by the tick
     uint32_t n_mesh;      // candidates left for the triangle-mesh path
+    uint32_t n_mesh_leaves, n_mesh_items;  // their overlapping leaf pairs and triangle-pair items
     uint32_t claim[2];    // solve policy 3: next unclaimed body of the colour (alternating)
     // Bodies bucketed by (colour, width class): bucket col * kWidthClasses + k.
     uint32_t color_count[kMaxColors * kWidthClasses];
@@ -179,6 +180,15 @@ struct Dev {
     float4 *frame, *frame_prev;  // at the predicted and at the previous poses
     uint32_t *jb_off, *jb_list;
     uint32_t* np_mesh;  // candidates for the triangle-mesh path
+    // the flat mesh path: per pair leaf-pair and item counts, their exclusive
+    // scans and flags; per leaf pair (first, count) of both ranges and its
+    // first item; per item the contact (point, impact), (normal, depth)
+    uint32_t cap_mesh, cap_mesh_leaves, cap_mesh_items;
+    uint32_t *mp_leaves, *mp_items, *mp_flags, *mp_leaf_off, *mp_item_off;
+    uint4* ml_rec;
+    uint32_t *ml_item, *ml_pair;
+    uint8_t* mi_valid;
+    float4 *mi_p, *mi_n;
     // AVBD body state
     float4 *dxl, *dxa, *dq;
     float4 *inA, *inB;  // inertia block: (m/dt2, h33, h43, h44), (h53, h54, h55, -)
