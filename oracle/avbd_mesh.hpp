@@ -13,12 +13,13 @@
 //   BVH pair traversal              :2156-2299 (rigid_collide_meshes)
 //   bounds transforms               src/slang/math.slang:43-49, :142-190
 //   swept triangle ranges           :1921-2155
+//   guided contacts                 :1118-1127 (guide direction), :1129-1170
 // What is restated: the BVH traversal of rigid_collide_meshes with the
 // unswept triangle ranges and, for a pair that moved more than its
-// threshold, the swept ranges (conservative advancement) after them at each
-// leaf pair; the per-body hinge frame fields those ranges read. Not restated:
-// guided contacts (a body on an unbreakable slider or piston to a static body
-// against a static body), which such pairs therefore do not get.
+// threshold (or a guided pair: a body on an unbreakable slider or piston to
+// a static body, against a static body), the swept ranges (conservative
+// advancement) after them at each leaf pair, guided contacts merged by guide
+// direction; the per-body hinge frames those ranges read.
 #pragma once
 #include <vector>
 
@@ -30,13 +31,26 @@ namespace oracle {
 // read, and the body's reference point (the hinge anchor of a non-axial
 // hinge member, else its position).
 template <class R> struct HingeFrame {
-    V3<R> anchor, reference;
-    bool present{}, axial{}, fixed_member{}, static_body{};
+    V3<R> anchor, reference, axis;
+    R inv_mass{}, inv_moment{};
+    bool present{}, fixed{}, axial{}, axial_rotation{}, fixed_member{}, static_body{};
 };
 
-// geometry.slang:404-492 (the anchor and flags; axis, guide mass and moment
-// only feed guided contacts). `joints_of_body`: the body's joints in
-// ascending index.
+// geometry.slang:384-402: the inverse moment of a body turning about its
+// guide axis through the anchor (pistons; zero otherwise).
+template <class R> inline R fixed_hinge_inverse_moment(const BodyDesc& b, const State<R>& s, const HingeFrame<R>& f) {
+    if ((!f.fixed && !f.axial_rotation) || !(R(b.inv_mass) > kEps<R>())) return R(0);
+    const V3<R> l = inv_rotate(s.q, f.axis);
+    const R center = l.x * l.x / mx(R(b.inv_inertia[0]), kEps<R>()) + l.y * l.y / mx(R(b.inv_inertia[1]), kEps<R>()) +
+                     l.z * l.z / mx(R(b.inv_inertia[2]), kEps<R>());
+    const V3<R> arm = sub(s.x, f.anchor);
+    const V3<R> perp = sub(arm, mul(f.axis, dot(arm, f.axis)));
+    const R pivot = center + len2(perp) / R(b.inv_mass);
+    return pivot > kEps<R>() ? R(1) / pivot : R(0);
+}
+
+// geometry.slang:404-492. `joints_of_body`: the body's joints in ascending
+// index.
 template <class R>
 inline HingeFrame<R> hinge_frame(const World<R>& w, const std::vector<State<R>>& st, uint32_t i,
                                  const std::vector<uint32_t>& joints_of_body) {
@@ -59,18 +73,30 @@ inline HingeFrame<R> hinge_frame(const World<R>& w, const std::vector<State<R>>&
         const bool static_anchor = other < w.n && w.body[other].motion == kStatic;
         if (f.present || (j.d.type != kHinge && !(axial && static_anchor && !(j.d.breaking_threshold > 0.0f))))
             continue;
+        const V3<R> local_axis = axial ? V3<R>{1, 0, 0} : V3<R>{0, 0, 1};
         const float* la = is_a ? j.d.anchor_a : j.d.anchor_b;
+        const Q4<R> lq = q4<R>(is_a ? j.d.frame_a : j.d.frame_b);
         f.anchor = add(st[i].x, rotate(st[i].q, v3<R>(la)));
+        f.axis = normalized_or(rotate(qmul(st[i].q, lq), local_axis), local_axis);
         f.present = true;
+        f.fixed = static_anchor && !axial;
         f.axial = static_anchor && axial;
+        f.axial_rotation = f.axial && j.d.type == kPiston;
         if (static_anchor) {
             const float* lo = is_a ? j.d.anchor_b : j.d.anchor_a;
+            const Q4<R> oq = q4<R>(is_a ? j.d.frame_b : j.d.frame_a);
             f.anchor = add(st[other].x, rotate(st[other].q, v3<R>(lo)));
+            f.axis = normalized_or(rotate(qmul(st[other].q, oq), local_axis), f.axis);
         }
     }
     if (f.axial && incident != 1u) {
         f.axial = false;
+        f.axial_rotation = false;
         f.present = false;
+    }
+    if (f.axial) {
+        f.inv_mass = R(w.body[i].inv_mass);
+        f.inv_moment = fixed_hinge_inverse_moment(w.body[i], st[i], f);
     }
     f.reference = f.present && !f.axial ? f.anchor : st[i].x;
     return f;
@@ -92,6 +118,61 @@ template <class R> inline std::vector<HingeFrame<R>> hinge_frames(const World<R>
 // geometry.slang:373-377
 template <class R> inline bool guided_pair(const HingeFrame<R>& a, const HingeFrame<R>& b) {
     return (a.axial && b.static_body) || (b.axial && a.static_body);
+}
+
+// geometry.slang:1118-1127: a guided contact's direction in the guide's
+// (translation, rotation) coordinates, scaled by the guide's inverse mass
+// and moment.
+template <class R> inline V3<R> guide_direction(V3<R> n, V3<R> p, const HingeFrame<R>& g) {
+    return {dot(n, g.axis) * std::sqrt(g.inv_mass),
+            g.axial_rotation ? dot(g.axis, cross(sub(p, g.anchor), n)) * std::sqrt(g.inv_moment) : R(0), R(0)};
+}
+
+// geometry.slang:1129-1170, the guided merge: a contact whose guide
+// direction is too weak is dropped; among impacts only the earliest
+// (within 1e-4 of the tick) are kept; a contact with the direction of a kept
+// one replaces it when deeper per unit direction; else it is added (a ninth
+// replaces the shallowest).
+template <class R> inline void add_guided_contact(Manifold<R>& m, const Contact<R>& c, const HingeFrame<R>& g) {
+    const V3<R> cd = guide_direction(c.normal, c.point, g);
+    const R cl = len(cd);
+    if (cl * cl <= kEps<R>()) return;
+    if (c.impact_fraction > R(0)) {
+        R first = R(1);
+        for (uint32_t i = 0; i < m.count; ++i)
+            if (m.c[i].impact_fraction > R(0)) first = mn(first, m.c[i].impact_fraction);
+        if (c.impact_fraction > first + R(1.0e-4)) return;
+        if (c.impact_fraction < first - R(1.0e-4)) {
+            uint32_t kept = 0;
+            for (uint32_t i = 0; i < m.count; ++i)
+                if (m.c[i].impact_fraction == R(0)) m.c[kept++] = m.c[i];
+            m.count = kept;
+        }
+    }
+    for (uint32_t i = 0; i < m.count; ++i) {
+        const V3<R> d = guide_direction(m.c[i].normal, m.c[i].point, g);
+        const R size = len(d);
+        if (dot(cd, d) > R(0.9999) * cl * size) {
+            if (c.penetration / cl > m.c[i].penetration / size) m.c[i] = c;
+            return;
+        }
+    }
+    if (m.count < 8) {
+        m.c[m.count++] = c;
+        return;
+    }
+    uint32_t sh = 0;
+    for (uint32_t i = 1; i < m.count; ++i)
+        if (m.c[i].penetration < m.c[sh].penetration) sh = i;
+    if (c.penetration > m.c[sh].penetration) m.c[sh] = c;
+}
+
+// geometry.slang:1910-1919
+template <class R> inline bool triangle_pair_face_contact(const V3<R> a[3], const V3<R> b[3], V3<R> sep) {
+    const V3<R> n = normalized_or(sep, V3<R>{});
+    const V3<R> fa = normalized_or(cross(sub(a[1], a[0]), sub(a[2], a[0])), V3<R>{});
+    const V3<R> fb = normalized_or(cross(sub(b[1], b[0]), sub(b[2], b[0])), V3<R>{});
+    return ab(dot(n, fa)) > R(0.9999) || ab(dot(n, fb)) > R(0.9999);
 }
 
 // geometry.slang:949-997
@@ -475,8 +556,9 @@ inline void collide_triangle_ranges_swept(const Mesh<R>& am, const State<R>& apr
                                           const Mesh<R>& bm, const State<R>& bprev, const State<R>& bs,
                                           const HingeFrame<R>& bh, uint32_t bf, uint32_t bc, R margin, R dt,
                                           Manifold<R>& out) {
-    if (guided_pair(ah, bh)) return;  // guided contacts are not restated
-    const R rest = mn(margin, R(1.0e-3));
+    const bool guided = guided_pair(ah, bh);
+    const HingeFrame<R>& guide = ah.axial ? ah : bh;
+    const R rest = guided ? mn(margin, R(1.0e-4)) : mn(margin, R(1.0e-3));
     const bool interior_a = ah.static_body && point_inside_convex(am, aprev, bprev.x);
     const bool interior_b = bh.static_body && point_inside_convex(bm, bprev, aprev.x);
     const uint32_t a_tris = uint32_t(am.idx.size() / 3), b_tris = uint32_t(bm.idx.size() / 3);
@@ -542,7 +624,15 @@ inline void collide_triangle_ranges_swept(const Mesh<R>& am, const State<R>& apr
                 closest_triangle_pair(A, B, pa, pb);
                 const V3<R> delta = sub(pa, pb);
                 const R dist = std::sqrt(mx(R(0), len2(delta)));
-                const R offset = rest;
+                R offset = rest;
+                if (guided && !triangle_pair_face_contact(A, B, delta)) {
+                    // A witness off the guide's face, with both an axial and a
+                    // turning component, is held at zero offset.
+                    const V3<R> dir = normalized_or(delta, V3<R>{});
+                    const R axial = dot(dir, guide.axis);
+                    const R angular = dot(guide.axis, cross(sub(pa, guide.anchor), dir));
+                    if (ab(axial) > R(1.0e-3) && ab(angular) > R(1.0e-3)) offset = R(0);
+                }
                 if (it == 0) {
                     starts_near = dist <= offset + R(5.0e-5);
                     // A gap wider than the largest relative motion of the tick
@@ -579,12 +669,32 @@ inline void collide_triangle_ranges_swept(const Mesh<R>& am, const State<R>& apr
                     c.penetration = mx(R(0), remaining + offset) + R(1.0e-5);
                     c.impact_fraction = starts_near ? R(0) : time;
                     c.init_speed = speed;
-                    add_contact(out, c, mx(margin * R(2), R(1.0e-4)));
+                    if (guided)
+                        add_guided_contact(out, c, guide);
+                    else
+                        add_contact(out, c, mx(margin * R(2), R(1.0e-4)));
                     break;
                 }
                 sep_n = triangle_feature_normal(A, B, pa, pb, normalized_or(delta, V3<R>{0, 1, 0}));
                 have_sep = true;
-                const R adv = (dist - offset) / (bound + kEps<R>()) * R(0.9);
+                R adv = (dist - offset) / (bound + kEps<R>()) * R(0.9);
+                if (guided) {
+                    // Advance by the gap along the separating feature plane
+                    // when that is faster; a separating, opening gap ends it.
+                    const V3<R> plane = triangle_feature_normal(A, B, pa, pb, sep_n);
+                    R min_a = R(3.402823466e38), max_b = R(-3.402823466e38);
+                    R min_va = R(3.402823466e38), max_vb = R(-3.402823466e38);
+                    for (uint32_t k = 0; k < 3; ++k) {
+                        min_a = mn(min_a, dot(sub(A[k], pb), plane));
+                        max_b = mx(max_b, dot(sub(B[k], pb), plane));
+                        min_va = mn(min_va, dot(DA[k], plane));
+                        max_vb = mx(max_vb, dot(DB[k], plane));
+                    }
+                    const R gap = min_a - max_b - offset;
+                    const R closing = max_vb - min_va;
+                    if (gap > R(1.0e-5) && closing <= R(0)) break;
+                    if (gap > R(0) && closing > kEps<R>()) adv = mx(adv, R(0.9) * gap / closing);
+                }
                 time += mx(adv, R(1.0e-5));
                 if (time > R(1)) break;
             }

@@ -168,6 +168,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
         }
         // A pair the face path declines goes to the triangle-mesh path.
         if (!face) collide_meshes(w, a, b, prev, pred, frames[a], frames[b], prev_frames[a].reference, dt, m);
+        m.guided = guided_pair(frames[a], frames[b]);
         if (m.count == 0) continue;
         bool persistent = face_capable(bm) && (!dynamic(w, b) || face_capable(cm));
         for (uint32_t p = 0; p < m.count; ++p) {
@@ -280,7 +281,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
                                                   sub(rotate(prev[b].q, c.anchor_b), rotate(prev[a].q, c.anchor_a)));
             V3<R> terr = add(anchor_motion, mul(old_delta, R(1) - K<R>::alpha));
             c.init_speed = -closing / dt;
-            R skin = contact_skin<R>(w.body[a], w.body[b]);
+            R skin = contact_skin<R>(w.body[a], w.body[b], m.guided);
             R impact_disp = realtime && c.cached == 0 && c.init_speed < R(-0.1)
                                 ? -(R(1) + mn(R(w.body[a].restitution), R(w.body[b].restitution))) * c.init_speed * dt
                                 : R(0);

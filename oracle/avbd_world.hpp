@@ -110,6 +110,7 @@ template <class R> struct Manifold {
     Contact<R> c[8];
     uint32_t count{};
     uint32_t next_a{kInvalid}, next_b{kInvalid};
+    bool guided{};  // a guided pair's contacts (geometry_constraints.slang:327-333)
 };
 template <class R> struct JointRt {
     JointDesc d{};
@@ -680,8 +681,10 @@ template <class R> inline void basis(V3<R> n, V3<R>& t0, V3<R>& t1) {
 template <class R> inline R pair_stiffness(const BodyDesc& a, const BodyDesc& b, R dt) {
     return R(1) / (mx(R(a.inv_mass) + R(b.inv_mass), R(1.0e-6)) * dt * dt);
 }
-template <class R> inline R contact_skin(const BodyDesc& a, const BodyDesc& b) {
-    return mn(R(a.margin) + R(b.margin), R(1.0e-3)) + R(2) * R(1.0e-5);
+// geometry_constraints.slang:438-446: a guided contact rests at the guided
+// offset (1e-4 m), any other at the rest offset (1e-3 m).
+template <class R> inline R contact_skin(const BodyDesc& a, const BodyDesc& b, bool guided = false) {
+    return mn(R(a.margin) + R(b.margin), guided ? R(1.0e-4) : R(1.0e-3)) + R(2) * R(1.0e-5);
 }
 template <class R> inline Vec6<R> jac(V3<R> l, V3<R> a) { return {{l.x, l.y, l.z, a.x, a.y, a.z}}; }
 
@@ -925,7 +928,7 @@ template <class R> inline bool contact_impact(const Manifold<R>& m, const BodyDe
     bool impact = false;
     for (uint32_t p = 0; p < m.count; ++p) {
         const Contact<R>& c = m.c[p];
-        R skin = contact_skin<R>(a, b);
+        R skin = contact_skin<R>(a, b, m.guided);
         bool fresh = (c.cached == 0 || c.dual[0].lambda <= R(1.0e-6) ||
                       (c.impact_fraction > R(0) && c.impact_fraction < R(1))) &&
                      c.init_speed < R(-0.1) && c.penetration >= R(-1.0e-5);

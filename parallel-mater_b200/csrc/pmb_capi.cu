@@ -311,6 +311,7 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     ALLOCP(d.m_bvh, 3 * z.bvh_nodes); ALLOCP(d.m_shell, z.shell_normals);
     ALLOCP(d.jb_off, nj ? size_t(n) + 1 : 0); ALLOCP(d.jb_list, 2 * size_t(nj)); ALLOC(d.frame, nj ? size_t(n) : 0);
     ALLOC(d.frame_prev, nj ? size_t(n) : 0);
+    ALLOC(d.frame_guide, nj ? size_t(n) : 0); ALLOC(d.frame_anchor, nj ? size_t(n) : 0);
     ALLOC(d.np_mesh, cap_cand);
     d.cap_mesh = uint32_t(cap_pair);
     d.cap_mesh_leaves = d.cap_mesh_items = uint32_t(cap_contact);

@@ -12,9 +12,10 @@
 // non-convex meshes (:1292-1306, :1855-1908) -- merged into at most eight
 // contacts (:1129-1220); for a pair that moved more than its threshold, the
 // swept triangle ranges (:1921-2155, conservative advancement) after the
-// unswept ones at each leaf pair. Guided contacts (a body on an unbreakable
-// slider or piston to a static body, against a static body) are not built:
-// such pairs get no contacts.
+// unswept ones at each leaf pair. A guided pair (a body on an unbreakable
+// slider or piston to a static body, against a static body) takes only the
+// swept ranges, with the guided offsets and advancement, and its contacts
+// merge by guide direction (:1118-1170).
 //
 // One block per pair on the path: the traversal runs identically in every
 // thread and the triangle pairs of each batch of leaf pairs are spread over
@@ -315,6 +316,14 @@ __device__ __forceinline__ Frame frame_of(const Dev& d, uint32_t i) {
 
 
 // The pair-invariant inputs of the triangle ranges (geometry.slang:1359-1379).
+// The guide of a guided pair: its axial member's anchor, axis, inverse mass
+// and moment, and whether it may turn about the axis (a piston).
+struct Guide {
+    V3 anchor, axis;
+    float inv_mass, inv_moment;
+    bool rotation;
+};
+
 struct RangeCtx {
     const MeshView* am;
     const MeshView* bm;
@@ -322,22 +331,87 @@ struct RangeCtx {
     Frame fa, fb;
     V3 prev_ref_a;  // the body's reference point at the previous pose
     float margin, rest, dt;
-    bool interior_a, interior_b, skip, swept;
+    bool interior_a, interior_b, guided, swept;
+    Guide guide;
 };
+
+__device__ __forceinline__ Guide guide_of(const Dev& d, uint32_t a, uint32_t b, uint32_t fa) {
+    const uint32_t g = (fa & kFrameAxial) ? a : b;
+    const float4 ax = d.frame_guide[g], an = d.frame_anchor[g];
+    return {v3(an), v3(ax), ax.w, an.w, (__float_as_uint(d.frame[g].w) & kFrameAxialRotation) != 0};
+}
+
+// geometry.slang:1118-1127
+__device__ __forceinline__ V3 guide_direction(V3 n, V3 p, const Guide& g) {
+    return V3{dot(n, g.axis) * sqrtf(g.inv_mass),
+              g.rotation ? dot(g.axis, cross(sub(p, g.anchor), n)) * sqrtf(g.inv_moment) : 0.0f, 0.0f};
+}
+
+// geometry.slang:1129-1170, the guided merge: weak guide directions are
+// dropped; among impacts only the earliest (within 1e-4 of the tick) stay; a
+// contact along a kept one's guide direction replaces it when deeper per
+// unit direction; else it is added (a ninth replaces the shallowest).
+__device__ void mm_add_guided(MeshMan& m, V3 p, V3 n, float pen, float impact, const Guide& g) {
+    const V3 cd = guide_direction(n, p, g);
+    const float cl = len(cd);
+    if (cl * cl <= kEps) return;
+    if (impact > 0.0f) {
+        float first = 1.0f;
+        for (uint32_t i = 0; i < m.count; ++i)
+            if (m.impact[i] > 0.0f) first = fmn(first, m.impact[i]);
+        if (impact > first + 1.0e-4f) return;
+        if (impact < first - 1.0e-4f) {
+            uint32_t kept = 0;
+            for (uint32_t i = 0; i < m.count; ++i)
+                if (m.impact[i] == 0.0f) {
+                    mm_put(m, kept, m.p[i], m.n[i], m.pen[i], m.impact[i]);
+                    ++kept;
+                }
+            m.count = kept;
+        }
+    }
+    for (uint32_t i = 0; i < m.count; ++i) {
+        const V3 dk = guide_direction(m.n[i], m.p[i], g);
+        const float size = len(dk);
+        if (dot(cd, dk) > 0.9999f * cl * size) {
+            if (pen / cl > m.pen[i] / size) mm_put(m, i, p, n, pen, impact);
+            return;
+        }
+    }
+    if (m.count < 8) {
+        mm_put(m, m.count++, p, n, pen, impact);
+        return;
+    }
+    uint32_t sh = 0;
+    for (uint32_t i = 1; i < m.count; ++i)
+        if (m.pen[i] < m.pen[sh]) sh = i;
+    if (pen > m.pen[sh]) mm_put(m, sh, p, n, pen, impact);
+}
+
+// geometry.slang:1910-1919
+__device__ __forceinline__ bool triangle_pair_face_contact(const Tri& A, const Tri& B, V3 sep) {
+    const V3 zero{0.0f, 0.0f, 0.0f};
+    const V3 n = normalized_or(sep, zero);
+    const V3 fa = normalized_or(cross(sub(A.v[1], A.v[0]), sub(A.v[2], A.v[0])), zero);
+    const V3 fb = normalized_or(cross(sub(B.v[1], B.v[0]), sub(B.v[2], B.v[0])), zero);
+    return fab(dot(n, fa)) > 0.9999f || fab(dot(n, fb)) > 0.9999f;
+}
 
 
 __device__ __forceinline__ RangeCtx range_ctx_flat(const MeshView& am, const MeshPose& aprev, const MeshPose& as,
                                                    const Frame& fa, V3 prev_ref_a, const MeshView& bm,
                                                    const MeshPose& bprev, const MeshPose& bs, const Frame& fb,
                                                    float margin, float dt, bool swept, bool interior_a,
-                                                   bool interior_b) {
-    return RangeCtx{&am,   &bm,        aprev,      as,    bprev, bs, fa, fb, prev_ref_a, margin, fmn(margin, 1.0e-3f),
-                    dt,    interior_a, interior_b, false, swept};
+                                                   bool interior_b, bool guided, const Guide& guide) {
+    return RangeCtx{&am,    &bm,        aprev,      as,     bprev, bs,   fa, fb, prev_ref_a,
+                    margin, guided ? fmn(margin, 1.0e-4f) : fmn(margin, 1.0e-3f),
+                    dt,     interior_a, interior_b, guided, swept, guide};
 }
 
 // The contact of triangle `at` of the body against triangle `bt` of the
 // collider (the loop body of geometry.slang:1380-1583); false: none.
 __device__ __noinline__ bool triangle_pair_contact(const RangeCtx& c, uint32_t at, uint32_t bt, V3& c_p, V3& c_n, float& c_pen) {
+    if (c.guided) return false;  // a guided pair's ranges return at once (geometry.slang:1373)
     const MeshView& am = *c.am;
     const MeshView& bm = *c.bm;
     const float margin = c.margin, rest = c.rest;
@@ -448,7 +522,7 @@ __device__ __noinline__ bool triangle_pair_swept_contact(const RangeCtx& c, uint
                                             float& c_pen, float& c_impact) {
     const MeshView& am = *c.am;
     const MeshView& bm = *c.bm;
-    const float margin = c.margin, offset = c.rest;
+    const float margin = c.margin, rest = c.rest;
     const Tri PA = posed_tri(am, at, c.aprev), CA = posed_tri(am, at, c.as);
     const Tri PB = posed_tri(bm, bt, c.bprev), CB = posed_tri(bm, bt, c.bs);
     V3 alo = vmin(PA.v[0], CA.v[0]), ahi = vmax(PA.v[0], CA.v[0]);
@@ -494,6 +568,15 @@ __device__ __noinline__ bool triangle_pair_swept_contact(const RangeCtx& c, uint
         closest_triangle_pair(A, B, pa, pb);
         const V3 delta = sub(pa, pb);
         const float dist = sqrtf(fmx(0.0f, len2(delta)));
+        float offset = rest;
+        if (c.guided && !triangle_pair_face_contact(A, B, delta)) {
+            // A witness off the guide's face, with both an axial and a turning
+            // component, is held at zero offset.
+            const V3 dir = normalized_or(delta, zero);
+            const float axial = dot(dir, c.guide.axis);
+            const float angular = dot(c.guide.axis, cross(sub(pa, c.guide.anchor), dir));
+            if (fab(axial) > 1.0e-3f && fab(angular) > 1.0e-3f) offset = 0.0f;
+        }
         if (it == 0) {
             starts_near = dist <= offset + 5.0e-5f;
             // No point of either triangle moves more than `bound` relative to
@@ -531,7 +614,24 @@ __device__ __noinline__ bool triangle_pair_swept_contact(const RangeCtx& c, uint
         }
         sep_n = triangle_feature_normal(A, B, pa, pb, normalized_or(delta, V3{0.0f, 1.0f, 0.0f}));
         have_sep = true;
-        const float adv = (dist - offset) / (bound + kEps) * 0.9f;
+        float adv = (dist - offset) / (bound + kEps) * 0.9f;
+        if (c.guided) {
+            // Advance by the gap along the separating feature plane when that
+            // is faster; a separating, opening gap ends the search.
+            const V3 plane = triangle_feature_normal(A, B, pa, pb, sep_n);
+            float min_a = 3.402823466e+38f, max_b = -3.402823466e+38f;
+            float min_va = 3.402823466e+38f, max_vb = -3.402823466e+38f;
+            for (uint32_t k = 0; k < 3; ++k) {
+                min_a = fmn(min_a, dot(sub(A.v[k], pb), plane));
+                max_b = fmx(max_b, dot(sub(B.v[k], pb), plane));
+                min_va = fmn(min_va, dot(DA.v[k], plane));
+                max_vb = fmx(max_vb, dot(DB.v[k], plane));
+            }
+            const float gap = min_a - max_b - offset;
+            const float closing = max_vb - min_va;
+            if (gap > 1.0e-5f && closing <= 0.0f) return false;
+            if (gap > 0.0f && closing > kEps) adv = fmx(adv, 0.9f * gap / closing);
+        }
         time += fmx(adv, 1.0e-5f);
         if (time > 1.0f) return false;
     }
@@ -675,8 +775,7 @@ __global__ void k_mesh_walk_count(Dev d) {
                       bounds_xf(p.as.x, p.as.q), swept, p.margin, alo, ahi);
         motion_bounds(p.bm.lo, p.bm.hi, swept ? bounds_xf(p.bprev.x, p.bprev.q) : zero_xf,
                       bounds_xf(p.bs.x, p.bs.q), swept, 0.0f, blo, bhi);
-        // A guided pair gets no contacts here (its ranges return at once).
-        if (!guided && bounds_overlap(alo, ahi, blo, bhi)) {
+        if (bounds_overlap(alo, ahi, blo, bhi)) {
             mesh_walk<false>(d, p, s, swept, 0, 0, leaves, items);
             flags = swept ? kPairSwept : 0u;
             if ((p.fa.flags & kFrameStatic) && point_inside_convex(p.am, p.aprev, p.bprev.x)) flags |= kPairInteriorA;
@@ -719,8 +818,12 @@ __global__ void __launch_bounds__(128, 4) k_mesh_items(Dev d, StepParams sp) {
         const uint32_t size = rec.y * rec.w, count = (swept ? 2u : 1u) * size, base = d.ml_item[j];
         if (!size) continue;
         const PairSetup p = pair_setup(d, d.np_mesh[s]);
+        const uint32_t k = d.np_mesh[s];
+        const bool guided = d.nj && frames_guided(p.fa.flags, p.fb.flags);
+        const Guide guide = guided ? guide_of(d, d.cand_a[k], d.cand_b[k], p.fa.flags) : Guide{};
         const RangeCtx c = range_ctx_flat(p.am, p.aprev, p.as, p.fa, p.prev_ref_a, p.bm, p.bprev, p.bs, p.fb, p.margin,
-                                          sp.dt, swept, (flags & kPairInteriorA) != 0, (flags & kPairInteriorB) != 0);
+                                          sp.dt, swept, (flags & kPairInteriorA) != 0, (flags & kPairInteriorB) != 0,
+                                          guided, guide);
         for (uint32_t local = lane; local < count; local += 32) {
             const uint32_t f = base + local;
             if (f >= items_total) break;
@@ -755,11 +858,18 @@ __global__ void k_mesh_merge(Dev d, StepParams sp) {
             d.np_scan[k] = 0ull;
             continue;
         }
-        const float spacing = fmx(2.0f * (d.p2[d.cand_a[k]].z + d.p2[d.cand_b[k]].z), 1.0e-4f);
+        const uint32_t a = d.cand_a[k], b = d.cand_b[k];
+        const float spacing = fmx(2.0f * (d.p2[a].z + d.p2[b].z), 1.0e-4f);
+        const uint32_t fa = d.nj ? __float_as_uint(d.frame[a].w) : 0u, fb = d.nj ? __float_as_uint(d.frame[b].w) : 0u;
+        const bool guided = d.nj && frames_guided(fa, fb);
+        const Guide guide = guided ? guide_of(d, a, b, fa) : Guide{};
         for (uint32_t f = i0; f < i1; ++f) {
             if (!d.mi_valid[f]) continue;
             const float4 pv = d.mi_p[f], nv = d.mi_n[f];
-            mm_add(m, v3(pv), v3(nv), nv.w, pv.w, spacing);
+            if (guided)
+                mm_add_guided(m, v3(pv), v3(nv), nv.w, pv.w, guide);
+            else
+                mm_add(m, v3(pv), v3(nv), nv.w, pv.w, spacing);
         }
         const uint32_t count = m.count;
         d.np_count[k] = count;
@@ -782,14 +892,18 @@ __global__ void k_mesh_merge(Dev d, StepParams sp) {
 
 // The frame of body i at one set of poses (pos/rot: the predicted or the
 // previous positions and orientations of every body): reference point, flags.
-__device__ float4 hinge_frame_at(const Dev& d, uint32_t i, const float4* pos, const float4* rot) {
+// guide/guide_anchor (optional): the axis and inverse mass, the anchor and
+// the inverse moment (geometry.slang:384-402) of an axial frame.
+__device__ float4 hinge_frame_at(const Dev& d, uint32_t i, const float4* pos, const float4* rot,
+                                 float4* guide = nullptr, float4* guide_anchor = nullptr) {
     uint32_t flags = d.motion[i] == kStatic ? kFrameStatic : 0u;
     const V3 x = v3(pos[i]);
     const Q4 q = q4(rot[i]);
+    if (guide) *guide = *guide_anchor = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (!(d.p0[i].x > 0.0f)) return f4(x, __uint_as_float(flags));
     uint32_t incident = 0;
-    bool present = false, axial = false, fixed_member = false;
-    V3 anchor{0.0f, 0.0f, 0.0f};
+    bool present = false, axial = false, fixed_member = false, fixed = false, rotation = false;
+    V3 anchor{0.0f, 0.0f, 0.0f}, axis{0.0f, 0.0f, 0.0f};
     for (uint32_t k = d.jb_off[i]; k < d.jb_off[i + 1]; ++k) {
         const uint32_t j = d.jb_list[k];
         const Joint& o = d.joints[j];
@@ -801,17 +915,40 @@ __device__ float4 hinge_frame_at(const Dev& d, uint32_t i, const float4* pos, co
         const uint32_t other = is_a ? o.body_b : o.body_a;
         const bool static_anchor = other < d.n && d.motion[other] == kStatic;
         if (present || (o.type != kHinge && !(ax && static_anchor && !(o.breaking_threshold > 0.0f)))) continue;
+        const V3 local_axis = ax ? V3{1.0f, 0.0f, 0.0f} : V3{0.0f, 0.0f, 1.0f};
         const float* la = is_a ? o.anchor_a : o.anchor_b;
+        const float* lq = is_a ? o.frame_a : o.frame_b;
         anchor = add(x, rotate(q, V3{la[0], la[1], la[2]}));
+        axis = normalized_or(rotate(qmul(q, Q4{lq[0], lq[1], lq[2], lq[3]}), local_axis), local_axis);
         present = true;
+        fixed = static_anchor && !ax;
         axial = static_anchor && ax;
+        rotation = axial && o.type == kPiston;
         if (static_anchor) {
             const float* lo = is_a ? o.anchor_b : o.anchor_a;
-            anchor = add(v3(pos[other]), rotate(q4(rot[other]), V3{lo[0], lo[1], lo[2]}));
+            const float* oq = is_a ? o.frame_b : o.frame_a;
+            const Q4 qo = q4(rot[other]);
+            anchor = add(v3(pos[other]), rotate(qo, V3{lo[0], lo[1], lo[2]}));
+            axis = normalized_or(rotate(qmul(qo, Q4{oq[0], oq[1], oq[2], oq[3]}), local_axis), axis);
         }
     }
-    if (axial && incident != 1u) axial = present = false;
-    flags |= (present ? kFramePresent : 0u) | (axial ? kFrameAxial : 0u) | (fixed_member ? kFrameFixedMember : 0u);
+    if (axial && incident != 1u) axial = rotation = present = false;
+    if (axial && guide) {
+        const float4 p0 = d.p0[i];
+        float moment = 0.0f;
+        if ((fixed || rotation) && p0.x > kEps) {
+            const V3 l = inv_rotate(q, axis);
+            const float center = l.x * l.x / fmx(p0.y, kEps) + l.y * l.y / fmx(p0.z, kEps) + l.z * l.z / fmx(p0.w, kEps);
+            const V3 arm = sub(x, anchor);
+            const V3 perp = sub(arm, mul(axis, dot(arm, axis)));
+            const float pivot = center + len2(perp) / p0.x;
+            moment = pivot > kEps ? 1.0f / pivot : 0.0f;
+        }
+        *guide = f4(axis, p0.x);
+        *guide_anchor = f4(anchor, moment);
+    }
+    flags |= (present ? kFramePresent : 0u) | (axial ? kFrameAxial : 0u) | (fixed_member ? kFrameFixedMember : 0u) |
+             (rotation ? kFrameAxialRotation : 0u);
     return f4(present && !axial ? anchor : x, __uint_as_float(flags));
 }
 
@@ -821,7 +958,10 @@ __device__ float4 hinge_frame_at(const Dev& d, uint32_t i, const float4* pos, co
 // frame needs the body's only joint. One thread per body.
 __global__ void k_hinge_frames(Dev d) {
     for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
-        d.frame[i] = hinge_frame_at(d, i, d.tx, d.tq);
+        float4 guide, guide_anchor;
+        d.frame[i] = hinge_frame_at(d, i, d.tx, d.tq, &guide, &guide_anchor);
+        d.frame_guide[i] = guide;
+        d.frame_anchor[i] = guide_anchor;
         d.frame_prev[i] = hinge_frame_at(d, i, d.x, d.q);
     }
 }

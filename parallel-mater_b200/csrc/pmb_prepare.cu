@@ -95,7 +95,11 @@ __global__ void k_prepare_pairs(Dev d, StepParams sp) {
         const float penalty = pair_stiffness(pa0.x, pb0.x, dt);
         const V3 xa0 = v3(d.x[a]), xb0 = v3(d.x[b]), xa = v3(d.tx[a]), xb = v3(d.tx[b]);
         const Q4 qa0 = q4(d.q[a]), qb0 = q4(d.q[b]), qa = q4(d.tq[a]), qb = q4(d.tq[b]);
-        const float skin = fmn(pa2.z + pb2.z, 1.0e-3f) + 2.0f * 1.0e-5f;
+        // rigid_avbd_contact_skin (geometry_constraints.slang:438-446): a
+        // guided pair's contacts rest at the guided offset.
+        const bool guided =
+            d.nj && frames_guided(__float_as_uint(d.frame[a].w), __float_as_uint(d.frame[b].w));
+        const float skin = fmn(pa2.z + pb2.z, guided ? 1.0e-4f : 1.0e-3f) + 2.0f * 1.0e-5f;
         const V3 mo_a = sub(xa, xa0), mo_b = sub(xb, xb0);
         const V3 an_a = mul(delta_velocity(qa0, qa, dt), dt);
         const V3 an_b = mul(delta_velocity(qb0, qb, dt), dt);

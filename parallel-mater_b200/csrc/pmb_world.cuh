@@ -178,6 +178,7 @@ struct Dev {
     // hinge contact frames of the tick (reference point; flags in w) and
     // each body's joints in ascending index
     float4 *frame, *frame_prev;  // at the predicted and at the previous poses
+    float4 *frame_guide, *frame_anchor;  // guide axis + inverse mass, anchor + inverse moment (predicted poses)
     uint32_t *jb_off, *jb_list;
     uint32_t* np_mesh;  // candidates for the triangle-mesh path
     // the flat mesh path: per pair leaf-pair and item counts, their exclusive
@@ -308,7 +309,8 @@ void launch_narrowphase(const Dev& d, const StepParams& sp, cudaStream_t s);
 void launch_hinge_frames(const Dev& d, cudaStream_t s);
 void launch_mesh_narrowphase(const Dev& d, const StepParams& sp, cudaStream_t s);
 // Hinge contact frame flags (d.frame[i].w bits).
-constexpr uint32_t kFramePresent = 1u, kFrameAxial = 2u, kFrameFixedMember = 4u, kFrameStatic = 8u;
+constexpr uint32_t kFramePresent = 1u, kFrameAxial = 2u, kFrameFixedMember = 4u, kFrameStatic = 8u,
+                   kFrameAxialRotation = 16u;
 // rigid_guided_pair (geometry.slang:373-377): a body guided along a static
 // rail meets a static body.
 __host__ __device__ __forceinline__ bool frames_guided(uint32_t fa, uint32_t fb) {

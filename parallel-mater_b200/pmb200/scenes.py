@@ -445,6 +445,23 @@ def mesh_mix(profile=LEGACY, iterations=10, seed=11, margin=0.04) -> Scene:
     return b.build("mesh mix", iterations, profile)
 
 
+def guided_stop(kind=None, profile=LEGACY, iterations=10, speed=3.0) -> Scene:
+    """Guided contacts: a box on an unbreakable piston (or slider) joint to a
+    static anchor slides along the joint's axis into a static stop block.
+    The box is the guide's only joint member, so the box-stop pair is guided:
+    the face path skips it and the triangle-mesh path's swept ranges give its
+    contacts, merged by guide direction and held at the guided offset."""
+    kind = PISTON if kind is None else kind
+    b = _Builder()
+    anchor = b.mesh(*box_mesh((0.1, 0.1, 0.1)))
+    box = b.mesh(*box_mesh((0.2, 0.2, 0.2)))
+    a = b.body(anchor, STATIC, (0.0, 1.0, 0.0))
+    body = b.body(box, DYNAMIC, (0.6, 1.0, 0.0), v=(speed, 0.0, 0.0), mass=1.0, inertia=box_inertia(1.0, (0.2,) * 3))
+    b.body(box, STATIC, (2.0, 1.0, 0.0))
+    b.joint(kind, a, body, (0.0, 0.0, 0.0), (0.0, 0.0, 0.0))
+    return b.build("guided stop", iterations, profile)
+
+
 def welded_groups(profile=LEGACY, iterations=10, disable_bc=True) -> Scene:
     """Fixed collision groups. Bars A, B, C (1.2 m long) in a row 0.5 m apart,
     welded A-B and B-C by collision-disabling fixed joints: A and C overlap

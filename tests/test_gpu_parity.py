@@ -180,6 +180,27 @@ def test_triangle_mesh_path_matches_oracle(gpu_available, margin):
     print("mesh mix worst |gpu-oracle| =", worst)
 
 
+@pytest.mark.parametrize("kind", [scenes.PISTON, scenes.SLIDER])
+def test_guided_contacts_match_oracle(gpu_available, kind):
+    """Guided contacts on the GPU (a piston or slider box sliding into a
+    static stop): contact counts, manifolds and poses equal the oracle's every
+    tick, and the box comes to rest at the guided offset."""
+    s = scenes.guided_stop(kind)
+    w = core.World(s)
+    o = O.OracleWorld(s)
+    for f in range(40):
+        sg, so = w.step(), o.step()
+        assert sg["status"] == 0 and so["status"] == 0
+        assert sg["contacts"] == so["contacts"], f
+        cg, ng, _ = w.manifolds()
+        co, no, _ = o.manifolds()
+        assert np.array_equal(cg, co) and np.array_equal(ng, no), f
+        xg, xo = w.states(), o.states()
+        err = max(np.abs(xg[k] - xo[k]).max() for k in ("x", "q", "v"))
+        assert err < 1e-4, (f, err)
+    assert 1.5998 <= w.states()["x"][1, 0] <= 1.6
+
+
 def test_graph_replay_equals_steps(gpu_available):
     s = scenes.pyramid()
     a = core.World(s)

@@ -294,3 +294,24 @@ def test_triangle_mesh_path_holds_concave_and_large_meshes():
     for _ in range(150):
         assert o.step()["status"] == 0
     assert abs(o.states()["x"][2, 1] - floor) < 5e-3
+
+
+@pytest.mark.parametrize("kind", [scenes.PISTON, scenes.SLIDER])
+def test_guided_contacts_stop_a_piston_at_the_guided_offset(kind):
+    """A box on an unbreakable piston (slider) joint to a static anchor slides
+    at 3 m/s into a static stop: the pair is guided (geometry.slang:373-377),
+    so the face path skips it and the swept triangle ranges give contacts
+    merged by guide direction (:1129-1170) -- one contact for the whole face
+    -- and the box rests within the guided offset (1e-4 m) of the stop."""
+    s = scenes.guided_stop(kind)
+    o = O.OracleWorld(s)
+    counts = []
+    for _ in range(40):
+        st = o.step()
+        assert st["status"] == 0
+        counts.append(int(st["contacts"]))
+    x = o.states()
+    stop_face = 2.0 - 0.2 - 0.2
+    assert stop_face - 2e-4 <= x["x"][1, 0] <= stop_face
+    assert abs(x["v"][1, 0]) < 1e-3
+    assert max(counts) == 1 and sum(counts) >= 3
