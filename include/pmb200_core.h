@@ -182,6 +182,24 @@ PMB_API int pmb_world_profile_step(pmb_world* world, const pmb_step_desc* step, 
  * the previous call, and sets the enable state. */
 PMB_API int pmb_world_solve_timer(pmb_world* world, int enable, float* total_ms, uint32_t* launches);
 
+/* Mesh BVH build on the GPU, for meshes too large to prepare on the host:
+ * the tree the host preparation builds (the reference's upload-time builder,
+ * src/simulation/runtime_deformables.cu.inc:136-210: median split on the
+ * longest axis of the node's triangle bounds, triangles ordered by centroid
+ * on that axis with ties by index, leaves of at most 4 triangles, nodes in
+ * pre-order). `vertices` (3 floats each), `indices` (3 per triangle),
+ * `order` (one per triangle: the original index of the triangle stored at
+ * each position) and `nodes` (10 words per node: lo[3], hi[3] as floats;
+ * first, count (0 for an inner node), left, right as uint32) are device
+ * memory; `node_count` (host) receives the node count, and a capacity below
+ * it returns PMB_ERROR_CAPACITY_EXCEEDED; an index at or past `vertex_count`
+ * returns PMB_ERROR_INVALID_ARGUMENT before any other device work. Work runs on `stream` (CUDA
+ * stream, null for the default); the call allocates scratch with cudaMalloc
+ * and returns after the stream has finished. */
+PMB_API int pmb_mesh_bvh_build(const float* vertices, uint32_t vertex_count, const uint32_t* indices,
+                               uint32_t index_count, uint32_t* order, float* nodes, uint32_t node_capacity,
+                               uint32_t* node_count, void* stream);
+
 /* Host mesh preparation used at world creation (no device work): triangles
  * reordered into median-split BVH leaf order, one outward plane (n, d) per
  * triangle when the mesh is a closed convex shell, bounds (lo, hi, centre,

@@ -75,6 +75,7 @@ def lib():
             "pmb_world_profile_step": [vp, vp, vp, u32],
             "pmb_world_solve_timer": [vp, i32, vp, vp], "pmb_kernel_launches": [vp],
             "pmb_prepare_mesh": [vp, u32, vp, u32, vp, vp, vp, vp],
+            "pmb_mesh_bvh_build": [vp, u32, vp, u32, vp, vp, u32, vp, vp],
             "pmb_world_get_states": [vp, vp], "pmb_world_set_states": [vp, vp],
             "pmb_world_last_stats": [vp, vp], "pmb_world_apply_impulse": [vp, u32, vp, vp],
             "pmb_world_candidate_pairs": [vp, vp, u32, vp],
