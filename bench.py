@@ -8,9 +8,11 @@ ground and four walls -- starting from the settled state in
 tests/golden/settled_pile_64x32x32.npz (300 ticks of plain AVBD from the spawn
 grid). A step is one rigid AVBD tick (legacy profile: predict, broadphase,
 narrowphase, contact cache, prepare, colouring, solve, impact phase, commit)
-run with the residual-driven schedule: sweep until the contact residual (RMS
-over active normal rows) is at or below --tolerance, at most --max-iterations
-sweeps. Inputs are synthetic (seeded); no dataset is involved.
+run with the residual-driven schedule: sweep until the residual -- the largest
+violation over the active contact normal rows and hard joint rows, in metres
+(--residual-norm max; `rms` tests the RMS instead) -- is at or below
+--tolerance, at most --max-iterations sweeps. Inputs are synthetic (seeded);
+no dataset is involved.
 
 GPU arm (default): the warm-start MLP is first trained online on
 --train-frames plain ticks (untimed); then, from the same settled snapshot,
@@ -23,7 +25,9 @@ learned arm through the C ABI with host buffers (state upload from pinned
 host memory, tick, state download each step). Multi-GPU runs independent replicas
 (the coupled pile does not shard). Reference arm (--impl reference): the CPU
 restatement of the reference's serial Slang CPU driver (oracle/, one core),
-on the same state and schedule, over a bounded number of ticks.
+on the same state and schedule, over a bounded number of ticks: the oracle
+first steps the same --warmup ticks as the GPU arms (untimed, so its contact
+cache is as warm as theirs), then times --cpu-ticks ticks.
 """
 import argparse
 import json
@@ -43,6 +47,7 @@ GRID = (64, 32, 32)
 SEED = 4
 SETTLED = os.path.join(ROOT, "tests", "golden", "settled_pile_64x32x32.npz")
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "k_solve_pile65k.md")
+NORMS = {"max": 0, "rms": 1}
 LANE_POLICIES = ["8/16/32 by colour size", "8", "8/16/32 by body rows, heaviest first",
                  "8/16/32 by colour size, bodies claimed dynamically"]
 
@@ -55,6 +60,8 @@ def parse():
     ap.add_argument("--impl", default="pmb", choices=["pmb", "reference"])
     ap.add_argument("--tolerance", type=float, default=1e-4)
     ap.add_argument("--max-iterations", type=int, default=64)
+    ap.add_argument("--residual-norm", default="max", choices=["max", "rms"],
+                    help="residual the schedule tests: largest row violation (default) or RMS over the rows")
     ap.add_argument("--cpu-ticks", type=int, default=1, help="ticks timed by the CPU baseline leg")
     ap.add_argument("--contact-capacity", type=int, default=0,
                     help="contact-point capacity of the world (0: the library default, 64 per body)")
@@ -129,10 +136,15 @@ def solve_bytes(stats, n_dynamic):
     return phases * int(stats["iterations"]) * per_iter
 
 
-def cpu_baseline(scene, desc, ticks):
+def cpu_baseline(scene, desc, ticks, warm=0):
+    """Steps/s of the CPU oracle over `ticks` ticks, after `warm` untimed
+    ticks with the same schedule (the GPU arms' warm-up, so the contact cache
+    and warm starts are as warm as theirs)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     w = O.OracleWorld(scene)
+    for _ in range(warm):
+        w.step(desc)
     t0 = time.perf_counter()
     stats = None
     for _ in range(ticks):
@@ -146,18 +158,22 @@ def reference_arm(args):
     if rank != 0:
         return
     scene = load_scene()
-    desc = scene.step_desc(residual_tolerance=args.tolerance, max_iterations=args.max_iterations)
+    desc = scene.step_desc(residual_tolerance=args.tolerance, max_iterations=args.max_iterations,
+                           residual_norm=NORMS[args.residual_norm])
     ticks = max(1, min(args.steps, args.cpu_ticks))
-    value, stats = cpu_baseline(scene, desc, ticks)
+    value, stats = cpu_baseline(scene, desc, ticks, warm=args.warmup)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
         "steps": ticks, "warmup": 0, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "box pile 64x32x32 (65,536 boxes), settled state, residual-driven AVBD",
-                   "bodies": scene.n, "tolerance": args.tolerance, "max_iterations": args.max_iterations,
-                   "iterations": int(stats["iterations"]), "contacts": int(stats["contacts"])},
+                   "bodies": scene.n, "tolerance": args.tolerance, "residual_norm": args.residual_norm,
+                   "max_iterations": args.max_iterations,
+                   "iterations": int(stats["iterations"]), "contacts": int(stats["contacts"]),
+                   "residual_row_max": float(stats["residual_max"])},
         "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "port",
-                         "sample": f"{ticks} tick(s) of the settled 65,541-body pile; CPU restatement of the "
+                         "sample": f"{ticks} warm tick(s) of the settled 65,541-body pile after {args.warmup} "
+                                   f"untimed ones, {int(stats['iterations'])} sweeps; CPU restatement of the "
                                    "reference's serial Slang CPU driver (the generated driver needs slangc, absent)"},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -205,8 +221,11 @@ def gpu_arm(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     scene = load_scene()
     n_dyn = int((scene.bodies["motion"] == scenes.DYNAMIC).sum())
-    plain = scene.step_desc(residual_tolerance=args.tolerance, max_iterations=args.max_iterations)
-    learned = scene.step_desc(residual_tolerance=args.tolerance, max_iterations=args.max_iterations, warm_start=1)
+    norm = NORMS[args.residual_norm]
+    plain = scene.step_desc(residual_tolerance=args.tolerance, max_iterations=args.max_iterations,
+                            residual_norm=norm)
+    learned = scene.step_desc(residual_tolerance=args.tolerance, max_iterations=args.max_iterations, warm_start=1,
+                              residual_norm=norm)
     world = core.World(scene, device=local, contact_capacity=args.contact_capacity)
     stream = torch.cuda.Stream()             # a capturable (non-default) stream for the graph
     world.set_stream(stream.cuda_stream)
@@ -300,10 +319,12 @@ def gpu_arm(args):
 
     cpu = None
     if rank == 0 and world_size == 1 and args.cpu_ticks > 0:
-        cv, cst = cpu_baseline(scene, plain, args.cpu_ticks)
+        cv, cst = cpu_baseline(scene, plain, args.cpu_ticks, warm=args.warmup)
         cpu = {"value": cv, "unit": "steps/s", "cores": 1, "kind": "port",
-               "sample": f"{args.cpu_ticks} tick(s) of the same settled pile, same schedule, plain warm start; "
-                         f"serial CPU restatement (oracle/), {int(cst['iterations'])} sweeps"}
+               "sample": f"{args.cpu_ticks} warm tick(s) of the same settled pile after the GPU arms' "
+                         f"{args.warmup} warm-up ticks (untimed), same schedule, plain warm start; serial CPU "
+                         f"restatement (oracle/), {int(cst['iterations'])} sweeps, row-max residual "
+                         f"{float(cst['residual_max']):.3g} m"}
 
     def mean(stats, key):
         return float(np.mean([int(st[key]) for st in stats]))
@@ -317,13 +338,19 @@ def gpu_arm(args):
             "config": {"workload": "box pile 64x32x32 (65,536 boxes + ground and walls), settled state, "
                                    "legacy AVBD profile, residual-driven schedule; learned warm start "
                                    "(BF16 tcgen05 MLP, penalty prediction) vs plain",
-                       "bodies": scene.n, "tolerance": args.tolerance,
+                       "bodies": scene.n, "tolerance": args.tolerance, "residual_norm": args.residual_norm,
                        "max_iterations": args.max_iterations,
                        "plain_steps_per_s": plain_value, "learned_over_plain": value / plain_value,
                        "iterations_mean_learned": mean(learned_stats, "iterations"),
                        "iterations_mean_plain": mean(plain_stats, "iterations"),
-                       "residual_max_learned": max(float(st["residual"]) for st in learned_stats),
-                       "residual_max_plain": max(float(st["residual"]) for st in plain_stats),
+                       "residual_row_max_learned": max(float(st["residual_max"]) for st in learned_stats),
+                       "residual_row_max_plain": max(float(st["residual_max"]) for st in plain_stats),
+                       "residual_rms_max_over_ticks_learned": max(float(st["residual"]) for st in learned_stats),
+                       "residual_rms_max_over_ticks_plain": max(float(st["residual"]) for st in plain_stats),
+                       "ticks_at_sweep_cap_learned": sum(int(st["iterations"]) >= args.max_iterations
+                                                         for st in learned_stats),
+                       "ticks_at_sweep_cap_plain": sum(int(st["iterations"]) >= args.max_iterations
+                                                       for st in plain_stats),
                        "contacts_mean": mean(learned_stats, "contacts"),
                        "mlp_training": {"frames": args.train_frames, "adam_lr": args.mlp_lr,
                                         "steps_per_frame": args.mlp_steps, "seconds": round(train_s, 2),

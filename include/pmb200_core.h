@@ -134,7 +134,9 @@ typedef struct pmb_world_capacity {
  * (requested_iterations, or base_iterations raised by joint iteration hints,
  * plus the velocity impact phase). residual_tolerance > 0 switches to the
  * residual-driven schedule: sweep until the residual is at or below the
- * tolerance, at most max_iterations sweeps. warm_start selects where each
+ * tolerance, at most max_iterations sweeps; residual_norm picks the residual
+ * the schedule tests: 0 the largest row violation of the sweep (every
+ * constraint within the tolerance, in metres), 1 the RMS over the rows. warm_start selects where each
  * contact's normal row (lambda, penalty) starts: 0 plain (the reference's
  * cached-and-decayed warm start), 1 learned (the world's MLP predictor, when
  * one is attached; plain otherwise), 2 the table set by
@@ -146,6 +148,7 @@ typedef struct pmb_step_desc {
     uint32_t max_iterations;
     uint32_t warm_start;
     uint32_t collect_events; /* nonzero: record this tick's contact events */
+    uint32_t residual_norm;  /* 0: largest row violation, 1: RMS (residual-driven schedule) */
 } pmb_step_desc;
 
 /* residual: RMS, over contact normal rows that carry force or penetrate and
@@ -223,7 +226,10 @@ PMB_API int pmb_prepare_mesh(const float* vertices, uint32_t vertex_count, const
  * the process exits) for at most 1,048,576 vertices; larger graphs return
  * PMB_ERROR_CAPACITY_EXCEEDED, and so do graphs needing more than 256 colours.
  * The first call on a device resolves that array's address, so make it before
- * any stream capture. Calls share the array: calls that overlap on the GPU
+ * any stream capture. Every call reads its status back and waits for `stream`;
+ * a `stream` in capture mode is rejected with PMB_ERROR_INVALID_ARGUMENT
+ * before any work is enqueued. The caller's current device is restored before
+ * the call returns. Calls share the array: calls that overlap on the GPU
  * (other streams, other threads) race and must be serialised by the caller. */
 PMB_API int pmb_graph_color_noalloc(const uint32_t* offsets, const uint32_t* neighbors, const uint32_t* dynamic,
                                     uint32_t vertex_count, uint32_t* colors, int32_t device, void* stream);
@@ -244,12 +250,15 @@ PMB_API int pmb_world_last_stats(pmb_world* world, pmb_step_stats* out);
 PMB_API int pmb_world_apply_impulse(pmb_world* world, uint32_t body, const float* linear, const float* angular);
 
 /* Inspection of the last tick (synchronous). Counts are returned even when
- * the output pointer is null or the capacity is too small. */
-PMB_API int pmb_world_candidate_pairs(pmb_world* world, uint32_t* codes, uint32_t capacity, uint32_t* count);
+ * the output pointer is null or the capacity is too small. A pair code is
+ * a * N + b for query body a, other body b and N bodies, held in 64 bits (the
+ * reference's 32-bit code, geometry.slang:907-913, overflows above 65,535
+ * bodies); codes ascend in the active-pair order. */
+PMB_API int pmb_world_candidate_pairs(pmb_world* world, uint64_t* codes, uint32_t capacity, uint32_t* count);
 /* Per non-empty manifold: pair code, point count; 8 contact slots of 22
  * floats (normal, point, penetration, error, dual lambda/penalty x3,
  * anchor a, anchor b). */
-PMB_API int pmb_world_manifolds(pmb_world* world, uint32_t* codes, uint32_t* counts, float* contacts,
+PMB_API int pmb_world_manifolds(pmb_world* world, uint64_t* codes, uint32_t* counts, float* contacts,
                                 uint32_t capacity, uint32_t* count);
 PMB_API int pmb_world_graph(pmb_world* world, uint32_t* colors, uint32_t* parents);
 PMB_API int pmb_world_residual_trace(pmb_world* world, float* out, uint32_t capacity, uint32_t* count);
@@ -410,6 +419,17 @@ PMB_API int pmb_world_scene_stats(pmb_world* world, float* residual, float* resi
  * claimed dynamically from a counter. Every plan computes bit-identical results;
  * only the speed differs. A new world starts with (1, 0). */
 PMB_API int pmb_world_set_launch_plan(pmb_world* world, uint32_t solve_variant, uint32_t solve_policy);
+/* Bound on the polls a thread block makes at a grid barrier of the tick's
+ * cooperative kernels (colouring fixpoint, solve) before it gives up (0: the
+ * default, 2^26 polls, seconds). A barrier that runs out latches
+ * PMB_STATUS_BARRIER_TIMEOUT in the tick's status, the remaining cooperative
+ * kernels of the tick return at once and the host reads the status after the
+ * tick (the pm* driver reports it as PM_ERROR_DEVICE_LOST); the next tick
+ * starts with clean counters. A small limit makes the waits run out on
+ * purpose, which is how failure detection is exercised without a GPU fault.
+ * Takes effect for ticks enqueued afterwards (not for graphs already
+ * captured). */
+PMB_API int pmb_world_set_barrier_limit(pmb_world* world, uint32_t spins);
 /* Time `ticks` ticks of every plan from the current state (restored before
  * each plan and at the end, so the world does not advance), keep the fastest
  * and report it; `report` receives one line per plan. Needs snapshot
@@ -451,7 +471,9 @@ PMB_API int pmb_event_elapsed_ms(int32_t device, void* start, void* end, float* 
  * block: in 27 floats (h[21], g[6]) -> out 7 floats (delta[6], solved).
  * dual:  in 7 floats -> out 5 (warm lambda/penalty, force, updated lambda/penalty).
  * contact: in 4 floats (trial n,t0,t1, friction) -> out 6 (projected, scales).
- * row: in 42 floats -> out 7 (see tests). */
+ * row: in 42 floats -> out 7 (see tests).
+ * trig (kind 4): in 3 floats (y, x, t) -> out 2 (atan2(y, x) for y, x >= 0,
+ * t cos(t) / sin(t) for t in [0, pi/2]), the tick's own evaluations. */
 PMB_API int pmb_math_eval(uint32_t kind, uint32_t count, const float* in, float* out);
 
 #ifdef __cplusplus

@@ -86,13 +86,53 @@ template <class R> inline V3<R> rotation_displacement(Q4<R> from, Q4<R> to, V3<R
     V3<R> oc = cross(o, v), dc = cross(d, v);
     return mul(add(add(mul(oc, to.w - from.w), mul(dc, to.w)), add(cross(d, oc), cross(n, dc))), R(2));
 }
+// Arctangent (first quadrant) and x cot(x) on [0, pi/2]. In FP32 they are
+// evaluated from basic operations -- the addition formula with pi/6 and the
+// Maclaurin series of atan to u^15, and of sin to x^15 and cos to x^16 --
+// the same steps as the CUDA library, so both round identically; the libm
+// functions would round differently on the host and on the device. The FP64
+// replay uses libm (the exact functions to double precision).
+template <class R> inline R atan2_q1(R y, R x) {
+    if constexpr (sizeof(R) == 8) {
+        return std::atan2(y, x);
+    } else {
+        const bool swap = y > x;
+        const float t = swap ? x / y : y / x;
+        const bool shift = t > 0.26794919f;  // tan(pi/12)
+        const float u = shift ? (t * 1.7320508f - 1.0f) / (t + 1.7320508f) : t;
+        const float u2 = u * u;
+        const float coef[8] = {1.0f, -1.0f / 3.0f, 1.0f / 5.0f, -1.0f / 7.0f,
+                               1.0f / 9.0f, -1.0f / 11.0f, 1.0f / 13.0f, -1.0f / 15.0f};
+        float p = coef[7];
+        for (int k = 6; k >= 0; --k) p = coef[k] + u2 * p;
+        float r = u * p;
+        if (shift) r = 0.52359878f + r;  // pi/6
+        return swap ? 1.5707964f - r : r;
+    }
+}
+template <class R> inline R x_cot(R x) {
+    if constexpr (sizeof(R) == 8) {
+        return x * std::cos(x) / std::sin(x);
+    } else {
+        const float x2 = x * x;
+        const float sc[8] = {1.0f, -1.0f / 6.0f, 1.0f / 120.0f, -1.0f / 5040.0f, 1.0f / 362880.0f,
+                             -1.0f / 39916800.0f, 1.0f / 6227020800.0f, -1.0f / 1307674368000.0f};
+        const float cc[9] = {1.0f, -0.5f, 1.0f / 24.0f, -1.0f / 720.0f, 1.0f / 40320.0f, -1.0f / 3628800.0f,
+                             1.0f / 479001600.0f, -1.0f / 87178291200.0f, 1.0f / 20922789888000.0f};
+        float s = sc[7];
+        for (int k = 6; k >= 0; --k) s = sc[k] + x2 * s;
+        float c = cc[8];
+        for (int k = 7; k >= 0; --k) c = cc[k] + x2 * c;
+        return c / s;
+    }
+}
 // math.slang:221-240
 template <class R> inline V3<R> rotation_vector(Q4<R> d) {
     R s = d.x * d.x + d.y * d.y + d.z * d.z;
     R scale = R(2) + s * (R(1) / R(3) + s * (R(3) / R(20) + s * (R(5) / R(56) + s * (R(35) / R(576)))));
     if (s > R(0.01)) {
         R vs = std::sqrt(s);
-        scale = R(2) * std::atan2(vs, clampv(d.w, R(0), R(1))) / vs;
+        scale = R(2) * atan2_q1(vs, clampv(d.w, R(0), R(1))) / vs;
     }
     return {d.x * scale, d.y * scale, d.z * scale};
 }

@@ -16,12 +16,23 @@ template <class R> inline bool overlaps(const V3<R>& alo, const V3<R>& ahi, cons
 }
 
 // Pair filter of geometry.slang:897-913 with identity order == dense order.
-template <class R> inline bool collision_disabled(const World<R>& w, uint32_t a, uint32_t b) {
+// constrained_collision_disabled (geometry.slang:494-511) scans every joint
+// for each pair; the same predicate (an alive, enabled, unbroken joint with
+// disable_collisions between a and b, either way round) is answered here from
+// the sorted (min, max) body keys of those joints, gathered once per tick.
+template <class R> inline std::vector<uint64_t> collision_disabled_keys(const World<R>& w) {
+    std::vector<uint64_t> keys;
     for (auto& j : w.joints) {
         if (!j.alive || !j.d.enabled || j.broken || !j.d.disable_collisions) continue;
-        if ((j.d.body_a == a && j.d.body_b == b) || (j.d.body_a == b && j.d.body_b == a)) return true;
+        const uint64_t lo = std::min(j.d.body_a, j.d.body_b), hi = std::max(j.d.body_a, j.d.body_b);
+        keys.push_back(lo << 32 | hi);
     }
-    return false;
+    std::sort(keys.begin(), keys.end());
+    return keys;
+}
+inline bool collision_disabled(const std::vector<uint64_t>& keys, uint32_t a, uint32_t b) {
+    const uint64_t lo = std::min(a, b), hi = std::max(a, b);
+    return std::binary_search(keys.begin(), keys.end(), lo << 32 | hi);
 }
 
 // pm_build_fixed_collision_groups (geometry.slang:3102-3136): bodies joined
@@ -51,9 +62,9 @@ template <class R> inline std::vector<uint32_t> fixed_groups(const World<R>& w) 
 // Sorted candidate pairs (a dynamic query body, b any other leaf whose swept
 // proxy overlaps a's). A uniform grid keyed on AABB centre lists candidates;
 // the predicate and the (a, b) order are the reference's.
-template <class R> inline std::vector<uint32_t> broadphase(const World<R>& w) {
+template <class R> inline std::vector<uint64_t> broadphase(const World<R>& w) {
     const uint32_t n = w.n;
-    std::vector<uint32_t> out;
+    std::vector<uint64_t> out;
     R cell = 0;
     for (uint32_t i = 0; i < n; ++i) {
         V3<R> e = sub(w.aabb_hi[i], w.aabb_lo[i]);
@@ -82,6 +93,7 @@ template <class R> inline std::vector<uint32_t> broadphase(const World<R>& w) {
     std::map<std::array<int64_t, 3>, std::vector<uint32_t>> grid;
     for (uint32_t i : small) grid[key(i, 0, 0, 0)].push_back(i);
     const std::vector<uint32_t> group = fixed_groups(w);
+    const std::vector<uint64_t> disabled = collision_disabled_keys(w);
     std::vector<uint32_t> cand;
     for (uint32_t a = 0; a < n; ++a) {
         if (!dynamic(w, a)) continue;
@@ -91,7 +103,7 @@ template <class R> inline std::vector<uint32_t> broadphase(const World<R>& w) {
             if (!overlaps(w.aabb_lo[b], w.aabb_hi[b], w.aabb_lo[a], w.aabb_hi[a])) return;
             if (dynamic(w, b) && !(a < b)) return;
             if (!group.empty() && group[a] == group[b]) return;
-            if (collision_disabled(w, a, b)) return;
+            if (collision_disabled(disabled, a, b)) return;
             cand.push_back(b);
         };
         for (uint32_t b : large) test(b);
@@ -107,7 +119,7 @@ template <class R> inline std::vector<uint32_t> broadphase(const World<R>& w) {
                     }
         }
         std::sort(cand.begin(), cand.end());
-        for (uint32_t b : cand) out.push_back(a * n + b);
+        for (uint32_t b : cand) out.push_back(uint64_t(a) * n + b);
     }
     return out;
 }
@@ -148,8 +160,8 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
     w.manifolds.clear();
     const std::vector<HingeFrame<R>> frames = hinge_frames(w, pred);
     const std::vector<HingeFrame<R>> prev_frames = hinge_frames(w, prev);
-    for (uint32_t code : w.candidate_pairs) {
-        uint32_t a = code / n, b = code % n;
+    for (uint64_t code : w.candidate_pairs) {
+        uint32_t a = uint32_t(code / n), b = uint32_t(code % n);
         const Mesh<R>& bm = w.meshes[w.body[a].mesh];
         const Mesh<R>& cm = w.meshes[w.body[b].mesh];
         R margin = R(w.body[a].margin) + R(w.body[b].margin);
@@ -186,9 +198,10 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
 
     // ---- contact cache load (geometry.slang:2941-3009)
     for (uint32_t k = 0; k < P; ++k) {
-        uint32_t code = w.active_pairs[k], a = code / n;
+        const uint64_t code = w.active_pairs[k];
+        const uint32_t a = uint32_t(code / n);
         auto it = std::lower_bound(w.saved.begin(), w.saved.end(), code,
-                                   [](const SavedPair<R>& s, uint32_t c) { return s.pair < c; });
+                                   [](const SavedPair<R>& s, uint64_t c) { return s.pair < c; });
         if (it == w.saved.end() || it->pair != code || it->epoch + 1 != epoch || ab(it->dt - dt) > R(1.0e-7)) continue;
         const SavedPair<R>& sp = *it;
         Manifold<R>& m = w.manifolds[k];
@@ -257,7 +270,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
     }
     std::vector<bool> pair_impact(P);
     for (uint32_t k = 0; k < P; ++k) {
-        uint32_t a = w.active_pairs[k] / n, b = w.active_pairs[k] % n;
+        uint32_t a = uint32_t(w.active_pairs[k] / n), b = uint32_t(w.active_pairs[k] % n);
         R penalty = pair_stiffness<R>(w.body[a], w.body[b], dt);
         Manifold<R>& m = w.manifolds[k];
         for (uint32_t p = 0; p < m.count; ++p) {
@@ -319,7 +332,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
     st.contacts = 0;
     for (uint32_t k = 0; k < P; ++k) {
         st.contacts += w.manifolds[k].count;
-        uint32_t a = w.active_pairs[k] / n, b = w.active_pairs[k] % n;
+        uint32_t a = uint32_t(w.active_pairs[k] / n), b = uint32_t(w.active_pairs[k] % n);
         unite(a, b);
         w.manifolds[k].next_a = bodies[a].contact_head;
         bodies[a].contact_head = k;
@@ -340,7 +353,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
     bool any_impact = false;
     for (uint32_t k = 0; k < P; ++k) {
         if (!pair_impact[k]) continue;
-        uint32_t a = w.active_pairs[k] / n, b = w.active_pairs[k] % n;
+        uint32_t a = uint32_t(w.active_pairs[k] / n), b = uint32_t(w.active_pairs[k] % n);
         if (dynamic(w, a)) bodies[bodies[a].parent].impact = 1;
         if (dynamic(w, b)) bodies[bodies[b].parent].impact = 1;
         any_impact = true;
@@ -359,7 +372,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
         for (;; ++color) {
             bool conflict = false;
             for (uint32_t k = bodies[i].contact_head; k != kInvalid;) {
-                uint32_t a = w.active_pairs[k] / n, b = w.active_pairs[k] % n;
+                uint32_t a = uint32_t(w.active_pairs[k] / n), b = uint32_t(w.active_pairs[k] % n);
                 bool first = i == a;
                 conflict = conflict || bodies[first ? b : a].color == color;
                 k = first ? w.manifolds[k].next_a : w.manifolds[k].next_b;
@@ -389,7 +402,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
         if (phase != 0) {
             // impact_gaps (:238-262)
             for (uint32_t k = 0; k < P; ++k) {
-                uint32_t a = w.active_pairs[k] / n, b = w.active_pairs[k] % n;
+                uint32_t a = uint32_t(w.active_pairs[k] / n), b = uint32_t(w.active_pairs[k] % n);
                 if (bodies[a].impact == 0 && bodies[b].impact == 0) continue;
                 Manifold<R>& m = w.manifolds[k];
                 for (uint32_t p = 0; p < m.count; ++p) {
@@ -417,7 +430,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
                 visit_joint(j, w, prev, bodies, dt, scratch, true, kImpact);
             }
             for (uint32_t k = 0; k < P; ++k) {
-                uint32_t a = w.active_pairs[k] / n, b = w.active_pairs[k] % n;
+                uint32_t a = uint32_t(w.active_pairs[k] / n), b = uint32_t(w.active_pairs[k] % n);
                 if (bodies[a].impact == 0 && bodies[b].impact == 0) continue;
                 Vec6<R> va = jac(mul(pred[a].v, dt), mul(pred[a].w, dt));
                 Vec6<R> vb = jac(mul(pred[b].v, dt), mul(pred[b].w, dt));
@@ -447,7 +460,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
                     for (unsigned r = 0; r < 6; ++r)
                         for (unsigned c = 0; c < 6; ++c) blk.g[r] += blk.h[bidx(r, c)] * B.dx.v[c];
                     for (uint32_t k = B.contact_head; k != kInvalid;) {
-                        uint32_t a = w.active_pairs[k] / n, b = w.active_pairs[k] % n;
+                        uint32_t a = uint32_t(w.active_pairs[k] / n), b = uint32_t(w.active_pairs[k] % n);
                         bool first = i == a;
                         R friction = std::sqrt(R(w.body[a].friction) * R(w.body[b].friction));
                         const Manifold<R>& m = w.manifolds[k];
@@ -491,7 +504,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
                     if (block_solve(blk, upd)) {
                         bool crossing = false;
                         for (uint32_t k = B.contact_head; k != kInvalid;) {
-                            uint32_t a = w.active_pairs[k] / n, b = w.active_pairs[k] % n;
+                            uint32_t a = uint32_t(w.active_pairs[k] / n), b = uint32_t(w.active_pairs[k] % n);
                             bool first = i == a;
                             const Manifold<R>& m = w.manifolds[k];
                             for (uint32_t p = 0; p < m.count; ++p) {
@@ -527,7 +540,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
             w.res_n = 0;
             w.res_max = 0;
             for (uint32_t k = 0; k < P; ++k) {
-                uint32_t a = w.active_pairs[k] / n, b = w.active_pairs[k] % n;
+                uint32_t a = uint32_t(w.active_pairs[k] / n), b = uint32_t(w.active_pairs[k] % n);
                 if (phase != 0 && bodies[a].impact == 0 && bodies[b].impact == 0) continue;
                 R friction = std::sqrt(R(w.body[a].friction) * R(w.body[b].friction));
                 R beta = pair_stiffness<R>(w.body[a], w.body[b], dt) * R(100);
@@ -585,9 +598,13 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
             }
             bool last = it + 1 == iters;
             if (phase == 0) {
-                R res = w.res_n ? R(std::sqrt(w.res_sq / double(w.res_n))) : R(0);
-                w.residual_trace.push_back(res);
+                const R rms = w.res_n ? R(std::sqrt(w.res_sq / double(w.res_n))) : R(0);
+                w.residual_rms_last = rms;
                 w.residual_max_last = w.res_max;
+                // The schedule's measure: the largest row violation (every
+                // constraint within the tolerance) or the RMS over the rows.
+                const R res = o.residual_norm == 1 ? rms : w.res_max;
+                w.residual_trace.push_back(res);
                 if (adaptive && res <= R(o.residual_tolerance)) last = true;
                 used_iterations = it + 1;
             }
@@ -595,7 +612,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
         }
         // Last-iteration contact work (:533-561).
         for (uint32_t k = 0; k < P; ++k) {
-            uint32_t a = w.active_pairs[k] / n, b = w.active_pairs[k] % n;
+            uint32_t a = uint32_t(w.active_pairs[k] / n), b = uint32_t(w.active_pairs[k] % n);
             if (phase != 0 && bodies[a].impact == 0 && bodies[b].impact == 0) continue;
             Manifold<R>& m = w.manifolds[k];
             for (uint32_t p = 0; p < m.count; ++p) {
@@ -632,7 +649,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
                 weighted = add(weighted, mul(V3<R>{bodies[i].dx.v[0], bodies[i].dx.v[1], bodies[i].dx.v[2]}, mass));
                 total += mass;
                 for (uint32_t k = bodies[i].contact_head; k != kInvalid;) {
-                    uint32_t a = w.active_pairs[k] / n, b = w.active_pairs[k] % n;
+                    uint32_t a = uint32_t(w.active_pairs[k] / n), b = uint32_t(w.active_pairs[k] % n);
                     bool first = i == a;
                     anchored = anchored || !dynamic(w, first ? b : a);
                     k = first ? w.manifolds[k].next_a : w.manifolds[k].next_b;
@@ -699,7 +716,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
         }
     }
     st.iterations = used_iterations;
-    st.residual = w.residual_trace.empty() ? 0.0f : float(w.residual_trace.back());
+    st.residual = w.residual_trace.empty() ? 0.0f : float(w.residual_rms_last);
     st.residual_max = float(w.residual_max_last);
 
     // ---- speed clamp (geometry.slang:3086-3100)
@@ -713,7 +730,8 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
     std::vector<SavedPair<R>> saved;
     saved.reserve(P);
     for (uint32_t k = 0; k < P; ++k) {
-        uint32_t code = w.active_pairs[k], a = code / n;
+        const uint64_t code = w.active_pairs[k];
+        const uint32_t a = uint32_t(code / n);
         const Manifold<R>& m = w.manifolds[k];
         SavedPair<R> sp{};
         sp.pair = code;

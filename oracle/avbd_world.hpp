@@ -68,6 +68,8 @@ struct StepDesc {
     float residual_tolerance;       // > 0: stop sweeping once the residual is below it
     uint32_t max_iterations;        // cap for the residual-driven loop
     uint32_t warm_start;            // 0: plain (the only source the oracle models)
+    uint32_t collect_events;        // not used by the oracle (it always keeps its events)
+    uint32_t residual_norm;         // stop rule: 0 largest row violation, 1 RMS
 };
 struct StepStats {
     uint32_t candidate_pairs, active_pairs, contacts, colors, islands, iterations, impact, status;
@@ -141,7 +143,7 @@ template <class R> struct SavedContact {
     V3<R> anchor_a, anchor_b;
 };
 template <class R> struct SavedPair {
-    uint32_t pair{};
+    uint64_t pair{};  // a * N + b in 64 bits (the reference's uint32 code for N <= 65,535)
     uint64_t epoch{};
     R dt{};
     uint32_t count{};
@@ -264,8 +266,8 @@ template <class R> struct World {
     std::vector<SavedPair<R>> saved;  // sorted by pair code
     uint64_t epoch{};
     // Last tick, for inspection by tests.
-    std::vector<uint32_t> candidate_pairs;
-    std::vector<uint32_t> active_pairs;  // non-empty manifolds only, code order
+    std::vector<uint64_t> candidate_pairs;
+    std::vector<uint64_t> active_pairs;  // non-empty manifolds only, code order
     std::vector<Manifold<R>> manifolds;   // parallel to active_pairs
     std::vector<V3<R>> aabb_lo, aabb_hi;
     std::vector<R> residual_trace;
@@ -273,7 +275,7 @@ template <class R> struct World {
     // Residual of the current dual pass: squares, rows, largest violation.
     double res_sq{};
     uint64_t res_n{};
-    R res_max{}, residual_max_last{};
+    R res_max{}, residual_max_last{}, residual_rms_last{};
     void residual_add(R v) {
         res_sq += double(v) * double(v);
         ++res_n;
@@ -716,7 +718,7 @@ template <class R> inline V3<R> log_axis(Q4<R> frame, V3<R> lg, unsigned axis) {
     if (s > R(1)) {
         R ang = std::sqrt(s);
         R half = R(0.5) * ang;
-        coef = (R(1) - half * std::cos(half) / std::sin(half)) / s;
+        coef = (R(1) - x_cot(half)) / s;
     }
     V3<R> u = unit_axis<R>(axis);
     V3<R> l = add(add(u, mul(cross(lg, u), R(0.5))), mul(cross(lg, cross(lg, u)), coef));
@@ -823,13 +825,23 @@ inline R visit_joint(JointRt<R>& j, const World<R>& w, const std::vector<State<R
     V3<R> old_error = sub(add(previous[b].x, rotate(previous[b].q, lb)), add(previous[a].x, rotate(previous[a].q, la)));
     Q4<R> frame_a = qnormalize(qmul(sa.q, fa_l)), frame_b = qnormalize(qmul(sb.q, fb_l));
     Q4<R> old_a = qnormalize(qmul(previous[a].q, fa_l)), old_b = qnormalize(qmul(previous[b].q, fb_l));
-    V3<R> twist = rotation_vector(qrelative(frame_a, frame_b, true));
-    V3<R> old_twist = rotation_vector(qrelative(old_a, old_b, true));
     const uint32_t t = o.type;
+    // The relative-rotation terms feed angular rows only. A point joint with
+    // no angular limit, spring or motor emits none, so for it they are not
+    // evaluated (pure functions of the poses: the rows are unchanged).
+    const bool angular_rows = t != kPoint || o.ang_limit_axes != 0 || o.ang_spring_axes != 0 || o.motor_angular != 0;
+    V3<R> twist{}, old_twist{};
+    if (angular_rows) {
+        twist = rotation_vector(qrelative(frame_a, frame_b, true));
+        old_twist = rotation_vector(qrelative(old_a, old_b, true));
+    }
     bool swing = t == kHinge || t == kPiston || (t == kMotor && o.motor_angular != 0);
     V3<R> free_axis = t == kHinge ? V3<R>{0, 0, 1} : V3<R>{1, 0, 0};
-    V3<R> swing_axis = inv_rotate(frame_a, rotate(frame_b, free_axis));
-    V3<R> old_swing = inv_rotate(old_a, rotate(old_b, free_axis));
+    V3<R> swing_axis{}, old_swing{};
+    if (angular_rows) {
+        swing_axis = inv_rotate(frame_a, rotate(frame_b, free_axis));
+        old_swing = inv_rotate(old_a, rotate(old_b, free_axis));
+    }
     V3<R> rotation = swing ? cross(free_axis, swing_axis) : twist;
     V3<R> old_rotation = swing ? cross(free_axis, old_swing) : old_twist;
     R lin_pen = pair_stiffness<R>(w.body[a], w.body[b], dt);
@@ -838,7 +850,7 @@ inline R visit_joint(JointRt<R>& j, const World<R>& w, const std::vector<State<R
         V3<R> old_dir = rotate(old_a, unit_axis<R>(axis));
         bool generic = t == kGeneric || t == kGenericSpring;
         bool motor_type = t == kMotor;
-        for (unsigned av = 0; av < 2; ++av) {
+        for (unsigned av = 0; av < (angular_rows ? 2u : 1u); ++av) {
             bool angular = av != 0;
             bool lock = angular ? (t == kFixed || t == kSlider || (t == kHinge && axis != 2) ||
                                    (t == kPiston && axis != 0) ||

@@ -62,6 +62,8 @@ def lib():
         L.oracle_update_dual.argtypes = [f32, f32, f32, f32, f32, f32, f32, vp]
         L.oracle_project_contact.argtypes = [vp, f32, vp]
         L.oracle_row_eval.argtypes = [vp, vp]
+        L.oracle_trig_eval.restype = None
+        L.oracle_trig_eval.argtypes = [vp, vp]
         _lib = L
     return _lib
 
@@ -137,14 +139,14 @@ class OracleWorld:
 
     def candidate_pairs(self):
         n = lib().oracle_candidate_pairs(self.h, None, 0)
-        out = np.zeros(max(n, 1), np.uint32)
+        out = np.zeros(max(n, 1), np.uint64)
         lib().oracle_candidate_pairs(self.h, out.ctypes.data, n)
         return out[:n]
 
     def manifolds(self):
         """codes[P], counts[P], contacts[P, 8, 22] (see oracle_capi.cpp)."""
         n = lib().oracle_manifolds(self.h, None, None, None, 0)
-        codes = np.zeros(max(n, 1), np.uint32)
+        codes = np.zeros(max(n, 1), np.uint64)
         counts = np.zeros(max(n, 1), np.uint32)
         contacts = np.zeros((max(n, 1), 8, 22), np.float32)
         lib().oracle_manifolds(self.h, codes.ctypes.data, counts.ctypes.data, contacts.ctypes.data, n)
@@ -226,4 +228,13 @@ def row_eval(values42):
     v = np.ascontiguousarray(values42, np.float32)
     out = np.zeros(7, np.float32)
     lib().oracle_row_eval(v.ctypes.data, out.ctypes.data)
+    return out
+
+
+def trig_eval(values3):
+    """(atan2(y, x), t cos(t) / sin(t)) of one (y, x, t) record, as the
+    oracle's FP32 tick evaluates them."""
+    v = np.ascontiguousarray(values3, np.float32)
+    out = np.zeros(2, np.float32)
+    lib().oracle_trig_eval(v.ctypes.data, out.ctypes.data)
     return out

@@ -165,7 +165,7 @@ void oracle_write_states(void* hp, uint32_t first, uint32_t count, const StateDe
     });
 }
 
-uint32_t oracle_candidate_pairs(void* hp, uint32_t* out, uint32_t cap) {
+uint32_t oracle_candidate_pairs(void* hp, uint64_t* out, uint32_t cap) {
     return with(static_cast<Handle*>(hp), [&](auto& w) {
         uint32_t n = uint32_t(w.candidate_pairs.size());
         for (uint32_t i = 0; i < n && i < cap; ++i) out[i] = w.candidate_pairs[i];
@@ -175,7 +175,7 @@ uint32_t oracle_candidate_pairs(void* hp, uint32_t* out, uint32_t cap) {
 
 // Per active (non-empty) pair: code, count; per contact: normal[3], point[3],
 // penetration, error[3], dual lambda/penalty x3, anchors a/b -> 22 floats.
-uint32_t oracle_manifolds(void* hp, uint32_t* codes, uint32_t* counts, float* contacts, uint32_t cap) {
+uint32_t oracle_manifolds(void* hp, uint64_t* codes, uint32_t* counts, float* contacts, uint32_t cap) {
     return with(static_cast<Handle*>(hp), [&](auto& w) {
         uint32_t n = uint32_t(w.active_pairs.size());
         if (cap < n) return n;
@@ -211,7 +211,7 @@ uint32_t oracle_contact_events(void* hp, float* out, uint32_t capacity) {
         const uint32_t n = w.n;
         for (uint32_t k = 0; k < w.active_pairs.size(); ++k) {
             const auto& m = w.manifolds[k];
-            const uint32_t a = w.active_pairs[k] / n, b = w.active_pairs[k] % n;
+            const uint32_t a = uint32_t(w.active_pairs[k] / n), b = uint32_t(w.active_pairs[k] % n);
             for (uint32_t p = 0; p < m.count; ++p, ++cursor) {
                 if (cursor >= capacity || !out) continue;
                 const auto& c = m.c[p];
@@ -327,6 +327,13 @@ void oracle_project_contact(const float* trial3, float friction, float* out6) {
 }
 // values: a[6] b[6] lambda penalty error velocity lower upper stiffness
 // damping beta reference_force, da[6] db[6] dt diag[6] first -> out: error,
+// The FP32 arctangent and x cot(x) the oracle's tick uses: in (y, x, t),
+// out (atan2(y, x), t cos(t) / sin(t)).
+void oracle_trig_eval(const float* v, float* out2) {
+    out2[0] = atan2_q1(v[0], v[1]);
+    out2[1] = x_cot(v[2]);
+}
+
 // trial, force, advanced lambda, advanced penalty, sum(g), sum(diag h)
 void oracle_row_eval(const float* v, float* out7) {
     Row<float> r{};

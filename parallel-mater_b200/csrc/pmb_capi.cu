@@ -152,6 +152,7 @@ StepParams params_from(const pmb_step_desc& s) {
     p.max_iterations = s.max_iterations;
     p.warm_start = s.warm_start;
     p.collect_events = s.collect_events;
+    p.residual_norm = s.residual_norm;
     return p;
 }
 
@@ -337,7 +338,7 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     ALLOC(d.c_aa, cap_contact); ALLOC(d.c_ab, cap_contact); ALLOC(d.c_lam, cap_contact);
     ALLOC(d.c_pen, cap_contact); ALLOC(d.c_accf, cap_contact);
     for (int side = 0; side < 2; ++side) {
-        uint32_t** code = side ? &d.out_code : &d.sv_code;
+        uint64_t** code = side ? &d.out_code : &d.sv_code;
         uint32_t** off = side ? &d.out_off : &d.sv_off;
         uint32_t** cnt = side ? &d.out_cnt : &d.sv_cnt;
         uint32_t** np = side ? &d.out_n_pairs : &d.sv_n_pairs;
@@ -691,6 +692,7 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     d.large_extent = 2.0f * sorted[n / 2] * 4.0f;
     d.solve_variant = 1;  // 384 threads: the fastest plan on a settled 65k-box pile
     d.solve_policy = 0;
+    d.barrier_spins = kDefaultBarrierSpins;
     for (uint32_t v = 0; v < kSolveVariants; ++v) {
         const SolveVariant& sv = solve_variants[v];
         cudaFuncSetAttribute(sv.ptr, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sv.smem));
@@ -921,7 +923,7 @@ int pmb_world_apply_impulse(pmb_world* w, uint32_t body, const float* linear, co
     return check(cudaStreamSynchronize(w->stream));
 }
 
-int pmb_world_candidate_pairs(pmb_world* w, uint32_t* codes, uint32_t capacity, uint32_t* count) {
+int pmb_world_candidate_pairs(pmb_world* w, uint64_t* codes, uint32_t capacity, uint32_t* count) {
     if (!w) return PMB_ERROR_INVALID_ARGUMENT;
     pmb_step_stats st;
     int r = pmb_world_last_stats(w, &st);
@@ -932,12 +934,12 @@ int pmb_world_candidate_pairs(pmb_world* w, uint32_t* codes, uint32_t capacity, 
         std::vector<uint32_t> a(n), b(n);
         cudaMemcpy(a.data(), w->d.cand_a, 4 * n, cudaMemcpyDeviceToHost);
         cudaMemcpy(b.data(), w->d.cand_b, 4 * n, cudaMemcpyDeviceToHost);
-        for (uint32_t k = 0; k < n; ++k) codes[k] = a[k] * w->d.n + b[k];
+        for (uint32_t k = 0; k < n; ++k) codes[k] = uint64_t(a[k]) * w->d.n + b[k];
     }
     return check(cudaGetLastError());
 }
 
-int pmb_world_manifolds(pmb_world* w, uint32_t* codes, uint32_t* counts, float* contacts, uint32_t capacity,
+int pmb_world_manifolds(pmb_world* w, uint64_t* codes, uint32_t* counts, float* contacts, uint32_t capacity,
                         uint32_t* count) {
     if (!w) return PMB_ERROR_INVALID_ARGUMENT;
     pmb_step_stats st;
@@ -947,7 +949,7 @@ int pmb_world_manifolds(pmb_world* w, uint32_t* codes, uint32_t* counts, float* 
     if (count) *count = n;
     if (!codes || capacity < n || n == 0) return PMB_SUCCESS;
     std::vector<uint32_t> off(n), cnt(n);
-    cudaMemcpy(codes, w->d.act_code, 4 * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(codes, w->d.act_code, 8 * size_t(n), cudaMemcpyDeviceToHost);
     cudaMemcpy(off.data(), w->d.act_off, 4 * n, cudaMemcpyDeviceToHost);
     cudaMemcpy(cnt.data(), w->d.act_cnt, 4 * n, cudaMemcpyDeviceToHost);
     if (counts) std::memcpy(counts, cnt.data(), 4 * n);
@@ -1443,6 +1445,12 @@ int pmb_world_set_launch_plan(pmb_world* w, uint32_t solve_variant, uint32_t sol
     return PMB_SUCCESS;
 }
 
+int pmb_world_set_barrier_limit(pmb_world* w, uint32_t spins) {
+    if (!w) return PMB_ERROR_INVALID_ARGUMENT;
+    w->d.barrier_spins = spins ? spins : kDefaultBarrierSpins;
+    return PMB_SUCCESS;
+}
+
 int pmb_world_autotune(pmb_world* w, const pmb_step_desc* step, uint32_t ticks, uint32_t* solve_variant,
                        uint32_t* solve_policy, char* report, uint32_t capacity) {
     if (!w || !step || ticks == 0) return PMB_ERROR_INVALID_ARGUMENT;
@@ -1499,8 +1507,8 @@ int pmb_world_stream(pmb_world* w, void** stream) {
 }
 
 int pmb_math_eval(uint32_t kind, uint32_t count, const float* in, float* out) {
-    static const uint32_t in_w[4] = {27, 7, 4, 42}, out_w[4] = {7, 5, 6, 7};
-    if (kind > 3 || !in || !out) return PMB_ERROR_INVALID_ARGUMENT;
+    static const uint32_t in_w[5] = {27, 7, 4, 42, 3}, out_w[5] = {7, 5, 6, 7, 2};
+    if (kind > 4 || !in || !out) return PMB_ERROR_INVALID_ARGUMENT;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return PMB_ERROR_NO_DEVICE;
     if (count == 0) return PMB_SUCCESS;
@@ -1558,6 +1566,10 @@ __global__ void k_math_eval(uint32_t kind, uint32_t count, const float* in, floa
         o[3] = s.n;
         o[4] = s.t0;
         o[5] = s.t1;
+    } else if (kind == 4) {
+        const float* v = in + 3 * size_t(i);
+        out[2 * size_t(i)] = atan2_q1(v[0], v[1]);
+        out[2 * size_t(i) + 1] = x_cot(v[2]);
     } else {
         const float* v = in + 42 * size_t(i);
         Row r;

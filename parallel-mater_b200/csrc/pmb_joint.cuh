@@ -46,7 +46,7 @@ __device__ __forceinline__ V3 log_axis(Q4 frame, V3 lg, unsigned axis) {
     if (s > 1.0f) {
         float ang = sqrtf(s);
         float half = 0.5f * ang;
-        coef = (1.0f - half * cosf(half) / sinf(half)) / s;
+        coef = (1.0f - x_cot(half)) / s;
     }
     V3 u = unit_axis(axis);
     V3 l = add(add(u, mul(cross(lg, u), 0.5f)), mul(cross(lg, cross(lg, u)), coef));

@@ -6,7 +6,8 @@
 // (the reference compiles with --fmad=false, CMakeLists.txt:421), and every
 // expression keeps the reference's evaluation order, so results track the
 // serial FP32 restatement to the last bit except where a libm function
-// (atan2f, sinf, cosf) rounds differently.
+// would round differently on the host and the device: arctangent and
+// cotangent are evaluated by atan2_q1 / x_cot below from basic operations.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -85,12 +86,64 @@ PMB_HD V3 rotation_displacement(Q4 from, Q4 to, V3 v) {
     V3 oc = cross(o, v), dc = cross(d, v);
     return mul(add(add(mul(oc, to.w - from.w), mul(dc, to.w)), add(cross(d, oc), cross(n, dc))), 2.0f);
 }
+// Arctangent and cotangent from IEEE-exact basic operations only (+ - * /
+// and sqrt, no contraction), so this library and a serial FP32 restatement
+// compiled without contraction evaluate them to the same bits; libm atan2f,
+// sinf and cosf round differently on the host and on the device.
+//
+// atan2 for the first quadrant (y >= 0, x >= 0, not both zero): with
+// t = min/max in [0, 1], the addition formula atan(t) = pi/6 +
+// atan((sqrt(3) t - 1) / (t + sqrt(3))) when t > tan(pi/12) leaves
+// |u| <= tan(pi/12), where the Maclaurin series u - u^3/3 + u^5/5 - ... is
+// summed to u^15 (truncation below 1e-10 relative); pi/2 - atan(x/y) when
+// y > x. A few ulp from the correctly rounded value.
+PMB_HD float atan2_q1(float y, float x) {
+    const bool swap = y > x;
+    const float t = swap ? x / y : y / x;
+    const bool shift = t > 0.26794919f;  // tan(pi/12)
+    const float u = shift ? (t * 1.7320508f - 1.0f) / (t + 1.7320508f) : t;
+    const float u2 = u * u;
+    float p = -1.0f / 15.0f;
+    p = 1.0f / 13.0f + u2 * p;
+    p = -1.0f / 11.0f + u2 * p;
+    p = 1.0f / 9.0f + u2 * p;
+    p = -1.0f / 7.0f + u2 * p;
+    p = 1.0f / 5.0f + u2 * p;
+    p = -1.0f / 3.0f + u2 * p;
+    p = 1.0f + u2 * p;
+    float r = u * p;
+    if (shift) r = 0.52359878f + r;  // pi/6
+    return swap ? 1.5707964f - r : r;
+}
+// x cos(x) / sin(x) for x in [0, pi/2]: Maclaurin series of sin to x^15
+// and of cos to x^16 (truncation below 1e-9 on that interval).
+PMB_HD float x_cot(float x) {
+    const float x2 = x * x;
+    float s = -1.0f / 1307674368000.0f;            // -1/15!
+    s = 1.0f / 6227020800.0f + x2 * s;             //  1/13!
+    s = -1.0f / 39916800.0f + x2 * s;              // -1/11!
+    s = 1.0f / 362880.0f + x2 * s;                 //  1/9!
+    s = -1.0f / 5040.0f + x2 * s;                  // -1/7!
+    s = 1.0f / 120.0f + x2 * s;                    //  1/5!
+    s = -1.0f / 6.0f + x2 * s;                     // -1/3!
+    s = 1.0f + x2 * s;                             // sin(x) / x
+    float c = 1.0f / 20922789888000.0f;            //  1/16!
+    c = -1.0f / 87178291200.0f + x2 * c;           // -1/14!
+    c = 1.0f / 479001600.0f + x2 * c;              //  1/12!
+    c = -1.0f / 3628800.0f + x2 * c;               // -1/10!
+    c = 1.0f / 40320.0f + x2 * c;                  //  1/8!
+    c = -1.0f / 720.0f + x2 * c;                   // -1/6!
+    c = 1.0f / 24.0f + x2 * c;                     //  1/4!
+    c = -0.5f + x2 * c;                            // -1/2!
+    c = 1.0f + x2 * c;                             // cos(x)
+    return c / s;                                  // x cos(x) / sin(x)
+}
 PMB_HD V3 rotation_vector(Q4 d) {
     float s = d.x * d.x + d.y * d.y + d.z * d.z;
     float scale = 2.0f + s * (1.0f / 3.0f + s * (3.0f / 20.0f + s * (5.0f / 56.0f + s * (35.0f / 576.0f))));
     if (s > 0.01f) {
         float vs = sqrtf(s);
-        scale = 2.0f * atan2f(vs, fclamp(d.w, 0.0f, 1.0f)) / vs;
+        scale = 2.0f * atan2_q1(vs, fclamp(d.w, 0.0f, 1.0f)) / vs;
     }
     return {d.x * scale, d.y * scale, d.z * scale};
 }

@@ -427,7 +427,7 @@ __global__ void k_compact(Dev d) {
         const uint32_t a = d.cand_a[k], b = d.cand_b[k];
         d.act_a[i] = a;
         d.act_b[i] = b;
-        d.act_code[i] = a * d.n + b;
+        d.act_code[i] = uint64_t(a) * d.n + b;
         d.act_off[i] = off;
         d.act_cnt[i] = count;
         const uint32_t src = d.np_stage[k];
@@ -463,7 +463,7 @@ __global__ void k_cache_load(Dev d, StepParams sp) {
     const bool dt_ok = !(fab(*d.sv_dt - dt) > 1.0e-7f);
     for (uint32_t i = grid_stride_begin(); i < n_act; i += grid_stride()) {
         if (!dt_ok || n_saved == 0) continue;
-        const uint32_t code = d.act_code[i];
+        const uint64_t code = d.act_code[i];
         uint32_t lo = 0, hi = n_saved;
         while (lo < hi) {
             uint32_t mid = (lo + hi) >> 1;

@@ -104,10 +104,13 @@ __global__ void k_color_noalloc(const uint32_t* offsets, const uint32_t* neighbo
                 ++changes;
             }
         }
-        if (overflow) atomicOr(h + kHStatus, 1u);
         if (changes) atomicAdd(h + kHChanged, changes);
         if (!barrier(h)) return;
         if (((volatile uint32_t*)h)[kHChanged] == before) {
+            // Converged: only this round's mex counts. A vertex may pass 255
+            // lower-neighbour colours in an intermediate round of the
+            // fixpoint and still settle below 256.
+            if (overflow) atomicOr(h + kHStatus, 1u);
             if (begin == 0) h[kHRounds] = round + 1;
             for (uint32_t v = begin; v < n; v += stride) colors[v] = work[v];
             return;
@@ -131,6 +134,20 @@ extern "C" int pmb_graph_color_noalloc(const uint32_t* offsets, const uint32_t* 
         return PMB_ERROR_CAPACITY_EXCEEDED;
     }
     if (device < 0 || device >= kMaxDevices) return PMB_ERROR_INVALID_ARGUMENT;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // The call reads its status back and waits for the stream, which a stream
+    // being captured into a graph cannot do: refuse before enqueuing anything
+    // (enqueuing would invalidate the caller's capture).
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &capturing) != cudaSuccess || capturing != cudaStreamCaptureStatusNone)
+        return PMB_ERROR_INVALID_ARGUMENT;
+    // The caller's current device is put back on every return.
+    int previous = -1;
+    if (cudaGetDevice(&previous) != cudaSuccess) return PMB_ERROR_NO_DEVICE;
+    struct Restore {
+        int dev;
+        ~Restore() { cudaSetDevice(dev); }
+    } restore{previous};
     if (cudaSetDevice(device) != cudaSuccess) return PMB_ERROR_NO_DEVICE;
     uint32_t* scratch = nullptr;
     {
@@ -151,7 +168,6 @@ extern "C" int pmb_graph_color_noalloc(const uint32_t* offsets, const uint32_t* 
         scratch = ds.ptr;
     }
     if (vertex_count == 0) return PMB_SUCCESS;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     // The header (barrier, counters, status) must start at zero; the working
     // colours are initialised by the kernel.
     if (cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * kHeaderWords, s) != cudaSuccess) return PMB_ERROR_DEVICE_LOST;
@@ -166,6 +182,7 @@ extern "C" int pmb_graph_color_noalloc(const uint32_t* offsets, const uint32_t* 
     if (cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&k_color_noalloc), dim3(blocks), dim3(kBlock), args,
                                     0, s) != cudaSuccess)
         return PMB_ERROR_DEVICE_LOST;
+    note_launch(uint32_t(blocks));
     uint32_t status = 0;
     if (cudaMemcpyAsync(&status, scratch + kHStatus, sizeof(status), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)

@@ -418,12 +418,13 @@ __device__ __forceinline__ void mark_higher(const Dev& d, uint32_t v, uint8_t* n
 // bodies whose mex can change), so the fixpoint is the same.
 __global__ void __launch_bounds__(kColorThreads) k_color(Dev d) {
     Counters* c = d.ctr;
+    if (c->status & kStBarrierTimeout) return;  // the tick was abandoned
     for (uint32_t round = 0; round < d.n + 2; ++round) {
         const uint32_t before = ((volatile uint32_t*)&c->changed)[0];
-        if (!grid_sync(c)) return;
+        if (!grid_sync(c, d.barrier_spins)) return;
         uint8_t* cur = d.cdirty + size_t(round & 1u) * d.n;
         uint8_t* next = d.cdirty + size_t((round + 1u) & 1u) * d.n;
-        bool overflow = false;
+        bool transient = false;  // a mex past 255 in this round (judged at the fixpoint)
         uint32_t changes = 0;
         for (uint32_t v = grid_stride_begin(); v < d.n; v += grid_stride()) {
             if (round != 0) {
@@ -431,18 +432,25 @@ __global__ void __launch_bounds__(kColorThreads) k_color(Dev d) {
                 cur[v] = 0;
             }
             if (d.motion[v] != kDynamic) continue;
-            uint32_t col = mex_lower(d, v, overflow);
+            uint32_t col = mex_lower(d, v, transient);
             if (col != d.color[v]) {
                 ((volatile uint32_t*)d.color)[v] = col;
                 ++changes;
                 mark_higher(d, v, next);
             }
         }
-        if (overflow) atomicOr(&c->status, kStColorOverflow);
         if (changes) atomicAdd(&c->changed, changes);
-        if (!grid_sync(c)) return;
+        if (!grid_sync(c, d.barrier_spins)) return;
         const uint32_t after = ((volatile uint32_t*)&c->changed)[0];
         if (after == before) {
+            // Converged. A body's mex can pass 255 colours in an intermediate
+            // round and still settle below 256, so overflow is judged on the
+            // final colours: a body left at the last colour whose lower
+            // neighbours still use every colour below it.
+            bool final_overflow = false;
+            for (uint32_t v = grid_stride_begin(); v < d.n; v += grid_stride())
+                if (d.motion[v] == kDynamic && d.color[v] == kMaxColors - 1) mex_lower(d, v, final_overflow);
+            if (final_overflow) atomicOr(&c->status, kStColorOverflow);
             if (grid_stride_begin() == 0) c->rounds = round + 1;
             return;
         }

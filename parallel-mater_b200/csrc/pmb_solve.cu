@@ -548,6 +548,7 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
     constexpr int kSolveThreads = T;
     Counters* c = d.ctr;
     if (phase != 0 && c->impact == 0) return;
+    if (c->status & kStBarrierTimeout) return;  // the tick was abandoned
     extern __shared__ __align__(16) uint8_t stage_raw[];
     const int lane = threadIdx.x & 31;
     uint8_t* warp_stage = stage_raw + (threadIdx.x >> 5) * kWarpStage;
@@ -645,7 +646,7 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
                 __syncthreads();
                 if (threadIdx.x == 0) atomicMax(&c->dbg_work[col], now());
             }
-            if (!grid_sync(c)) return;
+            if (!grid_sync(c, d.barrier_spins)) return;
             if (timing && it == 0 && col < 18 && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_release[col] = now();
         }
         Res res{0.0, 0u, 0.0f};
@@ -677,7 +678,7 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
             c->res_mx[blockIdx.x] = bm;
         }
         if (timing && it == 0 && threadIdx.x == 0) atomicMax(&c->dbg_work[19], now());
-        if (!grid_sync(c)) return;
+        if (!grid_sync(c, d.barrier_spins)) return;
         if (timing && it == 0 && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_release[19] = now();
         double tsq = 0.0;
         uint32_t tn = 0;
@@ -688,11 +689,14 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
             tmx = fmx(tmx, ((volatile float*)c->res_mx)[k]);
         }
         const float rms = tn ? float(sqrt(tsq / double(tn))) : 0.0f;
-        if (phase == 0 && grid_stride_begin() == 0) c->residual_trace[it] = rms;
+        // The schedule's measure: the largest row violation of the sweep
+        // (every constraint within the tolerance), or the RMS over the rows.
+        const float measure = sp.residual_norm == 1 ? rms : tmx;
+        if (phase == 0 && grid_stride_begin() == 0) c->residual_trace[it] = measure;
         bool last = it + 1 == iters;
-        if (adaptive && rms <= sp.tolerance) last = true;
+        if (adaptive && measure <= sp.tolerance) last = true;
         // Every block has read the partials before the next pass rewrites them.
-        if (!last && colors == 0 && !grid_sync(c)) return;
+        if (!last && colors == 0 && !grid_sync(c, d.barrier_spins)) return;
         if (last) {
             if (grid_stride_begin() == 0) {
                 c->claim[0] = c->claim[1] = 0u;  // every block is past its last claim

@@ -80,6 +80,7 @@ struct StepParams {
     uint32_t debug_timing;  // record solve-kernel timestamps for iteration 0
     uint32_t warm_start;    // 0 plain, 1 learned, 2 table
     uint32_t collect_events;
+    uint32_t residual_norm;  // residual-driven schedule: 0 largest row violation, 1 RMS
 };
 
 struct ContactEvent {  // pmb_contact_event
@@ -143,6 +144,9 @@ struct Dev {
     // Launch plan (pmb_world_autotune): solve kernel variant, colour width
     // policy (0: 8/16/32 lanes per body by colour size, 1: always 8).
     uint32_t solve_variant, solve_policy;
+    // Spins a block waits at a grid barrier before it gives up, latches
+    // kStBarrierTimeout and abandons the tick (pmb_world_set_barrier_limit).
+    uint32_t barrier_spins;
     // Batched independent scenes (n_scenes > 1): bodies of scene s are the
     // contiguous range [scene_body_off[s], scene_body_off[s+1]). Bodies of
     // different scenes never pair: grid buckets are keyed by scene, large
@@ -215,17 +219,20 @@ struct Dev {
     uint2* np_sat;      // their separation (float bits) and reference face (bit 31: side)
     float4 *st_n, *st_p;
     // active pairs / contacts
-    uint32_t *act_a, *act_b, *act_code, *act_off, *act_cnt, *act_impact;
+    uint32_t *act_a, *act_b, *act_off, *act_cnt, *act_impact;
+    uint64_t* act_code;  // a * N + b in 64 bits (the reference's uint32 code while N <= 65,535)
     uint32_t* c_pair;
     uint2* c_bodies;  // (a, b) of the contact's pair
     float4* c_jac;    // 9 per contact: jacobian rows n,t0,t1 of body a then body b
     float4 *c_n, *c_p, *c_e, *c_aa, *c_ab, *c_lam, *c_pen, *c_accf;
     // contact cache from the previous tick (double-buffered by the host)
-    uint32_t *sv_code, *sv_off, *sv_cnt;
+    uint64_t* sv_code;
+    uint32_t *sv_off, *sv_cnt;
     uint32_t* sv_n_pairs;  // device count of saved pairs
     float4 *sv_local, *sv_normal, *sv_fimp, *sv_lam, *sv_pen, *sv_aa, *sv_ab;
     float* sv_dt;
-    uint32_t *out_code, *out_off, *out_cnt, *out_n_pairs;
+    uint64_t* out_code;
+    uint32_t *out_off, *out_cnt, *out_n_pairs;
     float4 *out_local, *out_normal, *out_fimp, *out_lam, *out_pen, *out_aa, *out_ab;
     float* out_dt;
     // graph
@@ -267,9 +274,12 @@ __device__ __forceinline__ uint32_t grid_stride_begin() { return blockIdx.x * bl
 __device__ __forceinline__ uint32_t grid_stride() { return gridDim.x * blockDim.x; }
 
 // Grid barrier for cooperative launches: arrive on a counter, the last block
-// bumps the generation. Waits are bounded; a timeout latches
-// kStBarrierTimeout and the caller abandons the tick.
-__device__ __forceinline__ bool grid_sync(Counters* c) {
+// bumps the generation. Waits are bounded by `spins` polls (about 2^26 by
+// default, seconds); a timeout latches kStBarrierTimeout and the caller
+// abandons the tick: every later cooperative kernel of the tick returns at
+// once, and the host reports the status.
+constexpr uint32_t kDefaultBarrierSpins = 1u << 26;
+__device__ __forceinline__ bool grid_sync(Counters* c, uint32_t spins_limit) {
     __syncthreads();
     __shared__ int ok;
     if (threadIdx.x == 0) {
@@ -285,7 +295,7 @@ __device__ __forceinline__ bool grid_sync(Counters* c) {
         } else {
             uint32_t spins = 0;
             while (*gen == g) {
-                if (++spins > (1u << 26)) {
+                if (++spins > spins_limit) {
                     atomicOr(&c->status, kStBarrierTimeout);
                     ok = 0;
                     break;

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 
@@ -107,6 +108,14 @@ PmResult require_recording(PmCommandBuffer_T* buffer) {
 }
 
 PmResult record(PmCommandBuffer_T* buffer, std::function<PmResult()> command) {
+#if defined(PMB_TEST_FAILURE_DRIVER)
+    // Test build only (reference src/api/internal.hpp:375-381): a recording
+    // allocation failure, latched until the buffer is begun again.
+    if (std::getenv("PM_TEST_FAIL_RECORDING") != nullptr) {
+        buffer->latched = PM_ERROR_OUT_OF_HOST_MEMORY;
+        return buffer->latched;
+    }
+#endif
     try {
         buffer->commands.push_back(std::move(command));
     } catch (const std::bad_alloc&) {
@@ -348,6 +357,11 @@ PmResult PMAPI_CALL pmAllocateMemory(PmDevice device, const PmMemoryAllocateInfo
     if (!device || !info || !valid_structure(info->sType, PM_STRUCTURE_TYPE_MEMORY_ALLOCATE_INFO, info->pNext) ||
         info->allocationSize == 0u || info->memoryTypeIndex > 1u)
         return PM_ERROR_INVALID_ARGUMENT;
+#if defined(PMB_TEST_FAILURE_DRIVER)
+    // Test build only (reference src/device/cpu_device.cpp:119-122): a device
+    // allocation failure that publishes no handle.
+    if (std::getenv("PM_TEST_FAIL_ALLOCATION") != nullptr) return PM_ERROR_OUT_OF_DEVICE_MEMORY;
+#endif
     auto* created = new (std::nothrow) PmDeviceMemory_T;
     if (!created) return PM_ERROR_OUT_OF_HOST_MEMORY;
     const int r = pmb_device_alloc(device->ordinal, info->allocationSize, info->memoryTypeIndex == 1u ? 1 : 0,
@@ -855,6 +869,11 @@ PmResult PMAPI_CALL pmQueueSubmit(PmQueue queue, const PmSubmitInfo* info, PmFen
             if (info->pSignals[k].semaphore == s.semaphore) greatest = std::max(greatest, info->pSignals[k].value);
         if (s.value <= greatest) return PM_ERROR_INVALID_ARGUMENT;
     }
+#if defined(PMB_TEST_FAILURE_DRIVER)
+    // Test build only (reference src/device/submission.cpp:45-48): the
+    // submission fails before acceptance, so nothing becomes pending.
+    if (std::getenv("PM_TEST_FAIL_SUBMISSION") != nullptr) return PM_ERROR_OUT_OF_HOST_MEMORY;
+#endif
     auto completion = std::make_shared<Completion>();
     std::vector<std::function<PmResult()>> commands;
     std::vector<PmSimulation_T*> simulations;

@@ -16,6 +16,7 @@
 // the reference's command path runs (production_realtime_backend.cu.inc:7811-7830).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 
@@ -579,6 +580,17 @@ PmResult PMAPI_CALL pmCmdStepSimulation(PmCommandBuffer buffer, PmSimulation sim
                 r = from_core(pmb_world_set_targets(w, uint32_t(bodies.size()), bodies.data(), targets.data()));
                 simulation->targets.clear();
             }
+#if defined(PMB_TEST_FAILURE_DRIVER)
+            // Test build only: a device upload that fails at execution
+            // (reference src/device/cpu_device.cpp:151-153, reported through
+            // the fence), and grid-barrier waits bounded to a given number of
+            // polls so that they run out (a bounded wait, never a fault).
+            if (r == PM_SUCCESS && std::getenv("PM_TEST_FAIL_UPLOAD") != nullptr) r = PM_ERROR_OUT_OF_DEVICE_MEMORY;
+            if (r == PM_SUCCESS) {
+                const char* spins = std::getenv("PM_TEST_BARRIER_SPINS");
+                r = from_core(pmb_world_set_barrier_limit(w, spins ? uint32_t(std::strtoul(spins, nullptr, 10)) : 0u));
+            }
+#endif
             if (r == PM_SUCCESS) {
                 pmb_step_desc sd{};
                 sd.dt = copied.timestep;

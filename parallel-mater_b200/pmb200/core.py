@@ -90,6 +90,7 @@ def lib():
             "pmb_world_joints": [vp, vp, vp, vp, u32],
             "pmb_world_scene_stats": [vp, vp, vp, vp, vp, u32],
             "pmb_world_set_launch_plan": [vp, u32, u32], "pmb_world_autotune": [vp, vp, u32, vp, vp, vp, u32],
+            "pmb_world_set_barrier_limit": [vp, u32],
             "pmb_world_contact_duals": [vp, u32, vp, vp, u32, vp],
             "pmb_world_mlp_attach": [vp, vp, u32], "pmb_world_mlp_train": [vp, i32, ctypes.c_float, u32],
             "pmb_world_mlp_params": [vp, vp, vp, vp, vp], "pmb_world_mlp_apply_mode": [vp, u32], "pmb_world_mlp_rows": [vp, vp, vp, u32, vp],
@@ -238,7 +239,7 @@ class World:
     def candidate_pairs(self):
         n = ctypes.c_uint32()
         _check(lib().pmb_world_candidate_pairs(self.h, None, 0, ctypes.byref(n)), "candidate_pairs")
-        out = np.zeros(max(n.value, 1), np.uint32)
+        out = np.zeros(max(n.value, 1), np.uint64)
         _check(lib().pmb_world_candidate_pairs(self.h, out.ctypes.data, n.value, ctypes.byref(n)),
                "candidate_pairs")
         return out[:n.value]
@@ -247,7 +248,7 @@ class World:
         n = ctypes.c_uint32()
         _check(lib().pmb_world_manifolds(self.h, None, None, None, 0, ctypes.byref(n)), "manifolds")
         k = max(n.value, 1)
-        codes = np.zeros(k, np.uint32)
+        codes = np.zeros(k, np.uint64)
         counts = np.zeros(k, np.uint32)
         contacts = np.zeros((k, 8, 22), np.float32)
         _check(lib().pmb_world_manifolds(self.h, codes.ctypes.data, counts.ctypes.data,
@@ -295,6 +296,11 @@ class World:
 
     def set_launch_plan(self, solve_variant=0, solve_policy=0):
         _check(lib().pmb_world_set_launch_plan(self.h, solve_variant, solve_policy), "pmb_world_set_launch_plan")
+
+    def set_barrier_limit(self, spins=0):
+        """Polls a block makes at a grid barrier before the tick is abandoned
+        with PMB_STATUS_BARRIER_TIMEOUT (0: the default)."""
+        _check(lib().pmb_world_set_barrier_limit(self.h, spins), "set_barrier_limit")
 
     def autotune(self, desc=None, ticks=3, **kw):
         """Time every launch plan over `ticks` ticks (state restored), keep
@@ -398,11 +404,11 @@ def kernel_launches() -> int:
     return n.value
 
 
-_MATH_WIDTH = {0: (27, 7), 1: (7, 5), 2: (4, 6), 3: (42, 7)}
+_MATH_WIDTH = {0: (27, 7), 1: (7, 5), 2: (4, 6), 3: (42, 7), 4: (3, 2)}
 
 
 def math_eval(kind: int, inputs: np.ndarray) -> np.ndarray:
-    """Run the device AVBD math (0 block solve, 1 dual, 2 contact, 3 row)."""
+    """Run the device AVBD math (0 block solve, 1 dual, 2 contact, 3 row, 4 trig)."""
     win, wout = _MATH_WIDTH[kind]
     x = np.ascontiguousarray(inputs, np.float32).reshape(-1, win)
     out = np.zeros((len(x), wout), np.float32)

@@ -244,6 +244,15 @@ SIGNATURES = {
 _drv = None
 
 
+def use_driver(path=None):
+    """Load the driver from `path` (default: libpm_b200_driver.so) for the
+    sessions created afterwards; the test build with failure injection is
+    libpm_b200_driver_failtest.so."""
+    global _drv, DRIVER_PATH
+    DRIVER_PATH = path or os.path.join(PKG_DIR, "libpm_b200_driver.so")
+    _drv = None
+
+
 def driver():
     """The loaded driver with its four entry points typed."""
     global _drv

@@ -50,7 +50,7 @@ assert JOINT_DTYPE.itemsize == 220
 STEP_DTYPE = np.dtype([
     ("dt", "<f4"), ("gravity", "<f4", 3), ("profile", "<u4"), ("requested_iterations", "<u4"),
     ("base_iterations", "<u4"), ("residual_tolerance", "<f4"), ("max_iterations", "<u4"),
-    ("warm_start", "<u4"), ("collect_events", "<u4")])
+    ("warm_start", "<u4"), ("collect_events", "<u4"), ("residual_norm", "<u4")])
 
 STATS_DTYPE = np.dtype([
     ("candidate_pairs", "<u4"), ("active_pairs", "<u4"), ("contacts", "<u4"), ("colors", "<u4"),
@@ -81,7 +81,7 @@ class Scene:
         return len(self.bodies)
 
     def step_desc(self, *, dt=DT, profile=None, iterations=None, residual_tolerance=0.0,
-                  max_iterations=0, warm_start=0, collect_events=0) -> np.ndarray:
+                  max_iterations=0, warm_start=0, collect_events=0, residual_norm=0) -> np.ndarray:
         s = np.zeros((), STEP_DTYPE)
         s["dt"] = dt
         s["gravity"] = (0.0, -9.81, 0.0)
@@ -92,6 +92,7 @@ class Scene:
         s["max_iterations"] = max_iterations
         s["warm_start"] = warm_start
         s["collect_events"] = collect_events
+        s["residual_norm"] = residual_norm
         return s
 
 

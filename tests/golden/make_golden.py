@@ -18,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("PMB_REFERENCE_ROOT", "/root/reference"))
     args = ap.parse_args()
     with tempfile.TemporaryDirectory() as tmp:
         exe = os.path.join(tmp, "gen")

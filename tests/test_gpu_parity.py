@@ -308,3 +308,15 @@ def test_contact_events_match_oracle(gpu_available):
     w.step()
     assert len(w.contact_events()) == 0
     w.close()
+
+
+def test_device_trig_equals_oracle_bits(gpu_available):
+    """The tick's arctangent and x cot(x) evaluate to the oracle's bits."""
+    rng = np.random.Generator(np.random.Philox(22))
+    inp = np.zeros((5000, 3), np.float32)
+    inp[:, :2] = rng.uniform(0.0, 1.0, (5000, 2))
+    inp[:100, 1] = 0.0
+    inp[:, 2] = rng.uniform(0.0, np.pi / 2, 5000)
+    out = core.math_eval(4, inp)
+    ref = np.array([O.trig_eval(r) for r in inp])
+    assert np.array_equal(out.view(np.uint32), ref.view(np.uint32))

@@ -47,7 +47,11 @@ def test_forward_backward_matches_oracle(gpu_available, n):
 def test_online_training_and_learned_ticks(gpu_available):
     scene = scenes.box_pile((8, 6, 8), seed=12, spacing=1.3)
     w = core.World(scene)
-    kw = dict(residual_tolerance=2e-4, max_iterations=48)
+    # Training mechanics on ticks stopped by the RMS residual: the loss is
+    # measured against each tick's converged rows, and under the row-max stop
+    # the sweep count (and with it the converged penalties) of this small pile
+    # varies from tick to tick, which no per-contact prediction can follow.
+    kw = dict(residual_tolerance=2e-4, max_iterations=48, residual_norm=1)
     for _ in range(60):
         w.step(**kw)
     w.mlp_attach(seed=3)

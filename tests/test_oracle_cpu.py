@@ -23,7 +23,7 @@ from pmb200 import scenes
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
-REF = "/root/reference"
+REF = os.environ.get("PMB_REFERENCE_ROOT", "/root/reference")
 
 
 def _num(v):
@@ -315,3 +315,20 @@ def test_guided_contacts_stop_a_piston_at_the_guided_offset(kind):
     assert stop_face - 2e-4 <= x["x"][1, 0] <= stop_face
     assert abs(x["v"][1, 0]) < 1e-3
     assert max(counts) == 1 and sum(counts) >= 3
+
+
+def test_fp32_arctangent_and_cotangent_accuracy():
+    """The FP32 tick's own atan2 (first quadrant) and x cot(x) on [0, pi/2]
+    (addition formula plus Maclaurin series, basic operations only): within
+    3 ulp of the float64 atan2, and 3e-7 absolute of x cos(x) / sin(x)."""
+    rng = np.random.Generator(np.random.Philox(21))
+    yx = rng.uniform(0.0, 1.0, (4000, 2)).astype(np.float32)
+    yx[:200, 1] = 0.0                       # x = 0: pi/2
+    yx[200:400, 0] = yx[200:400, 1]         # y = x: pi/4
+    t = np.linspace(0.5, np.pi / 2, 4000).astype(np.float32)
+    for (y, x), tt in zip(yx, t):
+        a, c = O.trig_eval([y, x, tt])
+        exact = np.arctan2(np.float64(y), np.float64(x))
+        assert abs(float(a) - exact) <= 3 * float(np.spacing(np.float32(exact))), (y, x, a, exact)
+        ref = np.float64(tt) * np.cos(np.float64(tt)) / np.sin(np.float64(tt))
+        assert abs(float(c) - ref) <= 3e-7, (tt, c, ref)

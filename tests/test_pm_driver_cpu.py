@@ -24,7 +24,7 @@ from pmb200 import pm
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 HEADER = os.path.join(REPO, "include", "pm_b200.h")
-REF_INCLUDE = "/root/reference/include"
+REF_INCLUDE = os.path.join(os.environ.get("PMB_REFERENCE_ROOT", "/root/reference"), "include")
 ENTRY_POINTS = {"pm_driverNegotiateLoaderInterfaceVersion", "pm_driverGetInstanceProcAddr",
                 "pm_driverGetDeviceProcAddr", "pm_driverGetPhysicalDeviceProcAddr"}
 
