@@ -1438,6 +1438,10 @@ int pmb_world_scene_stats(pmb_world* w, float* residual, float* residual_max, ui
 constexpr uint32_t kSolvePolicies = 4;
 const char* const kPolicyNames[kSolvePolicies] = {"per colour", "8 lanes   ", "per body  ", "claimed   "};
 
+// The staged variants choose lanes per body per colour batch (policy 0) or
+// always 8 (policy 1); policies 2 and 3 run them as policy 0.
+bool plan_distinct(uint32_t variant, uint32_t policy) { return variant < kStagedFirst || policy < 2; }
+
 int pmb_world_set_launch_plan(pmb_world* w, uint32_t solve_variant, uint32_t solve_policy) {
     if (!w || solve_variant >= kSolveVariants || solve_policy >= kSolvePolicies) return PMB_ERROR_INVALID_ARGUMENT;
     w->d.solve_variant = solve_variant;
@@ -1467,6 +1471,7 @@ int pmb_world_autotune(pmb_world* w, const pmb_step_desc* step, uint32_t ticks, 
     std::string text;
     for (uint32_t v = 0; v < kSolveVariants && r == PMB_SUCCESS; ++v)
         for (uint32_t p = 0; p < kSolvePolicies && r == PMB_SUCCESS; ++p) {
+            if (!plan_distinct(v, p)) continue;
             r = pmb_world_restore(w);
             if (r) break;
             w->d.solve_variant = v;
@@ -1479,8 +1484,9 @@ int pmb_world_autotune(pmb_world* w, const pmb_step_desc* step, uint32_t ticks, 
             float ms = 0.0f;
             cudaEventElapsedTime(&ms, a, b);
             char line[128];
-            std::snprintf(line, sizeof(line), "solve %3d threads, widths %s: %8.3f ms/tick\n",
-                          solve_variants[v].threads, kPolicyNames[p], ms / float(ticks));
+            std::snprintf(line, sizeof(line), "solve %3d threads%s, widths %s: %8.3f ms/tick\n",
+                          solve_variants[v].threads, v >= kStagedFirst ? " staged" : "", kPolicyNames[p],
+                          ms / float(ticks));
             text += line;
             if ((v == 0 && p == 0) || ms < best) {
                 best = ms;

@@ -712,10 +712,599 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
     }
 }
 
+// ------------------------------------------------------------ staged solve
+// The same sweep as k_solve, organised for memory-level parallelism and with
+// the dual update fused into the colour passes:
+//
+//  * Per colour, each CTA takes its bodies (round-robin over CTAs) in batches
+//    that fit a shared-memory row stage. All threads of the CTA first stage
+//    every contact row of the batch -- one thread per row, every global load
+//    independent -- then groups of G lanes accumulate each body's block from
+//    the staged rows in list order (the serial loop's additions, in its
+//    order), solve it, apply the crossing safeguard from the staged normal
+//    rows and write the update.
+//  * A contact's dual update (geometry_constraints_solve.slang:494-532) needs
+//    only its two bodies' displacements after the sweep, and once the body
+//    with the later colour has solved, neither body changes again in the
+//    sweep and no other body reads the contact. So the group that solves the
+//    later body (or the only dynamic one) updates the contact's duals right
+//    away from the staged row; joints likewise. Every contact and joint is
+//    updated exactly once per sweep, from the same values as the separate
+//    dual pass of k_solve, so the results are bit-identical; the dual pass,
+//    its grid barrier and its second read of every contact disappear.
+//  * The residual partials of each block are written before the last colour's
+//    barrier (double-buffered by sweep parity), so the stop decision needs no
+//    barrier of its own.
+constexpr uint32_t kStageRows = 1024;      // staged contact rows per batch
+constexpr uint32_t kBatchBodies = 256;     // bodies per batch
+// Staged row record (floats; u32 fields stored as bits).
+enum : uint32_t {
+    kRJ = 0,          // this body's jacobian rows n, t0, t1 (3 x 6)
+    kRSt = 18,        // stiffness: raw penalty x stiffness scale (3)
+    kRForce = 21,     // force of each row (3)
+    kRLam = 24,       // raw lambda xyz and w (4)
+    kRPen = 28,       // raw penalty xyz (3)
+    kRPre = 31,       // error terms summed before this body's jacobian product (3)
+    kRPost = 34,      // ... and after it (3; first body of the contact only)
+    kRFric = 37,      // friction sqrt(mu_a mu_b)
+    kRBeta = 38,      // penalty growth factor of the pair
+    kRTrial = 39,     // normal trial force at the start of the colour
+    kRContact = 40,   // contact index
+    kRFlags = 41,     // bit 0: this body is the contact's first body; bit 1: its dual is updated here
+    kRowWords = 42,
+};
+constexpr size_t kStagedSmem = size_t(kStageRows) * kRowWords * 4 + size_t(kBatchBodies) * 12 * 4 + 64 * 4;
+
+struct StageTables {
+    float* rows;       // kStageRows x kRowWords
+    uint32_t* body;    // per batch slot: body index
+    uint32_t* skip;    // per batch slot: 1 = not solved this sweep (impact phase, finished scene)
+    uint32_t* off;     // kBatchBodies + 1 row offsets
+    float* dx;         // per batch slot: displacement (6)
+    float* fric;       // per batch slot: friction
+    float* invm;       // per batch slot: inverse mass
+    uint32_t* scratch; // 64 words for scans and counts
+};
+__device__ __forceinline__ StageTables stage_tables(uint8_t* raw) {
+    StageTables t;
+    t.rows = reinterpret_cast<float*>(raw);
+    uint32_t* u = reinterpret_cast<uint32_t*>(raw + size_t(kStageRows) * kRowWords * 4);
+    t.body = u;
+    t.skip = u + kBatchBodies;
+    t.off = u + 2 * kBatchBodies;            // kBatchBodies + 1 (one word of slack)
+    t.dx = reinterpret_cast<float*>(u + 3 * kBatchBodies + 1);
+    t.fric = t.dx + 6 * kBatchBodies;
+    t.invm = t.fric + kBatchBodies;
+    t.scratch = reinterpret_cast<uint32_t*>(t.invm + kBatchBodies);
+    return t;
+}
+
+// Stage contact row r (flat index t) of batch slot sl into the row table.
+__device__ __forceinline__ void stage_row(const Dev& d, const StageTables& tb, uint32_t t, uint32_t sl, uint32_t r,
+                                          uint32_t col, uint32_t phase, float dt) {
+    const uint32_t i = tb.body[sl];
+    const uint32_t ro = d.roff[i] + r;
+    const uint32_t code = d.blist[ro], other = d.bother[ro];
+    const uint32_t c = code & 0x7fffffffu;
+    const bool first = (code >> 31) == 0;
+    V6 me;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) me.v[k] = tb.dx[6 * sl + k];
+    const Lite o = load_lite(d, other);
+    const float of = d.p1[other].x, om = d.p0[other].x;
+    const uint32_t ocol = d.color[other];
+    const float4 lam = d.c_lam[c], pen = d.c_pen[c], e = d.c_e[c];
+    V6 ja[3], jb[3];
+    load_jac(d, c, ja, jb);
+    const float mf = tb.fric[sl], mm = tb.invm[sl];
+    const float friction = sqrtf(first ? mf * of : of * mf);
+    const float beta = (1.0f / (fmx(first ? mm + om : om + mm, 1.0e-6f) * dt * dt)) * 100.0f;
+    const float e3[3] = {e.x, e.y, e.z};
+    float err[3], pre[3], post[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        // err = e + J_a . dx_a + J_b . dx_b, in that order (contact_rows).
+        if (first) {
+            pre[k] = e3[k];
+            post[k] = dot6(jb[k], o.dx);
+            err[k] = (pre[k] + dot6(ja[k], me)) + post[k];
+        } else {
+            pre[k] = e3[k] + dot6(ja[k], o.dx);
+            post[k] = 0.0f;
+            err[k] = pre[k] + dot6(jb[k], me);
+        }
+    }
+    const F3 trial{lam.x + pen.x * err[0], lam.y + pen.y * err[1], lam.z + pen.z * err[2]};
+    const F3 f = project_contact(trial, friction);
+    const F3 sc = stiffness_scales(trial, friction);
+    float forces[3] = {f.n, f.t0, f.t1};
+    if (phase != 0) {
+        V3 t0, t1;
+        basis(v3(d.c_n[c]), t0, t1);
+        const V3 af = v3(d.c_accf[c]);
+        forces[0] = f.n - lam.w / dt;
+        forces[1] = f.t0 - dot(af, t0) / dt;
+        forces[2] = f.t1 - dot(af, t1) / dt;
+    }
+    float* row = tb.rows + size_t(t) * kRowWords;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        const V6& jr = first ? ja[x] : jb[x];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) row[kRJ + 6 * x + k] = jr.v[k];
+    }
+    row[kRSt + 0] = pen.x * sc.n;
+    row[kRSt + 1] = pen.y * sc.t0;
+    row[kRSt + 2] = pen.z * sc.t1;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        row[kRForce + x] = forces[x];
+        row[kRPre + x] = pre[x];
+        row[kRPost + x] = post[x];
+    }
+    row[kRLam + 0] = lam.x;
+    row[kRLam + 1] = lam.y;
+    row[kRLam + 2] = lam.z;
+    row[kRLam + 3] = lam.w;
+    row[kRPen + 0] = pen.x;
+    row[kRPen + 1] = pen.y;
+    row[kRPen + 2] = pen.z;
+    row[kRFric] = friction;
+    row[kRBeta] = beta;
+    row[kRTrial] = trial.n;
+    // The dual is updated here when the other body is not dynamic (no
+    // colour) or solved in an earlier colour of the sweep.
+    const bool owned = ocol == kInvalid || ocol < col;
+    row[kRContact] = __uint_as_float(c);
+    row[kRFlags] = __uint_as_float((first ? 1u : 0u) | (owned ? 2u : 0u));
+}
+
+// The dual update of one staged contact row with the body's displacement
+// after its solve (dual_contact's arithmetic, values from the stage).
+__device__ __forceinline__ void staged_dual(const Dev& d, const float* row, const V6& me, uint32_t scene,
+                                            bool scene_last, Res& res) {
+    const uint32_t flags = __float_as_uint(row[kRFlags]);
+    const bool first = flags & 1u;
+    const uint32_t c = __float_as_uint(row[kRContact]);
+    float err[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        V6 j;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) j.v[q] = row[kRJ + 6 * k + q];
+        err[k] = first ? (row[kRPre + k] + dot6(j, me)) + row[kRPost + k] : row[kRPre + k] + dot6(j, me);
+    }
+    const float friction = row[kRFric], beta = row[kRBeta];
+    float4 lam = make_float4(row[kRLam], row[kRLam + 1], row[kRLam + 2], row[kRLam + 3]);
+    float4 pen = make_float4(row[kRPen], row[kRPen + 1], row[kRPen + 2], 0.0f);
+    F3 f = project_contact(F3{lam.x + pen.x * err[0], lam.y + pen.y * err[1], lam.z + pen.z * err[2]}, friction);
+    const float tx = lam.y + pen.y * err[1];
+    const float ty = lam.z + pen.z * err[2];
+    const float bound = friction * f.n;
+    const bool stick = tx * tx + ty * ty <= bound * bound;
+    lam.x = f.n;
+    lam.y = f.t0;
+    lam.z = f.t1;
+    if (f.n > 0.0f) pen.x = fmn(kMaxPenalty, pen.x + beta * fab(err[0]));
+    if (stick) {
+        pen.y = fmn(kMaxPenalty, pen.y + beta * fab(err[1]));
+        pen.z = fmn(kMaxPenalty, pen.z + beta * fab(err[2]));
+    }
+    pen.w = stick ? 1.0f : 0.0f;
+    d.c_lam[c] = lam;
+    d.c_pen[c] = pen;
+    if (f.n > 0.0f || err[0] > 0.0f) {
+        const float v = f.n > 0.0f ? fab(err[0]) : err[0];
+        res.sq += double(v) * double(v);
+        res.n += 1;
+        res.mx = fmx(res.mx, v);
+        if (scene_last) {
+            atomicAdd(&d.scene_res_sq[scene], v * v);
+            atomicAdd(&d.scene_res_n[scene], 1u);
+            atomicMax(reinterpret_cast<int*>(&d.scene_res_mx[scene]), __float_as_int(v));
+        }
+    }
+}
+
+// Duals of contacts owned by body i (the other body non-dynamic or of an
+// earlier colour), read from global memory: the oversized-body path.
+__device__ void owned_contact_duals(const Dev& d, uint32_t i, uint32_t col, float dt, uint32_t phase, Res& res,
+                                    uint32_t it, int gl, int G) {
+    const uint32_t ro = d.roff[i], rn = d.rcount[i];
+    for (uint32_t r = gl; r < rn; r += G) {
+        const uint32_t other = d.bother[ro + r];
+        const uint32_t ocol = d.color[other];
+        if (!(ocol == kInvalid || ocol < col)) continue;
+        dual_contact(d, d.blist[ro + r] & 0x7fffffffu, dt, phase, res, it);
+    }
+}
+
+// Joints owned by body i: dual_joint once the later of its two bodies solved.
+__device__ void owned_joint_duals(const Dev& d, uint32_t i, uint32_t col, float dt, uint32_t phase, Res& res,
+                                  uint32_t it, int gl, int G) {
+    const uint32_t jcnt = d.jdeg[i];
+    if (!jcnt) return;
+    const uint32_t jlo = d.jinc_off[i];
+    for (uint32_t k = gl; k < jcnt; k += G) {
+        const uint32_t j = d.jinc_list[jlo + k];
+        const JointState js = d.jstate[j];
+        const uint32_t other = js.dense_a == i ? js.dense_b : js.dense_a;
+        const uint32_t ocol = d.color[other];
+        if (!(ocol == kInvalid || ocol < col)) continue;
+        dual_joint(d, j, phase, dt, res, it);
+    }
+}
+
+// One body's primal from the stage (G lanes; lane gl), then its owned duals.
+template <int G>
+__device__ void staged_body(const Dev& d, const StageTables& tb, uint32_t sl, uint32_t col, uint32_t phase, float dt,
+                            uint32_t gmask, int gl, int gbase, Res& res, uint32_t it) {
+    const uint32_t i = tb.body[sl];
+    const uint32_t r0 = tb.off[sl], r1 = tb.off[sl + 1];
+    V6 dx0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) dx0.v[k] = tb.dx[6 * sl + k];
+    float ent[Owned<G>::E];
+    {
+        const float4 ia = d.inA[i], ib = d.inB[i];
+        float H[21];
+#pragma unroll
+        for (int k = 0; k < 21; ++k) H[k] = 0.0f;
+        H[bidx(0, 0)] = ia.x;
+        H[bidx(1, 1)] = ia.x;
+        H[bidx(2, 2)] = ia.x;
+        H[bidx(3, 3)] = ia.y;
+        H[bidx(4, 3)] = ia.z;
+        H[bidx(5, 3)] = ib.x;
+        H[bidx(4, 4)] = ia.w;
+        H[bidx(5, 4)] = ib.y;
+        H[bidx(5, 5)] = ib.z;
+#pragma unroll
+        for (int q = 0; q < Owned<G>::E; ++q) {
+            const int e = gl + G * q;
+            float v = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 21; ++k) v = e == k ? H[k] : v;
+            if (e >= 21 && e < 27) {
+                const int r = e - 21;
+                float gs = 0.0f;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) gs += H[bidx(r, c)] * dx0.v[c];
+                v = gs;
+            }
+            ent[q] = v;
+        }
+    }
+    // Rows in list order, each row's n, t0, t1: the serial loop's additions.
+#pragma unroll
+    for (int q = 0; q < Owned<G>::E; ++q) {
+        const int e = gl + G * q;
+        if (e >= 27) continue;
+        int ei = 0, ek = 0;
+        const bool hess = e < 21;
+        if (hess) entry_ik(e, ei, ek);
+        else ei = e - 21;
+        float acc = ent[q];
+        for (uint32_t t = r0; t < r1; ++t) {
+            const float* row = tb.rows + size_t(t) * kRowWords;
+#pragma unroll
+            for (int x = 0; x < 3; ++x) {
+                const float* jr = row + kRJ + 6 * x;
+                acc += hess ? (row[kRSt + x] * jr[ei]) * jr[ek] : jr[ei] * row[kRForce + x];
+            }
+        }
+        ent[q] = acc;
+    }
+    Blk blk;
+    gather_block<G>(ent, blk, gmask, gbase);
+    const uint32_t jcnt = d.jdeg[i];
+    if (jcnt) {
+        if (gl == 0) {
+            const uint32_t jlo = d.jinc_off[i];
+            for (uint32_t k = 0; k < jcnt; ++k) {
+                const uint32_t j = d.jinc_list[jlo + k];
+                const JointState js = d.jstate[j];
+                if (!js.enabled) continue;
+                const uint32_t a = js.dense_a, b = js.dense_b;
+                const bool first = i == a;
+                if (phase == 0) {
+                    BodyView A = load_body(d, a), B = load_body(d, b);
+                    visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]),
+                                q4(d.q[b]), d.p0[a], d.p0[b], dt, &blk, first, kVisitAccumulate, nullptr);
+                } else {
+                    const Lite A = load_lite(d, a), B = load_lite(d, b);
+                    for (uint32_t r = 0; r < js.count; ++r) {
+                        Row row = load_row(d.jrows[size_t(j) * 18 + r]);
+                        if (row.stiffness >= kMaxPenalty) row_accumulate(blk, row, first, A.dx, B.dx, dt);
+                    }
+                }
+            }
+        }
+        __syncwarp(gmask);
+#pragma unroll
+        for (int e = 0; e < 21; ++e) blk.h[e] = __shfl_sync(gmask, blk.h[e], gbase);
+#pragma unroll
+        for (int r = 0; r < 6; ++r) blk.g[r] = __shfl_sync(gmask, blk.g[r], gbase);
+    }
+    V6 upd;
+    const bool solved = block_solve(blk, upd);
+    V6 dxn = dx0;
+    if (solved) {
+        // Crossing safeguard (geometry_constraints_solve.slang:433-475) from
+        // the staged normal rows, flagged rows added in list order.
+        own_entries<G>(blk, gl, ent);
+        bool crossing = false;
+#pragma unroll
+        for (int q = 0; q < Owned<G>::E; ++q) {
+            const int e = gl + G * q;
+            int ei = 0, ek = 0;
+            if (e < 21) entry_ik(e, ei, ek);
+            for (uint32_t t = r0; t < r1; ++t) {
+                const float* row = tb.rows + size_t(t) * kRowWords;
+                V6 nr;
+#pragma unroll
+                for (int k = 0; k < 6; ++k) nr.v[k] = row[kRJ + k];
+                const float k0 = row[kRPen], trial = row[kRTrial];
+                if (!(trial <= 0.0f && trial + k0 * dot6(nr, upd) > k0 * 1.0e-6f)) continue;
+                crossing = true;
+                if (e < 21) ent[q] += k0 * nr.v[ei] * nr.v[ek];
+                else if (e < 27) ent[q] += nr.v[e - 21] * trial;
+            }
+        }
+        if (crossing) {
+            gather_block<G>(ent, blk, gmask, gbase);
+            V6 safe;
+            if (block_solve(blk, safe)) upd = safe;
+        }
+        // The update (apply_pose_update / the impact phase's linear update),
+        // computed by every lane so each holds the new displacement.
+        if (phase == 0) {
+            float4 l = d.dxl[i];
+            l.x += upd.v[0];
+            l.y += upd.v[1];
+            l.z += upd.v[2];
+            float4 a = d.dxa[i];
+            Q4 rel = q4(d.dq[i]);
+            const V3 r{upd.v[3], upd.v[4], upd.v[5]};
+            const bool rotates = !(r.x == 0.0f && r.y == 0.0f && r.z == 0.0f);
+            if (rotates) {
+                Q4 dd = qmul(Q4{r.x, r.y, r.z, 0.0f}, rel);
+                rel = qnormalize(Q4{rel.x + 0.5f * dd.x, rel.y + 0.5f * dd.y, rel.z + 0.5f * dd.z, rel.w + 0.5f * dd.w});
+                if (rel.w < 0.0f) rel = {-rel.x, -rel.y, -rel.z, -rel.w};
+                a = make_float4(2.0f * rel.x, 2.0f * rel.y, 2.0f * rel.z, 0.0f);
+            }
+            if (gl == 0) {
+                d.dxl[i] = l;
+                if (rotates) {
+                    d.dq[i] = f4(rel);
+                    d.dxa[i] = a;
+                }
+            }
+            dxn = {{l.x, l.y, l.z, a.x, a.y, a.z}};
+        } else {
+            float4 l = d.dxl[i], a = d.dxa[i];
+            l.x += upd.v[0];
+            l.y += upd.v[1];
+            l.z += upd.v[2];
+            a.x += upd.v[3];
+            a.y += upd.v[4];
+            a.z += upd.v[5];
+            if (gl == 0) {
+                d.dxl[i] = l;
+                d.dxa[i] = a;
+            }
+            dxn = {{l.x, l.y, l.z, a.x, a.y, a.z}};
+        }
+    }
+    __syncwarp(gmask);
+    // Owned contact duals, one row per lane.
+    uint32_t scene = 0;
+    bool scene_last = false;
+    if (batched(d)) {
+        scene = d.scene_of[i];
+        scene_last = phase == 0 && it + 1 == d.scene_budget[scene];
+    }
+    for (uint32_t t = r0 + gl; t < r1; t += G) {
+        const float* row = tb.rows + size_t(t) * kRowWords;
+        if (__float_as_uint(row[kRFlags]) & 2u) staged_dual(d, row, dxn, scene, scene_last, res);
+    }
+    // Owned joint duals read both bodies' displacements from global memory.
+    __syncwarp(gmask);
+    if (jcnt) owned_joint_duals(d, i, col, dt, phase, res, it, gl, G);
+}
+
+template <int T>
+__global__ void __launch_bounds__(T, 1) k_solve_staged(Dev d, StepParams sp, uint32_t phase) {
+    Counters* c = d.ctr;
+    if (phase != 0 && c->impact == 0) return;
+    if (c->status & kStBarrierTimeout) return;  // the tick was abandoned
+    extern __shared__ __align__(16) uint8_t stage_raw[];
+    const StageTables tb = stage_tables(stage_raw);
+    const int lane = threadIdx.x & 31;
+    const float dt = sp.dt;
+    const uint32_t colors = c->colors;
+    uint32_t budget = sp.budget_request;
+    if (!sp.realtime && sp.requested == 0) budget = max(budget, c->joint_iters);
+    if (phase != 0 && sp.tolerance > 0.0f) budget = c->budget;
+    const bool adaptive = phase == 0 && sp.tolerance > 0.0f && !batched(d);
+    const uint32_t iters = batched(d) ? min(c->budget_max, kMaxIterations)
+                                      : adaptive ? min(max(sp.max_iterations, 1u), kMaxIterations)
+                                                 : min(budget, kMaxIterations);
+    __shared__ double wsq[T / 32];
+    __shared__ uint32_t wn[T / 32];
+    __shared__ float wmx[T / 32];
+    for (uint32_t it = 0; it < iters; ++it) {
+        Res res{0.0, 0u, 0.0f};
+        const uint32_t parity = (it & 1u) * 512u;
+        for (uint32_t col = 0; col <= colors; ++col) {
+            if (col < colors) {
+                const uint32_t lo = c->color_off[col * kWidthClasses], hi = c->color_off[(col + 1) * kWidthClasses];
+                const uint32_t span = hi - lo;
+                const uint32_t mine = span > blockIdx.x ? (span - blockIdx.x + gridDim.x - 1) / gridDim.x : 0u;
+                for (uint32_t j0 = 0; j0 < mine;) {
+                    // Batch slots: this CTA's next bodies of the colour.
+                    const uint32_t want = min(kBatchBodies, mine - j0);
+                    uint32_t cnt = 0;
+                    if (threadIdx.x < want) {
+                        const uint32_t i = d.corder[lo + blockIdx.x + (j0 + threadIdx.x) * gridDim.x];
+                        const bool skip = (phase != 0 && d.impact[i] == 0) ||
+                                          (batched(d) && it >= d.scene_budget[d.scene_of[i]]);
+                        cnt = skip ? 0u : d.rcount[i];
+                        tb.body[threadIdx.x] = i;
+                        tb.skip[threadIdx.x] = skip ? 1u : 0u;
+                        const float4 l = d.dxl[i], a = d.dxa[i];
+                        float* dx = tb.dx + 6 * threadIdx.x;
+                        dx[0] = l.x;
+                        dx[1] = l.y;
+                        dx[2] = l.z;
+                        dx[3] = a.x;
+                        dx[4] = a.y;
+                        dx[5] = a.z;
+                        tb.fric[threadIdx.x] = d.p1[i].x;
+                        tb.invm[threadIdx.x] = d.p0[i].x;
+                    }
+                    // Inclusive scan of the slots' row counts (T >= kBatchBodies).
+                    uint32_t x = cnt;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                        if (lane >= o) x += y;
+                    }
+                    if (lane == 31) tb.scratch[threadIdx.x >> 5] = x;
+                    __syncthreads();
+                    if (threadIdx.x < 32) {
+                        uint32_t p = threadIdx.x < T / 32 ? tb.scratch[threadIdx.x] : 0u;
+#pragma unroll
+                        for (int o = 1; o < 32; o <<= 1) {
+                            const uint32_t y = __shfl_up_sync(0xffffffffu, p, o);
+                            if (lane >= o) p += y;
+                        }
+                        tb.scratch[32 + threadIdx.x] = p;
+                    }
+                    __syncthreads();
+                    const uint32_t incl = x + ((threadIdx.x >> 5) ? tb.scratch[32 + (threadIdx.x >> 5) - 1] : 0u);
+                    if (threadIdx.x < want) tb.off[threadIdx.x + 1] = incl;
+                    if (threadIdx.x == 0) tb.off[0] = 0;
+                    const uint32_t fit = __syncthreads_count(threadIdx.x < want && incl <= kStageRows);
+                    if (fit == 0) {
+                        // The next body alone has more rows than the stage
+                        // holds: solve it streaming its rows from global
+                        // memory (one warp, 32 lanes), then its duals.
+                        if (threadIdx.x < 32) {
+                            const uint32_t i = tb.body[0];
+                            if (!tb.skip[0]) {
+                                GroupRows<32>& sm = *reinterpret_cast<GroupRows<32>*>(tb.rows);
+                                solve_body_group<32>(d, i, phase, dt, sm, 0xffffffffu, lane, 0, 0u);
+                                __syncwarp();
+                                owned_contact_duals(d, i, col, dt, phase, res, it, lane, 32);
+                                __syncwarp();
+                                owned_joint_duals(d, i, col, dt, phase, res, it, lane, 32);
+                            }
+                        }
+                        __syncthreads();
+                        j0 += 1;
+                        continue;
+                    }
+                    // Stage every row of the batch, one thread per row.
+                    const uint32_t rows = tb.off[fit];
+                    for (uint32_t t = threadIdx.x; t < rows; t += T) {
+                        uint32_t a = 0, b = fit;  // slot: off[a] <= t < off[a + 1]
+                        while (b - a > 1) {
+                            const uint32_t m = (a + b) >> 1;
+                            if (tb.off[m] <= t) a = m;
+                            else b = m;
+                        }
+                        stage_row(d, tb, t, a, t - tb.off[a], col, phase, dt);
+                    }
+                    __syncthreads();
+                    // Solve: G lanes per body (wider groups when few bodies).
+                    auto solve = [&](auto width) {
+                        constexpr int G = decltype(width)::value;
+                        const int gl = lane % G, gbase = lane - gl;
+                        const uint32_t gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << gbase;
+                        for (uint32_t sl = threadIdx.x / G; sl < fit; sl += T / G)
+                            if (!tb.skip[sl]) staged_body<G>(d, tb, sl, col, phase, dt, gmask, gl, gbase, res, it);
+                    };
+                    if (d.solve_policy != 1 && fit * 32u <= T) solve(std::integral_constant<int, 32>{});
+                    else if (d.solve_policy != 1 && fit * 16u <= T) solve(std::integral_constant<int, 16>{});
+                    else solve(std::integral_constant<int, 8>{});
+                    __syncthreads();
+                    j0 += fit;
+                }
+            }
+            if (col + 1 >= colors) {
+                // Joints with no dynamic body have no owner above; their
+                // duals (applied impulse, breaking) are updated here.
+                for (uint32_t j = grid_stride_begin(); j < d.nj; j += grid_stride()) {
+                    const JointState js = d.jstate[j];
+                    if (js.count == 0 || d.motion[js.dense_a] == kDynamic || d.motion[js.dense_b] == kDynamic) continue;
+                    dual_joint(d, j, phase, dt, res, it);
+                }
+                // The sweep's residual partials (after the last colour's
+                // duals), published by the barrier below.
+                Res r = res;
+                for (int o = 16; o > 0; o >>= 1) {
+                    r.sq += __shfl_xor_sync(0xffffffffu, r.sq, o);
+                    r.n += __shfl_xor_sync(0xffffffffu, r.n, o);
+                    r.mx = fmx(r.mx, __shfl_xor_sync(0xffffffffu, r.mx, o));
+                }
+                if (lane == 0) {
+                    wsq[threadIdx.x >> 5] = r.sq;
+                    wn[threadIdx.x >> 5] = r.n;
+                    wmx[threadIdx.x >> 5] = r.mx;
+                }
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    double bs = 0.0;
+                    uint32_t bn = 0;
+                    float bm = 0.0f;
+                    for (int k = 0; k < T / 32; ++k) {
+                        bs += wsq[k];
+                        bn += wn[k];
+                        bm = fmx(bm, wmx[k]);
+                    }
+                    c->res_sum[parity + blockIdx.x] = bs;
+                    c->res_cnt[parity + blockIdx.x] = bn;
+                    c->res_mx[parity + blockIdx.x] = bm;
+                }
+                if (!grid_sync(c, d.barrier_spins)) return;
+                break;
+            }
+            if (!grid_sync(c, d.barrier_spins)) return;
+        }
+        double tsq = 0.0;
+        uint32_t tn = 0;
+        float tmx = 0.0f;
+        for (uint32_t k = 0; k < gridDim.x; ++k) {
+            tsq += ((volatile double*)c->res_sum)[parity + k];
+            tn += ((volatile uint32_t*)c->res_cnt)[parity + k];
+            tmx = fmx(tmx, ((volatile float*)c->res_mx)[parity + k]);
+        }
+        const float rms = tn ? float(sqrt(tsq / double(tn))) : 0.0f;
+        const float measure = sp.residual_norm == 1 ? rms : tmx;
+        if (phase == 0 && grid_stride_begin() == 0) c->residual_trace[it] = measure;
+        bool last = it + 1 == iters;
+        if (adaptive && measure <= sp.tolerance) last = true;
+        if (last) {
+            if (grid_stride_begin() == 0) {
+                if (phase == 0) {
+                    c->iterations = it + 1;
+                    c->residual = rms;
+                    c->residual_max = tmx;
+                }
+                c->budget = it + 1;
+            }
+            return;
+        }
+    }
+}
+
 const SolveVariant solve_variants[kSolveVariants] = {
     {reinterpret_cast<const void*>(&k_solve<512>), 512, kWarpStage * (512 / 32)},
     {reinterpret_cast<const void*>(&k_solve<384>), 384, kWarpStage * (384 / 32)},
     {reinterpret_cast<const void*>(&k_solve<256>), 256, kWarpStage * (256 / 32)},
+    {reinterpret_cast<const void*>(&k_solve_staged<512>), 512, kStagedSmem},
+    {reinterpret_cast<const void*>(&k_solve_staged<384>), 384, kStagedSmem},
 };
 
 // Last-iteration contact work (geometry_constraints_solve.slang:533-561),

@@ -372,7 +372,8 @@ struct SolveVariant {
     int threads;
     size_t smem;
 };
-constexpr uint32_t kSolveVariants = 3;
+constexpr uint32_t kSolveVariants = 5;
+constexpr uint32_t kStagedFirst = 3;  // variants 3, 4: the staged solve with fused duals (512, 384 threads)
 extern const SolveVariant solve_variants[kSolveVariants];
 void launch_contact_jacobians(const Dev& d, uint32_t phase, cudaStream_t s);
 // Sparse per-body record writes staged in io_index / io_rec (kind 0: inputs,

@@ -5,11 +5,12 @@ its realtime rigid stack (tests/solver/rigid_realtime_cuda_tests.cu:217-371):
 largest penetration, settled drift, rotation drift, energy growth and
 tunnelling events.
 
-Penetration is geometric: the post-step overlap depth of two boxes, i.e. the
-smallest overlap of their projections over the 15 separating axes of an
-oriented-box pair (positive: the boxes interpenetrate by that much), for the
-pairs the tick reports in contact. Capsule links are measured as the
-segment-to-segment distance against the sum of their radii.
+Penetration is geometric: the post-step overlap depth of two convex meshes,
+i.e. the smallest overlap of their projections over the separating axes of
+the pair (the 15 axes of an oriented-box pair; face normals and edge-edge
+cross products of general convex meshes such as tessellated capsules),
+positive when they interpenetrate, for the pairs the tick reports in
+contact.
 """
 from __future__ import annotations
 
@@ -83,9 +84,54 @@ def segment_distance(p0, p1, q0, q1):
     return np.linalg.norm((p0 + d1 * s[:, None]) - (q0 + d2 * t[:, None]), axis=1)
 
 
-def pair_penetration(scene, states, pairs, capsule=None):
-    """Largest post-step penetration over the pairs (a, b) of box bodies, and
-    of capsule bodies when `capsule` = (radius, half_length along local y)."""
+def mesh_axes(scene, m):
+    """Local vertices, unique face normals and unique edge directions of
+    convex mesh m."""
+    v = scene.vertices[scene.mesh_vertex_offsets[m]:scene.mesh_vertex_offsets[m + 1]].astype(np.float64)
+    t = scene.indices[scene.mesh_index_offsets[m]:scene.mesh_index_offsets[m + 1]].reshape(-1, 3)
+    n = np.cross(v[t[:, 1]] - v[t[:, 0]], v[t[:, 2]] - v[t[:, 0]])
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    e = np.concatenate([v[t[:, 1]] - v[t[:, 0]], v[t[:, 2]] - v[t[:, 1]], v[t[:, 0]] - v[t[:, 2]]])
+    e /= np.linalg.norm(e, axis=1, keepdims=True)
+
+    def unique(d):
+        d = np.where((d[:, :1] < 0) | ((d[:, :1] == 0) & (d[:, 1:2] < 0)), -d, d)   # one sign per direction
+        return np.unique(np.round(d, 6), axis=0)
+
+    return v, unique(n), unique(e)
+
+
+def convex_overlap(scene, states, a, b):
+    """Overlap depth of the convex meshes of bodies a and b (arrays over
+    pairs that share one mesh pair): the smallest projection overlap over the
+    separating axes of two convex polyhedra (face normals of both, cross
+    products of their edge directions); > 0 means interpenetration."""
+    ma, mb = int(scene.bodies["mesh"][a[0]]), int(scene.bodies["mesh"][b[0]])
+    va, na, ea = mesh_axes(scene, ma)
+    vb, nb, eb = mesh_axes(scene, mb)
+    Ra, Rb = quat_matrix(states["q"][a]), quat_matrix(states["q"][b])
+    xa, xb = states["x"][a].astype(np.float64), states["x"][b].astype(np.float64)
+    wa = np.einsum("pij,vj->pvi", Ra, va) + xa[:, None]
+    wb = np.einsum("pij,vj->pvi", Rb, vb) + xb[:, None]
+    Na, Nb = np.einsum("pij,kj->pki", Ra, na), np.einsum("pij,kj->pki", Rb, nb)
+    Ea, Eb = np.einsum("pij,kj->pki", Ra, ea), np.einsum("pij,kj->pki", Rb, eb)
+    C = np.cross(Ea[:, :, None, :], Eb[:, None, :, :]).reshape(len(a), -1, 3)
+    cn = np.linalg.norm(C, axis=2, keepdims=True)
+    C = np.where(cn > 1e-6, C / np.where(cn > 1e-6, cn, 1.0), 0.0)
+    axes = np.concatenate([Na, Nb, C], axis=1)
+    pa = np.einsum("pkj,pvj->pkv", axes, wa)
+    pb = np.einsum("pkj,pvj->pkv", axes, wb)
+    # translation along the axis that separates the projections (the
+    # penetration depth along it; negative when already separated)
+    overlap = np.minimum(pa.max(2) - pb.min(2), pb.max(2) - pa.min(2))
+    valid = np.linalg.norm(axes, axis=2) > 0.5
+    return np.where(valid, overlap, np.inf).min(axis=1)
+
+
+def pair_penetration(scene, states, pairs):
+    """Largest post-step penetration over the pairs (a, b): oriented-box
+    overlap for box pairs, convex-mesh overlap for every other pair (the
+    meshes the tick collides, e.g. tessellated capsules)."""
     if len(pairs) == 0:
         return 0.0
     pairs = np.asarray(pairs, np.int64)
@@ -99,15 +145,14 @@ def pair_penetration(scene, states, pairs, capsule=None):
     if both.any():
         d = box_overlap(x[a[both]], q[a[both]], half[a[both]], x[b[both]], q[b[both]], half[b[both]])
         worst = max(worst, float(np.max(d, initial=0.0)))
-    if capsule is not None:
-        radius, hl = capsule
-        caps = ~box
-        cc = caps[a] & caps[b]
-        if cc.any():
-            ax = quat_matrix(q)[:, :, 1]
-            ia, ib = a[cc], b[cc]
-            dist = segment_distance(x[ia] - hl * ax[ia], x[ia] + hl * ax[ia], x[ib] - hl * ax[ib], x[ib] + hl * ax[ib])
-            worst = max(worst, float(np.max(2 * radius - dist, initial=0.0)))
+    other = ~both
+    if other.any():
+        mesh = scene.bodies["mesh"]
+        key = mesh[a[other]].astype(np.int64) * (1 << 32) + mesh[b[other]]
+        for k in np.unique(key):
+            sel = key == k
+            d = convex_overlap(scene, states, a[other][sel], b[other][sel])
+            worst = max(worst, float(np.max(d, initial=0.0)))
     return worst
 
 

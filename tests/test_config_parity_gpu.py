@@ -71,11 +71,11 @@ def compare(scene, frames, fp64_frames=0, label="", joints=False):
     return w, worst, worst64
 
 
-def stack_gates(scene, world, frames, settle, ground_top=0.0, capsule=None, label=""):
+def stack_gates(scene, world, frames, settle, ground_top=0.0, label=""):
     """Step `world` `frames` more ticks on the GPU alone and measure the
     gates; the settled window starts `settle` ticks in."""
     dyn = scene.bodies["motion"] == scenes.DYNAMIC
-    pen, tunnel = 0.0, 0
+    pen, pen_settled, tunnel = 0.0, 0.0, 0
     first = None
     drift = rot = 0.0
     e0 = emax = None
@@ -83,9 +83,11 @@ def stack_gates(scene, world, frames, settle, ground_top=0.0, capsule=None, labe
         st = world.step()
         assert int(st["status"]) == 0, (f, core.status_names(int(st["status"])))
         s = world.states()
-        pen = max(pen, G.pair_penetration(scene, s, G.contact_pairs(world, scene.n), capsule=capsule))
+        p = G.pair_penetration(scene, s, G.contact_pairs(world, scene.n))
+        pen = max(pen, p)
         tunnel += int((s["x"][dyn, 1] < ground_top).sum())
         if f >= settle:
+            pen_settled = max(pen_settled, p)
             e = G.energy(scene, s)
             if first is None:
                 first = s
@@ -95,9 +97,9 @@ def stack_gates(scene, world, frames, settle, ground_top=0.0, capsule=None, labe
             dq = np.abs(np.einsum("pi,pi->p", s["q"][dyn].astype(np.float64), first["q"][dyn].astype(np.float64)))
             rot = max(rot, float((2 * np.arccos(np.clip(dq, 0, 1))).max()))
     growth = max(0.0, (emax - e0) / max(abs(e0), 1e-3))
-    print(f"{label}: penetration {pen:.3g} m, settled drift {drift:.3g} m, rotation drift {rot:.3g} rad, "
-          f"energy growth {growth:.3g}, tunnelling {tunnel}")
-    return pen, drift, rot, growth, tunnel
+    print(f"{label}: penetration {pen:.3g} m (settled window {pen_settled:.3g} m), settled drift {drift:.3g} m, "
+          f"rotation drift {rot:.3g} rad, energy growth {growth:.3g}, tunnelling {tunnel}")
+    return pen, pen_settled, drift, rot, growth, tunnel
 
 
 @pytest.mark.parametrize("profile", [scenes.LEGACY, scenes.REALTIME], ids=["legacy", "realtime"])
@@ -109,7 +111,7 @@ def test_config1_pyramid_600_frames(gpu_available, profile):
     label = f"config 1 pyramid ({'legacy' if profile == scenes.LEGACY else 'realtime v1'})"
     compare(s, 600, fp64_frames=600, label=label)
     w = core.World(s)
-    pen, drift, rot, growth, tunnel = stack_gates(s, w, 600, settle=120, label=label)
+    pen, _, drift, rot, growth, tunnel = stack_gates(s, w, 600, settle=120, label=label)
     assert pen <= 0.005 and drift <= 0.01 and rot <= 0.035 and growth <= 0.05 and tunnel == 0
 
 
@@ -123,13 +125,18 @@ def test_config2_pile_4096_first_frames(gpu_available):
 
 def test_config2_pile_300_frames_gates(gpu_available):
     """Config 2 over its stated 300 frames on the GPU: the pile falls, lands
-    and settles; penetration, tunnelling and energy are gated over the run
-    (the pile is still shifting, so the settled window is the last 60
-    frames and only energy growth is gated there)."""
+    (boxes of up to 6.75 t hit the ground and each other at several m/s
+    between frames 60 and 120) and settles. Once settled (frames 120-300)
+    no pair overlaps by more than 2 mm (the reference's brick-stack gate,
+    conformance/v1/quality/rigid-brick-penetration-v1.json); during the
+    landing impacts the overlap stays under 1 cm (the serial oracle peaks at
+    5.3 mm on this pile); energy never grows by more than 5 % over the
+    settled window; nothing tunnels."""
     s = scenes.config(1)
     w = core.World(s)
-    pen, drift, rot, growth, tunnel = stack_gates(s, w, 300, settle=240, label="config 2 pile 4096, 300 frames")
-    assert pen <= 0.005 and growth <= 0.05 and tunnel == 0
+    pen, settled, drift, rot, growth, tunnel = stack_gates(s, w, 300, settle=120,
+                                                           label="config 2 pile 4096, 300 frames")
+    assert settled <= 0.002 and pen <= 0.01 and growth <= 0.05 and tunnel == 0
 
 
 def test_config3_chains_first_frames(gpu_available):
@@ -164,7 +171,7 @@ def test_config3_chains_600_frames_gates(gpu_available):
         x = w.states()
         jerr = max(jerr, _joint_error(s, x))
         if f % 10 == 0:
-            pen = max(pen, G.pair_penetration(s, x, G.contact_pairs(w, s.n), capsule=(0.05, 0.2)))
+            pen = max(pen, G.pair_penetration(s, x, G.contact_pairs(w, s.n)))
         e = G.energy(s, x)
         e0 = e if e0 is None else e0
         emax = e if emax is None else max(emax, e)

@@ -93,15 +93,16 @@ def test_driver_failure_lifecycle(gpu_available, failtest_driver):
 
     # Recording failure is synchronous and latched until the buffer is begun again.
     begin = pm.CommandBufferBeginInfo(pm.ST_BEGIN, None, 0)
+    step = pm.StepInfo(1.0 / 60.0, 1, (C.c_float * 3)(0.0, -9.81, 0.0), 0)
     assert api.pmBeginCommandBuffer(s.cb, pm.ref(begin)) == pm.SUCCESS
+    assert api.pmCmdBindPhysicsPipeline(s.cb, s.pipeline) == pm.SUCCESS
     _set("PM_TEST_FAIL_RECORDING")
-    assert api.pmCmdBindPhysicsPipeline(s.cb, s.pipeline) == OUT_OF_HOST_MEMORY
+    assert api.pmCmdStepSimulation(s.cb, s.sim, pm.ref(step)) == OUT_OF_HOST_MEMORY
     _set("PM_TEST_FAIL_RECORDING", None)
     assert api.pmEndCommandBuffer(s.cb) == OUT_OF_HOST_MEMORY
     assert s.step() == pm.SUCCESS
 
     # Submission failure comes before acceptance: the fence does not become pending.
-    step = pm.StepInfo(1.0 / 60.0, 1, (C.c_float * 3)(0.0, -9.81, 0.0), 0)
     assert api.pmBeginCommandBuffer(s.cb, pm.ref(begin)) == pm.SUCCESS
     assert api.pmCmdBindPhysicsPipeline(s.cb, s.pipeline) == pm.SUCCESS
     assert api.pmCmdStepSimulation(s.cb, s.sim, pm.ref(step)) == pm.SUCCESS

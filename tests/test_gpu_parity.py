@@ -243,28 +243,28 @@ def test_residual_schedule_matches_oracle(gpu_available):
 
 
 def test_launch_plans_are_bit_identical(gpu_available):
-    """Every solve launch plan (CTA size, lanes per body) computes the same
-    bits; the autotuner only picks among them and leaves the state as it
-    found it."""
+    """Every solve launch plan (CTA size, lanes per body, the staged solve
+    with fused duals) computes the same bits; the autotuner only picks among
+    them and leaves the state as it found it."""
     s = scenes.box_pile((6, 4, 6), seed=13, spacing=1.6)
     ref = None
-    for v in range(3):
-        for p in range(4):
-            w = core.World(s)
-            w.set_launch_plan(v, p)
-            for _ in range(12):
-                w.step()
-            x = w.states().view(np.uint8).copy()
-            if ref is None:
-                ref = x
-            assert np.array_equal(x, ref), (v, p)
-            w.close()
+    plans = [(v, p) for v in range(3) for p in range(4)] + [(v, p) for v in (3, 4) for p in range(2)]
+    for v, p in plans:
+        w = core.World(s)
+        w.set_launch_plan(v, p)
+        for _ in range(12):
+            w.step()
+        x = w.states().view(np.uint8).copy()
+        if ref is None:
+            ref = x
+        assert np.array_equal(x, ref), (v, p)
+        w.close()
     w = core.World(s)
     for _ in range(5):
         w.step()
     before = w.states().view(np.uint8).copy()
     v, p, report = w.autotune(ticks=2)
-    assert report.count("ms/tick") == 12
+    assert report.count("ms/tick") == len(plans)
     assert np.array_equal(w.states().view(np.uint8), before)
 
 
@@ -275,7 +275,7 @@ def test_launch_plans_are_bit_identical_on_the_settled_pile(gpu_available):
     z = np.load(os.path.join(os.path.dirname(__file__), "golden", "settled_pile_64x32x32.npz"))
     s.states = z["states"].astype(np.float32).view(scenes.STATE_DTYPE).reshape(-1).copy()
     ref = None
-    for v, p in ((1, 0), (0, 1), (0, 2), (1, 2), (2, 2), (1, 3), (0, 3)):
+    for v, p in ((1, 0), (0, 1), (0, 2), (1, 2), (2, 2), (1, 3), (0, 3), (3, 0), (4, 0), (4, 1)):
         w = core.World(s)
         w.set_launch_plan(v, p)
         for _ in range(4):
