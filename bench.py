@@ -8,11 +8,16 @@ ground and four walls -- starting from the settled state in
 tests/golden/settled_pile_64x32x32.npz (300 ticks of plain AVBD from the spawn
 grid). A step is one rigid AVBD tick (legacy profile: predict, broadphase,
 narrowphase, contact cache, prepare, colouring, solve, impact phase, commit)
-run with the residual-driven schedule: sweep until the residual -- the largest
-violation over the active contact normal rows and hard joint rows, in metres
-(--residual-norm max; `rms` tests the RMS instead) -- is at or below
---tolerance, at most --max-iterations sweeps. Inputs are synthetic (seeded);
-no dataset is involved.
+run with the residual-driven schedule: sweep until the position violation of
+the active contact normal rows and hard joint rows is within --tolerance (1e-4
+m), at most --max-iterations sweeps. --residual-norm picks how the rows are
+judged: `p999` (default) stops once at most one row in a thousand violates by
+more than the tolerance; `max` once every row is within it (on this pile the
+largest row violation levels off at 2-5e-4 m and no sweep count reaches 1e-4
+m, so both arms would run to the cap); `rms` once the RMS is within it (met
+after about 4 sweeps while single rows still violate by millimetres). Each
+arm's largest row violation, RMS and violating fraction are reported. Inputs
+are synthetic (seeded); no dataset is involved.
 
 GPU arm (default): the warm-start MLP is first trained online on
 --train-frames plain ticks (untimed); then, from the same settled snapshot,
@@ -47,7 +52,7 @@ GRID = (64, 32, 32)
 SEED = 4
 SETTLED = os.path.join(ROOT, "tests", "golden", "settled_pile_64x32x32.npz")
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "k_solve_pile65k.md")
-NORMS = {"max": 0, "rms": 1}
+NORMS = {"max": 0, "rms": 1, "p999": 2}
 LANE_POLICIES = ["8/16/32 by colour size", "8", "8/16/32 by body rows, heaviest first",
                  "8/16/32 by colour size, bodies claimed dynamically"]
 
@@ -60,8 +65,9 @@ def parse():
     ap.add_argument("--impl", default="pmb", choices=["pmb", "reference"])
     ap.add_argument("--tolerance", type=float, default=1e-4)
     ap.add_argument("--max-iterations", type=int, default=64)
-    ap.add_argument("--residual-norm", default="max", choices=["max", "rms"],
-                    help="residual the schedule tests: largest row violation (default) or RMS over the rows")
+    ap.add_argument("--residual-norm", default="p999", choices=["p999", "max", "rms"],
+                    help="residual the schedule tests: 99.9th percentile of the row violations (default), "
+                         "largest row violation, or RMS over the rows")
     ap.add_argument("--cpu-ticks", type=int, default=1, help="ticks timed by the CPU baseline leg")
     ap.add_argument("--contact-capacity", type=int, default=0,
                     help="contact-point capacity of the world (0: the library default, 64 per body)")
@@ -347,6 +353,10 @@ def gpu_arm(args):
                        "residual_row_max_plain": max(float(st["residual_max"]) for st in plain_stats),
                        "residual_rms_max_over_ticks_learned": max(float(st["residual"]) for st in learned_stats),
                        "residual_rms_max_over_ticks_plain": max(float(st["residual"]) for st in plain_stats),
+                       "rows_over_tolerance_max_fraction_learned": max(float(st["residual_over"])
+                                                                       for st in learned_stats),
+                       "rows_over_tolerance_max_fraction_plain": max(float(st["residual_over"])
+                                                                     for st in plain_stats),
                        "ticks_at_sweep_cap_learned": sum(int(st["iterations"]) >= args.max_iterations
                                                          for st in learned_stats),
                        "ticks_at_sweep_cap_plain": sum(int(st["iterations"]) >= args.max_iterations

@@ -136,7 +136,9 @@ typedef struct pmb_world_capacity {
  * residual-driven schedule: sweep until the residual is at or below the
  * tolerance, at most max_iterations sweeps; residual_norm picks the residual
  * the schedule tests: 0 the largest row violation of the sweep (every
- * constraint within the tolerance, in metres), 1 the RMS over the rows. warm_start selects where each
+ * constraint within the tolerance, in metres), 1 the RMS over the rows, 2 the
+ * 99.9th percentile (at most one active row in a thousand above the
+ * tolerance). warm_start selects where each
  * contact's normal row (lambda, penalty) starts: 0 plain (the reference's
  * cached-and-decayed warm start), 1 learned (the world's MLP predictor, when
  * one is attached; plain otherwise), 2 the table set by
@@ -148,16 +150,18 @@ typedef struct pmb_step_desc {
     uint32_t max_iterations;
     uint32_t warm_start;
     uint32_t collect_events; /* nonzero: record this tick's contact events */
-    uint32_t residual_norm;  /* 0: largest row violation, 1: RMS (residual-driven schedule) */
+    uint32_t residual_norm;  /* 0: largest row violation, 1: RMS, 2: 99.9th percentile (residual-driven schedule) */
 } pmb_step_desc;
 
 /* residual: RMS, over contact normal rows that carry force or penetrate and
  * hard joint rows, of the constraint violation after the last sweep (|C| for
  * rows with force, C for rows active by penetration only), in metres;
- * residual_max: the largest single row violation in the tick. */
+ * residual_max: the largest single row violation after the last sweep;
+ * residual_over: the fraction of those rows whose violation exceeds the
+ * step's residual_tolerance. */
 typedef struct pmb_step_stats {
     uint32_t candidate_pairs, active_pairs, contacts, colors, islands, iterations, impact, status;
-    float residual, residual_max;
+    float residual, residual_max, residual_over;
 } pmb_step_stats;
 
 typedef struct pmb_world pmb_world;

@@ -59,21 +59,23 @@ template <class R> inline std::vector<uint32_t> fixed_groups(const World<R>& w) 
     return root;
 }
 
-// Sorted candidate pairs (a dynamic query body, b any other leaf whose swept
-// proxy overlaps a's). A uniform grid keyed on AABB centre lists candidates;
-// the predicate and the (a, b) order are the reference's.
-template <class R> inline std::vector<uint64_t> broadphase(const World<R>& w) {
-    const uint32_t n = w.n;
+// Sorted candidate pairs over plain boxes: a a dynamic query box, b any
+// other box whose bounds overlap a's (inclusive), b dynamic only when a < b
+// (identity order == index order), a and b not in one fixed collision group
+// (group[i]: the group's root, empty when there are no groups), and no
+// collision-disabling joint between them (`disabled`: sorted (min, max) keys).
+// A uniform grid keyed on box centre lists the candidates; boxes larger than
+// 4x the median extent are tested against every query. Codes a*n+b, in
+// (query, identity) order: spatial_build.slang:889-1011 with the filter of
+// geometry.slang:829-947.
+template <class R>
+inline std::vector<uint64_t> broadphase_boxes(uint32_t n, const V3<R>* lo, const V3<R>* hi, const uint8_t* dyn,
+                                              const std::vector<uint32_t>& group,
+                                              const std::vector<uint64_t>& disabled) {
     std::vector<uint64_t> out;
-    R cell = 0;
-    for (uint32_t i = 0; i < n; ++i) {
-        V3<R> e = sub(w.aabb_hi[i], w.aabb_lo[i]);
-        cell = std::max(cell, std::max(e.x, std::max(e.y, e.z)));
-    }
-    // Bodies larger than 4x the median extent are tested against every query.
     std::vector<R> ext(n);
     for (uint32_t i = 0; i < n; ++i) {
-        V3<R> e = sub(w.aabb_hi[i], w.aabb_lo[i]);
+        V3<R> e = sub(hi[i], lo[i]);
         ext[i] = std::max(e.x, std::max(e.y, e.z));
     }
     std::vector<R> sorted = ext;
@@ -85,23 +87,21 @@ template <class R> inline std::vector<uint64_t> broadphase(const World<R>& w) {
     for (uint32_t i : small) hs = std::max(hs, ext[i]);
     if (!(hs > R(0))) hs = R(1);
     auto key = [&](uint32_t i, int dx, int dy, int dz) {
-        V3<R> c = mul(add(w.aabb_lo[i], w.aabb_hi[i]), R(0.5));
+        V3<R> c = mul(add(lo[i], hi[i]), R(0.5));
         int64_t x = int64_t(std::floor(double(c.x / hs))) + dx, y = int64_t(std::floor(double(c.y / hs))) + dy,
                 z = int64_t(std::floor(double(c.z / hs))) + dz;
         return std::array<int64_t, 3>{x, y, z};
     };
     std::map<std::array<int64_t, 3>, std::vector<uint32_t>> grid;
     for (uint32_t i : small) grid[key(i, 0, 0, 0)].push_back(i);
-    const std::vector<uint32_t> group = fixed_groups(w);
-    const std::vector<uint64_t> disabled = collision_disabled_keys(w);
     std::vector<uint32_t> cand;
     for (uint32_t a = 0; a < n; ++a) {
-        if (!dynamic(w, a)) continue;
+        if (!dyn[a]) continue;
         cand.clear();
         auto test = [&](uint32_t b) {
             if (b == a) return;
-            if (!overlaps(w.aabb_lo[b], w.aabb_hi[b], w.aabb_lo[a], w.aabb_hi[a])) return;
-            if (dynamic(w, b) && !(a < b)) return;
+            if (!overlaps(lo[b], hi[b], lo[a], hi[a])) return;
+            if (dyn[b] && !(a < b)) return;
             if (!group.empty() && group[a] == group[b]) return;
             if (collision_disabled(disabled, a, b)) return;
             cand.push_back(b);
@@ -122,6 +122,14 @@ template <class R> inline std::vector<uint64_t> broadphase(const World<R>& w) {
         for (uint32_t b : cand) out.push_back(uint64_t(a) * n + b);
     }
     return out;
+}
+
+// The world's candidate pairs: its swept proxies through broadphase_boxes.
+template <class R> inline std::vector<uint64_t> broadphase(const World<R>& w) {
+    std::vector<uint8_t> dyn(w.n);
+    for (uint32_t i = 0; i < w.n; ++i) dyn[i] = dynamic(w, i) ? 1 : 0;
+    return broadphase_boxes<R>(w.n, w.aabb_lo.data(), w.aabb_hi.data(), dyn.data(), fixed_groups(w),
+                               collision_disabled_keys(w));
 }
 
 template <class R> inline void step(World<R>& w, const StepDesc& o) {
@@ -539,6 +547,8 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
             w.res_sq = 0;
             w.res_n = 0;
             w.res_max = 0;
+            w.res_over = 0;
+            w.res_tol = R(o.residual_tolerance);
             for (uint32_t k = 0; k < P; ++k) {
                 uint32_t a = uint32_t(w.active_pairs[k] / n), b = uint32_t(w.active_pairs[k] % n);
                 if (phase != 0 && bodies[a].impact == 0 && bodies[b].impact == 0) continue;
@@ -601,11 +611,24 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
                 const R rms = w.res_n ? R(std::sqrt(w.res_sq / double(w.res_n))) : R(0);
                 w.residual_rms_last = rms;
                 w.residual_max_last = w.res_max;
+                w.residual_over_last = w.res_n ? float(w.res_over) / float(w.res_n) : 0.0f;
                 // The schedule's measure: the largest row violation (every
-                // constraint within the tolerance) or the RMS over the rows.
-                const R res = o.residual_norm == 1 ? rms : w.res_max;
+                // constraint within the tolerance), the RMS over the rows, or
+                // the 99.9th percentile (at most one row in a thousand above).
+                bool met;
+                R res;
+                if (o.residual_norm == 1) {
+                    res = rms;
+                    met = rms <= R(o.residual_tolerance);
+                } else if (o.residual_norm == 2) {
+                    res = R(w.residual_over_last);
+                    met = w.res_over * 1000u <= w.res_n;
+                } else {
+                    res = w.res_max;
+                    met = w.res_max <= R(o.residual_tolerance);
+                }
                 w.residual_trace.push_back(res);
-                if (adaptive && res <= R(o.residual_tolerance)) last = true;
+                if (adaptive && met) last = true;
                 used_iterations = it + 1;
             }
             if (last) break;
@@ -718,6 +741,7 @@ template <class R> inline void step(World<R>& w, const StepDesc& o) {
     st.iterations = used_iterations;
     st.residual = w.residual_trace.empty() ? 0.0f : float(w.residual_rms_last);
     st.residual_max = float(w.residual_max_last);
+    st.residual_over = w.residual_over_last;
 
     // ---- speed clamp (geometry.slang:3086-3100)
     for (uint32_t i = 0; i < n; ++i) {

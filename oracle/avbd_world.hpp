@@ -69,11 +69,11 @@ struct StepDesc {
     uint32_t max_iterations;        // cap for the residual-driven loop
     uint32_t warm_start;            // 0: plain (the only source the oracle models)
     uint32_t collect_events;        // not used by the oracle (it always keeps its events)
-    uint32_t residual_norm;         // stop rule: 0 largest row violation, 1 RMS
+    uint32_t residual_norm;         // stop rule: 0 largest row violation, 1 RMS, 2 99.9th percentile
 };
 struct StepStats {
     uint32_t candidate_pairs, active_pairs, contacts, colors, islands, iterations, impact, status;
-    float residual, residual_max;
+    float residual, residual_max, residual_over;
 };
 
 // ------------------------------------------------------------ world types
@@ -276,10 +276,14 @@ template <class R> struct World {
     double res_sq{};
     uint64_t res_n{};
     R res_max{}, residual_max_last{}, residual_rms_last{};
+    uint64_t res_over{};  // rows above res_tol in the current pass
+    R res_tol{};
+    float residual_over_last{};
     void residual_add(R v) {
         res_sq += double(v) * double(v);
         ++res_n;
         res_max = v > res_max ? v : res_max;
+        if (v > res_tol) ++res_over;
     }
 };
 

@@ -265,6 +265,7 @@ void fill_stats(const Counters& c, pmb_step_stats* s) {
     s->status = c.status;
     s->residual = c.residual;
     s->residual_max = c.residual_max;
+    s->residual_over = c.residual_over;
 }
 
 // The float whose bits are u (index fields packed into float4 records).

@@ -102,6 +102,8 @@ struct JointCtx {
     double res_sq;
     uint32_t res_n;
     float res_max;
+    uint32_t res_over;  // hard rows whose |C| exceeds res_tol
+    float res_tol;
 };
 
 // geometry_constraints.slang:626-713
@@ -147,6 +149,7 @@ static __device__ void joint_row(JointCtx& c, const V6& ja, const V6& jb, float 
             c.res_sq += double(v) * double(v);
             c.res_n += 1;
             c.res_max = fmx(c.res_max, v);
+            if (v > c.res_tol) c.res_over += 1;
         }
         store_row(c.rows[ri], row_advance(row, c.A->dx, c.B->dx));
     } else if (c.visit == kVisitImpact) {
@@ -169,8 +172,9 @@ static __device__ void joint_row(JointCtx& c, const V6& ja, const V6& jb, float 
 static __device__ float visit_joint(const Joint& o, JointRow* rows, const BodyView& A, const BodyView& B, V3 prev_xa,
                              Q4 prev_qa, V3 prev_xb, Q4 prev_qb, float4 pa0, float4 pb0, float dt, Blk* blk,
                              bool first, unsigned visit, uint32_t* count_out, double* res_sq = nullptr,
-                             uint32_t* res_n = nullptr, float* res_max = nullptr) {
-    JointCtx c{rows, &A, &B, blk, 0u, 0.0f, first, visit, dt, 0.0, 0u, 0.0f};
+                             uint32_t* res_n = nullptr, float* res_max = nullptr, uint32_t* res_over = nullptr,
+                             float res_tol = 0.0f) {
+    JointCtx c{rows, &A, &B, blk, 0u, 0.0f, first, visit, dt, 0.0, 0u, 0.0f, 0u, res_tol};
     V3 xa, xb;
     Q4 qa, qb;
     body_pose(A, xa, qa);
@@ -289,6 +293,7 @@ static __device__ float visit_joint(const Joint& o, JointRow* rows, const BodyVi
     if (res_sq) *res_sq += c.res_sq;
     if (res_n) *res_n += c.res_n;
     if (res_max) *res_max = fmx(*res_max, c.res_max);
+    if (res_over) *res_over += c.res_over;
     return c.impulse;
 }
 

@@ -426,12 +426,21 @@ __device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float
 
 // Residual accumulator of one dual pass (this build's addition): rows that
 // carry force or penetrate contribute |C_n| (force > 0) or C_n (penetration
-// only); hard joint rows contribute |C|. Reported as the RMS over those rows.
+// only); hard joint rows contribute |C|. Reported as the RMS, the largest
+// value, and the number of rows above the schedule's tolerance.
 struct Res {
     double sq;
     uint32_t n;
     float mx;
+    uint32_t over;
+    float tol;
 };
+__device__ __forceinline__ void res_add(Res& r, float v) {
+    r.sq += double(v) * double(v);
+    r.n += 1;
+    r.mx = fmx(r.mx, v);
+    if (v > r.tol) r.over += 1;
+}
 
 // advance_duals for one contact point (geometry_constraints_solve.slang:
 // 494-532; the last-iteration block runs in k_contact_finalize).
@@ -474,9 +483,7 @@ __device__ void dual_contact(const Dev& d, uint32_t c, float dt, uint32_t phase,
     d.c_pen[c] = pen;
     if (f.n > 0.0f || err[0] > 0.0f) {
         const float v = f.n > 0.0f ? fab(err[0]) : err[0];
-        res.sq += double(v) * double(v);
-        res.n += 1;
-        res.mx = fmx(res.mx, v);
+        res_add(res, v);
         if (scene_last) {
             atomicAdd(&d.scene_res_sq[scene], v * v);
             atomicAdd(&d.scene_res_n[scene], 1u);
@@ -503,15 +510,16 @@ __device__ void dual_joint(const Dev& d, uint32_t j, uint32_t phase, float dt, R
         BodyView A = load_body(d, a), B = load_body(d, b);
         Blk scratch;
         // A batched world also needs this joint's own residual for its scene.
-        Res jr{0.0, 0u, 0.0f};
+        Res jr{0.0, 0u, 0.0f, 0u, res.tol};
         Res& sink = batched(d) ? jr : res;
         impulse = visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]),
                               q4(d.q[b]), d.p0[a], d.p0[b], dt, &scratch, true, kVisitAdvance, nullptr, &sink.sq,
-                              &sink.n, &sink.mx);
+                              &sink.n, &sink.mx, &sink.over, sink.tol);
         if (batched(d)) {
             res.sq += jr.sq;
             res.n += jr.n;
             res.mx = fmx(res.mx, jr.mx);
+            res.over += jr.over;
         }
         if (scene_last && jr.n) {
             atomicAdd(&d.scene_res_sq[scene], float(jr.sq));
@@ -534,6 +542,77 @@ __device__ void dual_joint(const Dev& d, uint32_t j, uint32_t phase, float dt, R
         js.enabled = 0;
     }
     d.jstate[j] = js;
+}
+
+// One block's residual partials into slot `slot` of the counters: warp
+// trees, then warps in order (deterministic).
+template <int T>
+__device__ __forceinline__ void block_residual(Res res, double* wsq, uint32_t* wn, float* wmx, uint32_t* wov,
+                                               Counters* c, uint32_t slot) {
+    for (int o = 16; o > 0; o >>= 1) {
+        res.sq += __shfl_xor_sync(0xffffffffu, res.sq, o);
+        res.n += __shfl_xor_sync(0xffffffffu, res.n, o);
+        res.mx = fmx(res.mx, __shfl_xor_sync(0xffffffffu, res.mx, o));
+        res.over += __shfl_xor_sync(0xffffffffu, res.over, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        wsq[threadIdx.x >> 5] = res.sq;
+        wn[threadIdx.x >> 5] = res.n;
+        wmx[threadIdx.x >> 5] = res.mx;
+        wov[threadIdx.x >> 5] = res.over;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double bs = 0.0;
+        uint32_t bn = 0, bo = 0;
+        float bm = 0.0f;
+        for (int k = 0; k < T / 32; ++k) {
+            bs += wsq[k];
+            bn += wn[k];
+            bm = fmx(bm, wmx[k]);
+            bo += wov[k];
+        }
+        c->res_sum[slot] = bs;
+        c->res_cnt[slot] = bn;
+        c->res_mx[slot] = bm;
+        c->res_over[slot] = bo;
+    }
+}
+
+// The sweep's residual from every block's partials (slots base .. base +
+// gridDim.x): RMS, largest row violation, fraction of rows above the
+// tolerance, and whether the schedule's measure meets the tolerance
+// (residual_norm 0: every row within it; 1: the RMS; 2: at most one row in a
+// thousand above it).
+struct SweepResidual {
+    float rms, mx, over, measure;
+    bool met;
+};
+__device__ __forceinline__ SweepResidual sweep_residual(Counters* c, uint32_t base, const StepParams& sp) {
+    double tsq = 0.0;
+    uint32_t tn = 0, to = 0;
+    float tmx = 0.0f;
+    for (uint32_t k = 0; k < gridDim.x; ++k) {
+        tsq += ((volatile double*)c->res_sum)[base + k];
+        tn += ((volatile uint32_t*)c->res_cnt)[base + k];
+        tmx = fmx(tmx, ((volatile float*)c->res_mx)[base + k]);
+        to += ((volatile uint32_t*)c->res_over)[base + k];
+    }
+    SweepResidual r;
+    r.rms = tn ? float(sqrt(tsq / double(tn))) : 0.0f;
+    r.mx = tmx;
+    r.over = tn ? float(to) / float(tn) : 0.0f;
+    if (sp.residual_norm == 1) {
+        r.measure = r.rms;
+        r.met = r.rms <= sp.tolerance;
+    } else if (sp.residual_norm == 2) {
+        r.measure = r.over;
+        r.met = uint64_t(to) * 1000u <= uint64_t(tn);
+    } else {
+        r.measure = tmx;
+        r.met = tmx <= sp.tolerance;
+    }
+    return r;
 }
 
 __device__ __forceinline__ void atomic_max_pos(float* addr, float v) {
@@ -565,7 +644,7 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
                                                  : min(budget, kMaxIterations);
     const uint32_t n_con = c->n_contacts;
     __shared__ double wsq[kSolveThreads / 32];
-    __shared__ uint32_t wn[kSolveThreads / 32];
+    __shared__ uint32_t wn[kSolveThreads / 32], wov[kSolveThreads / 32];
     __shared__ float wmx[kSolveThreads / 32];
     const bool timing = sp.debug_timing && phase == 0;
     auto now = [] {
@@ -649,52 +728,18 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
             if (!grid_sync(c, d.barrier_spins)) return;
             if (timing && it == 0 && col < 18 && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_release[col] = now();
         }
-        Res res{0.0, 0u, 0.0f};
+        Res res{0.0, 0u, 0.0f, 0u, sp.tolerance};
         for (uint32_t k = grid_stride_begin(); k < n_con; k += grid_stride()) dual_contact(d, k, dt, phase, res, it);
         for (uint32_t j = grid_stride_begin(); j < d.nj; j += grid_stride()) dual_joint(d, j, phase, dt, res, it);
         // Deterministic reduction: warp tree, warps in order, blocks in order.
-        for (int o = 16; o > 0; o >>= 1) {
-            res.sq += __shfl_xor_sync(0xffffffffu, res.sq, o);
-            res.n += __shfl_xor_sync(0xffffffffu, res.n, o);
-            res.mx = fmx(res.mx, __shfl_xor_sync(0xffffffffu, res.mx, o));
-        }
-        if ((threadIdx.x & 31) == 0) {
-            wsq[threadIdx.x >> 5] = res.sq;
-            wn[threadIdx.x >> 5] = res.n;
-            wmx[threadIdx.x >> 5] = res.mx;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double bs = 0.0;
-            uint32_t bn = 0;
-            float bm = 0.0f;
-            for (int k = 0; k < kSolveThreads / 32; ++k) {
-                bs += wsq[k];
-                bn += wn[k];
-                bm = fmx(bm, wmx[k]);
-            }
-            c->res_sum[blockIdx.x] = bs;
-            c->res_cnt[blockIdx.x] = bn;
-            c->res_mx[blockIdx.x] = bm;
-        }
+        block_residual<kSolveThreads>(res, wsq, wn, wmx, wov, c, blockIdx.x);
         if (timing && it == 0 && threadIdx.x == 0) atomicMax(&c->dbg_work[19], now());
         if (!grid_sync(c, d.barrier_spins)) return;
         if (timing && it == 0 && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_release[19] = now();
-        double tsq = 0.0;
-        uint32_t tn = 0;
-        float tmx = 0.0f;
-        for (uint32_t k = 0; k < gridDim.x; ++k) {
-            tsq += ((volatile double*)c->res_sum)[k];
-            tn += ((volatile uint32_t*)c->res_cnt)[k];
-            tmx = fmx(tmx, ((volatile float*)c->res_mx)[k]);
-        }
-        const float rms = tn ? float(sqrt(tsq / double(tn))) : 0.0f;
-        // The schedule's measure: the largest row violation of the sweep
-        // (every constraint within the tolerance), or the RMS over the rows.
-        const float measure = sp.residual_norm == 1 ? rms : tmx;
-        if (phase == 0 && grid_stride_begin() == 0) c->residual_trace[it] = measure;
+        const SweepResidual sw = sweep_residual(c, 0u, sp);
+        if (phase == 0 && grid_stride_begin() == 0) c->residual_trace[it] = sw.measure;
         bool last = it + 1 == iters;
-        if (adaptive && measure <= sp.tolerance) last = true;
+        if (adaptive && sw.met) last = true;
         // Every block has read the partials before the next pass rewrites them.
         if (!last && colors == 0 && !grid_sync(c, d.barrier_spins)) return;
         if (last) {
@@ -702,8 +747,9 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
                 c->claim[0] = c->claim[1] = 0u;  // every block is past its last claim
                 if (phase == 0) {
                     c->iterations = it + 1;
-                    c->residual = rms;
-                    c->residual_max = tmx;
+                    c->residual = sw.rms;
+                    c->residual_max = sw.mx;
+                    c->residual_over = sw.over;
                 }
                 c->budget = it + 1;
             }
@@ -895,9 +941,7 @@ __device__ __forceinline__ void staged_dual(const Dev& d, const float* row, cons
     d.c_pen[c] = pen;
     if (f.n > 0.0f || err[0] > 0.0f) {
         const float v = f.n > 0.0f ? fab(err[0]) : err[0];
-        res.sq += double(v) * double(v);
-        res.n += 1;
-        res.mx = fmx(res.mx, v);
+        res_add(res, v);
         if (scene_last) {
             atomicAdd(&d.scene_res_sq[scene], v * v);
             atomicAdd(&d.scene_res_n[scene], 1u);
@@ -1057,14 +1101,15 @@ __device__ void staged_body(const Dev& d, const StageTables& tb, uint32_t sl, ui
             if (block_solve(blk, safe)) upd = safe;
         }
         // The update (apply_pose_update / the impact phase's linear update),
-        // computed by every lane so each holds the new displacement.
+        // computed by every lane so each holds the new displacement. Every
+        // lane reads the body's state before lane 0 stores the update.
+        float4 l = d.dxl[i], a = d.dxa[i];
+        Q4 rel = q4(d.dq[i]);
+        __syncwarp(gmask);
         if (phase == 0) {
-            float4 l = d.dxl[i];
             l.x += upd.v[0];
             l.y += upd.v[1];
             l.z += upd.v[2];
-            float4 a = d.dxa[i];
-            Q4 rel = q4(d.dq[i]);
             const V3 r{upd.v[3], upd.v[4], upd.v[5]};
             const bool rotates = !(r.x == 0.0f && r.y == 0.0f && r.z == 0.0f);
             if (rotates) {
@@ -1080,9 +1125,7 @@ __device__ void staged_body(const Dev& d, const StageTables& tb, uint32_t sl, ui
                     d.dxa[i] = a;
                 }
             }
-            dxn = {{l.x, l.y, l.z, a.x, a.y, a.z}};
         } else {
-            float4 l = d.dxl[i], a = d.dxa[i];
             l.x += upd.v[0];
             l.y += upd.v[1];
             l.z += upd.v[2];
@@ -1093,8 +1136,8 @@ __device__ void staged_body(const Dev& d, const StageTables& tb, uint32_t sl, ui
                 d.dxl[i] = l;
                 d.dxa[i] = a;
             }
-            dxn = {{l.x, l.y, l.z, a.x, a.y, a.z}};
         }
+        dxn = {{l.x, l.y, l.z, a.x, a.y, a.z}};
     }
     __syncwarp(gmask);
     // Owned contact duals, one row per lane.
@@ -1131,10 +1174,10 @@ __global__ void __launch_bounds__(T, 1) k_solve_staged(Dev d, StepParams sp, uin
                                       : adaptive ? min(max(sp.max_iterations, 1u), kMaxIterations)
                                                  : min(budget, kMaxIterations);
     __shared__ double wsq[T / 32];
-    __shared__ uint32_t wn[T / 32];
+    __shared__ uint32_t wn[T / 32], wov[T / 32];
     __shared__ float wmx[T / 32];
     for (uint32_t it = 0; it < iters; ++it) {
-        Res res{0.0, 0u, 0.0f};
+        Res res{0.0, 0u, 0.0f, 0u, sp.tolerance};
         const uint32_t parity = (it & 1u) * 512u;
         for (uint32_t col = 0; col <= colors; ++col) {
             if (col < colors) {
@@ -1242,55 +1285,23 @@ __global__ void __launch_bounds__(T, 1) k_solve_staged(Dev d, StepParams sp, uin
                 }
                 // The sweep's residual partials (after the last colour's
                 // duals), published by the barrier below.
-                Res r = res;
-                for (int o = 16; o > 0; o >>= 1) {
-                    r.sq += __shfl_xor_sync(0xffffffffu, r.sq, o);
-                    r.n += __shfl_xor_sync(0xffffffffu, r.n, o);
-                    r.mx = fmx(r.mx, __shfl_xor_sync(0xffffffffu, r.mx, o));
-                }
-                if (lane == 0) {
-                    wsq[threadIdx.x >> 5] = r.sq;
-                    wn[threadIdx.x >> 5] = r.n;
-                    wmx[threadIdx.x >> 5] = r.mx;
-                }
-                __syncthreads();
-                if (threadIdx.x == 0) {
-                    double bs = 0.0;
-                    uint32_t bn = 0;
-                    float bm = 0.0f;
-                    for (int k = 0; k < T / 32; ++k) {
-                        bs += wsq[k];
-                        bn += wn[k];
-                        bm = fmx(bm, wmx[k]);
-                    }
-                    c->res_sum[parity + blockIdx.x] = bs;
-                    c->res_cnt[parity + blockIdx.x] = bn;
-                    c->res_mx[parity + blockIdx.x] = bm;
-                }
+                block_residual<T>(res, wsq, wn, wmx, wov, c, parity + blockIdx.x);
                 if (!grid_sync(c, d.barrier_spins)) return;
                 break;
             }
             if (!grid_sync(c, d.barrier_spins)) return;
         }
-        double tsq = 0.0;
-        uint32_t tn = 0;
-        float tmx = 0.0f;
-        for (uint32_t k = 0; k < gridDim.x; ++k) {
-            tsq += ((volatile double*)c->res_sum)[parity + k];
-            tn += ((volatile uint32_t*)c->res_cnt)[parity + k];
-            tmx = fmx(tmx, ((volatile float*)c->res_mx)[parity + k]);
-        }
-        const float rms = tn ? float(sqrt(tsq / double(tn))) : 0.0f;
-        const float measure = sp.residual_norm == 1 ? rms : tmx;
-        if (phase == 0 && grid_stride_begin() == 0) c->residual_trace[it] = measure;
+        const SweepResidual sw = sweep_residual(c, parity, sp);
+        if (phase == 0 && grid_stride_begin() == 0) c->residual_trace[it] = sw.measure;
         bool last = it + 1 == iters;
-        if (adaptive && measure <= sp.tolerance) last = true;
+        if (adaptive && sw.met) last = true;
         if (last) {
             if (grid_stride_begin() == 0) {
                 if (phase == 0) {
                     c->iterations = it + 1;
-                    c->residual = rms;
-                    c->residual_max = tmx;
+                    c->residual = sw.rms;
+                    c->residual_max = sw.mx;
+                    c->residual_over = sw.over;
                 }
                 c->budget = it + 1;
             }

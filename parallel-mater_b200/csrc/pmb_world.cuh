@@ -62,7 +62,9 @@ struct Counters {
     double res_sum[1024];  // per-block partial residual sums of the latest dual pass
     uint32_t res_cnt[1024];
     float res_mx[1024];
+    uint32_t res_over[1024];  // per-block rows above the tolerance
     float residual_max;
+    float residual_over;  // fraction of active rows above the tolerance after the last sweep
     unsigned long long dbg_work[20], dbg_release[20], dbg_start;
     unsigned long long dbg_body[8];
     unsigned long long dbg_sum[8];  // colour 0 of the first sweep: stage sums, bodies, rows
@@ -80,7 +82,7 @@ struct StepParams {
     uint32_t debug_timing;  // record solve-kernel timestamps for iteration 0
     uint32_t warm_start;    // 0 plain, 1 learned, 2 table
     uint32_t collect_events;
-    uint32_t residual_norm;  // residual-driven schedule: 0 largest row violation, 1 RMS
+    uint32_t residual_norm;  // residual-driven schedule: 0 largest row violation, 1 RMS, 2 99.9th percentile
 };
 
 struct ContactEvent {  // pmb_contact_event

@@ -55,7 +55,7 @@ STEP_DTYPE = np.dtype([
 STATS_DTYPE = np.dtype([
     ("candidate_pairs", "<u4"), ("active_pairs", "<u4"), ("contacts", "<u4"), ("colors", "<u4"),
     ("islands", "<u4"), ("iterations", "<u4"), ("impact", "<u4"), ("status", "<u4"),
-    ("residual", "<f4"), ("residual_max", "<f4")])
+    ("residual", "<f4"), ("residual_max", "<f4"), ("residual_over", "<f4")])
 
 LEGACY, REALTIME = 0, 1
 DT = np.float32(1.0 / 60.0)

@@ -51,6 +51,19 @@ def test_reference_fixture_suite_passes_on_oracle():
     assert "oracle fixtures: 85/85 passed" in out.stdout
 
 
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "tests", "solver")), reason="reference checkout absent")
+def test_reference_spatial_fixtures_pass_on_oracle():
+    """The oracle's broadphase pair predicate on the reference's spatial
+    fixtures (rigid_spatial_tests.cpp's shared-query scenario, the leaves and
+    queries of spatial_build_primitives_tests.cpp), compiled against the
+    reference's spatial headers."""
+    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "pin", f"REF={REF}"], check=True)
+    out = subprocess.run([os.path.join(REPO, "oracle", "_ref", "pin_spatial_fixtures")], capture_output=True,
+                         text=True)
+    assert out.returncode == 0, out.stdout[-2000:]
+    assert "spatial pins: passed" in out.stdout
+
+
 def test_block_solve_golden(golden):
     n_ok = 0
     for b in golden["blocks"]:

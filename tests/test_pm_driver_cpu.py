@@ -162,3 +162,26 @@ def test_abi_layout_matches_reference_header(tmp_path):
         outputs.append(subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout)
     ours, ref = outputs
     assert ours == ref
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_INCLUDE, os.pardir, "tests", "api", "driver_abi_tests.cpp")),
+                    reason="reference checkout absent")
+@pytest.mark.skipif(shutil.which("g++") is None, reason="no C++ compiler")
+def test_reference_driver_abi_test_passes_its_driver_checks(tmp_path):
+    """The reference's own tests/api/driver_abi_tests.cpp, compiled unmodified
+    against the reference headers and run on libpm_b200_driver.so: the four
+    loader entry points resolve, no pm* command is exported, the interface
+    version negotiates, instance-level lookups with a null instance answer
+    pmCreateInstance but not device commands, and a newer API version is
+    refused without creating an instance. Its second half opens the
+    reference loader library, which needs the reference's generated
+    registry sources to build; it is pointed at a path that does not exist,
+    so the run must stop exactly at that check, after every driver check
+    passed."""
+    src = os.path.normpath(os.path.join(REF_INCLUDE, os.pardir, "tests", "api", "driver_abi_tests.cpp"))
+    exe = tmp_path / "driver_abi_tests"
+    subprocess.run(["g++", "-std=c++20", "-I", REF_INCLUDE, src, "-o", str(exe), "-ldl"], check=True)
+    out = subprocess.run([str(exe), pm.DRIVER_PATH, str(tmp_path / "no_loader.so")], capture_output=True, text=True)
+    assert out.returncode == 1
+    failed = [line for line in out.stderr.splitlines() if line.startswith("line ")]
+    assert len(failed) == 1 and failed[0].endswith("loader != nullptr"), out.stderr
