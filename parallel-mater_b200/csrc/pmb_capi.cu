@@ -697,7 +697,10 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     for (uint32_t v = 0; v < kSolveVariants; ++v) {
         const SolveVariant& sv = solve_variants[v];
         cudaFuncSetAttribute(sv.ptr, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sv.smem));
-        w->coop_solve[v] = coop_blocks_for(sv.ptr, sv.threads, sv.smem);
+        cudaFuncSetAttribute(sv.timed, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sv.smem));
+        // One grid for both builds: the smaller of their co-resident counts.
+        w->coop_solve[v] = std::min(coop_blocks_for(sv.ptr, sv.threads, sv.smem),
+                                    coop_blocks_for(sv.timed, sv.threads, sv.smem));
     }
     {
         int dev = 0, sms = 0;

@@ -136,6 +136,7 @@ template <int G> struct GroupRows {
     float r[G][3][14];
     float nrow[kNormSlots][8];  // normal row: jacobian[6], raw penalty, trial force
     uint32_t flag[G];
+    Blk jblk;  // the block while joint rows are added (joint_rows_shared)
 };
 // Per-warp staging area: four 8-lane groups, two 16-lane groups or one
 // 32-lane group.
@@ -234,8 +235,8 @@ __device__ __forceinline__ void stage_contact(const Dev& d, const Lite& me, floa
     const uint32_t c = code & 0x7fffffffu;
     const bool first = (code >> 31) == 0;
     const Lite other = load_lite(d, other_body);
-    const Lite& A = first ? me : other;
-    const Lite& B = first ? other : me;
+    const Lite A = first ? me : other;  // values, not run-time references (no local copies)
+    const Lite B = first ? other : me;
     const float of = d.p1[other_body].x;
     const float friction = sqrtf(first ? my_friction * of : of * my_friction);
     const float4 lam = d.c_lam[c], pen = d.c_pen[c];
@@ -244,9 +245,8 @@ __device__ __forceinline__ void stage_contact(const Dev& d, const Lite& me, floa
     contact_rows(d, c, d.c_e[c], A, B, ja, jb, err);
     F3 trial{lam.x + pen.x * err[0], lam.y + pen.y * err[1], lam.z + pen.z * err[2]};
     if (nslot >= 0) {
-        const V6& nr = first ? ja[0] : jb[0];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) sm.nrow[nslot][k] = nr.v[k];
+        for (int k = 0; k < 6; ++k) sm.nrow[nslot][k] = first ? ja[0].v[k] : jb[0].v[k];
         sm.nrow[nslot][6] = pen.x;
         sm.nrow[nslot][7] = trial.n;
     }
@@ -265,7 +265,11 @@ __device__ __forceinline__ void stage_contact(const Dev& d, const Lite& me, floa
     const float st[3] = {pen.x * sc.n, pen.y * sc.t0, pen.z * sc.t1};
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
-        const V6& row = first ? ja[x] : jb[x];
+        // Values selected element by element: a reference chosen at run time
+        // between the two arrays would give them addresses (local memory).
+        V6 row;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) row.v[k] = first ? ja[x].v[k] : jb[x].v[k];
 #pragma unroll
         for (int k = 0; k < 6; ++k) sm.r[slot][x][k] = row.v[k];
         sm.r[slot][x][6] = st[x];
@@ -273,6 +277,41 @@ __device__ __forceinline__ void stage_contact(const Dev& d, const Lite& me, floa
 #pragma unroll
         for (int k = 0; k < 6; ++k) sm.r[slot][x][8 + k] = st[x] * row.v[k];  // = (stiffness x J_i), as before
     }
+}
+
+// Joint rows of body i added to its block (geometry_constraints_solve.slang:
+// 381-400, the serial loop's order). The joint visit takes the block's
+// address, so lane 0 works on a copy in the group's shared-memory slot `sb`
+// and the group reads the result back: the register block never needs an
+// address (which would put it in local memory for every body).
+template <int G>
+__device__ __forceinline__ void joint_rows_shared(const Dev& d, uint32_t i, uint32_t phase, float dt, Blk& blk,
+                                                  Blk* sb, uint32_t gmask, int gl) {
+    if (gl == 0) {
+        *sb = blk;
+        const uint32_t jcnt = d.jdeg[i], jlo = d.jinc_off[i];
+        for (uint32_t k = 0; k < jcnt; ++k) {
+            const uint32_t j = d.jinc_list[jlo + k];
+            const JointState js = d.jstate[j];
+            if (!js.enabled) continue;
+            const uint32_t a = js.dense_a, b = js.dense_b;
+            const bool first = i == a;
+            if (phase == 0) {
+                BodyView A = load_body(d, a), B = load_body(d, b);
+                visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]),
+                            q4(d.q[b]), d.p0[a], d.p0[b], dt, sb, first, kVisitAccumulate, nullptr);
+            } else {
+                const Lite A = load_lite(d, a), B = load_lite(d, b);
+                for (uint32_t r = 0; r < js.count; ++r) {
+                    Row row = load_row(d.jrows[size_t(j) * 18 + r]);
+                    if (row.stiffness >= kMaxPenalty) row_accumulate(*sb, row, first, A.dx, B.dx, dt);
+                }
+            }
+        }
+    }
+    __syncwarp(gmask);
+    blk = *sb;
+    __syncwarp(gmask);
 }
 
 __device__ __forceinline__ unsigned long long gtimer() {
@@ -338,34 +377,7 @@ __device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float
     gather_block<G>(ent, blk, gmask, gbase);
     mark(1);
     const uint32_t jcnt = d.jdeg[i];
-    if (jcnt) {
-        if (gl == 0) {
-            const uint32_t jlo = d.jinc_off[i];
-            for (uint32_t k = 0; k < jcnt; ++k) {
-                const uint32_t j = d.jinc_list[jlo + k];
-                const JointState js = d.jstate[j];
-                if (!js.enabled) continue;
-                const uint32_t a = js.dense_a, b = js.dense_b;
-                const bool first = i == a;
-                if (phase == 0) {
-                    BodyView A = load_body(d, a), B = load_body(d, b);
-                    visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]),
-                                q4(d.q[b]), d.p0[a], d.p0[b], dt, &blk, first, kVisitAccumulate, nullptr);
-                } else {
-                    const Lite A = load_lite(d, a), B = load_lite(d, b);
-                    for (uint32_t r = 0; r < js.count; ++r) {
-                        Row row = load_row(d.jrows[size_t(j) * 18 + r]);
-                        if (row.stiffness >= kMaxPenalty) row_accumulate(blk, row, first, A.dx, B.dx, dt);
-                    }
-                }
-            }
-        }
-        __syncwarp(gmask);
-#pragma unroll
-        for (int e = 0; e < 21; ++e) blk.h[e] = __shfl_sync(gmask, blk.h[e], gbase);
-#pragma unroll
-        for (int r = 0; r < 6; ++r) blk.g[r] = __shfl_sync(gmask, blk.g[r], gbase);
-    }
+    if (jcnt) joint_rows_shared<G>(d, i, phase, dt, blk, &sm.jblk, gmask, gl);
     V6 upd;
     if (!block_solve(blk, upd)) return;
     mark(2);
@@ -621,8 +633,10 @@ __device__ __forceinline__ void atomic_max_pos(float* addr, float v) {
 
 // T threads per CTA, one CTA per SM (cooperative): 512 threads cap a thread
 // at 128 registers, 384 at 168, 256 at 255 -- fewer resident warps against
-// fewer spills; the world picks one (pmb_world_autotune).
-template <int T>
+// fewer spills; the world picks one (pmb_world_autotune). Timed: the
+// profiling build (pmb_world_profile_step), which records per-colour
+// timestamps of the first sweep; the ticks run the untimed build.
+template <int T, bool Timed>
 __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t phase) {
     constexpr int kSolveThreads = T;
     Counters* c = d.ctr;
@@ -646,7 +660,7 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
     __shared__ double wsq[kSolveThreads / 32];
     __shared__ uint32_t wn[kSolveThreads / 32], wov[kSolveThreads / 32];
     __shared__ float wmx[kSolveThreads / 32];
-    const bool timing = sp.debug_timing && phase == 0;
+    const bool timing = Timed && phase == 0;
     auto now = [] {
         unsigned long long t;
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -796,10 +810,13 @@ enum : uint32_t {
     kRBeta = 38,      // penalty growth factor of the pair
     kRTrial = 39,     // normal trial force at the start of the colour
     kRContact = 40,   // contact index
-    kRFlags = 41,     // bit 0: this body is the contact's first body; bit 1: its dual is updated here
-    kRowWords = 42,
+    kRFlags = 41,     // bit 0: this body is the contact's first body; bit 1: its dual is updated
+                      // here; bit 2: the row crosses (crossing safeguard, set by the body's group)
+    kRowWords = 43,   // odd: consecutive rows start in different shared-memory banks
 };
-constexpr size_t kStagedSmem = size_t(kStageRows) * kRowWords * 4 + size_t(kBatchBodies) * 12 * 4 + 64 * 4;
+constexpr uint32_t kStagedGroups = 64;  // lane groups per CTA at most (512 threads, 8 lanes)
+constexpr size_t kStagedSmem =
+    size_t(kStageRows) * kRowWords * 4 + size_t(kBatchBodies) * 12 * 4 + 64 * 4 + kStagedGroups * sizeof(Blk);
 
 struct StageTables {
     float* rows;       // kStageRows x kRowWords
@@ -810,6 +827,7 @@ struct StageTables {
     float* fric;       // per batch slot: friction
     float* invm;       // per batch slot: inverse mass
     uint32_t* scratch; // 64 words for scans and counts
+    Blk* jblk;         // per lane group: the block while joint rows are added
 };
 __device__ __forceinline__ StageTables stage_tables(uint8_t* raw) {
     StageTables t;
@@ -822,6 +840,7 @@ __device__ __forceinline__ StageTables stage_tables(uint8_t* raw) {
     t.fric = t.dx + 6 * kBatchBodies;
     t.invm = t.fric + kBatchBodies;
     t.scratch = reinterpret_cast<uint32_t*>(t.invm + kBatchBodies);
+    t.jblk = reinterpret_cast<Blk*>(t.scratch + 64);
     return t;
 }
 
@@ -875,9 +894,9 @@ __device__ __forceinline__ void stage_row(const Dev& d, const StageTables& tb, u
     float* row = tb.rows + size_t(t) * kRowWords;
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
-        const V6& jr = first ? ja[x] : jb[x];
+        // Selected element by element (no run-time reference into either array).
 #pragma unroll
-        for (int k = 0; k < 6; ++k) row[kRJ + 6 * x + k] = jr.v[k];
+        for (int k = 0; k < 6; ++k) row[kRJ + 6 * x + k] = first ? ja[x].v[k] : jb[x].v[k];
     }
     row[kRSt + 0] = pen.x * sc.n;
     row[kRSt + 1] = pen.y * sc.t0;
@@ -979,6 +998,10 @@ __device__ void owned_joint_duals(const Dev& d, uint32_t i, uint32_t col, float 
     }
 }
 
+template <int G>
+__device__ __forceinline__ V6 staged_update(const Dev& d, uint32_t i, uint32_t phase, const V6& upd, uint32_t gmask,
+                                            int gl);
+
 // One body's primal from the stage (G lanes; lane gl), then its owned duals.
 template <int G>
 __device__ void staged_body(const Dev& d, const StageTables& tb, uint32_t sl, uint32_t col, uint32_t phase, float dt,
@@ -1042,102 +1065,51 @@ __device__ void staged_body(const Dev& d, const StageTables& tb, uint32_t sl, ui
     Blk blk;
     gather_block<G>(ent, blk, gmask, gbase);
     const uint32_t jcnt = d.jdeg[i];
-    if (jcnt) {
-        if (gl == 0) {
-            const uint32_t jlo = d.jinc_off[i];
-            for (uint32_t k = 0; k < jcnt; ++k) {
-                const uint32_t j = d.jinc_list[jlo + k];
-                const JointState js = d.jstate[j];
-                if (!js.enabled) continue;
-                const uint32_t a = js.dense_a, b = js.dense_b;
-                const bool first = i == a;
-                if (phase == 0) {
-                    BodyView A = load_body(d, a), B = load_body(d, b);
-                    visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]),
-                                q4(d.q[b]), d.p0[a], d.p0[b], dt, &blk, first, kVisitAccumulate, nullptr);
-                } else {
-                    const Lite A = load_lite(d, a), B = load_lite(d, b);
-                    for (uint32_t r = 0; r < js.count; ++r) {
-                        Row row = load_row(d.jrows[size_t(j) * 18 + r]);
-                        if (row.stiffness >= kMaxPenalty) row_accumulate(blk, row, first, A.dx, B.dx, dt);
-                    }
-                }
-            }
-        }
-        __syncwarp(gmask);
-#pragma unroll
-        for (int e = 0; e < 21; ++e) blk.h[e] = __shfl_sync(gmask, blk.h[e], gbase);
-#pragma unroll
-        for (int r = 0; r < 6; ++r) blk.g[r] = __shfl_sync(gmask, blk.g[r], gbase);
-    }
+    if (jcnt) joint_rows_shared<G>(d, i, phase, dt, blk, tb.jblk + threadIdx.x / G, gmask, gl);
     V6 upd;
     const bool solved = block_solve(blk, upd);
     V6 dxn = dx0;
     if (solved) {
-        // Crossing safeguard (geometry_constraints_solve.slang:433-475) from
-        // the staged normal rows, flagged rows added in list order.
-        own_entries<G>(blk, gl, ent);
-        bool crossing = false;
+        // Crossing safeguard (geometry_constraints_solve.slang:433-475): each
+        // lane flags its share of the staged normal rows, then every lane adds
+        // the flagged rows to its entries in list order.
+        bool flagged = false;
+        for (uint32_t t = r0 + gl; t < r1; t += G) {
+            float* row = tb.rows + size_t(t) * kRowWords;
+            V6 nr;
 #pragma unroll
-        for (int q = 0; q < Owned<G>::E; ++q) {
-            const int e = gl + G * q;
-            int ei = 0, ek = 0;
-            if (e < 21) entry_ik(e, ei, ek);
-            for (uint32_t t = r0; t < r1; ++t) {
-                const float* row = tb.rows + size_t(t) * kRowWords;
-                V6 nr;
-#pragma unroll
-                for (int k = 0; k < 6; ++k) nr.v[k] = row[kRJ + k];
-                const float k0 = row[kRPen], trial = row[kRTrial];
-                if (!(trial <= 0.0f && trial + k0 * dot6(nr, upd) > k0 * 1.0e-6f)) continue;
-                crossing = true;
-                if (e < 21) ent[q] += k0 * nr.v[ei] * nr.v[ek];
-                else if (e < 27) ent[q] += nr.v[e - 21] * trial;
-            }
+            for (int k = 0; k < 6; ++k) nr.v[k] = row[kRJ + k];
+            const float k0 = row[kRPen], trial = row[kRTrial];
+            const bool cross = trial <= 0.0f && trial + k0 * dot6(nr, upd) > k0 * 1.0e-6f;
+            uint32_t flags = __float_as_uint(row[kRFlags]);
+            flags = cross ? (flags | 4u) : (flags & ~4u);
+            row[kRFlags] = __uint_as_float(flags);
+            flagged = flagged || cross;
         }
+        const bool crossing = __any_sync(gmask, flagged);
+        __syncwarp(gmask);
         if (crossing) {
+            own_entries<G>(blk, gl, ent);
+#pragma unroll
+            for (int q = 0; q < Owned<G>::E; ++q) {
+                const int e = gl + G * q;
+                if (e >= 27) continue;
+                int ei = 0, ek = 0;
+                if (e < 21) entry_ik(e, ei, ek);
+                float acc = ent[q];
+                for (uint32_t t = r0; t < r1; ++t) {
+                    const float* row = tb.rows + size_t(t) * kRowWords;
+                    if (!(__float_as_uint(row[kRFlags]) & 4u)) continue;
+                    const float k0 = row[kRPen];
+                    acc += e < 21 ? k0 * row[kRJ + ei] * row[kRJ + ek] : row[kRJ + e - 21] * row[kRTrial];
+                }
+                ent[q] = acc;
+            }
             gather_block<G>(ent, blk, gmask, gbase);
             V6 safe;
             if (block_solve(blk, safe)) upd = safe;
         }
-        // The update (apply_pose_update / the impact phase's linear update),
-        // computed by every lane so each holds the new displacement. Every
-        // lane reads the body's state before lane 0 stores the update.
-        float4 l = d.dxl[i], a = d.dxa[i];
-        Q4 rel = q4(d.dq[i]);
-        __syncwarp(gmask);
-        if (phase == 0) {
-            l.x += upd.v[0];
-            l.y += upd.v[1];
-            l.z += upd.v[2];
-            const V3 r{upd.v[3], upd.v[4], upd.v[5]};
-            const bool rotates = !(r.x == 0.0f && r.y == 0.0f && r.z == 0.0f);
-            if (rotates) {
-                Q4 dd = qmul(Q4{r.x, r.y, r.z, 0.0f}, rel);
-                rel = qnormalize(Q4{rel.x + 0.5f * dd.x, rel.y + 0.5f * dd.y, rel.z + 0.5f * dd.z, rel.w + 0.5f * dd.w});
-                if (rel.w < 0.0f) rel = {-rel.x, -rel.y, -rel.z, -rel.w};
-                a = make_float4(2.0f * rel.x, 2.0f * rel.y, 2.0f * rel.z, 0.0f);
-            }
-            if (gl == 0) {
-                d.dxl[i] = l;
-                if (rotates) {
-                    d.dq[i] = f4(rel);
-                    d.dxa[i] = a;
-                }
-            }
-        } else {
-            l.x += upd.v[0];
-            l.y += upd.v[1];
-            l.z += upd.v[2];
-            a.x += upd.v[3];
-            a.y += upd.v[4];
-            a.z += upd.v[5];
-            if (gl == 0) {
-                d.dxl[i] = l;
-                d.dxa[i] = a;
-            }
-        }
-        dxn = {{l.x, l.y, l.z, a.x, a.y, a.z}};
+        dxn = staged_update<G>(d, i, phase, upd, gmask, gl);
     }
     __syncwarp(gmask);
     // Owned contact duals, one row per lane.
@@ -1156,7 +1128,48 @@ __device__ void staged_body(const Dev& d, const StageTables& tb, uint32_t sl, ui
     if (jcnt) owned_joint_duals(d, i, col, dt, phase, res, it, gl, G);
 }
 
-template <int T>
+// The body's update (apply_pose_update, geometry_constraints_solve.slang:
+// 374-399, or the impact phase's linear update): lane 0 stores it; every lane
+// returns the new displacement. Every lane reads the body's state before
+// lane 0 stores.
+template <int G>
+__device__ __forceinline__ V6 staged_update(const Dev& d, uint32_t i, uint32_t phase, const V6& upd, uint32_t gmask,
+                                            int gl) {
+    float4 l = d.dxl[i], a = d.dxa[i];
+    Q4 rel = q4(d.dq[i]);
+    __syncwarp(gmask);
+    l.x += upd.v[0];
+    l.y += upd.v[1];
+    l.z += upd.v[2];
+    if (phase == 0) {
+        const V3 r{upd.v[3], upd.v[4], upd.v[5]};
+        const bool rotates = !(r.x == 0.0f && r.y == 0.0f && r.z == 0.0f);
+        if (rotates) {
+            Q4 dd = qmul(Q4{r.x, r.y, r.z, 0.0f}, rel);
+            rel = qnormalize(Q4{rel.x + 0.5f * dd.x, rel.y + 0.5f * dd.y, rel.z + 0.5f * dd.z, rel.w + 0.5f * dd.w});
+            if (rel.w < 0.0f) rel = {-rel.x, -rel.y, -rel.z, -rel.w};
+            a = make_float4(2.0f * rel.x, 2.0f * rel.y, 2.0f * rel.z, 0.0f);
+        }
+        if (gl == 0) {
+            d.dxl[i] = l;
+            if (rotates) {
+                d.dq[i] = f4(rel);
+                d.dxa[i] = a;
+            }
+        }
+    } else {
+        a.x += upd.v[3];
+        a.y += upd.v[4];
+        a.z += upd.v[5];
+        if (gl == 0) {
+            d.dxl[i] = l;
+            d.dxa[i] = a;
+        }
+    }
+    return {{l.x, l.y, l.z, a.x, a.y, a.z}};
+}
+
+template <int T, bool Timed>
 __global__ void __launch_bounds__(T, 1) k_solve_staged(Dev d, StepParams sp, uint32_t phase) {
     Counters* c = d.ctr;
     if (phase != 0 && c->impact == 0) return;
@@ -1176,6 +1189,8 @@ __global__ void __launch_bounds__(T, 1) k_solve_staged(Dev d, StepParams sp, uin
     __shared__ double wsq[T / 32];
     __shared__ uint32_t wn[T / 32], wov[T / 32];
     __shared__ float wmx[T / 32];
+    const bool timing = Timed && phase == 0;
+    if (timing && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_start = gtimer();
     for (uint32_t it = 0; it < iters; ++it) {
         Res res{0.0, 0u, 0.0f, 0u, sp.tolerance};
         const uint32_t parity = (it & 1u) * 512u;
@@ -1275,6 +1290,7 @@ __global__ void __launch_bounds__(T, 1) k_solve_staged(Dev d, StepParams sp, uin
                     j0 += fit;
                 }
             }
+            if (timing && it == 0 && col < 19 && threadIdx.x == 0) atomicMax(&c->dbg_work[col], gtimer());
             if (col + 1 >= colors) {
                 // Joints with no dynamic body have no owner above; their
                 // duals (applied impulse, breaking) are updated here.
@@ -1287,9 +1303,11 @@ __global__ void __launch_bounds__(T, 1) k_solve_staged(Dev d, StepParams sp, uin
                 // duals), published by the barrier below.
                 block_residual<T>(res, wsq, wn, wmx, wov, c, parity + blockIdx.x);
                 if (!grid_sync(c, d.barrier_spins)) return;
+                if (timing && it == 0 && col < 19 && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_release[col] = gtimer();
                 break;
             }
             if (!grid_sync(c, d.barrier_spins)) return;
+            if (timing && it == 0 && col < 19 && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_release[col] = gtimer();
         }
         const SweepResidual sw = sweep_residual(c, parity, sp);
         if (phase == 0 && grid_stride_begin() == 0) c->residual_trace[it] = sw.measure;
@@ -1311,11 +1329,16 @@ __global__ void __launch_bounds__(T, 1) k_solve_staged(Dev d, StepParams sp, uin
 }
 
 const SolveVariant solve_variants[kSolveVariants] = {
-    {reinterpret_cast<const void*>(&k_solve<512>), 512, kWarpStage * (512 / 32)},
-    {reinterpret_cast<const void*>(&k_solve<384>), 384, kWarpStage * (384 / 32)},
-    {reinterpret_cast<const void*>(&k_solve<256>), 256, kWarpStage * (256 / 32)},
-    {reinterpret_cast<const void*>(&k_solve_staged<512>), 512, kStagedSmem},
-    {reinterpret_cast<const void*>(&k_solve_staged<384>), 384, kStagedSmem},
+    {reinterpret_cast<const void*>(&k_solve<512, false>), reinterpret_cast<const void*>(&k_solve<512, true>), 512,
+     kWarpStage * (512 / 32)},
+    {reinterpret_cast<const void*>(&k_solve<384, false>), reinterpret_cast<const void*>(&k_solve<384, true>), 384,
+     kWarpStage * (384 / 32)},
+    {reinterpret_cast<const void*>(&k_solve<256, false>), reinterpret_cast<const void*>(&k_solve<256, true>), 256,
+     kWarpStage * (256 / 32)},
+    {reinterpret_cast<const void*>(&k_solve_staged<512, false>),
+     reinterpret_cast<const void*>(&k_solve_staged<512, true>), 512, kStagedSmem},
+    {reinterpret_cast<const void*>(&k_solve_staged<384, false>),
+     reinterpret_cast<const void*>(&k_solve_staged<384, true>), 384, kStagedSmem},
 };
 
 // Last-iteration contact work (geometry_constraints_solve.slang:533-561),
@@ -1656,7 +1679,10 @@ void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, const 
         StepParams spp = sp;
         void* args[] = {&dd, &spp, &ph};
         solve_timer_begin(s);
-        cudaLaunchCooperativeKernel(sv.ptr, dim3(coop), dim3(sv.threads), args, sv.smem, s);
+        // The profiling build only for pmb_world_profile_step (it has the
+        // same launch shape; the world sized its grid for both).
+        cudaLaunchCooperativeKernel(sp.debug_timing ? sv.timed : sv.ptr, dim3(coop), dim3(sv.threads), args, sv.smem,
+                                    s);
         note_launch(coop);
         solve_timer_end(s);
         prof_mark(s, phase ? "solve phase 1" : "solve phase 0");

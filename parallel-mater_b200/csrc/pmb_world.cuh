@@ -370,7 +370,8 @@ void solve_timer_begin(cudaStream_t s);
 void solve_timer_end(cudaStream_t s);
 // Cooperative solve kernel variants (threads per CTA) and their smem.
 struct SolveVariant {
-    const void* ptr;
+    const void* ptr;    // the tick's kernel
+    const void* timed;  // the same with per-colour timestamps (profiling)
     int threads;
     size_t smem;
 };

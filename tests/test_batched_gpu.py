@@ -106,3 +106,29 @@ def test_batched_plans_are_bit_identical(gpu_available):
             ref = x
         assert np.array_equal(x, ref), (v, p)
         w.close()
+
+
+def test_batch_of_config5_scenes_equals_the_oracle(gpu_available):
+    """Sixteen scenes drawn from the 1,024-scene batch (the config-5 mix of
+    piles and chains, log-uniform sizes, seed 5) stepped as one batched world
+    on the GPU for 20 ticks: every scene's states equal the CPU oracle
+    stepping that scene alone, bit for bit, and every scene's contact count
+    and sweep count match the oracle's."""
+    import oracle as O
+    ids = list(range(0, 1024, 64))
+    sizes, kinds = scenes.batched_plan(1024, 5)
+    parts = [scenes.batched_part(k, sizes[k], kinds[k], 5) for k in ids]
+    batch = scenes.batch(parts)
+    wb = core.World(batch)
+    cpu = [O.OracleWorld(p) for p in parts]
+    offs = np.concatenate([[0], np.cumsum([p.n for p in parts])])
+    for t in range(20):
+        sb = wb.step()
+        assert sb["status"] == 0, core.status_names(int(sb["status"]))
+        res = [o.step() for o in cpu]
+        xb = wb.states()
+        _, _, its, cts = wb.scene_stats()
+        for k, o in enumerate(cpu):
+            assert np.array_equal(xb[offs[k]:offs[k + 1]].view(np.uint8), o.states().view(np.uint8)), (t, ids[k])
+            assert cts[k] == res[k]["contacts"] and its[k] == res[k]["iterations"], (t, ids[k])
+    wb.close()

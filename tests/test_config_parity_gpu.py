@@ -4,12 +4,11 @@ the CPU oracle frame by frame, then long runs on the GPU against the
 reference's physical gates, and the error against an FP64 replay.
 
 Parity (every compared frame): candidate pair sets, manifold pair codes and
-point counts, colours of dynamic bodies and island roots are equal; poses
-(x, q, v) agree within POSE_TOL. The tick evaluates every expression in the
+point counts, colours of dynamic bodies and island roots are equal, and so
+are the poses, bit for bit: the tick evaluates every expression in the
 reference's order from IEEE-exact operations (no contraction, IEEE division
 and square root, arctangent and cotangent from series of basic operations),
-so GPU and oracle are expected to agree bit for bit; each test prints its
-worst pose difference and how many frames were bit-identical.
+as the oracle does.
 
 Physical gates (the reference's realtime stack gates,
 tests/solver/rigid_realtime_cuda_tests.cu:362-370, with the measures of
@@ -30,9 +29,6 @@ import oracle as O
 import physics_gates as G
 
 pytestmark = pytest.mark.gpu
-
-POSE_TOL = 1e-4  # m, m/s and quaternion components (FP32 trajectories of the same arithmetic)
-
 
 def compare(scene, frames, fp64_frames=0, label="", joints=False):
     """GPU and FP32 oracle side by side for `frames` ticks (and the FP64
@@ -62,7 +58,7 @@ def compare(scene, frames, fp64_frames=0, label="", joints=False):
         err = max(float(np.abs(xg[k] - xo[k]).max()) for k in ("x", "q", "v"))
         exact += int(all(np.array_equal(xg[k], xo[k]) for k in ("x", "q", "v", "w")))
         worst = max(worst, err)
-        assert err <= POSE_TOL, (label, f, err)
+        assert np.array_equal(xg.view(np.uint8), xo.view(np.uint8)), (label, f, err)
         if o64 is not None and f < fp64_frames:
             o64.step()
             worst64 = max(worst64, float(np.abs(xg["x"].astype(np.float64) - o64.states()["x"]).max()))

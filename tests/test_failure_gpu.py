@@ -100,6 +100,10 @@ def test_driver_failure_lifecycle(gpu_available, failtest_driver):
     assert api.pmCmdStepSimulation(s.cb, s.sim, pm.ref(step)) == OUT_OF_HOST_MEMORY
     _set("PM_TEST_FAIL_RECORDING", None)
     assert api.pmEndCommandBuffer(s.cb) == OUT_OF_HOST_MEMORY
+    # The buffer stays in the recording state with its error latched
+    # (reference src/api/commands.cpp:132-140); a reset clears it.
+    assert api.pmBeginCommandBuffer(s.cb, pm.ref(begin)) == pm.ERROR_INVALID_STATE
+    assert api.pmResetCommandBuffer(s.cb) == pm.SUCCESS
     assert s.step() == pm.SUCCESS
 
     # Submission failure comes before acceptance: the fence does not become pending.
