@@ -54,7 +54,9 @@ SETTLED = os.path.join(ROOT, "tests", "golden", "settled_pile_64x32x32.npz")
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "k_solve_pile65k.md")
 NORMS = {"max": 0, "rms": 1, "p999": 2}
 LANE_POLICIES = ["8/16/32 by colour size", "8", "8/16/32 by body rows, heaviest first",
-                 "8/16/32 by colour size, bodies claimed dynamically"]
+                 "8/16/32 by colour size, bodies claimed dynamically",
+                 "a body per thread in large colours, else 8/16/32 by colour size"]
+SOLVE_THREADS = [512, 384, 256, 512, 384]  # plans 3, 4: the staged solve with fused duals
 
 
 def parse():
@@ -79,7 +81,19 @@ def parse():
     ap.add_argument("--scenes", type=int, default=1024, help="batched: scene count")
     ap.add_argument("--settle", type=int, default=120, help="batched: plain ticks from the spawn before timing")
     ap.add_argument("--cpu-scenes", type=int, default=48, help="batched: scenes in the CPU baseline sample")
+    ap.add_argument("--plan", default="", help="solve launch plan 'variant,policy' instead of the autotuner's")
     return ap.parse_args()
+
+
+def choose_plan(world, desc, args):
+    """The launch plan: --plan if given (set at once), else the autotuner's
+    pick on this workload (state restored afterwards)."""
+    if args.plan:
+        v, p = (int(x) for x in args.plan.split(","))
+        world.set_launch_plan(v, p)
+        return v, p
+    v, p, _ = world.autotune(desc, ticks=3)
+    return v, p
 
 
 def load_scene():
@@ -236,6 +250,8 @@ def gpu_arm(args):
     stream = torch.cuda.Stream()             # a capturable (non-default) stream for the graph
     world.set_stream(stream.cuda_stream)
     steps = args.steps + (args.steps & 1)
+    if args.plan:
+        choose_plan(world, plain, args)
 
     def barrier():
         if world_size > 1:
@@ -249,8 +265,8 @@ def gpu_arm(args):
 
     for _ in range(args.warmup):
         world.step(plain, stats=False)
-    # Pick the solve launch plan on this workload (state restored afterwards).
-    plan_v, plan_p, _ = world.autotune(plain, ticks=3)
+    # The solve launch plan for this workload (autotuned unless --plan).
+    plan_v, plan_p = choose_plan(world, plain, args)
     world.snapshot()
 
     # ---- online training of the warm-start MLP on plain ticks (untimed)
@@ -296,14 +312,17 @@ def gpu_arm(args):
             peak, peak_src = float(json.load(f)["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
         peak, peak_src = 6650.0, "fallback"
-    # DRAM bytes per k_solve launch from the committed ncu capture of this
-    # workload (dram__bytes_read.sum + dram__bytes_write.sum).
+    # DRAM bytes per k_solve launch: the committed ncu capture of this
+    # workload gives dram__bytes_read.sum + dram__bytes_write.sum per sweep
+    # (one captured launch divided by its sweeps); scaled here by the mean
+    # sweeps of this run's launches, since the schedule sets the sweep count.
     traffic = None
     try:
         with open(PROFILE_SUMMARY) as f:
             for line in f:
-                if line.startswith("dram_bytes_per_launch:"):
-                    traffic = float(line.split(":")[1])
+                if line.startswith("dram_bytes_per_sweep:"):
+                    sweeps = sum((2 if int(st["impact"]) else 1) * int(st["iterations"]) for st in learned_stats)
+                    traffic = float(line.split(":")[1]) * sweeps / max(1, solve_launches)
     except (OSError, ValueError):
         pass
 
@@ -366,7 +385,7 @@ def gpu_arm(args):
                                         "steps_per_frame": args.mlp_steps, "seconds": round(train_s, 2),
                                         "loss_over_plain_loss": mlp_loss / mlp_plain_loss if mlp_plain_loss else None,
                                         "gate_open": bool(mlp_gate)},
-                       "launch_plan": {"solve_threads": [512, 384, 256][plan_v],
+                       "launch_plan": {"solve_threads": SOLVE_THREADS[plan_v], "staged": plan_v >= 3,
                                        "lanes_per_body": LANE_POLICIES[plan_p]},
                        "parallelism": f"replicas x{world_size}",
                        "tick": "CUDA graph replays (one graph = two ticks); e2e: one pmb_world_step per tick",
@@ -468,6 +487,8 @@ def gpu_batched(args):
     stream = torch.cuda.Stream()             # a capturable (non-default) stream for the graph
     world.set_stream(stream.cuda_stream)
     steps = args.steps + (args.steps & 1)
+    if args.plan:
+        choose_plan(world, plain, args)
 
     def barrier():
         if world_size > 1:
@@ -496,7 +517,7 @@ def gpu_batched(args):
     if status:
         raise RuntimeError("batched world status: %s" % core.status_names(status))
     settle_s = time.perf_counter() - t0
-    plan_v, plan_p, _ = world.autotune(plain, ticks=3)
+    plan_v, plan_p = choose_plan(world, plain, args)
     world.snapshot()
 
     def graph_arm(desc):
@@ -619,7 +640,7 @@ def gpu_batched(args):
                                         "loss_over_plain_loss": mlp_loss / mlp_plain_loss if mlp_plain_loss else None,
                                         "gate_open": bool(mlp_gate)},
                        "settle_seconds": round(settle_s, 1),
-                       "launch_plan": {"solve_threads": [512, 384, 256][plan_v],
+                       "launch_plan": {"solve_threads": SOLVE_THREADS[plan_v], "staged": plan_v >= 3,
                                        "lanes_per_body": LANE_POLICIES[plan_p]},
                        "parallelism": f"scenes bin-packed by body count over {world_size} GPU(s)",
                        "l2": "inputs larger than L2 (per-tick working set several hundred MB)"},

@@ -796,7 +796,14 @@ int pmb_world_profile_step(pmb_world* w, const pmb_step_desc* step, char* report
                       hc.dbg_rn, hc.dbg_body[0] * 1e-3, hc.dbg_body[1] * 1e-3, hc.dbg_body[2] * 1e-3, hc.dbg_body[3] * 1e-3,
                       hc.dbg_body[4] * 1e-3);
         text += line;
-        if (hc.dbg_sum[6]) {
+        if (hc.dbg_sum[6] && w->d.solve_variant >= kStagedFirst) {
+            const double nb = double(hc.dbg_sum[6]);
+            std::snprintf(line, sizeof(line),
+                          "  colour 0 mean over %.0f batches (mean rows %.1f): formation %.1f staging %.1f solve %.1f us\n",
+                          nb, hc.dbg_sum[7] / nb, hc.dbg_sum[0] * 1e-3 / nb, hc.dbg_sum[1] * 1e-3 / nb,
+                          hc.dbg_sum[2] * 1e-3 / nb);
+            text += line;
+        } else if (hc.dbg_sum[6]) {
             const double nb = double(hc.dbg_sum[6]);
             std::snprintf(line, sizeof(line),
                           "  colour 0 mean over %.0f bodies (mean rn %.1f): stage %.1f gather %.1f solve %.1f crossing "
@@ -1439,8 +1446,9 @@ int pmb_world_scene_stats(pmb_world* w, float* residual, float* residual_max, ui
     return PMB_SUCCESS;
 }
 
-constexpr uint32_t kSolvePolicies = 4;
-const char* const kPolicyNames[kSolvePolicies] = {"per colour", "8 lanes   ", "per body  ", "claimed   "};
+constexpr uint32_t kSolvePolicies = 5;
+const char* const kPolicyNames[kSolvePolicies] = {"per colour", "8 lanes   ", "per body  ", "claimed   ",
+                                                  "thread/body"};
 
 // The staged variants choose lanes per body per colour batch (policy 0) or
 // always 8 (policy 1); policies 2 and 3 run them as policy 0.

@@ -142,6 +142,7 @@ template <int G> struct GroupRows {
 // 32-lane group.
 constexpr size_t kWarpStage = 4 * sizeof(GroupRows<8>);
 static_assert(2 * sizeof(GroupRows<16>) <= kWarpStage && sizeof(GroupRows<32>) <= kWarpStage, "staging area");
+static_assert(32 * sizeof(Blk) <= kWarpStage, "a block slot per thread for the body-per-thread sweep");
 
 __device__ __forceinline__ void entry_ik(int e, int& i, int& k) {
     i = e >= 15 ? 5 : e >= 10 ? 4 : e >= 6 ? 3 : e >= 3 ? 2 : e >= 1 ? 1 : 0;
@@ -436,6 +437,144 @@ __device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float
     }
 }
 
+// One thread solves body i: the serial loop of geometry_constraints_solve.
+// slang:339-475 as written -- add_row per contact row in list order, the
+// joints' rows, LDL^T, then the crossing safeguard over the normal rows --
+// for colours with far more bodies than the grid has lane groups, where a
+// body per thread finishes the colour in fewer rounds than wider groups.
+// `sb`: this thread's shared-memory block slot for the joint visit.
+__device__ __forceinline__ void load_normal_rows(const Dev& d, uint32_t c, V6& ja, V6& jb) {
+    const float4* p = d.c_jac + size_t(c) * 9;
+    const float4 a0 = p[0], a1 = p[1], b4 = p[4], b5 = p[5];  // floats 0-7 and 16-23
+    ja = {{a0.x, a0.y, a0.z, a0.w, a1.x, a1.y}};
+    jb = {{b4.z, b4.w, b5.x, b5.y, b5.z, b5.w}};
+}
+__device__ void solve_body_thread(const Dev& d, uint32_t i, uint32_t phase, float dt, Blk* sb) {
+    const Lite me = load_lite(d, i);
+    const float my_friction = d.p1[i].x;
+    const uint32_t ro = d.roff[i], rn = d.rcount[i];
+    Blk blk;
+    {
+        const float4 ia = d.inA[i], ib = d.inB[i];
+#pragma unroll
+        for (int k = 0; k < 21; ++k) blk.h[k] = 0.0f;
+        blk.h[bidx(0, 0)] = ia.x;
+        blk.h[bidx(1, 1)] = ia.x;
+        blk.h[bidx(2, 2)] = ia.x;
+        blk.h[bidx(3, 3)] = ia.y;
+        blk.h[bidx(4, 3)] = ia.z;
+        blk.h[bidx(5, 3)] = ib.x;
+        blk.h[bidx(4, 4)] = ia.w;
+        blk.h[bidx(5, 4)] = ib.y;
+        blk.h[bidx(5, 5)] = ib.z;
+#pragma unroll
+        for (int r = 0; r < 6; ++r) {
+            float gs = 0.0f;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) gs += blk.h[bidx(r, c)] * me.dx.v[c];
+            blk.g[r] = gs;
+        }
+    }
+    for (uint32_t r = 0; r < rn; ++r) {
+        const uint32_t code = d.blist[ro + r], other_body = d.bother[ro + r];
+        const uint32_t c = code & 0x7fffffffu;
+        const bool first = (code >> 31) == 0;
+        const Lite other = load_lite(d, other_body);
+        const Lite A = first ? me : other, B = first ? other : me;
+        const float of = d.p1[other_body].x;
+        const float friction = sqrtf(first ? my_friction * of : of * my_friction);
+        const float4 lam = d.c_lam[c], pen = d.c_pen[c];
+        V6 ja[3], jb[3];
+        float err[3];
+        contact_rows(d, c, d.c_e[c], A, B, ja, jb, err);
+        const F3 trial{lam.x + pen.x * err[0], lam.y + pen.y * err[1], lam.z + pen.z * err[2]};
+        const F3 f = project_contact(trial, friction);
+        const F3 sc = stiffness_scales(trial, friction);
+        float forces[3] = {f.n, f.t0, f.t1};
+        if (phase != 0) {
+            V3 t0, t1;
+            basis(v3(d.c_n[c]), t0, t1);
+            const V3 af = v3(d.c_accf[c]);
+            forces[0] = f.n - lam.w / dt;
+            forces[1] = f.t0 - dot(af, t0) / dt;
+            forces[2] = f.t1 - dot(af, t1) / dt;
+        }
+        const float st[3] = {pen.x * sc.n, pen.y * sc.t0, pen.z * sc.t1};
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            V6 row;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) row.v[k] = first ? ja[x].v[k] : jb[x].v[k];
+            add_row(blk, row, st[x], forces[x]);
+        }
+    }
+    if (d.jdeg[i]) {
+        // The joint visit takes the block's address: work on this thread's
+        // shared-memory copy so the register block never needs one.
+        *sb = blk;
+        const uint32_t jcnt = d.jdeg[i], jlo = d.jinc_off[i];
+        for (uint32_t k = 0; k < jcnt; ++k) {
+            const uint32_t j = d.jinc_list[jlo + k];
+            const JointState js = d.jstate[j];
+            if (!js.enabled) continue;
+            const uint32_t a = js.dense_a, b = js.dense_b;
+            const bool first = i == a;
+            if (phase == 0) {
+                BodyView A = load_body(d, a), B = load_body(d, b);
+                visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]),
+                            q4(d.q[b]), d.p0[a], d.p0[b], dt, sb, first, kVisitAccumulate, nullptr);
+            } else {
+                const Lite A = load_lite(d, a), B = load_lite(d, b);
+                for (uint32_t r = 0; r < js.count; ++r) {
+                    Row row = load_row(d.jrows[size_t(j) * 18 + r]);
+                    if (row.stiffness >= kMaxPenalty) row_accumulate(*sb, row, first, A.dx, B.dx, dt);
+                }
+            }
+        }
+        blk = *sb;
+    }
+    V6 upd;
+    if (!block_solve(blk, upd)) return;
+    // Crossing safeguard: the normal rows again, at the same displacements.
+    bool crossing = false;
+    for (uint32_t r = 0; r < rn; ++r) {
+        const uint32_t code = d.blist[ro + r], other_body = d.bother[ro + r];
+        const uint32_t c = code & 0x7fffffffu;
+        const bool first = (code >> 31) == 0;
+        const Lite other = load_lite(d, other_body);
+        const Lite A = first ? me : other, B = first ? other : me;
+        V6 ja, jb;
+        load_normal_rows(d, c, ja, jb);
+        const float err0 = d.c_e[c].x + dot6(ja, A.dx) + dot6(jb, B.dx);
+        const float k0 = d.c_pen[c].x;
+        const float trial = d.c_lam[c].x + k0 * err0;
+        V6 nr;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) nr.v[k] = first ? ja.v[k] : jb.v[k];
+        if (trial <= 0.0f && trial + k0 * dot6(nr, upd) > k0 * 1.0e-6f) {
+            add_row(blk, nr, k0, trial);
+            crossing = true;
+        }
+    }
+    if (crossing) {
+        V6 safe;
+        if (block_solve(blk, safe)) upd = safe;
+    }
+    if (phase == 0) {
+        apply_pose_update(d, i, upd);
+    } else {
+        float4 l = d.dxl[i], a = d.dxa[i];
+        l.x += upd.v[0];
+        l.y += upd.v[1];
+        l.z += upd.v[2];
+        a.x += upd.v[3];
+        a.y += upd.v[4];
+        a.z += upd.v[5];
+        d.dxl[i] = l;
+        d.dxa[i] = a;
+    }
+}
+
 // Residual accumulator of one dual pass (this build's addition): rows that
 // carry force or penetrate contribute |C_n| (force > 0) or C_n (penetration
 // only); hard joint rows contribute |C|. Reported as the RMS, the largest
@@ -721,13 +860,25 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
             // width per colour by its size, 1 eight lanes, 2 a width per body
             // class (heaviest first) unless 32-lane groups cover the colour.
             uint32_t r32 = b0, r16 = b0, r8 = b0;  // 32 lanes [b0, r32), 16 [r32, r16), 8 [r16, r8)
-            if (d.solve_policy != 1 && nb * 32u <= nthreads) {
+            if (d.solve_policy == 4 && nb * 16u > nthreads) {
+                // A body per thread: the colour has more bodies than 16-lane
+                // groups could take in one round. Consecutive bodies go to
+                // consecutive CTAs, as for the groups.
+                Blk* slot = reinterpret_cast<Blk*>(warp_stage) + lane;
+                for (uint32_t k = b0 + threadIdx.x * gridDim.x + blockIdx.x; k < b1; k += nthreads) {
+                    const uint32_t i = d.corder[k];
+                    if (phase != 0 && d.impact[i] == 0) continue;
+                    if (batched(d) && it >= d.scene_budget[d.scene_of[i]]) continue;
+                    solve_body_thread(d, i, phase, dt, slot);
+                }
+                r32 = r16 = r8 = b0;
+            } else if (d.solve_policy != 1 && nb * 32u <= nthreads) {
                 r32 = r16 = r8 = b1;
             } else if (d.solve_policy == 2) {
                 r32 = off[1];
                 r16 = off[2];
                 r8 = b1;
-            } else if ((d.solve_policy == 0 || d.solve_policy == 3) && nb * 16u <= nthreads) {
+            } else if ((d.solve_policy == 0 || d.solve_policy >= 3) && nb * 16u <= nthreads) {
                 r16 = r8 = b1;
             } else {
                 r8 = b1;
@@ -1200,6 +1351,11 @@ __global__ void __launch_bounds__(T, 1) k_solve_staged(Dev d, StepParams sp, uin
                 const uint32_t span = hi - lo;
                 const uint32_t mine = span > blockIdx.x ? (span - blockIdx.x + gridDim.x - 1) / gridDim.x : 0u;
                 for (uint32_t j0 = 0; j0 < mine;) {
+                    // Profiling build: phase times of colour 0's batches in
+                    // the first sweep (formation, staging, solve) summed
+                    // over CTAs into dbg_sum[0..2], batches in dbg_sum[6].
+                    const bool phase_clock = timing && it == 0 && col == 0 && threadIdx.x == 0;
+                    unsigned long long tp0 = phase_clock ? gtimer() : 0ull;
                     // Batch slots: this CTA's next bodies of the colour.
                     const uint32_t want = min(kBatchBodies, mine - j0);
                     uint32_t cnt = 0;
@@ -1263,6 +1419,11 @@ __global__ void __launch_bounds__(T, 1) k_solve_staged(Dev d, StepParams sp, uin
                         j0 += 1;
                         continue;
                     }
+                    if (phase_clock) {
+                        const unsigned long long t = gtimer();
+                        atomicAdd(&c->dbg_sum[0], t - tp0);
+                        tp0 = t;
+                    }
                     // Stage every row of the batch, one thread per row.
                     const uint32_t rows = tb.off[fit];
                     for (uint32_t t = threadIdx.x; t < rows; t += T) {
@@ -1275,6 +1436,12 @@ __global__ void __launch_bounds__(T, 1) k_solve_staged(Dev d, StepParams sp, uin
                         stage_row(d, tb, t, a, t - tb.off[a], col, phase, dt);
                     }
                     __syncthreads();
+                    if (phase_clock) {
+                        const unsigned long long t = gtimer();
+                        atomicAdd(&c->dbg_sum[1], t - tp0);
+                        atomicAdd(&c->dbg_sum[7], (unsigned long long)rows);
+                        tp0 = t;
+                    }
                     // Solve: G lanes per body (wider groups when few bodies).
                     auto solve = [&](auto width) {
                         constexpr int G = decltype(width)::value;
@@ -1287,6 +1454,10 @@ __global__ void __launch_bounds__(T, 1) k_solve_staged(Dev d, StepParams sp, uin
                     else if (d.solve_policy != 1 && fit * 16u <= T) solve(std::integral_constant<int, 16>{});
                     else solve(std::integral_constant<int, 8>{});
                     __syncthreads();
+                    if (phase_clock) {
+                        atomicAdd(&c->dbg_sum[2], gtimer() - tp0);
+                        atomicAdd(&c->dbg_sum[6], 1ull);
+                    }
                     j0 += fit;
                 }
             }

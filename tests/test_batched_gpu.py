@@ -95,7 +95,7 @@ def test_batched_plans_are_bit_identical(gpu_available):
     claimed body assignment)."""
     batch = scenes.batch(_parts())
     ref = None
-    for v, p in ((1, 0), (1, 3), (0, 2), (2, 1), (0, 3), (4, 0), (3, 1)):
+    for v, p in ((1, 0), (1, 3), (0, 2), (2, 1), (0, 3), (4, 0), (3, 1), (1, 4)):
         w = core.World(batch)
         w.set_launch_plan(v, p)
         for _ in range(20):

@@ -252,7 +252,7 @@ def test_launch_plans_are_bit_identical(gpu_available):
     them and leaves the state as it found it."""
     s = scenes.box_pile((6, 4, 6), seed=13, spacing=1.6)
     ref = None
-    plans = [(v, p) for v in range(3) for p in range(4)] + [(v, p) for v in (3, 4) for p in range(2)]
+    plans = [(v, p) for v in range(3) for p in range(5)] + [(v, p) for v in (3, 4) for p in range(2)]
     for v, p in plans:
         w = core.World(s)
         w.set_launch_plan(v, p)
@@ -279,7 +279,7 @@ def test_launch_plans_are_bit_identical_on_the_settled_pile(gpu_available):
     z = np.load(os.path.join(os.path.dirname(__file__), "golden", "settled_pile_64x32x32.npz"))
     s.states = z["states"].astype(np.float32).view(scenes.STATE_DTYPE).reshape(-1).copy()
     ref = None
-    for v, p in ((1, 0), (0, 1), (0, 2), (1, 2), (2, 2), (1, 3), (0, 3), (3, 0), (4, 0), (4, 1)):
+    for v, p in ((1, 0), (0, 1), (0, 2), (1, 2), (2, 2), (1, 3), (0, 3), (3, 0), (4, 0), (4, 1), (1, 4), (0, 4)):
         w = core.World(s)
         w.set_launch_plan(v, p)
         for _ in range(4):
