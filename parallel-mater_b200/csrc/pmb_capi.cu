@@ -695,12 +695,16 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     d.solve_policy = 0;
     d.barrier_spins = kDefaultBarrierSpins;
     for (uint32_t v = 0; v < kSolveVariants; ++v) {
-        const SolveVariant& sv = solve_variants[v];
-        cudaFuncSetAttribute(sv.ptr, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sv.smem));
-        cudaFuncSetAttribute(sv.timed, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sv.smem));
-        // One grid for both builds: the smaller of their co-resident counts.
-        w->coop_solve[v] = std::min(coop_blocks_for(sv.ptr, sv.threads, sv.smem),
-                                    coop_blocks_for(sv.timed, sv.threads, sv.smem));
+        const SolveVariant& sv = solve_variant(v);
+        // One grid for every build of the variant: the smallest of their
+        // co-resident counts.
+        int blocks = 1 << 30;
+        for (int f = 0; f < kSolveFeatures; ++f)
+            for (const void* k : {sv.ptr[f], sv.timed[f]}) {
+                cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sv.smem));
+                blocks = std::min(blocks, coop_blocks_for(k, sv.threads, sv.smem));
+            }
+        w->coop_solve[v] = blocks;
     }
     {
         int dev = 0, sms = 0;
@@ -1497,7 +1501,7 @@ int pmb_world_autotune(pmb_world* w, const pmb_step_desc* step, uint32_t ticks, 
             cudaEventElapsedTime(&ms, a, b);
             char line[128];
             std::snprintf(line, sizeof(line), "solve %3d threads%s, widths %s: %8.3f ms/tick\n",
-                          solve_variants[v].threads, v >= kStagedFirst ? " staged" : "", kPolicyNames[p],
+                          ::pmb::solve_variant(v).threads, v >= kStagedFirst ? " staged" : "", kPolicyNames[p],
                           ms / float(ticks));
             text += line;
             if ((v == 0 && p == 0) || ms < best) {

@@ -76,9 +76,12 @@ __global__ void k_color_noalloc(const uint32_t* offsets, const uint32_t* neighbo
     volatile uint32_t* work = scratch + kHeaderWords;
     const uint32_t begin = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
     for (uint32_t v = begin; v < n; v += stride) work[v] = dynamic[v] ? 0u : kInvalid;
+    // The change counter is read by one thread per block and shared.
+    __shared__ uint32_t s_before, s_after;
     for (uint32_t round = 0; round < n + 2; ++round) {
-        const uint32_t before = ((volatile uint32_t*)h)[kHChanged];
+        if (threadIdx.x == 0) s_before = ((volatile uint32_t*)h)[kHChanged];
         if (!barrier(h)) return;
+        const uint32_t before = s_before;
         uint32_t changes = 0;
         bool overflow = false;
         for (uint32_t v = begin; v < n; v += stride) {
@@ -106,7 +109,9 @@ __global__ void k_color_noalloc(const uint32_t* offsets, const uint32_t* neighbo
         }
         if (changes) atomicAdd(h + kHChanged, changes);
         if (!barrier(h)) return;
-        if (((volatile uint32_t*)h)[kHChanged] == before) {
+        if (threadIdx.x == 0) s_after = ((volatile uint32_t*)h)[kHChanged];
+        __syncthreads();
+        if (s_after == before) {
             // Converged: only this round's mex counts. A vertex may pass 255
             // lower-neighbour colours in an intermediate round of the
             // fixpoint and still settle below 256.

@@ -419,9 +419,13 @@ __device__ __forceinline__ void mark_higher(const Dev& d, uint32_t v, uint8_t* n
 __global__ void __launch_bounds__(kColorThreads) k_color(Dev d) {
     Counters* c = d.ctr;
     if (c->status & kStBarrierTimeout) return;  // the tick was abandoned
+    // The change counter is read by one thread per block and shared: a read
+    // by every thread of the grid per round piles onto one L2 line.
+    __shared__ uint32_t s_before, s_after;
     for (uint32_t round = 0; round < d.n + 2; ++round) {
-        const uint32_t before = ((volatile uint32_t*)&c->changed)[0];
+        if (threadIdx.x == 0) s_before = ((volatile uint32_t*)&c->changed)[0];
         if (!grid_sync(c, d.barrier_spins)) return;
+        const uint32_t before = s_before;
         uint8_t* cur = d.cdirty + size_t(round & 1u) * d.n;
         uint8_t* next = d.cdirty + size_t((round + 1u) & 1u) * d.n;
         bool transient = false;  // a mex past 255 in this round (judged at the fixpoint)
@@ -439,9 +443,12 @@ __global__ void __launch_bounds__(kColorThreads) k_color(Dev d) {
                 mark_higher(d, v, next);
             }
         }
-        if (changes) atomicAdd(&c->changed, changes);
+        changes = __reduce_add_sync(0xffffffffu, changes);  // one atomic per warp
+        if (changes && (threadIdx.x & 31) == 0) atomicAdd(&c->changed, changes);
         if (!grid_sync(c, d.barrier_spins)) return;
-        const uint32_t after = ((volatile uint32_t*)&c->changed)[0];
+        if (threadIdx.x == 0) s_after = ((volatile uint32_t*)&c->changed)[0];
+        __syncthreads();
+        const uint32_t after = s_after;
         if (after == before) {
             // Converged. A body's mex can pass 255 colours in an intermediate
             // round and still settle below 256, so overflow is judged on the

@@ -10,65 +10,9 @@
 // last-iteration work (accumulated impulses, re-anchoring sliding contacts) is
 // applied after the loop from the final duals and the stick flag each dual
 // pass stores, which is the same arithmetic on the same values.
-#include <type_traits>
-
-#include "pmb_joint.cuh"
+#include "pmb_solve_common.cuh"
 
 namespace pmb {
-
-struct Lite {  // what a contact row needs of a body during the solve: its displacement
-    V6 dx;
-};
-__device__ __forceinline__ Lite load_lite(const Dev& d, uint32_t i) {
-    const float4 l = d.dxl[i], a = d.dxa[i];
-    return {{{l.x, l.y, l.z, a.x, a.y, a.z}}};
-}
-
-// Contact jacobians (geometry_constraints.slang:508-532). They depend only on
-// the contact geometry and the AVBD target poses, both fixed during a solve
-// phase, so they are evaluated once per phase (k_contact_jacobians) and
-// stored: 36 floats per contact, rows n, t0, t1 for body a then body b.
-__device__ __forceinline__ void contact_jacobians(V3 n, V3 pt, V3 anc_a, V3 anc_b, V3 xa, Q4 qa, V3 xb, Q4 qb,
-                                                  V6 ja[3], V6 jb[3]) {
-    V3 t0, t1;
-    basis(n, t0, t1);
-    const V3 axes[3] = {n, t0, t1};
-    const V3 arm_a = sub(pt, xa), arm_b = sub(pt, xb);
-    const V3 ra_t = rotate(qa, anc_a), rb_t = rotate(qb, anc_b);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        V3 ra = k == 0 ? arm_a : ra_t;
-        V3 rb = k == 0 ? arm_b : rb_t;
-        ja[k] = jac(mul(axes[k], -1.0f), mul(cross(ra, axes[k]), -1.0f));
-        jb[k] = jac(axes[k], cross(rb, axes[k]));
-    }
-}
-__device__ __forceinline__ void load_jac(const Dev& d, uint32_t c, V6 ja[3], V6 jb[3]) {
-    const float4* p = d.c_jac + size_t(c) * 9;
-    float f[36];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-        const float4 v = p[k];
-        f[4 * k] = v.x;
-        f[4 * k + 1] = v.y;
-        f[4 * k + 2] = v.z;
-        f[4 * k + 3] = v.w;
-    }
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            ja[r].v[k] = f[6 * r + k];
-            jb[r].v[k] = f[18 + 6 * r + k];
-        }
-}
-__device__ __forceinline__ void contact_rows(const Dev& d, uint32_t c, float4 e, const Lite& A, const Lite& B,
-                                             V6 ja[3], V6 jb[3], float err[3]) {
-    load_jac(d, c, ja, jb);
-    const float e3[3] = {e.x, e.y, e.z};
-#pragma unroll
-    for (int k = 0; k < 3; ++k) err[k] = e3[k] + dot6(ja[k], A.dx) + dot6(jb[k], B.dx);
-}
 
 __global__ void k_contact_jacobians(Dev d, uint32_t phase) {
     if (phase != 0 && d.ctr->impact == 0) return;
@@ -94,833 +38,6 @@ __global__ void k_contact_jacobians(Dev d, uint32_t phase) {
 void launch_contact_jacobians(const Dev& d, uint32_t phase, cudaStream_t s) {
     k_contact_jacobians<<<cap_blocks(d.cap_contact), kBlock, 0, s>>>(d, phase);
     note_launch(cap_blocks(d.cap_contact));
-}
-
-__device__ __forceinline__ void apply_pose_update(const Dev& d, uint32_t i, const V6& u) {
-    float4 l = d.dxl[i];
-    l.x += u.v[0];
-    l.y += u.v[1];
-    l.z += u.v[2];
-    d.dxl[i] = l;
-    V3 r{u.v[3], u.v[4], u.v[5]};
-    if (r.x == 0.0f && r.y == 0.0f && r.z == 0.0f) return;
-    Q4 rel = q4(d.dq[i]);
-    Q4 dd = qmul(Q4{r.x, r.y, r.z, 0.0f}, rel);
-    rel = qnormalize(Q4{rel.x + 0.5f * dd.x, rel.y + 0.5f * dd.y, rel.z + 0.5f * dd.z, rel.w + 0.5f * dd.w});
-    if (rel.w < 0.0f) rel = {-rel.x, -rel.y, -rel.z, -rel.w};
-    d.dq[i] = f4(rel);
-    d.dxa[i] = make_float4(2.0f * rel.x, 2.0f * rel.y, 2.0f * rel.z, 0.0f);
-}
-
-// Group-per-body primal: G lanes (G = 8, 16 or 32) solve one body. Lanes
-// evaluate the body's contact rows G at a time (coalesced SoA loads) and
-// stage them in shared memory; each lane owns ceil(27/G) of the 27 entries of
-// the packed 6x6 block (21 Hessian, 6 gradient) and adds the staged rows to
-// them in list order. Every entry thus sees exactly the additions, in exactly
-// the order, of the serial per-body loop of
-// geometry_constraints_solve.slang:339-400, whatever G is, and the block is
-// bit-identical to it; the LDL^T solve then runs in registers. The crossing
-// safeguard reuses the staged normal rows: its error term is the same
-// expression at the same displacements.
-//
-// G is chosen per colour: 8 lanes when the colour has more bodies than the
-// grid has 16-lane groups, else 16, or 32 when even 32-lane groups cover it.
-// The tail colours of a pile hold few but heavily loaded bodies (tens of
-// rows), and a colour ends when its slowest body does, so wider groups
-// there shorten the critical path.
-constexpr uint32_t kNormSlots = 32;
-template <int G> struct GroupRows {
-    // Chunk being accumulated: 3 rows of (jacobian[6], stiffness, force,
-    // stiffness x jacobian[6]); the last six are the Hessian products' first
-    // factors, formed once per row instead of once per entry.
-    float r[G][3][14];
-    float nrow[kNormSlots][8];  // normal row: jacobian[6], raw penalty, trial force
-    uint32_t flag[G];
-    Blk jblk;  // the block while joint rows are added (joint_rows_shared)
-};
-// Per-warp staging area: four 8-lane groups, two 16-lane groups or one
-// 32-lane group.
-constexpr size_t kWarpStage = 4 * sizeof(GroupRows<8>);
-static_assert(2 * sizeof(GroupRows<16>) <= kWarpStage && sizeof(GroupRows<32>) <= kWarpStage, "staging area");
-static_assert(32 * sizeof(Blk) <= kWarpStage, "a block slot per thread for the body-per-thread sweep");
-
-__device__ __forceinline__ void entry_ik(int e, int& i, int& k) {
-    i = e >= 15 ? 5 : e >= 10 ? 4 : e >= 6 ? 3 : e >= 3 ? 2 : e >= 1 ? 1 : 0;
-    k = e - i * (i + 1) / 2;
-}
-
-// Lane gl owns entries gl, gl+G, gl+2G, ... (those below 27).
-template <int G> struct Owned {
-    static constexpr int E = (27 + G - 1) / G;
-};
-template <int G>
-__device__ __forceinline__ void gather_block(const float* ent, Blk& blk, uint32_t gmask, int gbase) {
-#pragma unroll
-    for (int e = 0; e < 21; ++e) blk.h[e] = __shfl_sync(gmask, ent[e / G], gbase + (e % G));
-#pragma unroll
-    for (int r = 0; r < 6; ++r) blk.g[r] = __shfl_sync(gmask, ent[(21 + r) / G], gbase + ((21 + r) % G));
-}
-template <int G> __device__ __forceinline__ void own_entries(const Blk& blk, int gl, float* ent) {
-#pragma unroll
-    for (int m = 0; m < Owned<G>::E; ++m) {
-        const int e = gl + G * m;
-        float v = 0.0f;
-#pragma unroll
-        for (int q = 0; q < 21; ++q) v = e == q ? blk.h[q] : v;
-#pragma unroll
-        for (int r = 0; r < 6; ++r) v = e == 21 + r ? blk.g[r] : v;
-        ent[m] = v;
-    }
-}
-
-template <int G>
-__device__ __forceinline__ void accumulate_chunk(float* ent, int gl, const GroupRows<G>& sm, uint32_t m) {
-    // Products first (independent, pipelined loads), then the ordered adds.
-#pragma unroll
-    for (int q = 0; q < Owned<G>::E; ++q) {
-        const int e = gl + G * q;
-        if (e >= 27) continue;
-        int ei = 0, ek = 0;
-        const bool hess = e < 21;
-        if (hess) entry_ik(e, ei, ek);
-        else ei = e - 21;
-        if (G <= 8) {
-            float prod[G][3];
-#pragma unroll
-            for (int t = 0; t < G; ++t)
-#pragma unroll
-                for (int x = 0; x < 3; ++x) {
-                    const float* row = sm.r[t][x];
-                    prod[t][x] = hess ? row[8 + ei] * row[ek] : row[ei] * row[7];
-                }
-#pragma unroll
-            for (int t = 0; t < G; ++t)
-#pragma unroll
-                for (int x = 0; x < 3; ++x)
-                    if (t < int(m)) ent[q] += prod[t][x];
-        } else {
-            for (int t = 0; t < int(m); ++t)
-#pragma unroll
-                for (int x = 0; x < 3; ++x) {
-                    const float* row = sm.r[t][x];
-                    ent[q] += hess ? row[8 + ei] * row[ek] : row[ei] * row[7];
-                }
-        }
-    }
-}
-
-template <int G>
-__device__ __forceinline__ void accumulate_crossing(float* ent, int gl, const GroupRows<G>& sm, uint32_t s0,
-                                                    uint32_t m) {
-#pragma unroll
-    for (int q = 0; q < Owned<G>::E; ++q) {
-        const int e = gl + G * q;
-        if (e >= 27) continue;
-        int ei = 0, ek = 0;
-        if (e < 21) entry_ik(e, ei, ek);
-        for (uint32_t t = 0; t < m; ++t) {
-            if (!sm.flag[t]) continue;
-            const float* row = sm.nrow[(s0 + t) % kNormSlots];
-            if (e < 21) ent[q] += row[6] * row[ei] * row[ek];
-            else ent[q] += row[e - 21] * row[7];
-        }
-    }
-}
-
-// Rows of one contact for body i into chunk slot `slot`; its normal row,
-// raw penalty and normal trial also go to nrow[nslot].
-template <int G>
-__device__ __forceinline__ void stage_contact(const Dev& d, const Lite& me, float my_friction, uint32_t code,
-                                              uint32_t other_body, uint32_t phase, float dt, GroupRows<G>& sm,
-                                              int slot, int nslot) {
-    const uint32_t c = code & 0x7fffffffu;
-    const bool first = (code >> 31) == 0;
-    const Lite other = load_lite(d, other_body);
-    const Lite A = first ? me : other;  // values, not run-time references (no local copies)
-    const Lite B = first ? other : me;
-    const float of = d.p1[other_body].x;
-    const float friction = sqrtf(first ? my_friction * of : of * my_friction);
-    const float4 lam = d.c_lam[c], pen = d.c_pen[c];
-    V6 ja[3], jb[3];
-    float err[3];
-    contact_rows(d, c, d.c_e[c], A, B, ja, jb, err);
-    F3 trial{lam.x + pen.x * err[0], lam.y + pen.y * err[1], lam.z + pen.z * err[2]};
-    if (nslot >= 0) {
-#pragma unroll
-        for (int k = 0; k < 6; ++k) sm.nrow[nslot][k] = first ? ja[0].v[k] : jb[0].v[k];
-        sm.nrow[nslot][6] = pen.x;
-        sm.nrow[nslot][7] = trial.n;
-    }
-    if (slot < 0) return;
-    F3 f = project_contact(trial, friction);
-    F3 sc = stiffness_scales(trial, friction);
-    float forces[3] = {f.n, f.t0, f.t1};
-    if (phase != 0) {
-        V3 t0, t1;
-        basis(v3(d.c_n[c]), t0, t1);
-        const V3 af = v3(d.c_accf[c]);
-        forces[0] = f.n - lam.w / dt;
-        forces[1] = f.t0 - dot(af, t0) / dt;
-        forces[2] = f.t1 - dot(af, t1) / dt;
-    }
-    const float st[3] = {pen.x * sc.n, pen.y * sc.t0, pen.z * sc.t1};
-#pragma unroll
-    for (int x = 0; x < 3; ++x) {
-        // Values selected element by element: a reference chosen at run time
-        // between the two arrays would give them addresses (local memory).
-        V6 row;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) row.v[k] = first ? ja[x].v[k] : jb[x].v[k];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) sm.r[slot][x][k] = row.v[k];
-        sm.r[slot][x][6] = st[x];
-        sm.r[slot][x][7] = forces[x];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) sm.r[slot][x][8 + k] = st[x] * row.v[k];  // = (stiffness x J_i), as before
-    }
-}
-
-// Joint rows of body i added to its block (geometry_constraints_solve.slang:
-// 381-400, the serial loop's order). The joint visit takes the block's
-// address, so lane 0 works on a copy in the group's shared-memory slot `sb`
-// and the group reads the result back: the register block never needs an
-// address (which would put it in local memory for every body).
-template <int G>
-__device__ __forceinline__ void joint_rows_shared(const Dev& d, uint32_t i, uint32_t phase, float dt, Blk& blk,
-                                                  Blk* sb, uint32_t gmask, int gl) {
-    if (gl == 0) {
-        *sb = blk;
-        const uint32_t jcnt = d.jdeg[i], jlo = d.jinc_off[i];
-        for (uint32_t k = 0; k < jcnt; ++k) {
-            const uint32_t j = d.jinc_list[jlo + k];
-            const JointState js = d.jstate[j];
-            if (!js.enabled) continue;
-            const uint32_t a = js.dense_a, b = js.dense_b;
-            const bool first = i == a;
-            if (phase == 0) {
-                BodyView A = load_body(d, a), B = load_body(d, b);
-                visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]),
-                            q4(d.q[b]), d.p0[a], d.p0[b], dt, sb, first, kVisitAccumulate, nullptr);
-            } else {
-                const Lite A = load_lite(d, a), B = load_lite(d, b);
-                for (uint32_t r = 0; r < js.count; ++r) {
-                    Row row = load_row(d.jrows[size_t(j) * 18 + r]);
-                    if (row.stiffness >= kMaxPenalty) row_accumulate(*sb, row, first, A.dx, B.dx, dt);
-                }
-            }
-        }
-    }
-    __syncwarp(gmask);
-    blk = *sb;
-    __syncwarp(gmask);
-}
-
-__device__ __forceinline__ unsigned long long gtimer() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-template <int G>
-__device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float dt, GroupRows<G>& sm,
-                                 uint32_t gmask, int gl, int gbase, uint32_t trace = 0) {
-    // trace 1: slowest body of the colour per stage; 2: stage times summed
-    // over the colour's bodies (profiling only).
-    const unsigned long long t0 = trace ? gtimer() : 0ull;
-    auto mark = [&](int k) {
-        if (trace == 1 && gl == 0) atomicMax(&d.ctr->dbg_body[k], gtimer() - t0);
-        if (trace == 2 && gl == 0) atomicAdd(&d.ctr->dbg_sum[k], gtimer() - t0);
-    };
-    const Lite me = load_lite(d, i);
-    const float my_friction = d.p1[i].x;
-    const uint32_t ro = d.roff[i], rn = d.rcount[i];
-    float ent[Owned<G>::E];
-    {
-        const float4 ia = d.inA[i], ib = d.inB[i];
-        float H[21];
-#pragma unroll
-        for (int k = 0; k < 21; ++k) H[k] = 0.0f;
-        H[bidx(0, 0)] = ia.x;
-        H[bidx(1, 1)] = ia.x;
-        H[bidx(2, 2)] = ia.x;
-        H[bidx(3, 3)] = ia.y;
-        H[bidx(4, 3)] = ia.z;
-        H[bidx(5, 3)] = ib.x;
-        H[bidx(4, 4)] = ia.w;
-        H[bidx(5, 4)] = ib.y;
-        H[bidx(5, 5)] = ib.z;
-#pragma unroll
-        for (int q = 0; q < Owned<G>::E; ++q) {
-            const int e = gl + G * q;
-            float v = 0.0f;
-#pragma unroll
-            for (int k = 0; k < 21; ++k) v = e == k ? H[k] : v;
-            if (e >= 21 && e < 27) {
-                const int r = e - 21;
-                float gs = 0.0f;
-#pragma unroll
-                for (int c = 0; c < 6; ++c) gs += H[bidx(r, c)] * me.dx.v[c];
-                v = gs;
-            }
-            ent[q] = v;
-        }
-    }
-    for (uint32_t base = 0; base < rn; base += G) {
-        const uint32_t sidx = base + gl;
-        if (sidx < rn)
-            stage_contact<G>(d, me, my_friction, d.blist[ro + sidx], d.bother[ro + sidx], phase, dt, sm, gl,
-                             sidx < kNormSlots ? int(sidx) : -1);
-        __syncwarp(gmask);
-        accumulate_chunk<G>(ent, gl, sm, min(uint32_t(G), rn - base));
-        __syncwarp(gmask);
-    }
-    mark(0);
-    Blk blk;
-    gather_block<G>(ent, blk, gmask, gbase);
-    mark(1);
-    const uint32_t jcnt = d.jdeg[i];
-    if (jcnt) joint_rows_shared<G>(d, i, phase, dt, blk, &sm.jblk, gmask, gl);
-    V6 upd;
-    if (!block_solve(blk, upd)) return;
-    mark(2);
-    // Crossing safeguard (geometry_constraints_solve.slang:433-475).
-    own_entries<G>(blk, gl, ent);
-    bool crossing = false;
-    for (uint32_t base = 0; base < rn; base += G) {
-        const uint32_t sidx = base + gl;
-        if (rn > kNormSlots && base >= kNormSlots && sidx < rn)
-            stage_contact<G>(d, me, my_friction, d.blist[ro + sidx], d.bother[ro + sidx], phase, dt, sm, -1,
-                             int(sidx % kNormSlots));
-        __syncwarp(gmask);
-        uint32_t flag = 0;
-        if (sidx < rn) {
-            const float* row = sm.nrow[sidx % kNormSlots];
-            V6 nr;
-#pragma unroll
-            for (int k = 0; k < 6; ++k) nr.v[k] = row[k];
-            const float k0 = row[6], trial = row[7];
-            flag = (trial <= 0.0f && trial + k0 * dot6(nr, upd) > k0 * 1.0e-6f) ? 1u : 0u;
-        }
-        sm.flag[gl] = flag;
-        __syncwarp(gmask);
-        if (__any_sync(gmask, flag)) {
-            crossing = true;
-            accumulate_crossing<G>(ent, gl, sm, base % kNormSlots, min(uint32_t(G), rn - base));
-        }
-        __syncwarp(gmask);
-    }
-    mark(3);
-    if (crossing) {
-        gather_block<G>(ent, blk, gmask, gbase);
-        V6 safe;
-        if (block_solve(blk, safe)) upd = safe;
-    }
-    mark(4);
-    if (trace == 1 && gl == 0) atomicMax(&d.ctr->dbg_rn, rn);
-    if (trace == 2 && gl == 0) {
-        atomicAdd(&d.ctr->dbg_sum[6], 1ull);
-        atomicAdd(&d.ctr->dbg_sum[7], (unsigned long long)rn);
-    }
-    if (gl == 0) {
-        if (phase == 0) {
-            apply_pose_update(d, i, upd);
-        } else {
-            float4 l = d.dxl[i], a = d.dxa[i];
-            l.x += upd.v[0];
-            l.y += upd.v[1];
-            l.z += upd.v[2];
-            a.x += upd.v[3];
-            a.y += upd.v[4];
-            a.z += upd.v[5];
-            d.dxl[i] = l;
-            d.dxa[i] = a;
-        }
-    }
-}
-
-// One thread solves body i: the serial loop of geometry_constraints_solve.
-// slang:339-475 as written -- add_row per contact row in list order, the
-// joints' rows, LDL^T, then the crossing safeguard over the normal rows --
-// for colours with far more bodies than the grid has lane groups, where a
-// body per thread finishes the colour in fewer rounds than wider groups.
-// `sb`: this thread's shared-memory block slot for the joint visit.
-__device__ __forceinline__ void load_normal_rows(const Dev& d, uint32_t c, V6& ja, V6& jb) {
-    const float4* p = d.c_jac + size_t(c) * 9;
-    const float4 a0 = p[0], a1 = p[1], b4 = p[4], b5 = p[5];  // floats 0-7 and 16-23
-    ja = {{a0.x, a0.y, a0.z, a0.w, a1.x, a1.y}};
-    jb = {{b4.z, b4.w, b5.x, b5.y, b5.z, b5.w}};
-}
-__device__ void solve_body_thread(const Dev& d, uint32_t i, uint32_t phase, float dt, Blk* sb) {
-    const Lite me = load_lite(d, i);
-    const float my_friction = d.p1[i].x;
-    const uint32_t ro = d.roff[i], rn = d.rcount[i];
-    Blk blk;
-    {
-        const float4 ia = d.inA[i], ib = d.inB[i];
-#pragma unroll
-        for (int k = 0; k < 21; ++k) blk.h[k] = 0.0f;
-        blk.h[bidx(0, 0)] = ia.x;
-        blk.h[bidx(1, 1)] = ia.x;
-        blk.h[bidx(2, 2)] = ia.x;
-        blk.h[bidx(3, 3)] = ia.y;
-        blk.h[bidx(4, 3)] = ia.z;
-        blk.h[bidx(5, 3)] = ib.x;
-        blk.h[bidx(4, 4)] = ia.w;
-        blk.h[bidx(5, 4)] = ib.y;
-        blk.h[bidx(5, 5)] = ib.z;
-#pragma unroll
-        for (int r = 0; r < 6; ++r) {
-            float gs = 0.0f;
-#pragma unroll
-            for (int c = 0; c < 6; ++c) gs += blk.h[bidx(r, c)] * me.dx.v[c];
-            blk.g[r] = gs;
-        }
-    }
-    for (uint32_t r = 0; r < rn; ++r) {
-        const uint32_t code = d.blist[ro + r], other_body = d.bother[ro + r];
-        const uint32_t c = code & 0x7fffffffu;
-        const bool first = (code >> 31) == 0;
-        const Lite other = load_lite(d, other_body);
-        const Lite A = first ? me : other, B = first ? other : me;
-        const float of = d.p1[other_body].x;
-        const float friction = sqrtf(first ? my_friction * of : of * my_friction);
-        const float4 lam = d.c_lam[c], pen = d.c_pen[c];
-        V6 ja[3], jb[3];
-        float err[3];
-        contact_rows(d, c, d.c_e[c], A, B, ja, jb, err);
-        const F3 trial{lam.x + pen.x * err[0], lam.y + pen.y * err[1], lam.z + pen.z * err[2]};
-        const F3 f = project_contact(trial, friction);
-        const F3 sc = stiffness_scales(trial, friction);
-        float forces[3] = {f.n, f.t0, f.t1};
-        if (phase != 0) {
-            V3 t0, t1;
-            basis(v3(d.c_n[c]), t0, t1);
-            const V3 af = v3(d.c_accf[c]);
-            forces[0] = f.n - lam.w / dt;
-            forces[1] = f.t0 - dot(af, t0) / dt;
-            forces[2] = f.t1 - dot(af, t1) / dt;
-        }
-        const float st[3] = {pen.x * sc.n, pen.y * sc.t0, pen.z * sc.t1};
-#pragma unroll
-        for (int x = 0; x < 3; ++x) {
-            V6 row;
-#pragma unroll
-            for (int k = 0; k < 6; ++k) row.v[k] = first ? ja[x].v[k] : jb[x].v[k];
-            add_row(blk, row, st[x], forces[x]);
-        }
-    }
-    if (d.jdeg[i]) {
-        // The joint visit takes the block's address: work on this thread's
-        // shared-memory copy so the register block never needs one.
-        *sb = blk;
-        const uint32_t jcnt = d.jdeg[i], jlo = d.jinc_off[i];
-        for (uint32_t k = 0; k < jcnt; ++k) {
-            const uint32_t j = d.jinc_list[jlo + k];
-            const JointState js = d.jstate[j];
-            if (!js.enabled) continue;
-            const uint32_t a = js.dense_a, b = js.dense_b;
-            const bool first = i == a;
-            if (phase == 0) {
-                BodyView A = load_body(d, a), B = load_body(d, b);
-                visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]),
-                            q4(d.q[b]), d.p0[a], d.p0[b], dt, sb, first, kVisitAccumulate, nullptr);
-            } else {
-                const Lite A = load_lite(d, a), B = load_lite(d, b);
-                for (uint32_t r = 0; r < js.count; ++r) {
-                    Row row = load_row(d.jrows[size_t(j) * 18 + r]);
-                    if (row.stiffness >= kMaxPenalty) row_accumulate(*sb, row, first, A.dx, B.dx, dt);
-                }
-            }
-        }
-        blk = *sb;
-    }
-    V6 upd;
-    if (!block_solve(blk, upd)) return;
-    // Crossing safeguard: the normal rows again, at the same displacements.
-    bool crossing = false;
-    for (uint32_t r = 0; r < rn; ++r) {
-        const uint32_t code = d.blist[ro + r], other_body = d.bother[ro + r];
-        const uint32_t c = code & 0x7fffffffu;
-        const bool first = (code >> 31) == 0;
-        const Lite other = load_lite(d, other_body);
-        const Lite A = first ? me : other, B = first ? other : me;
-        V6 ja, jb;
-        load_normal_rows(d, c, ja, jb);
-        const float err0 = d.c_e[c].x + dot6(ja, A.dx) + dot6(jb, B.dx);
-        const float k0 = d.c_pen[c].x;
-        const float trial = d.c_lam[c].x + k0 * err0;
-        V6 nr;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) nr.v[k] = first ? ja.v[k] : jb.v[k];
-        if (trial <= 0.0f && trial + k0 * dot6(nr, upd) > k0 * 1.0e-6f) {
-            add_row(blk, nr, k0, trial);
-            crossing = true;
-        }
-    }
-    if (crossing) {
-        V6 safe;
-        if (block_solve(blk, safe)) upd = safe;
-    }
-    if (phase == 0) {
-        apply_pose_update(d, i, upd);
-    } else {
-        float4 l = d.dxl[i], a = d.dxa[i];
-        l.x += upd.v[0];
-        l.y += upd.v[1];
-        l.z += upd.v[2];
-        a.x += upd.v[3];
-        a.y += upd.v[4];
-        a.z += upd.v[5];
-        d.dxl[i] = l;
-        d.dxa[i] = a;
-    }
-}
-
-// Residual accumulator of one dual pass (this build's addition): rows that
-// carry force or penetrate contribute |C_n| (force > 0) or C_n (penetration
-// only); hard joint rows contribute |C|. Reported as the RMS, the largest
-// value, and the number of rows above the schedule's tolerance.
-struct Res {
-    double sq;
-    uint32_t n;
-    float mx;
-    uint32_t over;
-    float tol;
-};
-__device__ __forceinline__ void res_add(Res& r, float v) {
-    r.sq += double(v) * double(v);
-    r.n += 1;
-    r.mx = fmx(r.mx, v);
-    if (v > r.tol) r.over += 1;
-}
-
-// advance_duals for one contact point (geometry_constraints_solve.slang:
-// 494-532; the last-iteration block runs in k_contact_finalize).
-__device__ void dual_contact(const Dev& d, uint32_t c, float dt, uint32_t phase, Res& res, uint32_t it) {
-    const uint2 ab = d.c_bodies[c];
-    const uint32_t a = ab.x, b = ab.y;
-    if (phase != 0 && d.impact[a] == 0 && d.impact[b] == 0) return;
-    // Batched worlds: a scene past its budget is finished; its last sweep
-    // feeds the scene's residual.
-    uint32_t scene = 0;
-    bool scene_last = false;
-    if (batched(d)) {
-        scene = d.scene_of[a];
-        const uint32_t budget = d.scene_budget[scene];
-        if (it >= budget) return;
-        scene_last = phase == 0 && it + 1 == budget;  // the tick's residual is the pose phase's
-    }
-    const Lite A = load_lite(d, a), B = load_lite(d, b);
-    const float friction = sqrtf(d.p1[a].x * d.p1[b].x);
-    const float beta = (1.0f / (fmx(d.p0[a].x + d.p0[b].x, 1.0e-6f) * dt * dt)) * 100.0f;
-    float4 lam = d.c_lam[c], pen = d.c_pen[c];
-    V6 ja[3], jb[3];
-    float err[3];
-    contact_rows(d, c, d.c_e[c], A, B, ja, jb, err);
-    F3 f = project_contact(F3{lam.x + pen.x * err[0], lam.y + pen.y * err[1], lam.z + pen.z * err[2]}, friction);
-    const float tx = lam.y + pen.y * err[1];
-    const float ty = lam.z + pen.z * err[2];
-    const float bound = friction * f.n;
-    const bool stick = tx * tx + ty * ty <= bound * bound;
-    lam.x = f.n;
-    lam.y = f.t0;
-    lam.z = f.t1;
-    if (f.n > 0.0f) pen.x = fmn(kMaxPenalty, pen.x + beta * fab(err[0]));
-    if (stick) {
-        pen.y = fmn(kMaxPenalty, pen.y + beta * fab(err[1]));
-        pen.z = fmn(kMaxPenalty, pen.z + beta * fab(err[2]));
-    }
-    pen.w = stick ? 1.0f : 0.0f;
-    d.c_lam[c] = lam;
-    d.c_pen[c] = pen;
-    if (f.n > 0.0f || err[0] > 0.0f) {
-        const float v = f.n > 0.0f ? fab(err[0]) : err[0];
-        res_add(res, v);
-        if (scene_last) {
-            atomicAdd(&d.scene_res_sq[scene], v * v);
-            atomicAdd(&d.scene_res_n[scene], 1u);
-            atomicMax(reinterpret_cast<int*>(&d.scene_res_mx[scene]), __float_as_int(v));
-        }
-    }
-}
-
-__device__ void dual_joint(const Dev& d, uint32_t j, uint32_t phase, float dt, Res& res, uint32_t it) {
-    JointState js = d.jstate[j];
-    if (js.count == 0 || !js.enabled) return;
-    const uint32_t a = js.dense_a, b = js.dense_b;
-    if (phase != 0 && d.impact[a] == 0 && d.impact[b] == 0) return;
-    uint32_t scene = 0;
-    bool scene_last = false;
-    if (batched(d)) {
-        scene = d.scene_of[a];
-        const uint32_t budget = d.scene_budget[scene];
-        if (it >= budget) return;
-        scene_last = it + 1 == budget;
-    }
-    float impulse = 0.0f;
-    if (phase == 0) {
-        BodyView A = load_body(d, a), B = load_body(d, b);
-        Blk scratch;
-        // A batched world also needs this joint's own residual for its scene.
-        Res jr{0.0, 0u, 0.0f, 0u, res.tol};
-        Res& sink = batched(d) ? jr : res;
-        impulse = visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]),
-                              q4(d.q[b]), d.p0[a], d.p0[b], dt, &scratch, true, kVisitAdvance, nullptr, &sink.sq,
-                              &sink.n, &sink.mx, &sink.over, sink.tol);
-        if (batched(d)) {
-            res.sq += jr.sq;
-            res.n += jr.n;
-            res.mx = fmx(res.mx, jr.mx);
-            res.over += jr.over;
-        }
-        if (scene_last && jr.n) {
-            atomicAdd(&d.scene_res_sq[scene], float(jr.sq));
-            atomicAdd(&d.scene_res_n[scene], jr.n);
-            atomicMax(reinterpret_cast<int*>(&d.scene_res_mx[scene]), __float_as_int(fmx(jr.mx, 0.0f)));
-        }
-    } else {
-        const Lite A = load_lite(d, a), B = load_lite(d, b);
-        for (uint32_t r = 0; r < js.count; ++r) {
-            JointRow& s = d.jrows[size_t(j) * 18 + r];
-            Row row = load_row(s);
-            impulse += fab(row.stiffness < kMaxPenalty ? row.reference_force : row_force(row, A.dx, B.dx, dt)) * dt;
-            if (row.stiffness >= kMaxPenalty) store_row(s, row_advance(row, A.dx, B.dx));
-        }
-    }
-    js.applied = impulse;
-    const float thr = d.joints[j].breaking_threshold;
-    if (thr > 0.0f && impulse > thr) {
-        js.broken = 1;
-        js.enabled = 0;
-    }
-    d.jstate[j] = js;
-}
-
-// One block's residual partials into slot `slot` of the counters: warp
-// trees, then warps in order (deterministic).
-template <int T>
-__device__ __forceinline__ void block_residual(Res res, double* wsq, uint32_t* wn, float* wmx, uint32_t* wov,
-                                               Counters* c, uint32_t slot) {
-    for (int o = 16; o > 0; o >>= 1) {
-        res.sq += __shfl_xor_sync(0xffffffffu, res.sq, o);
-        res.n += __shfl_xor_sync(0xffffffffu, res.n, o);
-        res.mx = fmx(res.mx, __shfl_xor_sync(0xffffffffu, res.mx, o));
-        res.over += __shfl_xor_sync(0xffffffffu, res.over, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        wsq[threadIdx.x >> 5] = res.sq;
-        wn[threadIdx.x >> 5] = res.n;
-        wmx[threadIdx.x >> 5] = res.mx;
-        wov[threadIdx.x >> 5] = res.over;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double bs = 0.0;
-        uint32_t bn = 0, bo = 0;
-        float bm = 0.0f;
-        for (int k = 0; k < T / 32; ++k) {
-            bs += wsq[k];
-            bn += wn[k];
-            bm = fmx(bm, wmx[k]);
-            bo += wov[k];
-        }
-        c->res_sum[slot] = bs;
-        c->res_cnt[slot] = bn;
-        c->res_mx[slot] = bm;
-        c->res_over[slot] = bo;
-    }
-}
-
-// The sweep's residual from every block's partials (slots base .. base +
-// gridDim.x): RMS, largest row violation, fraction of rows above the
-// tolerance, and whether the schedule's measure meets the tolerance
-// (residual_norm 0: every row within it; 1: the RMS; 2: at most one row in a
-// thousand above it).
-struct SweepResidual {
-    float rms, mx, over, measure;
-    bool met;
-};
-__device__ __forceinline__ SweepResidual sweep_residual(Counters* c, uint32_t base, const StepParams& sp) {
-    double tsq = 0.0;
-    uint32_t tn = 0, to = 0;
-    float tmx = 0.0f;
-    for (uint32_t k = 0; k < gridDim.x; ++k) {
-        tsq += ((volatile double*)c->res_sum)[base + k];
-        tn += ((volatile uint32_t*)c->res_cnt)[base + k];
-        tmx = fmx(tmx, ((volatile float*)c->res_mx)[base + k]);
-        to += ((volatile uint32_t*)c->res_over)[base + k];
-    }
-    SweepResidual r;
-    r.rms = tn ? float(sqrt(tsq / double(tn))) : 0.0f;
-    r.mx = tmx;
-    r.over = tn ? float(to) / float(tn) : 0.0f;
-    if (sp.residual_norm == 1) {
-        r.measure = r.rms;
-        r.met = r.rms <= sp.tolerance;
-    } else if (sp.residual_norm == 2) {
-        r.measure = r.over;
-        r.met = uint64_t(to) * 1000u <= uint64_t(tn);
-    } else {
-        r.measure = tmx;
-        r.met = tmx <= sp.tolerance;
-    }
-    return r;
-}
-
-__device__ __forceinline__ void atomic_max_pos(float* addr, float v) {
-    atomicMax(reinterpret_cast<int*>(addr), __float_as_int(fmx(v, 0.0f)));
-}
-
-// T threads per CTA, one CTA per SM (cooperative): 512 threads cap a thread
-// at 128 registers, 384 at 168, 256 at 255 -- fewer resident warps against
-// fewer spills; the world picks one (pmb_world_autotune). Timed: the
-// profiling build (pmb_world_profile_step), which records per-colour
-// timestamps of the first sweep; the ticks run the untimed build.
-template <int T, bool Timed>
-__global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t phase) {
-    constexpr int kSolveThreads = T;
-    Counters* c = d.ctr;
-    if (phase != 0 && c->impact == 0) return;
-    if (c->status & kStBarrierTimeout) return;  // the tick was abandoned
-    extern __shared__ __align__(16) uint8_t stage_raw[];
-    const int lane = threadIdx.x & 31;
-    uint8_t* warp_stage = stage_raw + (threadIdx.x >> 5) * kWarpStage;
-    const uint32_t nthreads = gridDim.x * kSolveThreads;
-    const float dt = sp.dt;
-    const uint32_t colors = c->colors;
-    uint32_t budget = sp.budget_request;
-    if (!sp.realtime && sp.requested == 0) budget = max(budget, c->joint_iters);
-    if (phase != 0 && sp.tolerance > 0.0f) budget = c->budget;
-    // Batched worlds sweep every scene its own budget (no residual-driven stop).
-    const bool adaptive = phase == 0 && sp.tolerance > 0.0f && !batched(d);
-    const uint32_t iters = batched(d) ? min(c->budget_max, kMaxIterations)
-                                      : adaptive ? min(max(sp.max_iterations, 1u), kMaxIterations)
-                                                 : min(budget, kMaxIterations);
-    const uint32_t n_con = c->n_contacts;
-    __shared__ double wsq[kSolveThreads / 32];
-    __shared__ uint32_t wn[kSolveThreads / 32], wov[kSolveThreads / 32];
-    __shared__ float wmx[kSolveThreads / 32];
-    const bool timing = Timed && phase == 0;
-    auto now = [] {
-        unsigned long long t;
-        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-        return t;
-    };
-    if (timing && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_start = now();
-    for (uint32_t it = 0; it < iters; ++it) {
-        for (uint32_t col = 0; col < colors; ++col) {
-            const uint32_t* off = c->color_off + col * kWidthClasses;
-            const uint32_t b0 = off[0], b1 = off[kWidthClasses];
-            const uint32_t nb = b1 - b0;
-            const uint32_t trace = !timing || it != 0 ? 0u : col + 1 == colors ? 1u : col == 0 ? 2u : 0u;
-            // Bodies [lo, hi) with G lanes each. Consecutive bodies go to
-            // consecutive CTAs (group rank = local group x grid + CTA), so the
-            // heavy bodies at the front of a colour spread over all SMs.
-            // Policy 3 hands the bodies out dynamically instead: each group
-            // takes the next unclaimed body of the colour from a counter
-            // (claiming its following one while it solves), so groups that
-            // drew light bodies take more of them.
-            const uint32_t step = it * colors + col;
-            uint32_t* claim = &c->claim[step & 1u];
-            if (d.solve_policy == 3 && blockIdx.x == 0 && threadIdx.x == 0) c->claim[(step + 1u) & 1u] = 0u;
-            auto sweep = [&](auto width, uint32_t lo, uint32_t hi) {
-                constexpr int G = decltype(width)::value;
-                if (lo >= hi) return;
-                const int gl = lane % G, gbase = lane - gl;
-                const uint32_t gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << gbase;
-                GroupRows<G>& sm = reinterpret_cast<GroupRows<G>*>(warp_stage)[gbase / G];
-                auto body = [&](uint32_t k) {
-                    const uint32_t i = d.corder[k];
-                    if (phase != 0 && d.impact[i] == 0) return;
-                    if (batched(d) && it >= d.scene_budget[d.scene_of[i]]) return;
-                    solve_body_group<G>(d, i, phase, dt, sm, gmask, gl, gbase, trace);
-                };
-                // One call site of the body solve for both assignments (each
-                // inlined copy adds its own stack frame).
-                const bool dynamic = d.solve_policy == 3;
-                const uint32_t groups = nthreads / G;
-                uint32_t k = lo + (threadIdx.x / G) * gridDim.x + blockIdx.x;
-                if (dynamic) {
-                    uint32_t t = 0;
-                    if (gl == 0) t = atomicAdd(claim, 1u);
-                    k = lo + __shfl_sync(gmask, t, gbase);
-                }
-                while (k < hi) {
-                    uint32_t next = 0;
-                    if (dynamic && gl == 0) next = atomicAdd(claim, 1u);
-                    body(k);
-                    if (dynamic) k = lo + __shfl_sync(gmask, next, gbase);
-                    else k += groups;
-                }
-                __syncwarp();
-            };
-            using W32 = std::integral_constant<int, 32>;
-            using W16 = std::integral_constant<int, 16>;
-            using W8 = std::integral_constant<int, 8>;
-            // Widths (see the group-per-body comment): policy 0 (and 3) one
-            // width per colour by its size, 1 eight lanes, 2 a width per body
-            // class (heaviest first) unless 32-lane groups cover the colour.
-            uint32_t r32 = b0, r16 = b0, r8 = b0;  // 32 lanes [b0, r32), 16 [r32, r16), 8 [r16, r8)
-            if (d.solve_policy == 4 && nb * 16u > nthreads) {
-                // A body per thread: the colour has more bodies than 16-lane
-                // groups could take in one round. Consecutive bodies go to
-                // consecutive CTAs, as for the groups.
-                Blk* slot = reinterpret_cast<Blk*>(warp_stage) + lane;
-                for (uint32_t k = b0 + threadIdx.x * gridDim.x + blockIdx.x; k < b1; k += nthreads) {
-                    const uint32_t i = d.corder[k];
-                    if (phase != 0 && d.impact[i] == 0) continue;
-                    if (batched(d) && it >= d.scene_budget[d.scene_of[i]]) continue;
-                    solve_body_thread(d, i, phase, dt, slot);
-                }
-                r32 = r16 = r8 = b0;
-            } else if (d.solve_policy != 1 && nb * 32u <= nthreads) {
-                r32 = r16 = r8 = b1;
-            } else if (d.solve_policy == 2) {
-                r32 = off[1];
-                r16 = off[2];
-                r8 = b1;
-            } else if ((d.solve_policy == 0 || d.solve_policy >= 3) && nb * 16u <= nthreads) {
-                r16 = r8 = b1;
-            } else {
-                r8 = b1;
-            }
-            sweep(W32{}, b0, r32);
-            sweep(W16{}, r32, r16);
-            sweep(W8{}, r16, r8);
-            if (timing && it == 0 && col < 18) {
-                __syncthreads();
-                if (threadIdx.x == 0) atomicMax(&c->dbg_work[col], now());
-            }
-            if (!grid_sync(c, d.barrier_spins)) return;
-            if (timing && it == 0 && col < 18 && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_release[col] = now();
-        }
-        Res res{0.0, 0u, 0.0f, 0u, sp.tolerance};
-        for (uint32_t k = grid_stride_begin(); k < n_con; k += grid_stride()) dual_contact(d, k, dt, phase, res, it);
-        for (uint32_t j = grid_stride_begin(); j < d.nj; j += grid_stride()) dual_joint(d, j, phase, dt, res, it);
-        // Deterministic reduction: warp tree, warps in order, blocks in order.
-        block_residual<kSolveThreads>(res, wsq, wn, wmx, wov, c, blockIdx.x);
-        if (timing && it == 0 && threadIdx.x == 0) atomicMax(&c->dbg_work[19], now());
-        if (!grid_sync(c, d.barrier_spins)) return;
-        if (timing && it == 0 && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_release[19] = now();
-        const SweepResidual sw = sweep_residual(c, 0u, sp);
-        if (phase == 0 && grid_stride_begin() == 0) c->residual_trace[it] = sw.measure;
-        bool last = it + 1 == iters;
-        if (adaptive && sw.met) last = true;
-        // Every block has read the partials before the next pass rewrites them.
-        if (!last && colors == 0 && !grid_sync(c, d.barrier_spins)) return;
-        if (last) {
-            if (grid_stride_begin() == 0) {
-                c->claim[0] = c->claim[1] = 0u;  // every block is past its last claim
-                if (phase == 0) {
-                    c->iterations = it + 1;
-                    c->residual = sw.rms;
-                    c->residual_max = sw.mx;
-                    c->residual_over = sw.over;
-                }
-                c->budget = it + 1;
-            }
-            return;
-        }
-    }
 }
 
 // ------------------------------------------------------------ staged solve
@@ -1408,7 +525,7 @@ __global__ void __launch_bounds__(T, 1) k_solve_staged(Dev d, StepParams sp, uin
                             const uint32_t i = tb.body[0];
                             if (!tb.skip[0]) {
                                 GroupRows<32>& sm = *reinterpret_cast<GroupRows<32>*>(tb.rows);
-                                solve_body_group<32>(d, i, phase, dt, sm, 0xffffffffu, lane, 0, 0u);
+                                solve_body_group<32, true>(d, i, phase, dt, sm, 0xffffffffu, lane, 0, 0u);
                                 __syncwarp();
                                 owned_contact_duals(d, i, col, dt, phase, res, it, lane, 32);
                                 __syncwarp();
@@ -1499,18 +616,27 @@ __global__ void __launch_bounds__(T, 1) k_solve_staged(Dev d, StepParams sp, uin
     }
 }
 
-const SolveVariant solve_variants[kSolveVariants] = {
-    {reinterpret_cast<const void*>(&k_solve<512, false>), reinterpret_cast<const void*>(&k_solve<512, true>), 512,
-     kWarpStage * (512 / 32)},
-    {reinterpret_cast<const void*>(&k_solve<384, false>), reinterpret_cast<const void*>(&k_solve<384, true>), 384,
-     kWarpStage * (384 / 32)},
-    {reinterpret_cast<const void*>(&k_solve<256, false>), reinterpret_cast<const void*>(&k_solve<256, true>), 256,
-     kWarpStage * (256 / 32)},
-    {reinterpret_cast<const void*>(&k_solve_staged<512, false>),
-     reinterpret_cast<const void*>(&k_solve_staged<512, true>), 512, kStagedSmem},
-    {reinterpret_cast<const void*>(&k_solve_staged<384, false>),
-     reinterpret_cast<const void*>(&k_solve_staged<384, true>), 384, kStagedSmem},
-};
+// The staged solve has one build for every feature set.
+template <int T, bool Timed>
+static void staged_builds(const void* (&out)[kSolveFeatures]) {
+    for (int f = 0; f < kSolveFeatures; ++f) out[f] = reinterpret_cast<const void*>(&k_solve_staged<T, Timed>);
+}
+template <int T>
+static SolveVariant staged_variant() {
+    SolveVariant v{};
+    staged_builds<T, false>(v.ptr);
+    staged_builds<T, true>(v.timed);
+    v.threads = T;
+    v.smem = kStagedSmem;
+    return v;
+}
+
+const SolveVariant& solve_variant(uint32_t v) {
+    static const SolveVariant table[kSolveVariants] = {solve_group_variant_512(), solve_group_variant_384(),
+                                                       solve_group_variant_256(), staged_variant<512>(),
+                                                       staged_variant<384>()};
+    return table[v < kSolveVariants ? v : 0];
+}
 
 // Last-iteration contact work (geometry_constraints_solve.slang:533-561),
 // one thread per contact point.
@@ -1831,8 +957,9 @@ __global__ void k_contact_events(Dev d) {
 
 void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, const int* coop_blocks,
                       const SolveBuffers& o) {
-    const SolveVariant& sv = solve_variants[d.solve_variant < kSolveVariants ? d.solve_variant : 0];
+    const SolveVariant& sv = solve_variant(d.solve_variant);
     const int coop = coop_blocks[d.solve_variant < kSolveVariants ? d.solve_variant : 0];
+    const int feat = solve_features(d);
     const uint32_t pb = cap_blocks(d.cap_pair > d.nj ? d.cap_pair : d.nj);
     for (uint32_t phase = 0; phase < (sp.realtime ? 1u : 2u); ++phase) {
         if (phase != 0) {
@@ -1852,8 +979,8 @@ void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, const 
         solve_timer_begin(s);
         // The profiling build only for pmb_world_profile_step (it has the
         // same launch shape; the world sized its grid for both).
-        cudaLaunchCooperativeKernel(sp.debug_timing ? sv.timed : sv.ptr, dim3(coop), dim3(sv.threads), args, sv.smem,
-                                    s);
+        cudaLaunchCooperativeKernel(sp.debug_timing ? sv.timed[feat] : sv.ptr[feat], dim3(coop), dim3(sv.threads), args,
+                                    sv.smem, s);
         note_launch(coop);
         solve_timer_end(s);
         prof_mark(s, phase ? "solve phase 1" : "solve phase 0");

@@ -1,0 +1,175 @@
+// SPDX-License-Identifier: MIT
+// The group-per-body cooperative solve kernel (a persistent CTA per SM),
+// instantiated per CTA size in pmb_solve_t*.cu so that the instantiations
+// compile in parallel.
+#pragma once
+#include "pmb_solve_common.cuh"
+
+namespace pmb {
+
+// T threads per CTA, one CTA per SM (cooperative): 512 threads cap a thread
+// at 128 registers, 384 at 168, 256 at 255 -- fewer resident warps against
+// fewer spills; the world picks one (pmb_world_autotune). Timed: the
+// profiling build (pmb_world_profile_step), which records per-colour
+// timestamps of the first sweep; the ticks run the untimed build. Feat: the
+// code the world needs -- bit 0 (kFeatJoints) joint rows and joint duals,
+// bit 1 (kFeatThread) the body-per-thread sweep of policy 4. A build without
+// them has no call to the joint visit and no second body solver, so it needs
+// far fewer registers (127 against 168 at 384 threads): more warps fit at
+// 512 threads without spills. Every build computes the same bits.
+template <int T, bool Timed, int Feat>
+__global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t phase) {
+    constexpr int kSolveThreads = T;
+    constexpr bool kJoints = (Feat & kFeatJoints) != 0;
+    constexpr bool kThread = (Feat & kFeatThread) != 0;
+    Counters* c = d.ctr;
+    if (phase != 0 && c->impact == 0) return;
+    if (c->status & kStBarrierTimeout) return;  // the tick was abandoned
+    extern __shared__ __align__(16) uint8_t stage_raw[];
+    const int lane = threadIdx.x & 31;
+    uint8_t* warp_stage = stage_raw + (threadIdx.x >> 5) * kWarpStage;
+    const uint32_t nthreads = gridDim.x * kSolveThreads;
+    const float dt = sp.dt;
+    const uint32_t colors = c->colors;
+    uint32_t budget = sp.budget_request;
+    if (!sp.realtime && sp.requested == 0) budget = max(budget, c->joint_iters);
+    if (phase != 0 && sp.tolerance > 0.0f) budget = c->budget;
+    // Batched worlds sweep every scene its own budget (no residual-driven stop).
+    const bool adaptive = phase == 0 && sp.tolerance > 0.0f && !batched(d);
+    const uint32_t iters = batched(d) ? min(c->budget_max, kMaxIterations)
+                                      : adaptive ? min(max(sp.max_iterations, 1u), kMaxIterations)
+                                                 : min(budget, kMaxIterations);
+    const uint32_t n_con = c->n_contacts;
+    __shared__ double wsq[kSolveThreads / 32];
+    __shared__ uint32_t wn[kSolveThreads / 32], wov[kSolveThreads / 32];
+    __shared__ float wmx[kSolveThreads / 32];
+    const bool timing = Timed && phase == 0;
+    auto now = [] {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        return t;
+    };
+    if (timing && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_start = now();
+    for (uint32_t it = 0; it < iters; ++it) {
+        for (uint32_t col = 0; col < colors; ++col) {
+            const uint32_t* off = c->color_off + col * kWidthClasses;
+            const uint32_t b0 = off[0], b1 = off[kWidthClasses];
+            const uint32_t nb = b1 - b0;
+            const uint32_t trace = !timing || it != 0 ? 0u : col + 1 == colors ? 1u : col == 0 ? 2u : 0u;
+            // Bodies [lo, hi) with G lanes each. Consecutive bodies go to
+            // consecutive CTAs (group rank = local group x grid + CTA), so the
+            // heavy bodies at the front of a colour spread over all SMs.
+            // Policy 3 hands the bodies out dynamically instead: each group
+            // takes the next unclaimed body of the colour from a counter
+            // (claiming its following one while it solves), so groups that
+            // drew light bodies take more of them.
+            const uint32_t step = it * colors + col;
+            uint32_t* claim = &c->claim[step & 1u];
+            if (d.solve_policy == 3 && blockIdx.x == 0 && threadIdx.x == 0) c->claim[(step + 1u) & 1u] = 0u;
+            auto sweep = [&](auto width, uint32_t lo, uint32_t hi) {
+                constexpr int G = decltype(width)::value;
+                if (lo >= hi) return;
+                const int gl = lane % G, gbase = lane - gl;
+                const uint32_t gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << gbase;
+                GroupRows<G>& sm = reinterpret_cast<GroupRows<G>*>(warp_stage)[gbase / G];
+                auto body = [&](uint32_t k) {
+                    const uint32_t i = d.corder[k];
+                    if (phase != 0 && d.impact[i] == 0) return;
+                    if (batched(d) && it >= d.scene_budget[d.scene_of[i]]) return;
+                    solve_body_group<G, kJoints>(d, i, phase, dt, sm, gmask, gl, gbase, trace);
+                };
+                // One call site of the body solve for both assignments (each
+                // inlined copy adds its own stack frame).
+                const bool dynamic = d.solve_policy == 3;
+                const uint32_t groups = nthreads / G;
+                uint32_t k = lo + (threadIdx.x / G) * gridDim.x + blockIdx.x;
+                if (dynamic) {
+                    uint32_t t = 0;
+                    if (gl == 0) t = atomicAdd(claim, 1u);
+                    k = lo + __shfl_sync(gmask, t, gbase);
+                }
+                while (k < hi) {
+                    uint32_t next = 0;
+                    if (dynamic && gl == 0) next = atomicAdd(claim, 1u);
+                    body(k);
+                    if (dynamic) k = lo + __shfl_sync(gmask, next, gbase);
+                    else k += groups;
+                }
+                __syncwarp();
+            };
+            using W32 = std::integral_constant<int, 32>;
+            using W16 = std::integral_constant<int, 16>;
+            using W8 = std::integral_constant<int, 8>;
+            // Widths (see the group-per-body comment): policy 0 (and 3) one
+            // width per colour by its size, 1 eight lanes, 2 a width per body
+            // class (heaviest first) unless 32-lane groups cover the colour.
+            uint32_t r32 = b0, r16 = b0, r8 = b0;  // 32 lanes [b0, r32), 16 [r32, r16), 8 [r16, r8)
+            bool per_thread = false;
+            if constexpr (kThread) per_thread = d.solve_policy == 4 && nb * 16u > nthreads;
+            if (per_thread) {
+                // A body per thread: the colour has more bodies than 16-lane
+                // groups could take in one round. Consecutive bodies go to
+                // consecutive CTAs, as for the groups.
+                if constexpr (kThread) {
+                    Blk* slot = reinterpret_cast<Blk*>(warp_stage) + lane;
+                    for (uint32_t k = b0 + threadIdx.x * gridDim.x + blockIdx.x; k < b1; k += nthreads) {
+                        const uint32_t i = d.corder[k];
+                        if (phase != 0 && d.impact[i] == 0) continue;
+                        if (batched(d) && it >= d.scene_budget[d.scene_of[i]]) continue;
+                        solve_body_thread<kJoints>(d, i, phase, dt, slot);
+                    }
+                }
+                r32 = r16 = r8 = b0;
+            } else if (d.solve_policy != 1 && nb * 32u <= nthreads) {
+                r32 = r16 = r8 = b1;
+            } else if (d.solve_policy == 2) {
+                r32 = off[1];
+                r16 = off[2];
+                r8 = b1;
+            } else if ((d.solve_policy == 0 || d.solve_policy >= 3) && nb * 16u <= nthreads) {
+                r16 = r8 = b1;
+            } else {
+                r8 = b1;
+            }
+            sweep(W32{}, b0, r32);
+            sweep(W16{}, r32, r16);
+            sweep(W8{}, r16, r8);
+            if (timing && it == 0 && col < 18) {
+                __syncthreads();
+                if (threadIdx.x == 0) atomicMax(&c->dbg_work[col], now());
+            }
+            if (!grid_sync(c, d.barrier_spins)) return;
+            if (timing && it == 0 && col < 18 && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_release[col] = now();
+        }
+        Res res{0.0, 0u, 0.0f, 0u, sp.tolerance};
+        for (uint32_t k = grid_stride_begin(); k < n_con; k += grid_stride()) dual_contact(d, k, dt, phase, res, it);
+        if constexpr (kJoints)
+            for (uint32_t j = grid_stride_begin(); j < d.nj; j += grid_stride()) dual_joint(d, j, phase, dt, res, it);
+        // Deterministic reduction: warp tree, warps in order, blocks in order.
+        block_residual<kSolveThreads>(res, wsq, wn, wmx, wov, c, blockIdx.x);
+        if (timing && it == 0 && threadIdx.x == 0) atomicMax(&c->dbg_work[19], now());
+        if (!grid_sync(c, d.barrier_spins)) return;
+        if (timing && it == 0 && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_release[19] = now();
+        const SweepResidual sw = sweep_residual(c, 0u, sp);
+        if (phase == 0 && grid_stride_begin() == 0) c->residual_trace[it] = sw.measure;
+        bool last = it + 1 == iters;
+        if (adaptive && sw.met) last = true;
+        // Every block has read the partials before the next pass rewrites them.
+        if (!last && colors == 0 && !grid_sync(c, d.barrier_spins)) return;
+        if (last) {
+            if (grid_stride_begin() == 0) {
+                c->claim[0] = c->claim[1] = 0u;  // every block is past its last claim
+                if (phase == 0) {
+                    c->iterations = it + 1;
+                    c->residual = sw.rms;
+                    c->residual_max = sw.mx;
+                    c->residual_over = sw.over;
+                }
+                c->budget = it + 1;
+            }
+            return;
+        }
+    }
+}
+
+}  // namespace pmb

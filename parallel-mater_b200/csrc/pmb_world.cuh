@@ -368,16 +368,27 @@ inline void note_launch(unsigned long long blocks) {
 // Dominant-kernel timing: brackets each solve launch with CUDA events when on.
 void solve_timer_begin(cudaStream_t s);
 void solve_timer_end(cudaStream_t s);
-// Cooperative solve kernel variants (threads per CTA) and their smem.
+// Cooperative solve kernel variants (threads per CTA) and their smem. Each
+// has a build per feature set: bit 0 the world has joints, bit 1 the
+// body-per-thread sweep (policy 4) is compiled in.
+constexpr int kFeatJoints = 1;
+constexpr int kFeatThread = 2;
+constexpr int kSolveFeatures = 4;
 struct SolveVariant {
-    const void* ptr;    // the tick's kernel
-    const void* timed;  // the same with per-colour timestamps (profiling)
+    const void* ptr[kSolveFeatures];    // the tick's kernel
+    const void* timed[kSolveFeatures];  // the same with per-colour timestamps (profiling)
     int threads;
     size_t smem;
 };
 constexpr uint32_t kSolveVariants = 5;
 constexpr uint32_t kStagedFirst = 3;  // variants 3, 4: the staged solve with fused duals (512, 384 threads)
-extern const SolveVariant solve_variants[kSolveVariants];
+const SolveVariant& solve_variant(uint32_t v);
+// The feature set a world's launches use.
+inline int solve_features(const Dev& d) { return (d.nj ? kFeatJoints : 0) | (d.solve_policy == 4 ? kFeatThread : 0); }
+// Group-per-body builds, one translation unit per CTA size.
+SolveVariant solve_group_variant_512();
+SolveVariant solve_group_variant_384();
+SolveVariant solve_group_variant_256();
 void launch_contact_jacobians(const Dev& d, uint32_t phase, cudaStream_t s);
 // Sparse per-body record writes staged in io_index / io_rec (kind 0: inputs,
 // 1: kinematic targets, 2: states), and AoS state packing into `dst`.
