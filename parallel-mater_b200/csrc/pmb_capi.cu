@@ -353,7 +353,7 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     }
     ALLOC(d.deg, n); ALLOC(d.inc_off, n + 1); ALLOC(d.inc_cursor, n); ALLOC(d.inc_list, 2 * cap_pair);
     ALLOC(d.jdeg, n); ALLOC(d.jinc_off, n + 1); ALLOC(d.jinc_cursor, n); ALLOC(d.jinc_list, 2 * size_t(nj) + 2);
-    ALLOC(d.corder, n); ALLOC(d.cdirty, 2 * size_t(n));
+    ALLOC(d.corder, n); ALLOC(d.crec, n); ALLOC(d.cdirty, 2 * size_t(n));
     ALLOC(d.nbr, 2 * cap_pair + 2 * size_t(nj) + 2); ALLOC(d.nlow, n); ALLOC(d.nhigh, n);
     ALLOCP(d.events, z.events);
     ALLOC(d.rcount, n); ALLOC(d.roff, n + 1); ALLOC(d.blist, 2 * cap_contact); ALLOC(d.bother, 2 * cap_contact);

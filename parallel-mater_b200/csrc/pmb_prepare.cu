@@ -508,7 +508,9 @@ __global__ void k_color_scatter(Dev d) {
     for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
         if (d.motion[i] != kDynamic) continue;
         const uint32_t b = d.color[i] * kWidthClasses + width_class(d.rcount[i]);
-        d.corder[d.ctr->color_off[b] + atomicAdd(&d.ctr->color_count[b], 1u)] = i;
+        const uint32_t slot = d.ctr->color_off[b] + atomicAdd(&d.ctr->color_count[b], 1u);
+        d.corder[slot] = i;
+        d.crec[slot] = make_uint4(i, d.roff[i], d.rcount[i], 0u);
     }
 }
 

@@ -194,23 +194,55 @@ __device__ __forceinline__ void accumulate_crossing(float* ent, int gl, const Gr
     }
 }
 
+// What a body's solve reads of one of its contact rows: the contact (code:
+// index, bit 31 set when the body is the contact's second body) and the other
+// body. Loaded apart from the arithmetic so a body's first rows can be in
+// flight while its own state arrives.
+struct RawContact {
+    uint32_t c;
+    bool first;
+    Lite other;
+    float of;  // the other body's friction
+    float4 lam, pen, e;
+    V6 ja[3], jb[3];
+};
+__device__ __forceinline__ RawContact load_contact(const Dev& d, uint32_t code, uint32_t other_body) {
+    RawContact r;
+    r.c = code & 0x7fffffffu;
+    r.first = (code >> 31) == 0;
+    r.other = load_lite(d, other_body);
+    r.of = d.p1[other_body].x;
+    r.lam = d.c_lam[r.c];
+    r.pen = d.c_pen[r.c];
+    r.e = d.c_e[r.c];
+    load_jac(d, r.c, r.ja, r.jb);
+    return r;
+}
+
 // Rows of one contact for body i into chunk slot `slot`; its normal row,
 // raw penalty and normal trial also go to nrow[nslot].
 template <int G>
-__device__ __forceinline__ void stage_contact(const Dev& d, const Lite& me, float my_friction, uint32_t code,
-                                              uint32_t other_body, uint32_t phase, float dt, GroupRows<G>& sm,
-                                              int slot, int nslot) {
-    const uint32_t c = code & 0x7fffffffu;
-    const bool first = (code >> 31) == 0;
-    const Lite other = load_lite(d, other_body);
-    const Lite A = first ? me : other;  // values, not run-time references (no local copies)
-    const Lite B = first ? other : me;
-    const float of = d.p1[other_body].x;
+__device__ __forceinline__ void stage_loaded(const Dev& d, const Lite& me, float my_friction, const RawContact& rc,
+                                             uint32_t phase, float dt, GroupRows<G>& sm, int slot, int nslot) {
+    const uint32_t c = rc.c;
+    const bool first = rc.first;
+    const Lite A = first ? me : rc.other;  // values, not run-time references (no local copies)
+    const Lite B = first ? rc.other : me;
+    const float of = rc.of;
     const float friction = sqrtf(first ? my_friction * of : of * my_friction);
-    const float4 lam = d.c_lam[c], pen = d.c_pen[c];
+    const float4 lam = rc.lam, pen = rc.pen;
     V6 ja[3], jb[3];
     float err[3];
-    contact_rows(d, c, d.c_e[c], A, B, ja, jb, err);
+    {
+        // contact_rows' error terms, from the loaded jacobians
+        const float e3[3] = {rc.e.x, rc.e.y, rc.e.z};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            ja[k] = rc.ja[k];
+            jb[k] = rc.jb[k];
+            err[k] = e3[k] + dot6(ja[k], A.dx) + dot6(jb[k], B.dx);
+        }
+    }
     F3 trial{lam.x + pen.x * err[0], lam.y + pen.y * err[1], lam.z + pen.z * err[2]};
     if (nslot >= 0) {
 #pragma unroll
@@ -245,6 +277,36 @@ __device__ __forceinline__ void stage_contact(const Dev& d, const Lite& me, floa
 #pragma unroll
         for (int k = 0; k < 6; ++k) sm.r[slot][x][8 + k] = st[x] * row.v[k];  // = (stiffness x J_i), as before
     }
+}
+template <int G>
+__device__ __forceinline__ void stage_contact(const Dev& d, const Lite& me, float my_friction, uint32_t code,
+                                              uint32_t other_body, uint32_t phase, float dt, GroupRows<G>& sm,
+                                              int slot, int nslot) {
+    stage_loaded<G>(d, me, my_friction, load_contact(d, code, other_body), phase, dt, sm, slot, nslot);
+}
+
+// The body a lane group solves next in its colour, fetched while the current
+// one solves (bodies of one colour share no contact, so nothing the current
+// body writes is read here): its record and this lane's row codes of its
+// first two chunks.
+struct Ahead {
+    uint32_t i, ro, rn;
+    uint32_t code0, other0, code1, other1;
+};
+template <int G>
+__device__ __forceinline__ void fetch_codes(const Dev& d, Ahead& a, int gl) {
+    const uint32_t s0 = uint32_t(gl), s1 = uint32_t(gl) + uint32_t(G);
+    a.code0 = s0 < a.rn ? d.blist[a.ro + s0] : 0u;
+    a.other0 = s0 < a.rn ? d.bother[a.ro + s0] : 0u;
+    a.code1 = s1 < a.rn ? d.blist[a.ro + s1] : 0u;
+    a.other1 = s1 < a.rn ? d.bother[a.ro + s1] : 0u;
+}
+template <int G>
+__device__ __forceinline__ Ahead fetch_ahead(const Dev& d, uint32_t k, int gl) {
+    const uint4 r = d.crec[k];
+    Ahead a{r.x, r.y, r.z, 0u, 0u, 0u, 0u};
+    fetch_codes<G>(d, a, gl);
+    return a;
 }
 
 // Joint rows of body i added to its block (geometry_constraints_solve.slang:
@@ -289,8 +351,10 @@ __device__ __forceinline__ unsigned long long gtimer() {
 }
 // Joints: the world has joints (a world without them gets a build with no
 // joint code, which needs fewer registers).
+// ah: the body (its record and this lane's first row codes, fetched ahead);
+// on return it holds the same for slot kn of the colour order (~0u: none).
 template <int G, bool Joints>
-__device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float dt, GroupRows<G>& sm,
+__device__ void solve_body_group(const Dev& d, Ahead& ah, uint32_t kn, uint32_t phase, float dt, GroupRows<G>& sm,
                                  uint32_t gmask, int gl, int gbase, uint32_t trace = 0) {
     // trace 1: slowest body of the colour per stage; 2: stage times summed
     // over the colour's bodies (profiling only).
@@ -299,12 +363,18 @@ __device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float
         if (trace == 1 && gl == 0) atomicMax(&d.ctr->dbg_body[k], gtimer() - t0);
         if (trace == 2 && gl == 0) atomicAdd(&d.ctr->dbg_sum[k], gtimer() - t0);
     };
+    const uint32_t i = ah.i, ro = ah.ro, rn = ah.rn;
+    const uint32_t code0 = ah.code0, other0 = ah.other0, code1 = ah.code1, other1 = ah.other1;
+    uint4 nrec = make_uint4(0u, 0u, 0u, 0u);
+    if (kn != ~0u) nrec = d.crec[kn];
     const Lite me = load_lite(d, i);
     const float my_friction = d.p1[i].x;
-    const uint32_t ro = d.roff[i], rn = d.rcount[i];
     float ent[Owned<G>::E];
-    {
-        const float4 ia = d.inA[i], ib = d.inB[i];
+    const float4 ia = d.inA[i], ib = d.inB[i];
+    // The block's starting entries: inertia and its gradient. Formed after
+    // the first chunk's rows are requested, so those loads and this body's
+    // own state are in flight together.
+    auto init_entries = [&] {
         float H[21];
 #pragma unroll
         for (int k = 0; k < 21; ++k) H[k] = 0.0f;
@@ -332,15 +402,27 @@ __device__ void solve_body_group(const Dev& d, uint32_t i, uint32_t phase, float
             }
             ent[q] = v;
         }
-    }
+    };
+    if (rn == 0) init_entries();
     for (uint32_t base = 0; base < rn; base += G) {
         const uint32_t sidx = base + gl;
-        if (sidx < rn)
-            stage_contact<G>(d, me, my_friction, d.blist[ro + sidx], d.bother[ro + sidx], phase, dt, sm, gl,
-                             sidx < kNormSlots ? int(sidx) : -1);
+        if (sidx < rn) {
+            const int nslot = sidx < kNormSlots ? int(sidx) : -1;
+            const uint32_t code = base == 0 ? code0 : base == uint32_t(G) ? code1 : d.blist[ro + sidx];
+            const uint32_t other = base == 0 ? other0 : base == uint32_t(G) ? other1 : d.bother[ro + sidx];
+            stage_contact<G>(d, me, my_friction, code, other, phase, dt, sm, gl, nslot);
+        }
+        if (base == 0) init_entries();
         __syncwarp(gmask);
         accumulate_chunk<G>(ent, gl, sm, min(uint32_t(G), rn - base));
         __syncwarp(gmask);
+    }
+    // The next body's record and row codes, in flight while this one solves.
+    if (kn != ~0u) {
+        ah.i = nrec.x;
+        ah.ro = nrec.y;
+        ah.rn = nrec.z;
+        fetch_codes<G>(d, ah, gl);
     }
     mark(0);
     Blk blk;

@@ -72,14 +72,10 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
                 const int gl = lane % G, gbase = lane - gl;
                 const uint32_t gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << gbase;
                 GroupRows<G>& sm = reinterpret_cast<GroupRows<G>*>(warp_stage)[gbase / G];
-                auto body = [&](uint32_t k) {
-                    const uint32_t i = d.corder[k];
-                    if (phase != 0 && d.impact[i] == 0) return;
-                    if (batched(d) && it >= d.scene_budget[d.scene_of[i]]) return;
-                    solve_body_group<G, kJoints>(d, i, phase, dt, sm, gmask, gl, gbase, trace);
-                };
                 // One call site of the body solve for both assignments (each
-                // inlined copy adds its own stack frame).
+                // inlined copy adds its own stack frame). The group learns its
+                // next body before solving the current one and fetches that
+                // body's record and row codes during the solve.
                 const bool dynamic = d.solve_policy == 3;
                 const uint32_t groups = nthreads / G;
                 uint32_t k = lo + (threadIdx.x / G) * gridDim.x + blockIdx.x;
@@ -88,12 +84,25 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
                     if (gl == 0) t = atomicAdd(claim, 1u);
                     k = lo + __shfl_sync(gmask, t, gbase);
                 }
+                Ahead ah{};
+                if (k < hi) ah = fetch_ahead<G>(d, k, gl);
                 while (k < hi) {
-                    uint32_t next = 0;
-                    if (dynamic && gl == 0) next = atomicAdd(claim, 1u);
-                    body(k);
-                    if (dynamic) k = lo + __shfl_sync(gmask, next, gbase);
-                    else k += groups;
+                    uint32_t next = k + groups;
+                    if (dynamic) {
+                        uint32_t t = 0;
+                        if (gl == 0) t = atomicAdd(claim, 1u);
+                        next = lo + __shfl_sync(gmask, t, gbase);
+                    }
+                    const uint32_t kn = next < hi ? next : ~0u;
+                    const uint32_t i = ah.i;
+                    const bool skip = (phase != 0 && d.impact[i] == 0) ||
+                                      (batched(d) && it >= d.scene_budget[d.scene_of[i]]);
+                    if (skip) {
+                        if (kn != ~0u) ah = fetch_ahead<G>(d, kn, gl);
+                    } else {
+                        solve_body_group<G, kJoints>(d, ah, kn, phase, dt, sm, gmask, gl, gbase, trace);
+                    }
+                    k = next;
                 }
                 __syncwarp();
             };

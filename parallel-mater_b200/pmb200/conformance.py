@@ -55,10 +55,13 @@ class _Body:
     """RigidBodyOptions with the reference's defaults."""
 
     def __init__(self, name, mesh, position, motion=scenes.DYNAMIC, mass=1.0, inertia=(0.0, 0.0, 0.0),
-                 linear_damping=0.05, angular_damping=0.05):
+                 linear_damping=0.05, angular_damping=0.05, orientation=(0.0, 0.0, 0.0, 1.0),
+                 velocity=(0.0, 0.0, 0.0), friction=0.5, restitution=0.0, margin=0.005):
         self.name, self.mesh, self.position, self.motion = name, mesh, position, motion
         self.mass, self.inertia = mass, inertia
         self.linear_damping, self.angular_damping = linear_damping, angular_damping
+        self.orientation, self.velocity = orientation, velocity
+        self.friction, self.restitution, self.margin = friction, restitution, margin
 
 
 def _direct_scene():
@@ -91,12 +94,66 @@ def _scene(meshes, bodies, joints):
     ids = [b.mesh(v, i) for v, i in meshes]
     for body in bodies:
         inertia = tuple(body.inertia) if any(body.inertia) else (1.0, 1.0, 1.0)
-        b.body(ids[body.mesh], body.motion, body.position, mass=body.mass, inertia=inertia,
+        b.body(ids[body.mesh], body.motion, body.position, q=body.orientation, v=body.velocity, mass=body.mass,
+               inertia=inertia, friction=body.friction, restitution=body.restitution, margin=body.margin,
                linear_damping=body.linear_damping, angular_damping=body.angular_damping)
-    for name, a, c, threshold in joints:
+    for joint in joints:
+        if isinstance(joint, dict):  # an authored constraint (glb.load_glb_scene)
+            k = b.joint(joint["type"], joint["body_a"], joint["body_b"], joint["anchor_a"], joint["anchor_b"],
+                        disable_collisions=joint["disable_collisions"], iterations=joint["solver_iterations"])
+            o = b.joints[k]
+            o["frame_a"], o["frame_b"] = joint["frame_a"], joint["frame_b"]
+            o["enabled"] = 1 if joint["enabled"] else 0
+            o["breaking_threshold"] = joint["breaking_threshold"]
+            for f in ("lin_limit_axes", "ang_limit_axes", "lin_spring_axes", "ang_spring_axes", "lin_lower",
+                      "lin_upper", "ang_lower", "ang_upper", "lin_stiffness", "lin_damping", "ang_stiffness",
+                      "ang_damping", "motor_linear_velocity", "motor_linear_max_impulse", "motor_angular_velocity",
+                      "motor_angular_max_impulse"):
+                o[f] = joint[f]
+            o["motor_linear"] = 1 if joint["motor_linear"] else 0
+            o["motor_angular"] = 1 if joint["motor_angular"] else 0
+            continue
+        name, a, c, threshold = joint
         k = b.joint(scenes.FIXED, a, c, ANCHOR_A, ANCHOR_B, disable_collisions=True, iterations=8)
         b.joints[k]["breaking_threshold"] = threshold
     return b.build("conformance", 8, scenes.REALTIME)
+
+
+def glb_case_scene(gs):
+    """(meshes, bodies, joints, body ids, constraint ids) of an authored scene
+    (glb.load_glb_scene) as the conformance runner builds it
+    (command_runner.cpp:1063-1095; scene_builder.cpp:393-433): each body's
+    collision meshes -- its proxy's when it has one, else its render
+    primitives -- merged into one geometry (shared by bodies with the same
+    meshes), resource ids "rigid/<source name>/<index>" and
+    "constraint/<name>/<index>"."""
+    meshes, keys, bodies = [], {}, []
+    for k, body in enumerate(gs.bodies):
+        proxy = bool(body["collision_mesh_indices"])
+        parts = body["collision_mesh_indices"] if proxy else body["mesh_indices"]
+        key = (proxy, tuple(parts))
+        if key not in keys:
+            src = gs.collision_meshes if proxy else gs.meshes
+            verts, idx, base = [], [], 0
+            for m in parts:
+                v, i = src[m]
+                verts.append(v)
+                idx.append(i + base)
+                base += len(v)
+            keys[key] = len(meshes)
+            meshes.append((np.concatenate(verts).astype(np.float32), np.concatenate(idx).astype(np.uint32)))
+        bodies.append(_Body(f"rigid/{body['source_name'] or body['name']}/{k}", keys[key],
+                            tuple(float(x) for x in body["position"]), motion=body["motion"],
+                            mass=float(body["mass"]), inertia=(0.0, 0.0, 0.0),
+                            linear_damping=float(body["linear_damping"]),
+                            angular_damping=float(body["angular_damping"]),
+                            orientation=tuple(float(x) for x in body["orientation"]),
+                            velocity=tuple(float(x) for x in body["velocity"]),
+                            friction=float(body["friction"]), restitution=float(body["restitution"]),
+                            margin=float(body["margin"])))
+    joints = [dict(c) for c in gs.constraints]
+    jnames = [f"constraint/{c['name']}/{k}" for k, c in enumerate(gs.constraints)]
+    return meshes, bodies, joints, [b.name for b in bodies], jnames
 
 
 def _rotate(q, p):
@@ -125,28 +182,35 @@ def _vec(v):
     return [float(x) for x in v]
 
 
-def run_case(case, with_quality=False):
-    """Runs one analytic case through the pm* driver; returns the result
-    document {case_id, checkpoints: [...]} in the runner's layout.
-    with_quality adds the runner's rigid_quality invariants (joint anchor and
-    angle errors, mechanical energy), which the recorded CUDA results lack."""
+def run_case(case, with_quality=False, authored=None):
+    """Runs one case through the pm* driver; returns the result document
+    {case_id, checkpoints: [...]} in the runner's layout. Analytic cases build
+    their scene here; an integrated_glb case takes `authored`, the scene its
+    GLB loads to (glb.load_glb_scene). with_quality adds the runner's
+    rigid_quality invariants (joint anchor and angle errors, mechanical
+    energy; analytic cases), which the recorded CUDA results lack."""
     cid = case["id"]
-    meshes, bodies, joints = SCENES[cid]()
+    if authored is not None:
+        meshes, bodies, joints, names, jnames = glb_case_scene(authored)
+        with_quality = False
+    else:
+        meshes, bodies, joints = SCENES[cid]()
+        names = [body.name for body in bodies]
+        jnames = [j[0] for j in joints]
     scene = _scene(meshes, bodies, joints)
     world = case["world"]
     gravity = tuple(float(g) for g in world["gravity"])
     infos = {i: {"mass": float(body.mass), "inertiaDiagonal": tuple(float(v) for v in body.inertia)}
              for i, body in enumerate(bodies)}
     session = pm.RigidSession(scene, iterations=10, contact_capacity=65536, body_infos=infos)
-    names = [body.name for body in bodies]
-    jnames = [j[0] for j in joints]
     present = [True] * len(joints)
     flags = {"generation_changed": False, "constraints_rebuilt": False}
     profile = case["tolerances"]["profile"]
     states = np.zeros(len(bodies), scenes.STATE_DTYPE)
     for i, body in enumerate(bodies):
         states[i]["x"] = body.position
-        states[i]["q"] = (0.0, 0.0, 0.0, 1.0)
+        states[i]["q"] = body.orientation
+        states[i]["v"] = body.velocity
     cstates = [(True, False, 0.0)] * len(joints)
     events = np.zeros(0, pm.PM_EVENT_DTYPE)
 
@@ -183,7 +247,8 @@ def run_case(case, with_quality=False):
             pot = -body.mass * sum(gravity[k] * float(states[i]["x"][k]) for k in range(3))
             energy += 0.5 * body.mass * lin2 + ang + pot
         jpos = jang = 0.0
-        for k, (_, a, c, _) in enumerate(joints):
+        for k, joint in enumerate(joints if with_quality else []):
+            _, a, c, _ = joint
             if not present[k]:
                 continue
             pa = [float(states[a]["x"][m]) + float(r) for m, r in enumerate(_rotate(states[a]["q"], ANCHOR_A))]

@@ -10,19 +10,83 @@ CPU tests check the comparator itself on the golden documents; the GPU test
 runs the cases.
 """
 import copy
+import hashlib
 import json
 import os
 
+import numpy as np
 import pytest
 
-from pmb200 import conformance
+from pmb200 import conformance, glb
 
 FIXTURE = os.path.join(os.path.dirname(__file__), "golden", "conformance_analytic.json")
+GLB_FIXTURE = os.path.join(os.path.dirname(__file__), "golden", "conformance_glb.npz")
+GLB_CASES = ["constraint-fixed", "constraint-generic", "constraint-generic-spring", "constraint-hinge",
+             "constraint-motor", "constraint-piston", "constraint-point", "constraint-slider"]
+REFERENCE = os.environ.get("PMB_REFERENCE_ROOT", "/root/reference")
 
 
 def _fixture():
     with open(FIXTURE) as f:
         return json.load(f)
+
+
+def _glb_fixture():
+    """{case id: (metadata, GlbScene)} from conformance_glb.npz (extracted by
+    make_conformance_glb.py)."""
+    z = np.load(GLB_FIXTURE)
+    meta = json.loads(bytes(z["meta"]).decode())
+    out = {}
+    for cid, m in meta.items():
+        gs = glb.GlbScene()
+        gs.meshes = [[z[f"{cid}/mesh{k}/v"], z[f"{cid}/mesh{k}/i"]] for k in range(m["meshes"])]
+        gs.collision_meshes = [[z[f"{cid}/collision{k}/v"], z[f"{cid}/collision{k}/i"]]
+                               for k in range(m["collision_meshes"])]
+        vec = ("position", "orientation", "velocity", "anchor_a", "anchor_b", "frame_a", "frame_b", "lin_lower",
+               "lin_upper", "ang_lower", "ang_upper", "lin_stiffness", "lin_damping", "ang_stiffness", "ang_damping")
+        gs.bodies = [{k: (np.asarray(v, np.float32) if k in vec else v) for k, v in b.items()} for b in m["bodies"]]
+        gs.constraints = [{k: (np.asarray(v, np.float32) if k in vec else v) for k, v in c.items()}
+                          for c in m["constraints"]]
+        out[cid] = (m, gs)
+    return out
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REFERENCE, "examples", "assets")),
+                    reason="the reference checkout is not present")
+def test_glb_fixture_is_what_the_reference_assets_load_to():
+    """The committed scenes are what pmb200.glb loads from the reference's
+    GLBs today (same asset bytes, meshes, bodies and constraints)."""
+    for cid, (m, gs) in _glb_fixture().items():
+        with open(os.path.join(REFERENCE, m["asset"]), "rb") as f:
+            data = f.read()
+        assert hashlib.sha256(data).hexdigest() == m["sha256"], cid
+        fresh = glb.load_glb_scene(data)
+        for a, b in zip(fresh.meshes + fresh.collision_meshes, gs.meshes + gs.collision_meshes):
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), cid
+        assert len(fresh.bodies) == len(gs.bodies) and len(fresh.constraints) == len(gs.constraints), cid
+        for x, y in zip(fresh.bodies + fresh.constraints, gs.bodies + gs.constraints):
+            for k, v in x.items():
+                assert np.array_equal(np.asarray(v), np.asarray(y[k])), (cid, k)
+
+
+def test_glb_scenes_load_to_the_recorded_initial_state():
+    """Frame 0 of each recorded authored-scene result is the loaded scene:
+    the same bodies in order (ids "rigid/<source name>/<index>"), positions
+    and orientations bit for bit (bounds re-centring, Blender frame basis),
+    the same constraint ids and counts."""
+    for cid, (m, gs) in _glb_fixture().items():
+        golden = m["golden"]["checkpoints"][0]
+        assert golden["frame"] == 0
+        _, _, _, names, jnames = conformance.glb_case_scene(gs)
+        bodies = [r for r in golden["resources"] if r["type"] == "rigid_body"]
+        joints = [r for r in golden["resources"] if r["type"] == "rigid_constraint"]
+        assert [r["id"] for r in bodies] == names and [r["id"] for r in joints] == jnames, cid
+        for r, b in zip(bodies, gs.bodies):
+            assert np.array_equal(np.asarray(r["position"], np.float32), b["position"]), (cid, r["id"])
+            assert np.array_equal(np.asarray(r["orientation"], np.float32), b["orientation"]), (cid, r["id"])
+            assert np.array_equal(np.asarray(r["linear_velocity"], np.float32), b["velocity"]), (cid, r["id"])
+        inv = golden["invariants"]
+        assert inv["rigid_body_count"] == len(gs.bodies) and inv["constraint_count"] == len(gs.constraints), cid
 
 
 def test_comparator_accepts_the_golden_and_rejects_perturbations():
