@@ -416,12 +416,14 @@ PMB_API int pmb_world_scene_stats(pmb_world* world, float* residual, float* resi
 /* ---- launch plan ----
  * How the cooperative solve kernel is launched: solve_variant 0, 1, 2 = 512,
  * 384, 256 threads per CTA (one CTA per SM; fewer threads leave each thread
- * more registers); solve_policy 0 = 8, 16 or 32 lanes per body chosen per
- * colour by its size, 1 = always 8, 2 = per body by its contact rows (more
- * than 16: 32 lanes, 9-16: 16, else 8; heaviest bodies first) unless 32-lane
- * groups cover the whole colour, 3 = widths as 0 with the colour's bodies
- * claimed dynamically from a counter. Every plan computes bit-identical results;
- * only the speed differs. A new world starts with (1, 0). */
+ * more registers), 3, 4 = the staged solve with fused dual updates at 512 and
+ * 384 threads; solve_policy 0 = 8, 16 or 32 lanes per body chosen per colour
+ * by its size, 1 = always 8, 2 = per body by its contact rows (more than 16:
+ * 32 lanes, 9-16: 16, else 8; heaviest bodies first) unless 32-lane groups
+ * cover the whole colour, 3 = widths as 0 with the colour's bodies claimed
+ * dynamically from a counter, 4 = one thread per body in colours with more
+ * bodies than 16-lane groups, else as 0. Every plan computes bit-identical
+ * results; only the speed differs. A new world starts with (0, 0). */
 PMB_API int pmb_world_set_launch_plan(pmb_world* world, uint32_t solve_variant, uint32_t solve_policy);
 /* Bound on the polls a thread block makes at a grid barrier of the tick's
  * cooperative kernels (colouring fixpoint, solve) before it gives up (0: the

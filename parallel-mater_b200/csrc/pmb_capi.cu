@@ -691,7 +691,7 @@ int pmb_world_create(const pmb_world_desc* desc, pmb_world** out) {
     std::vector<float> sorted = expand;
     std::nth_element(sorted.begin(), sorted.begin() + n / 2, sorted.end());
     d.large_extent = 2.0f * sorted[n / 2] * 4.0f;
-    d.solve_variant = 1;  // 384 threads: the fastest plan on a settled 65k-box pile
+    d.solve_variant = 0;  // 512 threads: the fastest plan on a settled 65k-box pile
     d.solve_policy = 0;
     d.barrier_spins = kDefaultBarrierSpins;
     for (uint32_t v = 0; v < kSolveVariants; ++v) {

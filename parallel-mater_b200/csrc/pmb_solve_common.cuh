@@ -79,7 +79,7 @@ __device__ __forceinline__ void apply_pose_update(const Dev& d, uint32_t i, cons
     d.dxa[i] = make_float4(2.0f * rel.x, 2.0f * rel.y, 2.0f * rel.z, 0.0f);
 }
 
-// Group-per-body primal: G lanes (G = 8, 16 or 32) solve one body. Lanes
+// Group-per-body primal: G lanes (G = 4, 8, 16 or 32) solve one body. Lanes
 // evaluate the body's contact rows G at a time (coalesced SoA loads) and
 // stage them in shared memory; each lane owns ceil(27/G) of the 27 entries of
 // the packed 6x6 block (21 Hessian, 6 gradient) and adds the staged rows to
@@ -95,19 +95,23 @@ __device__ __forceinline__ void apply_pose_update(const Dev& d, uint32_t i, cons
 // The tail colours of a pile hold few but heavily loaded bodies (tens of
 // rows), and a colour ends when its slowest body does, so wider groups
 // there shorten the critical path.
-constexpr uint32_t kNormSlots = 32;
 template <int G> struct GroupRows {
+    // Normal rows kept for the crossing safeguard (rows past them are
+    // evaluated again there): 32, or 16 for the 4-lane groups whose eight
+    // slots share a warp's staging area.
+    static constexpr uint32_t kSlots = G == 4 ? 16u : 32u;
     // Chunk being accumulated: 3 rows of (jacobian[6], stiffness, force,
     // stiffness x jacobian[6]); the last six are the Hessian products' first
     // factors, formed once per row instead of once per entry.
     float r[G][3][14];
-    float nrow[kNormSlots][8];  // normal row: jacobian[6], raw penalty, trial force
+    float nrow[kSlots][8];  // normal row: jacobian[6], raw penalty, trial force
     uint32_t flag[G];
     Blk jblk;  // the block while joint rows are added (joint_rows_shared)
 };
-// Per-warp staging area: four 8-lane groups, two 16-lane groups or one
-// 32-lane group.
-constexpr size_t kWarpStage = 4 * sizeof(GroupRows<8>);
+// Per-warp staging area: eight 4-lane groups, four 8-lane groups, two
+// 16-lane groups or one 32-lane group.
+constexpr size_t kWarpStage = 8 * sizeof(GroupRows<4>) > 4 * sizeof(GroupRows<8>) ? 8 * sizeof(GroupRows<4>)
+                                                                                   : 4 * sizeof(GroupRows<8>);
 static_assert(2 * sizeof(GroupRows<16>) <= kWarpStage && sizeof(GroupRows<32>) <= kWarpStage, "staging area");
 static_assert(32 * sizeof(Blk) <= kWarpStage, "a block slot per thread for the body-per-thread sweep");
 
@@ -187,7 +191,7 @@ __device__ __forceinline__ void accumulate_crossing(float* ent, int gl, const Gr
         if (e < 21) entry_ik(e, ei, ek);
         for (uint32_t t = 0; t < m; ++t) {
             if (!sm.flag[t]) continue;
-            const float* row = sm.nrow[(s0 + t) % kNormSlots];
+            const float* row = sm.nrow[(s0 + t) % GroupRows<G>::kSlots];
             if (e < 21) ent[q] += row[6] * row[ei] * row[ek];
             else ent[q] += row[e - 21] * row[7];
         }
@@ -407,7 +411,7 @@ __device__ void solve_body_group(const Dev& d, Ahead& ah, uint32_t kn, uint32_t 
     for (uint32_t base = 0; base < rn; base += G) {
         const uint32_t sidx = base + gl;
         if (sidx < rn) {
-            const int nslot = sidx < kNormSlots ? int(sidx) : -1;
+            const int nslot = sidx < GroupRows<G>::kSlots ? int(sidx) : -1;
             const uint32_t code = base == 0 ? code0 : base == uint32_t(G) ? code1 : d.blist[ro + sidx];
             const uint32_t other = base == 0 ? other0 : base == uint32_t(G) ? other1 : d.bother[ro + sidx];
             stage_contact<G>(d, me, my_friction, code, other, phase, dt, sm, gl, nslot);
@@ -439,13 +443,14 @@ __device__ void solve_body_group(const Dev& d, Ahead& ah, uint32_t kn, uint32_t 
     bool crossing = false;
     for (uint32_t base = 0; base < rn; base += G) {
         const uint32_t sidx = base + gl;
-        if (rn > kNormSlots && base >= kNormSlots && sidx < rn)
+        constexpr uint32_t kSlots = GroupRows<G>::kSlots;
+        if (rn > kSlots && base >= kSlots && sidx < rn)
             stage_contact<G>(d, me, my_friction, d.blist[ro + sidx], d.bother[ro + sidx], phase, dt, sm, -1,
-                             int(sidx % kNormSlots));
+                             int(sidx % kSlots));
         __syncwarp(gmask);
         uint32_t flag = 0;
         if (sidx < rn) {
-            const float* row = sm.nrow[sidx % kNormSlots];
+            const float* row = sm.nrow[sidx % kSlots];
             V6 nr;
 #pragma unroll
             for (int k = 0; k < 6; ++k) nr.v[k] = row[k];
@@ -456,7 +461,7 @@ __device__ void solve_body_group(const Dev& d, Ahead& ah, uint32_t kn, uint32_t 
         __syncwarp(gmask);
         if (__any_sync(gmask, flag)) {
             crossing = true;
-            accumulate_crossing<G>(ent, gl, sm, base % kNormSlots, min(uint32_t(G), rn - base));
+            accumulate_crossing<G>(ent, gl, sm, base % kSlots, min(uint32_t(G), rn - base));
         }
         __syncwarp(gmask);
     }

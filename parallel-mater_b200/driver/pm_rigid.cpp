@@ -303,10 +303,13 @@ PmResult PMAPI_CALL pmCreateSimulation(PmDevice device, const PmSimulationCreate
     c.body_count = n;
     c.joint_count = info->constraintCapacity;
     c.mesh_count = std::max(16u, n);
-    // Distinct meshes are usually few and small; the budget allows a box
-    // mesh per body with room to spare.
-    c.mesh_vertex_count = 4096u + 16u * n;
-    c.mesh_triangle_count = 8192u + 32u * n;
+    // The simulation holds a copy of every geometry its bodies use (the
+    // reference keeps geometry in separate objects, so its create info names
+    // no geometry budget). The budget allows a box mesh per body plus 64k
+    // vertices and 128k triangles of authored meshes (gears, frames, scanned
+    // props): a few MB of persistent memory.
+    c.mesh_vertex_count = 65536u + 16u * n;
+    c.mesh_triangle_count = 131072u + 32u * n;
     // Contact events kept per tick (resources.cpp:212, contact_capacity).
     c.event_capacity = std::max(1u, info->contactCapacity);
     uint64_t persistent = 0, scratch = 0;

@@ -292,6 +292,10 @@ def run_case(case, with_quality=False, authored=None):
                     r["x"], r["q"] = tuple(value), (0.0, 0.0, 0.0, 1.0)
                     pm.check(session.set_states(i, [r]), "replace body")
                     flags["generation_changed"] = True
+                elif op == "set_constraints_enabled":
+                    # every constraint rewritten with its enabled (active)
+                    # option set to the value (command_runner.cpp:1221-1233)
+                    pm.check(session.write_constraints([bool(value[0])] * len(present)), op)
                 elif op in ("remove_constraints", "add_constraints"):
                     active = op == "add_constraints"
                     present[:] = [active] * len(present)

@@ -196,3 +196,40 @@ def test_analytic_case_against_reference_cuda(gpu_available, cid):
             (ex, ey), (evx, evy) = _current_law(k, 0.75)
             assert abs(pos[0] - ex) <= 1e-5 and abs(pos[1] - ey) <= 1e-5, (k, pos, (ex, ey))
             assert abs(vel[0] - evx) <= 1e-5 and abs(vel[1] - evy) <= 1e-5, (k, vel, (evx, evy))
+
+
+# Exact fields that follow the trajectory (how many contact points a tick
+# reports), not the scene's structure.
+_TRAJECTORY_EXACT = (".rigid_contact_count", ".rigid_contacts")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cid", GLB_CASES)
+def test_glb_case_against_reference_cuda(gpu_available, cid):
+    """The reference's authored-scene rigid constraint cases (one per joint
+    type, each a Blender-exported GLB) loaded by pmb200.glb and run through
+    the pm* driver: every checkpoint, body and constraint of the recorded
+    CUDA result is produced with equal ids, types and flags (present,
+    enabled, broken) and equal body, constraint and element counts, and the
+    state stays finite. Position, velocity and impulse values and contact
+    counts are reported against the recorded values (printed), not asserted:
+    the recorded results come from the earlier revision the analytic cases
+    show, and the runs diverge where contacts or limits engage."""
+    m, gs = _glb_fixture()[cid]
+    result = conformance.run_case(m["case"], authored=gs)
+    fails = conformance.compare(m["case"], m["golden"]["checkpoints"], result["checkpoints"], kinds=True)
+    structural = [f for f in fails if f[2] == "exact" and not f[0].endswith(_TRAJECTORY_EXACT)
+                  and ".rigid_contacts" not in f[0]]
+    numeric = [f for f in fails if f not in structural]
+    deviation = []
+    for cp_e, cp_a in zip(m["golden"]["checkpoints"], result["checkpoints"]):
+        dev = max((float(np.abs(np.asarray(e["position"]) - np.asarray(a["position"])).max())
+                   for e, a in zip(cp_e["resources"], cp_a["resources"]) if e["type"] == "rigid_body"), default=0.0)
+        deviation.append((cp_e["frame"], round(dev, 5), cp_e["contacts"]["rigid_contact_count"],
+                          cp_a["contacts"]["rigid_contact_count"]))
+    print(f"{cid}: {len(numeric)} values outside tolerance; (frame, largest position deviation m, recorded "
+          f"contacts, contacts): {deviation}")
+    for path, message, _ in numeric[:10]:
+        print("  ", path, message)
+    assert not structural, structural[:10]
+    assert all(cp["invariants"]["finite"] for cp in result["checkpoints"])
