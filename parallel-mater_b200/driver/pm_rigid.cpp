@@ -310,8 +310,13 @@ PmResult PMAPI_CALL pmCreateSimulation(PmDevice device, const PmSimulationCreate
     // props): a few MB of persistent memory.
     c.mesh_vertex_count = 65536u + 16u * n;
     c.mesh_triangle_count = 131072u + 32u * n;
-    // Contact events kept per tick (resources.cpp:212, contact_capacity).
+    // Contact events kept per tick (resources.cpp:212, contact_capacity),
+    // and at least as many contact points (with the triangle-pair work of
+    // the mesh path, which is sized like the contact points): authored
+    // meshes such as meshing gears make thousands of triangle pairs among a
+    // handful of bodies, more than the per-body default allows.
     c.event_capacity = std::max(1u, info->contactCapacity);
+    c.contact_capacity = std::max(64u * n + 4096u, info->contactCapacity);
     uint64_t persistent = 0, scratch = 0;
     if (pmb_world_memory_requirements(&c, &persistent, &scratch) != PMB_SUCCESS) {
         delete created;

@@ -201,6 +201,14 @@ def test_analytic_case_against_reference_cuda(gpu_available, cid):
 # Exact fields that follow the trajectory (how many contact points a tick
 # reports), not the scene's structure.
 _TRAJECTORY_EXACT = (".rigid_contact_count", ".rigid_contacts")
+# Values outside tolerance against the recorded results (the run is
+# deterministic, so these are exact counts; more is a regression). The
+# point case releases four tethered spheres circling at 2.4 m/s at frame 20:
+# under the current sources' x0.95 solver damping they are far slower at
+# release than the recorded (undamped) revision's, so they land metres apart.
+GLB_RECORDED_DIFFERENCES = {"constraint-fixed": 916, "constraint-generic": 42, "constraint-generic-spring": 39,
+                            "constraint-hinge": 26, "constraint-motor": 81, "constraint-piston": 2,
+                            "constraint-point": 90, "constraint-slider": 21}
 
 
 @pytest.mark.gpu
@@ -211,10 +219,12 @@ def test_glb_case_against_reference_cuda(gpu_available, cid):
     the pm* driver: every checkpoint, body and constraint of the recorded
     CUDA result is produced with equal ids, types and flags (present,
     enabled, broken) and equal body, constraint and element counts, and the
-    state stays finite. Position, velocity and impulse values and contact
-    counts are reported against the recorded values (printed), not asserted:
-    the recorded results come from the earlier revision the analytic cases
-    show, and the runs diverge where contacts or limits engage."""
+    state stays finite. Values outside tolerance (printed with the largest
+    position deviation per checkpoint) may not exceed the counts this driver
+    produces today: the recorded results come from the earlier revision the
+    analytic cases show, and the runs diverge where contacts, limits or the
+    solver damping act. The contact-free piston case stays within tolerance
+    in every pose and velocity."""
     m, gs = _glb_fixture()[cid]
     result = conformance.run_case(m["case"], authored=gs)
     fails = conformance.compare(m["case"], m["golden"]["checkpoints"], result["checkpoints"], kinds=True)
@@ -233,3 +243,8 @@ def test_glb_case_against_reference_cuda(gpu_available, cid):
         print("  ", path, message)
     assert not structural, structural[:10]
     assert all(cp["invariants"]["finite"] for cp in result["checkpoints"])
+    assert len(numeric) <= GLB_RECORDED_DIFFERENCES[cid], len(numeric)
+    if cid == "constraint-piston":
+        # no contact in this scene: every pose and velocity is within the
+        # case's tolerance; only the reported applied impulse differs
+        assert all(path.endswith("applied_impulse") for path, _, _ in numeric), numeric
