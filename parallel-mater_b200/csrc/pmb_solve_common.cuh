@@ -79,7 +79,7 @@ __device__ __forceinline__ void apply_pose_update(const Dev& d, uint32_t i, cons
     d.dxa[i] = make_float4(2.0f * rel.x, 2.0f * rel.y, 2.0f * rel.z, 0.0f);
 }
 
-// Group-per-body primal: G lanes (G = 4, 8, 16 or 32) solve one body. Lanes
+// Group-per-body primal: G lanes (G = 8, 16 or 32) solve one body. Lanes
 // evaluate the body's contact rows G at a time (coalesced SoA loads) and
 // stage them in shared memory; each lane owns ceil(27/G) of the 27 entries of
 // the packed 6x6 block (21 Hessian, 6 gradient) and adds the staged rows to
@@ -97,9 +97,9 @@ __device__ __forceinline__ void apply_pose_update(const Dev& d, uint32_t i, cons
 // there shorten the critical path.
 template <int G> struct GroupRows {
     // Normal rows kept for the crossing safeguard (rows past them are
-    // evaluated again there): 32, or 16 for the 4-lane groups whose eight
-    // slots share a warp's staging area.
-    static constexpr uint32_t kSlots = G == 4 ? 16u : 32u;
+    // evaluated again there): 32 for 8-lane groups, 64 for the 16- and
+    // 32-lane groups of the heavy bodies (which fit the same staging area).
+    static constexpr uint32_t kSlots = G >= 16 ? 64u : 32u;
     // Chunk being accumulated: 3 rows of (jacobian[6], stiffness, force,
     // stiffness x jacobian[6]); the last six are the Hessian products' first
     // factors, formed once per row instead of once per entry.
@@ -108,10 +108,9 @@ template <int G> struct GroupRows {
     uint32_t flag[G];
     Blk jblk;  // the block while joint rows are added (joint_rows_shared)
 };
-// Per-warp staging area: eight 4-lane groups, four 8-lane groups, two
-// 16-lane groups or one 32-lane group.
-constexpr size_t kWarpStage = 8 * sizeof(GroupRows<4>) > 4 * sizeof(GroupRows<8>) ? 8 * sizeof(GroupRows<4>)
-                                                                                   : 4 * sizeof(GroupRows<8>);
+// Per-warp staging area: four 8-lane groups, two 16-lane groups or one
+// 32-lane group.
+constexpr size_t kWarpStage = 4 * sizeof(GroupRows<8>);
 static_assert(2 * sizeof(GroupRows<16>) <= kWarpStage && sizeof(GroupRows<32>) <= kWarpStage, "staging area");
 static_assert(32 * sizeof(Blk) <= kWarpStage, "a block slot per thread for the body-per-thread sweep");
 
@@ -146,6 +145,7 @@ template <int G> __device__ __forceinline__ void own_entries(const Blk& blk, int
 
 template <int G>
 __device__ __forceinline__ void accumulate_chunk(float* ent, int gl, const GroupRows<G>& sm, uint32_t m) {
+    static_assert(G <= 8 || G % 4 == 0, "wide groups take rows four at a time");
     // Products first (independent, pipelined loads), then the ordered adds.
 #pragma unroll
     for (int q = 0; q < Owned<G>::E; ++q) {
@@ -170,12 +170,24 @@ __device__ __forceinline__ void accumulate_chunk(float* ent, int gl, const Group
                 for (int x = 0; x < 3; ++x)
                     if (t < int(m)) ent[q] += prod[t][x];
         } else {
-            for (int t = 0; t < int(m); ++t)
+            // Four rows' products at a time (their loads in flight together),
+            // then their adds in row order; products of rows past m are
+            // formed from the slot's stale values and dropped.
+            for (int t0 = 0; t0 < int(m); t0 += 4) {
+                float prod[4][3];
 #pragma unroll
-                for (int x = 0; x < 3; ++x) {
-                    const float* row = sm.r[t][x];
-                    ent[q] += hess ? row[8 + ei] * row[ek] : row[ei] * row[7];
-                }
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int x = 0; x < 3; ++x) {
+                        const float* row = sm.r[t0 + u][x];
+                        prod[u][x] = hess ? row[8 + ei] * row[ek] : row[ei] * row[7];
+                    }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int x = 0; x < 3; ++x)
+                        if (t0 + u < int(m)) ent[q] += prod[u][x];
+            }
         }
     }
 }

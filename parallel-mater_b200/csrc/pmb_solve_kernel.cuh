@@ -76,9 +76,15 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
                 // inlined copy adds its own stack frame). The group learns its
                 // next body before solving the current one and fetches that
                 // body's record and row codes during the solve.
+                // Static assignment runs the rounds in alternating directions
+                // (round r: slot r x groups + rank, or its mirror when r is
+                // odd): the colour's bodies come heaviest class first, so a
+                // group that drew a heavy body early draws a light one next.
                 const bool dynamic = d.solve_policy == 3;
                 const uint32_t groups = nthreads / G;
-                uint32_t k = lo + (threadIdx.x / G) * gridDim.x + blockIdx.x;
+                const uint32_t rank = (threadIdx.x / G) * gridDim.x + blockIdx.x;
+                uint32_t round = 0;
+                uint32_t k = lo + rank;
                 if (dynamic) {
                     uint32_t t = 0;
                     if (gl == 0) t = atomicAdd(claim, 1u);
@@ -87,7 +93,8 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
                 Ahead ah{};
                 if (k < hi) ah = fetch_ahead<G>(d, k, gl);
                 while (k < hi) {
-                    uint32_t next = k + groups;
+                    ++round;
+                    uint32_t next = lo + round * groups + ((round & 1u) ? groups - 1u - rank : rank);
                     if (dynamic) {
                         uint32_t t = 0;
                         if (gl == 0) t = atomicAdd(claim, 1u);
