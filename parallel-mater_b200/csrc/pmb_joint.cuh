@@ -89,6 +89,16 @@ __device__ __forceinline__ void store_row(JointRow& s, const Row& r) {
     s.reference_force = r.reference_force;
 }
 
+// Residual contributions of a joint's hard rows in an advance visit: the
+// sum of squares, count, largest |C| and count above the tolerance, added
+// to the target's fields.
+struct JointRes {
+    double sq;
+    uint32_t n;
+    float mx;
+    uint32_t over;
+};
+
 struct JointCtx {
     JointRow* rows;
     const BodyView* A;
@@ -171,8 +181,7 @@ static __device__ void joint_row(JointCtx& c, const V6& ja, const V6& jb, float 
 // geometry_constraints.slang:715-926. prevA/prevB: start-of-tick poses.
 static __device__ float visit_joint(const Joint& o, JointRow* rows, const BodyView& A, const BodyView& B, V3 prev_xa,
                              Q4 prev_qa, V3 prev_xb, Q4 prev_qb, float4 pa0, float4 pb0, float dt, Blk* blk,
-                             bool first, unsigned visit, uint32_t* count_out, double* res_sq = nullptr,
-                             uint32_t* res_n = nullptr, float* res_max = nullptr, uint32_t* res_over = nullptr,
+                             bool first, unsigned visit, uint32_t* count_out, JointRes* res_out = nullptr,
                              float res_tol = 0.0f) {
     JointCtx c{rows, &A, &B, blk, 0u, 0.0f, first, visit, dt, 0.0, 0u, 0.0f, 0u, res_tol};
     V3 xa, xb;
@@ -290,10 +299,12 @@ static __device__ float visit_joint(const Joint& o, JointRow* rows, const BodyVi
         }
     }
     if (count_out) *count_out = c.index;
-    if (res_sq) *res_sq += c.res_sq;
-    if (res_n) *res_n += c.res_n;
-    if (res_max) *res_max = fmx(*res_max, c.res_max);
-    if (res_over) *res_over += c.res_over;
+    if (res_out) {
+        res_out->sq += c.res_sq;
+        res_out->n += c.res_n;
+        res_out->mx = fmx(res_out->mx, c.res_max);
+        res_out->over += c.res_over;
+    }
     return c.impulse;
 }
 

@@ -84,7 +84,8 @@ enum : uint32_t {
 };
 constexpr uint32_t kStagedGroups = 64;  // lane groups per CTA at most (512 threads, 8 lanes)
 constexpr size_t kStagedSmem =
-    size_t(kStageRows) * kRowWords * 4 + size_t(kBatchBodies) * 12 * 4 + 64 * 4 + kStagedGroups * sizeof(Blk);
+    size_t(kStageRows) * kRowWords * 4 + size_t(kBatchBodies) * 12 * 4 + 64 * 4 + kStagedGroups * sizeof(Blk) +
+    kStagedGroups * 2 * sizeof(BodyView);
 
 struct StageTables {
     float* rows;       // kStageRows x kRowWords
@@ -96,6 +97,7 @@ struct StageTables {
     float* invm;       // per batch slot: inverse mass
     uint32_t* scratch; // 64 words for scans and counts
     Blk* jblk;         // per lane group: the block while joint rows are added
+    BodyView* jview;   // per lane group: the visited joint's two bodies
 };
 __device__ __forceinline__ StageTables stage_tables(uint8_t* raw) {
     StageTables t;
@@ -109,6 +111,7 @@ __device__ __forceinline__ StageTables stage_tables(uint8_t* raw) {
     t.invm = t.fric + kBatchBodies;
     t.scratch = reinterpret_cast<uint32_t*>(t.invm + kBatchBodies);
     t.jblk = reinterpret_cast<Blk*>(t.scratch + 64);
+    t.jview = reinterpret_cast<BodyView*>(t.jblk + kStagedGroups);
     return t;
 }
 
@@ -333,7 +336,8 @@ __device__ void staged_body(const Dev& d, const StageTables& tb, uint32_t sl, ui
     Blk blk;
     gather_block<G>(ent, blk, gmask, gbase);
     const uint32_t jcnt = d.jdeg[i];
-    if (jcnt) joint_rows_shared<G>(d, i, phase, dt, blk, tb.jblk + threadIdx.x / G, gmask, gl);
+    if (jcnt) joint_rows_shared<G>(d, i, phase, dt, blk, tb.jblk + threadIdx.x / G, tb.jview + 2 * (threadIdx.x / G),
+                                        gmask, gl);
     V6 upd;
     const bool solved = block_solve(blk, upd);
     V6 dxn = dx0;

@@ -106,13 +106,20 @@ template <int G> struct GroupRows {
     float r[G][3][14];
     float nrow[kSlots][8];  // normal row: jacobian[6], raw penalty, trial force
     uint32_t flag[G];
-    Blk jblk;  // the block while joint rows are added (joint_rows_shared)
+    Blk jblk;            // the block while joint rows are added (joint_rows_shared)
+    BodyView jview[2];   // the joint's two bodies during its visit
 };
 // Per-warp staging area: four 8-lane groups, two 16-lane groups or one
 // 32-lane group.
 constexpr size_t kWarpStage = 4 * sizeof(GroupRows<8>);
 static_assert(2 * sizeof(GroupRows<16>) <= kWarpStage && sizeof(GroupRows<32>) <= kWarpStage, "staging area");
-static_assert(32 * sizeof(Blk) <= kWarpStage, "a block slot per thread for the body-per-thread sweep");
+// Per-thread slots of the body-per-thread sweep and the dual pass: a block,
+// a joint's two body views and its residual contributions, in shared memory
+// so the joint visit (a call) reads them there rather than from local memory.
+constexpr size_t kThreadViews = 32 * sizeof(Blk);
+constexpr size_t kThreadJointRes = kThreadViews + 64 * sizeof(BodyView);
+static_assert(kThreadViews % 8 == 0 && kThreadJointRes % 8 == 0, "slot alignment");
+static_assert(kThreadJointRes + 32 * sizeof(JointRes) <= kWarpStage, "per-thread joint slots");
 
 __device__ __forceinline__ void entry_ik(int e, int& i, int& k) {
     i = e >= 15 ? 5 : e >= 10 ? 4 : e >= 6 ? 3 : e >= 3 ? 2 : e >= 1 ? 1 : 0;
@@ -332,7 +339,7 @@ __device__ __forceinline__ Ahead fetch_ahead(const Dev& d, uint32_t k, int gl) {
 // address (which would put it in local memory for every body).
 template <int G>
 __device__ __forceinline__ void joint_rows_shared(const Dev& d, uint32_t i, uint32_t phase, float dt, Blk& blk,
-                                                  Blk* sb, uint32_t gmask, int gl) {
+                                                  Blk* sb, BodyView* views, uint32_t gmask, int gl) {
     if (gl == 0) {
         *sb = blk;
         const uint32_t jcnt = d.jdeg[i], jlo = d.jinc_off[i];
@@ -343,9 +350,10 @@ __device__ __forceinline__ void joint_rows_shared(const Dev& d, uint32_t i, uint
             const uint32_t a = js.dense_a, b = js.dense_b;
             const bool first = i == a;
             if (phase == 0) {
-                BodyView A = load_body(d, a), B = load_body(d, b);
-                visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]),
-                            q4(d.q[b]), d.p0[a], d.p0[b], dt, sb, first, kVisitAccumulate, nullptr);
+                views[0] = load_body(d, a);
+                views[1] = load_body(d, b);
+                visit_joint(d.joints[j], d.jrows + size_t(j) * 18, views[0], views[1], v3(d.x[a]), q4(d.q[a]),
+                            v3(d.x[b]), q4(d.q[b]), d.p0[a], d.p0[b], dt, sb, first, kVisitAccumulate, nullptr);
             } else {
                 const Lite A = load_lite(d, a), B = load_lite(d, b);
                 for (uint32_t r = 0; r < js.count; ++r) {
@@ -445,7 +453,7 @@ __device__ void solve_body_group(const Dev& d, Ahead& ah, uint32_t kn, uint32_t 
     gather_block<G>(ent, blk, gmask, gbase);
     mark(1);
     if constexpr (Joints) {
-        if (d.jdeg[i]) joint_rows_shared<G>(d, i, phase, dt, blk, &sm.jblk, gmask, gl);
+        if (d.jdeg[i]) joint_rows_shared<G>(d, i, phase, dt, blk, &sm.jblk, sm.jview, gmask, gl);
     }
     V6 upd;
     if (!block_solve(blk, upd)) return;
@@ -519,7 +527,7 @@ __device__ __forceinline__ void load_normal_rows(const Dev& d, uint32_t c, V6& j
     jb = {{b4.z, b4.w, b5.x, b5.y, b5.z, b5.w}};
 }
 template <bool Joints>
-__device__ void solve_body_thread(const Dev& d, uint32_t i, uint32_t phase, float dt, Blk* sb) {
+__device__ void solve_body_thread(const Dev& d, uint32_t i, uint32_t phase, float dt, Blk* sb, BodyView* views) {
     const Lite me = load_lite(d, i);
     const float my_friction = d.p1[i].x;
     const uint32_t ro = d.roff[i], rn = d.rcount[i];
@@ -591,9 +599,10 @@ __device__ void solve_body_thread(const Dev& d, uint32_t i, uint32_t phase, floa
                 const uint32_t a = js.dense_a, b = js.dense_b;
                 const bool first = i == a;
                 if (phase == 0) {
-                    BodyView A = load_body(d, a), B = load_body(d, b);
-                    visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]),
-                                q4(d.q[b]), d.p0[a], d.p0[b], dt, sb, first, kVisitAccumulate, nullptr);
+                    views[0] = load_body(d, a);
+                    views[1] = load_body(d, b);
+                    visit_joint(d.joints[j], d.jrows + size_t(j) * 18, views[0], views[1], v3(d.x[a]), q4(d.q[a]),
+                                v3(d.x[b]), q4(d.q[b]), d.p0[a], d.p0[b], dt, sb, first, kVisitAccumulate, nullptr);
                 } else {
                     const Lite A = load_lite(d, a), B = load_lite(d, b);
                     for (uint32_t r = 0; r < js.count; ++r) {
@@ -715,7 +724,10 @@ static __device__ void dual_contact(const Dev& d, uint32_t c, float dt, uint32_t
     }
 }
 
-static __device__ void dual_joint(const Dev& d, uint32_t j, uint32_t phase, float dt, Res& res, uint32_t it) {
+// slots: this thread's two body views and joint residual in shared memory
+// (nullptr: local ones, for kernels without the per-thread slots).
+static __device__ void dual_joint(const Dev& d, uint32_t j, uint32_t phase, float dt, Res& res, uint32_t it,
+                                  BodyView* views = nullptr, JointRes* jres = nullptr) {
     JointState js = d.jstate[j];
     if (js.count == 0 || !js.enabled) return;
     const uint32_t a = js.dense_a, b = js.dense_b;
@@ -730,20 +742,23 @@ static __device__ void dual_joint(const Dev& d, uint32_t j, uint32_t phase, floa
     }
     float impulse = 0.0f;
     if (phase == 0) {
-        BodyView A = load_body(d, a), B = load_body(d, b);
-        Blk scratch;
-        // A batched world also needs this joint's own residual for its scene.
-        Res jr{0.0, 0u, 0.0f, 0u, res.tol};
-        Res& sink = batched(d) ? jr : res;
-        impulse = visit_joint(d.joints[j], d.jrows + size_t(j) * 18, A, B, v3(d.x[a]), q4(d.q[a]), v3(d.x[b]),
-                              q4(d.q[b]), d.p0[a], d.p0[b], dt, &scratch, true, kVisitAdvance, nullptr, &sink.sq,
-                              &sink.n, &sink.mx, &sink.over, sink.tol);
-        if (batched(d)) {
-            res.sq += jr.sq;
-            res.n += jr.n;
-            res.mx = fmx(res.mx, jr.mx);
-            res.over += jr.over;
-        }
+        BodyView local_views[2];
+        JointRes local_res;
+        BodyView* v = views ? views : local_views;
+        JointRes* out = jres ? jres : &local_res;
+        v[0] = load_body(d, a);
+        v[1] = load_body(d, b);
+        *out = JointRes{0.0, 0u, 0.0f, 0u};
+        // An advance visit leaves the block alone (no block pointer).
+        impulse = visit_joint(d.joints[j], d.jrows + size_t(j) * 18, v[0], v[1], v3(d.x[a]), q4(d.q[a]), v3(d.x[b]),
+                              q4(d.q[b]), d.p0[a], d.p0[b], dt, nullptr, true, kVisitAdvance, nullptr, out, res.tol);
+        // The joint's own residual (a batched world also needs it per scene),
+        // added in the same order as a running sum would.
+        const JointRes jr = *out;
+        res.sq += jr.sq;
+        res.n += jr.n;
+        res.mx = fmx(res.mx, jr.mx);
+        res.over += jr.over;
         if (scene_last && jr.n) {
             atomicAdd(&d.scene_res_sq[scene], float(jr.sq));
             atomicAdd(&d.scene_res_n[scene], jr.n);

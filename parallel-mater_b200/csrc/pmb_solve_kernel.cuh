@@ -128,11 +128,12 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
                 // consecutive CTAs, as for the groups.
                 if constexpr (kThread) {
                     Blk* slot = reinterpret_cast<Blk*>(warp_stage) + lane;
+                    BodyView* views = reinterpret_cast<BodyView*>(warp_stage + kThreadViews) + 2 * lane;
                     for (uint32_t k = b0 + threadIdx.x * gridDim.x + blockIdx.x; k < b1; k += nthreads) {
                         const uint32_t i = d.corder[k];
                         if (phase != 0 && d.impact[i] == 0) continue;
                         if (batched(d) && it >= d.scene_budget[d.scene_of[i]]) continue;
-                        solve_body_thread<kJoints>(d, i, phase, dt, slot);
+                        solve_body_thread<kJoints>(d, i, phase, dt, slot, views);
                     }
                 }
                 r32 = r16 = r8 = b0;
@@ -159,8 +160,12 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
         }
         Res res{0.0, 0u, 0.0f, 0u, sp.tolerance};
         for (uint32_t k = grid_stride_begin(); k < n_con; k += grid_stride()) dual_contact(d, k, dt, phase, res, it);
-        if constexpr (kJoints)
-            for (uint32_t j = grid_stride_begin(); j < d.nj; j += grid_stride()) dual_joint(d, j, phase, dt, res, it);
+        if constexpr (kJoints) {
+            BodyView* views = reinterpret_cast<BodyView*>(warp_stage + kThreadViews) + 2 * lane;
+            JointRes* jres = reinterpret_cast<JointRes*>(warp_stage + kThreadJointRes) + lane;
+            for (uint32_t j = grid_stride_begin(); j < d.nj; j += grid_stride())
+                dual_joint(d, j, phase, dt, res, it, views, jres);
+        }
         // Deterministic reduction: warp tree, warps in order, blocks in order.
         block_residual<kSolveThreads>(res, wsq, wn, wmx, wov, c, blockIdx.x);
         if (timing && it == 0 && threadIdx.x == 0) atomicMax(&c->dbg_work[19], now());
