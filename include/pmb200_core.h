@@ -375,9 +375,10 @@ PMB_API int pmb_world_mlp_attach(pmb_world* world, const float* params, uint32_t
 /* What learned ticks take from the predictor: bit 0 the normal lambda, bit 1
  * the normal penalty, bit 2 lambda corrections averaged over each
  * manifold's points (keeping the carried-over split of the pair's force).
- * Default 2 (penalty only): on the settled 65,536-box pile the predicted
- * penalty cuts the sweeps to the residual tolerance while predicted lambdas,
- * per point or averaged, add sweeps. */
+ * Default 3 (lambda and penalty per point): on the settled 65,536-box pile,
+ * under the 99.9th-percentile residual rule, the predicted lambda and
+ * penalty take a quarter of the sweeps off the plain warm start's, the
+ * penalty alone a tenth. */
 PMB_API int pmb_world_mlp_apply_mode(pmb_world* world, uint32_t mode);
 /* Online training: when enabled, every tick ends with steps_per_tick Adam
  * steps (learning_rate) on that tick's contacts, target = the converged

@@ -94,7 +94,7 @@ struct pmb_world {
         uint32_t steps_per_tick{1}, grid{};
         uint64_t adam_t{};
         float *params{}, *m{}, *v{}, *grad{}, *partial{}, *gate{}, *out{};
-        uint32_t mode{2};
+        uint32_t mode{3};
         uint8_t *img{}, *x{};
         MlpMeta* meta{};
         std::vector<void*> allocs;
