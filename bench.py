@@ -184,7 +184,8 @@ def reference_arm(args):
     value, stats = cpu_baseline(scene, desc, ticks, warm=args.warmup)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
-        "steps": ticks, "warmup": 0, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
+        "steps": ticks, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "box pile 64x32x32 (65,536 boxes), settled state, residual-driven AVBD",
                    "bodies": scene.n, "tolerance": args.tolerance, "residual_norm": args.residual_norm,
