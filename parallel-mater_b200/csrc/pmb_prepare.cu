@@ -469,18 +469,26 @@ __global__ void k_color_count(Dev d) {
     for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
         if (d.motion[i] != kDynamic) continue;
         const uint32_t col = d.color[i];
-        atomicAdd(&d.ctr->color_count[col * kWidthClasses + width_class(d.rcount[i])], 1u);
+        atomicAdd(&d.ctr->color_count[col * kSortClasses + sort_class(d.rcount[i])], 1u);
         atomicMax(&d.ctr->colors, col + 1);
     }
 }
 
-// Exclusive scan of the bucket counts (one block); counts become cursors.
-constexpr uint32_t kBuckets = kMaxColors * kWidthClasses;
+// Exclusive scan of the bucket counts (one block, kPer consecutive buckets
+// per thread); counts become cursors.
+constexpr uint32_t kBuckets = kMaxColors * kSortClasses;
+constexpr uint32_t kPer = (kBuckets + 1023) / 1024;
 __global__ void __launch_bounds__(1024) k_color_offsets(Dev d) {
     __shared__ uint32_t part[32];
     const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const uint32_t v = t < kBuckets ? d.ctr->color_count[t] : 0u;
-    uint32_t x = v;
+    uint32_t v[kPer], sum = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; ++k) {
+        const uint32_t b = t * kPer + k;
+        v[k] = b < kBuckets ? d.ctr->color_count[b] : 0u;
+        sum += v[k];
+    }
+    uint32_t x = sum;
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= uint32_t(o)) x += y;
@@ -496,18 +504,23 @@ __global__ void __launch_bounds__(1024) k_color_offsets(Dev d) {
         part[lane] = p;
     }
     __syncthreads();
-    const uint32_t incl = x + (warp ? part[warp - 1] : 0u);
-    if (t < kBuckets) {
-        d.ctr->color_off[t] = incl - v;
-        d.ctr->color_count[t] = 0;
+    uint32_t run = x - sum + (warp ? part[warp - 1] : 0u);  // exclusive prefix of this thread's first bucket
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; ++k) {
+        const uint32_t b = t * kPer + k;
+        if (b < kBuckets) {
+            d.ctr->color_off[b] = run;
+            d.ctr->color_count[b] = 0;
+        }
+        run += v[k];
+        if (b == kBuckets - 1) d.ctr->color_off[kBuckets] = run;
     }
-    if (t == kBuckets - 1) d.ctr->color_off[kBuckets] = incl;
 }
 
 __global__ void k_color_scatter(Dev d) {
     for (uint32_t i = grid_stride_begin(); i < d.n; i += grid_stride()) {
         if (d.motion[i] != kDynamic) continue;
-        const uint32_t b = d.color[i] * kWidthClasses + width_class(d.rcount[i]);
+        const uint32_t b = d.color[i] * kSortClasses + sort_class(d.rcount[i]);
         const uint32_t slot = d.ctr->color_off[b] + atomicAdd(&d.ctr->color_count[b], 1u);
         d.corder[slot] = i;
         d.crec[slot] = make_uint4(i, d.roff[i], d.rcount[i], 0u);
@@ -558,7 +571,7 @@ void launch_graph(const Dev& d, const StepParams& sp, cudaStream_t s, int coop_b
     prof_mark(s, "colour fixpoint");
     k_color_count<<<blocks_for(d.n), kBlock, 0, s>>>(d);
     note_launch(blocks_for(d.n));
-    static_assert(kBuckets <= 1024, "bucket scan is one block");
+    static_assert(kPer * 1024 >= kBuckets, "bucket scan is one block");
     k_color_offsets<<<1, 1024, 0, s>>>(d);
     note_launch(1);
     k_color_scatter<<<blocks_for(d.n), kBlock, 0, s>>>(d);

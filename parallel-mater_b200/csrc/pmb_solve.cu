@@ -82,6 +82,7 @@ enum : uint32_t {
                       // here; bit 2: the row crosses (crossing safeguard, set by the body's group)
     kRowWords = 43,   // odd: consecutive rows start in different shared-memory banks
 };
+static_assert(sizeof(GroupRows<32>) <= size_t(kStageRows) * kRowWords * 4, "oversized-body rows fit the stage");
 constexpr uint32_t kStagedGroups = 64;  // lane groups per CTA at most (512 threads, 8 lanes)
 constexpr size_t kStagedSmem =
     size_t(kStageRows) * kRowWords * 4 + size_t(kBatchBodies) * 12 * 4 + 64 * 4 + kStagedGroups * sizeof(Blk) +
@@ -249,7 +250,8 @@ __device__ void owned_contact_duals(const Dev& d, uint32_t i, uint32_t col, floa
         const uint32_t other = d.bother[ro + r];
         const uint32_t ocol = d.color[other];
         if (!(ocol == kInvalid || ocol < col)) continue;
-        dual_contact(d, d.blist[ro + r] & 0x7fffffffu, dt, phase, res, it);
+        const uint32_t c = d.blist[ro + r] & 0x7fffffffu;
+        dual_contact(d, c, d.c_bodies[c], dt, phase, res, it);
     }
 }
 
@@ -468,7 +470,7 @@ __global__ void __launch_bounds__(T, 1) k_solve_staged(Dev d, StepParams sp, uin
         const uint32_t parity = (it & 1u) * 512u;
         for (uint32_t col = 0; col <= colors; ++col) {
             if (col < colors) {
-                const uint32_t lo = c->color_off[col * kWidthClasses], hi = c->color_off[(col + 1) * kWidthClasses];
+                const uint32_t lo = c->color_off[col * kSortClasses], hi = c->color_off[(col + 1) * kSortClasses];
                 const uint32_t span = hi - lo;
                 const uint32_t mine = span > blockIdx.x ? (span - blockIdx.x + gridDim.x - 1) / gridDim.x : 0u;
                 for (uint32_t j0 = 0; j0 < mine;) {

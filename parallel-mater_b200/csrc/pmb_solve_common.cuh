@@ -95,20 +95,41 @@ __device__ __forceinline__ void apply_pose_update(const Dev& d, uint32_t i, cons
 // The tail colours of a pile hold few but heavily loaded bodies (tens of
 // rows), and a colour ends when its slowest body does, so wider groups
 // there shorten the critical path.
-template <int G> struct GroupRows {
+//
+// Shared-memory banks: the groups of a warp run in step, so their accesses
+// share instructions. A lane's slot is 43 words (odd) and a normal row 9, so
+// the lanes of a group write to distinct banks modulo 8; groups start 8, 16
+// or 24 banks apart, so the four 8-lane (two 16-lane) groups of a warp
+// neither collide on those writes nor on the row reads of the accumulation
+// (each group reads within a 14-word row).
+constexpr int kRowStride = 14;  // words of one staged row
+constexpr int kSlotWords = 43;  // a lane's three rows (42 words) and a pad word
+template <int G> struct GroupRowsData {
     // Normal rows kept for the crossing safeguard (rows past them are
     // evaluated again there): 32 for 8-lane groups, 64 for the 16- and
     // 32-lane groups of the heavy bodies (which fit the same staging area).
     static constexpr uint32_t kSlots = G >= 16 ? 64u : 32u;
-    // Chunk being accumulated: 3 rows of (jacobian[6], stiffness, force,
-    // stiffness x jacobian[6]); the last six are the Hessian products' first
-    // factors, formed once per row instead of once per entry.
-    float r[G][3][14];
-    float nrow[kSlots][8];  // normal row: jacobian[6], raw penalty, trial force
+    // Chunk being accumulated: per lane slot 3 rows of (jacobian[6],
+    // stiffness, force, stiffness x jacobian[6]); the last six are the
+    // Hessian products' first factors, formed once per row instead of once
+    // per entry.
+    float r[G][kSlotWords];
+    float nrow[kSlots][9];  // normal row: jacobian[6], raw penalty, trial force (and a pad word)
     uint32_t flag[G];
     Blk jblk;            // the block while joint rows are added (joint_rows_shared)
     BodyView jview[2];   // the joint's two bodies during its visit
 };
+template <int G> struct GroupRows : GroupRowsData<G> {
+    // Pads the group to 24 banks mod 32 (8 lanes: bases 0, 24, 16, 8) or 16
+    // (16 lanes: bases 0, 16).
+    static constexpr int kWords = int(sizeof(GroupRowsData<G>) / 4);
+    static constexpr int kTarget = G == 8 ? 24 : G == 16 ? 16 : kWords % 32;
+    static constexpr int kPad = (kTarget - kWords % 32 + 32) % 32;
+    float pad[kPad == 0 ? 32 : kPad];
+    __device__ __forceinline__ float* row(int slot, int x) { return &this->r[slot][kRowStride * x]; }
+    __device__ __forceinline__ const float* row(int slot, int x) const { return &this->r[slot][kRowStride * x]; }
+};
+static_assert(sizeof(GroupRows<8>) / 4 % 32 == 24 && sizeof(GroupRows<16>) / 4 % 32 == 16, "group bank offsets");
 // Per-warp staging area: four 8-lane groups, two 16-lane groups or one
 // 32-lane group.
 constexpr size_t kWarpStage = 4 * sizeof(GroupRows<8>);
@@ -168,7 +189,7 @@ __device__ __forceinline__ void accumulate_chunk(float* ent, int gl, const Group
             for (int t = 0; t < G; ++t)
 #pragma unroll
                 for (int x = 0; x < 3; ++x) {
-                    const float* row = sm.r[t][x];
+                    const float* row = sm.row(t, x);
                     prod[t][x] = hess ? row[8 + ei] * row[ek] : row[ei] * row[7];
                 }
 #pragma unroll
@@ -186,7 +207,7 @@ __device__ __forceinline__ void accumulate_chunk(float* ent, int gl, const Group
                 for (int u = 0; u < 4; ++u)
 #pragma unroll
                     for (int x = 0; x < 3; ++x) {
-                        const float* row = sm.r[t0 + u][x];
+                        const float* row = sm.row(t0 + u, x);
                         prod[u][x] = hess ? row[8 + ei] * row[ek] : row[ei] * row[7];
                     }
 #pragma unroll
@@ -293,12 +314,13 @@ __device__ __forceinline__ void stage_loaded(const Dev& d, const Lite& me, float
         V6 row;
 #pragma unroll
         for (int k = 0; k < 6; ++k) row.v[k] = first ? ja[x].v[k] : jb[x].v[k];
+        float* out = sm.row(slot, x);
 #pragma unroll
-        for (int k = 0; k < 6; ++k) sm.r[slot][x][k] = row.v[k];
-        sm.r[slot][x][6] = st[x];
-        sm.r[slot][x][7] = forces[x];
+        for (int k = 0; k < 6; ++k) out[k] = row.v[k];
+        out[6] = st[x];
+        out[7] = forces[x];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) sm.r[slot][x][8 + k] = st[x] * row.v[k];  // = (stiffness x J_i), as before
+        for (int k = 0; k < 6; ++k) out[8 + k] = st[x] * row.v[k];  // = (stiffness x J_i), as before
     }
 }
 template <int G>
@@ -675,9 +697,10 @@ __device__ __forceinline__ void res_add(Res& r, float v) {
 }
 
 // advance_duals for one contact point (geometry_constraints_solve.slang:
-// 494-532; the last-iteration block runs in k_contact_finalize).
-static __device__ void dual_contact(const Dev& d, uint32_t c, float dt, uint32_t phase, Res& res, uint32_t it) {
-    const uint2 ab = d.c_bodies[c];
+// 494-532; the last-iteration block runs in k_contact_finalize). ab: the
+// contact's bodies (c_bodies[c]), loaded by the caller ahead of time.
+static __device__ void dual_contact(const Dev& d, uint32_t c, uint2 ab, float dt, uint32_t phase, Res& res,
+                                    uint32_t it) {
     const uint32_t a = ab.x, b = ab.y;
     if (phase != 0 && d.impact[a] == 0 && d.impact[b] == 0) return;
     // Batched worlds: a scene past its budget is finished; its last sweep

@@ -52,8 +52,8 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
     if (timing && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_start = now();
     for (uint32_t it = 0; it < iters; ++it) {
         for (uint32_t col = 0; col < colors; ++col) {
-            const uint32_t* off = c->color_off + col * kWidthClasses;
-            const uint32_t b0 = off[0], b1 = off[kWidthClasses];
+            const uint32_t* off = c->color_off + col * kSortClasses;
+            const uint32_t b0 = off[0], b1 = off[kSortClasses];
             const uint32_t nb = b1 - b0;
             const uint32_t trace = !timing || it != 0 ? 0u : col + 1 == colors ? 1u : col == 0 ? 2u : 0u;
             // Bodies [lo, hi) with G lanes each. Consecutive bodies go to
@@ -140,8 +140,8 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
             } else if (d.solve_policy != 1 && nb * 32u <= nthreads) {
                 r32 = r16 = r8 = b1;
             } else if (d.solve_policy == 2) {
-                r32 = off[1];
-                r16 = off[2];
+                r32 = off[kClass16];
+                r16 = off[kClass8];
                 r8 = b1;
             } else if ((d.solve_policy == 0 || d.solve_policy >= 3) && nb * 16u <= nthreads) {
                 r16 = r8 = b1;
@@ -159,7 +159,19 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
             if (timing && it == 0 && col < 18 && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_release[col] = now();
         }
         Res res{0.0, 0u, 0.0f, 0u, sp.tolerance};
-        for (uint32_t k = grid_stride_begin(); k < n_con; k += grid_stride()) dual_contact(d, k, dt, phase, res, it);
+        {
+            // Each contact's bodies are loaded one contact ahead, so a
+            // contact's body and row loads go out together.
+            uint32_t k = grid_stride_begin();
+            uint2 ab = k < n_con ? d.c_bodies[k] : make_uint2(0u, 0u);
+            while (k < n_con) {
+                const uint32_t kn = k + grid_stride();
+                const uint2 abn = kn < n_con ? d.c_bodies[kn] : make_uint2(0u, 0u);
+                dual_contact(d, k, ab, dt, phase, res, it);
+                ab = abn;
+                k = kn;
+            }
+        }
         if constexpr (kJoints) {
             BodyView* views = reinterpret_cast<BodyView*>(warp_stage + kThreadViews) + 2 * lane;
             JointRes* jres = reinterpret_cast<JointRes*>(warp_stage + kThreadJointRes) + lane;

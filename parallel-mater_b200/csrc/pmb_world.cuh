@@ -25,10 +25,20 @@ constexpr uint32_t kQueryLanes = 8;  // broadphase query lanes per body
 // The colour fixpoint runs one 1024-thread CTA per SM: its ~30 rounds are
 // two grid barriers each, and a barrier's cost grows with the CTA count.
 constexpr int kColorThreads = 1024;
-// Width classes of a colour's bodies by contact rows: more than 16 rows
-// (class 0, 32 lanes), 9-16 (class 1, 16 lanes), at most 8 (class 2, 8 lanes).
-constexpr uint32_t kWidthClasses = 3;
-__host__ __device__ inline uint32_t width_class(uint32_t rows) { return rows > 16u ? 0u : rows > 8u ? 1u : 2u; }
+// Sort classes of a colour's bodies by the length of their row lists,
+// heaviest first, in steps of 8 rows (an 8-lane group stages 8 rows at a
+// time): more than 40, 33-40, 25-32, 17-24, 9-16, at most 8. A colour phase
+// ends with its slowest lane group, and the static assignment deals the
+// colour's bodies out in rounds of alternating direction, so with the bodies
+// in this order a group that draws a heavy body in one round draws a light
+// one in the next. The lane widths of solve policy 2 take unions of them:
+// more than 16 rows (classes 0-3) 32 lanes, 9-16 (class kClass16) 16 lanes,
+// at most 8 (class kClass8) 8 lanes.
+constexpr uint32_t kSortClasses = 6;
+constexpr uint32_t kClass16 = 4, kClass8 = 5;
+__host__ __device__ inline uint32_t sort_class(uint32_t rows) {
+    return rows > 40u ? 0u : rows > 32u ? 1u : rows > 24u ? 2u : rows > 16u ? 3u : rows > 8u ? kClass16 : kClass8;
+}
 constexpr uint32_t kMaxIterations = 256;
 constexpr int kBlock = 256;
 
@@ -55,9 +65,9 @@ struct Counters {
     uint32_t n_mesh;      // candidates left for the triangle-mesh path
     uint32_t n_mesh_leaves, n_mesh_items;  // their overlapping leaf pairs and triangle-pair items
     uint32_t claim[2];    // solve policy 3: next unclaimed body of the colour (alternating)
-    // Bodies bucketed by (colour, width class): bucket col * kWidthClasses + k.
-    uint32_t color_count[kMaxColors * kWidthClasses];
-    uint32_t color_off[kMaxColors * kWidthClasses + 1];
+    // Bodies bucketed by (colour, sort class): bucket col * kSortClasses + k.
+    uint32_t color_count[kMaxColors * kSortClasses];
+    uint32_t color_off[kMaxColors * kSortClasses + 1];
     float residual_trace[kMaxIterations];
     double res_sum[1024];  // per-block partial residual sums of the latest dual pass
     uint32_t res_cnt[1024];
