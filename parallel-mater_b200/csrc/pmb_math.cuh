@@ -194,6 +194,15 @@ PMB_HD F3 stiffness_scales(F3 t, float mu) {
     return {t.n > 0.0f ? 1.0f : 0.0f, s, s};
 }
 
+// project_contact and stiffness_scales of one trial force: they share the
+// friction scale (same inputs), evaluated once.
+PMB_HD void project_with_scales(F3 t, float mu, F3& f, F3& sc) {
+    const float n = fmx(t.n, 0.0f);
+    const float s = friction_scale(t.t0, t.t1, mu * n);
+    f = {n, t.t0 * s, t.t1 * s};
+    sc = {t.n > 0.0f ? 1.0f : 0.0f, s, s};
+}
+
 struct V6 { float v[6]; };
 PMB_HD float dot6(const V6& a, const V6& b) {
     float r = 0.0f;

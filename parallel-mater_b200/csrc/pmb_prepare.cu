@@ -536,7 +536,7 @@ void launch_prepare(const Dev& d, const StepParams& sp, cudaStream_t s) {
         k_prepare_joints<<<blocks_for(d.nj, 64), 64, 0, s>>>(d, sp);
         note_launch(blocks_for(d.nj, 64));
     }
-    launch_contact_jacobians(d, 0, s);
+    launch_contact_jacobians(d, 0, sp.dt, s);
     prof_mark(s, "prepare");
 }
 

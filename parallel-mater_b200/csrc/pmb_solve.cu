@@ -14,7 +14,11 @@
 
 namespace pmb {
 
-__global__ void k_contact_jacobians(Dev d, uint32_t phase) {
+// The velocity phase also forms each contact's force offsets (the row
+// forces are the projected trial forces less them): the normal impulse and
+// the accumulated friction of the position phase, both fixed by then
+// (k_contact_finalize), over dt.
+__global__ void k_contact_jacobians(Dev d, uint32_t phase, float dt) {
     if (phase != 0 && d.ctr->impact == 0) return;
     const uint32_t n_con = d.ctr->n_contacts;
     for (uint32_t c = grid_stride_begin(); c < n_con; c += grid_stride()) {
@@ -33,10 +37,16 @@ __global__ void k_contact_jacobians(Dev d, uint32_t phase) {
         float4* p = d.c_jac + size_t(c) * 9;
 #pragma unroll
         for (int k = 0; k < 9; ++k) p[k] = make_float4(f[4 * k], f[4 * k + 1], f[4 * k + 2], f[4 * k + 3]);
+        if (phase != 0) {
+            V3 t0, t1;
+            basis(v3(d.c_n[c]), t0, t1);
+            const V3 af = v3(d.c_accf[c]);
+            d.c_foff[c] = make_float4(d.c_lam[c].w / dt, dot(af, t0) / dt, dot(af, t1) / dt, 0.0f);
+        }
     }
 }
-void launch_contact_jacobians(const Dev& d, uint32_t phase, cudaStream_t s) {
-    k_contact_jacobians<<<cap_blocks(d.cap_contact), kBlock, 0, s>>>(d, phase);
+void launch_contact_jacobians(const Dev& d, uint32_t phase, float dt, cudaStream_t s) {
+    k_contact_jacobians<<<cap_blocks(d.cap_contact), kBlock, 0, s>>>(d, phase, dt);
     note_launch(cap_blocks(d.cap_contact));
 }
 
@@ -152,16 +162,14 @@ __device__ __forceinline__ void stage_row(const Dev& d, const StageTables& tb, u
         }
     }
     const F3 trial{lam.x + pen.x * err[0], lam.y + pen.y * err[1], lam.z + pen.z * err[2]};
-    const F3 f = project_contact(trial, friction);
-    const F3 sc = stiffness_scales(trial, friction);
+    F3 f, sc;
+    project_with_scales(trial, friction, f, sc);
     float forces[3] = {f.n, f.t0, f.t1};
     if (phase != 0) {
-        V3 t0, t1;
-        basis(v3(d.c_n[c]), t0, t1);
-        const V3 af = v3(d.c_accf[c]);
-        forces[0] = f.n - lam.w / dt;
-        forces[1] = f.t0 - dot(af, t0) / dt;
-        forces[2] = f.t1 - dot(af, t1) / dt;
+        const float4 fo = d.c_foff[c];
+        forces[0] = f.n - fo.x;
+        forces[1] = f.t0 - fo.y;
+        forces[2] = f.t1 - fo.z;
     }
     float* row = tb.rows + size_t(t) * kRowWords;
 #pragma unroll
@@ -975,7 +983,7 @@ void launch_solve_all(const Dev& d, const StepParams& sp, cudaStream_t s, const 
             note_launch(cap_blocks(d.cap_pair));
             k_impact_bodies<<<blocks_for(d.n), kBlock, 0, s>>>(d, o.ox, o.oq, o.ov, o.ow);
             note_launch(blocks_for(d.n));
-            launch_contact_jacobians(d, 1, s);
+            launch_contact_jacobians(d, 1, sp.dt, s);
             k_impact_constraints<<<pb, kBlock, 0, s>>>(d, sp, o.ov, o.ow);
             note_launch(pb);
             prof_mark(s, "impact setup");

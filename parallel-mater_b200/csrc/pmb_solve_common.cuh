@@ -295,16 +295,14 @@ __device__ __forceinline__ void stage_loaded(const Dev& d, const Lite& me, float
         sm.nrow[nslot][7] = trial.n;
     }
     if (slot < 0) return;
-    F3 f = project_contact(trial, friction);
-    F3 sc = stiffness_scales(trial, friction);
+    F3 f, sc;
+    project_with_scales(trial, friction, f, sc);
     float forces[3] = {f.n, f.t0, f.t1};
     if (phase != 0) {
-        V3 t0, t1;
-        basis(v3(d.c_n[c]), t0, t1);
-        const V3 af = v3(d.c_accf[c]);
-        forces[0] = f.n - lam.w / dt;
-        forces[1] = f.t0 - dot(af, t0) / dt;
-        forces[2] = f.t1 - dot(af, t1) / dt;
+        const float4 fo = d.c_foff[c];
+        forces[0] = f.n - fo.x;
+        forces[1] = f.t0 - fo.y;
+        forces[2] = f.t1 - fo.z;
     }
     const float st[3] = {pen.x * sc.n, pen.y * sc.t0, pen.z * sc.t1};
 #pragma unroll
@@ -588,16 +586,14 @@ __device__ void solve_body_thread(const Dev& d, uint32_t i, uint32_t phase, floa
         float err[3];
         contact_rows(d, c, d.c_e[c], A, B, ja, jb, err);
         const F3 trial{lam.x + pen.x * err[0], lam.y + pen.y * err[1], lam.z + pen.z * err[2]};
-        const F3 f = project_contact(trial, friction);
-        const F3 sc = stiffness_scales(trial, friction);
+        F3 f, sc;
+        project_with_scales(trial, friction, f, sc);
         float forces[3] = {f.n, f.t0, f.t1};
         if (phase != 0) {
-            V3 t0, t1;
-            basis(v3(d.c_n[c]), t0, t1);
-            const V3 af = v3(d.c_accf[c]);
-            forces[0] = f.n - lam.w / dt;
-            forces[1] = f.t0 - dot(af, t0) / dt;
-            forces[2] = f.t1 - dot(af, t1) / dt;
+            const float4 fo = d.c_foff[c];
+            forces[0] = f.n - fo.x;
+            forces[1] = f.t0 - fo.y;
+            forces[2] = f.t1 - fo.z;
         }
         const float st[3] = {pen.x * sc.n, pen.y * sc.t0, pen.z * sc.t1};
 #pragma unroll

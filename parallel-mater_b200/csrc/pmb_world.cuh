@@ -237,6 +237,10 @@ struct Dev {
     uint2* c_bodies;  // (a, b) of the contact's pair
     float4* c_jac;    // 9 per contact: jacobian rows n,t0,t1 of body a then body b
     float4 *c_n, *c_p, *c_e, *c_aa, *c_ab, *c_lam, *c_pen, *c_accf;
+    // Velocity phase: per contact the force offsets of its rows (lambda.w /
+    // dt, and the accumulated friction along each tangent / dt), fixed for
+    // the phase and formed once with its jacobians.
+    float4* c_foff;
     // contact cache from the previous tick (double-buffered by the host)
     uint64_t* sv_code;
     uint32_t *sv_off, *sv_cnt;
@@ -400,7 +404,7 @@ inline int solve_features(const Dev& d) { return (d.nj ? kFeatJoints : 0) | (d.s
 SolveVariant solve_group_variant_512();
 SolveVariant solve_group_variant_384();
 SolveVariant solve_group_variant_256();
-void launch_contact_jacobians(const Dev& d, uint32_t phase, cudaStream_t s);
+void launch_contact_jacobians(const Dev& d, uint32_t phase, float dt, cudaStream_t s);
 // Sparse per-body record writes staged in io_index / io_rec (kind 0: inputs,
 // 1: kinematic targets, 2: states), and AoS state packing into `dst`.
 void launch_scatter_records(const Dev& d, uint32_t kind, uint32_t count, cudaStream_t s);
