@@ -338,6 +338,7 @@ int allocate_world(pmb_world* w, Dev& d, const Sizes& z, Extra& e) {
     ALLOC(d.c_n, cap_contact); ALLOC(d.c_p, cap_contact); ALLOC(d.c_e, cap_contact);
     ALLOC(d.c_aa, cap_contact); ALLOC(d.c_ab, cap_contact); ALLOC(d.c_lam, cap_contact);
     ALLOC(d.c_pen, cap_contact); ALLOC(d.c_accf, cap_contact); ALLOC(d.c_foff, cap_contact);
+    ALLOC(d.c_mub, cap_contact);
     for (int side = 0; side < 2; ++side) {
         uint64_t** code = side ? &d.out_code : &d.sv_code;
         uint32_t** off = side ? &d.out_off : &d.sv_off;

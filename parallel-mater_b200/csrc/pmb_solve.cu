@@ -14,10 +14,11 @@
 
 namespace pmb {
 
-// The velocity phase also forms each contact's force offsets (the row
-// forces are the projected trial forces less them): the normal impulse and
-// the accumulated friction of the position phase, both fixed by then
-// (k_contact_finalize), over dt.
+// The position phase also forms each contact's friction and penalty growth
+// factor (c_mub, from its bodies' materials and masses); the velocity phase
+// its force offsets (the row forces are the projected trial forces less
+// them): the normal impulse and the accumulated friction of the position
+// phase, both fixed by then (k_contact_finalize), over dt.
 __global__ void k_contact_jacobians(Dev d, uint32_t phase, float dt) {
     if (phase != 0 && d.ctr->impact == 0) return;
     const uint32_t n_con = d.ctr->n_contacts;
@@ -37,7 +38,12 @@ __global__ void k_contact_jacobians(Dev d, uint32_t phase, float dt) {
         float4* p = d.c_jac + size_t(c) * 9;
 #pragma unroll
         for (int k = 0; k < 9; ++k) p[k] = make_float4(f[4 * k], f[4 * k + 1], f[4 * k + 2], f[4 * k + 3]);
-        if (phase != 0) {
+        if (phase == 0) {
+            const uint32_t a = ab.x, b = ab.y;
+            const float friction = sqrtf(d.p1[a].x * d.p1[b].x);
+            const float beta = (1.0f / (fmx(d.p0[a].x + d.p0[b].x, 1.0e-6f) * dt * dt)) * 100.0f;
+            d.c_mub[c] = make_float2(friction, beta);
+        } else {
             V3 t0, t1;
             basis(v3(d.c_n[c]), t0, t1);
             const V3 af = v3(d.c_accf[c]);
@@ -95,7 +101,7 @@ enum : uint32_t {
 static_assert(sizeof(GroupRows<32>) <= size_t(kStageRows) * kRowWords * 4, "oversized-body rows fit the stage");
 constexpr uint32_t kStagedGroups = 64;  // lane groups per CTA at most (512 threads, 8 lanes)
 constexpr size_t kStagedSmem =
-    size_t(kStageRows) * kRowWords * 4 + size_t(kBatchBodies) * 12 * 4 + 64 * 4 + kStagedGroups * sizeof(Blk) +
+    size_t(kStageRows) * kRowWords * 4 + size_t(kBatchBodies) * 10 * 4 + 64 * 4 + kStagedGroups * sizeof(Blk) +
     kStagedGroups * 2 * sizeof(BodyView);
 
 struct StageTables {
@@ -104,8 +110,6 @@ struct StageTables {
     uint32_t* skip;    // per batch slot: 1 = not solved this sweep (impact phase, finished scene)
     uint32_t* off;     // kBatchBodies + 1 row offsets
     float* dx;         // per batch slot: displacement (6)
-    float* fric;       // per batch slot: friction
-    float* invm;       // per batch slot: inverse mass
     uint32_t* scratch; // 64 words for scans and counts
     Blk* jblk;         // per lane group: the block while joint rows are added
     BodyView* jview;   // per lane group: the visited joint's two bodies
@@ -118,9 +122,7 @@ __device__ __forceinline__ StageTables stage_tables(uint8_t* raw) {
     t.skip = u + kBatchBodies;
     t.off = u + 2 * kBatchBodies;            // kBatchBodies + 1 (one word of slack)
     t.dx = reinterpret_cast<float*>(u + 3 * kBatchBodies + 1);
-    t.fric = t.dx + 6 * kBatchBodies;
-    t.invm = t.fric + kBatchBodies;
-    t.scratch = reinterpret_cast<uint32_t*>(t.invm + kBatchBodies);
+    t.scratch = reinterpret_cast<uint32_t*>(t.dx + 6 * kBatchBodies);
     t.jblk = reinterpret_cast<Blk*>(t.scratch + 64);
     t.jview = reinterpret_cast<BodyView*>(t.jblk + kStagedGroups);
     return t;
@@ -138,14 +140,12 @@ __device__ __forceinline__ void stage_row(const Dev& d, const StageTables& tb, u
 #pragma unroll
     for (int k = 0; k < 6; ++k) me.v[k] = tb.dx[6 * sl + k];
     const Lite o = load_lite(d, other);
-    const float of = d.p1[other].x, om = d.p0[other].x;
     const uint32_t ocol = d.color[other];
     const float4 lam = d.c_lam[c], pen = d.c_pen[c], e = d.c_e[c];
     V6 ja[3], jb[3];
     load_jac(d, c, ja, jb);
-    const float mf = tb.fric[sl], mm = tb.invm[sl];
-    const float friction = sqrtf(first ? mf * of : of * mf);
-    const float beta = (1.0f / (fmx(first ? mm + om : om + mm, 1.0e-6f) * dt * dt)) * 100.0f;
+    const float2 mub = d.c_mub[c];
+    const float friction = mub.x, beta = mub.y;
     const float e3[3] = {e.x, e.y, e.z};
     float err[3], pre[3], post[3];
 #pragma unroll
@@ -505,8 +505,6 @@ __global__ void __launch_bounds__(T, 1) k_solve_staged(Dev d, StepParams sp, uin
                         dx[3] = a.x;
                         dx[4] = a.y;
                         dx[5] = a.z;
-                        tb.fric[threadIdx.x] = d.p1[i].x;
-                        tb.invm[threadIdx.x] = d.p0[i].x;
                     }
                     // Inclusive scan of the slots' row counts (T >= kBatchBodies).
                     uint32_t x = cnt;

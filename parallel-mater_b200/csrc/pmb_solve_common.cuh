@@ -246,7 +246,7 @@ struct RawContact {
     uint32_t c;
     bool first;
     Lite other;
-    float of;  // the other body's friction
+    float2 mub;  // the pair's friction and penalty growth factor
     float4 lam, pen, e;
     V6 ja[3], jb[3];
 };
@@ -255,7 +255,7 @@ __device__ __forceinline__ RawContact load_contact(const Dev& d, uint32_t code, 
     r.c = code & 0x7fffffffu;
     r.first = (code >> 31) == 0;
     r.other = load_lite(d, other_body);
-    r.of = d.p1[other_body].x;
+    r.mub = d.c_mub[r.c];
     r.lam = d.c_lam[r.c];
     r.pen = d.c_pen[r.c];
     r.e = d.c_e[r.c];
@@ -266,14 +266,13 @@ __device__ __forceinline__ RawContact load_contact(const Dev& d, uint32_t code, 
 // Rows of one contact for body i into chunk slot `slot`; its normal row,
 // raw penalty and normal trial also go to nrow[nslot].
 template <int G>
-__device__ __forceinline__ void stage_loaded(const Dev& d, const Lite& me, float my_friction, const RawContact& rc,
+__device__ __forceinline__ void stage_loaded(const Dev& d, const Lite& me, const RawContact& rc,
                                              uint32_t phase, float dt, GroupRows<G>& sm, int slot, int nslot) {
     const uint32_t c = rc.c;
     const bool first = rc.first;
     const Lite A = first ? me : rc.other;  // values, not run-time references (no local copies)
     const Lite B = first ? rc.other : me;
-    const float of = rc.of;
-    const float friction = sqrtf(first ? my_friction * of : of * my_friction);
+    const float friction = rc.mub.x;
     const float4 lam = rc.lam, pen = rc.pen;
     V6 ja[3], jb[3];
     float err[3];
@@ -322,10 +321,10 @@ __device__ __forceinline__ void stage_loaded(const Dev& d, const Lite& me, float
     }
 }
 template <int G>
-__device__ __forceinline__ void stage_contact(const Dev& d, const Lite& me, float my_friction, uint32_t code,
+__device__ __forceinline__ void stage_contact(const Dev& d, const Lite& me, uint32_t code,
                                               uint32_t other_body, uint32_t phase, float dt, GroupRows<G>& sm,
                                               int slot, int nslot) {
-    stage_loaded<G>(d, me, my_friction, load_contact(d, code, other_body), phase, dt, sm, slot, nslot);
+    stage_loaded<G>(d, me, load_contact(d, code, other_body), phase, dt, sm, slot, nslot);
 }
 
 // The body a lane group solves next in its colour, fetched while the current
@@ -412,7 +411,6 @@ __device__ void solve_body_group(const Dev& d, Ahead& ah, uint32_t kn, uint32_t 
     uint4 nrec = make_uint4(0u, 0u, 0u, 0u);
     if (kn != ~0u) nrec = d.crec[kn];
     const Lite me = load_lite(d, i);
-    const float my_friction = d.p1[i].x;
     float ent[Owned<G>::E];
     const float4 ia = d.inA[i], ib = d.inB[i];
     // The block's starting entries: inertia and its gradient. Formed after
@@ -454,7 +452,7 @@ __device__ void solve_body_group(const Dev& d, Ahead& ah, uint32_t kn, uint32_t 
             const int nslot = sidx < GroupRows<G>::kSlots ? int(sidx) : -1;
             const uint32_t code = base == 0 ? code0 : base == uint32_t(G) ? code1 : d.blist[ro + sidx];
             const uint32_t other = base == 0 ? other0 : base == uint32_t(G) ? other1 : d.bother[ro + sidx];
-            stage_contact<G>(d, me, my_friction, code, other, phase, dt, sm, gl, nslot);
+            stage_contact<G>(d, me, code, other, phase, dt, sm, gl, nslot);
         }
         if (base == 0) init_entries();
         __syncwarp(gmask);
@@ -485,7 +483,7 @@ __device__ void solve_body_group(const Dev& d, Ahead& ah, uint32_t kn, uint32_t 
         const uint32_t sidx = base + gl;
         constexpr uint32_t kSlots = GroupRows<G>::kSlots;
         if (rn > kSlots && base >= kSlots && sidx < rn)
-            stage_contact<G>(d, me, my_friction, d.blist[ro + sidx], d.bother[ro + sidx], phase, dt, sm, -1,
+            stage_contact<G>(d, me, d.blist[ro + sidx], d.bother[ro + sidx], phase, dt, sm, -1,
                              int(sidx % kSlots));
         __syncwarp(gmask);
         uint32_t flag = 0;
@@ -549,7 +547,6 @@ __device__ __forceinline__ void load_normal_rows(const Dev& d, uint32_t c, V6& j
 template <bool Joints>
 __device__ void solve_body_thread(const Dev& d, uint32_t i, uint32_t phase, float dt, Blk* sb, BodyView* views) {
     const Lite me = load_lite(d, i);
-    const float my_friction = d.p1[i].x;
     const uint32_t ro = d.roff[i], rn = d.rcount[i];
     Blk blk;
     {
@@ -579,8 +576,7 @@ __device__ void solve_body_thread(const Dev& d, uint32_t i, uint32_t phase, floa
         const bool first = (code >> 31) == 0;
         const Lite other = load_lite(d, other_body);
         const Lite A = first ? me : other, B = first ? other : me;
-        const float of = d.p1[other_body].x;
-        const float friction = sqrtf(first ? my_friction * of : of * my_friction);
+        const float friction = d.c_mub[c].x;
         const float4 lam = d.c_lam[c], pen = d.c_pen[c];
         V6 ja[3], jb[3];
         float err[3];
@@ -710,8 +706,8 @@ static __device__ void dual_contact(const Dev& d, uint32_t c, uint2 ab, float dt
         scene_last = phase == 0 && it + 1 == budget;  // the tick's residual is the pose phase's
     }
     const Lite A = load_lite(d, a), B = load_lite(d, b);
-    const float friction = sqrtf(d.p1[a].x * d.p1[b].x);
-    const float beta = (1.0f / (fmx(d.p0[a].x + d.p0[b].x, 1.0e-6f) * dt * dt)) * 100.0f;
+    const float2 mub = d.c_mub[c];
+    const float friction = mub.x, beta = mub.y;
     float4 lam = d.c_lam[c], pen = d.c_pen[c];
     V6 ja[3], jb[3];
     float err[3];

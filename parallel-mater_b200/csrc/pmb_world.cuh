@@ -241,6 +241,10 @@ struct Dev {
     // dt, and the accumulated friction along each tangent / dt), fixed for
     // the phase and formed once with its jacobians.
     float4* c_foff;
+    // Per contact, fixed for the tick: friction sqrt(mu_a mu_b) and the
+    // penalty growth factor 100 / (max(w_a + w_b, 1e-6) dt^2) of its pair,
+    // formed with the position phase's jacobians.
+    float2* c_mub;
     // contact cache from the previous tick (double-buffered by the host)
     uint64_t* sv_code;
     uint32_t *sv_off, *sv_cnt;
