@@ -115,7 +115,6 @@ template <int G> struct GroupRowsData {
     // per entry.
     float r[G][kSlotWords];
     float nrow[kSlots][9];  // normal row: jacobian[6], raw penalty, trial force (and a pad word)
-    uint32_t flag[G];
     Blk jblk;            // the block while joint rows are added (joint_rows_shared)
     BodyView jview[2];   // the joint's two bodies during its visit
 };
@@ -220,9 +219,20 @@ __device__ __forceinline__ void accumulate_chunk(float* ent, int gl, const Group
     }
 }
 
+// Whether a staged normal row's trial force crosses zero under the update
+// (geometry_constraints_solve.slang:433-475).
+__device__ __forceinline__ bool crosses(const float* row, const V6& upd) {
+    V6 nr;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) nr.v[k] = row[k];
+    const float k0 = row[6], trial = row[7];
+    return trial <= 0.0f && trial + k0 * dot6(nr, upd) > k0 * 1.0e-6f;
+}
+// Adds the crossing rows of a chunk (bit t of `mask`: row s0 + t) to the
+// lane's entries, rows in list order.
 template <int G>
 __device__ __forceinline__ void accumulate_crossing(float* ent, int gl, const GroupRows<G>& sm, uint32_t s0,
-                                                    uint32_t m) {
+                                                    uint32_t m, uint32_t mask) {
 #pragma unroll
     for (int q = 0; q < Owned<G>::E; ++q) {
         const int e = gl + G * q;
@@ -230,7 +240,7 @@ __device__ __forceinline__ void accumulate_crossing(float* ent, int gl, const Gr
         int ei = 0, ek = 0;
         if (e < 21) entry_ik(e, ei, ek);
         for (uint32_t t = 0; t < m; ++t) {
-            if (!sm.flag[t]) continue;
+            if (!((mask >> t) & 1u)) continue;
             const float* row = sm.nrow[(s0 + t) % GroupRows<G>::kSlots];
             if (e < 21) ent[q] += row[6] * row[ei] * row[ek];
             else ent[q] += row[e - 21] * row[7];
@@ -476,32 +486,30 @@ __device__ void solve_body_group(const Dev& d, Ahead& ah, uint32_t kn, uint32_t 
     V6 upd;
     if (!block_solve(blk, upd)) return;
     mark(2);
-    // Crossing safeguard (geometry_constraints_solve.slang:433-475).
+    // Crossing safeguard (geometry_constraints_solve.slang:433-475): a
+    // ballot per chunk flags the rows; rows past the kept normal rows are
+    // evaluated again into the slots. (Reloading the entries from the block
+    // keeps them out of registers during the factorisation: keeping them
+    // live instead, when no joint rows changed the block, was slower.)
     own_entries<G>(blk, gl, ent);
+    constexpr uint32_t kSlots = GroupRows<G>::kSlots;
+    constexpr uint32_t kLanes = G == 32 ? 0xffffffffu : (1u << G) - 1u;
     bool crossing = false;
     for (uint32_t base = 0; base < rn; base += G) {
         const uint32_t sidx = base + gl;
-        constexpr uint32_t kSlots = GroupRows<G>::kSlots;
-        if (rn > kSlots && base >= kSlots && sidx < rn)
-            stage_contact<G>(d, me, d.blist[ro + sidx], d.bother[ro + sidx], phase, dt, sm, -1,
-                             int(sidx % kSlots));
-        __syncwarp(gmask);
-        uint32_t flag = 0;
-        if (sidx < rn) {
-            const float* row = sm.nrow[sidx % kSlots];
-            V6 nr;
-#pragma unroll
-            for (int k = 0; k < 6; ++k) nr.v[k] = row[k];
-            const float k0 = row[6], trial = row[7];
-            flag = (trial <= 0.0f && trial + k0 * dot6(nr, upd) > k0 * 1.0e-6f) ? 1u : 0u;
+        if (base >= kSlots) {
+            __syncwarp(gmask);  // the slots' previous rows are read
+            if (sidx < rn)
+                stage_contact<G>(d, me, d.blist[ro + sidx], d.bother[ro + sidx], phase, dt, sm, -1,
+                                 int(sidx % kSlots));
+            __syncwarp(gmask);
         }
-        sm.flag[gl] = flag;
-        __syncwarp(gmask);
-        if (__any_sync(gmask, flag)) {
+        const bool f = sidx < rn && crosses(sm.nrow[sidx % kSlots], upd);
+        const uint32_t m = (__ballot_sync(gmask, f) >> gbase) & kLanes;
+        if (m) {
             crossing = true;
-            accumulate_crossing<G>(ent, gl, sm, base % kSlots, min(uint32_t(G), rn - base));
+            accumulate_crossing<G>(ent, gl, sm, base % kSlots, min(uint32_t(G), rn - base), m);
         }
-        __syncwarp(gmask);
     }
     mark(3);
     if (crossing) {
