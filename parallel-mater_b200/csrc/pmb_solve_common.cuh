@@ -426,32 +426,60 @@ __device__ void solve_body_group(const Dev& d, Ahead& ah, uint32_t kn, uint32_t 
     // The block's starting entries: inertia and its gradient. Formed after
     // the first chunk's rows are requested, so those loads and this body's
     // own state are in flight together.
+    // The inertia block H is zero outside the linear diagonal and the
+    // angular 3x3. Its gradient H dx is the serial sum over c = 0..5 from +0;
+    // with dx finite, the sum's zero terms (0 x dx[c], exact zeros) leave
+    // every partial sum unchanged (it is never -0), so each sum reduces to
+    // its nonzero terms in order, bit for bit; a non-finite dx (0 x inf is
+    // NaN) takes the full sums. All indices are compile-time (a lane's entry
+    // picks its value by comparison), so nothing goes to local memory.
     auto init_entries = [&] {
-        float H[21];
+        const V6& x = me.dx;
+        bool finite = true;
 #pragma unroll
-        for (int k = 0; k < 21; ++k) H[k] = 0.0f;
-        H[bidx(0, 0)] = ia.x;
-        H[bidx(1, 1)] = ia.x;
-        H[bidx(2, 2)] = ia.x;
-        H[bidx(3, 3)] = ia.y;
-        H[bidx(4, 3)] = ia.z;
-        H[bidx(5, 3)] = ib.x;
-        H[bidx(4, 4)] = ia.w;
-        H[bidx(5, 4)] = ib.y;
-        H[bidx(5, 5)] = ib.z;
+        for (int c = 0; c < 6; ++c) finite = finite && fab(x.v[c]) < kFltMax;
+        float gr[6];
+        if (finite) {
+            gr[0] = 0.0f + ia.x * x.v[0];
+            gr[1] = 0.0f + ia.x * x.v[1];
+            gr[2] = 0.0f + ia.x * x.v[2];
+            gr[3] = ((0.0f + ia.y * x.v[3]) + ia.z * x.v[4]) + ib.x * x.v[5];
+            gr[4] = ((0.0f + ia.z * x.v[3]) + ia.w * x.v[4]) + ib.y * x.v[5];
+            gr[5] = ((0.0f + ib.x * x.v[3]) + ib.y * x.v[4]) + ib.z * x.v[5];
+        } else {
+            float H[21];
+#pragma unroll
+            for (int k = 0; k < 21; ++k) H[k] = 0.0f;
+            H[bidx(0, 0)] = ia.x;
+            H[bidx(1, 1)] = ia.x;
+            H[bidx(2, 2)] = ia.x;
+            H[bidx(3, 3)] = ia.y;
+            H[bidx(4, 3)] = ia.z;
+            H[bidx(5, 3)] = ib.x;
+            H[bidx(4, 4)] = ia.w;
+            H[bidx(5, 4)] = ib.y;
+            H[bidx(5, 5)] = ib.z;
+#pragma unroll
+            for (int r = 0; r < 6; ++r) {
+                float gs = 0.0f;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) gs += H[bidx(r, c)] * x.v[c];
+                gr[r] = gs;
+            }
+        }
 #pragma unroll
         for (int q = 0; q < Owned<G>::E; ++q) {
             const int e = gl + G * q;
             float v = 0.0f;
+            v = (e == int(bidx(0, 0)) || e == int(bidx(1, 1)) || e == int(bidx(2, 2))) ? ia.x : v;
+            v = e == int(bidx(3, 3)) ? ia.y : v;
+            v = e == int(bidx(4, 3)) ? ia.z : v;
+            v = e == int(bidx(5, 3)) ? ib.x : v;
+            v = e == int(bidx(4, 4)) ? ia.w : v;
+            v = e == int(bidx(5, 4)) ? ib.y : v;
+            v = e == int(bidx(5, 5)) ? ib.z : v;
 #pragma unroll
-            for (int k = 0; k < 21; ++k) v = e == k ? H[k] : v;
-            if (e >= 21 && e < 27) {
-                const int r = e - 21;
-                float gs = 0.0f;
-#pragma unroll
-                for (int c = 0; c < 6; ++c) gs += H[bidx(r, c)] * me.dx.v[c];
-                v = gs;
-            }
+            for (int r = 0; r < 6; ++r) v = e == 21 + r ? gr[r] : v;
             ent[q] = v;
         }
     };
