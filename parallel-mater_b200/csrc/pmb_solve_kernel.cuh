@@ -30,7 +30,7 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
     uint8_t* warp_stage = stage_raw + (threadIdx.x >> 5) * kWarpStage;
     const uint32_t nthreads = gridDim.x * kSolveThreads;
     const float dt = sp.dt;
-    const uint32_t colors = c->colors;
+    const uint32_t colors = min(c->colors, kMaxColors);  // the colouring never exceeds kMaxColors
     uint32_t budget = sp.budget_request;
     if (!sp.realtime && sp.requested == 0) budget = max(budget, c->joint_iters);
     if (phase != 0 && sp.tolerance > 0.0f) budget = c->budget;
@@ -50,11 +50,50 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
         return t;
     };
     if (timing && blockIdx.x == 0 && threadIdx.x == 0) c->dbg_start = now();
+    using W32 = std::integral_constant<int, 32>;
+    using W16 = std::integral_constant<int, 16>;
+    using W8 = std::integral_constant<int, 8>;
+    // Each colour's body ranges, read once per launch: its first body, the
+    // starts of its 16-lane and 8-lane sort classes, its end.
+    __shared__ uint4 s_col[kMaxColors];
+    for (uint32_t k = threadIdx.x; k < colors; k += kSolveThreads) {
+        const uint32_t* off = c->color_off + k * kSortClasses;
+        s_col[k] = make_uint4(off[0], off[kClass16], off[kClass8], off[kSortClasses]);
+    }
+    __syncthreads();
+    // Lane widths of a colour (see the group-per-body comment): policy 0
+    // (and 3) one width per colour by its size, 1 eight lanes, 2 a width per
+    // body class (heaviest first) unless 32-lane groups cover the colour, 4
+    // a body per thread when the colour has more bodies than 16-lane groups
+    // could take in one round. Bodies [b0, r32) take 32 lanes, [r32, r16)
+    // 16, [r16, r8) 8.
+    struct Ranges {
+        uint32_t b0, r32, r16, r8, b1;
+        bool per_thread;
+    };
+    auto ranges = [&](uint32_t col) {
+        const uint4 o = s_col[col];
+        const uint32_t b0 = o.x, b1 = o.w, nb = b1 - b0;
+        Ranges r{b0, b0, b0, b0, b1, false};
+        if constexpr (kThread) r.per_thread = d.solve_policy == 4 && nb * 16u > nthreads;
+        if (r.per_thread) {
+        } else if (d.solve_policy != 1 && nb * 32u <= nthreads) {
+            r.r32 = r.r16 = r.r8 = b1;
+        } else if (d.solve_policy == 2) {
+            r.r32 = o.y;
+            r.r16 = o.z;
+            r.r8 = b1;
+        } else if ((d.solve_policy == 0 || d.solve_policy >= 3) && nb * 16u <= nthreads) {
+            r.r16 = r.r8 = b1;
+        } else {
+            r.r8 = b1;
+        }
+        return r;
+    };
     for (uint32_t it = 0; it < iters; ++it) {
         for (uint32_t col = 0; col < colors; ++col) {
-            const uint32_t* off = c->color_off + col * kSortClasses;
-            const uint32_t b0 = off[0], b1 = off[kSortClasses];
-            const uint32_t nb = b1 - b0;
+            const Ranges rg = ranges(col);
+            const uint32_t b0 = rg.b0, b1 = rg.b1;
             const uint32_t trace = !timing || it != 0 ? 0u : col + 1 == colors ? 1u : col == 0 ? 2u : 0u;
             // Bodies [lo, hi) with G lanes each. Consecutive bodies go to
             // consecutive CTAs (group rank = local group x grid + CTA), so the
@@ -113,19 +152,9 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
                 }
                 __syncwarp();
             };
-            using W32 = std::integral_constant<int, 32>;
-            using W16 = std::integral_constant<int, 16>;
-            using W8 = std::integral_constant<int, 8>;
-            // Widths (see the group-per-body comment): policy 0 (and 3) one
-            // width per colour by its size, 1 eight lanes, 2 a width per body
-            // class (heaviest first) unless 32-lane groups cover the colour.
-            uint32_t r32 = b0, r16 = b0, r8 = b0;  // 32 lanes [b0, r32), 16 [r32, r16), 8 [r16, r8)
-            bool per_thread = false;
-            if constexpr (kThread) per_thread = d.solve_policy == 4 && nb * 16u > nthreads;
-            if (per_thread) {
-                // A body per thread: the colour has more bodies than 16-lane
-                // groups could take in one round. Consecutive bodies go to
-                // consecutive CTAs, as for the groups.
+            if (rg.per_thread) {
+                // A body per thread. Consecutive bodies go to consecutive
+                // CTAs, as for the groups.
                 if constexpr (kThread) {
                     Blk* slot = reinterpret_cast<Blk*>(warp_stage) + lane;
                     BodyView* views = reinterpret_cast<BodyView*>(warp_stage + kThreadViews) + 2 * lane;
@@ -136,21 +165,10 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
                         solve_body_thread<kJoints>(d, i, phase, dt, slot, views);
                     }
                 }
-                r32 = r16 = r8 = b0;
-            } else if (d.solve_policy != 1 && nb * 32u <= nthreads) {
-                r32 = r16 = r8 = b1;
-            } else if (d.solve_policy == 2) {
-                r32 = off[kClass16];
-                r16 = off[kClass8];
-                r8 = b1;
-            } else if ((d.solve_policy == 0 || d.solve_policy >= 3) && nb * 16u <= nthreads) {
-                r16 = r8 = b1;
-            } else {
-                r8 = b1;
             }
-            sweep(W32{}, b0, r32);
-            sweep(W16{}, r32, r16);
-            sweep(W8{}, r16, r8);
+            sweep(W32{}, b0, rg.r32);
+            sweep(W16{}, rg.r32, rg.r16);
+            sweep(W8{}, rg.r16, rg.r8);
             if (timing && it == 0 && col < 18) {
                 __syncthreads();
                 if (threadIdx.x == 0) atomicMax(&c->dbg_work[col], now());
