@@ -63,20 +63,22 @@ __device__ __forceinline__ void contact_rows(const Dev& d, uint32_t c, float4 e,
     for (int k = 0; k < 3; ++k) err[k] = e3[k] + dot6(ja[k], A.dx) + dot6(jb[k], B.dx);
 }
 
-__device__ __forceinline__ void apply_pose_update(const Dev& d, uint32_t i, const V6& u) {
-    float4 l = d.dxl[i];
+__device__ __forceinline__ void apply_pose_update(const Dev& d, uint32_t i, const V6& u, float4 l, float4 dq) {
     l.x += u.v[0];
     l.y += u.v[1];
     l.z += u.v[2];
     d.dxl[i] = l;
     V3 r{u.v[3], u.v[4], u.v[5]};
     if (r.x == 0.0f && r.y == 0.0f && r.z == 0.0f) return;
-    Q4 rel = q4(d.dq[i]);
+    Q4 rel = q4(dq);
     Q4 dd = qmul(Q4{r.x, r.y, r.z, 0.0f}, rel);
     rel = qnormalize(Q4{rel.x + 0.5f * dd.x, rel.y + 0.5f * dd.y, rel.z + 0.5f * dd.z, rel.w + 0.5f * dd.w});
     if (rel.w < 0.0f) rel = {-rel.x, -rel.y, -rel.z, -rel.w};
     d.dq[i] = f4(rel);
     d.dxa[i] = make_float4(2.0f * rel.x, 2.0f * rel.y, 2.0f * rel.z, 0.0f);
+}
+__device__ __forceinline__ void apply_pose_update(const Dev& d, uint32_t i, const V6& u) {
+    apply_pose_update(d, i, u, d.dxl[i], d.dq[i]);
 }
 
 // Group-per-body primal: G lanes (G = 8, 16 or 32) solve one body. Lanes
@@ -514,6 +516,10 @@ __device__ void solve_body_group(const Dev& d, Ahead& ah, uint32_t kn, uint32_t 
     V6 upd;
     if (!block_solve(blk, upd)) return;
     mark(2);
+    // The body's rotation offset, read while the safeguard runs (only this
+    // group writes it in the colour), so the update at the end waits on no
+    // load; its displacement is `me` (read at the start; both w are 0).
+    const float4 dq_start = phase == 0 ? d.dq[i] : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
     // Crossing safeguard (geometry_constraints_solve.slang:433-475): a
     // ballot per chunk flags the rows; rows past the kept normal rows are
     // evaluated again into the slots. (Reloading the entries from the block
@@ -552,10 +558,11 @@ __device__ void solve_body_group(const Dev& d, Ahead& ah, uint32_t kn, uint32_t 
         atomicAdd(&d.ctr->dbg_sum[7], (unsigned long long)rn);
     }
     if (gl == 0) {
+        float4 l = make_float4(me.dx.v[0], me.dx.v[1], me.dx.v[2], 0.0f);
         if (phase == 0) {
-            apply_pose_update(d, i, upd);
+            apply_pose_update(d, i, upd, l, dq_start);
         } else {
-            float4 l = d.dxl[i], a = d.dxa[i];
+            float4 a = make_float4(me.dx.v[3], me.dx.v[4], me.dx.v[5], 0.0f);
             l.x += upd.v[0];
             l.y += upd.v[1];
             l.z += upd.v[2];
