@@ -523,7 +523,7 @@ __global__ void k_color_scatter(Dev d) {
         const uint32_t b = d.color[i] * kSortClasses + sort_class(d.rcount[i]);
         const uint32_t slot = d.ctr->color_off[b] + atomicAdd(&d.ctr->color_count[b], 1u);
         d.corder[slot] = i;
-        d.crec[slot] = make_uint4(i, d.roff[i], d.rcount[i], 0u);
+        d.crec[slot] = make_uint4(i, d.roff[i], d.rcount[i], d.impact[i]);
     }
 }
 

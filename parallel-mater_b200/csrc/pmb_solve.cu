@@ -537,7 +537,7 @@ __global__ void __launch_bounds__(T, 1) k_solve_staged(Dev d, StepParams sp, uin
                             const uint32_t i = tb.body[0];
                             if (!tb.skip[0]) {
                                 GroupRows<32>& sm = *reinterpret_cast<GroupRows<32>*>(tb.rows);
-                                Ahead ah{i, d.roff[i], d.rcount[i], 0u, 0u, 0u, 0u};
+                                Ahead ah{i, d.roff[i], d.rcount[i], 0u, 0u, 0u, 0u, d.impact[i]};
                                 fetch_codes<32>(d, ah, lane);
                                 solve_body_group<32, true>(d, ah, ~0u, phase, dt, sm, 0xffffffffu, lane, 0, 0u);
                                 __syncwarp();

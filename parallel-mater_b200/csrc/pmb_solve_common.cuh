@@ -346,6 +346,7 @@ __device__ __forceinline__ void stage_contact(const Dev& d, const Lite& me, uint
 struct Ahead {
     uint32_t i, ro, rn;
     uint32_t code0, other0, code1, other1;
+    uint32_t impact;  // the body's impact flag (the velocity phase solves impacted bodies only)
 };
 template <int G>
 __device__ __forceinline__ void fetch_codes(const Dev& d, Ahead& a, int gl) {
@@ -358,7 +359,7 @@ __device__ __forceinline__ void fetch_codes(const Dev& d, Ahead& a, int gl) {
 template <int G>
 __device__ __forceinline__ Ahead fetch_ahead(const Dev& d, uint32_t k, int gl) {
     const uint4 r = d.crec[k];
-    Ahead a{r.x, r.y, r.z, 0u, 0u, 0u, 0u};
+    Ahead a{r.x, r.y, r.z, 0u, 0u, 0u, 0u, r.w};
     fetch_codes<G>(d, a, gl);
     return a;
 }
@@ -504,6 +505,7 @@ __device__ void solve_body_group(const Dev& d, Ahead& ah, uint32_t kn, uint32_t 
         ah.i = nrec.x;
         ah.ro = nrec.y;
         ah.rn = nrec.z;
+        ah.impact = nrec.w;
         fetch_codes<G>(d, ah, gl);
     }
     mark(0);

@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(T, 1) k_solve(Dev d, StepParams sp, uint32_t p
                     }
                     const uint32_t kn = next < hi ? next : ~0u;
                     const uint32_t i = ah.i;
-                    const bool skip = (phase != 0 && d.impact[i] == 0) ||
+                    const bool skip = (phase != 0 && ah.impact == 0) ||
                                       (batched(d) && it >= d.scene_budget[d.scene_of[i]]);
                     if (skip) {
                         if (kn != ~0u) ah = fetch_ahead<G>(d, kn, gl);

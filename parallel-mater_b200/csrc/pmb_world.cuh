@@ -259,7 +259,7 @@ struct Dev {
     uint32_t *deg, *inc_off, *inc_cursor, *inc_list;
     uint32_t *jdeg, *jinc_off, *jinc_cursor, *jinc_list;
     uint32_t* corder;
-    uint4* crec;  // per colour-order slot: body, row offset, row count (the solve's body records)
+    uint4* crec;  // per colour-order slot: body, row offset, row count, impact flag (the solve's body records)
     uint8_t* cdirty;  // colour rounds: two flag arrays of n (bodies to revisit)
     uint32_t *nbr, *nlow, *nhigh;  // dynamic neighbours per body (k_neighbour_lists)
     ContactEvent* events;
